@@ -1,0 +1,309 @@
+"""Benchmark of the Voronoi SPP timestep on B200 (cell-steps/s).
+
+Workload (default): the single large monolayer -- N = 262144 cells, periodic box 512 x 512, seeded
+uniform positions, A0 = 1, p0 = 3.8, KA = KP = 1, v0 = 0.1, Dr = 1, dt = 0.01, SPP dynamics with a
+Delaunay test/repair every step. Synthetic seeded data (the reference ships no dataset).
+
+A "step" = one full timestep of the whole monolayer: fused geometry + forces + exact Delaunay test,
+local repair, SPP integrate + move. The L2 (126 MB) is flushed (a 256 MB write) between timed steps.
+Timing: CUDA events on the system's stream around each step, max over ranks.
+
+--impl reference: the reference's CPU path on this host (oracle/_ref build of the reference's own
+sources when present, else the oracle port), bounded sample of the same workload.
+Multi-GPU: independent replicas, one per rank (weak scaling; the path has no exchange step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-steps/s batched vs plain on 1 B200 at ≤1e-6 force err; p50/p99 latency"
+N_CELLS = 262144
+BOX = 512.0
+P0, V0, DR, DT, MU = 3.8, 0.1, 1.0, 0.01, 1.0
+# compulsory bytes of the fused geometry+force(+test) pass per cell: R pos 16, nn 4, nbr 24 (z=6),
+# A0/P0 16; W A/P 16, F 16
+FORCE_PASS_BYTES = 92
+L2_FLUSH_BYTES = 256 << 20
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks sampled during the timed region."""
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_system(cg, torch, stream, precision, n_cells=N_CELLS, box=BOX, seed=1):
+    b = cg.VoronoiBatch([n_cells], [(box, box)], K=16, precision=precision)
+    rng = np.random.default_rng(seed)
+    b.set_positions(rng.random((n_cells, 2)) * box)
+    b.set_directors(rng.uniform(0, 2 * np.pi, n_cells))
+    b.set_motility(np.tile([V0, DR], (n_cells, 1)))
+    b.set_preferences(np.tile([1.0, P0], (n_cells, 1)))
+    b.set_seed(seed)
+    b._lib.cg_set_stream(b.handle, stream.cuda_stream)
+    b.triangulate()
+    return b
+
+
+def time_steps(cg, torch, b, stream, steps, flush):
+    """Per-step device time with an L2 flush between steps; returns (total_s, completed, kernels)."""
+    import ctypes as C
+    lib = b._lib
+    for attempt in range(3):
+        s0 = C.c_int(0)
+        lib.cg_poll(b.handle, C.byref(s0), None, 1)
+        k0 = lib.cg_kernels_launched(b.handle)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        with torch.cuda.stream(stream):
+            for i in range(steps):
+                flush.zero_()
+                ev[i][0].record(stream)
+                cg._lib.check(lib.cg_spp_enqueue(b.handle, 1, DT, MU))
+                ev[i][1].record(stream)
+        stream.synchronize()
+        k1 = lib.cg_kernels_launched(b.handle)
+        s1, h = C.c_int(0), C.c_int(0)
+        lib.cg_poll(b.handle, C.byref(s1), C.byref(h), 1)
+        done = s1.value - s0.value
+        total = sum(a.elapsed_time(e) for a, e in ev) / 1e3
+        if done == steps and not h.value:
+            return total, done, k1 - k0
+    return total, done, k1 - k0
+
+
+def time_force_pass(cg, torch, b, stream, reps, flush):
+    lib = b._lib
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    with torch.cuda.stream(stream):
+        for i in range(reps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            cg._lib.check(lib.cg_launch_force_pass(b.handle, 1))
+            ev[i][1].record(stream)
+    stream.synchronize()
+    return sum(a.elapsed_time(e) for a, e in ev) / reps / 1e3
+
+
+def e2e_steps(cg, torch, b, stream, steps):
+    """Public API with host buffers: pinned noise in, per-instance energy out, every step."""
+    import ctypes as C
+    lib = b._lib
+    noise = torch.empty(b.Ntot, dtype=torch.float64).pin_memory()
+    energy = torch.empty(1, dtype=torch.float64).pin_memory()
+    gen = np.random.default_rng(7)
+    ok = 0
+    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st.record(stream)
+    for i in range(steps):
+        noise.numpy()[:] = gen.standard_normal(b.Ntot)
+        rc = lib.cg_spp_step_host(b.handle, C.c_void_p(noise.data_ptr()), DT, MU, C.c_void_p(energy.data_ptr()))
+        ok += rc == 0
+    en.record(stream)
+    en.synchronize()
+    return st.elapsed_time(en) / 1e3, ok, 8 * b.Ntot, 8
+
+
+def cpu_baseline_port(n_cells=N_CELLS, box=BOX, steps=3, seed=1):
+    """Oracle port of the reference CPU path, 1 thread, on the same monolayer."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(seed)
+    pos = rng.random((n_cells, 2)) * box
+    theta = rng.uniform(0, 2 * np.pi, n_cells)
+    nn, nbr = O.periodic_delaunay(pos, (box, box), 16)
+    mot = np.tile([V0, DR], (n_cells, 1))
+    pref = np.tile([1.0, P0], (n_cells, 1))
+    noise = np.random.default_rng(seed + 1).standard_normal((steps, n_cells))
+    t0 = time.perf_counter()
+    O.voronoi_spp_run(pos, (box, box), nn, nbr, theta, mot, pref, noise, dt=DT, mu=MU)
+    t = time.perf_counter() - t0
+    return {"value": n_cells * steps / t, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+            "sample": f"{steps} SPP steps of the N={n_cells} monolayer (full Delaunay rebuild per step)"}
+
+
+def cpu_reference(steps):
+    ref = os.path.join(ROOT, "oracle", "_ref", "libcgref.so")
+    if os.path.exists(ref):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import ref_harness  # noqa
+        return ref_harness.bench_c2(steps)
+    return cpu_baseline_port(steps=steps)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        t0 = time.perf_counter()
+        steps = max(1, min(args.steps, 3))
+        base = cpu_reference(steps)
+        line = {"metric": METRIC, "value": base["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
+                "steps": steps, "warmup": 0, "ms_per_step": 1e3 * N_CELLS / base["value"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": "voronoi_spp_N262144_L512", "n_cells": N_CELLS, "box": BOX},
+                "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "wall_s": time.perf_counter() - t0}
+        print(json.dumps(line))
+        return
+
+    import torch
+
+    import cellgpu_b200 as cg
+    from cellgpu_b200 import build as cgbuild
+
+    if not os.path.exists(cgbuild.LIB):
+        raise SystemExit("libcellgpu_b200.so missing: run __graft_entry__.build()")
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    stream = torch.cuda.Stream()
+    precision = cg.CG_FP64 if args.precision == "fp64" else cg.CG_MIXED
+    b = make_system(cg, torch, stream, precision, seed=1 + rank)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    # warm-up (untimed; graph capture happens here)
+    for _ in range(max(3, args.warmup)):
+        cg._lib.check(b._lib.cg_spp_enqueue(b.handle, 1, DT, MU))
+    b._lib.cg_poll(b.handle, None, None, 1)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        total, done, kernels = time_steps(cg, torch, b, stream, args.steps, flush)
+    torch.cuda.synchronize()
+    if world > 1:
+        t = torch.tensor([total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+        dist.barrier()
+    value = world * N_CELLS * done / total
+    # dominant kernel: fused geometry + force + exact test
+    t_force = time_force_pass(cg, torch, b, stream, 20, flush)
+    hbm, kind = peaks()
+    achieved = FORCE_PASS_BYTES * N_CELLS / t_force / 1e9
+    # end to end through the host-buffer API
+    e2e_t, e2e_ok, h2d, d2h = e2e_steps(cg, torch, b, stream, max(3, args.steps // 5))
+    e2e_value = world * N_CELLS * e2e_ok / e2e_t if e2e_ok else 0.0
+    counters = b.counters()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            cpu = cpu_reference(2)
+        except Exception as e:  # the baseline must not take the bench down
+            cpu = {"error": str(e)}
+    prof = os.path.join(ROOT, "profiles", "force_pass_traffic.json")
+    traffic = None
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("traffic_bytes_per_launch")
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": done,
+        "warmup": max(3, args.warmup), "ms_per_step": 1e3 * total / max(done, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == cg.CG_FP64 else "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": "voronoi_spp_N262144_L512", "n_cells": N_CELLS, "box": BOX, "p0": P0,
+                   "v0": V0, "Dr": DR, "dt": DT, "precision": args.precision,
+                   "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic, "kernel": "k_voro_cells (force+test)",
+                     "kernel_ms": t_force * 1e3, "peak_kind": kind},
+        "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(kernels),
+        "clocks": clk.summary(),
+        "counters": counters,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

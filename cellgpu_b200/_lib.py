@@ -1,0 +1,112 @@
+"""ctypes binding of the C ABI declared in ``include/cellgpu_b200.h``.
+
+The library is the in-tree ``cellgpu_b200/libcellgpu_b200.so`` (built by ``cellgpu_b200.build``).
+There is no fallback: if the library is missing, loading fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcellgpu_b200.so")
+
+CG_OK = 0
+CG_ERR_CUDA = -1
+CG_ERR_ARG = -2
+CG_ERR_CAPACITY = -3
+CG_ERR_TOPOLOGY = -4
+CG_ERR_TIMEOUT = -5
+CG_ERR_STATE = -6
+CG_FP64 = 0
+CG_MIXED = 1
+
+_vp = C.c_void_p
+_i = C.c_int
+_d = C.c_double
+_u64 = C.c_uint64
+_u32 = C.c_uint32
+_sz = C.c_size_t
+
+# name -> (restype, argtypes); every symbol here is declared in include/cellgpu_b200.h
+SIGNATURES = {
+    "cg_last_error_string": (C.c_char_p, []),
+    "cg_version": (_i, []),
+    "cg_voronoi_geometry": (_i, [_vp, _vp, _vp, _i, _i, _d, _d, _vp, _vp]),
+    "cg_voronoi_forces": (_i, [_vp, _vp, _vp, _i, _i, _d, _d, _vp, _d, _d, _vp, _vp, _vp]),
+    "cg_voronoi_test_triangulation": (_i, [_vp, _vp, _vp, _i, _i, _d, _d, _vp, _vp, _vp]),
+    "cg_spp_step": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _d, _d, _d, _d, _u64, _u32, _vp]),
+    "cg_voronoi_triangulate": (_i, [_vp, _i, _d, _d, _i, _vp, _vp, _vp]),
+    "cg_voronoi_create": (_i, [_i, _vp, _vp, _i, _i, C.POINTER(_vp)]),
+    "cg_destroy": (_i, [_vp]),
+    "cg_num_cells": (_i, [_vp]),
+    "cg_num_dofs": (_i, [_vp]),
+    "cg_num_instances": (_i, [_vp]),
+    "cg_neighbor_capacity": (_i, [_vp]),
+    "cg_device_bytes": (_sz, [_vp]),
+    "cg_voronoi_footprint": (_sz, [_i, _vp, _i]),
+    "cg_set_positions": (_i, [_vp, _vp]),
+    "cg_get_positions": (_i, [_vp, _vp]),
+    "cg_set_cell_preferences": (_i, [_vp, _vp]),
+    "cg_set_moduli": (_i, [_vp, _d, _d]),
+    "cg_set_motility": (_i, [_vp, _vp]),
+    "cg_set_directors": (_i, [_vp, _vp]),
+    "cg_get_directors": (_i, [_vp, _vp]),
+    "cg_get_forces": (_i, [_vp, _vp]),
+    "cg_get_area_perimeter": (_i, [_vp, _vp]),
+    "cg_get_topology": (_i, [_vp, _vp, _vp]),
+    "cg_set_topology": (_i, [_vp, _vp, _vp]),
+    "cg_get_energies": (_i, [_vp, _vp]),
+    "cg_set_stream": (_i, [_vp, _vp]),
+    "cg_synchronize": (_i, [_vp]),
+    "cg_triangulate": (_i, [_vp]),
+    "cg_compute_forces": (_i, [_vp]),
+    "cg_enforce_topology": (_i, [_vp]),
+    "cg_set_seed": (_i, [_vp, _u64]),
+    "cg_spp_run": (_i, [_vp, _i, _d, _d, _vp]),
+    "cg_counters": (_i, [_vp, C.POINTER(C.c_longlong), _i]),
+    "cg_get_stream": (_vp, [_vp]),
+    "cg_spp_enqueue": (_i, [_vp, _i, _d, _d]),
+    "cg_poll": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), _i]),
+    "cg_spp_step_host": (_i, [_vp, _vp, _d, _d, _vp]),
+    "cg_launch_force_pass": (_i, [_vp, _i]),
+    "cg_kernels_launched": (C.c_longlong, [_vp]),
+}
+
+_lib = None
+
+
+class CellGPUError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cellgpu_b200 error {code}: {msg}")
+        self.code = code
+
+
+def load():
+    """Load the in-tree library (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing; build it with `python -m cellgpu_b200.build`")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(code):
+    if code != CG_OK:
+        raise CellGPUError(code, load().cg_last_error_string().decode())
+    return code
+
+
+def ptr(a):
+    """Device or host pointer of a torch tensor / numpy array (None -> NULL)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)

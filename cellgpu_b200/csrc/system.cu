@@ -1,0 +1,825 @@
+// cellgpu_b200 -- host side of the C ABI: kernel callers on caller memory, and the device-resident
+// batched system (cg_system). Built as one translation unit with the kernel files.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "voronoi.cu"
+
+using namespace cg;
+
+// ------------------------------------------------------------------------------------------
+// errors
+// ------------------------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+static int set_err(int code, const char *msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define CG_CUDA(call)                                                                           \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) {                                                                \
+            g_err = std::string(#call) + ": " + cudaGetErrorString(e_);                         \
+            return CG_ERR_CUDA;                                                                 \
+        }                                                                                       \
+    } while (0)
+
+#define CG_TRY(call)                 \
+    do {                             \
+        int s_ = (call);             \
+        if (s_ != CG_OK) return s_;  \
+    } while (0)
+
+extern "C" const char *cg_last_error_string(void) { return g_err.c_str(); }
+extern "C" int cg_version(void) { return 100; }
+
+static inline int nblk(int n, int b) { return (n + b - 1) / b; }
+
+static Inst make_inst(double Lx, double Ly, int off, int n, int bin_off, double bin_target)
+{
+    Inst in;
+    memset(&in, 0, sizeof(in));
+    in.Lx = Lx;
+    in.Ly = Ly;
+    in.iLx = 1.0 / Lx;
+    in.iLy = 1.0 / Ly;
+    in.off = off;
+    in.n = n;
+    in.bin_off = bin_off;
+    in.nbx = std::max(1, (int)std::floor(Lx / bin_target));
+    in.nby = std::max(1, (int)std::floor(Ly / bin_target));
+    in.bsx = Lx / in.nbx;
+    in.bsy = Ly / in.nby;
+    return in;
+}
+
+static const double BIN_TARGET = 0.8;
+
+// ------------------------------------------------------------------------------------------
+// 1. kernel callers on caller-owned memory
+// ------------------------------------------------------------------------------------------
+static VoroArgs raw_args(const double *pos, const int *nn, const int *nbr, int K, int N, double Lx,
+                         double Ly)
+{
+    VoroArgs a;
+    memset(&a, 0, sizeof(a));
+    a.N = N;
+    a.K = K;
+    a.n_inst = 1;
+    a.inst0 = make_inst(Lx, Ly, 0, N, 0, BIN_TARGET);
+    a.pos = (double2 *)pos;
+    a.nn = (int *)nn;
+    a.nbr = (int *)nbr;
+    return a;
+}
+
+static int check_launch()
+{
+    CG_CUDA(cudaGetLastError());
+    return CG_OK;
+}
+
+extern "C" int cg_voronoi_geometry(const double *pos, const int *nn, const int *nbr, int K, int N,
+                                   double Lx, double Ly, double *AP, cudaStream_t stream)
+{
+    if (N <= 0 || K < 3 || K > KMAX || !pos || !nn || !nbr || !AP) return set_err(CG_ERR_ARG, "bad args");
+    VoroArgs a = raw_args(pos, nn, nbr, K, N, Lx, Ly);
+    a.AP = AP;
+    k_voro_cells<double, false, false><<<nblk(N, 128), 128, 0, stream>>>(a);
+    return check_launch();
+}
+
+extern "C" int cg_voronoi_forces(const double *pos, const int *nn, const int *nbr, int K, int N,
+                                 double Lx, double Ly, const double *APpref, double KA, double KP,
+                                 double *AP, double *F, cudaStream_t stream)
+{
+    if (N <= 0 || K < 3 || K > KMAX || !pos || !nn || !nbr || !APpref || !F)
+        return set_err(CG_ERR_ARG, "bad args");
+    VoroArgs a = raw_args(pos, nn, nbr, K, N, Lx, Ly);
+    a.APpref = (const double2 *)APpref;
+    a.KA = KA;
+    a.KP = KP;
+    a.AP = AP;
+    a.F = F;
+    k_voro_cells<double, true, false><<<nblk(N, 128), 128, 0, stream>>>(a);
+    return check_launch();
+}
+
+extern "C" int cg_voronoi_test_triangulation(const double *pos, const int *nn, const int *nbr, int K,
+                                             int N, double Lx, double Ly, int *flag, int *any_fail,
+                                             cudaStream_t stream)
+{
+    if (N <= 0 || K < 3 || K > KMAX || !pos || !nn || !nbr || !flag || !any_fail)
+        return set_err(CG_ERR_ARG, "bad args");
+    VoroArgs a = raw_args(pos, nn, nbr, K, N, Lx, Ly);
+    a.mark = flag;
+    a.queue = any_fail;
+    k_voro_cells<double, false, true><<<nblk(N, 128), 128, 0, stream>>>(a);
+    return check_launch();
+}
+
+extern "C" int cg_spp_step(double *pos, double *theta, const double *F, const double *motility,
+                           const double *noise, int N, double Lx, double Ly, double dt, double mu,
+                           uint64_t seed, uint32_t step, cudaStream_t stream)
+{
+    if (N <= 0 || !pos || !theta || !F || !motility) return set_err(CG_ERR_ARG, "bad args");
+    VoroArgs a;
+    memset(&a, 0, sizeof(a));
+    a.N = N;
+    a.inst0 = make_inst(Lx, Ly, 0, N, 0, BIN_TARGET);
+    a.pos = (double2 *)pos;
+    a.theta = theta;
+    a.F = (void *)F;
+    a.motility = (const double2 *)motility;
+    (void)step;
+    k_spp<double><<<nblk(N, 256), 256, 0, stream>>>(a, noise, dt, mu, seed, 0);
+    return check_launch();
+}
+
+// ------------------------------------------------------------------------------------------
+// 2. systems
+// ------------------------------------------------------------------------------------------
+struct cg_system {
+    int model = CG_MODEL_VORONOI;
+    int precision = CG_FP64;
+    int n_inst = 0, N = 0, K = 0, n_bins = 0;
+    std::vector<Inst> h_inst;
+    std::vector<int> h_cell_inst;
+    cudaStream_t stream = 0;
+    uint64_t seed = 0x5eed;
+    double KA = 1.0, KP = 1.0;
+    size_t bytes = 0;
+    std::vector<void *> allocs;
+    // device
+    Inst *inst = nullptr;
+    int *cell_inst = nullptr;
+    double2 *pos = nullptr, *motility = nullptr, *APpref = nullptr;
+    double *theta = nullptr;
+    void *AP = nullptr, *F = nullptr;
+    int *nn = nullptr, *nbr = nullptr;
+    int *mark = nullptr, *queue = nullptr, *stage_nn = nullptr, *stage_nbr = nullptr, *changed = nullptr;
+    Ctl *ctl = nullptr;
+    int *bin_count = nullptr, *bin_start = nullptr, *bin_cells = nullptr, *cell_bin = nullptr,
+        *cell_slot = nullptr;
+    double2 *bin_pos = nullptr;
+    void *scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
+    int *d_status = nullptr;
+    unsigned long long *d_zsum = nullptr;
+    double *d_energy = nullptr;
+    bool topology_valid = false;
+    long long host_counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    cudaStream_t own_stream = nullptr;
+    struct GraphEntry {
+        int n;
+        double dt, mu;
+        const double *noise;
+        cudaGraphExec_t exec;
+        long long kernels;
+    };
+    std::vector<GraphEntry> graphs;
+    long long kernels_enqueued = 0;  // kernels of this library launched for this system
+    double *noise_buf = nullptr;     // staging for host-supplied noise (one step)
+};
+
+template <typename T>
+static int dalloc(cg_system *s, T **p, size_t count)
+{
+    size_t b = std::max<size_t>(count, 1) * sizeof(T);
+    void *q = nullptr;
+    CG_CUDA(cudaMalloc(&q, b));
+    CG_CUDA(cudaMemset(q, 0, b));
+    s->allocs.push_back(q);
+    s->bytes += b;
+    *p = (T *)q;
+    return CG_OK;
+}
+
+static VoroArgs sys_args(cg_system *s)
+{
+    VoroArgs a;
+    memset(&a, 0, sizeof(a));
+    a.N = s->N;
+    a.K = s->K;
+    a.n_inst = s->n_inst;
+    a.inst = s->inst;
+    a.cell_inst = s->cell_inst;
+    a.pos = s->pos;
+    a.theta = s->theta;
+    a.motility = s->motility;
+    a.APpref = s->APpref;
+    a.KA = s->KA;
+    a.KP = s->KP;
+    a.AP = s->AP;
+    a.F = s->F;
+    a.nn = s->nn;
+    a.nbr = s->nbr;
+    a.mark = s->mark;
+    a.queue = s->queue;
+    a.stage_nn = s->stage_nn;
+    a.stage_nbr = s->stage_nbr;
+    a.changed = s->changed;
+    a.ctl = s->ctl;
+    a.bin_count = s->bin_count;
+    a.bin_start = s->bin_start;
+    a.bin_cells = s->bin_cells;
+    a.cell_bin = s->cell_bin;
+    a.cell_slot = s->cell_slot;
+    a.bin_pos = s->bin_pos;
+    a.n_bins = s->n_bins;
+    return a;
+}
+
+static size_t voronoi_bytes(int N, int K, int n_bins, int n_inst, int precision)
+{
+    size_t real2 = precision == CG_FP64 ? 16 : 8;
+    size_t per_cell = 4 /*cell_inst*/ + 16 * 3 /*pos, motility, APpref*/ + 8 /*theta*/ + 2 * real2 +
+                      4 + 4 * (size_t)K /*nn, nbr*/ + 4 /*mark*/ + 4 * (R_MAX + 1) /*queue*/ + 4 +
+                      4 * (size_t)K /*stage*/ + 4 * R_MAX /*changed*/ + 4 * 3 + 16 /*cell list*/;
+    return per_cell * (size_t)N + (size_t)n_bins * 8 + (size_t)n_inst * (sizeof(Inst) + 16) + 4096;
+}
+
+extern "C" size_t cg_voronoi_footprint(int n_inst, const int *N, int K)
+{
+    long long tot = 0, bins = 0;
+    for (int i = 0; i < n_inst; ++i) {
+        tot += N[i];
+        double L = std::sqrt((double)N[i]);
+        long long nb = std::max(1, (int)std::floor(L / BIN_TARGET));
+        bins += nb * nb;
+    }
+    return voronoi_bytes((int)tot, K, (int)bins, n_inst, CG_FP64);
+}
+
+extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, int K, int precision,
+                                 cg_system **out)
+{
+    if (n_inst <= 0 || !N || !box || !out || K < 4 || K > KMAX ||
+        (precision != CG_FP64 && precision != CG_MIXED))
+        return set_err(CG_ERR_ARG, "bad args");
+    cg_system *s = new cg_system();
+    s->model = CG_MODEL_VORONOI;
+    s->precision = precision;
+    s->n_inst = n_inst;
+    s->K = K;
+    int off = 0, boff = 0;
+    for (int i = 0; i < n_inst; ++i) {
+        if (N[i] < 8 || !(box[2 * i] > 0) || !(box[2 * i + 1] > 0)) {
+            delete s;
+            return set_err(CG_ERR_ARG, "instance needs >= 8 cells and a positive box");
+        }
+        Inst in = make_inst(box[2 * i], box[2 * i + 1], off, N[i], boff, BIN_TARGET);
+        s->h_inst.push_back(in);
+        for (int c = 0; c < N[i]; ++c) s->h_cell_inst.push_back(i);
+        off += N[i];
+        boff += in.nbx * in.nby;
+    }
+    s->N = off;
+    s->n_bins = boff;
+    int Nt = s->N;
+    size_t r2 = precision == CG_FP64 ? sizeof(double2) : sizeof(float2);
+    int st = CG_OK;
+    do {
+        if ((st = dalloc(s, &s->inst, n_inst))) break;
+        if ((st = dalloc(s, &s->cell_inst, Nt))) break;
+        if ((st = dalloc(s, &s->pos, Nt))) break;
+        if ((st = dalloc(s, &s->motility, Nt))) break;
+        if ((st = dalloc(s, &s->APpref, Nt))) break;
+        if ((st = dalloc(s, &s->theta, Nt))) break;
+        if ((st = dalloc(s, (char **)&s->AP, r2 * Nt))) break;
+        if ((st = dalloc(s, (char **)&s->F, r2 * Nt))) break;
+        if ((st = dalloc(s, &s->nn, Nt))) break;
+        if ((st = dalloc(s, &s->nbr, (size_t)Nt * K))) break;
+        if ((st = dalloc(s, &s->mark, Nt))) break;
+        if ((st = dalloc(s, &s->queue, (size_t)Nt * (R_MAX + 1)))) break;
+        if ((st = dalloc(s, &s->stage_nn, Nt))) break;
+        if ((st = dalloc(s, &s->stage_nbr, (size_t)Nt * K))) break;
+        if ((st = dalloc(s, &s->changed, (size_t)Nt * R_MAX))) break;
+        if ((st = dalloc(s, &s->ctl, 1))) break;
+        if ((st = dalloc(s, &s->bin_count, s->n_bins))) break;
+        if ((st = dalloc(s, &s->bin_start, s->n_bins + 1))) break;
+        if ((st = dalloc(s, &s->bin_cells, Nt))) break;
+        if ((st = dalloc(s, &s->cell_bin, Nt))) break;
+        if ((st = dalloc(s, &s->cell_slot, Nt))) break;
+        if ((st = dalloc(s, &s->bin_pos, Nt))) break;
+        if ((st = dalloc(s, &s->d_status, 4))) break;
+        if ((st = dalloc(s, &s->d_zsum, n_inst))) break;
+        if ((st = dalloc(s, &s->d_energy, n_inst))) break;
+        if ((st = dalloc(s, &s->noise_buf, Nt))) break;
+        size_t tmpb = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tmpb, s->bin_count, s->bin_start, s->n_bins + 1);
+        s->scan_tmp_bytes = tmpb;
+        if ((st = dalloc(s, (char **)&s->scan_tmp, tmpb))) break;
+    } while (0);
+    if (st != CG_OK) {
+        for (void *p : s->allocs) cudaFree(p);
+        delete s;
+        return st;
+    }
+    cudaMemcpy(s->inst, s->h_inst.data(), sizeof(Inst) * n_inst, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->cell_inst, s->h_cell_inst.data(), sizeof(int) * Nt, cudaMemcpyHostToDevice);
+    // defaults of the reference: A0 = 1, P0 = 3.8 (Simple2DCell::initializeSimple2DCell,
+    // src/models/Simple2DCell.cpp:27), v0 = 0.05, Dr = 1 (VoronoiQuadraticEnergy(n,A0,P0,..),
+    // src/models/voronoiQuadraticEnergy.cpp:34)
+    std::vector<double2> pref(Nt, make_double2(1.0, 3.8)), mot(Nt, make_double2(0.05, 1.0));
+    cudaMemcpy(s->APpref, pref.data(), sizeof(double2) * Nt, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->motility, mot.data(), sizeof(double2) * Nt, cudaMemcpyHostToDevice);
+    if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        for (void *p : s->allocs) cudaFree(p);
+        delete s;
+        return set_err(CG_ERR_CUDA, "stream creation failed");
+    }
+    s->stream = s->own_stream;
+    Ctl c0;
+    memset(&c0, 0, sizeof(c0));
+    c0.epoch = 1;
+    cudaMemcpy(s->ctl, &c0, sizeof(Ctl), cudaMemcpyHostToDevice);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        for (void *p : s->allocs) cudaFree(p);
+        delete s;
+        return set_err(CG_ERR_CUDA, cudaGetErrorString(e));
+    }
+    *out = s;
+    return CG_OK;
+}
+
+extern "C" int cg_destroy(cg_system *s)
+{
+    if (!s) return CG_OK;
+    cudaStreamSynchronize(s->stream);
+    for (auto &g : s->graphs) cudaGraphExecDestroy(g.exec);
+    for (void *p : s->allocs) cudaFree(p);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    delete s;
+    return CG_OK;
+}
+
+extern "C" int cg_num_cells(const cg_system *s) { return s ? s->N : 0; }
+extern "C" int cg_num_dofs(const cg_system *s) { return s ? s->N : 0; }
+extern "C" int cg_num_instances(const cg_system *s) { return s ? s->n_inst : 0; }
+extern "C" int cg_neighbor_capacity(const cg_system *s) { return s ? s->K : 0; }
+extern "C" size_t cg_device_bytes(const cg_system *s) { return s ? s->bytes : 0; }
+
+extern "C" int cg_set_stream(cg_system *s, cudaStream_t stream)
+{
+    if (!s) return set_err(CG_ERR_ARG, "null system");
+    CG_CUDA(cudaStreamSynchronize(s->stream));
+    s->stream = stream ? stream : s->own_stream;
+    return CG_OK;
+}
+
+extern "C" cudaStream_t cg_get_stream(cg_system *s) { return s ? s->stream : nullptr; }
+
+extern "C" int cg_synchronize(cg_system *s)
+{
+    if (!s) return set_err(CG_ERR_ARG, "null system");
+    CG_CUDA(cudaStreamSynchronize(s->stream));
+    return CG_OK;
+}
+
+static int h2d(cg_system *s, void *dst, const void *src, size_t b)
+{
+    CG_CUDA(cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, s->stream));
+    CG_CUDA(cudaStreamSynchronize(s->stream));
+    return CG_OK;
+}
+
+static int d2h(cg_system *s, void *dst, const void *src, size_t b)
+{
+    CG_CUDA(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, s->stream));
+    CG_CUDA(cudaStreamSynchronize(s->stream));
+    return CG_OK;
+}
+
+extern "C" int cg_set_positions(cg_system *s, const double *pos)
+{
+    if (!s || !pos) return set_err(CG_ERR_ARG, "bad args");
+    s->topology_valid = false;
+    return h2d(s, s->pos, pos, sizeof(double2) * s->N);
+}
+extern "C" int cg_get_positions(cg_system *s, double *pos)
+{
+    if (!s || !pos) return set_err(CG_ERR_ARG, "bad args");
+    return d2h(s, pos, s->pos, sizeof(double2) * s->N);
+}
+extern "C" int cg_set_cell_preferences(cg_system *s, const double *p)
+{
+    if (!s || !p) return set_err(CG_ERR_ARG, "bad args");
+    return h2d(s, s->APpref, p, sizeof(double2) * s->N);
+}
+extern "C" int cg_set_moduli(cg_system *s, double KA, double KP)
+{
+    if (!s) return set_err(CG_ERR_ARG, "bad args");
+    s->KA = KA;
+    s->KP = KP;
+    return CG_OK;
+}
+extern "C" int cg_set_motility(cg_system *s, const double *m)
+{
+    if (!s || !m) return set_err(CG_ERR_ARG, "bad args");
+    return h2d(s, s->motility, m, sizeof(double2) * s->N);
+}
+extern "C" int cg_set_directors(cg_system *s, const double *t)
+{
+    if (!s || !t) return set_err(CG_ERR_ARG, "bad args");
+    return h2d(s, s->theta, t, sizeof(double) * s->N);
+}
+extern "C" int cg_get_directors(cg_system *s, double *t)
+{
+    if (!s || !t) return set_err(CG_ERR_ARG, "bad args");
+    return d2h(s, t, s->theta, sizeof(double) * s->N);
+}
+extern "C" int cg_set_seed(cg_system *s, uint64_t seed)
+{
+    if (!s) return set_err(CG_ERR_ARG, "bad args");
+    s->seed = seed;
+    return CG_OK;
+}
+
+static int get_real2(cg_system *s, const void *src, double *dst, int n)
+{
+    if (s->precision == CG_FP64) return d2h(s, dst, src, sizeof(double2) * n);
+    std::vector<float2> tmp(n);
+    CG_TRY(d2h(s, tmp.data(), src, sizeof(float2) * n));
+    for (int i = 0; i < n; ++i) {
+        dst[2 * i] = tmp[i].x;
+        dst[2 * i + 1] = tmp[i].y;
+    }
+    return CG_OK;
+}
+
+extern "C" int cg_get_forces(cg_system *s, double *F)
+{
+    if (!s || !F) return set_err(CG_ERR_ARG, "bad args");
+    return get_real2(s, s->F, F, s->N);
+}
+extern "C" int cg_get_area_perimeter(cg_system *s, double *AP)
+{
+    if (!s || !AP) return set_err(CG_ERR_ARG, "bad args");
+    return get_real2(s, s->AP, AP, s->N);
+}
+extern "C" int cg_get_topology(cg_system *s, int *nn, int *nbr)
+{
+    if (!s || !nn || !nbr) return set_err(CG_ERR_ARG, "bad args");
+    CG_TRY(d2h(s, nn, s->nn, sizeof(int) * s->N));
+    return d2h(s, nbr, s->nbr, sizeof(int) * (size_t)s->N * s->K);
+}
+extern "C" int cg_set_topology(cg_system *s, const int *nn, const int *nbr)
+{
+    if (!s || !nn || !nbr) return set_err(CG_ERR_ARG, "bad args");
+    for (int i = 0; i < s->N; ++i)
+        if (nn[i] < 3 || nn[i] > s->K) return set_err(CG_ERR_ARG, "row length out of range");
+    CG_TRY(h2d(s, s->nn, nn, sizeof(int) * s->N));
+    CG_TRY(h2d(s, s->nbr, nbr, sizeof(int) * (size_t)s->N * s->K));
+    s->topology_valid = true;
+    return CG_OK;
+}
+
+extern "C" int cg_counters(cg_system *s, long long *out, int n)
+{
+    if (!s || !out) return set_err(CG_ERR_ARG, "bad args");
+    Ctl c;
+    CG_TRY(d2h(s, &c, s->ctl, sizeof(Ctl)));
+    for (int i = 0; i < n && i < 8; ++i) out[i] = (long long)c.counters[i] + s->host_counters[i];
+    return CG_OK;
+}
+
+// ---- global triangulation on the device ---------------------------------------------------
+static int build_cell_list(cg_system *s)
+{
+    VoroArgs a = sys_args(s);
+    CG_CUDA(cudaMemsetAsync(s->bin_count, 0, sizeof(int) * (s->n_bins + 1), s->stream));
+    k_bin_count<<<nblk(s->N, 256), 256, 0, s->stream>>>(a);
+    CG_CUDA(cub::DeviceScan::ExclusiveSum(s->scan_tmp, s->scan_tmp_bytes, s->bin_count, s->bin_start,
+                                          s->n_bins + 1, s->stream));
+    k_bin_scatter<<<nblk(s->N, 256), 256, 0, s->stream>>>(a);
+    return check_launch();
+}
+
+static int triangulate_sys(cg_system *s)
+{
+    CG_TRY(build_cell_list(s));
+    VoroArgs a = sys_args(s);
+    CG_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(int) * 4, s->stream));
+    CG_CUDA(cudaMemsetAsync(s->d_zsum, 0, sizeof(unsigned long long) * s->n_inst, s->stream));
+    constexpr int WPB = 4;
+    k_star_global<WPB><<<nblk(s->N, WPB), WPB * 32, 0, s->stream>>>(a, s->d_status);
+    CG_TRY(check_launch());
+    int st = 0;
+    CG_TRY(d2h(s, &st, s->d_status, sizeof(int)));
+    if (st) return set_err(st, st == CG_ERR_CAPACITY ? "neighbour capacity exceeded in triangulation"
+                                                      : "global triangulation failed");
+    k_validate<<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_status, s->d_zsum);
+    CG_TRY(check_launch());
+    std::vector<unsigned long long> zs(s->n_inst);
+    CG_TRY(d2h(s, &st, s->d_status, sizeof(int)));
+    CG_TRY(d2h(s, zs.data(), s->d_zsum, sizeof(unsigned long long) * s->n_inst));
+    if (st) return set_err(CG_ERR_TOPOLOGY, "triangulation is not consistent");
+    for (int i = 0; i < s->n_inst; ++i)
+        if (zs[i] != 6ull * (unsigned long long)s->h_inst[i].n)
+            return set_err(CG_ERR_TOPOLOGY, "Euler check failed (sum of coordinations != 6N)");
+    s->topology_valid = true;
+    s->host_counters[4] += 1;
+    return CG_OK;
+}
+
+extern "C" int cg_triangulate(cg_system *s)
+{
+    if (!s || s->model != CG_MODEL_VORONOI) return set_err(CG_ERR_ARG, "bad args");
+    return triangulate_sys(s);
+}
+
+extern "C" int cg_voronoi_triangulate(const double *pos, int N, double Lx, double Ly, int K, int *nn,
+                                      int *nbr, cudaStream_t stream)
+{
+    if (!pos || !nn || !nbr || N < 8 || K < 4 || K > KMAX) return set_err(CG_ERR_ARG, "bad args");
+    cg_system *s = nullptr;
+    double box[2] = {Lx, Ly};
+    CG_TRY(cg_voronoi_create(1, &N, box, K, CG_FP64, &s));
+    s->stream = stream;
+    int st = CG_OK;
+    do {
+        if ((cudaMemcpyAsync(s->pos, pos, sizeof(double2) * N, cudaMemcpyDeviceToDevice, stream)) !=
+            cudaSuccess) {
+            st = set_err(CG_ERR_CUDA, "copy failed");
+            break;
+        }
+        if ((st = triangulate_sys(s))) break;
+        if (cudaMemcpyAsync(nn, s->nn, sizeof(int) * N, cudaMemcpyDeviceToDevice, stream) != cudaSuccess ||
+            cudaMemcpyAsync(nbr, s->nbr, sizeof(int) * (size_t)N * K, cudaMemcpyDeviceToDevice, stream) !=
+                cudaSuccess)
+            st = set_err(CG_ERR_CUDA, "copy failed");
+        cudaStreamSynchronize(stream);
+    } while (0);
+    cg_destroy(s);
+    return st;
+}
+
+// ---- one step of the Voronoi model ---------------------------------------------------------
+template <typename R>
+static void launch_force_test(cg_system *s, const VoroArgs &a, bool test)
+{
+    cudaMemsetAsync(s->F, 0, (s->precision == CG_FP64 ? sizeof(double2) : sizeof(float2)) * s->N,
+                    s->stream);
+    if (test)
+        k_voro_cells<R, true, true><<<nblk(s->N, 128), 128, 0, s->stream>>>(a);
+    else
+        k_voro_cells<R, true, false><<<nblk(s->N, 128), 128, 0, s->stream>>>(a);
+    s->kernels_enqueued += 1;
+}
+
+template <typename R>
+static void launch_repair(cg_system *s, const VoroArgs &a, bool forces)
+{
+    constexpr int WPB = 4;
+    int grid_w = 148 * 4;
+    k_expand<<<1, 512, 0, s->stream>>>(a);
+    for (int r = 0; r < R_MAX; ++r) {
+        k_star_local<WPB><<<grid_w, WPB * 32, 0, s->stream>>>(a, r);
+        if (forces)
+            k_commit<R, true><<<148 * 2, 128, 0, s->stream>>>(a, r);
+        else
+            k_commit<R, false><<<148 * 2, 128, 0, s->stream>>>(a, r);
+        k_check<<<148 * 2, 128, 0, s->stream>>>(a, r);
+    }
+    k_finish_repair<<<1, 1, 0, s->stream>>>(a);
+    s->kernels_enqueued += 2 + 3 * R_MAX;
+}
+
+static int read_ctl(cg_system *s, Ctl &c) { return d2h(s, &c, s->ctl, sizeof(Ctl)); }
+
+// clear a halted control block so the step can be re-run after the host-side fix
+static int reset_ctl_after_halt(cg_system *s)
+{
+    Ctl c;
+    CG_TRY(read_ctl(s, c));
+    c.halt = 0;
+    c.need_global = 0;
+    c.status = 0;
+    c.n_flagged = 0;
+    for (int r = 0; r <= R_MAX; ++r) c.q_count[r] = 0;
+    for (int r = 0; r < R_MAX; ++r) c.n_changed[r] = 0;
+    c.epoch += R_MAX + 2;
+    return h2d(s, s->ctl, &c, sizeof(Ctl));
+}
+
+// handle a halted step: global retriangulation (or report the error)
+static int recover(cg_system *s)
+{
+    Ctl c;
+    CG_TRY(read_ctl(s, c));
+    if (!c.halt) return CG_OK;
+    if (c.status == CG_ERR_CAPACITY) return set_err(CG_ERR_CAPACITY, "neighbour capacity exceeded");
+    CG_TRY(reset_ctl_after_halt(s));
+    return triangulate_sys(s);
+}
+
+template <typename R>
+static int compute_forces_t(cg_system *s)
+{
+    VoroArgs a = sys_args(s);
+    launch_force_test<R>(s, a, false);
+    return check_launch();
+}
+
+extern "C" int cg_compute_forces(cg_system *s)
+{
+    if (!s) return set_err(CG_ERR_ARG, "null system");
+    if (!s->topology_valid) CG_TRY(triangulate_sys(s));
+    int st = s->precision == CG_FP64 ? compute_forces_t<double>(s) : compute_forces_t<float>(s);
+    if (st) return st;
+    return cg_synchronize(s);
+}
+
+template <typename R>
+static int enforce_t(cg_system *s)
+{
+    VoroArgs a = sys_args(s);
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        k_voro_cells<R, false, true><<<nblk(s->N, 128), 128, 0, s->stream>>>(a);
+        launch_repair<R>(s, a, false);
+        k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 0);
+        CG_TRY(check_launch());
+        Ctl c;
+        CG_TRY(read_ctl(s, c));
+        if (!c.halt) return CG_OK;
+        CG_TRY(recover(s));
+    }
+    return set_err(CG_ERR_TOPOLOGY, "topology could not be enforced");
+}
+
+extern "C" int cg_enforce_topology(cg_system *s)
+{
+    if (!s) return set_err(CG_ERR_ARG, "null system");
+    if (!s->topology_valid) return triangulate_sys(s);
+    return s->precision == CG_FP64 ? enforce_t<double>(s) : enforce_t<float>(s);
+}
+
+template <typename R>
+static void enqueue_spp_steps(cg_system *s, int n, double dt, double mu, const double *noise, bool noise_per_step)
+{
+    VoroArgs a = sys_args(s);
+    for (int t = 0; t < n; ++t) {
+        launch_force_test<R>(s, a, true);
+        launch_repair<R>(s, a, true);
+        const double *nz = noise ? (noise_per_step ? noise + (size_t)t * s->N : noise) : nullptr;
+        k_spp<R><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, nz, dt, mu, s->seed, 0);
+        k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
+        s->kernels_enqueued += 2;
+    }
+}
+
+// Replay (capturing on first use) a CUDA graph of n steps. The kernels take their queue lengths,
+// epochs and step counter from the device control block, so one graph serves every call.
+template <typename R>
+static int enqueue_graph(cg_system *s, int n, double dt, double mu, const double *noise)
+{
+    for (auto &g : s->graphs)
+        if (g.n == n && g.dt == dt && g.mu == mu && g.noise == noise) {
+            CG_CUDA(cudaGraphLaunch(g.exec, s->stream));
+            s->kernels_enqueued += g.kernels;
+            return CG_OK;
+        }
+    cudaGraph_t graph;
+    long long k0 = s->kernels_enqueued;
+    CG_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_spp_steps<R>(s, n, dt, mu, noise, false);
+    CG_CUDA(cudaStreamEndCapture(s->stream, &graph));
+    cudaGraphExec_t exec;
+    CG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    long long nk = s->kernels_enqueued - k0;
+    s->kernels_enqueued = k0;
+    s->graphs.push_back({n, dt, mu, noise, exec, nk});
+    CG_CUDA(cudaGraphLaunch(exec, s->stream));
+    s->kernels_enqueued += nk;
+    return CG_OK;
+}
+
+static int read_status(cg_system *s, int *steps, int *halted)
+{
+    Ctl c;
+    CG_TRY(read_ctl(s, c));
+    if (steps) *steps = c.step;
+    if (halted) *halted = c.halt;
+    return CG_OK;
+}
+
+template <typename R>
+static int spp_run_t(cg_system *s, int n_steps, double dt, double mu, const double *noise)
+{
+    int step0 = 0, step = 0, halted = 0;
+    CG_TRY(read_status(s, &step0, nullptr));
+    int done = 0, recoveries = 0;
+    const int chunk = 32;
+    while (done < n_steps) {
+        int todo = std::min(chunk, n_steps - done);
+        if (noise)
+            enqueue_spp_steps<R>(s, todo, dt, mu, noise + (size_t)done * s->N, true);
+        else
+            CG_TRY(enqueue_graph<R>(s, todo, dt, mu, nullptr));
+        CG_TRY(check_launch());
+        CG_TRY(read_status(s, &step, &halted));
+        done = step - step0;
+        if (halted) {
+            if (++recoveries > 8 + n_steps / 16) return set_err(CG_ERR_TOPOLOGY, "too many global rebuilds");
+            CG_TRY(recover(s));
+        }
+    }
+    return CG_OK;
+}
+
+// enqueue n RNG-driven steps without any host synchronisation (graph replay)
+extern "C" int cg_spp_enqueue(cg_system *s, int n_steps, double dt, double mu)
+{
+    if (!s || s->model != CG_MODEL_VORONOI || n_steps <= 0) return set_err(CG_ERR_ARG, "bad args");
+    if (!s->topology_valid) CG_TRY(triangulate_sys(s));
+    return s->precision == CG_FP64 ? enqueue_graph<double>(s, n_steps, dt, mu, nullptr)
+                                   : enqueue_graph<float>(s, n_steps, dt, mu, nullptr);
+}
+
+// one step with host-supplied noise (copied in) and the per-instance energies copied out
+extern "C" int cg_spp_step_host(cg_system *s, const double *host_noise, double dt, double mu,
+                                double *host_energy)
+{
+    if (!s || s->model != CG_MODEL_VORONOI || !host_noise) return set_err(CG_ERR_ARG, "bad args");
+    if (!s->topology_valid) CG_TRY(triangulate_sys(s));
+    CG_CUDA(cudaMemcpyAsync(s->noise_buf, host_noise, sizeof(double) * s->N, cudaMemcpyHostToDevice,
+                            s->stream));
+    int st = s->precision == CG_FP64 ? enqueue_graph<double>(s, 1, dt, mu, s->noise_buf)
+                                     : enqueue_graph<float>(s, 1, dt, mu, s->noise_buf);
+    if (st) return st;
+    VoroArgs a = sys_args(s);
+    CG_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * s->n_inst, s->stream));
+    if (s->precision == CG_FP64)
+        k_energy<double><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
+    else
+        k_energy<float><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
+    s->kernels_enqueued += 1;
+    if (host_energy)
+        CG_CUDA(cudaMemcpyAsync(host_energy, s->d_energy, sizeof(double) * s->n_inst, cudaMemcpyDeviceToHost,
+                                s->stream));
+    CG_CUDA(cudaStreamSynchronize(s->stream));
+    int halted = 0;
+    CG_TRY(read_status(s, nullptr, &halted));
+    if (halted) {
+        CG_TRY(recover(s));
+        return set_err(CG_ERR_STATE, "step halted for a global rebuild; state restored, step not taken");
+    }
+    return CG_OK;
+}
+
+// poll: synchronise, report completed steps and whether the device halted; recover if asked
+extern "C" int cg_poll(cg_system *s, int *steps_done, int *halted, int recover_if_halted)
+{
+    if (!s) return set_err(CG_ERR_ARG, "null system");
+    CG_CUDA(cudaStreamSynchronize(s->stream));
+    int h = 0;
+    CG_TRY(read_status(s, steps_done, &h));
+    if (halted) *halted = h;
+    if (h && recover_if_halted) CG_TRY(recover(s));
+    return CG_OK;
+}
+
+// the fused geometry+force(+test) pass alone, enqueued without synchronisation
+extern "C" int cg_launch_force_pass(cg_system *s, int with_test)
+{
+    if (!s || s->model != CG_MODEL_VORONOI) return set_err(CG_ERR_ARG, "bad args");
+    VoroArgs a = sys_args(s);
+    if (s->precision == CG_FP64)
+        launch_force_test<double>(s, a, with_test != 0);
+    else
+        launch_force_test<float>(s, a, with_test != 0);
+    return check_launch();
+}
+
+extern "C" long long cg_kernels_launched(const cg_system *s) { return s ? s->kernels_enqueued : 0; }
+
+extern "C" int cg_spp_run(cg_system *s, int n_steps, double dt, double mu, const double *noise_dev)
+{
+    if (!s || s->model != CG_MODEL_VORONOI || n_steps < 0) return set_err(CG_ERR_ARG, "bad args");
+    if (!s->topology_valid) CG_TRY(triangulate_sys(s));
+    return s->precision == CG_FP64 ? spp_run_t<double>(s, n_steps, dt, mu, noise_dev)
+                                   : spp_run_t<float>(s, n_steps, dt, mu, noise_dev);
+}
+
+extern "C" int cg_get_energies(cg_system *s, double *E)
+{
+    if (!s || !E) return set_err(CG_ERR_ARG, "bad args");
+    VoroArgs a = sys_args(s);
+    CG_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * s->n_inst, s->stream));
+    if (s->precision == CG_FP64)
+        k_energy<double><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
+    else
+        k_energy<float><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
+    CG_TRY(check_launch());
+    return d2h(s, E, s->d_energy, sizeof(double) * s->n_inst);
+}

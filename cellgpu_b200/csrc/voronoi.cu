@@ -1,0 +1,777 @@
+// cellgpu_b200 -- Voronoi (SPV) model kernels for sm_100a.
+//
+// Design (B200-first, not a translation of the reference's kernels):
+//  * One fused pass per cell computes the Voronoi polygon, A and P, and the force contributions
+//    of that cell's energy to itself and to every neighbour (scatter form). A cell only needs its
+//    own neighbour ring, so no per-slot voroCur / voroLastNext / forceSets / delSets / delOther
+//    arrays are materialised in HBM (the reference writes and re-reads ~100 B per slot of those).
+//  * The same pass runs the exact local-Delaunay test of the stored triangulation on the current
+//    positions (every triangle counter-clockwise, every edge locally Delaunay). By Lawson's theorem
+//    a valid triangulation whose edges are all locally Delaunay is the Delaunay triangulation, so
+//    this test replaces the reference's cell-list circumcircle scan
+//    (src/models/voronoiModelBase.cu:24-109) for the per-step check.
+//  * Flagged cells and their neighbours (the reference's NeedsFixing set,
+//    src/models/voronoiModelBase.cpp:632-646) get their Delaunay star recomputed exactly on the
+//    device, one warp per cell; changed rows retract their old force contributions and add the new
+//    ones, so forces always correspond to the repaired topology. Rounds continue until every
+//    changed row is consistent with its partners; otherwise the step halts and the host runs the
+//    device-side global triangulation (cell list + exact stars), the role of
+//    globalTriangulationCGAL (src/models/voronoiModelBase.cpp:281-351).
+#include "voronoi.cuh"
+
+#include <cub/device/device_scan.cuh>
+
+namespace cg {
+
+// ------------------------------------------------------------------------------------------
+// small vector helpers for FP64 / FP32 geometry
+// ------------------------------------------------------------------------------------------
+template <typename R>
+struct Vec2;
+template <>
+struct Vec2<double> {
+    using T = double2;
+};
+template <>
+struct Vec2<float> {
+    using T = float2;
+};
+
+template <typename R>
+CG_D typename Vec2<R>::T mk(R x, R y)
+{
+    typename Vec2<R>::T v;
+    v.x = x;
+    v.y = y;
+    return v;
+}
+
+template <typename R>
+CG_D typename Vec2<R>::T cvt(double2 d)
+{
+    return mk<R>((R)d.x, (R)d.y);
+}
+
+// Circumcenter(x1,x2,xc) of (0, a, b) (inc/utility/functions.h:34-43)
+template <typename R, typename V>
+CG_D V circum0(V a, V b)
+{
+    R an = a.x * a.x + a.y * a.y;
+    R bn = b.x * b.x + b.y * b.y;
+    R den = R(0.5) / (a.x * b.y - a.y * b.x);
+    return mk<R>(den * (an * b.y - a.y * bn), den * (a.x * bn - an * b.x));
+}
+
+// getdhdr (inc/utility/functions.h:234-287): d h / d r_0 for h = circumcentre(r_0, r_0+rij, r_0+rik),
+// row = component of h, column = component of r_0.
+template <typename R, typename V>
+CG_D void dhdr(V rij, V rik, R &m11, R &m12, R &m21, R &m22)
+{
+    R cr = rij.y * rik.x - rij.x * rik.y;
+    R den = R(0.5) / (cr * cr);
+    R rik2 = rik.x * rik.x + rik.y * rik.y;
+    R rij2 = rij.x * rij.x + rij.y * rij.y;
+    R t1 = rik.y * rij2 - rij.y * rik2;
+    R t2 = rik.x * rij2 - rij.x * rik2;
+    m11 = den * (rik.y - rij.y) * t1;
+    m12 = den * (rij.y - rik.y) * t2;
+    m21 = den * (rij.x - rik.x) * t1;
+    m22 = den * (rik.x - rij.x) * t2;
+}
+
+template <typename R>
+CG_D void atomic_add2(void *F, int i, R x, R y);
+template <>
+CG_D void atomic_add2<double>(void *F, int i, double x, double y)
+{
+    double *f = reinterpret_cast<double *>(F) + 2 * (size_t)i;
+    atomicAdd(f, x);
+    atomicAdd(f + 1, y);
+}
+template <>
+CG_D void atomic_add2<float>(void *F, int i, float x, float y)
+{
+    atomicAdd(reinterpret_cast<float2 *>(F) + i, make_float2(x, y));
+}
+
+template <typename R>
+CG_D void store_ap(void *AP, int i, R A, R P)
+{
+    reinterpret_cast<typename Vec2<R>::T *>(AP)[i] = mk<R>(A, P);
+}
+
+CG_D const Inst &inst_of(const VoroArgs &a, int c)
+{
+    return a.inst ? a.inst[a.cell_inst ? a.cell_inst[c] : 0] : a.inst0;
+}
+
+// claim cell x for epoch e (first claimer wins) and append it to queue q
+CG_D void claim_enqueue(const VoroArgs &a, int x, int e, int q)
+{
+    if (atomicMax(&a.mark[x], e) < e) {
+        int slot = atomicAdd(&a.ctl->q_count[q], 1);
+        a.queue[(size_t)q * a.N + slot] = x;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// The per-cell pass. Pass 1: Voronoi vertices h_k = circumcentre(0, r_{k-1}, r_k) relative to the
+// cell (the CPU convention, src/models/voronoiModelBase.cpp:805-822), A = sum |h_k x h_{k+1}|/2,
+// P = sum |h_k - h_{k+1}|, and (TEST) the exact local-Delaunay test. Pass 2 (SCATTER): with
+// g_k = -dE_c/dh_k (E_c = KA (A-A0)^2 + KP (P-P0)^2; the derivatives of
+// src/models/voronoiQuadraticEnergy.cpp:241-256 with the THRESHOLD clamp of :275-278), the force on
+// cell x is the sum over the Voronoi vertices h of all cells of g . dh/dr_x; a vertex of c depends
+// on c and the two neighbours that define it, with dh/dr_c = getdhdr(r_a, r_b),
+// dh/dr_a = getdhdr(-r_a, r_b - r_a), dh/dr_b = I - dh/dr_c - dh/dr_a (translation invariance).
+// sign = -1 retracts a stale row's contributions.
+// Returns a test code: 0 ok, else (slot+1) of the first failing slot, negated for an orientation
+// failure.
+// ------------------------------------------------------------------------------------------
+template <typename R, bool SCATTER, bool TEST>
+CG_D int cell_pass(const VoroArgs &a, int c, const int *row, int z, double2 pc, double Lx, double Ly,
+                   R sign, R &A_out, R &P_out)
+{
+    using V = typename Vec2<R>::T;
+    const double2 *pos = a.pos;
+    int fail = 0;
+    if (z < 3) return -1;
+
+    // ---- pass 1
+    int nA = row[z - 1], nB = row[0];
+    double2 dA = min_dist(pos[nA], pc, Lx, Ly);
+    double2 dB = min_dist(pos[nB], pc, Lx, Ly);
+    V hprev = circum0<R>(cvt<R>(dA), cvt<R>(dB));  // h_0
+    V hfirst = hprev;
+    R Asum = 0, Psum = 0;
+    for (int k = 0; k < z; ++k) {
+        int kn = (k + 1 == z) ? 0 : k + 1;
+        int nC = row[kn];
+        double2 dC = min_dist(pos[nC], pc, Lx, Ly);
+        if (TEST && !fail) {
+            if (orient0(dB, dC) <= 0) fail = -(k + 1);
+            else if (c < nB && incircle0(dA, dB, dC) < 0) fail = k + 1;
+        }
+        V hnext = (kn == 0) ? hfirst : circum0<R>(cvt<R>(dB), cvt<R>(dC));
+        Asum += fabs(R(0.5) * (hprev.x * hnext.y - hprev.y * hnext.x));
+        R dx = hprev.x - hnext.x, dy = hprev.y - hnext.y;
+        Psum += sqrt(dx * dx + dy * dy);
+        hprev = hnext;
+        dA = dB;
+        dB = dC;
+        nB = nC;
+    }
+    A_out = Asum;
+    P_out = Psum;
+
+    if (SCATTER) {
+        const R thr = R(1e-18);
+        R Adiff = R(a.KA) * (Asum - (R)a.APpref[c].x);
+        R Pdiff = R(a.KP) * (Psum - (R)a.APpref[c].y);
+        // window: r_{k-1} = rA, r_k = rB, r_{k+1} = rC ; h_{k-1} = hP, h_k = hC, h_{k+1} = hN
+        V rZ = cvt<R>(min_dist(pos[row[z - 2]], pc, Lx, Ly));
+        V rA = cvt<R>(min_dist(pos[row[z - 1]], pc, Lx, Ly));
+        V rB = cvt<R>(min_dist(pos[row[0]], pc, Lx, Ly));
+        V rC = cvt<R>(min_dist(pos[row[1]], pc, Lx, Ly));
+        V hP = circum0<R>(rZ, rA);
+        V hC = circum0<R>(rA, rB);
+        V hN = circum0<R>(rB, rC);
+        R sx = 0, sy = 0;          // self
+        R pendx = 0, pendy = 0;    // slot k (b part), waiting for the a part of vertex k+1
+        R fax = 0, fay = 0;        // a part of vertex 0, belongs to slot z-1
+        for (int k = 0; k < z; ++k) {
+            // g = -dE/dh_k
+            R dAx = R(0.5) * (hN.y - hP.y), dAy = R(0.5) * (hP.x - hN.x);
+            R lx = hC.x - hP.x, ly = hC.y - hP.y;
+            R ln = sqrt(lx * lx + ly * ly);
+            if (ln < thr) ln = thr;
+            R nx = hC.x - hN.x, ny = hC.y - hN.y;
+            R nnm = sqrt(nx * nx + ny * ny);
+            if (nnm < thr) nnm = thr;
+            R dPx = lx / ln + nx / nnm, dPy = ly / ln + ny / nnm;
+            R gx = -R(2) * (Adiff * dAx + Pdiff * dPx);
+            R gy = -R(2) * (Adiff * dAy + Pdiff * dPy);
+            // Jacobians of h_k
+            R c11, c12, c21, c22, a11, a12, a21, a22;
+            dhdr<R>(rA, rB, c11, c12, c21, c22);
+            dhdr<R>(mk<R>(-rA.x, -rA.y), mk<R>(rB.x - rA.x, rB.y - rA.y), a11, a12, a21, a22);
+            R b11 = R(1) - c11 - a11, b12 = -c12 - a12, b21 = -c21 - a21, b22 = R(1) - c22 - a22;
+            sx += gx * c11 + gy * c21;
+            sy += gx * c12 + gy * c22;
+            R cax = gx * a11 + gy * a21, cay = gx * a12 + gy * a22;
+            R cbx = gx * b11 + gy * b21, cby = gx * b12 + gy * b22;
+            if (k == 0) {
+                fax = cax;
+                fay = cay;
+            } else {
+                atomic_add2<R>(a.F, row[k - 1], sign * (pendx + cax), sign * (pendy + cay));
+            }
+            pendx = cbx;
+            pendy = cby;
+            // advance the window
+            if (k + 1 < z) {
+                int k2 = k + 2;
+                if (k2 >= z) k2 -= z;
+                hP = hC;
+                hC = hN;
+                rA = rB;
+                rB = rC;
+                rC = cvt<R>(min_dist(pos[row[k2]], pc, Lx, Ly));
+                hN = circum0<R>(rB, rC);
+            }
+        }
+        atomic_add2<R>(a.F, row[z - 1], sign * (pendx + fax), sign * (pendy + fay));
+        atomic_add2<R>(a.F, c, sign * sx, sign * sy);
+    }
+    return fail;
+}
+
+// ------------------------------------------------------------------------------------------
+// fused geometry + forces (+ exact test, + repair queue seeding)
+// ------------------------------------------------------------------------------------------
+template <typename R, bool SCATTER, bool TEST>
+__global__ void __launch_bounds__(128) k_voro_cells(VoroArgs a)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.N) return;
+    if (a.ctl && a.ctl->halt) return;
+    const Inst &in = inst_of(a, c);
+    double2 pc = a.pos[c];
+    int z = a.nn[c];
+    const int *row = a.nbr + (size_t)c * a.K;
+    R A, P;
+    int fail = cell_pass<R, SCATTER, TEST>(a, c, row, z, pc, in.Lx, in.Ly, R(1), A, P);
+    if (a.AP) store_ap<R>(a.AP, c, A, P);
+    if (TEST && fail) {
+        if (a.ctl) {
+            int e = a.ctl->epoch;
+            atomicAdd(&a.ctl->n_flagged, 1);
+            int k = (fail > 0 ? fail : -fail) - 1;
+            // the cell, the edge's other end and the two apexes (or the triangle's corners)
+            claim_enqueue(a, c, e, 0);
+            claim_enqueue(a, row[k], e, 0);
+            claim_enqueue(a, row[(k + 1) % z], e, 0);
+            if (fail > 0) claim_enqueue(a, row[(k + z - 1) % z], e, 0);
+        } else if (a.mark) {
+            // raw test API: mark = flag array, queue[0] = any_fail word
+            int k = (fail > 0 ? fail : -fail) - 1;
+            a.mark[c] = 1;
+            a.mark[row[k]] = 1;
+            a.mark[row[(k + 1) % z]] = 1;
+            if (fail > 0) a.mark[row[(k + z - 1) % z]] = 1;
+            a.queue[0] = 1;
+        }
+    }
+}
+
+// flagged cells -> flagged cells and their neighbours (NeedsFixing,
+// src/models/voronoiModelBase.cpp:632-646); escalate when too many
+// (launched as ONE block: the seed count is read before any thread appends)
+__global__ void k_expand(VoroArgs a)
+{
+    Ctl *ctl = a.ctl;
+    if (ctl->halt) return;
+    int nflag = ctl->q_count[0];
+    __syncthreads();
+    if (nflag == 0) return;
+    int e = ctl->epoch;
+    for (int t = threadIdx.x; t < nflag; t += blockDim.x) {
+        int c = a.queue[t];
+        int z = a.nn[c];
+        for (int k = 0; k < z; ++k) claim_enqueue(a, a.nbr[(size_t)c * a.K + k], e, 0);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// warp-cooperative exact Delaunay star of the origin among m candidates in shared memory.
+// Gift wrapping: start from the nearest candidate (always a Delaunay neighbour); from neighbour a,
+// the next counter-clockwise neighbour is the candidate strictly counter-clockwise of a whose circle
+// through (0, a, b) is innermost in the pencil of circles through 0 and a (exact in-circle order,
+// ties by index). Each step is a warp argmin under that order. Writes global indices, CCW, rotated
+// to start at the smallest index. Returns z, -1 (not enclosed), -2 (capacity).
+// ------------------------------------------------------------------------------------------
+CG_D bool inner_than(double2 pa, double2 pc, int ic, double2 pb, int ib)
+{
+    // is c's circle through (0,a,c) strictly inside b's circle (0,a,b)?  <=> c inside circle(0,a,b)
+    int s = incircle0(pa, pb, pc);
+    return s < 0 || (s == 0 && ic < ib);
+}
+
+__device__ int warp_star(const double2 *rel, const int *gidx, int m, int K, int *out, int lane)
+{
+    // nearest candidate
+    double best = 1e300;
+    int bi = -1;
+    for (int t = lane; t < m; t += WARP) {
+        double d = rel[t].x * rel[t].x + rel[t].y * rel[t].y;
+        if (d < best || (d == best && bi >= 0 && gidx[t] < gidx[bi])) {
+            best = d;
+            bi = t;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        double ob = __shfl_xor_sync(0xffffffffu, best, off);
+        int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (oi >= 0 && (bi < 0 || ob < best || (ob == best && gidx[oi] < gidx[bi]))) {
+            best = ob;
+            bi = oi;
+        }
+    }
+    if (bi < 0) return -1;
+    int start = bi, cur = bi, z = 0;
+    for (int guard = 0; guard <= m; ++guard) {
+        if (z >= K) return -2;
+        if (lane == 0) out[z] = cur;
+        ++z;
+        double2 pa = rel[cur];
+        int b = -1;
+        for (int t = lane; t < m; t += WARP) {
+            if (t == cur) continue;
+            double2 pt = rel[t];
+            if (orient0(pa, pt) <= 0) continue;
+            if (b < 0 || inner_than(pa, pt, gidx[t], rel[b], gidx[b])) b = t;
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            int ob = __shfl_xor_sync(0xffffffffu, b, off);
+            if (ob >= 0 && (b < 0 || inner_than(pa, rel[ob], gidx[ob], rel[b], gidx[b]))) b = ob;
+        }
+        if (b < 0) return -1;
+        if (b == start) {
+            __syncwarp();
+            // map to global indices and rotate to the smallest
+            int mn = 0x7fffffff, mpos = 0;
+            for (int t = 0; t < z; ++t) {
+                int g = gidx[out[t]];
+                if (g < mn) {
+                    mn = g;
+                    mpos = t;
+                }
+            }
+            __syncwarp();
+            int tmp = 0;
+            if (lane < z) tmp = gidx[out[(mpos + lane) % z]];
+            __syncwarp();
+            if (lane < z) out[lane] = tmp;
+            __syncwarp();
+            return z;
+        }
+        cur = b;
+    }
+    return -1;
+}
+
+// dedupe the raw candidate list in place (drops `self` and repeats), keeping first occurrences
+CG_D int warp_unique(int *cand, int m, int self, int lane)
+{
+    int out = 0;
+    for (int base = 0; base < m; base += WARP) {
+        int t = base + lane;
+        int v = (t < m) ? cand[t] : -1;
+        bool keep = (t < m) && v != self;
+        if (keep)
+            for (int u = 0; u < t; ++u)
+                if (cand[u] == v) {
+                    keep = false;
+                    break;
+                }
+        unsigned bal = __ballot_sync(0xffffffffu, keep);
+        __syncwarp();
+        if (keep) cand[out + __popc(bal & ((1u << lane) - 1u))] = v;
+        out += __popc(bal);
+        __syncwarp();
+    }
+    return out;
+}
+
+// compact the candidate list in place, dropping `self` (no repeats possible)
+CG_D int warp_remove(int *cand, int m, int self, int lane)
+{
+    int out = 0;
+    for (int base = 0; base < m; base += WARP) {
+        int t = base + lane;
+        int v = (t < m) ? cand[t] : -1;
+        bool keep = (t < m) && v != self;
+        unsigned bal = __ballot_sync(0xffffffffu, keep);
+        __syncwarp();
+        if (keep) cand[out + __popc(bal & ((1u << lane) - 1u))] = v;
+        out += __popc(bal);
+        __syncwarp();
+    }
+    return out;
+}
+
+// Local repair star: candidates = the current 2-ring of the cell (its neighbours and theirs).
+// One warp per queued cell; result goes to the staging row of the queue slot.
+template <int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a, int round)
+{
+    __shared__ int s_cand[WPB][CAND_LOCAL];
+    __shared__ double2 s_rel[WPB][CAND_LOCAL];
+    __shared__ int s_out[WPB][KMAX];
+    Ctl *ctl = a.ctl;
+    if (ctl->halt) return;
+    int nq = ctl->q_count[round];
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int gw = blockIdx.x * WPB + w, nw = gridDim.x * WPB;
+    const int *queue = a.queue + (size_t)round * a.N;
+    for (int q = gw; q < nq; q += nw) {
+        int c = queue[q];
+        const Inst &in = inst_of(a, c);
+        int z = a.nn[c];
+        const int *row = a.nbr + (size_t)c * a.K;
+        int m = 0;
+        if (lane < z) s_cand[w][lane] = row[lane];
+        m = z;
+        __syncwarp();
+        for (int k = 0; k < z; ++k) {
+            int x = s_cand[w][k];
+            int zx = a.nn[x];
+            if (m + zx > CAND_LOCAL) break;
+            if (lane < zx) s_cand[w][m + lane] = a.nbr[(size_t)x * a.K + lane];
+            m += zx;
+            __syncwarp();
+        }
+        m = warp_unique(s_cand[w], m, c, lane);
+        double2 pc = a.pos[c];
+        for (int t = lane; t < m; t += WARP)
+            s_rel[w][t] = min_dist(a.pos[s_cand[w][t]], pc, in.Lx, in.Ly);
+        __syncwarp();
+        int zs = warp_star(s_rel[w], s_cand[w], m, a.K, s_out[w], lane);
+        if (zs < 0) {
+            if (lane == 0) {
+                atomicExch(&ctl->need_global, 1);
+                atomicExch(&ctl->status, zs == -2 ? CG_ERR_CAPACITY : CG_ERR_TOPOLOGY);
+                atomicExch(&ctl->halt, 1);
+            }
+            continue;
+        }
+        if (lane < zs) a.stage_nbr[(size_t)q * a.K + lane] = s_out[w][lane];
+        if (lane == 0) a.stage_nn[q] = zs;
+        __syncwarp();
+    }
+}
+
+// Commit staged rows: rows that changed retract their old contributions and add the new ones
+// (forces stay consistent with the topology), A/P are refreshed, and the old row is kept in the
+// staging slot for the consistency check.
+template <typename R, bool FORCES>
+__global__ void k_commit(VoroArgs a, int round)
+{
+    Ctl *ctl = a.ctl;
+    if (ctl->halt) return;
+    int nq = ctl->q_count[round];
+    const int *queue = a.queue + (size_t)round * a.N;
+    int stride = gridDim.x * blockDim.x;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
+        int c = queue[q];
+        int zo = a.nn[c], zn = a.stage_nn[q];
+        int *row = a.nbr + (size_t)c * a.K;
+        int *srow = a.stage_nbr + (size_t)q * a.K;
+        bool same = (zo == zn);
+        for (int k = 0; same && k < zn; ++k) same = (row[k] == srow[k]);
+        if (same) continue;
+        const Inst &in = inst_of(a, c);
+        double2 pc = a.pos[c];
+        R A, P;
+        if (FORCES) cell_pass<R, true, false>(a, c, row, zo, pc, in.Lx, in.Ly, R(-1), A, P);
+        // swap rows
+        for (int k = 0; k < a.K; ++k) {
+            int t = (k < zn) ? srow[k] : -1;
+            srow[k] = (k < zo) ? row[k] : -1;
+            row[k] = t;
+        }
+        a.stage_nn[q] = zo;
+        a.nn[c] = zn;
+        cell_pass<R, FORCES, false>(a, c, row, zn, pc, in.Lx, in.Ly, R(1), A, P);
+        if (a.AP) store_ap<R>(a.AP, c, A, P);
+        int slot = atomicAdd(&ctl->n_changed[round], 1);
+        a.changed[(size_t)round * a.N + slot] = q;
+        atomicAdd(&ctl->counters[2], 1ull);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&ctl->counters[1], (unsigned long long)nq);
+        atomicAdd(&ctl->counters[3], 1ull);
+    }
+}
+
+CG_D int row_find(const int *row, int z, int v)
+{
+    for (int k = 0; k < z; ++k)
+        if (row[k] == v) return k;
+    return -1;
+}
+
+// does row (length z) contain u immediately followed (cyclically) by v?
+CG_D bool row_has_pair(const int *row, int z, int u, int v)
+{
+    int s = row_find(row, z, u);
+    if (s < 0) return false;
+    int t = s + 1;
+    if (t == z) t = 0;
+    return row[t] == v;
+}
+
+// Consistency of the changed rows of a round: every new triangle (c,a,b) must appear in the rows of
+// a and b, every dropped triangle must be gone from them, and the new row must pass the exact local
+// test. Offending cells are queued for the next round.
+__global__ void k_check(VoroArgs a, int round)
+{
+    Ctl *ctl = a.ctl;
+    if (ctl->halt) return;
+    int nch = ctl->n_changed[round];
+    int e = ctl->epoch + round + 1;
+    int nq = round + 1;
+    const int *queue = a.queue + (size_t)round * a.N;
+    int stride = gridDim.x * blockDim.x;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nch; t += stride) {
+        int q = a.changed[(size_t)round * a.N + t];
+        int c = queue[q];
+        const int *row = a.nbr + (size_t)c * a.K;
+        int z = a.nn[c];
+        const int *orow = a.stage_nbr + (size_t)q * a.K;
+        int zo = a.stage_nn[q];
+        for (int k = 0; k < z; ++k) {
+            int u = row[k], v = row[(k + 1) % z];
+            if (!row_has_pair(a.nbr + (size_t)u * a.K, a.nn[u], v, c)) claim_enqueue(a, u, e, nq);
+            if (!row_has_pair(a.nbr + (size_t)v * a.K, a.nn[v], c, u)) claim_enqueue(a, v, e, nq);
+        }
+        for (int k = 0; k < zo; ++k) {
+            int u = orow[k], v = orow[(k + 1) % zo];
+            if (row_has_pair(row, z, u, v)) continue;  // triangle kept
+            if (row_has_pair(a.nbr + (size_t)u * a.K, a.nn[u], v, c)) claim_enqueue(a, u, e, nq);
+            if (row_has_pair(a.nbr + (size_t)v * a.K, a.nn[v], c, u)) claim_enqueue(a, v, e, nq);
+        }
+        // exact local test of the new row
+        const Inst &in = inst_of(a, c);
+        double2 pc = a.pos[c];
+        double2 dA = min_dist(a.pos[row[z - 1]], pc, in.Lx, in.Ly);
+        double2 dB = min_dist(a.pos[row[0]], pc, in.Lx, in.Ly);
+        bool bad = false;
+        for (int k = 0; k < z && !bad; ++k) {
+            double2 dC = min_dist(a.pos[row[(k + 1) % z]], pc, in.Lx, in.Ly);
+            if (orient0(dB, dC) <= 0) bad = true;
+            else if (incircle0(dA, dB, dC) < 0) bad = true;
+            dA = dB;
+            dB = dC;
+        }
+        if (bad) {
+            claim_enqueue(a, c, e, nq);
+            for (int k = 0; k < z; ++k) claim_enqueue(a, row[k], e, nq);
+        }
+    }
+}
+
+// after the last round: anything still queued means the local repair did not converge
+__global__ void k_finish_repair(VoroArgs a)
+{
+    Ctl *ctl = a.ctl;
+    if (ctl->halt) return;
+    if (ctl->q_count[R_MAX] > 0) {
+        ctl->need_global = 1;
+        ctl->status = CG_ERR_TOPOLOGY;
+        ctl->halt = 1;
+    }
+}
+
+// end of a step: reset the per-step queue counters and advance the claim epoch
+__global__ void k_step_done(Ctl *ctl, int advance_step)
+{
+    if (ctl->halt) return;
+    ctl->step += advance_step;
+    if (ctl->n_flagged) atomicAdd(&ctl->counters[0], (unsigned long long)ctl->n_flagged);
+    ctl->n_flagged = 0;
+    for (int r = 0; r <= R_MAX; ++r) ctl->q_count[r] = 0;
+    for (int r = 0; r < R_MAX; ++r) ctl->n_changed[r] = 0;
+    ctl->epoch += R_MAX + 2;
+}
+
+// ------------------------------------------------------------------------------------------
+// cell list (counting sort, per-instance grids) and the global triangulation
+// ------------------------------------------------------------------------------------------
+CG_D int bin_of(const Inst &in, double2 p)
+{
+    int bx = (int)floor(p.x / in.bsx), by = (int)floor(p.y / in.bsy);
+    bx = max(0, min(in.nbx - 1, bx));
+    by = max(0, min(in.nby - 1, by));
+    return in.bin_off + by * in.nbx + bx;
+}
+
+__global__ void k_bin_count(VoroArgs a)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.N) return;
+    const Inst &in = inst_of(a, c);
+    int b = bin_of(in, a.pos[c]);
+    a.cell_bin[c] = b;
+    a.cell_slot[c] = atomicAdd(&a.bin_count[b], 1);
+}
+
+__global__ void k_bin_scatter(VoroArgs a)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.N) return;
+    int s = a.bin_start[a.cell_bin[c]] + a.cell_slot[c];
+    a.bin_cells[s] = c;
+    a.bin_pos[s] = a.pos[c];
+}
+
+// Global star of every cell from cell-list candidates in a (2w+1)^2 bin block. A star is accepted
+// when every star triangle's circumcircle lies inside the covered disk of radius w*bin, which makes
+// it the exact Delaunay star; otherwise the block grows.
+template <int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_star_global(VoroArgs a, int *status)
+{
+    __shared__ int s_idx[WPB][CAND_GLOBAL];
+    __shared__ double2 s_rel[WPB][CAND_GLOBAL];
+    __shared__ int s_out[WPB][KMAX];
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int c = blockIdx.x * WPB + w;
+    if (c >= a.N) return;
+    const Inst &in = inst_of(a, c);
+    double2 pc = a.pos[c];
+    int cbx = (int)floor(pc.x / in.bsx), cby = (int)floor(pc.y / in.bsy);
+    cbx = max(0, min(in.nbx - 1, cbx));
+    cby = max(0, min(in.nby - 1, cby));
+    int wmaxx = (in.nbx - 1) / 2, wmaxy = (in.nby - 1) / 2;
+    double bs = fmin(in.bsx, in.bsy);
+    for (int wr = 2;; ++wr) {
+        int wx = min(wr, wmaxx), wy = min(wr, wmaxy);
+        int m = 0;
+        bool overflow = false;
+        for (int dy = -wy; dy <= wy && !overflow; ++dy)
+            for (int dx = -wx; dx <= wx && !overflow; ++dx) {
+                int bx = cbx + dx, by = cby + dy;
+                if (bx < 0) bx += in.nbx;
+                if (bx >= in.nbx) bx -= in.nbx;
+                if (by < 0) by += in.nby;
+                if (by >= in.nby) by -= in.nby;
+                int b = in.bin_off + by * in.nbx + bx;
+                int s0 = a.bin_start[b], cnt = a.bin_count[b];
+                if (m + cnt > CAND_GLOBAL) {
+                    overflow = true;
+                    break;
+                }
+                for (int t = lane; t < cnt; t += WARP) s_idx[w][m + t] = a.bin_cells[s0 + t];
+                m += cnt;
+            }
+        __syncwarp();
+        if (overflow) {
+            if (lane == 0) atomicCAS(status, 0, CG_ERR_CAPACITY);
+            return;
+        }
+        __syncwarp();
+        m = warp_remove(s_idx[w], m, c, lane);
+        for (int t = lane; t < m; t += WARP) s_rel[w][t] = min_dist(a.pos[s_idx[w][t]], pc, in.Lx, in.Ly);
+        __syncwarp();
+        int z = warp_star(s_rel[w], s_idx[w], m, a.K, s_out[w], lane);
+        bool ok = z > 0;
+        double R = (double)min(wx, wy) * bs;
+        if (ok) {
+            // containment: all triangle circumcircles inside the covered disk
+            bool good = true;
+            for (int t = lane; t < z; t += WARP) {
+                int u = s_out[w][t], v = s_out[w][(t + 1) % z];
+                double2 ru = min_dist(a.pos[u], pc, in.Lx, in.Ly);
+                double2 rv = min_dist(a.pos[v], pc, in.Lx, in.Ly);
+                double2 q = circum0<double>(ru, rv);
+                double r = sqrt(q.x * q.x + q.y * q.y);
+                if (!(2.0 * r < R * (1.0 - 1e-9))) good = false;
+            }
+            ok = __all_sync(0xffffffffu, good);
+        }
+        if (ok) {
+            if (lane < z) a.nbr[(size_t)c * a.K + lane] = s_out[w][lane];
+            if (lane == 0) a.nn[c] = z;
+            return;
+        }
+        if (z == -2) {
+            if (lane == 0) atomicCAS(status, 0, CG_ERR_CAPACITY);
+            return;
+        }
+        if (wx >= wmaxx && wy >= wmaxy) {
+            if (lane == 0) atomicCAS(status, 0, CG_ERR_TOPOLOGY);
+            return;
+        }
+    }
+}
+
+// triangle-consistency and Euler check of a full triangulation: every triangle (c,u,v) of every row
+// must appear in the rows of u and v; per instance, sum z = 6 N.
+__global__ void k_validate(VoroArgs a, int *status, unsigned long long *zsum)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.N) return;
+    const int *row = a.nbr + (size_t)c * a.K;
+    int z = a.nn[c];
+    atomicAdd(&zsum[a.cell_inst[c]], (unsigned long long)z);
+    for (int k = 0; k < z; ++k) {
+        int u = row[k], v = row[(k + 1) % z];
+        if (!row_has_pair(a.nbr + (size_t)u * a.K, a.nn[u], v, c) ||
+            !row_has_pair(a.nbr + (size_t)v * a.K, a.nn[v], c, u)) {
+            atomicCAS(status, 0, CG_ERR_TOPOLOGY);
+            return;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// integrators, fused with move-and-wrap
+// ------------------------------------------------------------------------------------------
+
+// selfPropelledParticleDynamics::integrateEquationsOfMotionCPU
+// (src/updaters/selfPropelledParticleDynamics.cpp:67-101) + movePoints (Simple2DCell.cu:21-58):
+// v from the current director, displacement dt (v + mu F), director <- atan2(v) + noise.
+template <typename R>
+__global__ void k_spp(VoroArgs a, const double *noise, double dt, double mu, uint64_t seed,
+                      int zero_force)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    Ctl *ctl = a.ctl;
+    if (ctl && ctl->halt) return;
+    if (c < a.N) {
+        const Inst &in = inst_of(a, c);
+        typename Vec2<R>::T f = reinterpret_cast<typename Vec2<R>::T *>(a.F)[c];
+        double fx = (double)f.x, fy = (double)f.y;
+        double2 mot = a.motility[c];
+        double th = a.theta[c];
+        double s, co;
+        sincos(th, &s, &co);
+        double vx = __dmul_rn(mot.x, co), vy = __dmul_rn(mot.x, s);
+        double dx = __dmul_rn(dt, __dadd_rn(vx, __dmul_rn(mu, fx)));
+        double dy = __dmul_rn(dt, __dadd_rn(vy, __dmul_rn(mu, fy)));
+        double thn = th;
+        if (!(vx == 0. && vy == 0.)) thn = atan2(vy, vx);
+        double xi;
+        if (noise) {
+            xi = noise[c];
+        } else {
+            uint32_t step = ctl ? (uint32_t)ctl->step : 0u;
+            xi = normal2(seed, (uint32_t)c, step, 0u).x;
+        }
+        a.theta[c] = __dadd_rn(thn, __dmul_rn(xi, sqrt(__dmul_rn(__dmul_rn(2.0, dt), mot.y))));
+        double2 p = a.pos[c];
+        p.x = __dadd_rn(p.x, dx);
+        p.y = __dadd_rn(p.y, dy);
+        a.pos[c] = put_in_box(p, in.Lx, in.Ly, in.iLx, in.iLy);
+        if (zero_force) reinterpret_cast<typename Vec2<R>::T *>(a.F)[c] = mk<R>(R(0), R(0));
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// energies per instance (FP64 accumulation)
+// ------------------------------------------------------------------------------------------
+template <typename R>
+__global__ void k_energy(VoroArgs a, double *E)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    int inst = 0;
+    if (c < a.N) {
+        typename Vec2<R>::T ap = reinterpret_cast<typename Vec2<R>::T *>(a.AP)[c];
+        double da = (double)ap.x - a.APpref[c].x, dp = (double)ap.y - a.APpref[c].y;
+        e = a.KA * da * da + a.KP * dp * dp;
+        inst = a.cell_inst ? a.cell_inst[c] : 0;
+        atomicAdd(&E[inst], e);
+    }
+}
+
+}  // namespace cg

@@ -1,0 +1,55 @@
+// cellgpu_b200 -- Voronoi-model device state and kernel declarations.
+#pragma once
+
+#include "cg_common.cuh"
+
+namespace cg {
+
+constexpr int KMAX = 32;          // largest supported neighbour-row capacity
+constexpr int R_MAX = 4;          // local repair rounds per step before escalating to a global rebuild
+constexpr int CAND_LOCAL = 320;   // candidate slots per warp for the local (2-ring) star
+constexpr int CAND_GLOBAL = 384;  // candidate slots per warp for the cell-list star
+
+// device control block of one system
+struct Ctl {
+    int epoch;               // base claim epoch of the current step
+    int halt;                // sticky: a step could not complete on the device
+    int need_global;         // a global retriangulation is required
+    int status;              // CG_* code explaining halt
+    int n_flagged;           // cells flagged by the test of this step
+    int q_count[R_MAX + 1];  // per-round queue lengths
+    int n_changed[R_MAX];    // per-round changed rows
+    int step;                // completed integrator steps since creation
+    int pad;
+    unsigned long long counters[8];  // 0 tests failed, 1 cells restarred, 2 rows changed, 3 rounds,
+                                     // 4 global rebuilds, 5 T1 flips, 6 fire iterations, 7 spare
+};
+
+// everything a Voronoi kernel needs, passed by value
+struct VoroArgs {
+    int N, K, n_inst;
+    Inst inst0;          // used when inst == nullptr (kernel callers on caller memory)
+    const Inst *inst;
+    const int *cell_inst;
+    double2 *pos;
+    double *theta;
+    const double2 *motility;
+    const double2 *APpref;
+    double KA, KP;
+    void *AP;       // double2 (FP64) or float2 (mixed)
+    void *F;        // double2 (FP64) or float2 (mixed), accumulated with atomics
+    int *nn, *nbr;
+    // repair
+    int *mark;
+    int *queue;     // (R_MAX+1) * N
+    int *stage_nn;  // N
+    int *stage_nbr; // N * K
+    int *changed;   // R_MAX * N  (queue slots whose rows changed)
+    Ctl *ctl;
+    // cell list
+    int *bin_count, *bin_start, *bin_cells, *cell_bin, *cell_slot;
+    double2 *bin_pos;
+    int n_bins;
+};
+
+}  // namespace cg

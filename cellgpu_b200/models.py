@@ -1,0 +1,309 @@
+"""Host-side mirror of the reference's class API (abaso/cellGPU ``inc/Simulation.h``,
+``inc/models/voronoiQuadraticEnergy.h``, ``inc/updaters/selfPropelledParticleDynamics.h`` ...) over the
+C ABI. Every compute call goes to the sm_100a library; there is no CPU branch.
+
+Names follow the reference so code written against it reads the same:
+
+    model = VoronoiQuadraticEnergy(300, 1.0, 3.8, reprod=True)   # Voronoi2D is an alias
+    spp = selfPropelledParticleDynamics(300)
+    sim = Simulation(); sim.setConfiguration(model); sim.addUpdater(spp, model)
+    sim.setIntegrationTimestep(0.01)
+    for t in range(1000): sim.performTimestep()
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import CG_FP64, CG_MIXED, check, load, ptr
+
+
+def _f64(a, shape):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(shape))
+
+
+class VoronoiBatch:
+    """A device-resident batch of independent Voronoi monolayers (one launch per step for all).
+
+    ``N`` is a list of cell counts, ``boxes`` a list of (Lx, Ly). A batch of one is the plain
+    drop-in of the reference's single-monolayer path.
+    """
+
+    def __init__(self, N, boxes, K=16, precision=CG_FP64):
+        self._lib = load()
+        self.N = [int(n) for n in N]
+        self.boxes = np.asarray(boxes, dtype=np.float64).reshape(len(self.N), 2)
+        self.K = int(K)
+        self.precision = precision
+        h = C.c_void_p()
+        n_arr = np.asarray(self.N, dtype=np.int32)
+        check(self._lib.cg_voronoi_create(len(self.N), ptr(n_arr), ptr(np.ascontiguousarray(self.boxes)),
+                                          self.K, precision, C.byref(h)))
+        self._h = h
+        self.Ntot = sum(self.N)
+        self.offsets = np.concatenate([[0], np.cumsum(self.N)]).astype(np.int64)
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.cg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- state
+    def set_positions(self, pos):
+        pos = _f64(pos, (self.Ntot, 2))
+        check(self._lib.cg_set_positions(self._h, ptr(pos)))
+
+    def positions(self):
+        out = np.zeros((self.Ntot, 2))
+        check(self._lib.cg_get_positions(self._h, ptr(out)))
+        return out
+
+    def set_preferences(self, APpref):
+        a = _f64(APpref, (self.Ntot, 2))
+        check(self._lib.cg_set_cell_preferences(self._h, ptr(a)))
+
+    def set_moduli(self, KA, KP):
+        check(self._lib.cg_set_moduli(self._h, float(KA), float(KP)))
+
+    def set_motility(self, motility):
+        m = _f64(motility, (self.Ntot, 2))
+        check(self._lib.cg_set_motility(self._h, ptr(m)))
+
+    def set_directors(self, theta):
+        t = _f64(theta, (self.Ntot,))
+        check(self._lib.cg_set_directors(self._h, ptr(t)))
+
+    def directors(self):
+        out = np.zeros(self.Ntot)
+        check(self._lib.cg_get_directors(self._h, ptr(out)))
+        return out
+
+    def set_seed(self, seed):
+        check(self._lib.cg_set_seed(self._h, int(seed) & (2**64 - 1)))
+
+    def forces(self):
+        out = np.zeros((self.Ntot, 2))
+        check(self._lib.cg_get_forces(self._h, ptr(out)))
+        return out
+
+    def area_perimeter(self):
+        out = np.zeros((self.Ntot, 2))
+        check(self._lib.cg_get_area_perimeter(self._h, ptr(out)))
+        return out
+
+    def topology(self):
+        nn = np.zeros(self.Ntot, np.int32)
+        nbr = np.zeros((self.Ntot, self.K), np.int32)
+        check(self._lib.cg_get_topology(self._h, ptr(nn), ptr(nbr)))
+        return nn, nbr
+
+    def set_topology(self, nn, nbr):
+        nn = np.ascontiguousarray(nn, np.int32)
+        nbr = np.ascontiguousarray(nbr, np.int32).reshape(self.Ntot, self.K)
+        check(self._lib.cg_set_topology(self._h, ptr(nn), ptr(nbr)))
+
+    def energies(self):
+        out = np.zeros(len(self.N))
+        check(self._lib.cg_get_energies(self._h, ptr(out)))
+        return out
+
+    def counters(self):
+        out = (C.c_longlong * 8)()
+        check(self._lib.cg_counters(self._h, out, 8))
+        keys = ["tests_failed", "cells_restarred", "rows_changed", "repair_rounds", "global_rebuilds",
+                "t1_flips", "fire_iterations", "spare"]
+        return dict(zip(keys, list(out)))
+
+    # -- compute
+    def triangulate(self):
+        check(self._lib.cg_triangulate(self._h))
+
+    def compute_forces(self):
+        check(self._lib.cg_compute_forces(self._h))
+
+    def enforce_topology(self):
+        check(self._lib.cg_enforce_topology(self._h))
+
+    def spp_run(self, n_steps, dt=0.01, mu=1.0, noise=None):
+        """n_steps SPP steps; noise: optional device tensor (torch) of n_steps*N normals."""
+        check(self._lib.cg_spp_run(self._h, int(n_steps), float(dt), float(mu), ptr(noise)))
+
+    def synchronize(self):
+        check(self._lib.cg_synchronize(self._h))
+
+    def device_bytes(self):
+        return int(self._lib.cg_device_bytes(self._h))
+
+
+def random_positions(N, box, seed):
+    """Seeded uniform positions in [0,Lx)x[0,Ly), x then y per cell like
+    Simple2DCell::setCellPositionsRandomly (src/models/Simple2DCell.cpp:85-100), from numpy's PCG64."""
+    rng = np.random.default_rng(seed)
+    u = rng.random((N, 2))
+    return u * np.asarray(box, dtype=np.float64).reshape(1, 2)
+
+
+class VoronoiQuadraticEnergy:
+    """Voronoi (SPV) model with E = sum KA (A-A0)^2 + KP (P-P0)^2
+    (inc/models/voronoiQuadraticEnergy.h; src/models/voronoiQuadraticEnergy.cpp:28-35)."""
+
+    def __init__(self, n, A0=1.0, P0=3.8, reprod=False, seed=None, K=16, precision=CG_FP64, box=None):
+        L = float(np.sqrt(n))
+        self.box = (L, L) if box is None else tuple(box)
+        self.Ncells = int(n)
+        self.reproducible = reprod
+        if seed is None:
+            seed = 13377 if reprod else int(np.random.SeedSequence().entropy % (2**31))
+        self.seed = seed
+        self.batch = VoronoiBatch([n], [self.box], K=K, precision=precision)
+        self.batch.set_seed(seed)
+        self.batch.set_positions(random_positions(n, self.box, seed))
+        rng = np.random.default_rng(seed + 1)
+        self.batch.set_directors(rng.uniform(0, 2 * np.pi, n))  # Simple2DActiveCell.cpp:55-70
+        self.setCellPreferencesUniform(A0, P0)
+        self.setv0Dr(0.05, 1.0)
+        self.KA, self.KP = 1.0, 1.0
+        self.batch.triangulate()
+        self.forcesUpToDate = False
+
+    # reference API
+    def getNumberOfDegreesOfFreedom(self):
+        return self.Ncells
+
+    def setCellPreferencesUniform(self, A0, P0):
+        self.batch.set_preferences(np.tile([A0, P0], (self.Ncells, 1)))
+        self.forcesUpToDate = False
+
+    def setCellPreferences(self, APpref):
+        self.batch.set_preferences(APpref)
+        self.forcesUpToDate = False
+
+    def setModuliUniform(self, KA, KP):
+        self.KA, self.KP = KA, KP
+        self.batch.set_moduli(KA, KP)
+        self.forcesUpToDate = False
+
+    def setv0Dr(self, v0, Dr):
+        self.batch.set_motility(np.tile([v0, Dr], (self.Ncells, 1)))
+
+    def setCellMotility(self, v0s, Drs):
+        self.batch.set_motility(np.stack([v0s, Drs], axis=1))
+
+    def setCellPositions(self, pos):
+        self.batch.set_positions(pos)
+        self.batch.triangulate()
+        self.forcesUpToDate = False
+
+    def returnPositions(self):
+        return self.batch.positions()
+
+    getCellPositions = returnPositions
+
+    def computeForces(self):
+        if self.forcesUpToDate:
+            return
+        self.batch.compute_forces()
+        self.forcesUpToDate = True
+
+    def returnForces(self):
+        return self.batch.forces()
+
+    getForces = returnForces
+
+    def returnAreaPeri(self):
+        return self.batch.area_perimeter()
+
+    def computeEnergy(self):
+        self.computeForces()
+        return float(self.batch.energies()[0])
+
+    def enforceTopology(self):
+        self.batch.enforce_topology()
+
+    def globalTriangulation(self):
+        self.batch.triangulate()
+
+    def neighbors(self):
+        return self.batch.topology()
+
+
+Voronoi2D = VoronoiQuadraticEnergy
+
+
+class selfPropelledParticleDynamics:
+    """SPP equations of motion (src/updaters/selfPropelledParticleDynamics.cpp:45-101)."""
+
+    def __init__(self, n=None):
+        self.deltaT = 0.01
+        self.mu = 1.0
+        self.model = None
+        self.noise = None
+
+    def setDeltaT(self, dt):
+        self.deltaT = dt
+
+    def setMu(self, mu):
+        self.mu = mu
+
+    def set2DModel(self, model):
+        self.model = model
+
+    def integrateEquationsOfMotion(self, n_steps=1):
+        self.model.batch.spp_run(n_steps, self.deltaT, self.mu, self.noise)
+        self.model.forcesUpToDate = False
+
+
+class Simulation:
+    """Owns a configuration and its updaters (inc/Simulation.h:18-87; performTimestep,
+    src/Simulation.cpp:141-166). GPU only: setCPUOperation(True) is rejected."""
+
+    def __init__(self):
+        self.configuration = None
+        self.updaters = []
+        self.integrationTimestep = 0.01
+        self.Time = 0.0
+        self.integerTimestep = 0
+
+    def setConfiguration(self, model):
+        self.configuration = model
+
+    def addUpdater(self, updater, model=None):
+        updater.set2DModel(model if model is not None else self.configuration)
+        self.updaters.append(updater)
+
+    def setIntegrationTimestep(self, dt):
+        self.integrationTimestep = dt
+        for u in self.updaters:
+            if hasattr(u, "setDeltaT"):
+                u.setDeltaT(dt)
+
+    def setCPUOperation(self, flag):
+        if flag:
+            raise NotImplementedError("cellgpu_b200 runs on the GPU only")
+
+    def setReproducible(self, flag):
+        if self.configuration is not None:
+            self.configuration.reproducible = bool(flag)
+
+    def performTimestep(self):
+        self.performTimesteps(1)
+
+    def performTimesteps(self, n):
+        """n steps of every updater back to back on the device."""
+        for u in self.updaters:
+            u.integrateEquationsOfMotion(n)
+        self.integerTimestep += n
+        self.Time += n * self.integrationTimestep

@@ -1,0 +1,173 @@
+/*
+ * cellgpu_b200 -- C ABI of the B200 (sm_100a) implementation of cellGPU's per-timestep hot path.
+ *
+ * Two layers, both plain C (extern "C", plain pointers and sizes, int status codes, no exceptions):
+ *
+ *  1. Kernel callers on caller-owned device memory. These replace the reference's L1 "gpu_*" free
+ *     functions (inc/models/*.cuh, inc/updaters/*.cuh, inc/utility/*.cuh), which take raw device
+ *     pointers obtained from ArrayHandle<T>(..., access_location::device, ...). Each takes a
+ *     cudaStream_t (0 = legacy default stream, as the reference used) and never allocates unless
+ *     its comment says so.
+ *  2. An opaque, device-resident system handle (cg_system) that owns one batch of independent
+ *     monolayers (a single monolayer is a batch of one) and runs whole timesteps, FIRE minimizations
+ *     and topology maintenance without per-step host round trips. It replaces the GPU branches of the
+ *     reference's model/updater classes (Simple2DCell, voronoiModelBase, VoronoiQuadraticEnergy,
+ *     vertexModelBase, VertexQuadraticEnergy, selfPropelledParticleDynamics,
+ *     brownianParticleDynamics, EnergyMinimizerFIRE).
+ *
+ * Layouts follow the reference: positions are interleaved (x, y) doubles (Dscalar2 = double2,
+ * inc/std_include.h:47-60); neighbour rows are per-cell contiguous, n_idx(k, c) = c*K + k
+ * (inc/utility/indexer.h:38-41), counter-clockwise. Boxes are rectangular (Lx, Ly), as gpubox's
+ * setSquare(x, y) (inc/utility/gpubox.h:83-93).
+ *
+ * Calls on one cg_system are not thread-safe; distinct systems may be used from distinct threads.
+ */
+#ifndef CELLGPU_B200_H
+#define CELLGPU_B200_H
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------- */
+#define CG_OK 0
+#define CG_ERR_CUDA (-1)          /* a CUDA call failed; cg_last_error_string() has the text */
+#define CG_ERR_ARG (-2)           /* invalid argument */
+#define CG_ERR_CAPACITY (-3)      /* a neighbour/vertex row exceeded its capacity; regrow needed */
+#define CG_ERR_TOPOLOGY (-4)      /* the triangulation could not be made consistent */
+#define CG_ERR_TIMEOUT (-5)       /* a bounded device wait gave up */
+#define CG_ERR_STATE (-6)         /* call not valid in the current state */
+
+/* precision modes */
+#define CG_FP64 0   /* plain FP64: the drop-in for the reference's Dscalar = double path */
+#define CG_MIXED 1  /* FP32 geometry/forces relative to each cell, FP64 positions and predicates */
+
+/* model kinds */
+#define CG_MODEL_VORONOI 0
+#define CG_MODEL_VERTEX 1
+
+const char *cg_last_error_string(void);
+int cg_version(void);
+
+/* =========================================================================================
+ * 1. Kernel callers (caller-owned device memory)
+ * ========================================================================================= */
+
+/* Voronoi geometry: area and perimeter of every cell's Voronoi polygon.
+ * Replaces gpu_compute_voronoi_geometry (inc/models/voronoiModelBase.cuh:35-48,
+ * src/models/voronoiModelBase.cu:115-201); the per-slot voroCur/voroLastNext scratch of the
+ * reference is not materialised. AP[c] = (A, P). */
+int cg_voronoi_geometry(const double *pos, const int *nn, const int *nbr, int K, int N, double Lx,
+                        double Ly, double *AP, cudaStream_t stream);
+
+/* Voronoi quadratic-energy forces, geometry included (one fused pass).
+ * Replaces gpu_compute_voronoi_geometry + gpu_force_sets + gpu_sum_force_sets
+ * (inc/models/voronoiQuadraticEnergy.cuh:20-54). F must be zeroed by the caller (forces are
+ * accumulated); AP receives (A, P). APpref[c] = (A0, P0); KA, KP are the uniform moduli the reference
+ * uses (inc/models/Simple2DCell.h:272-274). */
+int cg_voronoi_forces(const double *pos, const int *nn, const int *nbr, int K, int N, double Lx,
+                      double Ly, const double *APpref, double KA, double KP, double *AP, double *F,
+                      cudaStream_t stream);
+
+/* Exact local-Delaunay test of a stored triangulation: every triangle counter-clockwise and every
+ * edge locally Delaunay. Cells touching a failing edge get flag[c] = 1 (flag is not cleared);
+ * *any_fail is set to 1 if anything failed. Same role as gpu_test_circumcenters
+ * (inc/models/voronoiModelBase.cuh:20-33) with exact predicates. */
+int cg_voronoi_test_triangulation(const double *pos, const int *nn, const int *nbr, int K, int N,
+                                  double Lx, double Ly, int *flag, int *any_fail, cudaStream_t stream);
+
+/* Self-propelled particle step, CPU semantics of the reference
+ * (src/updaters/selfPropelledParticleDynamics.cpp:67-101), fused with the move-and-wrap of
+ * gpu_move_degrees_of_freedom (inc/models/Simple2DCell.cuh:22-40):
+ *   v = v0 (cos th, sin th); pos <- wrap(pos + dt (v + mu F)); th <- atan2(v) + xi sqrt(2 dt Dr).
+ * noise: one normal per cell (device pointer), or NULL to draw from the counter-based RNG with
+ * (seed, step). motility[c] = (v0, Dr). Replaces gpu_spp_eom_integration
+ * (inc/updaters/selfPropelledParticleDynamics.cuh:17-27). */
+int cg_spp_step(double *pos, double *theta, const double *F, const double *motility, const double *noise,
+                int N, double Lx, double Ly, double dt, double mu, uint64_t seed, uint32_t step,
+                cudaStream_t stream);
+
+/* Periodic Delaunay triangulation of N points on the device (exact predicates), written as
+ * counter-clockwise neighbour rows that start at the smallest neighbour index. Replaces the CPU/CGAL
+ * voronoiModelBase::globalTriangulationCGAL (src/models/voronoiModelBase.cpp:281-351).
+ * Allocates and frees its own scratch (cell list, candidate buffers). */
+int cg_voronoi_triangulate(const double *pos, int N, double Lx, double Ly, int K, int *nn, int *nbr,
+                           cudaStream_t stream);
+
+/* =========================================================================================
+ * 2. Device-resident systems (batched; a single instance is the plain drop-in)
+ * ========================================================================================= */
+typedef struct cg_system cg_system;
+
+/* Create a batch of n_inst Voronoi monolayers with N[i] cells in boxes (box[2i], box[2i+1]).
+ * K is the neighbour-row capacity (>= max coordination + 1; 16 is ample for random points).
+ * precision: CG_FP64 or CG_MIXED. */
+int cg_voronoi_create(int n_inst, const int *N, const double *box, int K, int precision,
+                      cg_system **out);
+int cg_destroy(cg_system *sys);
+
+/* sizes and footprint */
+int cg_num_cells(const cg_system *sys);
+int cg_num_dofs(const cg_system *sys);      /* cells (Voronoi) or vertices (vertex model) */
+int cg_num_instances(const cg_system *sys);
+int cg_neighbor_capacity(const cg_system *sys);
+size_t cg_device_bytes(const cg_system *sys);
+/* bytes a system of this shape would hold on the device (admission control) */
+size_t cg_voronoi_footprint(int n_inst, const int *N, int K);
+
+/* host <-> device state (host buffers; copies are ordered on the system's stream and complete
+ * before return for get_*) */
+int cg_set_positions(cg_system *sys, const double *pos);     /* cells (Voronoi) / vertices (vertex) */
+int cg_get_positions(cg_system *sys, double *pos);
+int cg_set_cell_preferences(cg_system *sys, const double *APpref); /* (A0, P0) per cell */
+int cg_set_moduli(cg_system *sys, double KA, double KP);
+int cg_set_motility(cg_system *sys, const double *motility);  /* (v0, Dr) per cell */
+int cg_set_directors(cg_system *sys, const double *theta);
+int cg_get_directors(cg_system *sys, double *theta);
+int cg_get_forces(cg_system *sys, double *F);                 /* per dof */
+int cg_get_area_perimeter(cg_system *sys, double *AP);        /* per cell */
+int cg_get_topology(cg_system *sys, int *nn, int *nbr);       /* Voronoi rows (N x K) */
+int cg_set_topology(cg_system *sys, const int *nn, const int *nbr);
+/* per-instance energies E = sum KA (A-A0)^2 + KP (P-P0)^2 (computeEnergy,
+ * src/models/voronoiQuadraticEnergy.cpp:384-397), accumulated in FP64 */
+int cg_get_energies(cg_system *sys, double *E);
+/* the stream the system enqueues on (its own non-blocking stream unless set; NULL restores it).
+ * CUDA graphs are captured on it, so it must not be the legacy default stream. */
+int cg_set_stream(cg_system *sys, cudaStream_t stream);
+cudaStream_t cg_get_stream(cg_system *sys);
+int cg_synchronize(cg_system *sys);
+
+/* topology and forces */
+int cg_triangulate(cg_system *sys);       /* full Delaunay triangulation (Voronoi) */
+int cg_compute_forces(cg_system *sys);    /* forces on the current topology, geometry included */
+int cg_enforce_topology(cg_system *sys);  /* Voronoi: test+repair; vertex: T1 sweep */
+
+/* dynamics: n_steps integrator steps, each = forces, integrate, move, topology.
+ * noise == NULL: counter-based RNG with the system seed; else a device pointer with n_steps blocks of
+ * per-step normals (SPP: N per step; Brownian: 2*Nv per step). */
+int cg_set_seed(cg_system *sys, uint64_t seed);
+int cg_spp_run(cg_system *sys, int n_steps, double dt, double mu, const double *noise_dev);
+/* Enqueue n_steps RNG-driven SPP steps (one CUDA graph replay) with no host synchronisation.
+ * A step that cannot finish on the device (a global rebuild is needed) sets a sticky halt flag and
+ * the remaining enqueued steps do nothing; cg_poll reports completed steps and recovers. */
+int cg_spp_enqueue(cg_system *sys, int n_steps, double dt, double mu);
+int cg_poll(cg_system *sys, int *steps_done, int *halted, int recover_if_halted);
+/* One step through host buffers: host_noise (N normals) is copied in, the per-instance energies
+ * after the step are copied out to host_energy (may be NULL); returns when they are available. */
+int cg_spp_step_host(cg_system *sys, const double *host_noise, double dt, double mu, double *host_energy);
+/* The fused geometry + force (+ exact Delaunay test) pass alone, enqueued without synchronisation. */
+int cg_launch_force_pass(cg_system *sys, int with_test);
+/* number of this library's kernels enqueued for the system so far (graph replays included) */
+long long cg_kernels_launched(const cg_system *sys);
+
+/* counters: topology repairs, global retriangulations, T1 flips, fallbacks (per system) */
+int cg_counters(cg_system *sys, long long *out, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

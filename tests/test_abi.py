@@ -1,0 +1,41 @@
+"""CPU checks of the C ABI: the library builds, loads, and exports every symbol that
+include/cellgpu_b200.h declares (no compute calls: there is no GPU here)."""
+import os
+import re
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for f in os.listdir(os.path.join(ROOT, "include")):
+        if not f.endswith(".h"):
+            continue
+        txt = open(os.path.join(ROOT, "include", f)).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        for m in re.finditer(r"\b(cg_[a-z0-9_]+)\s*\(", txt):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol(cglib):
+    missing = [n for n in sorted(declared_functions()) if not hasattr(cglib, n)]
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_python_binding_covers_declarations(cglib):
+    from cellgpu_b200 import _lib
+    assert set(_lib.SIGNATURES) <= declared_functions()
+
+
+def test_version(cglib):
+    assert cglib.cg_version() >= 100
+
+
+def test_error_string_roundtrip(cglib):
+    import ctypes as C
+    h = C.c_void_p()
+    # invalid arguments are rejected on the host before any CUDA call
+    rc = cglib.cg_voronoi_create(0, None, None, 16, 0, C.byref(h))
+    assert rc == -2
+    assert b"bad" in cglib.cg_last_error_string()

@@ -1,0 +1,229 @@
+"""GPU parity of the Voronoi (SPV) hot path against the CPU oracle, through the C ABI.
+
+Tolerances (written here, used below):
+  * topology (Delaunay neighbour rows, canonical rotation): bit-exact;
+  * FP64 forces: force_error <= 1e-10 (max |dF| / max(|F|, RMS F); summation order differs);
+  * FP64 areas/perimeters: relative 1e-12;
+  * mixed precision forces vs FP64: force_error <= 1e-6 (the target bound of the mixed form).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from helpers import canonical, force_error, monolayer
+
+pytestmark = pytest.mark.gpu
+
+TOL_F64 = 1e-10
+TOL_AP = 1e-12
+TOL_MIXED = 1e-6
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    return torch
+
+
+def _batch(pos, box, precision=0, K=16):
+    from cellgpu_b200 import VoronoiBatch
+    b = VoronoiBatch([len(pos)], [box], K=K, precision=precision)
+    b.set_positions(pos)
+    return b
+
+
+@pytest.mark.parametrize("N,seed", [(64, 1), (300, 2), (1000, 3), (4096, 4)])
+def test_triangulation_matches_oracle(cglib, oracle, N, seed):
+    pos, box = monolayer(N, seed)
+    b = _batch(pos, box)
+    b.triangulate()
+    nn, nbr = b.topology()
+    onn, onbr = oracle.periodic_delaunay(pos, box, 16)
+    assert np.array_equal(nn, onn)
+    assert np.array_equal(canonical(nn, nbr), canonical(onn, onbr))
+
+
+def test_hexagonal_lattice_known_answer(cglib):
+    from test_oracle import _hex_lattice
+    pts, box = _hex_lattice()
+    b = _batch(pts, box)
+    b.triangulate()
+    b.compute_forces()
+    AP = b.area_perimeter()
+    np.testing.assert_allclose(AP[:, 0], 1.0, rtol=1e-12)
+    np.testing.assert_allclose(AP[:, 1], np.sqrt(8 * np.sqrt(3)), rtol=1e-12)
+    assert np.abs(b.forces()).max() < 1e-11
+
+
+@pytest.mark.parametrize("N,seed", [(300, 5), (2000, 6)])
+def test_forces_match_oracle(cglib, oracle, N, seed):
+    pos, box = monolayer(N, seed)
+    b = _batch(pos, box)
+    b.triangulate()
+    pref = np.tile([1.0, 3.8], (N, 1))
+    b.compute_forces()
+    nn, nbr = b.topology()
+    AP = oracle.voronoi_geometry(pos, box, nn, nbr)
+    F = oracle.voronoi_forces(pos, box, nn, nbr, AP, pref)
+    np.testing.assert_allclose(b.area_perimeter(), AP, rtol=TOL_AP, atol=1e-12)
+    assert force_error(b.forces(), F) < TOL_F64
+    E = b.energies()[0]
+    assert abs(E - oracle.voronoi_energy(AP, pref)) < 1e-12 * max(1.0, E)
+
+
+def test_raw_kernel_callers(cglib, oracle, torch):
+    """The L1 drop-in entry points on caller-owned device memory."""
+    N = 500
+    pos, box = monolayer(N, 8)
+    nn, nbr = oracle.periodic_delaunay(pos, box, 16)
+    dev = torch.device("cuda:0")
+    tpos = torch.tensor(pos, device=dev)
+    tnn = torch.tensor(nn, device=dev)
+    tnbr = torch.tensor(nbr, device=dev)
+    pref = np.tile([1.0, 3.9], (N, 1))
+    tpref = torch.tensor(pref, device=dev)
+    tAP = torch.zeros((N, 2), dtype=torch.float64, device=dev)
+    tF = torch.zeros((N, 2), dtype=torch.float64, device=dev)
+    p = lambda t: C.c_void_p(t.data_ptr())
+    assert cglib.cg_voronoi_forces(p(tpos), p(tnn), p(tnbr), 16, N, box[0], box[1], p(tpref), 1.0, 1.0,
+                                   p(tAP), p(tF), None) == 0
+    torch.cuda.synchronize()
+    AP = oracle.voronoi_geometry(pos, box, nn, nbr)
+    F = oracle.voronoi_forces(pos, box, nn, nbr, AP, pref)
+    assert force_error(tF.cpu().numpy(), F) < TOL_F64
+    tAP2 = torch.zeros_like(tAP)
+    assert cglib.cg_voronoi_geometry(p(tpos), p(tnn), p(tnbr), 16, N, box[0], box[1], p(tAP2), None) == 0
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(tAP2.cpu().numpy(), AP, rtol=TOL_AP)
+    # triangulate on the device into caller memory
+    tnn2 = torch.zeros(N, dtype=torch.int32, device=dev)
+    tnbr2 = torch.zeros((N, 16), dtype=torch.int32, device=dev)
+    assert cglib.cg_voronoi_triangulate(p(tpos), N, box[0], box[1], 16, p(tnn2), p(tnbr2), None) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(canonical(tnn2.cpu().numpy(), tnbr2.cpu().numpy()), canonical(nn, nbr))
+    # exact test: the Delaunay triangulation passes; a perturbed point makes it fail
+    flag = torch.zeros(N, dtype=torch.int32, device=dev)
+    anyf = torch.zeros(1, dtype=torch.int32, device=dev)
+    assert cglib.cg_voronoi_test_triangulation(p(tpos), p(tnn), p(tnbr), 16, N, box[0], box[1], p(flag),
+                                               p(anyf), None) == 0
+    torch.cuda.synchronize()
+    assert int(anyf.item()) == 0
+    pos2 = pos.copy()
+    j = int(nbr[0, 0])
+    pos2[0] = pos[j] + 0.02 * (pos[0] - pos[j])  # move cell 0 right next to a neighbour
+    tpos2 = torch.tensor(pos2, device=dev)
+    assert cglib.cg_voronoi_test_triangulation(p(tpos2), p(tnn), p(tnbr), 16, N, box[0], box[1], p(flag),
+                                               p(anyf), None) == 0
+    torch.cuda.synchronize()
+    assert oracle.topology_mismatch(pos2, box, nn, nbr) > 0
+    assert int(anyf.item()) == 1 and int(flag.sum().item()) > 0
+
+
+@pytest.mark.parametrize("N,steps,seed", [(300, 30, 10), (1500, 15, 11)])
+def test_spp_steps_match_oracle(cglib, oracle, torch, N, steps, seed):
+    """SPP dynamics with identical supplied noise: positions, directors, topology and the forces
+    of the last step agree with the oracle's CPU path."""
+    pos, box = monolayer(N, seed)
+    rng = np.random.default_rng(seed + 100)
+    theta = rng.uniform(0, 2 * np.pi, N)
+    mot = np.tile([0.05, 1.0], (N, 1))
+    pref = np.tile([1.0, 3.8], (N, 1))
+    noise = rng.normal(size=(steps, N))
+    b = _batch(pos, box)
+    b.set_directors(theta)
+    b.set_motility(mot)
+    b.set_preferences(pref)
+    b.triangulate()
+    tnoise = torch.tensor(noise, device="cuda:0")
+    b.spp_run(steps, dt=0.01, mu=1.0, noise=tnoise)
+    b.enforce_topology()
+    onn, onbr = oracle.periodic_delaunay(pos, box, 16)
+    opos, oth = pos.copy(), theta.copy()
+    F, AP = oracle.voronoi_spp_run(opos, box, onn, onbr, oth, mot, pref, noise)
+    gpos = b.positions()
+    assert np.abs(gpos - opos).max() < 1e-9
+    assert np.abs(np.angle(np.exp(1j * (b.directors() - oth)))).max() < 1e-9
+    nn, nbr = b.topology()
+    assert np.array_equal(canonical(nn, nbr), canonical(onn, onbr))
+    assert force_error(b.forces(), F) < 1e-8
+    assert b.counters()["global_rebuilds"] >= 1
+
+
+def test_fast_cells_force_repairs(cglib, oracle, torch):
+    """Large per-step displacements: many repairs per step, still bit-exact topology."""
+    N = 800
+    pos, box = monolayer(N, 21)
+    rng = np.random.default_rng(22)
+    theta = rng.uniform(0, 2 * np.pi, N)
+    mot = np.tile([1.0, 1.0], (N, 1))
+    pref = np.tile([1.0, 3.8], (N, 1))
+    steps = 10
+    noise = rng.normal(size=(steps, N))
+    b = _batch(pos, box)
+    b.set_directors(theta)
+    b.set_motility(mot)
+    b.triangulate()
+    b.spp_run(steps, dt=0.05, mu=1.0, noise=torch.tensor(noise, device="cuda:0"))
+    b.enforce_topology()
+    onn, onbr = oracle.periodic_delaunay(pos, box, 16)
+    opos, oth = pos.copy(), theta.copy()
+    oracle.voronoi_spp_run(opos, box, onn, onbr, oth, mot, pref, noise, dt=0.05)
+    assert np.abs(b.positions() - opos).max() < 1e-8
+    nn, nbr = b.topology()
+    assert np.array_equal(canonical(nn, nbr), canonical(onn, onbr))
+    c = b.counters()
+    assert c["rows_changed"] > 0
+
+
+def test_mixed_precision_force_error(cglib, oracle):
+    N = 4096
+    pos, box = monolayer(N, 31)
+    b64 = _batch(pos, box, precision=0)
+    b32 = _batch(pos, box, precision=1)
+    b64.triangulate()
+    b32.triangulate()
+    b64.compute_forces()
+    b32.compute_forces()
+    err = force_error(b32.forces(), b64.forces())
+    print("mixed max normalised force error", err)
+    assert err < TOL_MIXED
+
+
+def test_batch_equals_singles(cglib):
+    """Instances of a batch evolve exactly as they do alone (RNG counter = global cell index, so
+    single runs use the same offsets)."""
+    from cellgpu_b200 import VoronoiBatch
+    Ns = [100, 257, 1000]
+    boxes = [(np.sqrt(n), np.sqrt(n)) for n in Ns]
+    poss = [monolayer(n, 40 + i)[0] for i, n in enumerate(Ns)]
+    b = VoronoiBatch(Ns, boxes)
+    b.set_positions(np.concatenate(poss))
+    b.triangulate()
+    b.compute_forces()
+    Fb = b.forces()
+    off = 0
+    for i, n in enumerate(Ns):
+        s = _batch(poss[i], boxes[i])
+        s.triangulate()
+        s.compute_forces()
+        assert force_error(Fb[off:off + n], s.forces()) < 1e-12
+        off += n
+
+
+@pytest.mark.parametrize("N", [262144])
+def test_large_monolayer_invariants(cglib, N):
+    pos, box = monolayer(N, 50)
+    b = _batch(pos, box)
+    b.triangulate()
+    nn, _ = b.topology()
+    assert nn.sum() == 6 * N
+    b.spp_run(20, dt=0.01)
+    b.enforce_topology()
+    nn, _ = b.topology()
+    assert nn.sum() == 6 * N
+    b.compute_forces()
+    F = b.forces()
+    AP = b.area_perimeter()
+    assert abs(AP[:, 0].sum() - box[0] * box[1]) < 1e-6
+    assert np.abs(F.sum(axis=0)).max() < 1e-8 * N
