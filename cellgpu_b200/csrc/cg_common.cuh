@@ -29,11 +29,15 @@ struct Inst {
 };
 
 // gpubox::minDist for a rectangular box (inc/utility/gpubox.h:154-165). The while loops and
-// half-box thresholds are kept so the FP64 result is bit-identical to the reference's.
+// half-box thresholds are kept so the FP64 result is bit-identical to the reference's. Inputs far
+// outside the box (or non-finite) are first reduced in one step, so no loop can run away on the
+// device: for points inside the box the pre-reduction never triggers.
 CG_HD double2 min_dist(double2 p1, double2 p2, double Lx, double Ly)
 {
     double hx = Lx * 0.5, hy = Ly * 0.5;
     double x = p1.x - p2.x, y = p1.y - p2.y;
+    if (!(fabs(x) <= 2.0 * Lx)) x -= Lx * rint(x / Lx);
+    if (!(fabs(y) <= 2.0 * Ly)) y -= Ly * rint(y / Ly);
     while (x < -hx) x += Lx;
     while (y < -hy) y += Ly;
     while (x > hx) x -= Lx;
@@ -46,6 +50,10 @@ CG_HD double2 min_dist(double2 p1, double2 p2, double Lx, double Ly)
 CG_D double2 put_in_box(double2 p, double Lx, double Ly, double iLx, double iLy)
 {
     double vx = __dmul_rn(iLx, p.x), vy = __dmul_rn(iLy, p.y);
+    // one-step reduction for displacements of more than a box (or non-finite values), bounding
+    // the loops below; a step that moves a point by less than one box never takes this branch
+    if (!(vx >= -1.0 && vx < 2.0)) vx -= floor(vx);
+    if (!(vy >= -1.0 && vy < 2.0)) vy -= floor(vy);
     while (vx < 0) vx = __dadd_rn(vx, 1.0);
     while (vy < 0) vy = __dadd_rn(vy, 1.0);
     while (vx >= 1.0) vx = __dsub_rn(vx, 1.0);

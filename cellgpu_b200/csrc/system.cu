@@ -303,7 +303,7 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
         if ((st = dalloc(s, &s->stage_nbr, (size_t)Nt * K))) break;
         if ((st = dalloc(s, &s->changed, (size_t)Nt * R_MAX))) break;
         if ((st = dalloc(s, &s->ctl, 1))) break;
-        if ((st = dalloc(s, &s->bin_count, s->n_bins))) break;
+        if ((st = dalloc(s, &s->bin_count, s->n_bins + 1))) break;
         if ((st = dalloc(s, &s->bin_start, s->n_bins + 1))) break;
         if ((st = dalloc(s, &s->bin_cells, Nt))) break;
         if ((st = dalloc(s, &s->cell_bin, Nt))) break;

@@ -241,7 +241,16 @@ __global__ void __launch_bounds__(128) k_voro_cells(VoroArgs a)
     R A, P;
     int fail = cell_pass<R, SCATTER, TEST>(a, c, row, z, pc, in.Lx, in.Ly, R(1), A, P);
     if (a.AP) store_ap<R>(a.AP, c, A, P);
-    if (TEST && fail) {
+    if (TEST && fail && z < 3) {
+        // degenerate row: only the cell itself can be queued
+        if (a.ctl) {
+            atomicAdd(&a.ctl->n_flagged, 1);
+            claim_enqueue(a, c, a.ctl->epoch, 0);
+        } else if (a.mark) {
+            a.mark[c] = 1;
+            a.queue[0] = 1;
+        }
+    } else if (TEST && fail) {
         if (a.ctl) {
             int e = a.ctl->epoch;
             atomicAdd(&a.ctl->n_flagged, 1);

@@ -25,6 +25,8 @@ void cgo_min_dist(const double *box, const double *p1, const double *p2, double 
     double hx = Lx * 0.5, hy = Ly * 0.5;
     double x = p1[0] - p2[0];
     double y = p1[1] - p2[1];
+    if (!(fabs(x) <= 2.0 * Lx)) x -= Lx * rint(x / Lx); /* bound the loops (never taken in-box) */
+    if (!(fabs(y) <= 2.0 * Ly)) y -= Ly * rint(y / Ly);
     while (x < -hx) x += Lx;
     while (y < -hy) y += Ly;
     while (x > hx) x -= Lx;
@@ -40,6 +42,8 @@ void cgo_put_in_box(const double *box, double *p)
     double ix = 1.0 / box[0], iy = 1.0 / box[1];
     double vx = ix * p[0];
     double vy = iy * p[1];
+    if (!(vx >= -1.0 && vx < 2.0)) vx -= floor(vx); /* bound the loops (never taken for small moves) */
+    if (!(vy >= -1.0 && vy < 2.0)) vy -= floor(vy);
     while (vx < 0) vx += 1.0;
     while (vy < 0) vy += 1.0;
     while (vx >= 1.0) vx -= 1.0;

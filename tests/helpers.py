@@ -26,3 +26,19 @@ def canonical(nn, nbr):
         s = int(np.argmin(r))
         out[i, :z] = np.roll(r, -s)
     return out
+
+
+def jittered_lattice(nx, ny, jitter, seed):
+    """Triangular lattice of unit-area cells in a rectangular periodic box, each point displaced by
+    a uniform jitter (a well-conditioned state: no near-coincident points)."""
+    rng = np.random.default_rng(seed)
+    s = np.sqrt(2 / np.sqrt(3))
+    pts = []
+    for j in range(ny):
+        for i in range(nx):
+            pts.append(((i + 0.5 * (j % 2)) * s, j * s * np.sqrt(3) / 2))
+    pts = np.array(pts) + rng.uniform(-jitter, jitter, (nx * ny, 2))
+    box = (nx * s, ny * s * np.sqrt(3) / 2)
+    pts[:, 0] %= box[0]
+    pts[:, 1] %= box[1]
+    return pts, box

@@ -11,7 +11,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from helpers import canonical, force_error, monolayer
+from helpers import canonical, force_error, jittered_lattice, monolayer
 
 pytestmark = pytest.mark.gpu
 
@@ -120,60 +120,64 @@ def test_raw_kernel_callers(cglib, oracle, torch):
     assert int(anyf.item()) == 1 and int(flag.sum().item()) > 0
 
 
-@pytest.mark.parametrize("N,steps,seed", [(300, 30, 10), (1500, 15, 11)])
-def test_spp_steps_match_oracle(cglib, oracle, torch, N, steps, seed):
-    """SPP dynamics with identical supplied noise: positions, directors, topology and the forces
-    of the last step agree with the oracle's CPU path."""
-    pos, box = monolayer(N, seed)
+def _spp_setup(pos, box, seed, v0=0.05):
+    N = len(pos)
     rng = np.random.default_rng(seed + 100)
     theta = rng.uniform(0, 2 * np.pi, N)
-    mot = np.tile([0.05, 1.0], (N, 1))
+    mot = np.tile([v0, 1.0], (N, 1))
     pref = np.tile([1.0, 3.8], (N, 1))
-    noise = rng.normal(size=(steps, N))
     b = _batch(pos, box)
     b.set_directors(theta)
     b.set_motility(mot)
     b.set_preferences(pref)
     b.triangulate()
-    tnoise = torch.tensor(noise, device="cuda:0")
-    b.spp_run(steps, dt=0.01, mu=1.0, noise=tnoise)
+    return b, theta, mot, pref, rng
+
+
+@pytest.mark.parametrize("N,steps,seed", [(300, 20, 10), (1500, 15, 11)])
+def test_spp_each_step_matches_oracle(cglib, oracle, torch, N, steps, seed):
+    """Per-step parity from a common state: each GPU step (forces on the repaired topology,
+    integrate, move) against the oracle's CPU step with the same supplied noise; the state is then
+    re-synchronised to the oracle's so that chaotic amplification of 1e-16 differences in random
+    initial states (near-coincident points) cannot mask a real error."""
+    pos, box = monolayer(N, seed)
+    b, theta, mot, pref, rng = _spp_setup(pos, box, seed)
+    noise = rng.normal(size=(steps, N))
+    onn, onbr = oracle.periodic_delaunay(pos, box, 16)
+    opos, oth = pos.copy(), theta.copy()
+    for s in range(steps):
+        b.spp_run(1, dt=0.01, mu=1.0, noise=torch.tensor(noise[s:s + 1], device="cuda:0"))
+        F, _ = oracle.voronoi_spp_run(opos, box, onn, onbr, oth, mot, pref, noise[s:s + 1])
+        assert np.abs(b.positions() - opos).max() < 1e-12
+        assert force_error(b.forces(), F) < TOL_F64
+        b.enforce_topology()
+        nn, nbr = b.topology()
+        assert np.array_equal(canonical(nn, nbr), canonical(onn, onbr))
+        b.set_positions(opos)
+        b.set_directors(oth)
+        b.set_topology(onn, onbr)
+
+
+@pytest.mark.parametrize("nx,ny,steps,v0,dt", [(20, 24, 40, 0.05, 0.01), (32, 36, 25, 1.0, 0.05)])
+def test_spp_free_run_matches_oracle(cglib, oracle, torch, nx, ny, steps, v0, dt):
+    """Free-running trajectories (no re-synchronisation) from a well-conditioned jittered lattice;
+    the fast case (v0 = 1, dt = 0.05) exercises many repairs per step."""
+    pos, box = jittered_lattice(nx, ny, 0.25, 7)
+    N = len(pos)
+    b, theta, mot, pref, rng = _spp_setup(pos, box, 12, v0=v0)
+    noise = rng.normal(size=(steps, N))
+    b.spp_run(steps, dt=dt, mu=1.0, noise=torch.tensor(noise, device="cuda:0"))
     b.enforce_topology()
     onn, onbr = oracle.periodic_delaunay(pos, box, 16)
     opos, oth = pos.copy(), theta.copy()
-    F, AP = oracle.voronoi_spp_run(opos, box, onn, onbr, oth, mot, pref, noise)
-    gpos = b.positions()
-    assert np.abs(gpos - opos).max() < 1e-9
+    F, _ = oracle.voronoi_spp_run(opos, box, onn, onbr, oth, mot, pref, noise, dt=dt)
+    assert np.abs(b.positions() - opos).max() < 1e-9
     assert np.abs(np.angle(np.exp(1j * (b.directors() - oth)))).max() < 1e-9
     nn, nbr = b.topology()
     assert np.array_equal(canonical(nn, nbr), canonical(onn, onbr))
     assert force_error(b.forces(), F) < 1e-8
-    assert b.counters()["global_rebuilds"] >= 1
-
-
-def test_fast_cells_force_repairs(cglib, oracle, torch):
-    """Large per-step displacements: many repairs per step, still bit-exact topology."""
-    N = 800
-    pos, box = monolayer(N, 21)
-    rng = np.random.default_rng(22)
-    theta = rng.uniform(0, 2 * np.pi, N)
-    mot = np.tile([1.0, 1.0], (N, 1))
-    pref = np.tile([1.0, 3.8], (N, 1))
-    steps = 10
-    noise = rng.normal(size=(steps, N))
-    b = _batch(pos, box)
-    b.set_directors(theta)
-    b.set_motility(mot)
-    b.triangulate()
-    b.spp_run(steps, dt=0.05, mu=1.0, noise=torch.tensor(noise, device="cuda:0"))
-    b.enforce_topology()
-    onn, onbr = oracle.periodic_delaunay(pos, box, 16)
-    opos, oth = pos.copy(), theta.copy()
-    oracle.voronoi_spp_run(opos, box, onn, onbr, oth, mot, pref, noise, dt=0.05)
-    assert np.abs(b.positions() - opos).max() < 1e-8
-    nn, nbr = b.topology()
-    assert np.array_equal(canonical(nn, nbr), canonical(onn, onbr))
-    c = b.counters()
-    assert c["rows_changed"] > 0
+    if v0 >= 1.0:
+        assert b.counters()["rows_changed"] > 0
 
 
 def test_mixed_precision_force_error(cglib, oracle):
