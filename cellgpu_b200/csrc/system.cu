@@ -92,7 +92,10 @@ extern "C" int cg_voronoi_geometry(const double *pos, const int *nn, const int *
     if (N <= 0 || K < 3 || K > KMAX || !pos || !nn || !nbr || !AP) return set_err(CG_ERR_ARG, "bad args");
     VoroArgs a = raw_args(pos, nn, nbr, K, N, Lx, Ly);
     a.AP = AP;
-    k_voro_cells<double, false, false><<<nblk(N, 128), 128, 0, stream>>>(a);
+    if (K <= VG)
+        k_voro_groups<double, false, false, 4><<<nblk(N, 4 * GPW), 128, 0, stream>>>(a);
+    else
+        k_voro_cells<double, false, false><<<nblk(N, 128), 128, 0, stream>>>(a);
     return check_launch();
 }
 
@@ -108,7 +111,10 @@ extern "C" int cg_voronoi_forces(const double *pos, const int *nn, const int *nb
     a.KP = KP;
     a.AP = AP;
     a.F = F;
-    k_voro_cells<double, true, false><<<nblk(N, 128), 128, 0, stream>>>(a);
+    if (K <= VG)
+        k_voro_groups<double, true, false, 4><<<nblk(N, 4 * GPW), 128, 0, stream>>>(a);
+    else
+        k_voro_cells<double, true, false><<<nblk(N, 128), 128, 0, stream>>>(a);
     return check_launch();
 }
 
@@ -121,7 +127,10 @@ extern "C" int cg_voronoi_test_triangulation(const double *pos, const int *nn, c
     VoroArgs a = raw_args(pos, nn, nbr, K, N, Lx, Ly);
     a.mark = flag;
     a.queue = any_fail;
-    k_voro_cells<double, false, true><<<nblk(N, 128), 128, 0, stream>>>(a);
+    if (K <= VG)
+        k_voro_groups<double, false, true, 4><<<nblk(N, 4 * GPW), 128, 0, stream>>>(a);
+    else
+        k_voro_cells<double, false, true><<<nblk(N, 128), 128, 0, stream>>>(a);
     return check_launch();
 }
 
@@ -177,6 +186,7 @@ struct cg_system {
     bool topology_valid = false;
     long long host_counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     cudaStream_t own_stream = nullptr;
+    cudaStream_t body_stream = nullptr;  // captures the bodies of conditional graph nodes
     struct GraphEntry {
         int n;
         double dt, mu;
@@ -261,7 +271,7 @@ extern "C" size_t cg_voronoi_footprint(int n_inst, const int *N, int K)
 extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, int K, int precision,
                                  cg_system **out)
 {
-    if (n_inst <= 0 || !N || !box || !out || K < 4 || K > KMAX ||
+    if (n_inst <= 0 || !N || !box || !out || K < 4 || K > VG ||
         (precision != CG_FP64 && precision != CG_MIXED))
         return set_err(CG_ERR_ARG, "bad args");
     cg_system *s = new cg_system();
@@ -337,6 +347,7 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
         return set_err(CG_ERR_CUDA, "stream creation failed");
     }
     s->stream = s->own_stream;
+    cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking);
     Ctl c0;
     memset(&c0, 0, sizeof(c0));
     c0.epoch = 1;
@@ -358,6 +369,7 @@ extern "C" int cg_destroy(cg_system *s)
     for (auto &g : s->graphs) cudaGraphExecDestroy(g.exec);
     for (void *p : s->allocs) cudaFree(p);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    if (s->body_stream) cudaStreamDestroy(s->body_stream);
     delete s;
     return CG_OK;
 }
@@ -570,28 +582,33 @@ static void launch_force_test(cg_system *s, const VoroArgs &a, bool test)
     cudaMemsetAsync(s->F, 0, (s->precision == CG_FP64 ? sizeof(double2) : sizeof(float2)) * s->N,
                     s->stream);
     if (test)
-        k_voro_cells<R, true, true><<<nblk(s->N, 128), 128, 0, s->stream>>>(a);
+        k_voro_groups<R, true, true, 4><<<nblk(s->N, 4 * GPW), 128, 0, s->stream>>>(a);
     else
-        k_voro_cells<R, true, false><<<nblk(s->N, 128), 128, 0, s->stream>>>(a);
+        k_voro_groups<R, true, false, 4><<<nblk(s->N, 4 * GPW), 128, 0, s->stream>>>(a);
     s->kernels_enqueued += 1;
 }
 
 template <typename R>
-static void launch_repair(cg_system *s, const VoroArgs &a, bool forces)
+static void launch_round(cg_system *s, const VoroArgs &a, bool forces, cudaStream_t st, unsigned long long cond,
+                         int use_cond)
 {
     constexpr int WPB = 4;
-    int grid_w = 148 * 4;
-    k_expand<<<1, 512, 0, s->stream>>>(a);
-    for (int r = 0; r < R_MAX; ++r) {
-        k_star_local<WPB><<<grid_w, WPB * 32, 0, s->stream>>>(a, r);
-        if (forces)
-            k_commit<R, true><<<148 * 2, 128, 0, s->stream>>>(a, r);
-        else
-            k_commit<R, false><<<148 * 2, 128, 0, s->stream>>>(a, r);
-        k_check<<<148 * 2, 128, 0, s->stream>>>(a, r);
-    }
-    k_finish_repair<<<1, 1, 0, s->stream>>>(a);
-    s->kernels_enqueued += 2 + 3 * R_MAX;
+    k_star_local<WPB><<<148 * 4, WPB * 32, 0, st>>>(a);
+    if (forces)
+        k_commit<R, true><<<148 * 2, 128, 0, st>>>(a);
+    else
+        k_commit<R, false><<<148 * 2, 128, 0, st>>>(a);
+    k_check<<<148 * 2, 128, 0, st>>>(a);
+    k_round_end<<<1, 1, 0, st>>>(a, cond, use_cond);
+}
+
+// repair rounds as plain launches (used outside graphs): every round is launched; empty rounds exit
+template <typename R>
+static void launch_repair(cg_system *s, const VoroArgs &a, bool forces)
+{
+    k_repair_begin<<<1, 1, 0, s->stream>>>(a, 0ull, 0);
+    for (int r = 0; r < R_MAX; ++r) launch_round<R>(s, a, forces, s->stream, 0ull, 0);
+    s->kernels_enqueued += 1;
 }
 
 static int read_ctl(cg_system *s, Ctl &c) { return d2h(s, &c, s->ctl, sizeof(Ctl)); }
@@ -644,7 +661,7 @@ static int enforce_t(cg_system *s)
 {
     VoroArgs a = sys_args(s);
     for (int attempt = 0; attempt < 3; ++attempt) {
-        k_voro_cells<R, false, true><<<nblk(s->N, 128), 128, 0, s->stream>>>(a);
+        k_voro_groups<R, false, true, 4><<<nblk(s->N, 4 * GPW), 128, 0, s->stream>>>(a);
         launch_repair<R>(s, a, false);
         k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 0);
         CG_TRY(check_launch());
@@ -677,8 +694,73 @@ static void enqueue_spp_steps(cg_system *s, int n, double dt, double mu, const d
     }
 }
 
-// Replay (capturing on first use) a CUDA graph of n steps. The kernels take their queue lengths,
-// epochs and step counter from the device control block, so one graph serves every call.
+// Build a CUDA graph of n steps. Per step: zero F, fused force + exact test pass, then the local
+// repair rounds inside a WHILE conditional node (the device decides whether another round runs),
+// then integrate + move and the step epilogue. Kernels take queue lengths, epochs, rounds and the
+// step counter from the device control block, so one graph serves every call.
+template <typename R>
+static int build_graph(cg_system *s, int n, double dt, double mu, const double *noise, cudaGraphExec_t *exec,
+                       long long *static_kernels)
+{
+    VoroArgs a = sys_args(s);
+    cudaGraph_t graph;
+    CG_CUDA(cudaGraphCreate(&graph, 0));
+    const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+    std::vector<cudaGraphNode_t> deps;
+    long long k0 = s->kernels_enqueued;
+    auto capture_deps = [&](cudaStream_t st) -> int {
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t *d = nullptr;
+        size_t nd = 0;
+        CG_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &d, &nd));
+        deps.assign(d, d + nd);
+        return CG_OK;
+    };
+    int st = CG_OK;
+    for (int t = 0; t < n && st == CG_OK; ++t) {
+        cudaGraphConditionalHandle h;
+        CG_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
+        CG_CUDA(cudaStreamBeginCaptureToGraph(s->stream, graph, deps.empty() ? nullptr : deps.data(), nullptr,
+                                              deps.size(), mode));
+        launch_force_test<R>(s, a, true);
+        k_repair_begin<<<1, 1, 0, s->stream>>>(a, (unsigned long long)h, 1);
+        s->kernels_enqueued += 1;
+        st = capture_deps(s->stream);
+        cudaGraph_t g2;
+        CG_CUDA(cudaStreamEndCapture(s->stream, &g2));
+        if (st) break;
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cn;
+        CG_CUDA(cudaGraphAddNode(&cn, graph, deps.data(), deps.size(), &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CG_CUDA(cudaStreamBeginCaptureToGraph(s->body_stream, body, nullptr, nullptr, 0, mode));
+        launch_round<R>(s, a, true, s->body_stream, (unsigned long long)h, 1);  // counted on the device
+        cudaGraph_t gb;
+        CG_CUDA(cudaStreamEndCapture(s->body_stream, &gb));
+        deps.assign(1, cn);
+        CG_CUDA(cudaStreamBeginCaptureToGraph(s->stream, graph, deps.data(), nullptr, deps.size(), mode));
+        const double *nz = noise;
+        k_spp<R><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, nz, dt, mu, s->seed, 0);
+        k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
+        s->kernels_enqueued += 2;
+        st = capture_deps(s->stream);
+        CG_CUDA(cudaStreamEndCapture(s->stream, &g2));
+    }
+    if (st == CG_OK) {
+        cudaError_t e = cudaGraphInstantiate(exec, graph, 0);
+        if (e != cudaSuccess) st = set_err(CG_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaGraphDestroy(graph);
+    *static_kernels = s->kernels_enqueued - k0;
+    s->kernels_enqueued = k0;
+    return st;
+}
+
+// Replay (building on first use) the n-step graph
 template <typename R>
 static int enqueue_graph(cg_system *s, int n, double dt, double mu, const double *noise)
 {
@@ -688,16 +770,9 @@ static int enqueue_graph(cg_system *s, int n, double dt, double mu, const double
             s->kernels_enqueued += g.kernels;
             return CG_OK;
         }
-    cudaGraph_t graph;
-    long long k0 = s->kernels_enqueued;
-    CG_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_spp_steps<R>(s, n, dt, mu, noise, false);
-    CG_CUDA(cudaStreamEndCapture(s->stream, &graph));
     cudaGraphExec_t exec;
-    CG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-    cudaGraphDestroy(graph);
-    long long nk = s->kernels_enqueued - k0;
-    s->kernels_enqueued = k0;
+    long long nk = 0;
+    CG_TRY(build_graph<R>(s, n, dt, mu, noise, &exec, &nk));
     s->graphs.push_back({n, dt, mu, noise, exec, nk});
     CG_CUDA(cudaGraphLaunch(exec, s->stream));
     s->kernels_enqueued += nk;
@@ -801,7 +876,15 @@ extern "C" int cg_launch_force_pass(cg_system *s, int with_test)
     return check_launch();
 }
 
-extern "C" long long cg_kernels_launched(const cg_system *s) { return s ? s->kernels_enqueued : 0; }
+// kernels launched for this system: host-enqueued ones plus the 4 kernels of every repair round
+// executed inside graph WHILE nodes (counted on the device); synchronises the stream
+extern "C" long long cg_kernels_launched(cg_system *s)
+{
+    if (!s) return 0;
+    Ctl c;
+    if (read_ctl(s, c) != CG_OK) return -1;
+    return s->kernels_enqueued + 4 * (long long)c.counters[7];
+}
 
 extern "C" int cg_spp_run(cg_system *s, int n_steps, double dt, double mu, const double *noise_dev)
 {

@@ -181,13 +181,22 @@ CG_D int cell_pass(const VoroArgs &a, int c, const int *row, int z, double2 pc, 
         for (int k = 0; k < z; ++k) {
             // g = -dE/dh_k
             R dAx = R(0.5) * (hN.y - hP.y), dAy = R(0.5) * (hP.x - hN.x);
-            R lx = hC.x - hP.x, ly = hC.y - hP.y;
-            R ln = sqrt(lx * lx + ly * ly);
-            if (ln < thr) ln = thr;
-            R nx = hC.x - hN.x, ny = hC.y - hN.y;
-            R nnm = sqrt(nx * nx + ny * ny);
-            if (nnm < thr) nnm = thr;
-            R dPx = lx / ln + nx / nnm, dPy = ly / ln + ny / nnm;
+            R dPx, dPy;
+            if (sizeof(R) == sizeof(double)) {
+                R lx = hC.x - hP.x, ly = hC.y - hP.y;
+                R ln = sqrt(lx * lx + ly * ly);
+                if (ln < thr) ln = thr;
+                R nx = hC.x - hN.x, ny = hC.y - hN.y;
+                R nnm = sqrt(nx * nx + ny * ny);
+                if (nnm < thr) nnm = thr;
+                dPx = lx / ln + nx / nnm;
+                dPy = ly / ln + ny / nnm;
+            } else {
+                // exact tangent directions of the edges dual to r_{k-1} and r_k (see k_voro_groups)
+                R ia = R(1) / sqrt(rA.x * rA.x + rA.y * rA.y), ib = R(1) / sqrt(rB.x * rB.x + rB.y * rB.y);
+                dPx = -rA.y * ia + rB.y * ib;
+                dPy = rA.x * ia - rB.x * ib;
+            }
             R gx = -R(2) * (Adiff * dAx + Pdiff * dPx);
             R gy = -R(2) * (Adiff * dAy + Pdiff * dPy);
             // Jacobians of h_k
@@ -272,22 +281,250 @@ __global__ void __launch_bounds__(128) k_voro_cells(VoroArgs a)
     }
 }
 
-// flagged cells -> flagged cells and their neighbours (NeedsFixing,
-// src/models/voronoiModelBase.cpp:632-646); escalate when too many
-// (launched as ONE block: the seed count is read before any thread appends)
-__global__ void k_expand(VoroArgs a)
+// ------------------------------------------------------------------------------------------
+// Lane-per-Voronoi-vertex form of the same pass (the step's workhorse). A group of G = 8 lanes owns
+// one cell; lane l handles vertices l and l+8 (rows up to 16). Ring neighbours (k-1, k+1) are
+// exchanged through shared memory, A and P are reduced with group shuffles, and each vertex's
+// three force contributions are formed once (no recomputation, no local arrays). One reciprocal of
+// the cross product r_{k-1} x r_k serves the circumcentre and both Jacobians.
+// In FP64 the perimeter derivative uses the unit vectors of h_{k+1}-h_k as the reference does
+// (src/models/voronoiQuadraticEnergy.cpp:247-256). In mixed precision it uses their exact
+// direction: both ends of the Voronoi edge dual to (c, n_k) lie on the perpendicular bisector of
+// r_k, so the counter-clockwise unit tangent is (-r_k.y, r_k.x)/|r_k|; this removes the
+// cancellation of nearly equal FP32 circumcentres on short edges.
+// ------------------------------------------------------------------------------------------
+constexpr int G = 8;
+constexpr int GPW = 32 / G;  // cells per warp
+constexpr int VG = 16;       // vertices per cell in the group kernel (K <= 16)
+
+template <typename R>
+CG_D R group_sum(R v)
+{
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    return v;
+}
+
+CG_D int group_min(int v)
+{
+    v = min(v, __shfl_xor_sync(0xffffffffu, v, 1));
+    v = min(v, __shfl_xor_sync(0xffffffffu, v, 2));
+    v = min(v, __shfl_xor_sync(0xffffffffu, v, 4));
+    return v;
+}
+
+template <typename R, bool SCATTER, bool TEST, int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_voro_groups(VoroArgs a)
+{
+    using V = typename Vec2<R>::T;
+    __shared__ double2 sR[WPB * GPW][VG];
+    __shared__ V sH[WPB * GPW][VG];
+    __shared__ V sU[WPB * GPW][VG];
+    __shared__ V sCA[WPB * GPW][VG];
+    __shared__ V sCB[WPB * GPW][VG];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int gl = lane & (G - 1), gi = lane >> 3;
+    const int sl = w * GPW + gi;
+    const int c = (blockIdx.x * WPB + w) * GPW + gi;
+    bool live = c < a.N;
+    if (a.ctl && a.ctl->halt) live = false;  // uniform across the grid
+    int z = 0;
+    double2 pc = make_double2(0, 0);
+    double Lx = 1, Ly = 1;
+    const int *row = nullptr;
+    if (live) {
+        const Inst &in = inst_of(a, c);
+        Lx = in.Lx;
+        Ly = in.Ly;
+        pc = a.pos[c];
+        z = a.nn[c];
+        row = a.nbr + (size_t)c * a.K;
+    }
+    const bool ok = live && z >= 3 && z <= VG;
+    // phase A: relative positions (FP64, exact Delaunay inputs)
+    int nbk[2] = {-1, -1};
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        int k = gl + G * r;
+        if (ok && k < z) {
+            nbk[r] = row[k];
+            sR[sl][k] = min_dist(a.pos[nbk[r]], pc, Lx, Ly);
+        }
+    }
+    __syncwarp();
+    // phase B: Voronoi vertices h_k = circumcentre(0, r_{k-1}, r_k); exact local Delaunay test
+    int fail = 0x7fffffff;  // smallest failing slot (x2, +1 for orientation)
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        int k = gl + G * r;
+        if (ok && k < z) {
+            int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
+            double2 ra = sR[sl][km], rb = sR[sl][k];
+            sH[sl][k] = circum0<R>(cvt<R>(ra), cvt<R>(rb));
+            if (TEST) {
+                double2 rc = sR[sl][kp];
+                if (orient0(rb, rc) <= 0) fail = min(fail, 2 * k + 1);
+                else if (c < nbk[r] && incircle0(ra, rb, rc) < 0) fail = min(fail, 2 * k);
+            }
+        }
+    }
+    __syncwarp();
+    // phase C: edges h_k -> h_{k+1}: area, perimeter, unit tangents
+    R Ap = 0, Pp = 0;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        int k = gl + G * r;
+        if (ok && k < z) {
+            int kp = k + 1 == z ? 0 : k + 1;
+            V h0 = sH[sl][k], h1 = sH[sl][kp];
+            R dx = h1.x - h0.x, dy = h1.y - h0.y;
+            R len = sqrt(dx * dx + dy * dy);
+            Ap += fabs(R(0.5) * (h0.x * h1.y - h0.y * h1.x));
+            Pp += len;
+            if (SCATTER) {
+                V u;
+                if (sizeof(R) == sizeof(double)) {
+                    R l = len < R(1e-18) ? R(1e-18) : len;
+                    u = mk<R>(dx / l, dy / l);
+                } else {
+                    V rk = cvt<R>(sR[sl][k]);
+                    R il = R(1) / sqrt(rk.x * rk.x + rk.y * rk.y);
+                    u = mk<R>(-rk.y * il, rk.x * il);
+                }
+                sU[sl][k] = u;
+            }
+        }
+    }
+    R A = group_sum<R>(Ap), P = group_sum<R>(Pp);
+    if (TEST) fail = group_min(fail);
+    if (ok && gl == 0 && a.AP) store_ap<R>(a.AP, c, A, P);
+    if (SCATTER) {
+        __syncwarp();
+        R Adiff = 0, Pdiff = 0;
+        if (ok) {
+            Adiff = R(a.KA) * (A - (R)a.APpref[c].x);
+            Pdiff = R(a.KP) * (P - (R)a.APpref[c].y);
+        }
+        R sx = 0, sy = 0;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            int k = gl + G * r;
+            if (ok && k < z) {
+                int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
+                V hm = sH[sl][km], hp = sH[sl][kp];
+                V um = sU[sl][km], uk = sU[sl][k];
+                R dAx = R(0.5) * (hp.y - hm.y), dAy = R(0.5) * (hm.x - hp.x);
+                R dPx = um.x - uk.x, dPy = um.y - uk.y;
+                R gx = -R(2) * (Adiff * dAx + Pdiff * dPx);
+                R gy = -R(2) * (Adiff * dAy + Pdiff * dPy);
+                V ra = cvt<R>(sR[sl][km]), rb = cvt<R>(sR[sl][k]);
+                // shared denominator: |ra x rb|^2 (the same for dh/dr_c and dh/dr_a)
+                R cr = ra.y * rb.x - ra.x * rb.y;
+                R half_inv = R(0.5) / (cr * cr);
+                R ra2 = ra.x * ra.x + ra.y * ra.y, rb2 = rb.x * rb.x + rb.y * rb.y;
+                R t1 = rb.y * ra2 - ra.y * rb2, t2 = rb.x * ra2 - ra.x * rb2;
+                R c11 = half_inv * (rb.y - ra.y) * t1, c12 = half_inv * (ra.y - rb.y) * t2;
+                R c21 = half_inv * (ra.x - rb.x) * t1, c22 = half_inv * (rb.x - ra.x) * t2;
+                // dh/dr_a = getdhdr(-ra, rb-ra)
+                V p = mk<R>(-ra.x, -ra.y), q = mk<R>(rb.x - ra.x, rb.y - ra.y);
+                R p2 = ra2, q2 = q.x * q.x + q.y * q.y;
+                R u1 = q.y * p2 - p.y * q2, u2 = q.x * p2 - p.x * q2;
+                R a11 = half_inv * (q.y - p.y) * u1, a12 = half_inv * (p.y - q.y) * u2;
+                R a21 = half_inv * (p.x - q.x) * u1, a22 = half_inv * (q.x - p.x) * u2;
+                R b11 = R(1) - c11 - a11, b12 = -c12 - a12, b21 = -c21 - a21, b22 = R(1) - c22 - a22;
+                sx += gx * c11 + gy * c21;
+                sy += gx * c12 + gy * c22;
+                sCA[sl][k] = mk<R>(gx * a11 + gy * a21, gx * a12 + gy * a22);
+                sCB[sl][k] = mk<R>(gx * b11 + gy * b21, gx * b12 + gy * b22);
+            }
+        }
+        sx = group_sum<R>(sx);
+        sy = group_sum<R>(sy);
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            int k = gl + G * r;
+            if (ok && k < z) {
+                int kp = k + 1 == z ? 0 : k + 1;
+                V cb = sCB[sl][k], ca = sCA[sl][kp];
+                atomic_add2<R>(a.F, nbk[r], cb.x + ca.x, cb.y + ca.y);
+            }
+        }
+        if (ok && gl == 0) atomic_add2<R>(a.F, c, sx, sy);
+    }
+    if (TEST && live && gl == 0 && (fail != 0x7fffffff || !ok)) {
+        if (!ok) {
+            if (a.ctl) {
+                atomicAdd(&a.ctl->n_flagged, 1);
+                claim_enqueue(a, c, a.ctl->epoch, 0);
+                if (z > VG) {
+                    atomicExch(&a.ctl->status, CG_ERR_CAPACITY);
+                    atomicExch(&a.ctl->halt, 1);
+                }
+            } else if (a.mark) {
+                a.mark[c] = 1;
+                a.queue[0] = 1;
+            }
+        } else {
+            int k = fail >> 1;
+            bool orient_fail = fail & 1;
+            int nk = row[k], nk1 = row[(k + 1) % z], nkm = row[(k + z - 1) % z];
+            if (a.ctl) {
+                int e = a.ctl->epoch;
+                atomicAdd(&a.ctl->n_flagged, 1);
+                claim_enqueue(a, c, e, 0);
+                claim_enqueue(a, nk, e, 0);
+                claim_enqueue(a, nk1, e, 0);
+                if (!orient_fail) claim_enqueue(a, nkm, e, 0);
+            } else if (a.mark) {
+                a.mark[c] = 1;
+                a.mark[nk] = 1;
+                a.mark[nk1] = 1;
+                if (!orient_fail) a.mark[nkm] = 1;
+                a.queue[0] = 1;
+            }
+        }
+    }
+}
+
+// Repair control. The exact test seeds queue 0 with the cells of every failing edge (its two ends
+// and both apexes, or the corners of an inverted triangle). Their stars are recomputed exactly;
+// rows that changed must agree with their partners' rows, and disagreeing partners are queued for
+// the next round. A round's kernels take their round index from the control block, so the rounds
+// can run inside a CUDA-graph WHILE node whose condition the device sets (cudaGraphSetConditional),
+// and an empty round costs nothing.
+__global__ void k_repair_begin(VoroArgs a, unsigned long long cond, int use_cond)
 {
     Ctl *ctl = a.ctl;
-    if (ctl->halt) return;
-    int nflag = ctl->q_count[0];
-    __syncthreads();
-    if (nflag == 0) return;
-    int e = ctl->epoch;
-    for (int t = threadIdx.x; t < nflag; t += blockDim.x) {
-        int c = a.queue[t];
-        int z = a.nn[c];
-        for (int k = 0; k < z; ++k) claim_enqueue(a, a.nbr[(size_t)c * a.K + k], e, 0);
+    ctl->round = 0;
+    unsigned v = (!ctl->halt && ctl->q_count[0] > 0) ? 1u : 0u;
+    if (use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, v);
+}
+
+__global__ void k_round_end(VoroArgs a, unsigned long long cond, int use_cond)
+{
+    Ctl *ctl = a.ctl;
+    int r = ctl->round;
+    unsigned v = 0;
+    ctl->counters[7] += 1ull;  // executed round epilogues (4 kernels per round)
+    if (!ctl->halt) {
+        ctl->counters[1] += (unsigned long long)ctl->q_count[r];
+        if (ctl->q_count[r] > 0) ctl->counters[3] += 1ull;
+        int nxt = r + 1;
+        ctl->round = nxt;
+        if (ctl->q_count[nxt] > 0) {
+            if (nxt >= R_MAX) {
+                // the local repair did not converge: escalate to a global rebuild
+                ctl->need_global = 1;
+                ctl->status = CG_ERR_TOPOLOGY;
+                ctl->halt = 1;
+            } else {
+                v = 1;
+            }
+        }
     }
+    if (use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, v);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -411,13 +648,15 @@ CG_D int warp_remove(int *cand, int m, int self, int lane)
 // Local repair star: candidates = the current 2-ring of the cell (its neighbours and theirs).
 // One warp per queued cell; result goes to the staging row of the queue slot.
 template <int WPB>
-__global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a, int round)
+__global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
 {
     __shared__ int s_cand[WPB][CAND_LOCAL];
     __shared__ double2 s_rel[WPB][CAND_LOCAL];
     __shared__ int s_out[WPB][KMAX];
     Ctl *ctl = a.ctl;
     if (ctl->halt) return;
+    int round = ctl->round;
+    if (round >= R_MAX) return;
     int nq = ctl->q_count[round];
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int gw = blockIdx.x * WPB + w, nw = gridDim.x * WPB;
@@ -463,10 +702,12 @@ __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a, int round)
 // (forces stay consistent with the topology), A/P are refreshed, and the old row is kept in the
 // staging slot for the consistency check.
 template <typename R, bool FORCES>
-__global__ void k_commit(VoroArgs a, int round)
+__global__ void k_commit(VoroArgs a)
 {
     Ctl *ctl = a.ctl;
     if (ctl->halt) return;
+    int round = ctl->round;
+    if (round >= R_MAX) return;
     int nq = ctl->q_count[round];
     const int *queue = a.queue + (size_t)round * a.N;
     int stride = gridDim.x * blockDim.x;
@@ -496,10 +737,6 @@ __global__ void k_commit(VoroArgs a, int round)
         a.changed[(size_t)round * a.N + slot] = q;
         atomicAdd(&ctl->counters[2], 1ull);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        atomicAdd(&ctl->counters[1], (unsigned long long)nq);
-        atomicAdd(&ctl->counters[3], 1ull);
-    }
 }
 
 CG_D int row_find(const int *row, int z, int v)
@@ -522,10 +759,12 @@ CG_D bool row_has_pair(const int *row, int z, int u, int v)
 // Consistency of the changed rows of a round: every new triangle (c,a,b) must appear in the rows of
 // a and b, every dropped triangle must be gone from them, and the new row must pass the exact local
 // test. Offending cells are queued for the next round.
-__global__ void k_check(VoroArgs a, int round)
+__global__ void k_check(VoroArgs a)
 {
     Ctl *ctl = a.ctl;
     if (ctl->halt) return;
+    int round = ctl->round;
+    if (round >= R_MAX) return;
     int nch = ctl->n_changed[round];
     int e = ctl->epoch + round + 1;
     int nq = round + 1;
@@ -569,18 +808,6 @@ __global__ void k_check(VoroArgs a, int round)
     }
 }
 
-// after the last round: anything still queued means the local repair did not converge
-__global__ void k_finish_repair(VoroArgs a)
-{
-    Ctl *ctl = a.ctl;
-    if (ctl->halt) return;
-    if (ctl->q_count[R_MAX] > 0) {
-        ctl->need_global = 1;
-        ctl->status = CG_ERR_TOPOLOGY;
-        ctl->halt = 1;
-    }
-}
-
 // end of a step: reset the per-step queue counters and advance the claim epoch
 __global__ void k_step_done(Ctl *ctl, int advance_step)
 {
@@ -590,6 +817,7 @@ __global__ void k_step_done(Ctl *ctl, int advance_step)
     ctl->n_flagged = 0;
     for (int r = 0; r <= R_MAX; ++r) ctl->q_count[r] = 0;
     for (int r = 0; r < R_MAX; ++r) ctl->n_changed[r] = 0;
+    ctl->round = 0;
     ctl->epoch += R_MAX + 2;
 }
 

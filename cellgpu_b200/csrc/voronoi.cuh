@@ -20,9 +20,10 @@ struct Ctl {
     int q_count[R_MAX + 1];  // per-round queue lengths
     int n_changed[R_MAX];    // per-round changed rows
     int step;                // completed integrator steps since creation
-    int pad;
+    int round;               // current local-repair round of this step
     unsigned long long counters[8];  // 0 tests failed, 1 cells restarred, 2 rows changed, 3 rounds,
-                                     // 4 global rebuilds, 5 T1 flips, 6 fire iterations, 7 spare
+                                     // 4 global rebuilds, 5 T1 flips, 6 fire iterations,
+                                     // 7 executed repair-round epilogues
 };
 
 // everything a Voronoi kernel needs, passed by value

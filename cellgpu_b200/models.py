@@ -124,7 +124,7 @@ class VoronoiBatch:
         out = (C.c_longlong * 8)()
         check(self._lib.cg_counters(self._h, out, 8))
         keys = ["tests_failed", "cells_restarred", "rows_changed", "repair_rounds", "global_rebuilds",
-                "t1_flips", "fire_iterations", "spare"]
+                "t1_flips", "fire_iterations", "round_epilogues"]
         return dict(zip(keys, list(out)))
 
     # -- compute

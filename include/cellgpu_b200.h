@@ -104,7 +104,7 @@ int cg_voronoi_triangulate(const double *pos, int N, double Lx, double Ly, int K
 typedef struct cg_system cg_system;
 
 /* Create a batch of n_inst Voronoi monolayers with N[i] cells in boxes (box[2i], box[2i+1]).
- * K is the neighbour-row capacity (>= max coordination + 1; 16 is ample for random points).
+ * K is the neighbour-row capacity, at most 16 (>= max coordination + 1; 16 is ample for random points).
  * precision: CG_FP64 or CG_MIXED. */
 int cg_voronoi_create(int n_inst, const int *N, const double *box, int K, int precision,
                       cg_system **out);
@@ -161,8 +161,9 @@ int cg_poll(cg_system *sys, int *steps_done, int *halted, int recover_if_halted)
 int cg_spp_step_host(cg_system *sys, const double *host_noise, double dt, double mu, double *host_energy);
 /* The fused geometry + force (+ exact Delaunay test) pass alone, enqueued without synchronisation. */
 int cg_launch_force_pass(cg_system *sys, int with_test);
-/* number of this library's kernels enqueued for the system so far (graph replays included) */
-long long cg_kernels_launched(const cg_system *sys);
+/* number of this library's kernels launched for the system so far, graph replays and the repair
+ * rounds run inside graph conditional nodes included (synchronises the system's stream) */
+long long cg_kernels_launched(cg_system *sys);
 
 /* counters: topology repairs, global retriangulations, T1 flips, fallbacks (per system) */
 int cg_counters(cg_system *sys, long long *out, int n);
