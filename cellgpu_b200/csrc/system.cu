@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -717,7 +718,22 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
         return CG_OK;
     };
     int st = CG_OK;
-    for (int t = 0; t < n && st == CG_OK; ++t) {
+    // CG_GRAPH_UNROLLED=1 builds the same steps with the R_MAX rounds as plain kernel nodes (empty
+    // rounds exit at once). Profilers that cannot see into conditional nodes need this form.
+    const char *unrolled = getenv("CG_GRAPH_UNROLLED");
+    if (unrolled && unrolled[0] == '1') {
+        CG_CUDA(cudaStreamBeginCaptureToGraph(s->stream, graph, nullptr, nullptr, 0, mode));
+        for (int t = 0; t < n; ++t) {
+            launch_force_test<R>(s, a, true);
+            launch_repair<R>(s, a, true);
+            k_spp<R><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, noise, dt, mu, s->seed, 0);
+            k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
+            s->kernels_enqueued += 2;
+        }
+        cudaGraph_t g2;
+        CG_CUDA(cudaStreamEndCapture(s->stream, &g2));
+    }
+    for (int t = 0; t < n && st == CG_OK && !(unrolled && unrolled[0] == '1'); ++t) {
         cudaGraphConditionalHandle h;
         CG_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
         CG_CUDA(cudaStreamBeginCaptureToGraph(s->stream, graph, deps.empty() ? nullptr : deps.data(), nullptr,

@@ -666,19 +666,40 @@ __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
         const Inst &in = inst_of(a, c);
         int z = a.nn[c];
         const int *row = a.nbr + (size_t)c * a.K;
+        // candidates: the cell's neighbours and theirs (2-ring); from round 1 on, also the
+        // neighbours of the whole 2-ring (3-ring), for cells whose new star reaches further
         int m = 0;
         if (lane < z) s_cand[w][lane] = row[lane];
         m = z;
         __syncwarp();
-        for (int k = 0; k < z; ++k) {
-            int x = s_cand[w][k];
-            int zx = a.nn[x];
-            if (m + zx > CAND_LOCAL) break;
-            if (lane < zx) s_cand[w][m + lane] = a.nbr[(size_t)x * a.K + lane];
-            m += zx;
-            __syncwarp();
+        int nsrc = z;
+        bool full = false;
+        for (int ring = 0; ring < (round == 0 ? 1 : 2) && !full; ++ring) {
+            int src_end = m;
+            for (int k = (ring == 0 ? 0 : z); k < (ring == 0 ? nsrc : src_end) && !full; ++k) {
+                int x = s_cand[w][k];
+                int zx = a.nn[x];
+                // append members of x's row that are new (warp-parallel membership test)
+                int v = (lane < zx) ? a.nbr[(size_t)x * a.K + lane] : -1;
+                bool isnew = (lane < zx) && v != c;
+                if (isnew)
+                    for (int u = 0; u < m; ++u)
+                        if (s_cand[w][u] == v) {
+                            isnew = false;
+                            break;
+                        }
+                unsigned bal = __ballot_sync(0xffffffffu, isnew);
+                if (m + __popc(bal) > CAND_LOCAL) {
+                    full = true;
+                    break;
+                }
+                __syncwarp();
+                if (isnew) s_cand[w][m + __popc(bal & ((1u << lane) - 1u))] = v;
+                m += __popc(bal);
+                __syncwarp();
+            }
+            // after the first ring, rows of the new members (k from z) extend to the next ring
         }
-        m = warp_unique(s_cand[w], m, c, lane);
         double2 pc = a.pos[c];
         for (int t = lane; t < m; t += WARP)
             s_rel[w][t] = min_dist(a.pos[s_cand[w][t]], pc, in.Lx, in.Ly);
@@ -718,7 +739,13 @@ __global__ void k_commit(VoroArgs a)
         int *srow = a.stage_nbr + (size_t)q * a.K;
         bool same = (zo == zn);
         for (int k = 0; same && k < zn; ++k) same = (row[k] == srow[k]);
-        if (same) continue;
+        if (same) {
+            // unchanged rows are still checked against their partners
+            a.stage_nn[q] = -1;
+            int slot = atomicAdd(&ctl->n_changed[round], 1);
+            a.changed[(size_t)round * a.N + slot] = q;
+            continue;
+        }
         const Inst &in = inst_of(a, c);
         double2 pc = a.pos[c];
         R A, P;
@@ -782,6 +809,7 @@ __global__ void k_check(VoroArgs a)
             if (!row_has_pair(a.nbr + (size_t)u * a.K, a.nn[u], v, c)) claim_enqueue(a, u, e, nq);
             if (!row_has_pair(a.nbr + (size_t)v * a.K, a.nn[v], c, u)) claim_enqueue(a, v, e, nq);
         }
+        if (zo < 0) continue;  // unchanged row: nothing dropped, already tested
         for (int k = 0; k < zo; ++k) {
             int u = orow[k], v = orow[(k + 1) % zo];
             if (row_has_pair(row, z, u, v)) continue;  // triangle kept
