@@ -37,6 +37,7 @@ SIGNATURES = {
     "cg_voronoi_test_triangulation": (_i, [_vp, _vp, _vp, _i, _i, _d, _d, _vp, _vp, _vp]),
     "cg_spp_step": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _d, _d, _d, _d, _u64, _u32, _vp]),
     "cg_voronoi_triangulate": (_i, [_vp, _i, _d, _d, _i, _vp, _vp, _vp]),
+    "cg_voronoi_triangulate_noalloc": (_i, [_vp, _i, _d, _d, _i, _vp, _vp, _vp]),
     "cg_voronoi_create": (_i, [_i, _vp, _vp, _i, _i, C.POINTER(_vp)]),
     "cg_destroy": (_i, [_vp]),
     "cg_num_cells": (_i, [_vp]),

@@ -922,3 +922,6 @@ extern "C" int cg_get_energies(cg_system *s, double *E)
     CG_TRY(check_launch());
     return d2h(s, E, s->d_energy, sizeof(double) * s->n_inst);
 }
+
+// allocation-free triangulation (file-scope device scratch)
+#include "noalloc.cu"
