@@ -1,0 +1,177 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes front end of oracle/_ref/libcgref.so, the reference's own CPU
+sources (abaso/cellGPU src/...) compiled in place with the DelaunayCGAL stand-in (oracle/shim).
+Only tests/ and bench.py's CPU-baseline / reference arm load it."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import time
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "libcgref.so")
+_lib = None
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def available():
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(LIB_PATH)
+        L.ref_reproducible_normals.argtypes = [C.c_int, _dp]
+        L.ref_voronoi_new.restype = C.c_void_p
+        L.ref_voronoi_new.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.ref_free.argtypes = [C.c_void_p]
+        L.ref_voronoi_set_state.argtypes = [C.c_void_p, _dp, C.c_void_p]
+        L.ref_voronoi_set_motility.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.ref_voronoi_set_preferences.argtypes = [C.c_void_p, _dp]
+        L.ref_voronoi_forces.restype = C.c_double
+        L.ref_voronoi_forces.argtypes = [C.c_void_p, _dp, _dp]
+        L.ref_voronoi_get.argtypes = [C.c_void_p, _dp, C.c_void_p, C.c_int, _ip, _ip]
+        L.ref_voronoi_spp_run.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
+        L.ref_fire.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                               C.c_double, C.c_int, C.c_double, C.c_int]
+        L.ref_vertex_new.restype = C.c_void_p
+        L.ref_vertex_new.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.ref_vertex_counts.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.ref_vertex_get.argtypes = [C.c_void_p, C.c_void_p, _dp, _ip, _ip, _ip, _ip]
+        L.ref_vertex_set_positions.argtypes = [C.c_void_p, _dp]
+        L.ref_vertex_set_preferences.argtypes = [C.c_void_p, _dp]
+        L.ref_vertex_set_t1.argtypes = [C.c_void_p, C.c_double]
+        L.ref_vertex_forces.restype = C.c_double
+        L.ref_vertex_forces.argtypes = [C.c_void_p, _dp, _dp]
+        L.ref_vertex_brownian_run.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double]
+        _lib = L
+    return _lib
+
+
+def reproducible_normals(n):
+    out = np.zeros(n)
+    lib().ref_reproducible_normals(n, out)
+    return out
+
+
+class RefVoronoi:
+    """VoronoiQuadraticEnergy of the reference, CPU branch."""
+
+    def __init__(self, N, A0=1.0, P0=3.8):
+        self.N = N
+        self.h = lib().ref_voronoi_new(N, A0, P0)
+
+    def __del__(self):
+        try:
+            lib().ref_free(self.h)
+        except Exception:
+            pass
+
+    def set_state(self, pos, theta=None):
+        pos = np.ascontiguousarray(pos, np.float64)
+        th = None if theta is None else np.ascontiguousarray(theta, np.float64)
+        lib().ref_voronoi_set_state(self.h, pos, None if th is None else th.ctypes.data_as(C.c_void_p))
+        self._th = th
+
+    def set_motility(self, v0, Dr):
+        lib().ref_voronoi_set_motility(self.h, v0, Dr)
+
+    def set_preferences(self, pref):
+        lib().ref_voronoi_set_preferences(self.h, np.ascontiguousarray(pref, np.float64))
+
+    def forces(self):
+        F = np.zeros((self.N, 2))
+        AP = np.zeros((self.N, 2))
+        E = lib().ref_voronoi_forces(self.h, F, AP)
+        return F, AP, E
+
+    def state(self, K=16):
+        pos = np.zeros((self.N, 2))
+        th = np.zeros(self.N)
+        nn = np.zeros(self.N, np.int32)
+        nbr = np.zeros((self.N, K), np.int32)
+        st = lib().ref_voronoi_get(self.h, pos, th.ctypes.data_as(C.c_void_p), K, nn, nbr)
+        if st:
+            raise RuntimeError("row longer than K")
+        return pos, th, nn, nbr
+
+    def spp_run(self, steps, dt=0.01, local_repair=True):
+        lib().ref_voronoi_spp_run(self.h, steps, dt, 1 if local_repair else 0)
+
+    def fire(self, dt=0.01, alpha_start=0.99, dt_max=0.1, dt_inc=1.05, dt_dec=0.95, alpha_dec=0.9, n_min=5,
+             force_cutoff=1e-7, max_iterations=1000):
+        lib().ref_fire(self.h, 0, dt, alpha_start, dt_max, dt_inc, dt_dec, alpha_dec, n_min, force_cutoff,
+                       max_iterations)
+
+
+class RefVertex:
+    """VertexQuadraticEnergy of the reference, CPU branch, initialised from the Delaunay dual."""
+
+    def __init__(self, Nc, A0=1.0, P0=3.8):
+        self.h = lib().ref_vertex_new(Nc, A0, P0)
+        nc, nv, vm = C.c_int(), C.c_int(), C.c_int()
+        lib().ref_vertex_counts(self.h, C.byref(nc), C.byref(nv), C.byref(vm))
+        self.Nc, self.Nv, self.vmax = nc.value, nv.value, vm.value
+
+    def __del__(self):
+        try:
+            lib().ref_free(self.h)
+        except Exception:
+            pass
+
+    def state(self):
+        cp = np.zeros((self.Nc, 2))
+        vp = np.zeros((self.Nv, 2))
+        vn = np.zeros(3 * self.Nv, np.int32)
+        vcn = np.zeros(3 * self.Nv, np.int32)
+        cvn = np.zeros(self.Nc, np.int32)
+        cv = np.zeros((self.Nc, self.vmax), np.int32)
+        lib().ref_vertex_get(self.h, cp.ctypes.data_as(C.c_void_p), vp, vn, vcn, cvn, cv)
+        return cp, vp, vn, vcn, cvn, cv
+
+    def set_positions(self, vpos):
+        lib().ref_vertex_set_positions(self.h, np.ascontiguousarray(vpos, np.float64))
+
+    def set_preferences(self, pref):
+        lib().ref_vertex_set_preferences(self.h, np.ascontiguousarray(pref, np.float64))
+
+    def set_t1(self, t):
+        lib().ref_vertex_set_t1(self.h, t)
+
+    def forces(self):
+        F = np.zeros((self.Nv, 2))
+        AP = np.zeros((self.Nc, 2))
+        E = lib().ref_vertex_forces(self.h, F, AP)
+        return F, AP, E
+
+    def brownian_run(self, steps, dt=0.005, T=1e-3, mu=1.0):
+        lib().ref_vertex_brownian_run(self.h, steps, dt, T, mu)
+
+    def fire(self, dt=0.01, alpha_start=0.99, dt_max=0.1, dt_inc=1.05, dt_dec=0.95, alpha_dec=0.9, n_min=5,
+             force_cutoff=1e-7, max_iterations=1000):
+        lib().ref_fire(self.h, 1, dt, alpha_start, dt_max, dt_inc, dt_dec, alpha_dec, n_min, force_cutoff,
+                       max_iterations)
+
+
+def bench_c2(steps, n_cells=262144, box=512.0, v0=0.1, seed=1):
+    """The reference's CPU SPP path (local test-and-repair mode, as voronoi.cpp:106-107 switches to)
+    on the large monolayer; returns the cpu_baseline record."""
+    import io
+    import contextlib
+    rng = np.random.default_rng(seed)
+    pos = rng.random((n_cells, 2)) * box
+    th = rng.uniform(0, 2 * np.pi, n_cells)
+    with contextlib.redirect_stdout(io.StringIO()):
+        r = RefVoronoi(n_cells)
+        r.set_state(pos, th)
+        r.set_motility(v0, 1.0)
+        r.spp_run(1, 0.01, True)  # first step builds the updater
+    t0 = time.perf_counter()
+    r.spp_run(steps, 0.01, True)
+    t = time.perf_counter() - t0
+    return {"value": n_cells * steps / t, "unit": "cell-steps/s", "cores": 1, "kind": "reference",
+            "sample": f"{steps} SPP steps of the N={n_cells} monolayer, reference CPU path (local "
+                      f"test-and-repair), random initial state, 1 thread"}

@@ -1,0 +1,118 @@
+"""Pins the CPU oracle against the reference's own CPU path.
+
+tests/golden/*.npz are outputs of the reference's sources (compiled in place by
+oracle/Makefile.ref, see tests/golden/make_golden.py). The oracle must reproduce them: Voronoi and
+vertex geometry, forces and energies, SPP and Brownian trajectories with the reference's own
+reproducible noise (topology and T1 rewiring bit-exact), and FIRE minimisations to the same
+force threshold. When the reference build is present, the same checks run live against it too.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from helpers import canonical, force_error
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+
+
+def _load(pattern):
+    files = sorted(glob.glob(os.path.join(GOLD, pattern)))
+    assert files, f"missing golden fixtures {pattern}"
+    return [dict(np.load(f, allow_pickle=False)) for f in files]
+
+
+@pytest.mark.parametrize("g", _load("voronoi_N*.npz"), ids=lambda g: f"N{int(g['N'])}")
+def test_voronoi_golden(oracle, g):
+    N, box = int(g["N"]), tuple(g["box"])
+    pos = g["pos"].copy()
+    nn, nbr = oracle.periodic_delaunay(pos, box, 16)
+    assert np.array_equal(canonical(nn, nbr), canonical(g["nn0"], g["nbr0"]))
+    pref = np.tile([1.0, 3.8], (N, 1))
+    AP = oracle.voronoi_geometry(pos, box, nn, nbr)
+    F = oracle.voronoi_forces(pos, box, nn, nbr, AP, pref)
+    assert np.abs(AP - g["AP0"]).max() < 1e-12
+    assert force_error(F, g["F0"]) < 1e-12
+    assert abs(oracle.voronoi_energy(AP, pref) - float(g["E0"])) < 1e-10
+    # SPP with the reference's reproducible deviates
+    theta = g["theta"].copy()
+    mot = np.tile([float(g["v0"]), float(g["Dr"])], (N, 1))
+    oracle.voronoi_spp_run(pos, box, nn, nbr, theta, mot, pref, g["noise"], dt=float(g["dt"]))
+    assert np.abs(pos - g["pos1"]).max() < 1e-11
+    assert np.abs(theta - g["theta1"]).max() < 1e-11
+    assert np.array_equal(canonical(nn, nbr), canonical(g["nn1"], g["nbr1"]))
+
+
+def test_vertex_golden(oracle):
+    g = _load("vertex_Nc*.npz")[0]
+    box, vmax = tuple(g["box"]), int(g["vmax"])
+    cp = g["cellpos"]
+    nn, nbr = oracle.periodic_delaunay(cp, box, 16)
+    vpos, vn, vcn, cvn, cv = oracle.vertex_from_delaunay(cp, box, nn, nbr, vmax=vmax)
+    assert np.abs(vpos - g["vpos"]).max() == 0.0
+    assert np.array_equal(vn, g["vn"]) and np.array_equal(vcn, g["vcn"]) and np.array_equal(cvn, g["cvn"])
+    for c in range(len(cvn)):
+        assert np.array_equal(cv[c, :cvn[c]], g["cv"][c, :cvn[c]])
+    AP = oracle.vertex_geometry(vpos, box, cvn, cv)
+    F = oracle.vertex_forces(vpos, box, cvn, cv, vcn, AP, g["pref"])
+    assert np.abs(AP - g["AP0"]).max() < 1e-12
+    assert force_error(F, g["F0"]) < 1e-12
+    oracle.vertex_brownian_run(vpos, box, vn, vcn, cvn, cv, g["pref"], g["noise"], dt=float(g["dt"]),
+                               T=float(g["T"]), t1_threshold=float(g["t1"]))
+    assert np.abs(vpos - g["vpos1"]).max() < 1e-12
+    assert np.array_equal(vn, g["vn1"]) and np.array_equal(vcn, g["vcn1"]) and np.array_equal(cvn, g["cvn1"])
+    for c in range(len(cvn)):
+        assert np.array_equal(cv[c, :cvn[c]], g["cv1"][c, :cvn[c]])
+
+
+def test_fire_voronoi_golden(oracle):
+    g = _load("fire_voronoi_*.npz")[0]
+    N, box = int(g["N"]), tuple(g["box"])
+    pos = g["pos"].copy()
+    nn, nbr = oracle.periodic_delaunay(pos, box, 16)
+    prm = oracle.FireParams.defaults(force_cutoff=float(g["cutoff"]), max_iterations=int(g["max_iterations"]))
+    F, AP, _ = oracle.fire_voronoi(pos, box, nn, nbr, np.tile([1.0, 3.8], (N, 1)), prm)
+    assert np.sqrt(np.max(np.sum(F ** 2, axis=1))) <= float(g["cutoff"])
+    assert np.abs(pos - g["pos1"]).max() < 1e-8
+    E = oracle.voronoi_energy(AP, np.tile([1.0, 3.8], (N, 1)))
+    assert abs(E - float(g["E1"])) < 1e-10 * max(1.0, abs(E))
+
+
+def test_fire_vertex_golden(oracle):
+    g = _load("fire_vertex_*.npz")[0]
+    box, vmax, Nc = tuple(g["box"]), int(g["vmax"]), int(g["Nc"])
+    vpos, vn, vcn, cvn, cv = (g["vpos"].copy(), g["vn"].copy(), g["vcn"].copy(), g["cvn"].copy(),
+                              np.ascontiguousarray(g["cv"]).copy())
+    prm = oracle.FireParams.defaults(force_cutoff=float(g["cutoff"]), max_iterations=int(g["max_iterations"]))
+    # the reference's VertexQuadraticEnergy(n, A0=1, P0=3.8) and its T1 threshold default 0.01
+    F, AP, _ = oracle.fire_vertex(vpos, box, vn, vcn, cvn, cv, np.tile([1.0, 3.8], (Nc, 1)), prm, t1_threshold=0.01)
+    assert np.abs(vpos - g["vpos1"]).max() < 1e-8
+    assert abs(oracle.voronoi_energy(AP, np.tile([1.0, 3.8], (Nc, 1))) - float(g["E1"])) < 1e-9
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libcgref.so")),
+                    reason="reference build not present")
+def test_live_reference_spp_matches_oracle(oracle):
+    import contextlib
+    import io
+
+    from oracle import ref_harness as R
+    N, steps = 500, 15
+    L = float(np.sqrt(N))
+    rng = np.random.default_rng(99)
+    pos = rng.random((N, 2)) * L
+    theta = rng.uniform(0, 2 * np.pi, N)
+    with contextlib.redirect_stdout(io.StringIO()):
+        r = R.RefVoronoi(N)
+        r.set_state(pos, theta)
+        r.set_motility(0.1, 1.0)
+        r.spp_run(steps, 0.01, True)
+        p1, t1, nn1, nbr1 = r.state()
+    noise = R.reproducible_normals(steps * N).reshape(steps, N)
+    nn, nbr = oracle.periodic_delaunay(pos, (L, L), 16)
+    oracle.voronoi_spp_run(pos, (L, L), nn, nbr, theta, np.tile([0.1, 1.0], (N, 1)), np.tile([1.0, 3.8], (N, 1)),
+                           noise)
+    assert np.abs(pos - p1).max() < 1e-11
+    assert np.array_equal(canonical(nn, nbr), canonical(nn1, nbr1))
