@@ -174,6 +174,133 @@ def e2e_steps(cg, torch, b, stream, steps):
     return st.elapsed_time(en) / 1e3, ok, 8 * b.Ntot, 8
 
 
+def c4_ensemble(seed=4, n_inst=512):
+    """512 monolayers, N log-uniform in [64, 8192], box sqrt(N), p0 U[3.6,4.0], v0 U[0.01,0.1]."""
+    rng = np.random.default_rng(seed)
+    Ns = np.round(np.exp(rng.uniform(np.log(64), np.log(8192), n_inst))).astype(int)
+    boxes = [(float(np.sqrt(n)), float(np.sqrt(n))) for n in Ns]
+    pos = [rng.random((n, 2)) * np.sqrt(n) for n in Ns]
+    theta = [rng.uniform(0, 2 * np.pi, n) for n in Ns]
+    p0 = rng.uniform(3.6, 4.0, n_inst)
+    v0 = rng.uniform(0.01, 0.1, n_inst)
+    return Ns, boxes, pos, theta, p0, v0
+
+
+def time_enqueued(torch, stream, fn, reps, flush=None):
+    """Device time of `reps` calls of fn (each enqueueing work on `stream`), runahead first."""
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    with torch.cuda.stream(stream):
+        torch.cuda._sleep(RUNAHEAD_CYCLES)
+        for i in range(reps):
+            if flush is not None:
+                flush.zero_()
+            ev[i][0].record(stream)
+            fn()
+            ev[i][1].record(stream)
+    stream.synchronize()
+    return sum(a.elapsed_time(e) for a, e in ev) / 1e3
+
+
+def bench_batched(cg, torch, flush, steps=40, equil=150):
+    """Batched ensemble (one system, one launch sequence per step for all instances) against the
+    plain path (one single-instance system per monolayer, steps enqueued instance by instance)."""
+    import ctypes as C
+    Ns, boxes, pos, theta, p0, v0 = c4_ensemble()
+    total = int(Ns.sum())
+    out = {"n_instances": len(Ns), "cells": total}
+    for name, prec in (("fp64", cg.CG_FP64), ("mixed", cg.CG_MIXED)):
+        b = cg.VoronoiBatch(list(Ns), boxes, precision=prec)
+        b.set_positions(np.concatenate(pos))
+        b.set_directors(np.concatenate(theta))
+        b.set_motility(np.concatenate([np.tile([v, 1.0], (n, 1)) for n, v in zip(Ns, v0)]))
+        b.set_preferences(np.concatenate([np.tile([1.0, p], (n, 1)) for n, p in zip(Ns, p0)]))
+        st = torch.cuda.Stream()
+        b._lib.cg_set_stream(b.handle, st.cuda_stream)
+        b.triangulate()
+        b.spp_run(equil, dt=DT, mu=MU)
+        s0 = C.c_int(0)
+        b._lib.cg_poll(b.handle, C.byref(s0), None, 1)
+        t = time_enqueued(torch, st, lambda: cg._lib.check(b._lib.cg_spp_enqueue(b.handle, 1, DT, MU)), steps, flush)
+        s1, h = C.c_int(0), C.c_int(0)
+        b._lib.cg_poll(b.handle, C.byref(s1), C.byref(h), 1)
+        done = s1.value - s0.value
+        out[f"batched_{name}"] = total * done / t
+        out[f"batched_{name}_ms_per_step"] = 1e3 * t / max(done, 1)
+        out[f"batched_{name}_counters"] = b.counters()
+        if name == "fp64":
+            keep_state = (b.positions(), b.directors())
+        del b
+    # plain: the single-instance drop-in, one system per monolayer, sampled over a subset
+    rng = np.random.default_rng(11)
+    sample = rng.choice(len(Ns), 48, replace=False)
+    systems = []
+    allpos, allth = keep_state
+    offs = np.concatenate([[0], np.cumsum(Ns)])
+    st = torch.cuda.Stream()
+    for i in sample:
+        s = cg.VoronoiBatch([int(Ns[i])], [boxes[i]])
+        s.set_positions(allpos[offs[i]:offs[i + 1]])
+        s.set_directors(allth[offs[i]:offs[i + 1]])
+        s.set_motility(np.tile([v0[i], 1.0], (Ns[i], 1)))
+        s.set_preferences(np.tile([1.0, p0[i]], (Ns[i], 1)))
+        s._lib.cg_set_stream(s.handle, st.cuda_stream)
+        s.triangulate()
+        s.spp_run(5, dt=DT, mu=MU)
+        systems.append(s)
+    plain_steps = 10
+
+    def one_round():
+        for s in systems:
+            cg._lib.check(s._lib.cg_spp_enqueue(s.handle, 1, DT, MU))
+
+    t = time_enqueued(torch, st, one_round, plain_steps)
+    cells = int(Ns[sample].sum())
+    out["plain_fp64"] = cells * plain_steps / t
+    out["plain_sample_instances"] = len(sample)
+    out["batched_over_plain_fp64"] = out["batched_fp64"] / out["plain_fp64"]
+    out["batched_mixed_over_plain_fp64"] = out["batched_mixed"] / out["plain_fp64"]
+    return out
+
+
+def bench_vertex(cg, torch, flush, steps=40, fire=True):
+    """Vertex model, Nc = 16384 in a box of side 128, p0 U[3.7,3.9], Brownian T = 1e-3, dt = 0.005,
+    T1 threshold 0.04; then FIRE to sqrt(max|F|^2) <= 1e-12."""
+    import ctypes as C
+    Nc, L = 16384, 128.0
+    rng = np.random.default_rng(3)
+    b = cg.VertexBatch([Nc], [(L, L)], vmax=30)
+    st = torch.cuda.Stream()
+    b._lib.cg_set_stream(b.handle, st.cuda_stream)
+    b.from_cells(rng.random((Nc, 2)) * L)
+    b.set_preferences(np.stack([np.ones(Nc), rng.uniform(3.7, 3.9, Nc)], 1))
+    b.set_t1_threshold(0.04)
+    b.brownian_run(50, dt=0.005, mu=1.0, T=1e-3)
+
+    def step():
+        cg._lib.check(b._lib.cg_brownian_run(b.handle, 1, 0.005, 1.0, 1e-3, None))
+
+    # cg_brownian_run synchronises (T1 status check), so time with wall-clock-free events per call
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(st)
+    b.brownian_run(steps, dt=0.005, mu=1.0, T=1e-3)
+    ev1.record(st)
+    ev1.synchronize()
+    t = ev0.elapsed_time(ev1) / 1e3
+    out = {"cells": Nc, "vertices": 2 * Nc, "brownian_cell_steps_per_s": Nc * steps / t,
+           "brownian_ms_per_step": 1e3 * t / steps, "t1_flips": b.counters()["t1_flips"]}
+    if fire:
+        p = cg.FireParams.defaults(force_cutoff=1e-12, max_iterations=20000)
+        ev0.record(st)
+        b.fire_minimize(p)
+        ev1.record(st)
+        ev1.synchronize()
+        it, fmax, fnorm = b.fire_state()
+        tf = ev0.elapsed_time(ev1) / 1e3
+        out.update({"fire_iterations": int(it[0]), "fire_fmax": float(fmax[0]), "fire_fnorm_mean_conv": float(fnorm[0]),
+                    "fire_s": tf, "fire_cell_iterations_per_s": Nc * int(it[0]) / tf})
+    return out
+
+
 def cpu_baseline_port(n_cells=N_CELLS, box=BOX, steps=3, seed=1):
     """Oracle port of the reference CPU path, 1 thread, on the same monolayer."""
     from oracle import oracle as O
@@ -208,6 +335,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched-ensemble and vertex-model measurements")
     ap.add_argument("--equilibrate", type=int, default=300,
                     help="untimed SPP steps from the random initial state before warm-up")
     args = ap.parse_args()
@@ -277,6 +406,37 @@ def main():
     e2e_t, e2e_ok, h2d, d2h = e2e_steps(cg, torch, b, stream, max(3, args.steps // 5))
     e2e_value = world * N_CELLS * e2e_ok / e2e_t if e2e_ok else 0.0
     counters = b.counters()
+    # mixed-precision force error on this (relaxed) state, against FP64
+    F64 = None
+    try:
+        import ctypes as C
+        bm = cg.VoronoiBatch([N_CELLS], [(BOX, BOX)], K=16, precision=cg.CG_MIXED if precision == cg.CG_FP64 else cg.CG_FP64)
+        b.enforce_topology()  # the mixed perimeter derivative assumes a Delaunay triangulation
+        nn, nbr = b.topology()
+        bm.set_positions(b.positions())
+        bm.set_topology(nn, nbr)
+        bm.set_preferences(np.tile([1.0, P0], (N_CELLS, 1)))
+        b.compute_forces()
+        bm.compute_forces()
+        Fa, Fb = b.forces(), bm.forces()
+        F64, Fmx = (Fa, Fb) if precision == cg.CG_FP64 else (Fb, Fa)
+        scale = float(np.sqrt(np.mean(np.sum(F64 ** 2, axis=1))))
+        d = np.linalg.norm(Fmx - F64, axis=1)
+        mixed_err = {"max": float(np.max(d / np.maximum(np.linalg.norm(F64, axis=1), scale))),
+                     "rms": float(np.sqrt(np.mean(d ** 2)) / scale), "F_scale_rms": scale}
+        del bm
+    except Exception as e:
+        mixed_err = {"error": str(e)}
+    extras = {}
+    if not args.no_extras and world == 1:
+        try:
+            extras["c4_ensemble"] = bench_batched(cg, torch, flush)
+        except Exception as e:
+            extras["c4_ensemble"] = {"error": str(e)}
+        try:
+            extras["c3_vertex"] = bench_vertex(cg, torch, flush)
+        except Exception as e:
+            extras["c3_vertex"] = {"error": str(e)}
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -309,6 +469,8 @@ def main():
         "clocks": clk.summary(),
         "counters": counters,
         "equilibrate_steps": args.equilibrate,
+        "mixed_force_error_vs_fp64": mixed_err,
+        **extras,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))

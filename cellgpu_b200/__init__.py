@@ -5,10 +5,14 @@ The compute lives in ``libcellgpu_b200.so`` (hand-written CUDA behind the C ABI 
 """
 from ._lib import (CG_ERR_ARG, CG_ERR_CAPACITY, CG_ERR_CUDA, CG_ERR_STATE, CG_ERR_TIMEOUT,  # noqa: F401
                    CG_ERR_TOPOLOGY, CG_FP64, CG_MIXED, CG_OK, CellGPUError, load)
-from .models import (Simulation, Voronoi2D, VoronoiBatch, VoronoiQuadraticEnergy,  # noqa: F401
-                     random_positions, selfPropelledParticleDynamics)
+from ._lib import FireParams  # noqa: F401
+from .models import (EnergyMinimizerFIRE, Simulation, VertexBatch, VertexQuadraticEnergy,  # noqa: F401
+                     Voronoi2D, VoronoiBatch, VoronoiQuadraticEnergy, brownianParticleDynamics,
+                     random_positions, selfPropelledCellVertexDynamics, selfPropelledParticleDynamics)
 
 __all__ = [
-    "CG_FP64", "CG_MIXED", "CellGPUError", "load", "Simulation", "Voronoi2D", "VoronoiBatch",
-    "VoronoiQuadraticEnergy", "random_positions", "selfPropelledParticleDynamics",
+    "CG_FP64", "CG_MIXED", "CellGPUError", "EnergyMinimizerFIRE", "FireParams", "load", "Simulation",
+    "VertexBatch", "VertexQuadraticEnergy", "Voronoi2D", "VoronoiBatch", "VoronoiQuadraticEnergy",
+    "brownianParticleDynamics", "random_positions", "selfPropelledCellVertexDynamics",
+    "selfPropelledParticleDynamics",
 ]

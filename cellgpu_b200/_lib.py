@@ -72,7 +72,36 @@ SIGNATURES = {
     "cg_spp_step_host": (_i, [_vp, _vp, _d, _d, _vp]),
     "cg_launch_force_pass": (_i, [_vp, _i]),
     "cg_kernels_launched": (C.c_longlong, [_vp]),
+    "cg_vertex_create": (_i, [_i, _vp, _vp, _i, _i, C.POINTER(_vp)]),
+    "cg_vertex_footprint": (_sz, [_i, _vp, _i]),
+    "cg_get_vertex_topology": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "cg_set_vertex_topology": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "cg_vertex_from_voronoi": (_i, [_vp, _vp]),
+    "cg_brownian_run": (_i, [_vp, _i, _d, _d, _d, _vp]),
+    "cg_vertex_spp_run": (_i, [_vp, _i, _d, _d, _vp]),
+    "cg_set_t1_threshold": (_i, [_vp, _d]),
+    "cg_fire_minimize": (_i, [_vp, _vp]),
+    "cg_fire_state": (_i, [_vp, _vp, _vp, _vp]),
 }
+
+class FireParams(C.Structure):
+    """cg_fire_params; defaults of EnergyMinimizerFIRE::initializeParameters
+    (src/updaters/EnergyMinimizerFIRE2D.cpp:24-41)."""
+
+    _fields_ = [("dt", _d), ("dt_max", _d), ("dt_min", _d), ("dt_inc", _d), ("dt_dec", _d),
+                ("alpha_start", _d), ("alpha_dec", _d), ("force_cutoff", _d), ("n_min", _i),
+                ("max_iterations", _i)]
+
+    @classmethod
+    def defaults(cls, **kw):
+        p = cls(dt=0.01, dt_max=0.1, dt_min=1e-4, dt_inc=1.05, dt_dec=0.95, alpha_start=0.99, alpha_dec=0.9,
+                force_cutoff=1e-7, n_min=5, max_iterations=1000)
+        for k, v in kw.items():
+            setattr(p, k, v)
+        if "dt" in kw and "dt_min" not in kw:
+            p.dt_min = 0.01 * kw["dt"]  # setDeltaT: deltaTMin = 0.01 dt (EnergyMinimizerFIRE2D.h:42)
+        return p
+
 
 _lib = None
 

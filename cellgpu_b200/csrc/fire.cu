@@ -1,0 +1,175 @@
+// cellgpu_b200 -- FIRE minimisation on the device, every instance of a batch independently.
+// EnergyMinimizerFIRE::minimize (src/updaters/EnergyMinimizerFIRE2D.cpp:269-284) with the CPU
+// conventions of velocityVerletCPU (:120-151) and fireStepCPU (:212-264): forceMax = max |F|^2,
+// dt clamped below by dt_min, the mix uses the forces just computed. Per-instance dt, alpha,
+// counters and the power / norm reductions live in device memory; an iteration is a handful of
+// kernels with no host round trip, and converged instances stop moving.
+
+namespace cg {
+
+struct FireInst {
+    double dt, alpha;
+    double power, fnorm, vnorm;
+    unsigned long long fmax_bits;  // max |F|^2 as the bit pattern of a non-negative double
+    double fmax;                   // max |F|^2 of the last completed iteration
+    double fnorm_last;             // sum |F|^2 of the last completed iteration
+    int n_since, iterations, converged, ndof;
+};
+
+struct FireArgs {
+    int ndof, n_inst;
+    const Inst *inst;
+    const int *dof_inst;
+    double2 *pos, *vel;
+    const double2 *F;
+    FireInst *st;
+    cg_fire_params prm;
+    const Ctl *ctl;  // a halted step (pending global rebuild) freezes the iteration
+};
+
+// velocity Verlet, first half: d = dt v + dt^2/2 F ; v += dt/2 F ; move and wrap
+__global__ void k_fire_vv1(FireArgs a)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.ndof) return;
+    if (a.ctl && a.ctl->halt) return;
+    int inst = a.dof_inst[i];
+    const FireInst &st = a.st[inst];
+    if (st.converged) return;
+    const Inst &in = a.inst[inst];
+    double dt = st.dt;
+    double2 v = a.vel[i], f = a.F[i];
+    double dx = __dadd_rn(__dmul_rn(dt, v.x), __dmul_rn(__dmul_rn(__dmul_rn(0.5, dt), dt), f.x));
+    double dy = __dadd_rn(__dmul_rn(dt, v.y), __dmul_rn(__dmul_rn(__dmul_rn(0.5, dt), dt), f.y));
+    v.x = __dadd_rn(v.x, __dmul_rn(__dmul_rn(0.5, dt), f.x));
+    v.y = __dadd_rn(v.y, __dmul_rn(__dmul_rn(0.5, dt), f.y));
+    a.vel[i] = v;
+    double2 p = a.pos[i];
+    p.x = __dadd_rn(p.x, dx);
+    p.y = __dadd_rn(p.y, dy);
+    a.pos[i] = put_in_box(p, in.Lx, in.Ly, in.iLx, in.iLy);
+}
+
+// second half-kick with the new forces, then the FIRE reductions per instance (block-level
+// partial sums, one atomic per block and instance run)
+__global__ void k_fire_vv2(FireArgs a)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a.ctl && a.ctl->halt) return;
+    int inst = -1;
+    double P = 0, ff = 0, vv = 0, fm = 0;
+    if (i < a.ndof) {
+        inst = a.dof_inst[i];
+        const FireInst &st = a.st[inst];
+        if (!st.converged) {
+            double dt = st.dt;
+            double2 v = a.vel[i], f = a.F[i];
+            v.x = __dadd_rn(v.x, __dmul_rn(__dmul_rn(0.5, dt), f.x));
+            v.y = __dadd_rn(v.y, __dmul_rn(__dmul_rn(0.5, dt), f.y));
+            a.vel[i] = v;
+            P = f.x * v.x + f.y * v.y;
+            ff = f.x * f.x + f.y * f.y;
+            vv = v.x * v.x + v.y * v.y;
+            fm = ff;
+        } else {
+            inst = -1;
+        }
+    }
+    // warp-level segmented reduction (lanes of one instance are contiguous)
+    unsigned full = 0xffffffffu;
+    int lane = threadIdx.x & 31;
+    int first = __shfl_sync(full, inst, 0);
+    bool uniform = __all_sync(full, inst == first);
+    if (uniform) {
+        for (int off = 16; off > 0; off >>= 1) {
+            P += __shfl_down_sync(full, P, off);
+            ff += __shfl_down_sync(full, ff, off);
+            vv += __shfl_down_sync(full, vv, off);
+            fm = fmax(fm, __shfl_down_sync(full, fm, off));
+        }
+        if (lane == 0 && inst >= 0) {
+            atomicAdd(&a.st[inst].power, P);
+            atomicAdd(&a.st[inst].fnorm, ff);
+            atomicAdd(&a.st[inst].vnorm, vv);
+            atomicMax(&a.st[inst].fmax_bits, (unsigned long long)__double_as_longlong(fm));
+        }
+    } else if (inst >= 0) {
+        atomicAdd(&a.st[inst].power, P);
+        atomicAdd(&a.st[inst].fnorm, ff);
+        atomicAdd(&a.st[inst].vnorm, vv);
+        atomicMax(&a.st[inst].fmax_bits, (unsigned long long)__double_as_longlong(fm));
+    }
+}
+
+// FIRE mix v <- (1-alpha) v + alpha sqrt(|v|^2/|F|^2) F, or v <- 0 when the power is not positive
+__global__ void k_fire_mix(FireArgs a)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.ndof) return;
+    if (a.ctl && a.ctl->halt) return;
+    const FireInst &st = a.st[a.dof_inst[i]];
+    if (st.converged) return;
+    if (!(st.power > 0)) {
+        a.vel[i] = make_double2(0.0, 0.0);
+        return;
+    }
+    double scaling = st.fnorm > 0. ? sqrt(st.vnorm / st.fnorm) : 0.0;
+    double al = st.alpha;
+    double2 v = a.vel[i], f = a.F[i];
+    v.x = (1.0 - al) * v.x + al * scaling * f.x;
+    v.y = (1.0 - al) * v.y + al * scaling * f.y;
+    a.vel[i] = v;
+}
+
+// per instance: dt / alpha / N_since update, iteration count, convergence test of the loop head
+__global__ void k_fire_update(FireArgs a, unsigned long long *iter_counter)
+{
+    int inst = blockIdx.x * blockDim.x + threadIdx.x;
+    if (inst >= a.n_inst) return;
+    if (a.ctl && a.ctl->halt) return;
+    FireInst &st = a.st[inst];
+    if (st.converged) return;
+    st.iterations += 1;
+    atomicAdd(iter_counter, 1ull);
+    const cg_fire_params &p = a.prm;
+    if (st.power > 0) {
+        if (st.n_since > p.n_min) {
+            st.dt = fmin(st.dt * p.dt_inc, p.dt_max);
+            st.alpha = st.alpha * p.alpha_dec;
+        }
+        st.n_since += 1;
+    } else {
+        st.dt = st.dt * p.dt_dec;
+        st.dt = fmax(st.dt, p.dt_min);
+        st.alpha = p.alpha_start;
+    }
+    st.fmax = __longlong_as_double((long long)st.fmax_bits);
+    st.fnorm_last = st.fnorm;
+    st.converged = !(st.iterations < p.max_iterations && sqrt(st.fmax) > p.force_cutoff);
+    st.power = 0;
+    st.fnorm = 0;
+    st.vnorm = 0;
+    st.fmax_bits = 0;
+}
+
+__global__ void k_fire_init(FireArgs a)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.ndof) a.vel[i] = make_double2(0.0, 0.0);
+    if (i < a.n_inst) {
+        FireInst s;
+        s.dt = a.prm.dt;
+        s.alpha = a.prm.alpha_start;
+        s.power = s.fnorm = s.vnorm = 0;
+        s.fmax_bits = 0;
+        s.fmax = 110.0;  // minimize() starts the loop with forceMax = 110
+        s.fnorm_last = 0;
+        s.n_since = 0;
+        s.iterations = 0;
+        s.converged = !(0 < a.prm.max_iterations && sqrt(110.0) > a.prm.force_cutoff);
+        s.ndof = a.inst[i].nv > 0 ? a.inst[i].nv : a.inst[i].n;
+        a.st[i] = s;
+    }
+}
+
+}  // namespace cg

@@ -1,0 +1,147 @@
+// cellgpu_b200 -- host side of FIRE minimisation (both models). Included by system.cu.
+
+static int fire_alloc(cg_system *s)
+{
+    if (s->fire_vel) return CG_OK;
+    CG_TRY(dalloc(s, &s->fire_vel, ndof(s)));
+    FireInst *fs = nullptr;
+    CG_TRY(dalloc(s, &fs, s->n_inst));
+    s->fire_st = fs;
+    CG_TRY(dalloc(s, &s->fire_dofinst, ndof(s)));
+    if (s->model == CG_MODEL_VORONOI) {
+        CG_CUDA(cudaMemcpy(s->fire_dofinst, s->cell_inst, sizeof(int) * s->N, cudaMemcpyDeviceToDevice));
+    } else {
+        CG_CUDA(cudaMemcpy(s->fire_dofinst, s->vert_inst, sizeof(int) * s->Nv, cudaMemcpyDeviceToDevice));
+    }
+    return CG_OK;
+}
+
+static FireArgs fire_args(cg_system *s, const cg_fire_params &prm)
+{
+    FireArgs a;
+    memset(&a, 0, sizeof(a));
+    a.ndof = ndof(s);
+    a.n_inst = s->n_inst;
+    a.inst = s->inst;
+    a.dof_inst = s->fire_dofinst;
+    a.pos = s->pos;
+    a.vel = s->fire_vel;
+    a.F = reinterpret_cast<const double2 *>(s->F);
+    a.st = reinterpret_cast<FireInst *>(s->fire_st);
+    a.prm = prm;
+    a.ctl = s->ctl;
+    return a;
+}
+
+// forces on the current topology (the loop head of minimize: computeForces before the loop)
+static void fire_forces(cg_system *s, bool test_and_repair)
+{
+    if (s->model == CG_MODEL_VORONOI) {
+        VoroArgs a = sys_args(s);
+        if (s->precision == CG_FP64) {
+            launch_force_test<double>(s, a, test_and_repair);
+            if (test_and_repair) launch_repair<double>(s, a, true);
+        } else {
+            launch_force_test<float>(s, a, test_and_repair);
+            if (test_and_repair) launch_repair<float>(s, a, true);
+        }
+        if (test_and_repair) {
+            k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 0);
+            s->kernels_enqueued += 1;
+        }
+    } else {
+        VertArgs a = vm_args(s);
+        if (test_and_repair) vm_launch_t1(s, a);
+        cudaMemsetAsync(s->F, 0, sizeof(double2) * s->Nv, s->stream);
+        k_vm_forces<<<nblk(s->N, 128), 128, 0, s->stream>>>(a, 1);
+        s->kernels_enqueued += 1;
+    }
+}
+
+// one FIRE iteration: velocity Verlet (move, topology, forces), then the FIRE step
+static void fire_enqueue_iteration(cg_system *s, const cg_fire_params &prm)
+{
+    FireArgs f = fire_args(s, prm);
+    int nd = ndof(s);
+    k_fire_vv1<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
+    fire_forces(s, true);
+    k_fire_vv2<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
+    k_fire_mix<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
+    k_fire_update<<<nblk(s->n_inst, 64), 64, 0, s->stream>>>(f, &s->ctl->counters[6]);
+    s->kernels_enqueued += 4;
+}
+
+extern "C" int cg_fire_minimize(cg_system *s, const cg_fire_params *prm)
+{
+    if (!s || !prm || prm->max_iterations < 0 || !(prm->dt > 0)) return set_err(CG_ERR_ARG, "bad args");
+    if (!s->topology_valid) {
+        if (s->model == CG_MODEL_VORONOI) CG_TRY(triangulate_sys(s));
+        else return set_err(CG_ERR_STATE, "vertex topology not set");
+    }
+    CG_TRY(fire_alloc(s));
+    FireArgs f = fire_args(s, *prm);
+    k_fire_init<<<nblk(std::max(ndof(s), s->n_inst), 256), 256, 0, s->stream>>>(f);
+    fire_forces(s, false);
+    CG_TRY(check_launch());
+    std::vector<FireInst> st(s->n_inst);
+    const int chunk = 16;
+    int rounds = 0;
+    for (;;) {
+        // a graph of `chunk` iterations (direct launches of the same kernels if capture is refused)
+        cudaGraphExec_t exec = nullptr;
+        long long nk = 0;
+        for (auto &g : s->graphs)
+            if (g.kind == 3 && g.n == chunk && g.dt == prm->dt && g.mu == prm->force_cutoff && g.T == prm->dt_max) {
+                exec = g.exec;
+                nk = g.kernels;
+            }
+        if (!exec) {
+            cudaGraph_t graph;
+            long long k0 = s->kernels_enqueued;
+            CG_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            for (int t = 0; t < chunk; ++t) fire_enqueue_iteration(s, *prm);
+            CG_CUDA(cudaStreamEndCapture(s->stream, &graph));
+            CG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+            cudaGraphDestroy(graph);
+            nk = s->kernels_enqueued - k0;
+            s->kernels_enqueued = k0;
+            s->graphs.push_back({3, chunk, prm->dt, prm->force_cutoff, prm->dt_max, nullptr, exec, nk});
+        }
+        CG_CUDA(cudaGraphLaunch(exec, s->stream));
+        s->kernels_enqueued += nk;
+        CG_TRY(check_launch());
+        Ctl c;
+        CG_TRY(read_ctl(s, c));
+        if (c.halt) {
+            // a Voronoi step needed a global rebuild: rebuild, recompute forces and finish the
+            // halted iteration (its first half-kick and move already happened)
+            if (s->model != CG_MODEL_VORONOI) return vm_check_halt(s);
+            CG_TRY(recover(s));
+            fire_forces(s, false);
+            int nd = ndof(s);
+            k_fire_vv2<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
+            k_fire_mix<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
+            k_fire_update<<<nblk(s->n_inst, 64), 64, 0, s->stream>>>(f, &s->ctl->counters[6]);
+            CG_TRY(check_launch());
+        }
+        CG_TRY(d2h(s, st.data(), s->fire_st, sizeof(FireInst) * s->n_inst));
+        bool all = true;
+        for (auto &x : st) all = all && x.converged;
+        if (all) break;
+        if (++rounds > prm->max_iterations / chunk + 64) return set_err(CG_ERR_STATE, "FIRE did not stop");
+    }
+    return CG_OK;
+}
+
+extern "C" int cg_fire_state(cg_system *s, int *iterations, double *fmax_cpu, double *fnorm_gpu)
+{
+    if (!s || !s->fire_st) return set_err(CG_ERR_STATE, "no FIRE run on this system");
+    std::vector<FireInst> st(s->n_inst);
+    CG_TRY(d2h(s, st.data(), s->fire_st, sizeof(FireInst) * s->n_inst));
+    for (int i = 0; i < s->n_inst; ++i) {
+        if (iterations) iterations[i] = st[i].iterations;
+        if (fmax_cpu) fmax_cpu[i] = sqrt(st[i].fmax);
+        if (fnorm_gpu) fnorm_gpu[i] = st[i].ndof > 0 ? sqrt(st[i].fnorm_last / st[i].ndof) : 0.0;
+    }
+    return CG_OK;
+}

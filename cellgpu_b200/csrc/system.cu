@@ -9,6 +9,8 @@
 #include <vector>
 
 #include "voronoi.cu"
+#include "vertex.cu"
+#include "fire.cu"
 
 using namespace cg;
 
@@ -175,6 +177,7 @@ struct cg_system {
     void *AP = nullptr, *F = nullptr;
     int *nn = nullptr, *nbr = nullptr;
     int *mark = nullptr, *queue = nullptr, *stage_nn = nullptr, *stage_nbr = nullptr, *changed = nullptr;
+    int *held = nullptr;
     Ctl *ctl = nullptr;
     int *bin_count = nullptr, *bin_start = nullptr, *bin_cells = nullptr, *cell_bin = nullptr,
         *cell_slot = nullptr;
@@ -189,8 +192,9 @@ struct cg_system {
     cudaStream_t own_stream = nullptr;
     cudaStream_t body_stream = nullptr;  // captures the bodies of conditional graph nodes
     struct GraphEntry {
+        int kind;  // 0 Voronoi SPP, 1 vertex Brownian, 2 vertex SPP, 3 FIRE iterations
         int n;
-        double dt, mu;
+        double dt, mu, T;
         const double *noise;
         cudaGraphExec_t exec;
         long long kernels;
@@ -198,7 +202,18 @@ struct cg_system {
     std::vector<GraphEntry> graphs;
     long long kernels_enqueued = 0;  // kernels of this library launched for this system
     double *noise_buf = nullptr;     // staging for host-supplied noise (one step)
+    // vertex model (model == CG_MODEL_VERTEX): pos/F are per vertex, AP/APpref/theta/motility per cell
+    int Nv = 0, vmax = 0;
+    int *vert_inst = nullptr, *vn = nullptr, *vcn = nullptr, *cvn = nullptr, *cv = nullptr;
+    int *t1_cand = nullptr, *t1_count = nullptr;
+    double t1 = 0.01;  // vertexModelBase default (src/models/vertexModelBase.cpp:59)
+    // FIRE (allocated on first use)
+    double2 *fire_vel = nullptr;
+    void *fire_st = nullptr;
+    int *fire_dofinst = nullptr;
 };
+
+static int ndof(const cg_system *s) { return s->model == CG_MODEL_VERTEX ? s->Nv : s->N; }
 
 template <typename T>
 static int dalloc(cg_system *s, T **p, size_t count)
@@ -237,6 +252,7 @@ static VoroArgs sys_args(cg_system *s)
     a.stage_nn = s->stage_nn;
     a.stage_nbr = s->stage_nbr;
     a.changed = s->changed;
+    a.held = s->held;
     a.ctl = s->ctl;
     a.bin_count = s->bin_count;
     a.bin_start = s->bin_start;
@@ -251,7 +267,7 @@ static VoroArgs sys_args(cg_system *s)
 static size_t voronoi_bytes(int N, int K, int n_bins, int n_inst, int precision)
 {
     size_t real2 = precision == CG_FP64 ? 16 : 8;
-    size_t per_cell = 4 /*cell_inst*/ + 16 * 3 /*pos, motility, APpref*/ + 8 /*theta*/ + 2 * real2 +
+    size_t per_cell = 4 /*cell_inst*/ + 4 /*held*/ + 16 * 3 /*pos, motility, APpref*/ + 8 /*theta*/ + 2 * real2 +
                       4 + 4 * (size_t)K /*nn, nbr*/ + 4 /*mark*/ + 4 * (R_MAX + 1) /*queue*/ + 4 +
                       4 * (size_t)K /*stage*/ + 4 * R_MAX /*changed*/ + 4 * 3 + 16 /*cell list*/;
     return per_cell * (size_t)N + (size_t)n_bins * 8 + (size_t)n_inst * (sizeof(Inst) + 16) + 4096;
@@ -313,6 +329,7 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
         if ((st = dalloc(s, &s->stage_nn, Nt))) break;
         if ((st = dalloc(s, &s->stage_nbr, (size_t)Nt * K))) break;
         if ((st = dalloc(s, &s->changed, (size_t)Nt * R_MAX))) break;
+        if ((st = dalloc(s, &s->held, Nt))) break;
         if ((st = dalloc(s, &s->ctl, 1))) break;
         if ((st = dalloc(s, &s->bin_count, s->n_bins + 1))) break;
         if ((st = dalloc(s, &s->bin_start, s->n_bins + 1))) break;
@@ -376,7 +393,7 @@ extern "C" int cg_destroy(cg_system *s)
 }
 
 extern "C" int cg_num_cells(const cg_system *s) { return s ? s->N : 0; }
-extern "C" int cg_num_dofs(const cg_system *s) { return s ? s->N : 0; }
+extern "C" int cg_num_dofs(const cg_system *s) { return s ? ndof(s) : 0; }
 extern "C" int cg_num_instances(const cg_system *s) { return s ? s->n_inst : 0; }
 extern "C" int cg_neighbor_capacity(const cg_system *s) { return s ? s->K : 0; }
 extern "C" size_t cg_device_bytes(const cg_system *s) { return s ? s->bytes : 0; }
@@ -415,13 +432,13 @@ static int d2h(cg_system *s, void *dst, const void *src, size_t b)
 extern "C" int cg_set_positions(cg_system *s, const double *pos)
 {
     if (!s || !pos) return set_err(CG_ERR_ARG, "bad args");
-    s->topology_valid = false;
-    return h2d(s, s->pos, pos, sizeof(double2) * s->N);
+    s->topology_valid = s->model == CG_MODEL_VERTEX ? s->topology_valid : false;
+    return h2d(s, s->pos, pos, sizeof(double2) * ndof(s));
 }
 extern "C" int cg_get_positions(cg_system *s, double *pos)
 {
     if (!s || !pos) return set_err(CG_ERR_ARG, "bad args");
-    return d2h(s, pos, s->pos, sizeof(double2) * s->N);
+    return d2h(s, pos, s->pos, sizeof(double2) * ndof(s));
 }
 extern "C" int cg_set_cell_preferences(cg_system *s, const double *p)
 {
@@ -472,7 +489,7 @@ static int get_real2(cg_system *s, const void *src, double *dst, int n)
 extern "C" int cg_get_forces(cg_system *s, double *F)
 {
     if (!s || !F) return set_err(CG_ERR_ARG, "bad args");
-    return get_real2(s, s->F, F, s->N);
+    return get_real2(s, s->F, F, ndof(s));
 }
 extern "C" int cg_get_area_perimeter(cg_system *s, double *AP)
 {
@@ -481,13 +498,13 @@ extern "C" int cg_get_area_perimeter(cg_system *s, double *AP)
 }
 extern "C" int cg_get_topology(cg_system *s, int *nn, int *nbr)
 {
-    if (!s || !nn || !nbr) return set_err(CG_ERR_ARG, "bad args");
+    if (!s || !nn || !nbr || s->model != CG_MODEL_VORONOI) return set_err(CG_ERR_ARG, "bad args");
     CG_TRY(d2h(s, nn, s->nn, sizeof(int) * s->N));
     return d2h(s, nbr, s->nbr, sizeof(int) * (size_t)s->N * s->K);
 }
 extern "C" int cg_set_topology(cg_system *s, const int *nn, const int *nbr)
 {
-    if (!s || !nn || !nbr) return set_err(CG_ERR_ARG, "bad args");
+    if (!s || !nn || !nbr || s->model != CG_MODEL_VORONOI) return set_err(CG_ERR_ARG, "bad args");
     for (int i = 0; i < s->N; ++i)
         if (nn[i] < 3 || nn[i] > s->K) return set_err(CG_ERR_ARG, "row length out of range");
     CG_TRY(h2d(s, s->nn, nn, sizeof(int) * s->N));
@@ -637,6 +654,7 @@ static int recover(cg_system *s)
     if (!c.halt) return CG_OK;
     if (c.status == CG_ERR_CAPACITY) return set_err(CG_ERR_CAPACITY, "neighbour capacity exceeded");
     CG_TRY(reset_ctl_after_halt(s));
+    if (s->held) CG_CUDA(cudaMemsetAsync(s->held, 0, sizeof(int) * s->N, s->stream));
     return triangulate_sys(s);
 }
 
@@ -648,9 +666,13 @@ static int compute_forces_t(cg_system *s)
     return check_launch();
 }
 
+static int vm_compute_forces(cg_system *s);
+static int vm_enforce(cg_system *s);
+
 extern "C" int cg_compute_forces(cg_system *s)
 {
     if (!s) return set_err(CG_ERR_ARG, "null system");
+    if (s->model == CG_MODEL_VERTEX) return vm_compute_forces(s);
     if (!s->topology_valid) CG_TRY(triangulate_sys(s));
     int st = s->precision == CG_FP64 ? compute_forces_t<double>(s) : compute_forces_t<float>(s);
     if (st) return st;
@@ -677,6 +699,7 @@ static int enforce_t(cg_system *s)
 extern "C" int cg_enforce_topology(cg_system *s)
 {
     if (!s) return set_err(CG_ERR_ARG, "null system");
+    if (s->model == CG_MODEL_VERTEX) return vm_enforce(s);
     if (!s->topology_valid) return triangulate_sys(s);
     return s->precision == CG_FP64 ? enforce_t<double>(s) : enforce_t<float>(s);
 }
@@ -781,7 +804,7 @@ template <typename R>
 static int enqueue_graph(cg_system *s, int n, double dt, double mu, const double *noise)
 {
     for (auto &g : s->graphs)
-        if (g.n == n && g.dt == dt && g.mu == mu && g.noise == noise) {
+        if (g.kind == 0 && g.n == n && g.dt == dt && g.mu == mu && g.noise == noise) {
             CG_CUDA(cudaGraphLaunch(g.exec, s->stream));
             s->kernels_enqueued += g.kernels;
             return CG_OK;
@@ -789,7 +812,7 @@ static int enqueue_graph(cg_system *s, int n, double dt, double mu, const double
     cudaGraphExec_t exec;
     long long nk = 0;
     CG_TRY(build_graph<R>(s, n, dt, mu, noise, &exec, &nk));
-    s->graphs.push_back({n, dt, mu, noise, exec, nk});
+    s->graphs.push_back({0, n, dt, mu, 0.0, noise, exec, nk});
     CG_CUDA(cudaGraphLaunch(exec, s->stream));
     s->kernels_enqueued += nk;
     return CG_OK;
@@ -913,7 +936,7 @@ extern "C" int cg_spp_run(cg_system *s, int n_steps, double dt, double mu, const
 extern "C" int cg_get_energies(cg_system *s, double *E)
 {
     if (!s || !E) return set_err(CG_ERR_ARG, "bad args");
-    VoroArgs a = sys_args(s);
+    VoroArgs a = sys_args(s);  // N = cells: A/P and preferences are per cell in both models
     CG_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * s->n_inst, s->stream));
     if (s->precision == CG_FP64)
         k_energy<double><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
@@ -925,3 +948,9 @@ extern "C" int cg_get_energies(cg_system *s, double *E)
 
 // allocation-free triangulation (file-scope device scratch)
 #include "noalloc.cu"
+
+// vertex model systems
+#include "vertex_sys.cu"
+
+// FIRE
+#include "fire_sys.cu"

@@ -1,0 +1,452 @@
+// cellgpu_b200 -- vertex (AVM) model kernels for sm_100a: fused geometry + forces, Brownian and
+// self-propelled integrators, the T1 edge test-and-flip, and the vertex initialisation from a
+// Delaunay triangulation (the Voronoi dual). Included into system.cu after voronoi.cu.
+#include "voronoi.cuh"
+
+namespace cg {
+
+// T1 candidate queue: one slot per edge of the instance (3 * its vertices), so neither the
+// detection nor the keys queued during the replay can overflow
+
+struct VertArgs {
+    int Nc, Nv, vmax, n_inst;
+    const Inst *inst;
+    const int *cell_inst, *vert_inst;
+    double2 *vpos;
+    double2 *F;
+    double2 *AP;
+    const double2 *APpref;
+    double KA, KP;
+    int *vn, *vcn, *cvn, *cv;
+    double *theta;
+    const double2 *motility;
+    // T1
+    double t1;
+    int *cand;        // 3*Nv edge keys (3*v + slot), instance i at 3 * (its first vertex)
+    int *cand_count;  // n_inst
+    Ctl *ctl;
+};
+
+// ------------------------------------------------------------------------------------------
+// geometry + forces. Per cell: the polygon relative to its vertex at slot z-2, signed shoelace
+// area and perimeter (vertexModelBase::computeGeometryCPU, src/models/vertexModelBase.cpp:248-297);
+// then every vertex of the cell receives the force set computeForceSetVertexModel(vcur, vlast,
+// vnext, KA(A-A0), KP(P-P0)) (inc/utility/functions.h:330-354) -- added directly to the vertex's
+// force, which is the sum of its three sets (src/models/vertexQuadraticEnergy.cpp:100-112).
+// ------------------------------------------------------------------------------------------
+__global__ void k_vm_forces(VertArgs a, int scatter)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.Nc) return;
+    if (a.ctl && a.ctl->halt) return;
+    const Inst &in = a.inst[a.cell_inst[c]];
+    int z = a.cvn[c];
+    const int *row = a.cv + (size_t)c * a.vmax;
+    double2 cp = a.vpos[row[z - 2]];
+    double2 vcur = min_dist(a.vpos[row[z - 1]], cp, in.Lx, in.Ly);
+    double A = 0.0, P = 0.0;
+    for (int n = 0; n < z; ++n) {
+        double2 vnext = min_dist(a.vpos[row[n]], cp, in.Lx, in.Ly);
+        A += 0.5 * (vcur.x + vnext.x) * (vnext.y - vcur.y);
+        double dx = vcur.x - vnext.x, dy = vcur.y - vnext.y;
+        P += sqrt(dx * dx + dy * dy);
+        vcur = vnext;
+    }
+    a.AP[c] = make_double2(A, P);
+    if (!scatter) return;
+    double Adiff = a.KA * (A - a.APpref[c].x), Pdiff = a.KP * (P - a.APpref[c].y);
+    double2 vlast = min_dist(a.vpos[row[z - 2]], cp, in.Lx, in.Ly);
+    vcur = min_dist(a.vpos[row[z - 1]], cp, in.Lx, in.Ly);
+    int vidx = row[z - 1];
+    for (int n = 0; n < z; ++n) {
+        int nv = row[n];
+        double2 vnext = min_dist(a.vpos[nv], cp, in.Lx, in.Ly);
+        double dAx = 0.5 * (vlast.y - vnext.y), dAy = -0.5 * (vlast.x - vnext.x);
+        double lx = vlast.x - vcur.x, ly = vlast.y - vcur.y;
+        double ln = sqrt(lx * lx + ly * ly);
+        double nx = vcur.x - vnext.x, ny = vcur.y - vnext.y;
+        double nnm = sqrt(nx * nx + ny * ny);
+        double fx = 2.0 * (Adiff * dAx + Pdiff * (lx / ln - nx / nnm));
+        double fy = 2.0 * (Adiff * dAy + Pdiff * (ly / ln - ny / nnm));
+        atomicAdd(&a.F[vidx].x, fx);
+        atomicAdd(&a.F[vidx].y, fy);
+        vlast = vcur;
+        vcur = vnext;
+        vidx = nv;
+    }
+}
+
+// brownianParticleDynamics::integrateEquationsOfMotionCPU (src/updaters/brownianParticleDynamics.cpp:92-109)
+// + vertexModelBase::moveDegreesOfFreedom (src/models/vertexModelBase.cpp:11-47):
+// d = xi sqrt(2 dt T mu) + dt mu F, two normals per vertex (x then y)
+__global__ void k_vm_brownian(VertArgs a, const double *noise2, double dt, double mu, double T, uint64_t seed)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= a.Nv) return;
+    if (a.ctl && a.ctl->halt) return;
+    const Inst &in = a.inst[a.vert_inst[v]];
+    double r1, r2;
+    if (noise2) {
+        r1 = noise2[2 * (size_t)v];
+        r2 = noise2[2 * (size_t)v + 1];
+    } else {
+        double2 g = normal2(seed, (uint32_t)v, a.ctl ? (uint32_t)a.ctl->step : 0u, 1u);
+        r1 = g.x;
+        r2 = g.y;
+    }
+    double amp = sqrt(__dmul_rn(__dmul_rn(__dmul_rn(2.0, dt), T), mu));
+    double2 f = a.F[v];
+    double dx = __dadd_rn(__dmul_rn(r1, amp), __dmul_rn(__dmul_rn(dt, mu), f.x));
+    double dy = __dadd_rn(__dmul_rn(r2, amp), __dmul_rn(__dmul_rn(dt, mu), f.y));
+    double2 p = a.vpos[v];
+    p.x = __dadd_rn(p.x, dx);
+    p.y = __dadd_rn(p.y, dy);
+    a.vpos[v] = put_in_box(p, in.Lx, in.Ly, in.iLx, in.iLy);
+}
+
+// selfPropelledCellVertexDynamics::integrateEquationsOfMotionCPU
+// (src/updaters/selfPropelledCellVertexDynamics.cpp:81-122): vertex velocity = mean of its three
+// cells' v0 n, displacement dt (v + mu F), then move; directors are advanced afterwards (below)
+__global__ void k_vm_spp_vertices(VertArgs a, double dt, double mu)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= a.Nv) return;
+    if (a.ctl && a.ctl->halt) return;
+    const Inst &in = a.inst[a.vert_inst[v]];
+    double dx = 0.0, dy = 0.0;
+    for (int f = 0; f < 3; ++f) {
+        int c = a.vcn[3 * v + f];
+        double s, co;
+        sincos(a.theta[c], &s, &co);
+        double v0 = a.motility[c].x;
+        dx = __dadd_rn(dx, __dmul_rn(v0, co));
+        dy = __dadd_rn(dy, __dmul_rn(v0, s));
+    }
+    dx = __ddiv_rn(dx, 3.0);
+    dy = __ddiv_rn(dy, 3.0);
+    double2 fo = a.F[v];
+    double2 p = a.vpos[v];
+    p.x = __dadd_rn(p.x, __dmul_rn(dt, __dadd_rn(dx, __dmul_rn(mu, fo.x))));
+    p.y = __dadd_rn(p.y, __dmul_rn(dt, __dadd_rn(dy, __dmul_rn(mu, fo.y))));
+    a.vpos[v] = put_in_box(p, in.Lx, in.Ly, in.iLx, in.iLy);
+}
+
+__global__ void k_vm_spp_directors(VertArgs a, const double *noise, double dt, uint64_t seed)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.Nc) return;
+    if (a.ctl && a.ctl->halt) return;
+    double xi = noise ? noise[c] : normal2(seed, (uint32_t)c, a.ctl ? (uint32_t)a.ctl->step : 0u, 2u).x;
+    a.theta[c] = __dadd_rn(a.theta[c], __dmul_rn(xi, sqrt(__dmul_rn(__dmul_rn(2.0, dt), a.motility[c].y))));
+}
+
+// ------------------------------------------------------------------------------------------
+// T1 transitions. The reference's CPU sweep (vertexModelBase::testAndPerformT1TransitionsCPU,
+// src/models/vertexModelBase.cpp:631-787) visits vertex1 ascending and its three neighbour slots,
+// tests norm(edge) < threshold on the current state and flips at once, so later tests see moved
+// vertices and rewired lists. Here: (1) every edge is tested in parallel on the state at the start
+// of the sweep (edges that fail there and are not touched by a flip fail in the sweep too);
+// (2) one thread per instance replays the sweep over the candidate keys (3*vertex1 + slot) in
+// ascending order, and after each flip queues the keys of every edge the flip moved or rewired that
+// lie ahead of the current key -- exactly the edges whose test could change. Equivalent to the
+// full sequential sweep, at the cost of the candidates only.
+// ------------------------------------------------------------------------------------------
+CG_D double edge_len(double2 p1, double2 p2, const Inst &in)
+{
+    double2 e = min_dist(p1, p2, in.Lx, in.Ly);
+    return __dsqrt_rn(__dadd_rn(__dmul_rn(e.x, e.x), __dmul_rn(e.y, e.y)));
+}
+
+__global__ void k_vm_t1_detect(VertArgs a)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a.ctl && a.ctl->halt) return;
+    bool any[3] = {false, false, false};
+    int inst = 0;
+    if (v < a.Nv) {
+        inst = a.vert_inst[v];
+        const Inst &in = a.inst[inst];
+        double2 p = a.vpos[v];
+        for (int s = 0; s < 3; ++s) {
+            int w = a.vn[3 * v + s];
+            if (v < w && edge_len(p, a.vpos[w], in) < a.t1) any[s] = true;
+        }
+    }
+    for (int s = 0; s < 3; ++s) {
+        if (any[s]) {
+            int slot = atomicAdd(&a.cand_count[inst], 1);
+            a.cand[3 * (size_t)a.inst[inst].voff + slot] = 3 * v + s;
+        }
+    }
+}
+
+CG_D void find_in_cell_d(const int *row, int cneigh, int target, int &vlast, int &vcur, int &vnext)
+{
+    int l = row[cneigh - 2], c = row[cneigh - 1], nx = row[0];
+    for (int cn = 0; cn < cneigh; ++cn) {
+        nx = row[cn];
+        if (c == target) break;
+        l = c;
+        c = nx;
+    }
+    vlast = l;
+    vcur = c;
+    vnext = nx;
+}
+
+// getCellVertexSetForT1 (src/models/vertexModelBase.cpp:507-625), without its unused first loop
+CG_D void t1_sets_d(const VertArgs &a, int v1, int v2, int cs[4], int vs[4])
+{
+    int c1 = a.vcn[3 * v1], c2 = a.vcn[3 * v1 + 1], c3 = a.vcn[3 * v1 + 2];
+    for (int f = 0; f < 3; ++f) {
+        int t = a.vcn[3 * v2 + f];
+        if (t != c1 && t != c2 && t != c3) cs[3] = t;
+    }
+    int cells[3] = {c1, c2, c3};
+    for (int q = 0; q < 3; ++q) {
+        int c = cells[q], l, cur, nx;
+        find_in_cell_d(a.cv + (size_t)c * a.vmax, a.cvn[c], v1, l, cur, nx);
+        if (l == v2) cs[0] = c;
+        else if (nx == v2) cs[2] = c;
+        else cs[1] = c;
+    }
+    int l, cur, nx;
+    find_in_cell_d(a.cv + (size_t)cs[1] * a.vmax, a.cvn[cs[1]], v1, l, cur, nx);
+    vs[0] = l;
+    vs[1] = nx;
+    find_in_cell_d(a.cv + (size_t)cs[3] * a.vmax, a.cvn[cs[3]], v2, l, cur, nx);
+    vs[3] = l;
+    vs[2] = nx;
+}
+
+CG_D void row_remove(int *row, int &n, int v)
+{
+    int cidx = 0;
+    for (int cc = 0; cc < n - 1; ++cc) {
+        if (row[cc] == v) cidx += 1;
+        row[cc] = row[cidx];
+        cidx += 1;
+    }
+    n -= 1;
+}
+
+// insert w right after v
+CG_D void row_insert_after(int *row, int &n, int v, int w)
+{
+    int k = 0;
+    while (k < n && row[k] != v) ++k;
+    for (int t = n; t > k + 1; --t) row[t] = row[t - 1];
+    row[k + 1] = w;
+    n += 1;
+}
+
+// insert key into the pending part q[head, n) of an ascending queue (no repeats)
+CG_D void queue_push(int *q, int head, int &n, int cap, int key, bool &overflow)
+{
+    int k = n;
+    while (k > head && q[k - 1] > key) --k;
+    if (k > head && q[k - 1] == key) return;
+    if (n >= cap) {
+        overflow = true;
+        return;
+    }
+    for (int t = n; t > k; --t) q[t] = q[t - 1];
+    q[k] = key;
+    ++n;
+}
+
+__global__ void k_vm_t1_replay(VertArgs a)
+{
+    int inst = blockIdx.x * blockDim.x + threadIdx.x;
+    if (inst >= a.n_inst) return;
+    Ctl *ctl = a.ctl;
+    if (ctl && ctl->halt) return;
+    int nc = a.cand_count[inst];
+    a.cand_count[inst] = 0;
+    if (nc == 0) return;
+    const Inst &in = a.inst[inst];
+    const int cap = 3 * in.nv;
+    int *q = a.cand + 3 * (size_t)in.voff;
+    // sort the detected keys (insertion sort: the list is short)
+    for (int i = 1; i < nc; ++i) {
+        int key = q[i], j = i - 1;
+        while (j >= 0 && q[j] > key) {
+            q[j + 1] = q[j];
+            --j;
+        }
+        q[j + 1] = key;
+    }
+    int head = 0, n = nc;
+    bool overflow = false;
+    int flips = 0;
+    while (head < n) {
+        int key = q[head++];
+        int vertex1 = key / 3, vv = key % 3;
+        int vertex2 = a.vn[3 * vertex1 + vv];
+        if (!(vertex1 < vertex2)) continue;
+        double2 v1 = a.vpos[vertex1], v2 = a.vpos[vertex2];
+        double2 e = min_dist(v1, v2, in.Lx, in.Ly);
+        if (!(__dsqrt_rn(__dadd_rn(__dmul_rn(e.x, e.x), __dmul_rn(e.y, e.y))) < a.t1)) continue;
+        int cs[4] = {0, 0, 0, 0}, vs[4] = {0, 0, 0, 0};
+        t1_sets_d(a, vertex1, vertex2, cs, vs);
+        if (a.cvn[cs[0]] == 3 || a.cvn[cs[2]] == 3) continue;
+        if (a.cvn[cs[1]] + 1 > a.vmax || a.cvn[cs[3]] + 1 > a.vmax) {
+            if (ctl) {
+                atomicExch(&ctl->status, CG_ERR_CAPACITY);
+                atomicExch(&ctl->halt, 1);
+            }
+            return;
+        }
+        // rotate the edge by 90 degrees about its midpoint
+        double2 mid = make_double2(__dadd_rn(v2.x, __dmul_rn(0.5, e.x)), __dadd_rn(v2.y, __dmul_rn(0.5, e.y)));
+        v1 = make_double2(__dsub_rn(mid.x, e.y), __dadd_rn(mid.y, e.x));
+        v2 = make_double2(__dadd_rn(mid.x, e.y), __dsub_rn(mid.y, e.x));
+        a.vpos[vertex1] = put_in_box(v1, in.Lx, in.Ly, in.iLx, in.iLy);
+        a.vpos[vertex2] = put_in_box(v2, in.Lx, in.Ly, in.iLx, in.iLy);
+        for (int vert = 0; vert < 3; ++vert) {
+            if (a.vcn[3 * vertex1 + vert] == cs[2]) a.vcn[3 * vertex1 + vert] = cs[3];
+            if (a.vcn[3 * vertex2 + vert] == cs[0]) a.vcn[3 * vertex2 + vert] = cs[1];
+            if (a.vn[3 * vs[1] + vert] == vertex1) a.vn[3 * vs[1] + vert] = vertex2;
+            if (a.vn[3 * vs[2] + vert] == vertex2) a.vn[3 * vs[2] + vert] = vertex1;
+            if (a.vn[3 * vertex1 + vert] == vs[1]) a.vn[3 * vertex1 + vert] = vs[2];
+            if (a.vn[3 * vertex2 + vert] == vs[2]) a.vn[3 * vertex2 + vert] = vs[1];
+        }
+        int *ri = a.cv + (size_t)cs[0] * a.vmax;
+        row_remove(ri, a.cvn[cs[0]], vertex2);
+        int *rj = a.cv + (size_t)cs[1] * a.vmax;
+        row_insert_after(rj, a.cvn[cs[1]], vertex1, vertex2);
+        int *rk = a.cv + (size_t)cs[2] * a.vmax;
+        row_remove(rk, a.cvn[cs[2]], vertex1);
+        int *rl = a.cv + (size_t)cs[3] * a.vmax;
+        row_insert_after(rl, a.cvn[cs[3]], vertex2, vertex1);
+        ++flips;
+        // edges that moved or were rewired, ahead of the sweep position
+        int touched[4] = {vertex1, vertex2, vs[1], vs[2]};
+        for (int t = 0; t < 4; ++t) {
+            int u = touched[t];
+            for (int s = 0; s < 3; ++s) {
+                int w = a.vn[3 * u + s];
+                int k2;
+                if (u < w) {
+                    k2 = 3 * u + s;
+                } else {
+                    int sw = 0;
+                    while (sw < 3 && a.vn[3 * w + sw] != u) ++sw;
+                    if (sw == 3) continue;
+                    k2 = 3 * w + sw;
+                }
+                if (k2 > key) queue_push(q, head, n, cap, k2, overflow);
+            }
+        }
+        if (overflow) break;
+    }
+    if (ctl) atomicAdd(&ctl->counters[5], (unsigned long long)flips);
+    if (overflow && ctl) {
+        atomicExch(&ctl->status, CG_ERR_CAPACITY);
+        atomicExch(&ctl->halt, 1);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// vertex model from a Delaunay triangulation (vertexModelBase::setCellsVoronoiTesselation,
+// src/models/vertexModelBase.cpp:115-229): one vertex per Delaunay triangle at its circumcentre.
+// Triangles are numbered with their smallest cell as owner, in cell order then slot order; cell
+// rows list their triangles counter-clockwise from (c, nbr[0], nbr[1]); vcn[3v+f] are the
+// triangle's cells (owner first, counter-clockwise) and vn[3v+f] the triangle across from cell f.
+// ------------------------------------------------------------------------------------------
+struct DualArgs {
+    int N, K, vmax;
+    const Inst *inst;
+    const int *cell_inst;
+    const double2 *pos;
+    const int *nn, *nbr;
+    int *owned, *tri;  // owned[N] counts -> exclusive offsets; tri[N*K]
+    double2 *vpos;
+    int *vn, *vcn, *cvn, *cv;
+    int *status;
+};
+
+__global__ void k_dual_count(DualArgs d)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.N) return;
+    int z = d.nn[c], cnt = 0;
+    for (int k = 0; k < z; ++k) {
+        int a = d.nbr[(size_t)c * d.K + k], b = d.nbr[(size_t)c * d.K + (k + 1) % z];
+        if (c < a && c < b) ++cnt;
+    }
+    d.owned[c] = cnt;
+}
+
+__global__ void k_dual_assign(DualArgs d)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.N) return;
+    int z = d.nn[c], id = d.owned[c];  // exclusive offset after the scan
+    for (int k = 0; k < z; ++k) {
+        int a = d.nbr[(size_t)c * d.K + k], b = d.nbr[(size_t)c * d.K + (k + 1) % z];
+        d.tri[(size_t)c * d.K + k] = (c < a && c < b) ? id++ : -1;
+    }
+}
+
+CG_D int row_slot(const int *row, int z, int v)
+{
+    for (int k = 0; k < z; ++k)
+        if (row[k] == v) return k;
+    return -1;
+}
+
+__global__ void k_dual_resolve(DualArgs d)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.N) return;
+    int z = d.nn[c];
+    if (z > d.vmax) {
+        atomicCAS(d.status, 0, CG_ERR_CAPACITY);
+        return;
+    }
+    for (int k = 0; k < z; ++k) {
+        int t = d.tri[(size_t)c * d.K + k];
+        if (t < 0) {
+            int a = d.nbr[(size_t)c * d.K + k], b = d.nbr[(size_t)c * d.K + (k + 1) % z];
+            int o = a < b ? a : b, nxt = (o == a) ? b : c;
+            int s = row_slot(d.nbr + (size_t)o * d.K, d.nn[o], nxt);
+            if (s < 0) {
+                atomicCAS(d.status, 0, CG_ERR_TOPOLOGY);
+                return;
+            }
+            // the owner's entry is written by k_dual_assign only, so it is final here
+            t = d.tri[(size_t)o * d.K + s];
+        }
+        d.cv[(size_t)c * d.vmax + k] = t;
+    }
+    d.cvn[c] = z;
+}
+
+__global__ void k_dual_vertices(DualArgs d)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.N) return;
+    const Inst &in = d.inst[d.cell_inst[c]];
+    int z = d.nn[c];
+    for (int k = 0; k < z; ++k) {
+        int a = d.nbr[(size_t)c * d.K + k], b = d.nbr[(size_t)c * d.K + (k + 1) % z];
+        if (!(c < a && c < b)) continue;
+        int v = d.tri[(size_t)c * d.K + k];
+        double2 ra = min_dist(d.pos[a], d.pos[c], in.Lx, in.Ly), rb = min_dist(d.pos[b], d.pos[c], in.Lx, in.Ly);
+        double an = ra.x * ra.x + ra.y * ra.y, bn = rb.x * rb.x + rb.y * rb.y;
+        double den = 0.5 / (ra.x * rb.y - ra.y * rb.x);
+        double2 q = make_double2(d.pos[c].x + den * (an * rb.y - ra.y * bn), d.pos[c].y + den * (ra.x * bn - an * rb.x));
+        d.vpos[v] = put_in_box(q, in.Lx, in.Ly, in.iLx, in.iLy);
+        int cells[3] = {c, a, b};
+        for (int f = 0; f < 3; ++f) {
+            d.vcn[3 * v + f] = cells[f];
+            int qc = cells[(f + 1) % 3], rc = cells[(f + 2) % 3];
+            int s = row_slot(d.nbr + (size_t)qc * d.K, d.nn[qc], rc);
+            int zq = d.nn[qc];
+            d.vn[3 * v + f] = d.cv[(size_t)qc * d.vmax + (s + zq - 1) % zq];
+        }
+    }
+}
+
+}  // namespace cg

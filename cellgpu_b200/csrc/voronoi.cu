@@ -140,9 +140,9 @@ CG_D int cell_pass(const VoroArgs &a, int c, const int *row, int z, double2 pc, 
     int nA = row[z - 1], nB = row[0];
     double2 dA = min_dist(pos[nA], pc, Lx, Ly);
     double2 dB = min_dist(pos[nB], pc, Lx, Ly);
-    V hprev = circum0<R>(cvt<R>(dA), cvt<R>(dB));  // h_0
-    V hfirst = hprev;
-    R Asum = 0, Psum = 0;
+    double2 hprev = circum0<double>(dA, dB);  // h_0 (vertex geometry and sums in FP64)
+    double2 hfirst = hprev;
+    double Asum = 0, Psum = 0;
     for (int k = 0; k < z; ++k) {
         int kn = (k + 1 == z) ? 0 : k + 1;
         int nC = row[kn];
@@ -151,30 +151,30 @@ CG_D int cell_pass(const VoroArgs &a, int c, const int *row, int z, double2 pc, 
             if (orient0(dB, dC) <= 0) fail = -(k + 1);
             else if (c < nB && incircle0(dA, dB, dC) < 0) fail = k + 1;
         }
-        V hnext = (kn == 0) ? hfirst : circum0<R>(cvt<R>(dB), cvt<R>(dC));
-        Asum += fabs(R(0.5) * (hprev.x * hnext.y - hprev.y * hnext.x));
-        R dx = hprev.x - hnext.x, dy = hprev.y - hnext.y;
+        double2 hnext = (kn == 0) ? hfirst : circum0<double>(dB, dC);
+        Asum += fabs(0.5 * (hprev.x * hnext.y - hprev.y * hnext.x));
+        double dx = hprev.x - hnext.x, dy = hprev.y - hnext.y;
         Psum += sqrt(dx * dx + dy * dy);
         hprev = hnext;
         dA = dB;
         dB = dC;
         nB = nC;
     }
-    A_out = Asum;
-    P_out = Psum;
+    A_out = (R)Asum;
+    P_out = (R)Psum;
 
     if (SCATTER) {
         const R thr = R(1e-18);
-        R Adiff = R(a.KA) * (Asum - (R)a.APpref[c].x);
-        R Pdiff = R(a.KP) * (Psum - (R)a.APpref[c].y);
+        R Adiff = (R)(a.KA * (Asum - a.APpref[c].x));
+        R Pdiff = (R)(a.KP * (Psum - a.APpref[c].y));
         // window: r_{k-1} = rA, r_k = rB, r_{k+1} = rC ; h_{k-1} = hP, h_k = hC, h_{k+1} = hN
-        V rZ = cvt<R>(min_dist(pos[row[z - 2]], pc, Lx, Ly));
-        V rA = cvt<R>(min_dist(pos[row[z - 1]], pc, Lx, Ly));
-        V rB = cvt<R>(min_dist(pos[row[0]], pc, Lx, Ly));
-        V rC = cvt<R>(min_dist(pos[row[1]], pc, Lx, Ly));
-        V hP = circum0<R>(rZ, rA);
-        V hC = circum0<R>(rA, rB);
-        V hN = circum0<R>(rB, rC);
+        double2 rZ = min_dist(pos[row[z - 2]], pc, Lx, Ly);
+        double2 rA = min_dist(pos[row[z - 1]], pc, Lx, Ly);
+        double2 rB = min_dist(pos[row[0]], pc, Lx, Ly);
+        double2 rC = min_dist(pos[row[1]], pc, Lx, Ly);
+        V hP = cvt<R>(circum0<double>(rZ, rA));
+        V hC = cvt<R>(circum0<double>(rA, rB));
+        V hN = cvt<R>(circum0<double>(rB, rC));
         R sx = 0, sy = 0;          // self
         R pendx = 0, pendy = 0;    // slot k (b part), waiting for the a part of vertex k+1
         R fax = 0, fay = 0;        // a part of vertex 0, belongs to slot z-1
@@ -193,17 +193,20 @@ CG_D int cell_pass(const VoroArgs &a, int c, const int *row, int z, double2 pc, 
                 dPy = ly / ln + ny / nnm;
             } else {
                 // exact tangent directions of the edges dual to r_{k-1} and r_k (see k_voro_groups)
-                R ia = R(1) / sqrt(rA.x * rA.x + rA.y * rA.y), ib = R(1) / sqrt(rB.x * rB.x + rB.y * rB.y);
-                dPx = -rA.y * ia + rB.y * ib;
-                dPy = rA.x * ia - rB.x * ib;
+                V fa = cvt<R>(rA), fb = cvt<R>(rB);
+                R ia = R(1) / sqrt(fa.x * fa.x + fa.y * fa.y), ib = R(1) / sqrt(fb.x * fb.x + fb.y * fb.y);
+                dPx = -fa.y * ia + fb.y * ib;
+                dPy = fa.x * ia - fb.x * ib;
             }
             R gx = -R(2) * (Adiff * dAx + Pdiff * dPx);
             R gy = -R(2) * (Adiff * dAy + Pdiff * dPy);
-            // Jacobians of h_k
-            R c11, c12, c21, c22, a11, a12, a21, a22;
-            dhdr<R>(rA, rB, c11, c12, c21, c22);
-            dhdr<R>(mk<R>(-rA.x, -rA.y), mk<R>(rB.x - rA.x, rB.y - rA.y), a11, a12, a21, a22);
-            R b11 = R(1) - c11 - a11, b12 = -c12 - a12, b21 = -c21 - a21, b22 = R(1) - c22 - a22;
+            // Jacobians of h_k (FP64, see k_voro_groups)
+            double d11, d12, d21, d22, e11, e12, e21, e22;
+            dhdr<double>(rA, rB, d11, d12, d21, d22);
+            dhdr<double>(make_double2(-rA.x, -rA.y), make_double2(rB.x - rA.x, rB.y - rA.y), e11, e12, e21, e22);
+            R c11 = (R)d11, c12 = (R)d12, c21 = (R)d21, c22 = (R)d22;
+            R a11 = (R)e11, a12 = (R)e12, a21 = (R)e21, a22 = (R)e22;
+            R b11 = (R)(1.0 - d11 - e11), b12 = (R)(-d12 - e12), b21 = (R)(-d21 - e21), b22 = (R)(1.0 - d22 - e22);
             sx += gx * c11 + gy * c21;
             sy += gx * c12 + gy * c22;
             R cax = gx * a11 + gy * a21, cay = gx * a12 + gy * a22;
@@ -224,8 +227,8 @@ CG_D int cell_pass(const VoroArgs &a, int c, const int *row, int z, double2 pc, 
                 hC = hN;
                 rA = rB;
                 rB = rC;
-                rC = cvt<R>(min_dist(pos[row[k2]], pc, Lx, Ly));
-                hN = circum0<R>(rB, rC);
+                rC = min_dist(pos[row[k2]], pc, Lx, Ly);
+                hN = cvt<R>(circum0<double>(rB, rC));
             }
         }
         atomic_add2<R>(a.F, row[z - 1], sign * (pendx + fax), sign * (pendy + fay));
@@ -319,7 +322,7 @@ __global__ void __launch_bounds__(WPB * 32) k_voro_groups(VoroArgs a)
 {
     using V = typename Vec2<R>::T;
     __shared__ double2 sR[WPB * GPW][VG];
-    __shared__ V sH[WPB * GPW][VG];
+    __shared__ double2 sH[WPB * GPW][VG];  // Voronoi vertices, FP64 in both modes
     __shared__ V sU[WPB * GPW][VG];
     __shared__ V sCA[WPB * GPW][VG];
     __shared__ V sCB[WPB * GPW][VG];
@@ -361,7 +364,8 @@ __global__ void __launch_bounds__(WPB * 32) k_voro_groups(VoroArgs a)
         if (ok && k < z) {
             int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
             double2 ra = sR[sl][km], rb = sR[sl][k];
-            sH[sl][k] = circum0<R>(cvt<R>(ra), cvt<R>(rb));
+            // Voronoi vertices are ill-conditioned (skinny triangles): always formed in FP64
+            sH[sl][k] = circum0<double>(ra, rb);
             if (TEST) {
                 double2 rc = sR[sl][kp];
                 if (orient0(rb, rc) <= 0) fail = min(fail, 2 * k + 1);
@@ -370,23 +374,24 @@ __global__ void __launch_bounds__(WPB * 32) k_voro_groups(VoroArgs a)
         }
     }
     __syncwarp();
-    // phase C: edges h_k -> h_{k+1}: area, perimeter, unit tangents
-    R Ap = 0, Pp = 0;
+    // phase C: edges h_k -> h_{k+1}: area, perimeter (FP64 sums in both modes: A - A0 and P - P0
+    // are small differences), unit tangents
+    double Ap = 0, Pp = 0;
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
         int k = gl + G * r;
         if (ok && k < z) {
             int kp = k + 1 == z ? 0 : k + 1;
-            V h0 = sH[sl][k], h1 = sH[sl][kp];
-            R dx = h1.x - h0.x, dy = h1.y - h0.y;
-            R len = sqrt(dx * dx + dy * dy);
-            Ap += fabs(R(0.5) * (h0.x * h1.y - h0.y * h1.x));
+            double2 h0 = sH[sl][k], h1 = sH[sl][kp];
+            double dx = h1.x - h0.x, dy = h1.y - h0.y;
+            double len = sqrt(dx * dx + dy * dy);
+            Ap += fabs(0.5 * (h0.x * h1.y - h0.y * h1.x));
             Pp += len;
             if (SCATTER) {
                 V u;
                 if (sizeof(R) == sizeof(double)) {
-                    R l = len < R(1e-18) ? R(1e-18) : len;
-                    u = mk<R>(dx / l, dy / l);
+                    double l = len < 1e-18 ? 1e-18 : len;
+                    u = mk<R>((R)(dx / l), (R)(dy / l));
                 } else {
                     V rk = cvt<R>(sR[sl][k]);
                     R il = R(1) / sqrt(rk.x * rk.x + rk.y * rk.y);
@@ -396,15 +401,20 @@ __global__ void __launch_bounds__(WPB * 32) k_voro_groups(VoroArgs a)
             }
         }
     }
-    R A = group_sum<R>(Ap), P = group_sum<R>(Pp);
+    double A = group_sum<double>(Ap), P = group_sum<double>(Pp);
     if (TEST) fail = group_min(fail);
-    if (ok && gl == 0 && a.AP) store_ap<R>(a.AP, c, A, P);
-    if (SCATTER) {
+    if (ok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
+    // A cell whose own row fails the test holds its contributions back: the row is about to be
+    // replaced, and a stale row can contain a nearly collinear triangle whose Jacobians (1/cross^2)
+    // would swamp the forces. The repair commit adds the contributions of the new row.
+    bool hold = SCATTER && TEST && a.held && ok && fail != 0x7fffffff;
+    if (hold && gl == 0) a.held[c] = 1;
+    if (SCATTER && !hold) {
         __syncwarp();
         R Adiff = 0, Pdiff = 0;
         if (ok) {
-            Adiff = R(a.KA) * (A - (R)a.APpref[c].x);
-            Pdiff = R(a.KP) * (P - (R)a.APpref[c].y);
+            Adiff = (R)(a.KA * (A - a.APpref[c].x));
+            Pdiff = (R)(a.KP * (P - a.APpref[c].y));
         }
         R sx = 0, sy = 0;
 #pragma unroll
@@ -412,27 +422,31 @@ __global__ void __launch_bounds__(WPB * 32) k_voro_groups(VoroArgs a)
             int k = gl + G * r;
             if (ok && k < z) {
                 int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
-                V hm = sH[sl][km], hp = sH[sl][kp];
+                V hm = cvt<R>(sH[sl][km]), hp = cvt<R>(sH[sl][kp]);
                 V um = sU[sl][km], uk = sU[sl][k];
                 R dAx = R(0.5) * (hp.y - hm.y), dAy = R(0.5) * (hm.x - hp.x);
                 R dPx = um.x - uk.x, dPy = um.y - uk.y;
                 R gx = -R(2) * (Adiff * dAx + Pdiff * dPx);
                 R gy = -R(2) * (Adiff * dAy + Pdiff * dPy);
-                V ra = cvt<R>(sR[sl][km]), rb = cvt<R>(sR[sl][k]);
-                // shared denominator: |ra x rb|^2 (the same for dh/dr_c and dh/dr_a)
-                R cr = ra.y * rb.x - ra.x * rb.y;
-                R half_inv = R(0.5) / (cr * cr);
-                R ra2 = ra.x * ra.x + ra.y * ra.y, rb2 = rb.x * rb.x + rb.y * rb.y;
-                R t1 = rb.y * ra2 - ra.y * rb2, t2 = rb.x * ra2 - ra.x * rb2;
-                R c11 = half_inv * (rb.y - ra.y) * t1, c12 = half_inv * (ra.y - rb.y) * t2;
-                R c21 = half_inv * (ra.x - rb.x) * t1, c22 = half_inv * (rb.x - ra.x) * t2;
+                // Jacobians of h_k (always FP64: their entries scale as 1/|ra x rb|^2), with the
+                // shared denominator |ra x rb|^2 for dh/dr_c and dh/dr_a
+                double2 ra = sR[sl][km], rb = sR[sl][k];
+                double cr = ra.y * rb.x - ra.x * rb.y;
+                double half_inv = 0.5 / (cr * cr);
+                double ra2 = ra.x * ra.x + ra.y * ra.y, rb2 = rb.x * rb.x + rb.y * rb.y;
+                double t1 = rb.y * ra2 - ra.y * rb2, t2 = rb.x * ra2 - ra.x * rb2;
+                double d11 = half_inv * (rb.y - ra.y) * t1, d12 = half_inv * (ra.y - rb.y) * t2;
+                double d21 = half_inv * (ra.x - rb.x) * t1, d22 = half_inv * (rb.x - ra.x) * t2;
                 // dh/dr_a = getdhdr(-ra, rb-ra)
-                V p = mk<R>(-ra.x, -ra.y), q = mk<R>(rb.x - ra.x, rb.y - ra.y);
-                R p2 = ra2, q2 = q.x * q.x + q.y * q.y;
-                R u1 = q.y * p2 - p.y * q2, u2 = q.x * p2 - p.x * q2;
-                R a11 = half_inv * (q.y - p.y) * u1, a12 = half_inv * (p.y - q.y) * u2;
-                R a21 = half_inv * (p.x - q.x) * u1, a22 = half_inv * (q.x - p.x) * u2;
-                R b11 = R(1) - c11 - a11, b12 = -c12 - a12, b21 = -c21 - a21, b22 = R(1) - c22 - a22;
+                double2 p = make_double2(-ra.x, -ra.y), q = make_double2(rb.x - ra.x, rb.y - ra.y);
+                double q2 = q.x * q.x + q.y * q.y;
+                double u1 = q.y * ra2 - p.y * q2, u2 = q.x * ra2 - p.x * q2;
+                double e11 = half_inv * (q.y - p.y) * u1, e12 = half_inv * (p.y - q.y) * u2;
+                double e21 = half_inv * (p.x - q.x) * u1, e22 = half_inv * (q.x - p.x) * u2;
+                R c11 = (R)d11, c12 = (R)d12, c21 = (R)d21, c22 = (R)d22;
+                R a11 = (R)e11, a12 = (R)e12, a21 = (R)e21, a22 = (R)e22;
+                R b11 = (R)(1.0 - d11 - e11), b12 = (R)(-d12 - e12), b21 = (R)(-d21 - e21),
+                  b22 = (R)(1.0 - d22 - e22);
                 sx += gx * c11 + gy * c21;
                 sy += gx * c12 + gy * c22;
                 sCA[sl][k] = mk<R>(gx * a11 + gy * a21, gx * a12 + gy * a22);
@@ -740,7 +754,14 @@ __global__ void k_commit(VoroArgs a)
         bool same = (zo == zn);
         for (int k = 0; same && k < zn; ++k) same = (row[k] == srow[k]);
         if (same) {
-            // unchanged rows are still checked against their partners
+            // unchanged rows are still checked against their partners; held contributions are added
+            if (FORCES && a.held && a.held[c]) {
+                const Inst &in0 = inst_of(a, c);
+                R A0, P0;
+                cell_pass<R, true, false>(a, c, row, zo, a.pos[c], in0.Lx, in0.Ly, R(1), A0, P0);
+                if (a.AP) store_ap<R>(a.AP, c, A0, P0);
+            }
+            if (a.held) a.held[c] = 0;
             a.stage_nn[q] = -1;
             int slot = atomicAdd(&ctl->n_changed[round], 1);
             a.changed[(size_t)round * a.N + slot] = q;
@@ -749,7 +770,9 @@ __global__ void k_commit(VoroArgs a)
         const Inst &in = inst_of(a, c);
         double2 pc = a.pos[c];
         R A, P;
-        if (FORCES) cell_pass<R, true, false>(a, c, row, zo, pc, in.Lx, in.Ly, R(-1), A, P);
+        bool was_held = a.held && a.held[c];
+        if (a.held) a.held[c] = 0;
+        if (FORCES && !was_held) cell_pass<R, true, false>(a, c, row, zo, pc, in.Lx, in.Ly, R(-1), A, P);
         // swap rows
         for (int k = 0; k < a.K; ++k) {
             int t = (k < zn) ? srow[k] : -1;

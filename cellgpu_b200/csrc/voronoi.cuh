@@ -46,6 +46,7 @@ struct VoroArgs {
     int *stage_nn;  // N
     int *stage_nbr; // N * K
     int *changed;   // R_MAX * N  (queue slots whose rows changed)
+    int *held;      // N: 1 while a cell's contributions are held back (its own row failed the test)
     Ctl *ctl;
     // cell list
     int *bin_count, *bin_start, *bin_cells, *cell_bin, *cell_slot;

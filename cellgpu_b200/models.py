@@ -17,7 +17,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import CG_FP64, CG_MIXED, check, load, ptr
+from ._lib import CG_FP64, CG_MIXED, FireParams, check, load, ptr
 
 
 def _f64(a, shape):
@@ -147,6 +147,81 @@ class VoronoiBatch:
     def device_bytes(self):
         return int(self._lib.cg_device_bytes(self._h))
 
+    # -- FIRE
+    def fire_minimize(self, params=None, **kw):
+        p = params if params is not None else FireParams.defaults(**kw)
+        check(self._lib.cg_fire_minimize(self._h, C.byref(p)))
+
+    def fire_state(self):
+        n = len(self.N)
+        it = np.zeros(n, np.int32)
+        fm = np.zeros(n)
+        fn = np.zeros(n)
+        check(self._lib.cg_fire_state(self._h, ptr(it), ptr(fm), ptr(fn)))
+        return it, fm, fn
+
+
+class VertexBatch(VoronoiBatch):
+    """A device-resident batch of vertex-model monolayers: Nc[i] cells, 2 Nc[i] vertices each."""
+
+    def __init__(self, Nc, boxes, vmax=30, precision=CG_FP64):
+        self._lib = load()
+        self.N = [int(n) for n in Nc]
+        self.boxes = np.asarray(boxes, dtype=np.float64).reshape(len(self.N), 2)
+        self.K = self.vmax = int(vmax)
+        self.precision = precision
+        h = C.c_void_p()
+        n_arr = np.asarray(self.N, dtype=np.int32)
+        check(self._lib.cg_vertex_create(len(self.N), ptr(n_arr), ptr(np.ascontiguousarray(self.boxes)),
+                                         self.vmax, precision, C.byref(h)))
+        self._h = h
+        self.Ntot = sum(self.N)
+        self.Nv = 2 * self.Ntot
+        self.offsets = np.concatenate([[0], np.cumsum(self.N)]).astype(np.int64)
+
+    def from_cells(self, cell_pos):
+        p = _f64(cell_pos, (self.Ntot, 2))
+        check(self._lib.cg_vertex_from_voronoi(self._h, ptr(p)))
+
+    def set_positions(self, vpos):
+        p = _f64(vpos, (self.Nv, 2))
+        check(self._lib.cg_set_positions(self._h, ptr(p)))
+
+    def positions(self):
+        out = np.zeros((self.Nv, 2))
+        check(self._lib.cg_get_positions(self._h, ptr(out)))
+        return out
+
+    def forces(self):
+        out = np.zeros((self.Nv, 2))
+        check(self._lib.cg_get_forces(self._h, ptr(out)))
+        return out
+
+    def vertex_topology(self):
+        vn = np.zeros(3 * self.Nv, np.int32)
+        vcn = np.zeros(3 * self.Nv, np.int32)
+        cvn = np.zeros(self.Ntot, np.int32)
+        cv = np.zeros((self.Ntot, self.vmax), np.int32)
+        check(self._lib.cg_get_vertex_topology(self._h, ptr(vn), ptr(vcn), ptr(cvn), ptr(cv)))
+        return vn, vcn, cvn, cv
+
+    def set_vertex_topology(self, vn, vcn, cvn, cv):
+        vn = np.ascontiguousarray(vn, np.int32)
+        vcn = np.ascontiguousarray(vcn, np.int32)
+        cvn = np.ascontiguousarray(cvn, np.int32)
+        cv = np.ascontiguousarray(cv, np.int32).reshape(self.Ntot, self.vmax)
+        check(self._lib.cg_set_vertex_topology(self._h, ptr(vn), ptr(vcn), ptr(cvn), ptr(cv)))
+
+    def set_t1_threshold(self, t):
+        check(self._lib.cg_set_t1_threshold(self._h, float(t)))
+
+    def brownian_run(self, n_steps, dt=0.005, mu=1.0, T=1e-3, noise=None):
+        """noise: optional device tensor with n_steps*2*Nv normals (x then y per vertex)."""
+        check(self._lib.cg_brownian_run(self._h, int(n_steps), float(dt), float(mu), float(T), ptr(noise)))
+
+    def spp_run(self, n_steps, dt=0.01, mu=1.0, noise=None):
+        check(self._lib.cg_vertex_spp_run(self._h, int(n_steps), float(dt), float(mu), ptr(noise)))
+
 
 def random_positions(N, box, seed):
     """Seeded uniform positions in [0,Lx)x[0,Ly), x then y per cell like
@@ -264,6 +339,132 @@ class selfPropelledParticleDynamics:
     def integrateEquationsOfMotion(self, n_steps=1):
         self.model.batch.spp_run(n_steps, self.deltaT, self.mu, self.noise)
         self.model.forcesUpToDate = False
+
+
+class VertexQuadraticEnergy:
+    """Vertex (AVM) model (inc/models/vertexQuadraticEnergy.h; src/models/vertexQuadraticEnergy.cpp:18-24):
+    cells from seeded random points, vertices from their Delaunay dual."""
+
+    def __init__(self, n, A0=1.0, P0=3.8, reprod=False, seed=None, vmax=30, box=None):
+        L = float(np.sqrt(n))
+        self.box = (L, L) if box is None else tuple(box)
+        self.Ncells = int(n)
+        if seed is None:
+            seed = 13377 if reprod else int(np.random.SeedSequence().entropy % (2**31))
+        self.seed = seed
+        self.batch = VertexBatch([n], [self.box], vmax=vmax)
+        self.batch.set_seed(seed)
+        self.batch.from_cells(random_positions(n, self.box, seed))
+        rng = np.random.default_rng(seed + 1)
+        self.batch.set_directors(rng.uniform(0, 2 * np.pi, n))
+        self.setCellPreferencesUniform(A0, P0)
+        self.setT1Threshold(0.01)
+
+    def getNumberOfDegreesOfFreedom(self):
+        return self.batch.Nv
+
+    def setCellPreferencesUniform(self, A0, P0):
+        self.batch.set_preferences(np.tile([A0, P0], (self.Ncells, 1)))
+
+    def setCellPreferences(self, APpref):
+        self.batch.set_preferences(APpref)
+
+    def setModuliUniform(self, KA, KP):
+        self.batch.set_moduli(KA, KP)
+
+    def setT1Threshold(self, t):
+        self.batch.set_t1_threshold(t)
+
+    def setv0Dr(self, v0, Dr):
+        self.batch.set_motility(np.tile([v0, Dr], (self.Ncells, 1)))
+
+    def computeForces(self):
+        self.batch.compute_forces()
+
+    def returnForces(self):
+        return self.batch.forces()
+
+    def returnPositions(self):
+        return self.batch.positions()
+
+    def computeEnergy(self):
+        self.batch.compute_forces()
+        return float(self.batch.energies()[0])
+
+    def enforceTopology(self):
+        self.batch.enforce_topology()
+
+
+class brownianParticleDynamics:
+    """Brownian dynamics (src/updaters/brownianParticleDynamics.cpp:46-109), vertex model."""
+
+    def __init__(self, n=None):
+        self.deltaT, self.mu, self.T = 0.01, 1.0, 0.0
+        self.model = None
+
+    def setDeltaT(self, dt):
+        self.deltaT = dt
+
+    def setMu(self, mu):
+        self.mu = mu
+
+    def setT(self, T):
+        self.T = T
+
+    def set2DModel(self, model):
+        self.model = model
+
+    def integrateEquationsOfMotion(self, n_steps=1):
+        self.model.batch.brownian_run(n_steps, self.deltaT, self.mu, self.T)
+
+
+class selfPropelledCellVertexDynamics(selfPropelledParticleDynamics):
+    """SPP of the vertex model (src/updaters/selfPropelledCellVertexDynamics.cpp:28-122)."""
+
+
+class EnergyMinimizerFIRE:
+    """FIRE minimiser (src/updaters/EnergyMinimizerFIRE2D.cpp), CPU conventions, on the GPU."""
+
+    def __init__(self, model=None):
+        self.model = model
+        self.params = FireParams.defaults()
+
+    def set2DModel(self, model):
+        self.model = model
+
+    def setMaximumIterations(self, n):
+        self.params.max_iterations = int(n)
+
+    def setForceCutoff(self, fc):
+        self.params.force_cutoff = fc
+
+    def setDeltaT(self, dt):
+        self.params.dt = dt
+        self.params.dt_min = 0.01 * dt
+
+    def setAlphaStart(self, a):
+        self.params.alpha_start = a
+
+    def setDeltaTMax(self, t):
+        self.params.dt_max = t
+
+    def setDeltaTInc(self, t):
+        self.params.dt_inc = t
+
+    def setDeltaTDec(self, t):
+        self.params.dt_dec = t
+
+    def setAlphaDec(self, a):
+        self.params.alpha_dec = a
+
+    def setNMin(self, n):
+        self.params.n_min = int(n)
+
+    def minimize(self):
+        self.model.batch.fire_minimize(self.params)
+
+    def integrateEquationsOfMotion(self, n_steps=1):
+        self.minimize()
 
 
 class Simulation:

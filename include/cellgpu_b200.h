@@ -125,6 +125,12 @@ typedef struct cg_system cg_system;
  * precision: CG_FP64 or CG_MIXED. */
 int cg_voronoi_create(int n_inst, const int *N, const double *box, int K, int precision,
                       cg_system **out);
+/* Vertex model batch: n_inst monolayers with Nc[i] cells and Nv[i] = 2*Nc[i] three-valent vertices;
+ * vmax is the vertex-row capacity per cell (the reference fixes 30,
+ * src/models/vertexModelBase.cpp:209-210). FP64 only. Initialise with cg_vertex_from_voronoi or
+ * cg_set_positions + cg_set_vertex_topology. */
+int cg_vertex_create(int n_inst, const int *Nc, const double *box, int vmax, int precision,
+                     cg_system **out);
 int cg_destroy(cg_system *sys);
 
 /* sizes and footprint */
@@ -135,6 +141,7 @@ int cg_neighbor_capacity(const cg_system *sys);
 size_t cg_device_bytes(const cg_system *sys);
 /* bytes a system of this shape would hold on the device (admission control) */
 size_t cg_voronoi_footprint(int n_inst, const int *N, int K);
+size_t cg_vertex_footprint(int n_inst, const int *Nc, int vmax);
 
 /* host <-> device state (host buffers; copies are ordered on the system's stream and complete
  * before return for get_*) */
@@ -149,6 +156,11 @@ int cg_get_forces(cg_system *sys, double *F);                 /* per dof */
 int cg_get_area_perimeter(cg_system *sys, double *AP);        /* per cell */
 int cg_get_topology(cg_system *sys, int *nn, int *nbr);       /* Voronoi rows (N x K) */
 int cg_set_topology(cg_system *sys, const int *nn, const int *nbr);
+/* vertex model wiring (vertexModelBase arrays, inc/models/Simple2DCell.h:160-290): vn[3*Nv] vertex
+ * neighbours, vcn[3*Nv] cells of each vertex, cvn[Nc] vertices per cell, cv[Nc*vmax] cell vertices
+ * counter-clockwise */
+int cg_get_vertex_topology(cg_system *sys, int *vn, int *vcn, int *cvn, int *cv);
+int cg_set_vertex_topology(cg_system *sys, const int *vn, const int *vcn, const int *cvn, const int *cv);
 /* per-instance energies E = sum KA (A-A0)^2 + KP (P-P0)^2 (computeEnergy,
  * src/models/voronoiQuadraticEnergy.cpp:384-397), accumulated in FP64 */
 int cg_get_energies(cg_system *sys, double *E);
@@ -160,6 +172,10 @@ int cg_synchronize(cg_system *sys);
 
 /* topology and forces */
 int cg_triangulate(cg_system *sys);       /* full Delaunay triangulation (Voronoi) */
+/* vertex model from the Delaunay triangulation of cell positions (Nc points, (x,y) pairs): one
+ * vertex per Delaunay triangle at its circumcentre (vertexModelBase::setCellsVoronoiTesselation,
+ * src/models/vertexModelBase.cpp:115-229) */
+int cg_vertex_from_voronoi(cg_system *vertex_sys, const double *cell_pos);
 int cg_compute_forces(cg_system *sys);    /* forces on the current topology, geometry included */
 int cg_enforce_topology(cg_system *sys);  /* Voronoi: test+repair; vertex: T1 sweep */
 
@@ -181,6 +197,32 @@ int cg_launch_force_pass(cg_system *sys, int with_test);
 /* number of this library's kernels launched for the system so far, graph replays and the repair
  * rounds run inside graph conditional nodes included (synchronises the system's stream) */
 long long cg_kernels_launched(cg_system *sys);
+
+/* Brownian dynamics of the vertex model (brownianParticleDynamics, src/updaters/
+ * brownianParticleDynamics.cpp:92-109): two normals per vertex and step (x then y); noise_dev holds
+ * n_steps*2*Nv normals or is NULL for the counter-based RNG. Each step: forces, integrate + move,
+ * T1 sweep. */
+int cg_brownian_run(cg_system *sys, int n_steps, double dt, double mu, double T, const double *noise_dev);
+/* self-propelled vertex model (selfPropelledCellVertexDynamics, src/updaters/
+ * selfPropelledCellVertexDynamics.cpp:81-122): noise_dev holds n_steps*Nc normals or NULL */
+int cg_vertex_spp_run(cg_system *sys, int n_steps, double dt, double mu, const double *noise_dev);
+/* T1 edge-length threshold (vertexModelBase::setT1Threshold; default 0.01) */
+int cg_set_t1_threshold(cg_system *sys, double threshold);
+
+/* FIRE minimisation (EnergyMinimizerFIRE::minimize, src/updaters/EnergyMinimizerFIRE2D.cpp:269-284)
+ * with the CPU conventions of the reference (forceMax = max |F|^2; dt >= dt_min), every instance
+ * independently (its own dt, alpha, counters). Each call starts a fresh minimisation (zero
+ * velocities, dt, alpha_start). Defaults of the reference (:24-41): dt 0.01, dt_max 0.1,
+ * dt_min 0.01*dt, dt_inc 1.05, dt_dec 0.95, alpha_start 0.99, alpha_dec 0.9, n_min 5,
+ * force_cutoff 1e-7, max_iterations 1000. */
+typedef struct {
+    double dt, dt_max, dt_min, dt_inc, dt_dec, alpha_start, alpha_dec, force_cutoff;
+    int n_min, max_iterations;
+} cg_fire_params;
+int cg_fire_minimize(cg_system *sys, const cg_fire_params *prm);
+/* per instance: iterations, sqrt(max |F|^2) (CPU convention) and sqrt(mean |F|^2) (the reference's
+ * GPU convention, src/updaters/EnergyMinimizerFIRE2D.cpp:184) of the last iteration */
+int cg_fire_state(cg_system *sys, int *iterations, double *fmax_cpu, double *fnorm_gpu);
 
 /* counters: topology repairs, global retriangulations, T1 flips, fallbacks (per system) */
 int cg_counters(cg_system *sys, long long *out, int n);

@@ -1030,3 +1030,48 @@ int cgo_fire_vertex(int Nc, int Nv, double *vpos, const double *box, int vmax, i
     free(s.AP);
     return st;
 }
+
+/* selfPropelledCellVertexDynamics::integrateEquationsOfMotionCPU
+ * (src/updaters/selfPropelledCellVertexDynamics.cpp:81-122): vertex displacement from the mean of
+ * its three cells' v0 (cos th, sin th) plus mu F, then the cells' directors advance by
+ * xi sqrt(2 dt Dr) (one normal per cell, in index order); then move and T1 sweep. */
+int cgo_vertex_spp_run(int Nc, int Nv, double *vpos, const double *box, int vmax, int *vn, int *vcn,
+                       int *cvn, int *cv, const double *APpref, double KA, double KP, double *theta,
+                       const double *motility, double dt, double mu, double t1_threshold, int n_steps,
+                       const double *noise)
+{
+    double *AP = (double *)malloc(sizeof(double) * 2 * Nc);
+    double *F = (double *)malloc(sizeof(double) * 2 * Nv);
+    double *disp = (double *)malloc(sizeof(double) * 2 * Nv);
+    int st = 0;
+    for (int s = 0; s < n_steps; ++s) {
+        cgo_vertex_geometry(Nc, vpos, box, vmax, cvn, cv, AP);
+        cgo_vertex_forces(Nc, Nv, vpos, box, vmax, cvn, cv, vcn, AP, APpref, KA, KP, F);
+        for (int i = 0; i < Nv; ++i) {
+            int c0 = vcn[3 * i], c1 = vcn[3 * i + 1], c2 = vcn[3 * i + 2];
+            double v1 = motility[2 * c0], v2 = motility[2 * c1], v3 = motility[2 * c2];
+            double dx = v1 * cos(theta[c0]);
+            dx += v2 * cos(theta[c1]);
+            dx += v3 * cos(theta[c2]);
+            dx /= 3.0;
+            double dy = v1 * sin(theta[c0]);
+            dy += v2 * sin(theta[c1]);
+            dy += v3 * sin(theta[c2]);
+            dy /= 3.0;
+            disp[2 * i] = dt * (dx + mu * F[2 * i]);
+            disp[2 * i + 1] = dt * (dy + mu * F[2 * i + 1]);
+        }
+        for (int c = 0; c < Nc; ++c) theta[c] += noise[(size_t)s * Nc + c] * sqrt(2.0 * dt * motility[2 * c + 1]);
+        for (int v = 0; v < Nv; ++v) {
+            vpos[2 * v] += disp[2 * v];
+            vpos[2 * v + 1] += disp[2 * v + 1];
+            cgo_put_in_box(box, vpos + 2 * v);
+        }
+        int nf = cgo_vertex_t1(Nc, Nv, vpos, box, t1_threshold, vmax, vn, vcn, cvn, cv, 0, NULL);
+        if (nf < 0) { st = nf; break; }
+    }
+    free(AP);
+    free(F);
+    free(disp);
+    return st;
+}

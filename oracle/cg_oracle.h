@@ -77,6 +77,12 @@ int cgo_vertex_brownian_run(int Nc, int Nv, double *vpos, const double *box, int
                             double mu, double T, double t1_threshold, int n_steps, const double *noise,
                             double *F_out, double *AP_out, int *n_t1_out);
 
+/* self-propelled vertex model with supplied noise (one normal per cell per step) */
+int cgo_vertex_spp_run(int Nc, int Nv, double *vpos, const double *box, int vmax, int *vn, int *vcn,
+                       int *cvn, int *cv, const double *APpref, double KA, double KP, double *theta,
+                       const double *motility, double dt, double mu, double t1_threshold, int n_steps,
+                       const double *noise);
+
 /* ---- FIRE (src/updaters/EnergyMinimizerFIRE2D.cpp:120-151,212-284), CPU conventions ---- */
 typedef struct {
     double dt, dt_max, dt_min, dt_inc, dt_dec, alpha, alpha_start, alpha_dec, force_cutoff;

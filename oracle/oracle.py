@@ -84,6 +84,9 @@ def lib():
                                               _dp, C.c_double, C.c_double, C.c_double, C.c_double,
                                               C.c_double, C.c_double, C.c_int, _dp, _dp, _dp,
                                               C.POINTER(C.c_int)]
+        L.cgo_vertex_spp_run.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip, _ip, _dp,
+                                         C.c_double, C.c_double, _dp, _dp, C.c_double, C.c_double,
+                                         C.c_double, C.c_int, _dp]
         L.cgo_fire_voronoi.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, _ip, _dp, C.c_double, C.c_double,
                                        C.POINTER(FireParams), _dp, _dp, _dp]
         L.cgo_fire_vertex.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip, _ip, _dp,
@@ -246,6 +249,17 @@ def vertex_brownian_run(vpos, box, vn, vcn, cvn, cv, APpref, noise, dt=0.005, mu
     if st:
         raise RuntimeError(f"oracle vertex run failed ({st})")
     return F, AP, nt1.value
+
+
+def vertex_spp_run(vpos, box, vn, vcn, cvn, cv, APpref, theta, motility, noise, dt=0.01, mu=1.0,
+                   t1_threshold=0.04, KA=1.0, KP=1.0):
+    Nv = vpos.shape[0]
+    Nc = cv.shape[0]
+    noise = _f64(noise).reshape(-1, Nc)
+    st = lib().cgo_vertex_spp_run(Nc, Nv, vpos, _box(box), cv.shape[1], vn, vcn, cvn, cv, _f64(APpref), KA, KP,
+                                  theta, _f64(motility), dt, mu, t1_threshold, noise.shape[0], noise)
+    if st:
+        raise RuntimeError(f"oracle vertex SPP failed ({st})")
 
 
 def fire_voronoi(pos, box, nn, nbr, APpref, params, vel=None, KA=1.0, KP=1.0):
