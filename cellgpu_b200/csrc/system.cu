@@ -611,12 +611,14 @@ static void launch_round(cg_system *s, const VoroArgs &a, bool forces, cudaStrea
                          int use_cond)
 {
     constexpr int WPB = 4;
+    // commit / check: 8 queue slots per 64-thread block, so a short queue still spreads over the SMs
+    constexpr int WPB_C = 2;
     k_star_local<WPB><<<148 * 4, WPB * 32, 0, st>>>(a);
     if (forces)
-        k_commit<R, true><<<148 * 2, 128, 0, st>>>(a);
+        k_commit<R, true, WPB_C><<<148 * 8, WPB_C * 32, 0, st>>>(a);
     else
-        k_commit<R, false><<<148 * 2, 128, 0, st>>>(a);
-    k_check<<<148 * 2, 128, 0, st>>>(a);
+        k_commit<R, false, WPB_C><<<148 * 8, WPB_C * 32, 0, st>>>(a);
+    k_check<WPB_C><<<148 * 8, WPB_C * 32, 0, st>>>(a);
     k_round_end<<<1, 1, 0, st>>>(a, cond, use_cond);
 }
 

@@ -317,6 +317,154 @@ CG_D int group_min(int v)
     return v;
 }
 
+CG_D bool group_any(bool v)
+{
+    int x = v ? 1 : 0;
+    x |= __shfl_xor_sync(0xffffffffu, x, 1);
+    x |= __shfl_xor_sync(0xffffffffu, x, 2);
+    x |= __shfl_xor_sync(0xffffffffu, x, 4);
+    return x != 0;
+}
+
+// Phases A-C of one group's cell (called by the whole warp; `ok` switches a group off): relative
+// neighbour positions (FP64, the exact Delaunay inputs), Voronoi vertices, A, P, the exact local
+// test (TEST) and the edge unit vectors (SCATTER). nbk receives the neighbours of the lane's slots.
+template <typename R, bool SCATTER, bool TEST>
+CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok, double2 pc, double Lx,
+                       double Ly, int gl, double2 *sR, double2 *sH, typename Vec2<R>::T *sU, int (&nbk)[2],
+                       double &A, double &P, int &fail)
+{
+    using V = typename Vec2<R>::T;
+    nbk[0] = nbk[1] = -1;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        int k = gl + G * r;
+        if (ok && k < z) {
+            nbk[r] = row[k];
+            sR[k] = min_dist(a.pos[nbk[r]], pc, Lx, Ly);
+        }
+    }
+    __syncwarp();
+    // phase B: Voronoi vertices h_k = circumcentre(0, r_{k-1}, r_k); exact local Delaunay test
+    fail = 0x7fffffff;  // smallest failing slot (x2, +1 for orientation)
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        int k = gl + G * r;
+        if (ok && k < z) {
+            int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
+            double2 ra = sR[km], rb = sR[k];
+            // Voronoi vertices are ill-conditioned (skinny triangles): always formed in FP64
+            sH[k] = circum0<double>(ra, rb);
+            if (TEST) {
+                double2 rc = sR[kp];
+                if (orient0(rb, rc) <= 0) fail = min(fail, 2 * k + 1);
+                else if (c < nbk[r] && incircle0(ra, rb, rc) < 0) fail = min(fail, 2 * k);
+            }
+        }
+    }
+    __syncwarp();
+    // phase C: edges h_k -> h_{k+1}: area, perimeter (FP64 sums in both modes: A - A0 and P - P0
+    // are small differences), unit tangents
+    double Ap = 0, Pp = 0;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        int k = gl + G * r;
+        if (ok && k < z) {
+            int kp = k + 1 == z ? 0 : k + 1;
+            double2 h0 = sH[k], h1 = sH[kp];
+            double dx = h1.x - h0.x, dy = h1.y - h0.y;
+            double len = sqrt(dx * dx + dy * dy);
+            Ap += fabs(0.5 * (h0.x * h1.y - h0.y * h1.x));
+            Pp += len;
+            if (SCATTER) {
+                V u;
+                if (sizeof(R) == sizeof(double)) {
+                    double l = len < 1e-18 ? 1e-18 : len;
+                    u = mk<R>((R)(dx / l), (R)(dy / l));
+                } else {
+                    V rk = cvt<R>(sR[k]);
+                    R il = R(1) / sqrt(rk.x * rk.x + rk.y * rk.y);
+                    u = mk<R>(-rk.y * il, rk.x * il);
+                }
+                sU[k] = u;
+            }
+        }
+    }
+    A = group_sum<double>(Ap);
+    P = group_sum<double>(Pp);
+    if (TEST) fail = group_min(fail);
+}
+
+// Phases D-E (called by the whole warp): g_k = -dE_c/dh_k, the three Jacobian contractions of every
+// vertex, and the scatter of SIGN x (contribution) to the cell and its neighbours.
+template <typename R, int SIGN>
+CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, const double2 *sR, const double2 *sH,
+                      const typename Vec2<R>::T *sU, typename Vec2<R>::T *sCA, typename Vec2<R>::T *sCB,
+                      const int (&nbk)[2], double A, double P)
+{
+    using V = typename Vec2<R>::T;
+    __syncwarp();
+    R Adiff = 0, Pdiff = 0;
+    if (ok) {
+        Adiff = (R)(a.KA * (A - a.APpref[c].x));
+        Pdiff = (R)(a.KP * (P - a.APpref[c].y));
+    }
+    R sx = 0, sy = 0;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        int k = gl + G * r;
+        if (ok && k < z) {
+            int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
+            V hm = cvt<R>(sH[km]), hp = cvt<R>(sH[kp]);
+            V um = sU[km], uk = sU[k];
+            R dAx = R(0.5) * (hp.y - hm.y), dAy = R(0.5) * (hm.x - hp.x);
+            R dPx = um.x - uk.x, dPy = um.y - uk.y;
+            R gx = -R(2) * (Adiff * dAx + Pdiff * dPx);
+            R gy = -R(2) * (Adiff * dAy + Pdiff * dPy);
+            // Jacobians of h_k (always FP64: their entries scale as 1/|ra x rb|^2), with the
+            // shared denominator |ra x rb|^2 for dh/dr_c and dh/dr_a
+            double2 ra = sR[km], rb = sR[k];
+            double cr = ra.y * rb.x - ra.x * rb.y;
+            double half_inv = 0.5 / (cr * cr);
+            double ra2 = ra.x * ra.x + ra.y * ra.y, rb2 = rb.x * rb.x + rb.y * rb.y;
+            double t1 = rb.y * ra2 - ra.y * rb2, t2 = rb.x * ra2 - ra.x * rb2;
+            double d11 = half_inv * (rb.y - ra.y) * t1, d12 = half_inv * (ra.y - rb.y) * t2;
+            double d21 = half_inv * (ra.x - rb.x) * t1, d22 = half_inv * (rb.x - ra.x) * t2;
+            // dh/dr_a = getdhdr(-ra, rb-ra)
+            double2 p = make_double2(-ra.x, -ra.y), q = make_double2(rb.x - ra.x, rb.y - ra.y);
+            double q2 = q.x * q.x + q.y * q.y;
+            double u1 = q.y * ra2 - p.y * q2, u2 = q.x * ra2 - p.x * q2;
+            double e11 = half_inv * (q.y - p.y) * u1, e12 = half_inv * (p.y - q.y) * u2;
+            double e21 = half_inv * (p.x - q.x) * u1, e22 = half_inv * (q.x - p.x) * u2;
+            R c11 = (R)d11, c12 = (R)d12, c21 = (R)d21, c22 = (R)d22;
+            R a11 = (R)e11, a12 = (R)e12, a21 = (R)e21, a22 = (R)e22;
+            R b11 = (R)(1.0 - d11 - e11), b12 = (R)(-d12 - e12), b21 = (R)(-d21 - e21),
+              b22 = (R)(1.0 - d22 - e22);
+            sx += gx * c11 + gy * c21;
+            sy += gx * c12 + gy * c22;
+            sCA[k] = mk<R>(gx * a11 + gy * a21, gx * a12 + gy * a22);
+            sCB[k] = mk<R>(gx * b11 + gy * b21, gx * b12 + gy * b22);
+        }
+    }
+    sx = group_sum<R>(sx);
+    sy = group_sum<R>(sy);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        int k = gl + G * r;
+        if (ok && k < z) {
+            int kp = k + 1 == z ? 0 : k + 1;
+            V cb = sCB[k], ca = sCA[kp];
+            if (SIGN > 0) atomic_add2<R>(a.F, nbk[r], cb.x + ca.x, cb.y + ca.y);
+            else atomic_add2<R>(a.F, nbk[r], -(cb.x + ca.x), -(cb.y + ca.y));
+        }
+    }
+    if (ok && gl == 0) {
+        if (SIGN > 0) atomic_add2<R>(a.F, c, sx, sy);
+        else atomic_add2<R>(a.F, c, -sx, -sy);
+    }
+}
+
 template <typename R, bool SCATTER, bool TEST, int WPB>
 __global__ void __launch_bounds__(WPB * 32) k_voro_groups(VoroArgs a)
 {
@@ -345,128 +493,17 @@ __global__ void __launch_bounds__(WPB * 32) k_voro_groups(VoroArgs a)
         row = a.nbr + (size_t)c * a.K;
     }
     const bool ok = live && z >= 3 && z <= VG;
-    // phase A: relative positions (FP64, exact Delaunay inputs)
-    int nbk[2] = {-1, -1};
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-        int k = gl + G * r;
-        if (ok && k < z) {
-            nbk[r] = row[k];
-            sR[sl][k] = min_dist(a.pos[nbk[r]], pc, Lx, Ly);
-        }
-    }
-    __syncwarp();
-    // phase B: Voronoi vertices h_k = circumcentre(0, r_{k-1}, r_k); exact local Delaunay test
-    int fail = 0x7fffffff;  // smallest failing slot (x2, +1 for orientation)
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-        int k = gl + G * r;
-        if (ok && k < z) {
-            int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
-            double2 ra = sR[sl][km], rb = sR[sl][k];
-            // Voronoi vertices are ill-conditioned (skinny triangles): always formed in FP64
-            sH[sl][k] = circum0<double>(ra, rb);
-            if (TEST) {
-                double2 rc = sR[sl][kp];
-                if (orient0(rb, rc) <= 0) fail = min(fail, 2 * k + 1);
-                else if (c < nbk[r] && incircle0(ra, rb, rc) < 0) fail = min(fail, 2 * k);
-            }
-        }
-    }
-    __syncwarp();
-    // phase C: edges h_k -> h_{k+1}: area, perimeter (FP64 sums in both modes: A - A0 and P - P0
-    // are small differences), unit tangents
-    double Ap = 0, Pp = 0;
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-        int k = gl + G * r;
-        if (ok && k < z) {
-            int kp = k + 1 == z ? 0 : k + 1;
-            double2 h0 = sH[sl][k], h1 = sH[sl][kp];
-            double dx = h1.x - h0.x, dy = h1.y - h0.y;
-            double len = sqrt(dx * dx + dy * dy);
-            Ap += fabs(0.5 * (h0.x * h1.y - h0.y * h1.x));
-            Pp += len;
-            if (SCATTER) {
-                V u;
-                if (sizeof(R) == sizeof(double)) {
-                    double l = len < 1e-18 ? 1e-18 : len;
-                    u = mk<R>((R)(dx / l), (R)(dy / l));
-                } else {
-                    V rk = cvt<R>(sR[sl][k]);
-                    R il = R(1) / sqrt(rk.x * rk.x + rk.y * rk.y);
-                    u = mk<R>(-rk.y * il, rk.x * il);
-                }
-                sU[sl][k] = u;
-            }
-        }
-    }
-    double A = group_sum<double>(Ap), P = group_sum<double>(Pp);
-    if (TEST) fail = group_min(fail);
+    int nbk[2];
+    double A, P;
+    int fail;
+    grp_geometry<R, SCATTER, TEST>(a, c, row, z, ok, pc, Lx, Ly, gl, sR[sl], sH[sl], sU[sl], nbk, A, P, fail);
     if (ok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
     // A cell whose own row fails the test holds its contributions back: the row is about to be
     // replaced, and a stale row can contain a nearly collinear triangle whose Jacobians (1/cross^2)
     // would swamp the forces. The repair commit adds the contributions of the new row.
     bool hold = SCATTER && TEST && a.held && ok && fail != 0x7fffffff;
     if (hold && gl == 0) a.held[c] = 1;
-    if (SCATTER && !hold) {
-        __syncwarp();
-        R Adiff = 0, Pdiff = 0;
-        if (ok) {
-            Adiff = (R)(a.KA * (A - a.APpref[c].x));
-            Pdiff = (R)(a.KP * (P - a.APpref[c].y));
-        }
-        R sx = 0, sy = 0;
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            int k = gl + G * r;
-            if (ok && k < z) {
-                int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
-                V hm = cvt<R>(sH[sl][km]), hp = cvt<R>(sH[sl][kp]);
-                V um = sU[sl][km], uk = sU[sl][k];
-                R dAx = R(0.5) * (hp.y - hm.y), dAy = R(0.5) * (hm.x - hp.x);
-                R dPx = um.x - uk.x, dPy = um.y - uk.y;
-                R gx = -R(2) * (Adiff * dAx + Pdiff * dPx);
-                R gy = -R(2) * (Adiff * dAy + Pdiff * dPy);
-                // Jacobians of h_k (always FP64: their entries scale as 1/|ra x rb|^2), with the
-                // shared denominator |ra x rb|^2 for dh/dr_c and dh/dr_a
-                double2 ra = sR[sl][km], rb = sR[sl][k];
-                double cr = ra.y * rb.x - ra.x * rb.y;
-                double half_inv = 0.5 / (cr * cr);
-                double ra2 = ra.x * ra.x + ra.y * ra.y, rb2 = rb.x * rb.x + rb.y * rb.y;
-                double t1 = rb.y * ra2 - ra.y * rb2, t2 = rb.x * ra2 - ra.x * rb2;
-                double d11 = half_inv * (rb.y - ra.y) * t1, d12 = half_inv * (ra.y - rb.y) * t2;
-                double d21 = half_inv * (ra.x - rb.x) * t1, d22 = half_inv * (rb.x - ra.x) * t2;
-                // dh/dr_a = getdhdr(-ra, rb-ra)
-                double2 p = make_double2(-ra.x, -ra.y), q = make_double2(rb.x - ra.x, rb.y - ra.y);
-                double q2 = q.x * q.x + q.y * q.y;
-                double u1 = q.y * ra2 - p.y * q2, u2 = q.x * ra2 - p.x * q2;
-                double e11 = half_inv * (q.y - p.y) * u1, e12 = half_inv * (p.y - q.y) * u2;
-                double e21 = half_inv * (p.x - q.x) * u1, e22 = half_inv * (q.x - p.x) * u2;
-                R c11 = (R)d11, c12 = (R)d12, c21 = (R)d21, c22 = (R)d22;
-                R a11 = (R)e11, a12 = (R)e12, a21 = (R)e21, a22 = (R)e22;
-                R b11 = (R)(1.0 - d11 - e11), b12 = (R)(-d12 - e12), b21 = (R)(-d21 - e21),
-                  b22 = (R)(1.0 - d22 - e22);
-                sx += gx * c11 + gy * c21;
-                sy += gx * c12 + gy * c22;
-                sCA[sl][k] = mk<R>(gx * a11 + gy * a21, gx * a12 + gy * a22);
-                sCB[sl][k] = mk<R>(gx * b11 + gy * b21, gx * b12 + gy * b22);
-            }
-        }
-        sx = group_sum<R>(sx);
-        sy = group_sum<R>(sy);
-        __syncwarp();
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            int k = gl + G * r;
-            if (ok && k < z) {
-                int kp = k + 1 == z ? 0 : k + 1;
-                V cb = sCB[sl][k], ca = sCA[sl][kp];
-                atomic_add2<R>(a.F, nbk[r], cb.x + ca.x, cb.y + ca.y);
-            }
-        }
-        if (ok && gl == 0) atomic_add2<R>(a.F, c, sx, sy);
-    }
+    if (SCATTER) grp_scatter<R, 1>(a, c, z, ok && !hold, gl, sR[sl], sH[sl], sU[sl], sCA[sl], sCB[sl], nbk, A, P);
     if (TEST && live && gl == 0 && (fail != 0x7fffffff || !ok)) {
         if (!ok) {
             if (a.ctl) {
@@ -546,8 +583,10 @@ __global__ void k_round_end(VoroArgs a, unsigned long long cond, int use_cond)
 // Gift wrapping: start from the nearest candidate (always a Delaunay neighbour); from neighbour a,
 // the next counter-clockwise neighbour is the candidate strictly counter-clockwise of a whose circle
 // through (0, a, b) is innermost in the pencil of circles through 0 and a (exact in-circle order,
-// ties by index). Each step is a warp argmin under that order. Writes global indices, CCW, rotated
-// to start at the smallest index. Returns z, -1 (not enclosed), -2 (capacity).
+// ties by index). Each step is a warp argmin under that order: a floating-point key with a rigorous
+// error interval picks the minimum, and the exact predicate runs only among the candidates whose
+// intervals reach below the smallest upper end. Writes global indices, CCW, rotated to start at the
+// smallest index. Returns z, -1 (not enclosed), -2 (capacity).
 // ------------------------------------------------------------------------------------------
 CG_D bool inner_than(double2 pa, double2 pc, int ic, double2 pb, int ib)
 {
@@ -556,8 +595,40 @@ CG_D bool inner_than(double2 pa, double2 pc, int ic, double2 pb, int ib)
     return s < 0 || (s == 0 && ic < ib);
 }
 
+// Position of the circle through 0, a and t in the pencil of circles through 0 and a: its centre is
+// a/2 + s (-a.y, a.x) with s = t.(t - a) / (2 a x t). For t strictly counter-clockwise of a
+// (a x t > 0), a point t' on that side lies strictly inside the circle of t exactly when
+// s(t') < s(t), so the next Delaunay neighbour minimises s. [lo, hi] encloses the exact s: with
+// u = 2^-53, the numerator's error is below 4u(|t.x dx| + |t.y dy|), the cross product's below
+// ED = 3u(|a.x t.y| + |a.y t.x|), and for den > ED the quotient's below
+// |num| ED / (den (den - ED)) + EN / (den - ED), plus u|s| for the division; the interval doubles
+// the total. Near-collinear t (den <= 2 ED) gets an unbounded interval.
+CG_D void pencil_key(double2 a, double2 t, double &lo, double &hi)
+{
+    const double u = 1.1102230246251565e-16;
+    double dx = t.x - a.x, dy = t.y - a.y;
+    double n1 = t.x * dx, n2 = t.y * dy;
+    double num = n1 + n2;
+    double EN = 4.0 * u * (fabs(n1) + fabs(n2));
+    double d1 = a.x * t.y, d2 = a.y * t.x;
+    double den = d1 - d2;
+    double ED = 3.0 * u * (fabs(d1) + fabs(d2));
+    if (!(den > 2.0 * ED)) {
+        lo = -HUGE_VAL;
+        hi = HUGE_VAL;
+        return;
+    }
+    double s = 0.5 * num / den;
+    double dm = den - ED;
+    double err = 0.5 * (fabs(num) * ED / (den * dm) + EN / dm) + 2.0 * u * fabs(s);
+    err *= 2.0;
+    lo = s - err;
+    hi = s + err;
+}
+
 __device__ int warp_star(const double2 *rel, const int *gidx, int m, int K, int *out, int lane)
 {
+    const unsigned full = 0xffffffffu;
     // nearest candidate
     double best = 1e300;
     int bi = -1;
@@ -569,8 +640,8 @@ __device__ int warp_star(const double2 *rel, const int *gidx, int m, int K, int 
         }
     }
     for (int off = 16; off > 0; off >>= 1) {
-        double ob = __shfl_xor_sync(0xffffffffu, best, off);
-        int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        double ob = __shfl_xor_sync(full, best, off);
+        int oi = __shfl_xor_sync(full, bi, off);
         if (oi >= 0 && (bi < 0 || ob < best || (ob == best && gidx[oi] < gidx[bi]))) {
             best = ob;
             bi = oi;
@@ -583,16 +654,40 @@ __device__ int warp_star(const double2 *rel, const int *gidx, int m, int K, int 
         if (lane == 0) out[z] = cur;
         ++z;
         double2 pa = rel[cur];
-        int b = -1;
+        // pass 1: smallest upper end U of the key intervals of the counter-clockwise candidates
+        double U = HUGE_VAL;
+        bool any = false;
         for (int t = lane; t < m; t += WARP) {
             if (t == cur) continue;
             double2 pt = rel[t];
             if (orient0(pa, pt) <= 0) continue;
+            double lo, hi;
+            pencil_key(pa, pt, lo, hi);
+            U = fmin(U, hi);
+            any = true;
+        }
+        if (!__any_sync(full, any)) return -1;
+        for (int off = 16; off > 0; off >>= 1) U = fmin(U, __shfl_xor_sync(full, U, off));
+        // pass 2: only candidates with lo <= U can be the minimum; order them exactly
+        int b = -1, cnt = 0;
+        for (int t = lane; t < m; t += WARP) {
+            if (t == cur) continue;
+            double2 pt = rel[t];
+            if (orient0(pa, pt) <= 0) continue;
+            double lo, hi;
+            pencil_key(pa, pt, lo, hi);
+            if (!(lo <= U)) continue;
+            ++cnt;
             if (b < 0 || inner_than(pa, pt, gidx[t], rel[b], gidx[b])) b = t;
         }
-        for (int off = 16; off > 0; off >>= 1) {
-            int ob = __shfl_xor_sync(0xffffffffu, b, off);
-            if (ob >= 0 && (b < 0 || inner_than(pa, rel[ob], gidx[ob], rel[b], gidx[b]))) b = ob;
+        unsigned has = __ballot_sync(full, cnt > 0);
+        if (__reduce_add_sync(full, (unsigned)cnt) > 1u) {
+            for (int off = 16; off > 0; off >>= 1) {
+                int ob = __shfl_xor_sync(full, b, off);
+                if (ob >= 0 && (b < 0 || inner_than(pa, rel[ob], gidx[ob], rel[b], gidx[b]))) b = ob;
+            }
+        } else {
+            b = __shfl_sync(full, b, __ffs(has) - 1);
         }
         if (b < 0) return -1;
         if (b == start) {
@@ -619,29 +714,6 @@ __device__ int warp_star(const double2 *rel, const int *gidx, int m, int K, int 
     return -1;
 }
 
-// dedupe the raw candidate list in place (drops `self` and repeats), keeping first occurrences
-CG_D int warp_unique(int *cand, int m, int self, int lane)
-{
-    int out = 0;
-    for (int base = 0; base < m; base += WARP) {
-        int t = base + lane;
-        int v = (t < m) ? cand[t] : -1;
-        bool keep = (t < m) && v != self;
-        if (keep)
-            for (int u = 0; u < t; ++u)
-                if (cand[u] == v) {
-                    keep = false;
-                    break;
-                }
-        unsigned bal = __ballot_sync(0xffffffffu, keep);
-        __syncwarp();
-        if (keep) cand[out + __popc(bal & ((1u << lane) - 1u))] = v;
-        out += __popc(bal);
-        __syncwarp();
-    }
-    return out;
-}
-
 // compact the candidate list in place, dropping `self` (no repeats possible)
 CG_D int warp_remove(int *cand, int m, int self, int lane)
 {
@@ -660,13 +732,35 @@ CG_D int warp_remove(int *cand, int m, int self, int lane)
 }
 
 // Local repair star: candidates = the current 2-ring of the cell (its neighbours and theirs).
-// One warp per queued cell; result goes to the staging row of the queue slot.
+// One warp per queued cell; result goes to the staging row of the queue slot. Rows are expanded
+// two at a time (16 lanes each, rows hold at most 16 entries), and candidates are deduplicated in a
+// per-warp open-addressing table in shared memory, so collecting a ring costs a few parallel loads.
+constexpr int CAND_HASH = 512;  // > CAND_LOCAL + 32: the table never fills
+
+CG_D void cand_insert(int *table, int *list, int *count, int v)
+{
+    unsigned h = ((unsigned)v * 2654435761u) >> 23;  // 9 bits
+    for (int probe = 0; probe < CAND_HASH; ++probe) {
+        int prev = atomicCAS(&table[h], -1, v);
+        if (prev == -1) {
+            int idx = atomicAdd(count, 1);
+            if (idx < CAND_LOCAL) list[idx] = v;
+            return;
+        }
+        if (prev == v) return;
+        h = (h + 1) & (CAND_HASH - 1);
+    }
+}
+
 template <int WPB>
 __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
 {
     __shared__ int s_cand[WPB][CAND_LOCAL];
     __shared__ double2 s_rel[WPB][CAND_LOCAL];
     __shared__ int s_out[WPB][KMAX];
+    __shared__ int s_hash[WPB][CAND_HASH];
+    __shared__ int s_m[WPB];
+    const unsigned full = 0xffffffffu;
     Ctl *ctl = a.ctl;
     if (ctl->halt) return;
     int round = ctl->round;
@@ -675,45 +769,39 @@ __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int gw = blockIdx.x * WPB + w, nw = gridDim.x * WPB;
     const int *queue = a.queue + (size_t)round * a.N;
+    volatile int *vm = &s_m[w];
     for (int q = gw; q < nq; q += nw) {
         int c = queue[q];
         const Inst &in = inst_of(a, c);
         int z = a.nn[c];
         const int *row = a.nbr + (size_t)c * a.K;
-        // candidates: the cell's neighbours and theirs (2-ring); from round 1 on, also the
-        // neighbours of the whole 2-ring (3-ring), for cells whose new star reaches further
-        int m = 0;
-        if (lane < z) s_cand[w][lane] = row[lane];
-        m = z;
+        for (int i = lane; i < CAND_HASH; i += WARP) s_hash[w][i] = -1;
+        if (lane == 0) *vm = 0;
         __syncwarp();
-        int nsrc = z;
-        bool full = false;
-        for (int ring = 0; ring < (round == 0 ? 1 : 2) && !full; ++ring) {
-            int src_end = m;
-            for (int k = (ring == 0 ? 0 : z); k < (ring == 0 ? nsrc : src_end) && !full; ++k) {
-                int x = s_cand[w][k];
-                int zx = a.nn[x];
-                // append members of x's row that are new (warp-parallel membership test)
-                int v = (lane < zx) ? a.nbr[(size_t)x * a.K + lane] : -1;
-                bool isnew = (lane < zx) && v != c;
-                if (isnew)
-                    for (int u = 0; u < m; ++u)
-                        if (s_cand[w][u] == v) {
-                            isnew = false;
-                            break;
-                        }
-                unsigned bal = __ballot_sync(0xffffffffu, isnew);
-                if (m + __popc(bal) > CAND_LOCAL) {
-                    full = true;
-                    break;
+        if (lane < z) cand_insert(s_hash[w], s_cand[w], &s_m[w], row[lane]);
+        __syncwarp();
+        // ring 1 expands the row's members; from round 1 on, ring 2 expands the new 2-ring members
+        // too (3-ring), for cells whose new star reaches further
+        int lo = 0, hi = min(*vm, CAND_LOCAL);
+        for (int ring = 0; ring < (round == 0 ? 1 : 2); ++ring) {
+            for (int base = lo; base < hi; base += WARP) {
+                int j = base + lane;
+                int x = j < hi ? s_cand[w][j] : -1;
+                int zx = x >= 0 ? a.nn[x] : 0;
+                int cnt = min(hi - base, WARP);
+                for (int p = 0; p < cnt; p += 2) {
+                    int src = p + (lane >> 4), e = lane & 15;
+                    int xs = __shfl_sync(full, x, src);
+                    int zs = __shfl_sync(full, zx, src);
+                    int v = (src < cnt && e < zs) ? a.nbr[(size_t)xs * a.K + e] : -1;
+                    if (v >= 0 && v != c && *vm < CAND_LOCAL) cand_insert(s_hash[w], s_cand[w], &s_m[w], v);
                 }
-                __syncwarp();
-                if (isnew) s_cand[w][m + __popc(bal & ((1u << lane) - 1u))] = v;
-                m += __popc(bal);
-                __syncwarp();
             }
-            // after the first ring, rows of the new members (k from z) extend to the next ring
+            __syncwarp();
+            lo = hi;
+            hi = min(*vm, CAND_LOCAL);
         }
+        int m = min(*vm, CAND_LOCAL);
         double2 pc = a.pos[c];
         for (int t = lane; t < m; t += WARP)
             s_rel[w][t] = min_dist(a.pos[s_cand[w][t]], pc, in.Lx, in.Ly);
@@ -733,59 +821,99 @@ __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
     }
 }
 
-// Commit staged rows: rows that changed retract their old contributions and add the new ones
-// (forces stay consistent with the topology), A/P are refreshed, and the old row is kept in the
-// staging slot for the consistency check.
-template <typename R, bool FORCES>
-__global__ void k_commit(VoroArgs a)
+// Commit staged rows, one 8-lane group per queue slot (lane = Voronoi vertex, as in the force pass):
+// rows that changed retract their old contributions and add the new ones (forces stay consistent
+// with the topology), A/P are refreshed, and the old row is kept in the staging slot for the
+// consistency check. Unchanged rows whose force contributions the force pass held back add them now.
+template <typename R, bool FORCES, int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
 {
+    using V = typename Vec2<R>::T;
+    __shared__ double2 sR[WPB * GPW][VG];
+    __shared__ double2 sH[WPB * GPW][VG];
+    __shared__ V sU[WPB * GPW][VG];
+    __shared__ V sCA[WPB * GPW][VG];
+    __shared__ V sCB[WPB * GPW][VG];
     Ctl *ctl = a.ctl;
     if (ctl->halt) return;
     int round = ctl->round;
     if (round >= R_MAX) return;
-    int nq = ctl->q_count[round];
+    const int nq = ctl->q_count[round];
     const int *queue = a.queue + (size_t)round * a.N;
-    int stride = gridDim.x * blockDim.x;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
-        int c = queue[q];
-        int zo = a.nn[c], zn = a.stage_nn[q];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int gl = lane & (G - 1), gi = lane >> 3;
+    const int sl = w * GPW + gi;
+    const int step = gridDim.x * WPB * GPW;
+    for (int base = (blockIdx.x * WPB + w) * GPW; base < nq; base += step) {  // warp-uniform loop
+        const int q = base + gi;
+        const bool live = q < nq;
+        int c = 0, zo = 0, zn = 0;
+        if (live) {
+            c = queue[q];
+            zo = a.nn[c];
+            zn = a.stage_nn[q];
+        }
         int *row = a.nbr + (size_t)c * a.K;
-        int *srow = a.stage_nbr + (size_t)q * a.K;
-        bool same = (zo == zn);
-        for (int k = 0; same && k < zn; ++k) same = (row[k] == srow[k]);
-        if (same) {
-            // unchanged rows are still checked against their partners; held contributions are added
-            if (FORCES && a.held && a.held[c]) {
-                const Inst &in0 = inst_of(a, c);
-                R A0, P0;
-                cell_pass<R, true, false>(a, c, row, zo, a.pos[c], in0.Lx, in0.Ly, R(1), A0, P0);
-                if (a.AP) store_ap<R>(a.AP, c, A0, P0);
+        int *srow = a.stage_nbr + (size_t)(live ? q : 0) * a.K;
+        bool diff = live && zo != zn;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            int k = gl + G * r;
+            if (live && !diff && k < zn && row[k] != srow[k]) diff = true;
+        }
+        diff = group_any(diff);
+        const bool was_held = live && a.held && a.held[c];
+        double2 pc = make_double2(0, 0);
+        double Lx = 1, Ly = 1;
+        if (live) {
+            const Inst &in = inst_of(a, c);
+            Lx = in.Lx;
+            Ly = in.Ly;
+            pc = a.pos[c];
+        }
+        int nbk[2];
+        double A, P;
+        int fail;
+        if (FORCES) {
+            // retract the old row's contributions (skipped if the force pass held them back)
+            const bool ok1 = live && diff && !was_held && zo >= 3 && zo <= VG;
+            grp_geometry<R, true, false>(a, c, row, zo, ok1, pc, Lx, Ly, gl, sR[sl], sH[sl], sU[sl], nbk, A, P,
+                                         fail);
+            grp_scatter<R, -1>(a, c, zo, ok1, gl, sR[sl], sH[sl], sU[sl], sCA[sl], sCB[sl], nbk, A, P);
+        }
+        __syncwarp();
+        // swap rows; each lane moves the slots it owns
+        if (live && diff) {
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                int k = gl + G * r;
+                if (k < a.K) {
+                    int t = (k < zn) ? srow[k] : -1;
+                    srow[k] = (k < zo) ? row[k] : -1;
+                    row[k] = t;
+                }
             }
+        }
+        if (live && gl == 0) {
             if (a.held) a.held[c] = 0;
-            a.stage_nn[q] = -1;
+            if (diff) {
+                a.stage_nn[q] = zo;
+                a.nn[c] = zn;
+            } else {
+                a.stage_nn[q] = -1;  // unchanged: still checked against its partners
+            }
+        }
+        // add the new row's contributions and refresh A/P
+        const bool ok2 = live && (diff || (FORCES && was_held)) && zn >= 3 && zn <= VG;
+        grp_geometry<R, FORCES, false>(a, c, row, zn, ok2, pc, Lx, Ly, gl, sR[sl], sH[sl], sU[sl], nbk, A, P, fail);
+        if (FORCES) grp_scatter<R, 1>(a, c, zn, ok2, gl, sR[sl], sH[sl], sU[sl], sCA[sl], sCB[sl], nbk, A, P);
+        if (ok2 && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
+        if (live && gl == 0) {
             int slot = atomicAdd(&ctl->n_changed[round], 1);
             a.changed[(size_t)round * a.N + slot] = q;
-            continue;
+            if (diff) atomicAdd(&ctl->counters[2], 1ull);
         }
-        const Inst &in = inst_of(a, c);
-        double2 pc = a.pos[c];
-        R A, P;
-        bool was_held = a.held && a.held[c];
-        if (a.held) a.held[c] = 0;
-        if (FORCES && !was_held) cell_pass<R, true, false>(a, c, row, zo, pc, in.Lx, in.Ly, R(-1), A, P);
-        // swap rows
-        for (int k = 0; k < a.K; ++k) {
-            int t = (k < zn) ? srow[k] : -1;
-            srow[k] = (k < zo) ? row[k] : -1;
-            row[k] = t;
-        }
-        a.stage_nn[q] = zo;
-        a.nn[c] = zn;
-        cell_pass<R, FORCES, false>(a, c, row, zn, pc, in.Lx, in.Ly, R(1), A, P);
-        if (a.AP) store_ap<R>(a.AP, c, A, P);
-        int slot = atomicAdd(&ctl->n_changed[round], 1);
-        a.changed[(size_t)round * a.N + slot] = q;
-        atomicAdd(&ctl->counters[2], 1ull);
+        __syncwarp();
     }
 }
 
@@ -806,56 +934,88 @@ CG_D bool row_has_pair(const int *row, int z, int u, int v)
     return row[t] == v;
 }
 
-// Consistency of the changed rows of a round: every new triangle (c,a,b) must appear in the rows of
-// a and b, every dropped triangle must be gone from them, and the new row must pass the exact local
-// test. Offending cells are queued for the next round.
-__global__ void k_check(VoroArgs a)
+// Consistency of the processed rows of a round, one 8-lane group per row (lane = slot): every
+// triangle (c,a,b) of the row must appear in the rows of a and b, every dropped triangle must be
+// gone from them, and a changed row must pass the exact local test. Offending cells are queued for
+// the next round.
+template <int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_check(VoroArgs a)
 {
+    __shared__ double2 sR[WPB * GPW][VG];
     Ctl *ctl = a.ctl;
     if (ctl->halt) return;
     int round = ctl->round;
     if (round >= R_MAX) return;
-    int nch = ctl->n_changed[round];
-    int e = ctl->epoch + round + 1;
-    int nq = round + 1;
+    const int nch = ctl->n_changed[round];
+    const int e = ctl->epoch + round + 1;
+    const int nq = round + 1;
     const int *queue = a.queue + (size_t)round * a.N;
-    int stride = gridDim.x * blockDim.x;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nch; t += stride) {
-        int q = a.changed[(size_t)round * a.N + t];
-        int c = queue[q];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int gl = lane & (G - 1), gi = lane >> 3;
+    const int sl = w * GPW + gi;
+    const int step = gridDim.x * WPB * GPW;
+    for (int base = (blockIdx.x * WPB + w) * GPW; base < nch; base += step) {  // warp-uniform loop
+        const int t = base + gi;
+        const bool live = t < nch;
+        int q = 0, c = 0, z = 0, zo = -1;
+        if (live) {
+            q = a.changed[(size_t)round * a.N + t];
+            c = queue[q];
+            z = a.nn[c];
+            zo = a.stage_nn[q];
+        }
         const int *row = a.nbr + (size_t)c * a.K;
-        int z = a.nn[c];
         const int *orow = a.stage_nbr + (size_t)q * a.K;
-        int zo = a.stage_nn[q];
-        for (int k = 0; k < z; ++k) {
-            int u = row[k], v = row[(k + 1) % z];
-            if (!row_has_pair(a.nbr + (size_t)u * a.K, a.nn[u], v, c)) claim_enqueue(a, u, e, nq);
-            if (!row_has_pair(a.nbr + (size_t)v * a.K, a.nn[v], c, u)) claim_enqueue(a, v, e, nq);
+        const bool tested = live && zo >= 0;  // unchanged rows: nothing dropped, already tested
+        double2 pc = make_double2(0, 0);
+        double Lx = 1, Ly = 1;
+        if (tested) {
+            const Inst &in = inst_of(a, c);
+            Lx = in.Lx;
+            Ly = in.Ly;
+            pc = a.pos[c];
         }
-        if (zo < 0) continue;  // unchanged row: nothing dropped, already tested
-        for (int k = 0; k < zo; ++k) {
-            int u = orow[k], v = orow[(k + 1) % zo];
-            if (row_has_pair(row, z, u, v)) continue;  // triangle kept
-            if (row_has_pair(a.nbr + (size_t)u * a.K, a.nn[u], v, c)) claim_enqueue(a, u, e, nq);
-            if (row_has_pair(a.nbr + (size_t)v * a.K, a.nn[v], c, u)) claim_enqueue(a, v, e, nq);
+        int nb[2] = {-1, -1};
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            int k = gl + G * r;
+            if (live && k < z) {
+                nb[r] = row[k];
+                if (tested) sR[sl][k] = min_dist(a.pos[nb[r]], pc, Lx, Ly);
+            }
         }
-        // exact local test of the new row
-        const Inst &in = inst_of(a, c);
-        double2 pc = a.pos[c];
-        double2 dA = min_dist(a.pos[row[z - 1]], pc, in.Lx, in.Ly);
-        double2 dB = min_dist(a.pos[row[0]], pc, in.Lx, in.Ly);
-        bool bad = false;
-        for (int k = 0; k < z && !bad; ++k) {
-            double2 dC = min_dist(a.pos[row[(k + 1) % z]], pc, in.Lx, in.Ly);
-            if (orient0(dB, dC) <= 0) bad = true;
-            else if (incircle0(dA, dB, dC) < 0) bad = true;
-            dA = dB;
-            dB = dC;
+        __syncwarp();
+        bool bad = tested && z < 3;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            int k = gl + G * r;
+            if (live && k < z) {
+                int kp = k + 1 == z ? 0 : k + 1;
+                int u = nb[r], v = row[kp];
+                if (!row_has_pair(a.nbr + (size_t)u * a.K, a.nn[u], v, c)) claim_enqueue(a, u, e, nq);
+                if (!row_has_pair(a.nbr + (size_t)v * a.K, a.nn[v], c, u)) claim_enqueue(a, v, e, nq);
+                if (tested && z >= 3) {
+                    int km = k == 0 ? z - 1 : k - 1;
+                    double2 dA = sR[sl][km], dB = sR[sl][k], dC = sR[sl][kp];
+                    if (orient0(dB, dC) <= 0 || incircle0(dA, dB, dC) < 0) bad = true;
+                }
+            }
+            if (tested && k < zo) {
+                int u = orow[k], v = orow[k + 1 == zo ? 0 : k + 1];
+                if (!row_has_pair(row, z, u, v)) {  // dropped triangle
+                    if (row_has_pair(a.nbr + (size_t)u * a.K, a.nn[u], v, c)) claim_enqueue(a, u, e, nq);
+                    if (row_has_pair(a.nbr + (size_t)v * a.K, a.nn[v], c, u)) claim_enqueue(a, v, e, nq);
+                }
+            }
         }
+        bad = group_any(bad);
         if (bad) {
-            claim_enqueue(a, c, e, nq);
-            for (int k = 0; k < z; ++k) claim_enqueue(a, row[k], e, nq);
+            if (gl == 0) claim_enqueue(a, c, e, nq);
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
+                if (nb[r] >= 0) claim_enqueue(a, nb[r], e, nq);
         }
+        __syncwarp();
     }
 }
 
