@@ -45,6 +45,13 @@ extern "C" int cg_version(void) { return 100; }
 
 static inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
+// launch of the fused per-cell pass (groups of 8 lanes, CG_FORCE_WPB warps per block)
+template <typename R, bool SCATTER, bool TEST>
+static inline void launch_groups(const VoroArgs &a, int N, cudaStream_t st)
+{
+    k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB><<<nblk(N, CG_FORCE_WPB * GPW), CG_FORCE_WPB * 32, 0, st>>>(a);
+}
+
 static Inst make_inst(double Lx, double Ly, int off, int n, int bin_off, double bin_target)
 {
     Inst in;
@@ -96,7 +103,7 @@ extern "C" int cg_voronoi_geometry(const double *pos, const int *nn, const int *
     VoroArgs a = raw_args(pos, nn, nbr, K, N, Lx, Ly);
     a.AP = AP;
     if (K <= VG)
-        k_voro_groups<double, false, false, 4><<<nblk(N, 4 * GPW), 128, 0, stream>>>(a);
+        launch_groups<double, false, false>(a, N, stream);
     else
         k_voro_cells<double, false, false><<<nblk(N, 128), 128, 0, stream>>>(a);
     return check_launch();
@@ -115,7 +122,7 @@ extern "C" int cg_voronoi_forces(const double *pos, const int *nn, const int *nb
     a.AP = AP;
     a.F = F;
     if (K <= VG)
-        k_voro_groups<double, true, false, 4><<<nblk(N, 4 * GPW), 128, 0, stream>>>(a);
+        launch_groups<double, true, false>(a, N, stream);
     else
         k_voro_cells<double, true, false><<<nblk(N, 128), 128, 0, stream>>>(a);
     return check_launch();
@@ -131,7 +138,7 @@ extern "C" int cg_voronoi_test_triangulation(const double *pos, const int *nn, c
     a.mark = flag;
     a.queue = any_fail;
     if (K <= VG)
-        k_voro_groups<double, false, true, 4><<<nblk(N, 4 * GPW), 128, 0, stream>>>(a);
+        launch_groups<double, false, true>(a, N, stream);
     else
         k_voro_cells<double, false, true><<<nblk(N, 128), 128, 0, stream>>>(a);
     return check_launch();
@@ -151,7 +158,7 @@ extern "C" int cg_spp_step(double *pos, double *theta, const double *F, const do
     a.F = (void *)F;
     a.motility = (const double2 *)motility;
     (void)step;
-    k_spp<double><<<nblk(N, 256), 256, 0, stream>>>(a, noise, dt, mu, seed, 0);
+    k_spp<double><<<nblk((N + 1) / 2, 256), 256, 0, stream>>>(a, noise, dt, mu, seed, 0);
     return check_launch();
 }
 
@@ -600,9 +607,9 @@ static void launch_force_test(cg_system *s, const VoroArgs &a, bool test)
     cudaMemsetAsync(s->F, 0, (s->precision == CG_FP64 ? sizeof(double2) : sizeof(float2)) * s->N,
                     s->stream);
     if (test)
-        k_voro_groups<R, true, true, 4><<<nblk(s->N, 4 * GPW), 128, 0, s->stream>>>(a);
+        launch_groups<R, true, true>(a, s->N, s->stream);
     else
-        k_voro_groups<R, true, false, 4><<<nblk(s->N, 4 * GPW), 128, 0, s->stream>>>(a);
+        launch_groups<R, true, false>(a, s->N, s->stream);
     s->kernels_enqueued += 1;
 }
 
@@ -686,7 +693,7 @@ static int enforce_t(cg_system *s)
 {
     VoroArgs a = sys_args(s);
     for (int attempt = 0; attempt < 3; ++attempt) {
-        k_voro_groups<R, false, true, 4><<<nblk(s->N, 4 * GPW), 128, 0, s->stream>>>(a);
+        launch_groups<R, false, true>(a, s->N, s->stream);
         launch_repair<R>(s, a, false);
         k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 0);
         CG_TRY(check_launch());
@@ -714,7 +721,7 @@ static void enqueue_spp_steps(cg_system *s, int n, double dt, double mu, const d
         launch_force_test<R>(s, a, true);
         launch_repair<R>(s, a, true);
         const double *nz = noise ? (noise_per_step ? noise + (size_t)t * s->N : noise) : nullptr;
-        k_spp<R><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, nz, dt, mu, s->seed, 0);
+        k_spp<R><<<nblk((s->N + 1) / 2, 256), 256, 0, s->stream>>>(a, nz, dt, mu, s->seed, 0);
         k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
         s->kernels_enqueued += 2;
     }
@@ -751,7 +758,7 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
         for (int t = 0; t < n; ++t) {
             launch_force_test<R>(s, a, true);
             launch_repair<R>(s, a, true);
-            k_spp<R><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, noise, dt, mu, s->seed, 0);
+            k_spp<R><<<nblk((s->N + 1) / 2, 256), 256, 0, s->stream>>>(a, noise, dt, mu, s->seed, 0);
             k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
             s->kernels_enqueued += 2;
         }
@@ -785,7 +792,7 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
         deps.assign(1, cn);
         CG_CUDA(cudaStreamBeginCaptureToGraph(s->stream, graph, deps.data(), nullptr, deps.size(), mode));
         const double *nz = noise;
-        k_spp<R><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, nz, dt, mu, s->seed, 0);
+        k_spp<R><<<nblk((s->N + 1) / 2, 256), 256, 0, s->stream>>>(a, nz, dt, mu, s->seed, 0);
         k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
         s->kernels_enqueued += 2;
         st = capture_deps(s->stream);

@@ -326,37 +326,52 @@ CG_D bool group_any(bool v)
     return x != 0;
 }
 
+// Shared-memory tile of one group's cell: relative neighbour positions r_k, Voronoi vertices h_k,
+// the reciprocal 1 / (2 r_{k-1} x r_k) (shared by h_k and its Jacobians), unit tangents of the
+// edges h_k -> h_{k+1}, and the dh_k/dr_{k-1} contraction consumed by the neighbouring lane.
+template <typename R>
+struct GrpTile {
+    double2 r[VG];
+    double2 h[VG];
+    double den[VG];
+    typename Vec2<R>::T u[VG];
+    typename Vec2<R>::T ca[VG];
+};
+
 // Phases A-C of one group's cell (called by the whole warp; `ok` switches a group off): relative
 // neighbour positions (FP64, the exact Delaunay inputs), Voronoi vertices, A, P, the exact local
 // test (TEST) and the edge unit vectors (SCATTER). nbk receives the neighbours of the lane's slots.
 template <typename R, bool SCATTER, bool TEST>
 CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok, double2 pc, double Lx,
-                       double Ly, int gl, double2 *sR, double2 *sH, typename Vec2<R>::T *sU, int (&nbk)[2],
-                       double &A, double &P, int &fail)
+                       double Ly, int gl, GrpTile<R> &T, int (&nbk)[2], double &A, double &P, int &fail)
 {
     using V = typename Vec2<R>::T;
-    nbk[0] = nbk[1] = -1;
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
         int k = gl + G * r;
+        nbk[r] = -1;
         if (ok && k < z) {
             nbk[r] = row[k];
-            sR[k] = min_dist(a.pos[nbk[r]], pc, Lx, Ly);
+            T.r[k] = min_dist(a.pos[nbk[r]], pc, Lx, Ly);
         }
     }
     __syncwarp();
-    // phase B: Voronoi vertices h_k = circumcentre(0, r_{k-1}, r_k); exact local Delaunay test
+    // phase B: Voronoi vertices h_k = circumcentre(0, r_{k-1}, r_k) (inc/utility/functions.h:34-43);
+    // exact local Delaunay test
     fail = 0x7fffffff;  // smallest failing slot (x2, +1 for orientation)
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
         int k = gl + G * r;
         if (ok && k < z) {
-            int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
-            double2 ra = sR[km], rb = sR[k];
+            int km = k == 0 ? z - 1 : k - 1;
+            double2 ra = T.r[km], rb = T.r[k];
             // Voronoi vertices are ill-conditioned (skinny triangles): always formed in FP64
-            sH[k] = circum0<double>(ra, rb);
+            double an = ra.x * ra.x + ra.y * ra.y, bn = rb.x * rb.x + rb.y * rb.y;
+            double den = 0.5 / (ra.x * rb.y - ra.y * rb.x);
+            if (SCATTER) T.den[k] = den;
+            T.h[k] = make_double2(den * (an * rb.y - ra.y * bn), den * (ra.x * bn - an * rb.x));
             if (TEST) {
-                double2 rc = sR[kp];
+                double2 rc = T.r[k + 1 == z ? 0 : k + 1];
                 if (orient0(rb, rc) <= 0) fail = min(fail, 2 * k + 1);
                 else if (c < nbk[r] && incircle0(ra, rb, rc) < 0) fail = min(fail, 2 * k);
             }
@@ -370,8 +385,7 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
     for (int r = 0; r < 2; ++r) {
         int k = gl + G * r;
         if (ok && k < z) {
-            int kp = k + 1 == z ? 0 : k + 1;
-            double2 h0 = sH[k], h1 = sH[kp];
+            double2 h0 = T.h[k], h1 = T.h[k + 1 == z ? 0 : k + 1];
             double dx = h1.x - h0.x, dy = h1.y - h0.y;
             double len = sqrt(dx * dx + dy * dy);
             Ap += fabs(0.5 * (h0.x * h1.y - h0.y * h1.x));
@@ -379,14 +393,14 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
             if (SCATTER) {
                 V u;
                 if (sizeof(R) == sizeof(double)) {
-                    double l = len < 1e-18 ? 1e-18 : len;
-                    u = mk<R>((R)(dx / l), (R)(dy / l));
+                    double il = 1.0 / (len < 1e-18 ? 1e-18 : len);
+                    u = mk<R>((R)(dx * il), (R)(dy * il));
                 } else {
-                    V rk = cvt<R>(sR[k]);
+                    V rk = cvt<R>(T.r[k]);
                     R il = R(1) / sqrt(rk.x * rk.x + rk.y * rk.y);
                     u = mk<R>(-rk.y * il, rk.x * il);
                 }
-                sU[k] = u;
+                T.u[k] = u;
             }
         }
     }
@@ -398,9 +412,8 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
 // Phases D-E (called by the whole warp): g_k = -dE_c/dh_k, the three Jacobian contractions of every
 // vertex, and the scatter of SIGN x (contribution) to the cell and its neighbours.
 template <typename R, int SIGN>
-CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, const double2 *sR, const double2 *sH,
-                      const typename Vec2<R>::T *sU, typename Vec2<R>::T *sCA, typename Vec2<R>::T *sCB,
-                      const int (&nbk)[2], double A, double P)
+CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<R> &T, const int (&nbk)[2],
+                      double A, double P)
 {
     using V = typename Vec2<R>::T;
     __syncwarp();
@@ -410,27 +423,28 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, const do
         Pdiff = (R)(a.KP * (P - a.APpref[c].y));
     }
     R sx = 0, sy = 0;
+    V cb[2];
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
         int k = gl + G * r;
         if (ok && k < z) {
             int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
-            V hm = cvt<R>(sH[km]), hp = cvt<R>(sH[kp]);
-            V um = sU[km], uk = sU[k];
+            V hm = cvt<R>(T.h[km]), hp = cvt<R>(T.h[kp]);
+            V um = T.u[km], uk = T.u[k];
             R dAx = R(0.5) * (hp.y - hm.y), dAy = R(0.5) * (hm.x - hp.x);
             R dPx = um.x - uk.x, dPy = um.y - uk.y;
             R gx = -R(2) * (Adiff * dAx + Pdiff * dPx);
             R gy = -R(2) * (Adiff * dAy + Pdiff * dPy);
-            // Jacobians of h_k (always FP64: their entries scale as 1/|ra x rb|^2), with the
-            // shared denominator |ra x rb|^2 for dh/dr_c and dh/dr_a
-            double2 ra = sR[km], rb = sR[k];
-            double cr = ra.y * rb.x - ra.x * rb.y;
-            double half_inv = 0.5 / (cr * cr);
+            // Jacobians of h_k (getdhdr, inc/utility/functions.h:234-287; always FP64: their entries
+            // scale as 1/|ra x rb|^2). dh/dr_c = getdhdr(ra, rb) and dh/dr_a = getdhdr(-ra, rb-ra)
+            // share the denominator 2 (ra x rb)^2 = 1 / (2 den^2).
+            double2 ra = T.r[km], rb = T.r[k];
+            double den = T.den[k];
+            double half_inv = 2.0 * den * den;
             double ra2 = ra.x * ra.x + ra.y * ra.y, rb2 = rb.x * rb.x + rb.y * rb.y;
             double t1 = rb.y * ra2 - ra.y * rb2, t2 = rb.x * ra2 - ra.x * rb2;
             double d11 = half_inv * (rb.y - ra.y) * t1, d12 = half_inv * (ra.y - rb.y) * t2;
             double d21 = half_inv * (ra.x - rb.x) * t1, d22 = half_inv * (rb.x - ra.x) * t2;
-            // dh/dr_a = getdhdr(-ra, rb-ra)
             double2 p = make_double2(-ra.x, -ra.y), q = make_double2(rb.x - ra.x, rb.y - ra.y);
             double q2 = q.x * q.x + q.y * q.y;
             double u1 = q.y * ra2 - p.y * q2, u2 = q.x * ra2 - p.x * q2;
@@ -442,8 +456,8 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, const do
               b22 = (R)(1.0 - d22 - e22);
             sx += gx * c11 + gy * c21;
             sy += gx * c12 + gy * c22;
-            sCA[k] = mk<R>(gx * a11 + gy * a21, gx * a12 + gy * a22);
-            sCB[k] = mk<R>(gx * b11 + gy * b21, gx * b12 + gy * b22);
+            T.ca[k] = mk<R>(gx * a11 + gy * a21, gx * a12 + gy * a22);
+            cb[r] = mk<R>(gx * b11 + gy * b21, gx * b12 + gy * b22);
         }
     }
     sx = group_sum<R>(sx);
@@ -453,10 +467,9 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, const do
     for (int r = 0; r < 2; ++r) {
         int k = gl + G * r;
         if (ok && k < z) {
-            int kp = k + 1 == z ? 0 : k + 1;
-            V cb = sCB[k], ca = sCA[kp];
-            if (SIGN > 0) atomic_add2<R>(a.F, nbk[r], cb.x + ca.x, cb.y + ca.y);
-            else atomic_add2<R>(a.F, nbk[r], -(cb.x + ca.x), -(cb.y + ca.y));
+            V ca = T.ca[k + 1 == z ? 0 : k + 1];
+            if (SIGN > 0) atomic_add2<R>(a.F, nbk[r], cb[r].x + ca.x, cb[r].y + ca.y);
+            else atomic_add2<R>(a.F, nbk[r], -(cb[r].x + ca.x), -(cb[r].y + ca.y));
         }
     }
     if (ok && gl == 0) {
@@ -466,14 +479,9 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, const do
 }
 
 template <typename R, bool SCATTER, bool TEST, int WPB>
-__global__ void __launch_bounds__(WPB * 32) k_voro_groups(VoroArgs a)
+__global__ void CG_FORCE_BOUNDS(WPB) k_voro_groups(VoroArgs a)
 {
-    using V = typename Vec2<R>::T;
-    __shared__ double2 sR[WPB * GPW][VG];
-    __shared__ double2 sH[WPB * GPW][VG];  // Voronoi vertices, FP64 in both modes
-    __shared__ V sU[WPB * GPW][VG];
-    __shared__ V sCA[WPB * GPW][VG];
-    __shared__ V sCB[WPB * GPW][VG];
+    __shared__ GrpTile<R> tile[WPB * GPW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int gl = lane & (G - 1), gi = lane >> 3;
     const int sl = w * GPW + gi;
@@ -496,14 +504,14 @@ __global__ void __launch_bounds__(WPB * 32) k_voro_groups(VoroArgs a)
     int nbk[2];
     double A, P;
     int fail;
-    grp_geometry<R, SCATTER, TEST>(a, c, row, z, ok, pc, Lx, Ly, gl, sR[sl], sH[sl], sU[sl], nbk, A, P, fail);
+    grp_geometry<R, SCATTER, TEST>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail);
     if (ok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
     // A cell whose own row fails the test holds its contributions back: the row is about to be
     // replaced, and a stale row can contain a nearly collinear triangle whose Jacobians (1/cross^2)
     // would swamp the forces. The repair commit adds the contributions of the new row.
     bool hold = SCATTER && TEST && a.held && ok && fail != 0x7fffffff;
     if (hold && gl == 0) a.held[c] = 1;
-    if (SCATTER) grp_scatter<R, 1>(a, c, z, ok && !hold, gl, sR[sl], sH[sl], sU[sl], sCA[sl], sCB[sl], nbk, A, P);
+    if (SCATTER) grp_scatter<R, 1>(a, c, z, ok && !hold, gl, tile[sl], nbk, A, P);
     if (TEST && live && gl == 0 && (fail != 0x7fffffff || !ok)) {
         if (!ok) {
             if (a.ctl) {
@@ -828,12 +836,7 @@ __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
 template <typename R, bool FORCES, int WPB>
 __global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
 {
-    using V = typename Vec2<R>::T;
-    __shared__ double2 sR[WPB * GPW][VG];
-    __shared__ double2 sH[WPB * GPW][VG];
-    __shared__ V sU[WPB * GPW][VG];
-    __shared__ V sCA[WPB * GPW][VG];
-    __shared__ V sCB[WPB * GPW][VG];
+    __shared__ GrpTile<R> tile[WPB * GPW];
     Ctl *ctl = a.ctl;
     if (ctl->halt) return;
     int round = ctl->round;
@@ -877,9 +880,8 @@ __global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
         if (FORCES) {
             // retract the old row's contributions (skipped if the force pass held them back)
             const bool ok1 = live && diff && !was_held && zo >= 3 && zo <= VG;
-            grp_geometry<R, true, false>(a, c, row, zo, ok1, pc, Lx, Ly, gl, sR[sl], sH[sl], sU[sl], nbk, A, P,
-                                         fail);
-            grp_scatter<R, -1>(a, c, zo, ok1, gl, sR[sl], sH[sl], sU[sl], sCA[sl], sCB[sl], nbk, A, P);
+            grp_geometry<R, true, false>(a, c, row, zo, ok1, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail);
+            grp_scatter<R, -1>(a, c, zo, ok1, gl, tile[sl], nbk, A, P);
         }
         __syncwarp();
         // swap rows; each lane moves the slots it owns
@@ -905,8 +907,8 @@ __global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
         }
         // add the new row's contributions and refresh A/P
         const bool ok2 = live && (diff || (FORCES && was_held)) && zn >= 3 && zn <= VG;
-        grp_geometry<R, FORCES, false>(a, c, row, zn, ok2, pc, Lx, Ly, gl, sR[sl], sH[sl], sU[sl], nbk, A, P, fail);
-        if (FORCES) grp_scatter<R, 1>(a, c, zn, ok2, gl, sR[sl], sH[sl], sU[sl], sCA[sl], sCB[sl], nbk, A, P);
+        grp_geometry<R, FORCES, false>(a, c, row, zn, ok2, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail);
+        if (FORCES) grp_scatter<R, 1>(a, c, zn, ok2, gl, tile[sl], nbk, A, P);
         if (ok2 && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
         if (live && gl == 0) {
             int slot = atomicAdd(&ctl->n_changed[round], 1);
@@ -932,6 +934,31 @@ CG_D bool row_has_pair(const int *row, int z, int u, int v)
     int t = s + 1;
     if (t == z) t = 0;
     return row[t] == v;
+}
+
+// does the row of cell x contain u immediately followed (cyclically) by v? Rows of 16-byte aligned
+// capacity (K % 4 == 0) are read with independent 16-byte loads, so a lookup costs one memory latency.
+CG_D bool pair_in_row(const VoroArgs &a, int x, int u, int v)
+{
+    const int *row = a.nbr + (size_t)x * a.K;
+    if ((a.K & 3) != 0) return row_has_pair(row, a.nn[x], u, v);
+    int z = a.nn[x];
+    int e[VG + 1];
+    const int4 *r4 = reinterpret_cast<const int4 *>(row);
+#pragma unroll
+    for (int j = 0; j < VG / 4; ++j) {
+        int4 t = (4 * j < a.K) ? r4[j] : make_int4(-1, -1, -1, -1);
+        e[4 * j] = t.x;
+        e[4 * j + 1] = t.y;
+        e[4 * j + 2] = t.z;
+        e[4 * j + 3] = t.w;
+    }
+    e[VG] = -1;
+    bool found = false;
+#pragma unroll
+    for (int k = 0; k < VG; ++k)
+        if (k < z && e[k] == u) found = (k + 1 < z ? e[k + 1] : e[0]) == v;
+    return found;
 }
 
 // Consistency of the processed rows of a round, one 8-lane group per row (lane = slot): every
@@ -992,8 +1019,9 @@ __global__ void __launch_bounds__(WPB * 32) k_check(VoroArgs a)
             if (live && k < z) {
                 int kp = k + 1 == z ? 0 : k + 1;
                 int u = nb[r], v = row[kp];
-                if (!row_has_pair(a.nbr + (size_t)u * a.K, a.nn[u], v, c)) claim_enqueue(a, u, e, nq);
-                if (!row_has_pair(a.nbr + (size_t)v * a.K, a.nn[v], c, u)) claim_enqueue(a, v, e, nq);
+                bool in_u = pair_in_row(a, u, v, c), in_v = pair_in_row(a, v, c, u);
+                if (!in_u) claim_enqueue(a, u, e, nq);
+                if (!in_v) claim_enqueue(a, v, e, nq);
                 if (tested && z >= 3) {
                     int km = k == 0 ? z - 1 : k - 1;
                     double2 dA = sR[sl][km], dB = sR[sl][k], dC = sR[sl][kp];
@@ -1002,9 +1030,10 @@ __global__ void __launch_bounds__(WPB * 32) k_check(VoroArgs a)
             }
             if (tested && k < zo) {
                 int u = orow[k], v = orow[k + 1 == zo ? 0 : k + 1];
-                if (!row_has_pair(row, z, u, v)) {  // dropped triangle
-                    if (row_has_pair(a.nbr + (size_t)u * a.K, a.nn[u], v, c)) claim_enqueue(a, u, e, nq);
-                    if (row_has_pair(a.nbr + (size_t)v * a.K, a.nn[v], c, u)) claim_enqueue(a, v, e, nq);
+                if (!pair_in_row(a, c, u, v)) {  // dropped triangle
+                    bool in_u = pair_in_row(a, u, v, c), in_v = pair_in_row(a, v, c, u);
+                    if (in_u) claim_enqueue(a, u, e, nq);
+                    if (in_v) claim_enqueue(a, v, e, nq);
                 }
             }
         }
@@ -1169,39 +1198,49 @@ __global__ void k_validate(VoroArgs a, int *status, unsigned long long *zsum)
 // (src/updaters/selfPropelledParticleDynamics.cpp:67-101) + movePoints (Simple2DCell.cu:21-58):
 // v from the current director, displacement dt (v + mu F), director <- atan2(v) + noise.
 template <typename R>
+CG_D void spp_cell(const VoroArgs &a, int c, double xi, double dt, double mu, int zero_force)
+{
+    const Inst &in = inst_of(a, c);
+    typename Vec2<R>::T f = reinterpret_cast<typename Vec2<R>::T *>(a.F)[c];
+    double fx = (double)f.x, fy = (double)f.y;
+    double2 mot = a.motility[c];
+    double th = a.theta[c];
+    double s, co;
+    sincos(th, &s, &co);
+    double vx = __dmul_rn(mot.x, co), vy = __dmul_rn(mot.x, s);
+    double dx = __dmul_rn(dt, __dadd_rn(vx, __dmul_rn(mu, fx)));
+    double dy = __dmul_rn(dt, __dadd_rn(vy, __dmul_rn(mu, fy)));
+    double thn = th;
+    if (!(vx == 0. && vy == 0.)) thn = atan2(vy, vx);
+    a.theta[c] = __dadd_rn(thn, __dmul_rn(xi, sqrt(__dmul_rn(__dmul_rn(2.0, dt), mot.y))));
+    double2 p = a.pos[c];
+    p.x = __dadd_rn(p.x, dx);
+    p.y = __dadd_rn(p.y, dy);
+    a.pos[c] = put_in_box(p, in.Lx, in.Ly, in.iLx, in.iLy);
+    if (zero_force) reinterpret_cast<typename Vec2<R>::T *>(a.F)[c] = mk<R>(R(0), R(0));
+}
+
+// Two cells per thread: one Box-Muller pair (Philox counter = (cell pair, step)) serves both when
+// the noise is generated on the device.
+template <typename R>
 __global__ void k_spp(VoroArgs a, const double *noise, double dt, double mu, uint64_t seed,
                       int zero_force)
 {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
     Ctl *ctl = a.ctl;
     if (ctl && ctl->halt) return;
-    if (c < a.N) {
-        const Inst &in = inst_of(a, c);
-        typename Vec2<R>::T f = reinterpret_cast<typename Vec2<R>::T *>(a.F)[c];
-        double fx = (double)f.x, fy = (double)f.y;
-        double2 mot = a.motility[c];
-        double th = a.theta[c];
-        double s, co;
-        sincos(th, &s, &co);
-        double vx = __dmul_rn(mot.x, co), vy = __dmul_rn(mot.x, s);
-        double dx = __dmul_rn(dt, __dadd_rn(vx, __dmul_rn(mu, fx)));
-        double dy = __dmul_rn(dt, __dadd_rn(vy, __dmul_rn(mu, fy)));
-        double thn = th;
-        if (!(vx == 0. && vy == 0.)) thn = atan2(vy, vx);
-        double xi;
-        if (noise) {
-            xi = noise[c];
-        } else {
-            uint32_t step = ctl ? (uint32_t)ctl->step : 0u;
-            xi = normal2(seed, (uint32_t)c, step, 0u).x;
-        }
-        a.theta[c] = __dadd_rn(thn, __dmul_rn(xi, sqrt(__dmul_rn(__dmul_rn(2.0, dt), mot.y))));
-        double2 p = a.pos[c];
-        p.x = __dadd_rn(p.x, dx);
-        p.y = __dadd_rn(p.y, dy);
-        a.pos[c] = put_in_box(p, in.Lx, in.Ly, in.iLx, in.iLy);
-        if (zero_force) reinterpret_cast<typename Vec2<R>::T *>(a.F)[c] = mk<R>(R(0), R(0));
+    int c0 = 2 * t;
+    if (c0 >= a.N) return;
+    bool two = c0 + 1 < a.N;
+    double2 xi;
+    if (noise) {
+        xi = make_double2(noise[c0], two ? noise[c0 + 1] : 0.0);
+    } else {
+        uint32_t step = ctl ? (uint32_t)ctl->step : 0u;
+        xi = normal2(seed, (uint32_t)t, step, 0u);
     }
+    spp_cell<R>(a, c0, xi.x, dt, mu, zero_force);
+    if (two) spp_cell<R>(a, c0 + 1, xi.y, dt, mu, zero_force);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -10,6 +10,20 @@ constexpr int R_MAX = 4;          // local repair rounds per step before escalat
 constexpr int CAND_LOCAL = 320;   // candidate slots per warp for the local (2-ring) star
 constexpr int CAND_GLOBAL = 384;  // candidate slots per warp for the cell-list star
 
+// launch shape of the fused per-cell pass: warps per block and (if > 0) the minimum resident blocks
+// per SM handed to __launch_bounds__; compile-time overridable for tuning sweeps
+#ifndef CG_FORCE_WPB
+#define CG_FORCE_WPB 2
+#endif
+#ifndef CG_FORCE_MINB
+#define CG_FORCE_MINB 16
+#endif
+#if CG_FORCE_MINB > 0
+#define CG_FORCE_BOUNDS(W) __launch_bounds__((W) * 32, CG_FORCE_MINB)
+#else
+#define CG_FORCE_BOUNDS(W) __launch_bounds__((W) * 32)
+#endif
+
 // device control block of one system
 struct Ctl {
     int epoch;               // base claim epoch of the current step
