@@ -301,6 +301,12 @@ def bench_vertex(cg, torch, flush, steps=40, fire=True):
     return out
 
 
+def workload_config(precision, world):
+    return {"workload": "voronoi_spp_N262144_L512", "n_cells": N_CELLS, "box": BOX, "p0": P0, "v0": V0,
+            "Dr": DR, "dt": DT, "precision": precision, "l2": "flushed (256 MB write) between timed steps",
+            "parallelism": f"replicas{world}"}
+
+
 def cpu_baseline_port(n_cells=N_CELLS, box=BOX, steps=3, seed=1):
     """Oracle port of the reference CPU path, 1 thread, on the same monolayer."""
     from oracle import oracle as O
@@ -318,12 +324,14 @@ def cpu_baseline_port(n_cells=N_CELLS, box=BOX, steps=3, seed=1):
             "sample": f"{steps} SPP steps of the N={n_cells} monolayer (full Delaunay rebuild per step)"}
 
 
-def cpu_reference(steps):
+def cpu_reference(steps, all_cores=False):
+    """The reference's CPU path (oracle/_ref, its own sources) on a relaxed sample of the workload:
+    one instance on one core, or one instance per host core; the oracle port when _ref is absent."""
     ref = os.path.join(ROOT, "oracle", "_ref", "libcgref.so")
     if os.path.exists(ref):
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import ref_harness  # noqa
-        return ref_harness.bench_c2(steps)
+        return ref_harness.bench_c2_all_cores(steps) if all_cores else ref_harness.bench_c2(steps)
     return cpu_baseline_port(steps=steps)
 
 
@@ -350,12 +358,12 @@ def main():
             return
         t0 = time.perf_counter()
         steps = max(1, min(args.steps, 3))
-        base = cpu_reference(steps)
+        base = cpu_reference(steps, all_cores=True)
         line = {"metric": METRIC, "value": base["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
                 "steps": steps, "warmup": 0, "ms_per_step": 1e3 * N_CELLS / base["value"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "impl": "reference",
-                "config": {"workload": "voronoi_spp_N262144_L512", "n_cells": N_CELLS, "box": BOX},
+                "config": workload_config(args.precision, args.gpus),
                 "cpu_baseline": base,
                 "e2e": {"value": base["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0},
@@ -457,11 +465,9 @@ def main():
         "warmup": max(3, args.warmup), "ms_per_step": 1e3 * total / max(done, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == cg.CG_FP64 else "f32+f64",
         "data": "synthetic",
-        "config": {"workload": "voronoi_spp_N262144_L512", "n_cells": N_CELLS, "box": BOX, "p0": P0,
-                   "v0": V0, "Dr": DR, "dt": DT, "precision": args.precision,
-                   "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas{world}"},
+        "config": workload_config(args.precision, world),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": traffic, "kernel": "k_voro_cells (force+test)",
+                     "frac": achieved / hbm, "traffic": traffic, "kernel": "k_voro_groups (force+test)",
                      "kernel_ms": t_force * 1e3, "peak_kind": kind},
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
