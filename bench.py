@@ -156,21 +156,29 @@ def time_force_pass(cg, torch, b, stream, reps, flush):
 
 
 def e2e_steps(cg, torch, b, stream, steps):
-    """Public API with host buffers: pinned noise in, per-instance energy out, every step."""
+    """Public API with host buffers, every step: that step's noise copied in from pinned host memory
+    (cg_spp_enqueue_host: copy stream, double-buffered, so the copy of step i+1 overlaps step i) and
+    the per-instance energy after the step copied out to pinned host memory. The noise is drawn on
+    the host before the timed region."""
     import ctypes as C
     lib = b._lib
-    noise = torch.empty(b.Ntot, dtype=torch.float64).pin_memory()
-    energy = torch.empty(1, dtype=torch.float64).pin_memory()
     gen = np.random.default_rng(7)
-    ok = 0
+    noise = torch.from_numpy(gen.standard_normal((steps, b.Ntot))).pin_memory()
+    energy = torch.zeros((steps, 1), dtype=torch.float64).pin_memory()
+    s0 = C.c_int(0)
+    lib.cg_poll(b.handle, C.byref(s0), None, 1)
     st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     st.record(stream)
     for i in range(steps):
-        noise.numpy()[:] = gen.standard_normal(b.Ntot)
-        rc = lib.cg_spp_step_host(b.handle, C.c_void_p(noise.data_ptr()), DT, MU, C.c_void_p(energy.data_ptr()))
-        ok += rc == 0
+        cg._lib.check(lib.cg_spp_enqueue_host(b.handle, C.c_void_p(noise[i].data_ptr()), DT, MU,
+                                              C.c_void_p(energy[i].data_ptr())))
     en.record(stream)
     en.synchronize()
+    s1, h = C.c_int(0), C.c_int(0)
+    lib.cg_poll(b.handle, C.byref(s1), C.byref(h), 1)
+    ok = s1.value - s0.value
+    if not np.all(np.isfinite(energy.numpy()[:ok])):
+        ok = 0
     return st.elapsed_time(en) / 1e3, ok, 8 * b.Ntot, 8
 
 

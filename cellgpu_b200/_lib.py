@@ -70,6 +70,7 @@ SIGNATURES = {
     "cg_spp_enqueue": (_i, [_vp, _i, _d, _d]),
     "cg_poll": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), _i]),
     "cg_spp_step_host": (_i, [_vp, _vp, _d, _d, _vp]),
+    "cg_spp_enqueue_host": (_i, [_vp, _vp, _d, _d, _vp]),
     "cg_launch_force_pass": (_i, [_vp, _i]),
     "cg_kernels_launched": (C.c_longlong, [_vp]),
     "cg_vertex_create": (_i, [_i, _vp, _vp, _i, _i, C.POINTER(_vp)]),

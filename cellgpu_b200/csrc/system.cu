@@ -209,6 +209,11 @@ struct cg_system {
     std::vector<GraphEntry> graphs;
     long long kernels_enqueued = 0;  // kernels of this library launched for this system
     double *noise_buf = nullptr;     // staging for host-supplied noise (one step)
+    // asynchronous host-buffer steps: copy stream, a second staging buffer, per-buffer events
+    cudaStream_t copy_stream = nullptr;
+    double *noise_buf2 = nullptr;
+    cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_consumed[2] = {nullptr, nullptr};
+    int host_slot = 0;
     // vertex model (model == CG_MODEL_VERTEX): pos/F are per vertex, AP/APpref/theta/motility per cell
     int Nv = 0, vmax = 0;
     int *vert_inst = nullptr, *vn = nullptr, *vcn = nullptr, *cvn = nullptr, *cv = nullptr;
@@ -394,6 +399,11 @@ extern "C" int cg_destroy(cg_system *s)
     for (auto &g : s->graphs) cudaGraphExecDestroy(g.exec);
     for (void *p : s->allocs) cudaFree(p);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+    for (int i = 0; i < 2; ++i) {
+        if (s->ev_copied[i]) cudaEventDestroy(s->ev_copied[i]);
+        if (s->ev_consumed[i]) cudaEventDestroy(s->ev_consumed[i]);
+    }
     if (s->body_stream) cudaStreamDestroy(s->body_stream);
     delete s;
     return CG_OK;
@@ -898,6 +908,45 @@ extern "C" int cg_spp_step_host(cg_system *s, const double *host_noise, double d
         return set_err(CG_ERR_STATE, "step halted for a global rebuild; state restored, step not taken");
     }
     return CG_OK;
+}
+
+extern "C" int cg_spp_enqueue_host(cg_system *s, const double *host_noise, double dt, double mu,
+                                   double *host_energy)
+{
+    if (!s || s->model != CG_MODEL_VORONOI || !host_noise) return set_err(CG_ERR_ARG, "bad args");
+    if (!s->topology_valid) CG_TRY(triangulate_sys(s));
+    if (!s->copy_stream) {
+        CG_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; ++i) {
+            CG_CUDA(cudaEventCreateWithFlags(&s->ev_copied[i], cudaEventDisableTiming));
+            CG_CUDA(cudaEventCreateWithFlags(&s->ev_consumed[i], cudaEventDisableTiming));
+        }
+        CG_TRY(dalloc(s, &s->noise_buf2, s->N));
+    }
+    int slot = s->host_slot;
+    s->host_slot ^= 1;
+    double *buf = slot ? s->noise_buf2 : s->noise_buf;
+    // the buffer is free once the step that last read it has run (no-op before its first use)
+    CG_CUDA(cudaStreamWaitEvent(s->copy_stream, s->ev_consumed[slot], 0));
+    CG_CUDA(cudaMemcpyAsync(buf, host_noise, sizeof(double) * s->N, cudaMemcpyHostToDevice, s->copy_stream));
+    CG_CUDA(cudaEventRecord(s->ev_copied[slot], s->copy_stream));
+    CG_CUDA(cudaStreamWaitEvent(s->stream, s->ev_copied[slot], 0));
+    int st = s->precision == CG_FP64 ? enqueue_graph<double>(s, 1, dt, mu, buf)
+                                     : enqueue_graph<float>(s, 1, dt, mu, buf);
+    if (st) return st;
+    CG_CUDA(cudaEventRecord(s->ev_consumed[slot], s->stream));
+    if (host_energy) {
+        VoroArgs a = sys_args(s);
+        CG_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * s->n_inst, s->stream));
+        if (s->precision == CG_FP64)
+            k_energy<double><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
+        else
+            k_energy<float><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
+        s->kernels_enqueued += 1;
+        CG_CUDA(cudaMemcpyAsync(host_energy, s->d_energy, sizeof(double) * s->n_inst, cudaMemcpyDeviceToHost,
+                                s->stream));
+    }
+    return check_launch();
 }
 
 // poll: synchronise, report completed steps and whether the device halted; recover if asked

@@ -189,9 +189,17 @@ int cg_spp_run(cg_system *sys, int n_steps, double dt, double mu, const double *
  * the remaining enqueued steps do nothing; cg_poll reports completed steps and recovers. */
 int cg_spp_enqueue(cg_system *sys, int n_steps, double dt, double mu);
 int cg_poll(cg_system *sys, int *steps_done, int *halted, int recover_if_halted);
-/* One step through host buffers: host_noise (N normals) is copied in, the per-instance energies
- * after the step are copied out to host_energy (may be NULL); returns when they are available. */
+/* One step through host buffers: host_noise (N normals) is copied in, the per-instance energies of
+ * the step's force evaluation (the configuration at the start of the step) are copied out to
+ * host_energy (may be NULL); returns when they are available. */
 int cg_spp_step_host(cg_system *sys, const double *host_noise, double dt, double mu, double *host_energy);
+/* The same step, asynchronous: host_noise (N normals; pinned memory, or the copy is staged by the
+ * driver) is copied on the system's copy stream into one of two device buffers, so the copy for the
+ * next step overlaps this one; the step waits for its copy; host_energy (may be NULL) receives the
+ * per-instance energies. Nothing is synchronised: both host buffers must stay
+ * untouched until the step has completed (cg_poll, cg_synchronize, or an event recorded on the
+ * system stream). Energies are those of cg_spp_step_host. Halts behave as for cg_spp_enqueue. */
+int cg_spp_enqueue_host(cg_system *sys, const double *host_noise, double dt, double mu, double *host_energy);
 /* The fused geometry + force (+ exact Delaunay test) pass alone, enqueued without synchronisation. */
 int cg_launch_force_pass(cg_system *sys, int with_test);
 /* number of this library's kernels launched for the system so far, graph replays and the repair

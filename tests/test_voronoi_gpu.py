@@ -191,6 +191,33 @@ def test_spp_free_run_matches_oracle(cglib, oracle, torch, nx, ny, steps, v0, dt
         assert b.counters()["rows_changed"] > 0
 
 
+def test_enqueue_host_matches_oracle(cglib, oracle, torch):
+    """The asynchronous host-buffer step (noise copied from pinned host memory on a copy stream,
+    double-buffered; energy copied back every step) follows the oracle like the device-noise run."""
+    pos, box = jittered_lattice(20, 24, 0.25, 9)
+    N = len(pos)
+    steps = 12
+    b, theta, mot, pref, rng = _spp_setup(pos, box, 12, v0=0.1)
+    noise = torch.from_numpy(rng.normal(size=(steps, N))).pin_memory()
+    energy = torch.zeros((steps, 1), dtype=torch.float64).pin_memory()
+    lib = b._lib
+    for i in range(steps):
+        assert lib.cg_spp_enqueue_host(b.handle, C.c_void_p(noise[i].data_ptr()), 0.01, 1.0,
+                                       C.c_void_p(energy[i].data_ptr())) == 0
+    done, halted = C.c_int(0), C.c_int(0)
+    assert lib.cg_poll(b.handle, C.byref(done), C.byref(halted), 1) == 0
+    assert not halted.value
+    # each step reports the energy of the configuration its forces were computed on
+    E_last = b.energies()[0]
+    assert abs(energy[-1, 0].item() - E_last) <= 1e-12 * max(1.0, abs(E_last))
+    assert np.all(np.diff(energy.numpy()[:, 0]) != 0)
+    b.enforce_topology()
+    onn, onbr = oracle.periodic_delaunay(pos, box, 16)
+    opos, oth = pos.copy(), theta.copy()
+    F, _ = oracle.voronoi_spp_run(opos, box, onn, onbr, oth, mot, pref, noise.numpy(), dt=0.01)
+    assert np.abs(b.positions() - opos).max() < 1e-9
+
+
 def test_mixed_precision_force_error(cglib, oracle):
     """Mixed precision (FP32 energy derivatives and contractions relative to each cell, FP64 vertex
     geometry, positions and predicates) against FP64 on the same state: on raw random points and
