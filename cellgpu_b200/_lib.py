@@ -64,6 +64,7 @@ SIGNATURES = {
     "cg_compute_forces": (_i, [_vp]),
     "cg_enforce_topology": (_i, [_vp]),
     "cg_set_seed": (_i, [_vp, _u64]),
+    "cg_set_instance_seeds": (_i, [_vp, _vp]),
     "cg_spp_run": (_i, [_vp, _i, _d, _d, _vp]),
     "cg_counters": (_i, [_vp, C.POINTER(C.c_longlong), _i]),
     "cg_get_stream": (_vp, [_vp]),
@@ -75,6 +76,7 @@ SIGNATURES = {
     "cg_kernels_launched": (C.c_longlong, [_vp]),
     "cg_vertex_create": (_i, [_i, _vp, _vp, _i, _i, C.POINTER(_vp)]),
     "cg_vertex_footprint": (_sz, [_i, _vp, _i]),
+    "cg_device_memory": (_i, [_vp, _vp]),
     "cg_get_vertex_topology": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cg_set_vertex_topology": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cg_vertex_from_voronoi": (_i, [_vp, _vp]),

@@ -25,8 +25,18 @@ struct Inst {
     int bin_off, nbx, nby;  // cell-list bins of this instance
     double bsx, bsy;    // bin sides
     int voff, nv;       // vertex-model vertices (off/n are cells)
-    int pad0, pad1;
+    unsigned long long seed;  // Philox key of the instance's device noise (counters are local indices)
 };
+
+// SplitMix64 finaliser (G. Steele, D. Lea, C. Flood, "Fast splittable pseudorandom number
+// generators", OOPSLA 2014): decorrelated per-instance keys from one seed and the instance index.
+CG_HD unsigned long long mix_seed(unsigned long long seed, unsigned long long index)
+{
+    unsigned long long z = seed + (index + 1ull) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
 
 // gpubox::minDist for a rectangular box (inc/utility/gpubox.h:154-165). The while loops and
 // half-box thresholds are kept so the FP64 result is bit-identical to the reference's. Inputs far

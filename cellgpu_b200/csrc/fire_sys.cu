@@ -9,9 +9,11 @@ static int fire_alloc(cg_system *s)
     s->fire_st = fs;
     CG_TRY(dalloc(s, &s->fire_dofinst, ndof(s)));
     if (s->model == CG_MODEL_VORONOI) {
-        CG_CUDA(cudaMemcpy(s->fire_dofinst, s->cell_inst, sizeof(int) * s->N, cudaMemcpyDeviceToDevice));
+        CG_CUDA(cudaMemcpyAsync(s->fire_dofinst, s->cell_inst, sizeof(int) * s->N, cudaMemcpyDeviceToDevice,
+                                s->stream));
     } else {
-        CG_CUDA(cudaMemcpy(s->fire_dofinst, s->vert_inst, sizeof(int) * s->Nv, cudaMemcpyDeviceToDevice));
+        CG_CUDA(cudaMemcpyAsync(s->fire_dofinst, s->vert_inst, sizeof(int) * s->Nv, cudaMemcpyDeviceToDevice,
+                                s->stream));
     }
     return CG_OK;
 }

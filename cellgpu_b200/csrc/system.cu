@@ -157,8 +157,8 @@ extern "C" int cg_spp_step(double *pos, double *theta, const double *F, const do
     a.theta = theta;
     a.F = (void *)F;
     a.motility = (const double2 *)motility;
-    (void)step;
-    k_spp<double><<<nblk((N + 1) / 2, 256), 256, 0, stream>>>(a, noise, dt, mu, seed, 0);
+    a.inst0.seed = seed;
+    k_spp<double><<<nblk((N + 1) / 2, 256), 256, 0, stream>>>(a, noise, dt, mu, step, 0);
     return check_launch();
 }
 
@@ -227,17 +227,52 @@ struct cg_system {
 
 static int ndof(const cg_system *s) { return s->model == CG_MODEL_VERTEX ? s->Nv : s->N; }
 
+// Device memory of a system comes from the stream-ordered allocator on the system's stream, and
+// is freed the same way: creating or destroying a system never synchronises the device, so
+// systems served concurrently on other streams keep running.
 template <typename T>
 static int dalloc(cg_system *s, T **p, size_t count)
 {
     size_t b = std::max<size_t>(count, 1) * sizeof(T);
     void *q = nullptr;
-    CG_CUDA(cudaMalloc(&q, b));
-    CG_CUDA(cudaMemset(q, 0, b));
+    CG_CUDA(cudaMallocAsync(&q, b, s->stream));
     s->allocs.push_back(q);
     s->bytes += b;
+    CG_CUDA(cudaMemsetAsync(q, 0, b, s->stream));
     *p = (T *)q;
     return CG_OK;
+}
+
+// streams of a new system (before any allocation)
+static int sys_streams(cg_system *s)
+{
+    CG_CUDA(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking));
+    CG_CUDA(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
+    s->stream = s->own_stream;
+    return CG_OK;
+}
+
+// release everything a system holds (also on a failed creation)
+static void sys_release(cg_system *s)
+{
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto &g : s->graphs) cudaGraphExecDestroy(g.exec);
+    s->graphs.clear();
+    cudaStream_t fs = s->own_stream;
+    for (void *p : s->allocs) {
+        if (fs) cudaFreeAsync(p, fs);
+        else cudaFree(p);
+    }
+    s->allocs.clear();
+    if (fs) cudaStreamSynchronize(fs);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+    for (int i = 0; i < 2; ++i) {
+        if (s->ev_copied[i]) cudaEventDestroy(s->ev_copied[i]);
+        if (s->ev_consumed[i]) cudaEventDestroy(s->ev_consumed[i]);
+    }
+    if (s->body_stream) cudaStreamDestroy(s->body_stream);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    delete s;
 }
 
 static VoroArgs sys_args(cg_system *s)
@@ -315,6 +350,7 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
             return set_err(CG_ERR_ARG, "instance needs >= 8 cells and a positive box");
         }
         Inst in = make_inst(box[2 * i], box[2 * i + 1], off, N[i], boff, BIN_TARGET);
+        in.seed = mix_seed(s->seed, (unsigned long long)i);
         s->h_inst.push_back(in);
         for (int c = 0; c < N[i]; ++c) s->h_cell_inst.push_back(i);
         off += N[i];
@@ -324,7 +360,11 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
     s->n_bins = boff;
     int Nt = s->N;
     size_t r2 = precision == CG_FP64 ? sizeof(double2) : sizeof(float2);
-    int st = CG_OK;
+    int st = sys_streams(s);
+    if (st != CG_OK) {
+        sys_release(s);
+        return st;
+    }
     do {
         if ((st = dalloc(s, &s->inst, n_inst))) break;
         if ((st = dalloc(s, &s->cell_inst, Nt))) break;
@@ -359,33 +399,26 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
         if ((st = dalloc(s, (char **)&s->scan_tmp, tmpb))) break;
     } while (0);
     if (st != CG_OK) {
-        for (void *p : s->allocs) cudaFree(p);
-        delete s;
+        sys_release(s);
         return st;
     }
-    cudaMemcpy(s->inst, s->h_inst.data(), sizeof(Inst) * n_inst, cudaMemcpyHostToDevice);
-    cudaMemcpy(s->cell_inst, s->h_cell_inst.data(), sizeof(int) * Nt, cudaMemcpyHostToDevice);
+    cudaStream_t str = s->stream;
+    cudaMemcpyAsync(s->inst, s->h_inst.data(), sizeof(Inst) * n_inst, cudaMemcpyHostToDevice, str);
+    cudaMemcpyAsync(s->cell_inst, s->h_cell_inst.data(), sizeof(int) * Nt, cudaMemcpyHostToDevice, str);
     // defaults of the reference: A0 = 1, P0 = 3.8 (Simple2DCell::initializeSimple2DCell,
     // src/models/Simple2DCell.cpp:27), v0 = 0.05, Dr = 1 (VoronoiQuadraticEnergy(n,A0,P0,..),
     // src/models/voronoiQuadraticEnergy.cpp:34)
     std::vector<double2> pref(Nt, make_double2(1.0, 3.8)), mot(Nt, make_double2(0.05, 1.0));
-    cudaMemcpy(s->APpref, pref.data(), sizeof(double2) * Nt, cudaMemcpyHostToDevice);
-    cudaMemcpy(s->motility, mot.data(), sizeof(double2) * Nt, cudaMemcpyHostToDevice);
-    if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
-        for (void *p : s->allocs) cudaFree(p);
-        delete s;
-        return set_err(CG_ERR_CUDA, "stream creation failed");
-    }
-    s->stream = s->own_stream;
-    cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking);
+    cudaMemcpyAsync(s->APpref, pref.data(), sizeof(double2) * Nt, cudaMemcpyHostToDevice, str);
+    cudaMemcpyAsync(s->motility, mot.data(), sizeof(double2) * Nt, cudaMemcpyHostToDevice, str);
     Ctl c0;
     memset(&c0, 0, sizeof(c0));
     c0.epoch = 1;
-    cudaMemcpy(s->ctl, &c0, sizeof(Ctl), cudaMemcpyHostToDevice);
-    cudaError_t e = cudaDeviceSynchronize();
+    cudaMemcpyAsync(s->ctl, &c0, sizeof(Ctl), cudaMemcpyHostToDevice, str);
+    cudaError_t e = cudaStreamSynchronize(str);  // host staging above must outlive the copies
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) {
-        for (void *p : s->allocs) cudaFree(p);
-        delete s;
+        sys_release(s);
         return set_err(CG_ERR_CUDA, cudaGetErrorString(e));
     }
     *out = s;
@@ -395,17 +428,7 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
 extern "C" int cg_destroy(cg_system *s)
 {
     if (!s) return CG_OK;
-    cudaStreamSynchronize(s->stream);
-    for (auto &g : s->graphs) cudaGraphExecDestroy(g.exec);
-    for (void *p : s->allocs) cudaFree(p);
-    if (s->own_stream) cudaStreamDestroy(s->own_stream);
-    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
-    for (int i = 0; i < 2; ++i) {
-        if (s->ev_copied[i]) cudaEventDestroy(s->ev_copied[i]);
-        if (s->ev_consumed[i]) cudaEventDestroy(s->ev_consumed[i]);
-    }
-    if (s->body_stream) cudaStreamDestroy(s->body_stream);
-    delete s;
+    sys_release(s);
     return CG_OK;
 }
 
@@ -414,6 +437,15 @@ extern "C" int cg_num_dofs(const cg_system *s) { return s ? ndof(s) : 0; }
 extern "C" int cg_num_instances(const cg_system *s) { return s ? s->n_inst : 0; }
 extern "C" int cg_neighbor_capacity(const cg_system *s) { return s ? s->K : 0; }
 extern "C" size_t cg_device_bytes(const cg_system *s) { return s ? s->bytes : 0; }
+
+extern "C" int cg_device_memory(size_t *free_bytes, size_t *total_bytes)
+{
+    size_t f = 0, t = 0;
+    CG_CUDA(cudaMemGetInfo(&f, &t));
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
+    return CG_OK;
+}
 
 extern "C" int cg_set_stream(cg_system *s, cudaStream_t stream)
 {
@@ -484,11 +516,28 @@ extern "C" int cg_get_directors(cg_system *s, double *t)
     if (!s || !t) return set_err(CG_ERR_ARG, "bad args");
     return d2h(s, t, s->theta, sizeof(double) * s->N);
 }
+// per-instance Philox keys live in the device instance table, so graphs never capture a seed
+static int upload_inst(cg_system *s)
+{
+    CG_CUDA(cudaMemcpyAsync(s->inst, s->h_inst.data(), sizeof(Inst) * s->n_inst, cudaMemcpyHostToDevice,
+                            s->stream));
+    CG_CUDA(cudaStreamSynchronize(s->stream));
+    return CG_OK;
+}
+
 extern "C" int cg_set_seed(cg_system *s, uint64_t seed)
 {
     if (!s) return set_err(CG_ERR_ARG, "bad args");
     s->seed = seed;
-    return CG_OK;
+    for (int i = 0; i < s->n_inst; ++i) s->h_inst[i].seed = mix_seed(seed, (unsigned long long)i);
+    return upload_inst(s);
+}
+
+extern "C" int cg_set_instance_seeds(cg_system *s, const uint64_t *seeds)
+{
+    if (!s || !seeds) return set_err(CG_ERR_ARG, "bad args");
+    for (int i = 0; i < s->n_inst; ++i) s->h_inst[i].seed = seeds[i];
+    return upload_inst(s);
 }
 
 static int get_real2(cg_system *s, const void *src, double *dst, int n)
@@ -731,7 +780,7 @@ static void enqueue_spp_steps(cg_system *s, int n, double dt, double mu, const d
         launch_force_test<R>(s, a, true);
         launch_repair<R>(s, a, true);
         const double *nz = noise ? (noise_per_step ? noise + (size_t)t * s->N : noise) : nullptr;
-        k_spp<R><<<nblk((s->N + 1) / 2, 256), 256, 0, s->stream>>>(a, nz, dt, mu, s->seed, 0);
+        k_spp<R><<<nblk((s->N + 1) / 2, 256), 256, 0, s->stream>>>(a, nz, dt, mu, 0u, 0);
         k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
         s->kernels_enqueued += 2;
     }
@@ -768,7 +817,7 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
         for (int t = 0; t < n; ++t) {
             launch_force_test<R>(s, a, true);
             launch_repair<R>(s, a, true);
-            k_spp<R><<<nblk((s->N + 1) / 2, 256), 256, 0, s->stream>>>(a, noise, dt, mu, s->seed, 0);
+            k_spp<R><<<nblk((s->N + 1) / 2, 256), 256, 0, s->stream>>>(a, noise, dt, mu, 0u, 0);
             k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
             s->kernels_enqueued += 2;
         }
@@ -802,7 +851,7 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
         deps.assign(1, cn);
         CG_CUDA(cudaStreamBeginCaptureToGraph(s->stream, graph, deps.data(), nullptr, deps.size(), mode));
         const double *nz = noise;
-        k_spp<R><<<nblk((s->N + 1) / 2, 256), 256, 0, s->stream>>>(a, nz, dt, mu, s->seed, 0);
+        k_spp<R><<<nblk((s->N + 1) / 2, 256), 256, 0, s->stream>>>(a, nz, dt, mu, 0u, 0);
         k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
         s->kernels_enqueued += 2;
         st = capture_deps(s->stream);

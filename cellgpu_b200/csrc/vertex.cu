@@ -79,7 +79,7 @@ __global__ void k_vm_forces(VertArgs a, int scatter)
 // brownianParticleDynamics::integrateEquationsOfMotionCPU (src/updaters/brownianParticleDynamics.cpp:92-109)
 // + vertexModelBase::moveDegreesOfFreedom (src/models/vertexModelBase.cpp:11-47):
 // d = xi sqrt(2 dt T mu) + dt mu F, two normals per vertex (x then y)
-__global__ void k_vm_brownian(VertArgs a, const double *noise2, double dt, double mu, double T, uint64_t seed)
+__global__ void k_vm_brownian(VertArgs a, const double *noise2, double dt, double mu, double T)
 {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= a.Nv) return;
@@ -90,7 +90,8 @@ __global__ void k_vm_brownian(VertArgs a, const double *noise2, double dt, doubl
         r1 = noise2[2 * (size_t)v];
         r2 = noise2[2 * (size_t)v + 1];
     } else {
-        double2 g = normal2(seed, (uint32_t)v, a.ctl ? (uint32_t)a.ctl->step : 0u, 1u);
+        // counter = the vertex's index within its instance, key = the instance's seed
+        double2 g = normal2(in.seed, (uint32_t)(v - in.voff), a.ctl ? (uint32_t)a.ctl->step : 0u, 1u);
         r1 = g.x;
         r2 = g.y;
     }
@@ -131,12 +132,18 @@ __global__ void k_vm_spp_vertices(VertArgs a, double dt, double mu)
     a.vpos[v] = put_in_box(p, in.Lx, in.Ly, in.iLx, in.iLy);
 }
 
-__global__ void k_vm_spp_directors(VertArgs a, const double *noise, double dt, uint64_t seed)
+__global__ void k_vm_spp_directors(VertArgs a, const double *noise, double dt)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a.Nc) return;
     if (a.ctl && a.ctl->halt) return;
-    double xi = noise ? noise[c] : normal2(seed, (uint32_t)c, a.ctl ? (uint32_t)a.ctl->step : 0u, 2u).x;
+    double xi;
+    if (noise) {
+        xi = noise[c];
+    } else {
+        const Inst &in = a.inst[a.cell_inst[c]];
+        xi = normal2(in.seed, (uint32_t)(c - in.off), a.ctl ? (uint32_t)a.ctl->step : 0u, 2u).x;
+    }
     a.theta[c] = __dadd_rn(a.theta[c], __dmul_rn(xi, sqrt(__dmul_rn(__dmul_rn(2.0, dt), a.motility[c].y))));
 }
 

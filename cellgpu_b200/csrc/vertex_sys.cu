@@ -66,6 +66,7 @@ extern "C" int cg_vertex_create(int n_inst, const int *Nc, const double *box, in
         Inst in = make_inst(box[2 * i], box[2 * i + 1], off, Nc[i], 0, BIN_TARGET);
         in.voff = 2 * off;
         in.nv = 2 * Nc[i];
+        in.seed = mix_seed(s->seed, (unsigned long long)i);
         s->h_inst.push_back(in);
         for (int c = 0; c < Nc[i]; ++c) s->h_cell_inst.push_back(i);
         for (int v = 0; v < 2 * Nc[i]; ++v) vinst.push_back(i);
@@ -73,7 +74,11 @@ extern "C" int cg_vertex_create(int n_inst, const int *Nc, const double *box, in
     }
     s->N = off;
     s->Nv = 2 * off;
-    int st = CG_OK;
+    int st = sys_streams(s);
+    if (st != CG_OK) {
+        sys_release(s);
+        return st;
+    }
     do {
         if ((st = dalloc(s, &s->inst, n_inst))) break;
         if ((st = dalloc(s, &s->cell_inst, s->N))) break;
@@ -95,29 +100,24 @@ extern "C" int cg_vertex_create(int n_inst, const int *Nc, const double *box, in
         if ((st = dalloc(s, &s->noise_buf, 2 * (size_t)s->Nv))) break;
     } while (0);
     if (st != CG_OK) {
-        for (void *p : s->allocs) cudaFree(p);
-        delete s;
+        sys_release(s);
         return st;
     }
-    cudaMemcpy(s->inst, s->h_inst.data(), sizeof(Inst) * n_inst, cudaMemcpyHostToDevice);
-    cudaMemcpy(s->cell_inst, s->h_cell_inst.data(), sizeof(int) * s->N, cudaMemcpyHostToDevice);
-    cudaMemcpy(s->vert_inst, vinst.data(), sizeof(int) * s->Nv, cudaMemcpyHostToDevice);
+    cudaStream_t str = s->stream;
+    cudaMemcpyAsync(s->inst, s->h_inst.data(), sizeof(Inst) * n_inst, cudaMemcpyHostToDevice, str);
+    cudaMemcpyAsync(s->cell_inst, s->h_cell_inst.data(), sizeof(int) * s->N, cudaMemcpyHostToDevice, str);
+    cudaMemcpyAsync(s->vert_inst, vinst.data(), sizeof(int) * s->Nv, cudaMemcpyHostToDevice, str);
     std::vector<double2> pref(s->N, make_double2(1.0, 3.8)), mot(s->N, make_double2(0.05, 1.0));
-    cudaMemcpy(s->APpref, pref.data(), sizeof(double2) * s->N, cudaMemcpyHostToDevice);
-    cudaMemcpy(s->motility, mot.data(), sizeof(double2) * s->N, cudaMemcpyHostToDevice);
-    if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
-        for (void *p : s->allocs) cudaFree(p);
-        delete s;
-        return set_err(CG_ERR_CUDA, "stream creation failed");
-    }
-    s->stream = s->own_stream;
+    cudaMemcpyAsync(s->APpref, pref.data(), sizeof(double2) * s->N, cudaMemcpyHostToDevice, str);
+    cudaMemcpyAsync(s->motility, mot.data(), sizeof(double2) * s->N, cudaMemcpyHostToDevice, str);
     Ctl c0;
     memset(&c0, 0, sizeof(c0));
     c0.epoch = 1;
-    cudaMemcpy(s->ctl, &c0, sizeof(Ctl), cudaMemcpyHostToDevice);
-    cudaError_t e = cudaDeviceSynchronize();
+    cudaMemcpyAsync(s->ctl, &c0, sizeof(Ctl), cudaMemcpyHostToDevice, str);
+    cudaError_t e = cudaStreamSynchronize(str);  // host staging above must outlive the copies
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) {
-        cg_destroy(s);
+        sys_release(s);
         return set_err(CG_ERR_CUDA, cudaGetErrorString(e));
     }
     *out = s;
@@ -173,9 +173,10 @@ extern "C" int cg_vertex_from_voronoi(cg_system *s, const double *cell_pos)
     int st = cg_set_positions(v, cell_pos);
     if (st == CG_OK) st = triangulate_sys(v);
     int *owned = nullptr, *tri = nullptr;
+    cudaStream_t str = s->stream;
     if (st == CG_OK) {
-        if (cudaMalloc(&owned, sizeof(int) * (s->N + 1)) != cudaSuccess ||
-            cudaMalloc(&tri, sizeof(int) * (size_t)s->N * K) != cudaSuccess)
+        if (cudaMallocAsync(&owned, sizeof(int) * (s->N + 1), str) != cudaSuccess ||
+            cudaMallocAsync(&tri, sizeof(int) * (size_t)s->N * K, str) != cudaSuccess)
             st = set_err(CG_ERR_CUDA, "allocation failed");
     }
     if (st == CG_OK) {
@@ -197,14 +198,13 @@ extern "C" int cg_vertex_from_voronoi(cg_system *s, const double *cell_pos)
         d.cvn = s->cvn;
         d.cv = s->cv;
         d.status = v->d_status;
-        cudaStream_t str = s->stream;
         cudaMemsetAsync(v->d_status, 0, sizeof(int), str);
         k_dual_count<<<nblk(s->N, 256), 256, 0, str>>>(d);
         cudaMemsetAsync(owned + s->N, 0, sizeof(int), str);
         size_t tmpb = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, tmpb, owned, owned, s->N + 1);
         void *tmp = nullptr;
-        if (cudaMalloc(&tmp, tmpb + 16) != cudaSuccess) st = set_err(CG_ERR_CUDA, "allocation failed");
+        if (cudaMallocAsync(&tmp, tmpb + 16, str) != cudaSuccess) st = set_err(CG_ERR_CUDA, "allocation failed");
         if (st == CG_OK) {
             cub::DeviceScan::ExclusiveSum(tmp, tmpb, owned, owned, s->N + 1, str);
             k_dual_assign<<<nblk(s->N, 256), 256, 0, str>>>(d);
@@ -217,11 +217,12 @@ extern "C" int cg_vertex_from_voronoi(cg_system *s, const double *cell_pos)
             if (e != cudaSuccess) st = set_err(CG_ERR_CUDA, cudaGetErrorString(e));
             else if (h_status) st = set_err(h_status, "vertex initialisation failed");
             else if (total != s->Nv) st = set_err(CG_ERR_TOPOLOGY, "number of Delaunay triangles != 2N");
-            cudaFree(tmp);
+            cudaFreeAsync(tmp, str);
         }
     }
-    if (owned) cudaFree(owned);
-    if (tri) cudaFree(tri);
+    if (owned) cudaFreeAsync(owned, str);
+    if (tri) cudaFreeAsync(tri, str);
+    cudaStreamSynchronize(str);
     cg_destroy(v);
     if (st == CG_OK) s->topology_valid = true;
     return st;
@@ -273,12 +274,12 @@ static void vm_enqueue_step(cg_system *s, int kind, int t, double dt, double mu,
     k_vm_forces<<<nblk(s->N, 128), 128, 0, s->stream>>>(a, 1);
     if (kind == 0) {
         const double *nz = noise ? (per_step_noise ? noise + (size_t)t * 2 * s->Nv : noise) : nullptr;
-        k_vm_brownian<<<nblk(s->Nv, 256), 256, 0, s->stream>>>(a, nz, dt, mu, T, s->seed);
+        k_vm_brownian<<<nblk(s->Nv, 256), 256, 0, s->stream>>>(a, nz, dt, mu, T);
         s->kernels_enqueued += 2;
     } else {
         const double *nz = noise ? (per_step_noise ? noise + (size_t)t * s->N : noise) : nullptr;
         k_vm_spp_vertices<<<nblk(s->Nv, 256), 256, 0, s->stream>>>(a, dt, mu);
-        k_vm_spp_directors<<<nblk(s->N, 256), 256, 0, s->stream>>>(a, nz, dt, s->seed);
+        k_vm_spp_directors<<<nblk(s->N, 256), 256, 0, s->stream>>>(a, nz, dt);
         s->kernels_enqueued += 3;
     }
     vm_launch_t1(s, a);

@@ -1220,10 +1220,21 @@ CG_D void spp_cell(const VoroArgs &a, int c, double xi, double dt, double mu, in
     if (zero_force) reinterpret_cast<typename Vec2<R>::T *>(a.F)[c] = mk<R>(R(0), R(0));
 }
 
-// Two cells per thread: one Box-Muller pair (Philox counter = (cell pair, step)) serves both when
-// the noise is generated on the device.
+// device noise of cell c: component (l & 1) of the Box-Muller pair with Philox counter
+// (l >> 1, step), key = the instance's seed, l = the cell's index within its instance -- so a cell's
+// noise does not depend on where its instance sits in a batch
+CG_D double2 cell_pair_noise(const VoroArgs &a, int c, uint32_t step, int &local)
+{
+    const Inst &in = inst_of(a, c);
+    local = c - in.off;
+    return normal2(in.seed, (uint32_t)(local >> 1), step, 0u);
+}
+
+// Two cells per thread: one Box-Muller pair serves both when they are consecutive cells of one
+// instance (the usual case) and the noise is generated on the device. step0 is the step counter
+// when there is no control block (raw caller).
 template <typename R>
-__global__ void k_spp(VoroArgs a, const double *noise, double dt, double mu, uint64_t seed,
+__global__ void k_spp(VoroArgs a, const double *noise, double dt, double mu, uint32_t step0,
                       int zero_force)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1236,8 +1247,20 @@ __global__ void k_spp(VoroArgs a, const double *noise, double dt, double mu, uin
     if (noise) {
         xi = make_double2(noise[c0], two ? noise[c0 + 1] : 0.0);
     } else {
-        uint32_t step = ctl ? (uint32_t)ctl->step : 0u;
-        xi = normal2(seed, (uint32_t)t, step, 0u);
+        uint32_t step = ctl ? (uint32_t)ctl->step : step0;
+        int l0, l1;
+        double2 g0 = cell_pair_noise(a, c0, step, l0);
+        xi.x = (l0 & 1) ? g0.y : g0.x;
+        xi.y = 0.0;
+        if (two) {
+            const Inst &i0 = inst_of(a, c0);
+            if (!(l0 & 1) && c0 + 1 < i0.off + i0.n) {
+                xi.y = g0.y;
+            } else {
+                double2 g1 = cell_pair_noise(a, c0 + 1, step, l1);
+                xi.y = (l1 & 1) ? g1.y : g1.x;
+            }
+        }
     }
     spp_cell<R>(a, c0, xi.x, dt, mu, zero_force);
     if (two) spp_cell<R>(a, c0 + 1, xi.y, dt, mu, zero_force);

@@ -94,6 +94,14 @@ class VoronoiBatch:
     def set_seed(self, seed):
         check(self._lib.cg_set_seed(self._h, int(seed) & (2**64 - 1)))
 
+    def set_instance_seeds(self, seeds):
+        """Philox key of each instance's device noise (its noise is then independent of where the
+        instance sits in a batch)."""
+        arr = np.ascontiguousarray([int(x) & (2**64 - 1) for x in seeds], dtype=np.uint64)
+        if len(arr) != len(self.N):
+            raise ValueError("one seed per instance")
+        check(self._lib.cg_set_instance_seeds(self._h, arr.ctypes.data))
+
     def forces(self):
         out = np.zeros((self.Ntot, 2))
         check(self._lib.cg_get_forces(self._h, ptr(out)))

@@ -142,6 +142,8 @@ size_t cg_device_bytes(const cg_system *sys);
 /* bytes a system of this shape would hold on the device (admission control) */
 size_t cg_voronoi_footprint(int n_inst, const int *N, int K);
 size_t cg_vertex_footprint(int n_inst, const int *Nc, int vmax);
+/* free and total device memory of the current device (admission budgets) */
+int cg_device_memory(size_t *free_bytes, size_t *total_bytes);
 
 /* host <-> device state (host buffers; copies are ordered on the system's stream and complete
  * before return for get_*) */
@@ -182,7 +184,12 @@ int cg_enforce_topology(cg_system *sys);  /* Voronoi: test+repair; vertex: T1 sw
 /* dynamics: n_steps integrator steps, each = forces, integrate, move, topology.
  * noise == NULL: counter-based RNG with the system seed; else a device pointer with n_steps blocks of
  * per-step normals (SPP: N per step; Brownian: 2*Nv per step). */
+/* Device noise: instance i draws with Philox key seed_i and counters made of its local cell (or
+ * vertex) index and the step, so its noise does not depend on where it sits in a batch.
+ * cg_set_seed sets seed_i = SplitMix64(seed, i) (also the default, seed = 0x5eed);
+ * cg_set_instance_seeds sets every seed_i explicitly (n_inst values). */
 int cg_set_seed(cg_system *sys, uint64_t seed);
+int cg_set_instance_seeds(cg_system *sys, const uint64_t *seeds);
 int cg_spp_run(cg_system *sys, int n_steps, double dt, double mu, const double *noise_dev);
 /* Enqueue n_steps RNG-driven SPP steps (one CUDA graph replay) with no host synchronisation.
  * A step that cannot finish on the device (a global rebuild is needed) sets a sticky halt flag and

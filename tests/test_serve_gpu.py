@@ -1,0 +1,87 @@
+"""Serving (continuous batching): each request gives the same result alone and in a mix with other
+requests of every kind and size, and admission respects the memory budget.
+
+Tolerances (written here): SPP runs -- positions within 1e-9 (periodic minimum image), energies
+within 1e-10 relative (floating-point atomics are summed in another order in a larger batch);
+FIRE -- both runs reach the force threshold, energies within 1e-9 relative, positions within 1e-6.
+"""
+import copy
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests():
+    from cellgpu_b200.serve import Request
+    # the FIRE cases converge to 1e-10 on the oracle in 468 (Voronoi) and 1401 (vertex) iterations
+    return [Request("voronoi", "spp", 150, p0=3.75, seed=1, steps=60),
+            Request("voronoi", "fire", 130, p0=3.70, seed=2, fire_tol=1e-10, fire_max_iterations=8000),
+            Request("vertex", "spp", 110, p0=3.80, seed=3, steps=40),
+            Request("vertex", "fire", 130, p0=3.80, seed=2, fire_tol=1e-10, fire_max_iterations=8000)]
+
+
+def _fillers():
+    from cellgpu_b200.serve import Request
+    out = []
+    for i in range(3):
+        out.append(Request("voronoi", "spp", 90 + 40 * i, p0=3.85, seed=100 + i, steps=60))
+        out.append(Request("voronoi", "fire", 100 + 20 * i, p0=3.65, seed=200 + i, fire_tol=1e-10,
+                           fire_max_iterations=8000))
+        out.append(Request("vertex", "spp", 80 + 30 * i, p0=3.75, seed=300 + i, steps=40))
+        out.append(Request("vertex", "fire", 90 + 25 * i, p0=3.85, seed=400 + i, fire_tol=1e-10,
+                           fire_max_iterations=8000))
+    return out
+
+
+def _pdist(a, b, n):
+    L = np.sqrt(n)
+    d = a - b
+    d -= L * np.round(d / L)
+    return np.abs(d).max()
+
+
+def test_same_result_alone_and_in_mix(cglib):
+    from cellgpu_b200.serve import Server
+    reqs = _requests()
+    alone = []
+    for r in reqs:
+        with Server(lanes=1) as srv:
+            alone.append(srv.submit(copy.deepcopy(r)).result())
+    mix_in, where = [], []
+    fill = _fillers()
+    for i, r in enumerate(reqs):  # interleave: every batch kind holds several instances
+        mix_in.extend(fill[3 * i:3 * i + 3])
+        where.append(len(mix_in))
+        mix_in.append(copy.deepcopy(r))
+    with Server(lanes=3) as srv:
+        futs = srv.submit_many(mix_in)
+        mix = [f.result() for f in futs]
+    for r, a, k in zip(reqs, alone, where):
+        m = mix[k]
+        assert m.batch_requests > 1  # it really shared a batch
+        if r.task == "spp":
+            assert _pdist(a.positions, m.positions, r.n) < 1e-9
+            assert abs(a.energy - m.energy) <= 1e-10 * max(1.0, abs(a.energy))
+        else:
+            assert a.fmax <= r.fire_tol and m.fmax <= r.fire_tol
+            assert abs(a.energy - m.energy) <= 1e-9 * max(1.0, abs(a.energy))
+            assert _pdist(a.positions, m.positions, r.n) < 1e-6
+
+
+def test_admission_by_footprint(cglib):
+    """A budget that fits about one batch at a time: every request still completes, and the
+    resident footprint never exceeds the budget."""
+    from cellgpu_b200.serve import Request, Server, footprint
+    reqs = [Request("voronoi", "spp", 400 + 50 * i, seed=i, steps=20) for i in range(8)]
+    budget = footprint("voronoi", [max(r.n for r in reqs)]) * 2
+    with Server(lanes=4, memory_budget=budget) as srv:
+        res = [f.result() for f in srv.submit_many(reqs)]
+        peak = srv.peak_resident
+    assert len(res) == 8 and all(np.isfinite(r.energy) for r in res)
+    assert peak <= budget
+    with Server(lanes=1, memory_budget=1000) as srv:
+        fut = srv.submit(Request("voronoi", "spp", 500, seed=1, steps=5))
+        with pytest.raises(MemoryError):
+            fut.result()

@@ -254,23 +254,40 @@ def test_mixed_precision_force_error(cglib, oracle):
 
 
 def test_batch_equals_singles(cglib):
-    """Instances of a batch evolve exactly as they do alone (RNG counter = global cell index, so
-    single runs use the same offsets)."""
+    """Instances of a batch evolve as they do alone: forces per instance, and device-noise SPP runs
+    (each instance's noise is keyed by its own seed and local cell index, so where it sits in the
+    batch does not matter). Tolerance 1e-10 on positions after 20 steps (atomic summation order)."""
     from cellgpu_b200 import VoronoiBatch
-    Ns = [100, 257, 1000]
-    boxes = [(np.sqrt(n), np.sqrt(n)) for n in Ns]
-    poss = [monolayer(n, 40 + i)[0] for i, n in enumerate(Ns)]
+    shapes = [(10, 12), (16, 16), (20, 22)]
+    lat = [jittered_lattice(nx, ny, 0.25, 40 + i) for i, (nx, ny) in enumerate(shapes)]
+    poss = [p for p, _ in lat]
+    boxes = [bx for _, bx in lat]
+    Ns = [len(p) for p in poss]
+    seeds = [11, 22, 33]
+    rng = np.random.default_rng(5)
+    ths = [rng.uniform(0, 2 * np.pi, n) for n in Ns]
     b = VoronoiBatch(Ns, boxes)
     b.set_positions(np.concatenate(poss))
+    b.set_directors(np.concatenate(ths))
+    b.set_motility(np.tile([0.1, 1.0], (sum(Ns), 1)))
+    b.set_instance_seeds(seeds)
     b.triangulate()
     b.compute_forces()
     Fb = b.forces()
+    b.spp_run(20, dt=0.01)
+    Pb = b.positions()
     off = 0
     for i, n in enumerate(Ns):
-        s = _batch(poss[i], boxes[i])
+        s = VoronoiBatch([n], [boxes[i]])
+        s.set_positions(poss[i])
+        s.set_directors(ths[i])
+        s.set_motility(np.tile([0.1, 1.0], (n, 1)))
+        s.set_instance_seeds([seeds[i]])
         s.triangulate()
         s.compute_forces()
         assert force_error(Fb[off:off + n], s.forces()) < 1e-12
+        s.spp_run(20, dt=0.01)
+        assert np.abs(Pb[off:off + n] - s.positions()).max() < 1e-10
         off += n
 
 
