@@ -35,6 +35,28 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+CPP = os.path.join(HERE, "cpp")
+CPP_PROGRAMS = ["api_check", "voronoi_example"]
+CUDA_INCLUDE = os.environ.get("CUDA_INCLUDE", "/usr/local/cuda/include")
+
+
+def build_cpp(force: bool = False) -> list:
+    """The C++ class-API programs (cellgpu_b200/cpp), linked against the in-tree library."""
+    out = []
+    inc = os.path.join(HERE, "..", "include")
+    for name in CPP_PROGRAMS:
+        src = os.path.join(CPP, name + ".cpp")
+        exe = os.path.join(CPP, name)
+        deps = [src, os.path.join(CPP, "cellgpu.hpp"), LIB]
+        if force or not os.path.exists(exe) or any(os.path.getmtime(d) > os.path.getmtime(exe) for d in deps):
+            subprocess.check_call([os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-Wall", "-I", inc,
+                                   "-I", CUDA_INCLUDE, src, "-o", exe, "-L", HERE, "-lcellgpu_b200",
+                                   "-Wl,-rpath,$ORIGIN/.."])
+        out.append(exe)
+    return out
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    build_cpp(force="--force" in sys.argv)
     print(LIB)

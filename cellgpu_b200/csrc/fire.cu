@@ -50,12 +50,15 @@ __global__ void k_fire_vv1(FireArgs a)
     a.pos[i] = put_in_box(p, in.Lx, in.Ly, in.iLx, in.iLy);
 }
 
-// second half-kick with the new forces, then the FIRE reductions per instance (block-level
-// partial sums, one atomic per block and instance run)
-__global__ void k_fire_vv2(FireArgs a)
+// second half-kick with the new forces, then the FIRE reductions per instance. Degrees of freedom
+// of one instance are contiguous: a block that lies inside one (unconverged) instance reduces in
+// shared memory and adds once per quantity; other blocks reduce per warp where the warp is uniform
+// and per lane otherwise. (Launched with 256 threads.)
+__global__ void __launch_bounds__(256) k_fire_vv2(FireArgs a)
 {
+    __shared__ double s_red[4][8];
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a.ctl && a.ctl->halt) return;
+    if (a.ctl && a.ctl->halt) return;  // uniform across the grid
     int inst = -1;
     double P = 0, ff = 0, vv = 0, fm = 0;
     if (i < a.ndof) {
@@ -75,9 +78,40 @@ __global__ void k_fire_vv2(FireArgs a)
             inst = -1;
         }
     }
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int d0 = blockIdx.x * blockDim.x, d1 = min(a.ndof, d0 + (int)blockDim.x) - 1;
+    const int b0 = a.dof_inst[d0], b1 = a.dof_inst[d1];
+    if (b0 == b1 && !a.st[b0].converged) {  // uniform across the block
+        for (int off = 16; off > 0; off >>= 1) {
+            P += __shfl_down_sync(full, P, off);
+            ff += __shfl_down_sync(full, ff, off);
+            vv += __shfl_down_sync(full, vv, off);
+            fm = fmax(fm, __shfl_down_sync(full, fm, off));
+        }
+        if (lane == 0) {
+            s_red[0][w] = P;
+            s_red[1][w] = ff;
+            s_red[2][w] = vv;
+            s_red[3][w] = fm;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tp = 0, tf = 0, tv = 0, tm = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+                tp += s_red[0][k];
+                tf += s_red[1][k];
+                tv += s_red[2][k];
+                tm = fmax(tm, s_red[3][k]);
+            }
+            atomicAdd(&a.st[b0].power, tp);
+            atomicAdd(&a.st[b0].fnorm, tf);
+            atomicAdd(&a.st[b0].vnorm, tv);
+            atomicMax(&a.st[b0].fmax_bits, (unsigned long long)__double_as_longlong(tm));
+        }
+        return;
+    }
     // warp-level segmented reduction (lanes of one instance are contiguous)
-    unsigned full = 0xffffffffu;
-    int lane = threadIdx.x & 31;
     int first = __shfl_sync(full, inst, 0);
     bool uniform = __all_sync(full, inst == first);
     if (uniform) {

@@ -93,7 +93,7 @@ extern "C" int cg_fire_minimize(cg_system *s, const cg_fire_params *prm)
         cudaGraphExec_t exec = nullptr;
         long long nk = 0;
         for (auto &g : s->graphs)
-            if (g.kind == 3 && g.n == chunk && g.dt == prm->dt && g.mu == prm->force_cutoff && g.T == prm->dt_max) {
+            if (g.kind == 3 && g.n == chunk && memcmp(&g.fire, prm, sizeof(cg_fire_params)) == 0) {
                 exec = g.exec;
                 nk = g.kernels;
             }
@@ -107,7 +107,8 @@ extern "C" int cg_fire_minimize(cg_system *s, const cg_fire_params *prm)
             cudaGraphDestroy(graph);
             nk = s->kernels_enqueued - k0;
             s->kernels_enqueued = k0;
-            s->graphs.push_back({3, chunk, prm->dt, prm->force_cutoff, prm->dt_max, nullptr, exec, nk});
+            cg_system::GraphEntry ge{3, chunk, prm->dt, prm->force_cutoff, prm->dt_max, nullptr, exec, nk, *prm};
+            s->graphs.push_back(ge);
         }
         CG_CUDA(cudaGraphLaunch(exec, s->stream));
         s->kernels_enqueued += nk;

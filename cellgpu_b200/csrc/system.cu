@@ -205,6 +205,7 @@ struct cg_system {
         const double *noise;
         cudaGraphExec_t exec;
         long long kernels;
+        cg_fire_params fire;  // FIRE graphs: the parameters captured into the iteration kernels
     };
     std::vector<GraphEntry> graphs;
     long long kernels_enqueued = 0;  // kernels of this library launched for this system
@@ -901,9 +902,10 @@ static int spp_run_t(cg_system *s, int n_steps, double dt, double mu, const doub
     int step0 = 0, step = 0, halted = 0;
     CG_TRY(read_status(s, &step0, nullptr));
     int done = 0, recoveries = 0;
-    const int chunk = 32;
+    const int chunk = 32;  // graphs of 32, 16, ..., 1 steps: any n_steps reuses at most six graphs
     while (done < n_steps) {
-        int todo = std::min(chunk, n_steps - done);
+        int todo = chunk;
+        while (todo > n_steps - done) todo >>= 1;
         if (noise)
             enqueue_spp_steps<R>(s, todo, dt, mu, noise + (size_t)done * s->N, true);
         else

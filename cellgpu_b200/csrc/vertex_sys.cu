@@ -290,9 +290,10 @@ static void vm_enqueue_step(cg_system *s, int kind, int t, double dt, double mu,
 static int vm_run(cg_system *s, int kind, int n_steps, double dt, double mu, double T, const double *noise)
 {
     if (!s->topology_valid) return set_err(CG_ERR_STATE, "vertex topology not set");
-    const int chunk = 32;
+    const int chunk = 32;  // graphs of 32, 16, ..., 1 steps: any n_steps reuses at most six graphs
     for (int done = 0; done < n_steps;) {
-        int todo = std::min(chunk, n_steps - done);
+        int todo = chunk;
+        while (todo > n_steps - done) todo >>= 1;
         if (noise) {
             for (int t = 0; t < todo; ++t) vm_enqueue_step(s, kind, done + t, dt, mu, T, noise, true);
         } else {

@@ -1270,9 +1270,10 @@ __global__ void k_spp(VoroArgs a, const double *noise, double dt, double mu, uin
 // energies per instance (FP64 accumulation)
 // ------------------------------------------------------------------------------------------
 template <typename R>
-__global__ void k_energy(VoroArgs a, double *E)
+__global__ void __launch_bounds__(256) k_energy(VoroArgs a, double *E)
 {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ double s_part[8];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
     double e = 0.0;
     int inst = 0;
     if (c < a.N) {
@@ -1280,6 +1281,21 @@ __global__ void k_energy(VoroArgs a, double *E)
         double da = (double)ap.x - a.APpref[c].x, dp = (double)ap.y - a.APpref[c].y;
         e = a.KA * da * da + a.KP * dp * dp;
         inst = a.cell_inst ? a.cell_inst[c] : 0;
+    }
+    // instances are contiguous: a block whose first and last cells share an instance reduces in
+    // shared memory and adds once; a block across an instance boundary adds per cell
+    const int c0 = blockIdx.x * blockDim.x, c1 = min(a.N, c0 + (int)blockDim.x) - 1;
+    const int i0 = a.cell_inst ? a.cell_inst[c0] : 0, i1 = a.cell_inst ? a.cell_inst[c1] : 0;
+    if (i0 == i1) {
+        for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
+        if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = e;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
+            atomicAdd(&E[i0], t);
+        }
+    } else if (c < a.N) {
         atomicAdd(&E[inst], e);
     }
 }

@@ -4,7 +4,7 @@
  * Two layers, both plain C (extern "C", plain pointers and sizes, int status codes, no exceptions):
  *
  *  1. Kernel callers on caller-owned device memory. These replace the reference's L1 "gpu_*" free
- *     functions (inc/models/*.cuh, inc/updaters/*.cuh, inc/utility/*.cuh), which take raw device
+ *     functions (the .cuh headers of inc/models, inc/updaters and inc/utility), which take raw device
  *     pointers obtained from ArrayHandle<T>(..., access_location::device, ...). Each takes a
  *     cudaStream_t (0 = legacy default stream, as the reference used) and never allocates unless
  *     its comment says so.
