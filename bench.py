@@ -337,6 +337,22 @@ def bench_vertex(cg, torch, flush, steps=40, fire=True):
     return out
 
 
+def replica_aggregate(total_s, done, n_cells, world, device):
+    """Whole-job throughput of `world` independent replicas (one per rank, no exchange on the step
+    path): the time is the max over ranks of the device-timed region, the work is the sum of the
+    cell-steps every rank completed. Collective: every rank calls it at the same point."""
+    units = float(done * n_cells)
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([total_s], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        u = torch.tensor([units], dtype=torch.float64, device=device)
+        dist.all_reduce(u, op=dist.ReduceOp.SUM)
+        total_s, units = float(t.item()), float(u.item())
+    return (units / total_s if total_s > 0 else 0.0), total_s
+
+
 def workload_config(precision, world):
     return {"workload": "voronoi_spp_N262144_L512", "n_cells": N_CELLS, "box": BOX, "p0": P0, "v0": V0,
             "Dr": DR, "dt": DT, "precision": precision, "l2": "flushed (256 MB write) between timed steps",
@@ -446,19 +462,14 @@ def main():
     with ClockSampler(local) as clk:
         total, done, kernels = time_steps(cg, torch, b, stream, args.steps, flush)
     torch.cuda.synchronize()
-    if world > 1:
-        t = torch.tensor([total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
-        dist.barrier()
-    value = world * N_CELLS * done / total
+    value, total = replica_aggregate(total, done, N_CELLS, world, "cuda")
     # dominant kernel: fused geometry + force + exact test
     t_force = time_force_pass(cg, torch, b, stream, 20, flush)
     hbm, kind = peaks()
     achieved = FORCE_PASS_BYTES * N_CELLS / t_force / 1e9
     # end to end through the host-buffer API
     e2e_t, e2e_ok, h2d, d2h = e2e_steps(cg, torch, b, stream, max(3, args.steps // 5))
-    e2e_value = world * N_CELLS * e2e_ok / e2e_t if e2e_ok else 0.0
+    e2e_value, _ = replica_aggregate(e2e_t, e2e_ok, N_CELLS, world, "cuda")
     counters = b.counters()
     # mixed-precision force error on this (relaxed) state, against FP64
     F64 = None
