@@ -262,19 +262,91 @@ CG_D void queue_push(int *q, int head, int &n, int cap, int key, bool &overflow)
     ++n;
 }
 
-__global__ void k_vm_t1_replay(VertArgs a)
+// One step of the sweep at edge key = 3*vertex1 + slot, on the current state (the body of the
+// CPU sweep, src/models/vertexModelBase.cpp:653-787): 0 no flip, 1 flipped (cs, vs and vertex2
+// filled), -1 a cell row would exceed vmax.
+CG_D int t1_try(const VertArgs &a, const Inst &in, int key, int cs[4], int vs[4], int &vertex2)
 {
-    int inst = blockIdx.x * blockDim.x + threadIdx.x;
-    if (inst >= a.n_inst) return;
-    Ctl *ctl = a.ctl;
-    if (ctl && ctl->halt) return;
-    int nc = a.cand_count[inst];
-    a.cand_count[inst] = 0;
-    if (nc == 0) return;
-    const Inst &in = a.inst[inst];
+    int vertex1 = key / 3, vv = key % 3;
+    vertex2 = a.vn[3 * vertex1 + vv];
+    if (!(vertex1 < vertex2)) return 0;
+    double2 v1 = a.vpos[vertex1], v2 = a.vpos[vertex2];
+    double2 e = min_dist(v1, v2, in.Lx, in.Ly);
+    if (!(__dsqrt_rn(__dadd_rn(__dmul_rn(e.x, e.x), __dmul_rn(e.y, e.y))) < a.t1)) return 0;
+    t1_sets_d(a, vertex1, vertex2, cs, vs);
+    if (a.cvn[cs[0]] == 3 || a.cvn[cs[2]] == 3) return 0;
+    if (a.cvn[cs[1]] + 1 > a.vmax || a.cvn[cs[3]] + 1 > a.vmax) return -1;
+    // rotate the edge by 90 degrees about its midpoint
+    double2 mid = make_double2(__dadd_rn(v2.x, __dmul_rn(0.5, e.x)), __dadd_rn(v2.y, __dmul_rn(0.5, e.y)));
+    v1 = make_double2(__dsub_rn(mid.x, e.y), __dadd_rn(mid.y, e.x));
+    v2 = make_double2(__dadd_rn(mid.x, e.y), __dsub_rn(mid.y, e.x));
+    a.vpos[vertex1] = put_in_box(v1, in.Lx, in.Ly, in.iLx, in.iLy);
+    a.vpos[vertex2] = put_in_box(v2, in.Lx, in.Ly, in.iLx, in.iLy);
+    for (int vert = 0; vert < 3; ++vert) {
+        if (a.vcn[3 * vertex1 + vert] == cs[2]) a.vcn[3 * vertex1 + vert] = cs[3];
+        if (a.vcn[3 * vertex2 + vert] == cs[0]) a.vcn[3 * vertex2 + vert] = cs[1];
+        if (a.vn[3 * vs[1] + vert] == vertex1) a.vn[3 * vs[1] + vert] = vertex2;
+        if (a.vn[3 * vs[2] + vert] == vertex2) a.vn[3 * vs[2] + vert] = vertex1;
+        if (a.vn[3 * vertex1 + vert] == vs[1]) a.vn[3 * vertex1 + vert] = vs[2];
+        if (a.vn[3 * vertex2 + vert] == vs[2]) a.vn[3 * vertex2 + vert] = vs[1];
+    }
+    int *ri = a.cv + (size_t)cs[0] * a.vmax;
+    row_remove(ri, a.cvn[cs[0]], vertex2);
+    int *rj = a.cv + (size_t)cs[1] * a.vmax;
+    row_insert_after(rj, a.cvn[cs[1]], vertex1, vertex2);
+    int *rk = a.cv + (size_t)cs[2] * a.vmax;
+    row_remove(rk, a.cvn[cs[2]], vertex1);
+    int *rl = a.cv + (size_t)cs[3] * a.vmax;
+    row_insert_after(rl, a.cvn[cs[3]], vertex2, vertex1);
+    return 1;
+}
+
+// after a flip at `key`: queue the edges that moved or were rewired (those of vertex1, vertex2,
+// vs[1], vs[2]) ahead of the sweep position, into the pending part q[head, n) of an ascending queue.
+// Only edges shorter than the threshold are queued: a longer edge can become short only when one of
+// its ends moves, and the flip that moves it queues it again. The rows and positions are loaded
+// up front so the single sweeping thread waits for memory once, not once per edge.
+CG_D void t1_requeue(const VertArgs &a, const Inst &in, int key, int vertex2, const int vs[4], int *q,
+                     int head, int &n, int cap, bool &overflow)
+{
+    const int u4[4] = {key / 3, vertex2, vs[1], vs[2]};
+    int w12[12];
+    double2 pu[4], pw[12];
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int s = 0; s < 3; ++s) w12[3 * t + s] = a.vn[3 * u4[t] + s];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) pu[t] = a.vpos[u4[t]];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) pw[i] = a.vpos[w12[i]];
+    for (int t = 0; t < 4; ++t) {
+        const int u = u4[t];
+        for (int s = 0; s < 3; ++s) {
+            const int w = w12[3 * t + s];
+            // the length exactly as the sweep computes it (from the smaller index to the larger)
+            double2 e = u < w ? min_dist(pu[t], pw[3 * t + s], in.Lx, in.Ly)
+                              : min_dist(pw[3 * t + s], pu[t], in.Lx, in.Ly);
+            if (!(__dsqrt_rn(__dadd_rn(__dmul_rn(e.x, e.x), __dmul_rn(e.y, e.y))) < a.t1)) continue;
+            int k2;
+            if (u < w) {
+                k2 = 3 * u + s;
+            } else {
+                int sw = 0;
+                while (sw < 3 && a.vn[3 * w + sw] != u) ++sw;
+                if (sw == 3) continue;
+                k2 = 3 * w + sw;
+            }
+            if (k2 > key) queue_push(q, head, n, cap, k2, overflow);
+        }
+    }
+}
+
+// the whole sweep by one thread over the candidate keys q[0, nc) (sorted here); used when the
+// candidates do not fit the shared-memory path
+CG_D void t1_sweep_serial(const VertArgs &a, const Inst &in, int *q, int nc, int &flips, int &status)
+{
     const int cap = 3 * in.nv;
-    int *q = a.cand + 3 * (size_t)in.voff;
-    // sort the detected keys (insertion sort: the list is short)
     for (int i = 1; i < nc; ++i) {
         int key = q[i], j = i - 1;
         while (j >= 0 && q[j] > key) {
@@ -285,72 +357,178 @@ __global__ void k_vm_t1_replay(VertArgs a)
     }
     int head = 0, n = nc;
     bool overflow = false;
-    int flips = 0;
     while (head < n) {
         int key = q[head++];
-        int vertex1 = key / 3, vv = key % 3;
-        int vertex2 = a.vn[3 * vertex1 + vv];
-        if (!(vertex1 < vertex2)) continue;
-        double2 v1 = a.vpos[vertex1], v2 = a.vpos[vertex2];
-        double2 e = min_dist(v1, v2, in.Lx, in.Ly);
-        if (!(__dsqrt_rn(__dadd_rn(__dmul_rn(e.x, e.x), __dmul_rn(e.y, e.y))) < a.t1)) continue;
-        int cs[4] = {0, 0, 0, 0}, vs[4] = {0, 0, 0, 0};
-        t1_sets_d(a, vertex1, vertex2, cs, vs);
-        if (a.cvn[cs[0]] == 3 || a.cvn[cs[2]] == 3) continue;
-        if (a.cvn[cs[1]] + 1 > a.vmax || a.cvn[cs[3]] + 1 > a.vmax) {
-            if (ctl) {
-                atomicExch(&ctl->status, CG_ERR_CAPACITY);
-                atomicExch(&ctl->halt, 1);
-            }
+        int cs[4] = {0, 0, 0, 0}, vs[4] = {0, 0, 0, 0}, vertex2 = 0;
+        int r = t1_try(a, in, key, cs, vs, vertex2);
+        if (r < 0) {
+            status = CG_ERR_CAPACITY;
             return;
         }
-        // rotate the edge by 90 degrees about its midpoint
-        double2 mid = make_double2(__dadd_rn(v2.x, __dmul_rn(0.5, e.x)), __dadd_rn(v2.y, __dmul_rn(0.5, e.y)));
-        v1 = make_double2(__dsub_rn(mid.x, e.y), __dadd_rn(mid.y, e.x));
-        v2 = make_double2(__dadd_rn(mid.x, e.y), __dsub_rn(mid.y, e.x));
-        a.vpos[vertex1] = put_in_box(v1, in.Lx, in.Ly, in.iLx, in.iLy);
-        a.vpos[vertex2] = put_in_box(v2, in.Lx, in.Ly, in.iLx, in.iLy);
-        for (int vert = 0; vert < 3; ++vert) {
-            if (a.vcn[3 * vertex1 + vert] == cs[2]) a.vcn[3 * vertex1 + vert] = cs[3];
-            if (a.vcn[3 * vertex2 + vert] == cs[0]) a.vcn[3 * vertex2 + vert] = cs[1];
-            if (a.vn[3 * vs[1] + vert] == vertex1) a.vn[3 * vs[1] + vert] = vertex2;
-            if (a.vn[3 * vs[2] + vert] == vertex2) a.vn[3 * vs[2] + vert] = vertex1;
-            if (a.vn[3 * vertex1 + vert] == vs[1]) a.vn[3 * vertex1 + vert] = vs[2];
-            if (a.vn[3 * vertex2 + vert] == vs[2]) a.vn[3 * vertex2 + vert] = vs[1];
-        }
-        int *ri = a.cv + (size_t)cs[0] * a.vmax;
-        row_remove(ri, a.cvn[cs[0]], vertex2);
-        int *rj = a.cv + (size_t)cs[1] * a.vmax;
-        row_insert_after(rj, a.cvn[cs[1]], vertex1, vertex2);
-        int *rk = a.cv + (size_t)cs[2] * a.vmax;
-        row_remove(rk, a.cvn[cs[2]], vertex1);
-        int *rl = a.cv + (size_t)cs[3] * a.vmax;
-        row_insert_after(rl, a.cvn[cs[3]], vertex2, vertex1);
+        if (r == 0) continue;
         ++flips;
-        // edges that moved or were rewired, ahead of the sweep position
-        int touched[4] = {vertex1, vertex2, vs[1], vs[2]};
-        for (int t = 0; t < 4; ++t) {
-            int u = touched[t];
-            for (int s = 0; s < 3; ++s) {
-                int w = a.vn[3 * u + s];
-                int k2;
-                if (u < w) {
-                    k2 = 3 * u + s;
-                } else {
-                    int sw = 0;
-                    while (sw < 3 && a.vn[3 * w + sw] != u) ++sw;
-                    if (sw == 3) continue;
-                    k2 = 3 * w + sw;
+        t1_requeue(a, in, key, vertex2, vs, q, head, n, cap, overflow);
+        if (overflow) {
+            status = CG_ERR_CAPACITY;
+            return;
+        }
+    }
+}
+
+// Shared-memory sweep state (dynamic shared memory; T1_CAP candidates at most)
+constexpr int T1_CAP = 4096;
+constexpr int T1_HASH = 4096;  // touched vertices (2v) and cells (2c+1)
+constexpr size_t T1_SMEM = (size_t)T1_CAP * (sizeof(int4) + 2 * sizeof(int) + 1) + (size_t)T1_HASH * sizeof(int);
+
+CG_D unsigned t1_hash_slot(int id) { return ((unsigned)id * 2654435761u) >> 20; }  // 12 bits
+
+CG_D bool t1_touched(const int *h, int id)
+{
+    unsigned sl = t1_hash_slot(id);
+    for (int p = 0; p < T1_HASH; ++p) {
+        int v = h[sl];
+        if (v == id) return true;
+        if (v < 0) return false;
+        sl = (sl + 1) & (T1_HASH - 1);
+    }
+    return false;
+}
+
+// returns false once the table is 3/4 full (the caller then stops trusting start-of-sweep results)
+CG_D bool t1_touch(int *h, int id, int &count)
+{
+    unsigned sl = t1_hash_slot(id);
+    for (int p = 0; p < T1_HASH; ++p) {
+        int v = h[sl];
+        if (v == id) return true;
+        if (v < 0) {
+            h[sl] = id;
+            return ++count < (3 * T1_HASH) / 4;
+        }
+        sl = (sl + 1) & (T1_HASH - 1);
+    }
+    return false;
+}
+
+// One block per instance. The candidates are sorted in parallel (bitonic, shared memory) and
+// evaluated in parallel on the state at the start of the sweep; then one thread replays the
+// sweep in ascending key order. A candidate rejected at the start stays rejected unless an
+// earlier flip of this sweep touched one of its endpoints (positions, vn, vcn) or one of the four
+// cells around it (rows, sizes), which are exactly the data the test reads; such candidates, and
+// every candidate that was not rejected, are evaluated on the current state as the CPU sweep does.
+__global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
+{
+    extern __shared__ __align__(16) unsigned char t1_smem[];
+    int4 *s_cs = reinterpret_cast<int4 *>(t1_smem);
+    int *s_key = reinterpret_cast<int *>(s_cs + T1_CAP);
+    int *s_v2 = s_key + T1_CAP;
+    int *s_hash = s_v2 + T1_CAP;
+    unsigned char *s_dec = reinterpret_cast<unsigned char *>(s_hash + T1_HASH);
+    const int inst = blockIdx.x;
+    Ctl *ctl = a.ctl;
+    if (ctl && ctl->halt) return;  // uniform
+    const int nc = a.cand_count[inst];
+    __syncthreads();
+    if (threadIdx.x == 0) a.cand_count[inst] = 0;
+    if (nc == 0) return;
+    const Inst &in = a.inst[inst];
+    int *q = a.cand + 3 * (size_t)in.voff;
+    int flips = 0, status = 0;
+    if (nc > T1_CAP) {
+        if (threadIdx.x == 0) t1_sweep_serial(a, in, q, nc, flips, status);
+    } else {
+        int P = 1;
+        while (P < nc) P <<= 1;
+        for (int i = threadIdx.x; i < P; i += blockDim.x) s_key[i] = i < nc ? q[i] : 0x7fffffff;
+        for (int i = threadIdx.x; i < T1_HASH; i += blockDim.x) s_hash[i] = -1;
+        __syncthreads();
+        for (int k = 2; k <= P; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                    int ixj = i ^ j;
+                    if (ixj > i) {
+                        int x = s_key[i], y = s_key[ixj];
+                        bool up = (i & k) == 0;
+                        if ((x > y) == up) {
+                            s_key[i] = y;
+                            s_key[ixj] = x;
+                        }
+                    }
                 }
-                if (k2 > key) queue_push(q, head, n, cap, k2, overflow);
+                __syncthreads();
             }
         }
-        if (overflow) break;
+        // start-of-sweep evaluation (read-only)
+        for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+            int key = s_key[i];
+            int v1 = key / 3;
+            int v2 = a.vn[3 * v1 + key % 3];
+            int cs[4] = {-1, -1, -1, -1}, vs[4];
+            unsigned char dec = 0;  // 0: rejected, 1: evaluate at its turn
+            if (v1 < v2) {
+                double2 e = min_dist(a.vpos[v1], a.vpos[v2], in.Lx, in.Ly);
+                if (__dsqrt_rn(__dadd_rn(__dmul_rn(e.x, e.x), __dmul_rn(e.y, e.y))) < a.t1) {
+                    t1_sets_d(a, v1, v2, cs, vs);
+                    dec = (a.cvn[cs[0]] == 3 || a.cvn[cs[2]] == 3) ? 0 : 1;
+                }
+            }
+            s_v2[i] = v2;
+            s_cs[i] = make_int4(cs[0], cs[1], cs[2], cs[3]);
+            s_dec[i] = dec;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            // sweep: the sorted candidates merged with the keys queued by flips (q[nc, ...))
+            int *ex = q + nc;
+            const int ecap = 3 * in.nv - nc;
+            int hm = 0, eh = 0, en = 0, touched_n = 0;
+            bool trust = true, overflow = false;
+            while (hm < nc || eh < en) {
+                int key;
+                bool pre = false;
+                int idx = -1;
+                if (eh < en && (hm >= nc || ex[eh] <= s_key[hm])) {
+                    key = ex[eh++];
+                    if (hm < nc && s_key[hm] == key) ++hm;  // queued again by a flip: evaluate once
+                } else {
+                    idx = hm++;
+                    key = s_key[idx];
+                    pre = true;
+                }
+                if (pre && trust && s_dec[idx] == 0) {
+                    int4 c4 = s_cs[idx];
+                    bool stale = t1_touched(s_hash, 2 * (key / 3)) || t1_touched(s_hash, 2 * s_v2[idx]);
+                    if (!stale && c4.x >= 0)
+                        stale = t1_touched(s_hash, 2 * c4.x + 1) || t1_touched(s_hash, 2 * c4.y + 1) ||
+                                t1_touched(s_hash, 2 * c4.z + 1) || t1_touched(s_hash, 2 * c4.w + 1);
+                    if (!stale) continue;  // still rejected
+                }
+                int cs[4] = {0, 0, 0, 0}, vs[4] = {0, 0, 0, 0}, vertex2 = 0;
+                int r = t1_try(a, in, key, cs, vs, vertex2);
+                if (r < 0) {
+                    status = CG_ERR_CAPACITY;
+                    break;
+                }
+                if (r == 0) continue;
+                ++flips;
+                int ids[8] = {2 * (key / 3), 2 * vertex2, 2 * vs[1], 2 * vs[2],
+                              2 * cs[0] + 1, 2 * cs[1] + 1, 2 * cs[2] + 1, 2 * cs[3] + 1};
+                for (int t = 0; t < 8; ++t)
+                    if (!t1_touch(s_hash, ids[t], touched_n)) trust = false;
+                t1_requeue(a, in, key, vertex2, vs, ex, eh, en, ecap, overflow);
+                if (overflow) {
+                    status = CG_ERR_CAPACITY;
+                    break;
+                }
+            }
+        }
     }
-    if (ctl) atomicAdd(&ctl->counters[5], (unsigned long long)flips);
-    if (overflow && ctl) {
-        atomicExch(&ctl->status, CG_ERR_CAPACITY);
-        atomicExch(&ctl->halt, 1);
+    if (threadIdx.x == 0) {
+        if (ctl) atomicAdd(&ctl->counters[5], (unsigned long long)flips);
+        if (status && ctl) {
+            atomicExch(&ctl->status, status);
+            atomicExch(&ctl->halt, 1);
+        }
     }
 }
 

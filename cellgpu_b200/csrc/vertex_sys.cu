@@ -74,6 +74,8 @@ extern "C" int cg_vertex_create(int n_inst, const int *Nc, const double *box, in
     }
     s->N = off;
     s->Nv = 2 * off;
+    // the T1 sweep stages up to T1_CAP candidates per instance in dynamic shared memory
+    cudaFuncSetAttribute(k_vm_t1_replay, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T1_SMEM);
     int st = sys_streams(s);
     if (st != CG_OK) {
         sys_release(s);
@@ -242,7 +244,7 @@ static int vm_compute_forces(cg_system *s)
 static void vm_launch_t1(cg_system *s, const VertArgs &a)
 {
     k_vm_t1_detect<<<nblk(s->Nv, 256), 256, 0, s->stream>>>(a);
-    k_vm_t1_replay<<<nblk(s->n_inst, 32), 32, 0, s->stream>>>(a);
+    k_vm_t1_replay<<<s->n_inst, 256, T1_SMEM, s->stream>>>(a);
     s->kernels_enqueued += 2;
 }
 
