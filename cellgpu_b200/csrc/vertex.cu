@@ -265,7 +265,7 @@ CG_D void queue_push(int *q, int head, int &n, int cap, int key, bool &overflow)
 // One step of the sweep at edge key = 3*vertex1 + slot, on the current state (the body of the
 // CPU sweep, src/models/vertexModelBase.cpp:653-787): 0 no flip, 1 flipped (cs, vs and vertex2
 // filled), -1 a cell row would exceed vmax.
-CG_D int t1_try(const VertArgs &a, const Inst &in, int key, int cs[4], int vs[4], int &vertex2)
+CG_D int t1_try_global(const VertArgs &a, const Inst &in, int key, int cs[4], int vs[4], int &vertex2)
 {
     int vertex1 = key / 3, vv = key % 3;
     vertex2 = a.vn[3 * vertex1 + vv];
@@ -298,6 +298,137 @@ CG_D int t1_try(const VertArgs &a, const Inst &in, int key, int cs[4], int vs[4]
     row_remove(rk, a.cvn[cs[2]], vertex1);
     int *rl = a.cv + (size_t)cs[3] * a.vmax;
     row_insert_after(rl, a.cvn[cs[3]], vertex2, vertex1);
+    return 1;
+}
+
+// row walk of find_in_cell_d on a local copy of a cell's row
+CG_D void find_in_row(const int *row, int cneigh, int target, int &vlast, int &vcur, int &vnext)
+{
+    int l = row[cneigh - 2], c = row[cneigh - 1], nx = row[0];
+    for (int cn = 0; cn < cneigh; ++cn) {
+        nx = row[cn];
+        if (c == target) break;
+        l = c;
+        c = nx;
+    }
+    vlast = l;
+    vcur = c;
+    vnext = nx;
+}
+
+constexpr int T1_ROW_LOCAL = 32;  // cell rows up to this length are staged in local copies
+
+// The same step as t1_try_global with the data it reads loaded in a few independent batches
+// (the four cell rows and sizes at once, the four vertex rows at once) and the edits applied to
+// local copies in the same order before being written back, so one sweeping thread waits for
+// memory a handful of times per flip instead of once per access. Falls back to t1_try_global
+// (before writing anything) when rows are longer than T1_ROW_LOCAL or the cells / vertices of
+// the flip are not all distinct (where in-place edits of one row would be seen by the next).
+CG_D int t1_try(const VertArgs &a, const Inst &in, int key, int cs[4], int vs[4], int &vertex2)
+{
+    if (a.vmax > T1_ROW_LOCAL) return t1_try_global(a, in, key, cs, vs, vertex2);
+    const int vertex1 = key / 3, vv = key % 3;
+    vertex2 = a.vn[3 * vertex1 + vv];
+    if (!(vertex1 < vertex2)) return 0;
+    double2 p1 = a.vpos[vertex1], p2 = a.vpos[vertex2];
+    int c3v1[3], c3v2[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        c3v1[f] = a.vcn[3 * vertex1 + f];
+        c3v2[f] = a.vcn[3 * vertex2 + f];
+    }
+    double2 e = min_dist(p1, p2, in.Lx, in.Ly);
+    if (!(__dsqrt_rn(__dadd_rn(__dmul_rn(e.x, e.x), __dmul_rn(e.y, e.y))) < a.t1)) return 0;
+    // cs[3]: the cell of vertex2 that vertex1 does not touch (left as given if there is none)
+    int c4 = cs[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        int t = c3v2[f];
+        if (t != c3v1[0] && t != c3v1[1] && t != c3v1[2]) c4 = t;
+    }
+    const int cid[4] = {c3v1[0], c3v1[1], c3v1[2], c4};
+    int R[4][T1_ROW_LOCAL];
+    int nr[4];
+    // all four rows in flight at once (fully unrolled, predicated on vmax)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        nr[q] = a.cvn[cid[q]];
+        const int *src = a.cv + (size_t)cid[q] * a.vmax;
+#pragma unroll
+        for (int k = 0; k < T1_ROW_LOCAL; ++k) R[q][k] = k < a.vmax ? src[k] : 0;
+    }
+    // classify vertex1's cells by the neighbours of vertex1 in their rows (t1_sets_d)
+    int i0 = -1, i1 = -1, i2 = -1;
+    for (int q = 0; q < 3; ++q) {
+        int l, cur, nx;
+        find_in_row(R[q], nr[q], vertex1, l, cur, nx);
+        if (l == vertex2) i0 = q;
+        else if (nx == vertex2) i2 = q;
+        else i1 = q;
+    }
+    if (i0 < 0 || i1 < 0 || i2 < 0 || c4 == cid[0] || c4 == cid[1] || c4 == cid[2] || cid[0] == cid[1] ||
+        cid[0] == cid[2] || cid[1] == cid[2])
+        return t1_try_global(a, in, key, cs, vs, vertex2);
+    cs[0] = cid[i0];
+    cs[1] = cid[i1];
+    cs[2] = cid[i2];
+    cs[3] = c4;
+    {
+        int l, cur, nx;
+        find_in_row(R[i1], nr[i1], vertex1, l, cur, nx);
+        vs[0] = l;
+        vs[1] = nx;
+        find_in_row(R[3], nr[3], vertex2, l, cur, nx);
+        vs[3] = l;
+        vs[2] = nx;
+    }
+    if (nr[i0] == 3 || nr[i2] == 3) return 0;
+    if (nr[i1] + 1 > a.vmax || nr[3] + 1 > a.vmax) return -1;
+    const int vx[4] = {vertex1, vertex2, vs[1], vs[2]};
+    if (vs[1] == vs[2] || vs[1] == vertex1 || vs[1] == vertex2 || vs[2] == vertex1 || vs[2] == vertex2)
+        return t1_try_global(a, in, key, cs, vs, vertex2);
+    int VN[4][3];
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int f = 0; f < 3; ++f) VN[t][f] = a.vn[3 * vx[t] + f];
+    // rotate the edge by 90 degrees about its midpoint
+    double2 mid = make_double2(__dadd_rn(p2.x, __dmul_rn(0.5, e.x)), __dadd_rn(p2.y, __dmul_rn(0.5, e.y)));
+    double2 n1 = make_double2(__dsub_rn(mid.x, e.y), __dadd_rn(mid.y, e.x));
+    double2 n2 = make_double2(__dadd_rn(mid.x, e.y), __dsub_rn(mid.y, e.x));
+    a.vpos[vertex1] = put_in_box(n1, in.Lx, in.Ly, in.iLx, in.iLy);
+    a.vpos[vertex2] = put_in_box(n2, in.Lx, in.Ly, in.iLx, in.iLy);
+    // rewiring, in the order of the CPU sweep (rows are distinct here)
+#pragma unroll
+    for (int vert = 0; vert < 3; ++vert) {
+        if (c3v1[vert] == cs[2]) c3v1[vert] = cs[3];
+        if (c3v2[vert] == cs[0]) c3v2[vert] = cs[1];
+        if (VN[2][vert] == vertex1) VN[2][vert] = vertex2;
+        if (VN[3][vert] == vertex2) VN[3][vert] = vertex1;
+        if (VN[0][vert] == vs[1]) VN[0][vert] = vs[2];
+        if (VN[1][vert] == vs[2]) VN[1][vert] = vs[1];
+    }
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        a.vcn[3 * vertex1 + f] = c3v1[f];
+        a.vcn[3 * vertex2 + f] = c3v2[f];
+    }
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int f = 0; f < 3; ++f) a.vn[3 * vx[t] + f] = VN[t][f];
+    row_remove(R[i0], nr[i0], vertex2);
+    row_insert_after(R[i1], nr[i1], vertex1, vertex2);
+    row_remove(R[i2], nr[i2], vertex1);
+    row_insert_after(R[3], nr[3], vertex2, vertex1);
+    const int qi[4] = {i0, i1, i2, 3};
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        int q = qi[t];
+        int *dst = a.cv + (size_t)cid[q] * a.vmax;
+        for (int k = 0; k < nr[q]; ++k) dst[k] = R[q][k];
+        a.cvn[cid[q]] = nr[q];
+    }
     return 1;
 }
 
@@ -378,7 +509,9 @@ CG_D void t1_sweep_serial(const VertArgs &a, const Inst &in, int *q, int nc, int
 // Shared-memory sweep state (dynamic shared memory; T1_CAP candidates at most)
 constexpr int T1_CAP = 4096;
 constexpr int T1_HASH = 4096;  // touched vertices (2v) and cells (2c+1)
-constexpr size_t T1_SMEM = (size_t)T1_CAP * (sizeof(int4) + 2 * sizeof(int) + 1) + (size_t)T1_HASH * sizeof(int);
+constexpr int T1_EXQ = 2048;   // keys queued by flips, in shared memory until they outgrow it
+constexpr size_t T1_SMEM =
+    (size_t)T1_CAP * (sizeof(int4) + 2 * sizeof(int) + 1) + (size_t)(T1_HASH + T1_EXQ) * sizeof(int);
 
 CG_D unsigned t1_hash_slot(int id) { return ((unsigned)id * 2654435761u) >> 20; }  // 12 bits
 
@@ -423,7 +556,8 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
     int *s_key = reinterpret_cast<int *>(s_cs + T1_CAP);
     int *s_v2 = s_key + T1_CAP;
     int *s_hash = s_v2 + T1_CAP;
-    unsigned char *s_dec = reinterpret_cast<unsigned char *>(s_hash + T1_HASH);
+    int *s_exq = s_hash + T1_HASH;
+    unsigned char *s_dec = reinterpret_cast<unsigned char *>(s_exq + T1_EXQ);
     const int inst = blockIdx.x;
     Ctl *ctl = a.ctl;
     if (ctl && ctl->halt) return;  // uniform
@@ -478,9 +612,11 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            // sweep: the sorted candidates merged with the keys queued by flips (q[nc, ...))
-            int *ex = q + nc;
-            const int ecap = 3 * in.nv - nc;
+            // sweep: the sorted candidates merged with the keys queued by flips, kept in shared
+            // memory and moved to q[nc, 3 nv) if they outgrow it
+            int *ex = s_exq;
+            int ecap = T1_EXQ;
+            const int gcap = 3 * in.nv - nc;
             int hm = 0, eh = 0, en = 0, touched_n = 0;
             bool trust = true, overflow = false;
             while (hm < nc || eh < en) {
@@ -515,6 +651,19 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
                               2 * cs[0] + 1, 2 * cs[1] + 1, 2 * cs[2] + 1, 2 * cs[3] + 1};
                 for (int t = 0; t < 8; ++t)
                     if (!t1_touch(s_hash, ids[t], touched_n)) trust = false;
+                if (ex == s_exq && en + 12 > ecap) {  // room for one flip's keys, else move to global
+                    int *g = q + nc;
+                    int m = en - eh;
+                    if (m + 12 > gcap) {
+                        status = CG_ERR_CAPACITY;
+                        break;
+                    }
+                    for (int t = 0; t < m; ++t) g[t] = ex[eh + t];
+                    ex = g;
+                    eh = 0;
+                    en = m;
+                    ecap = gcap;
+                }
                 t1_requeue(a, in, key, vertex2, vs, ex, eh, en, ecap, overflow);
                 if (overflow) {
                     status = CG_ERR_CAPACITY;
