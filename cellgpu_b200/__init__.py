@@ -8,11 +8,12 @@ from ._lib import (CG_ERR_ARG, CG_ERR_CAPACITY, CG_ERR_CUDA, CG_ERR_STATE, CG_ER
 from ._lib import FireParams  # noqa: F401
 from .models import (EnergyMinimizerFIRE, Simulation, VertexBatch, VertexQuadraticEnergy,  # noqa: F401
                      Voronoi2D, VoronoiBatch, VoronoiQuadraticEnergy, brownianParticleDynamics,
-                     random_positions, selfPropelledCellVertexDynamics, selfPropelledParticleDynamics)
+                     random_positions, restore, selfPropelledCellVertexDynamics,
+                     selfPropelledParticleDynamics)
 
 __all__ = [
     "CG_FP64", "CG_MIXED", "CellGPUError", "EnergyMinimizerFIRE", "FireParams", "load", "Simulation",
     "VertexBatch", "VertexQuadraticEnergy", "Voronoi2D", "VoronoiBatch", "VoronoiQuadraticEnergy",
-    "brownianParticleDynamics", "random_positions", "selfPropelledCellVertexDynamics",
+    "brownianParticleDynamics", "random_positions", "restore", "selfPropelledCellVertexDynamics",
     "selfPropelledParticleDynamics",
 ]

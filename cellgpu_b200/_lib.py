@@ -77,6 +77,14 @@ SIGNATURES = {
     "cg_vertex_create": (_i, [_i, _vp, _vp, _i, _i, C.POINTER(_vp)]),
     "cg_vertex_footprint": (_sz, [_i, _vp, _i]),
     "cg_device_memory": (_i, [_vp, _vp]),
+    "cg_snapshot_size": (_sz, [_vp]),
+    "cg_snapshot": (_i, [_vp, _vp, _sz]),
+    "cg_restore": (_i, [_vp, _sz, _vp]),
+    "cg_get_instances": (_i, [_vp, _vp, _vp]),
+    "cg_model_kind": (_i, [_vp]),
+    "cg_precision": (_i, [_vp]),
+    "cg_set_reference_positions": (_i, [_vp]),
+    "cg_observables": (_i, [_vp, _d, _vp]),
     "cg_get_vertex_topology": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cg_set_vertex_topology": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cg_vertex_from_voronoi": (_i, [_vp, _vp]),

@@ -220,6 +220,9 @@ struct cg_system {
     int *vert_inst = nullptr, *vn = nullptr, *vcn = nullptr, *cvn = nullptr, *cv = nullptr;
     int *t1_cand = nullptr, *t1_count = nullptr;
     double t1 = 0.01;  // vertexModelBase default (src/models/vertexModelBase.cpp:59)
+    // observables (allocated on first use): reference positions, per-instance sums and means
+    double2 *obs_ref = nullptr;
+    double *obs_acc = nullptr, *obs_mean = nullptr;
     // FIRE (allocated on first use)
     double2 *fire_vel = nullptr;
     void *fire_st = nullptr;
@@ -1063,3 +1066,9 @@ extern "C" int cg_get_energies(cg_system *s, double *E)
 
 // FIRE
 #include "fire_sys.cu"
+
+// snapshots and exact resume
+#include "snapshot.cu"
+
+// observables
+#include "observables.cu"

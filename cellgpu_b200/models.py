@@ -61,6 +61,29 @@ class VoronoiBatch:
     def handle(self):
         return self._h
 
+    # -- observables (per instance, on the device)
+    OBS_FIELDS = ("mean_q", "var_q", "mean_A", "mean_P", "var_A", "var_P", "msd", "overlap")
+
+    def set_reference_positions(self):
+        """Capture the current positions as the reference of msd / overlap."""
+        check(self._lib.cg_set_reference_positions(self._h))
+
+    def observables(self, cutoff=0.5):
+        """Per instance: mean and variance of q = P/sqrt(A), mean and variance of A and P (stored
+        areas/perimeters of the last force evaluation), MSD and overlap fraction against the
+        reference positions. Returns a dict of arrays."""
+        out = np.zeros((len(self.N), len(self.OBS_FIELDS)))
+        check(self._lib.cg_observables(self._h, float(cutoff), ptr(out)))
+        return {k: out[:, i] for i, k in enumerate(self.OBS_FIELDS)}
+
+    # -- snapshots (exact resume: device noise is keyed per instance and counted by step)
+    def snapshot(self) -> bytes:
+        """The whole state of the batch as bytes; ``restore(bytes)`` continues it exactly."""
+        n = self._lib.cg_snapshot_size(self._h)
+        buf = C.create_string_buffer(n)
+        check(self._lib.cg_snapshot(self._h, buf, n))
+        return buf.raw
+
     # -- state
     def set_positions(self, pos):
         pos = _f64(pos, (self.Ntot, 2))
@@ -229,6 +252,32 @@ class VertexBatch(VoronoiBatch):
 
     def spp_run(self, n_steps, dt=0.01, mu=1.0, noise=None):
         check(self._lib.cg_vertex_spp_run(self._h, int(n_steps), float(dt), float(mu), ptr(noise)))
+
+
+def restore(snapshot: bytes):
+    """A new VoronoiBatch or VertexBatch holding the state saved by ``snapshot()``."""
+    lib = load()
+    buf = C.create_string_buffer(bytes(snapshot), len(snapshot))
+    h = C.c_void_p()
+    check(lib.cg_restore(buf, len(snapshot), C.byref(h)))
+    n_inst = lib.cg_num_instances(h)
+    Ns = np.zeros(n_inst, np.int32)
+    boxes = np.zeros((n_inst, 2))
+    check(lib.cg_get_instances(h, ptr(Ns), ptr(boxes)))
+    vertex = lib.cg_model_kind(h) == 1
+    b = (VertexBatch if vertex else VoronoiBatch).__new__(VertexBatch if vertex else VoronoiBatch)
+    b._lib = lib
+    b._h = h
+    b.N = [int(n) for n in Ns]
+    b.boxes = boxes
+    b.K = lib.cg_neighbor_capacity(h)
+    b.precision = lib.cg_precision(h)
+    b.Ntot = sum(b.N)
+    b.offsets = np.concatenate([[0], np.cumsum(b.N)]).astype(np.int64)
+    if vertex:
+        b.vmax = b.K
+        b.Nv = 2 * b.Ntot
+    return b
 
 
 def random_positions(N, box, seed):

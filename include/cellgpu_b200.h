@@ -239,6 +239,34 @@ int cg_fire_minimize(cg_system *sys, const cg_fire_params *prm);
  * GPU convention, src/updaters/EnergyMinimizerFIRE2D.cpp:184) of the last iteration */
 int cg_fire_state(cg_system *sys, int *iterations, double *fmax_cpu, double *fnorm_gpu);
 
+/* Snapshots and exact resume. No counterpart in the reference, whose state files (netCDF,
+ * src/databases/DatabaseNetCDFSPV.cpp:32-46, DatabaseNetCDFAVM.cpp:33-52) store no RNG state.
+ * cg_snapshot writes the whole state of a system (instances with their boxes and noise keys,
+ * positions, directors, motility, preferences, moduli, topology or vertex wiring, T1 threshold,
+ * step counter) into a host buffer of cg_snapshot_size bytes; cg_restore builds a new system from
+ * it. Device noise is keyed per instance and counted by step and local index, so the restored
+ * system continues the original trajectory (up to the summation order of atomics). FIRE
+ * velocities and derived quantities (forces, A/P) are not stored. */
+size_t cg_snapshot_size(cg_system *sys);
+int cg_snapshot(cg_system *sys, void *buf, size_t bytes);
+int cg_restore(const void *buf, size_t bytes, cg_system **out);
+/* instance sizes (cells) and boxes (Lx, Ly), n_inst entries each; model kind and precision */
+int cg_get_instances(cg_system *sys, int *N, double *box);
+int cg_model_kind(cg_system *sys);
+int cg_precision(cg_system *sys);
+
+/* Observables per instance, computed on the device. Shape statistics from the stored areas and
+ * perimeters (those of the last force evaluation), as Simple2DCell::reportq / reportVarq /
+ * reportMeanP / reportVarAP (src/models/Simple2DCell.cpp:699-765); mean squared displacement and
+ * overlap function (fraction with minimum-image displacement < cutoff) as dynamicalFeatures
+ * (src/analysis/dynamicalFeatures.cpp:17-50) against the positions captured by
+ * cg_set_reference_positions (cells for the Voronoi model, vertices for the vertex model).
+ * out: n_inst records of CG_OBS_FIELDS doubles: mean q, var q, mean A, mean P, var A, var P,
+ * MSD, overlap (the last two NaN before any reference is set). */
+#define CG_OBS_FIELDS 8
+int cg_set_reference_positions(cg_system *sys);
+int cg_observables(cg_system *sys, double cutoff, double *out);
+
 /* counters: topology repairs, global retriangulations, T1 flips, fallbacks (per system) */
 int cg_counters(cg_system *sys, long long *out, int n);
 

@@ -39,3 +39,14 @@ def test_error_string_roundtrip(cglib):
     rc = cglib.cg_voronoi_create(0, None, None, 16, 0, C.byref(h))
     assert rc == -2
     assert b"bad" in cglib.cg_last_error_string()
+
+
+def test_restore_rejects_a_foreign_buffer():
+    """cg_restore validates the snapshot header before touching the device."""
+    import ctypes as C
+    from cellgpu_b200._lib import CG_ERR_ARG, load
+    lib = load()
+    junk = C.create_string_buffer(b"definitely not a snapshot" * 8)
+    h = C.c_void_p()
+    assert lib.cg_restore(junk, len(junk.raw), C.byref(h)) == CG_ERR_ARG
+    assert b"snapshot" in lib.cg_last_error_string()
