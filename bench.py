@@ -410,6 +410,10 @@ def main():
                     help="requests in the serving (C5) extra; 0 skips it")
     ap.add_argument("--serve-only", action="store_true",
                     help="run only the serving stream and print its JSON line")
+    ap.add_argument("--case", default="c2", choices=["c2", "c3", "c4"],
+                    help="c2: the headline line (default); c3 / c4: only the vertex-model or the "
+                         "batched-ensemble measurement, printed as one JSON line")
+    ap.add_argument("--c3-steps", type=int, default=10000, help="Brownian steps of the c3 case")
     ap.add_argument("--equilibrate", type=int, default=300,
                     help="untimed SPP steps from the random initial state before warm-up")
     args = ap.parse_args()
@@ -444,6 +448,15 @@ def main():
     if not os.path.exists(cgbuild.LIB):
         raise SystemExit("libcellgpu_b200.so missing: run __graft_entry__.build()")
     torch.cuda.set_device(local)
+    if args.case != "c2":
+        if rank == 0:
+            flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+            if args.case == "c3":
+                out = {"c3_vertex": bench_vertex(cg, torch, flush, steps=max(1001, args.c3_steps))}
+            else:
+                out = {"c4_ensemble": bench_batched(cg, torch, flush)}
+            print(json.dumps({"metric": METRIC, "impl": "ours", "n_gpus": 1, "case": args.case, **out}))
+        return
     if args.serve_only:
         if rank == 0:
             out = bench_serving(max(1, args.serve_requests))
