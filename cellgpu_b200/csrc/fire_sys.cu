@@ -55,7 +55,7 @@ static void fire_forces(cg_system *s, bool test_and_repair)
         VertArgs a = vm_args(s);
         if (test_and_repair) vm_launch_t1(s, a);
         cudaMemsetAsync(s->F, 0, sizeof(double2) * s->Nv, s->stream);
-        k_vm_forces<<<nblk(s->N, 128), 128, 0, s->stream>>>(a, 1);
+        launch_vm_forces(s, a);
         s->kernels_enqueued += 1;
     }
 }

@@ -76,6 +76,94 @@ __global__ void k_vm_forces(VertArgs a, int scatter)
     }
 }
 
+// The same pass with 8 lanes per cell (lane = vertex slot, rows up to VM_ROW_G vertices): the
+// relative vertex positions and the per-vertex area and perimeter terms are formed in parallel,
+// one lane adds the terms in the reference's vertex order (so A and P are summed as the CPU sums
+// them), and every lane forms and scatters the force sets of its vertices.
+constexpr int VM_G = 8;
+constexpr int VM_ROW_G = 32;
+
+template <int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_vm_forces_groups(VertArgs a, int scatter)
+{
+    constexpr int GPW_ = 32 / VM_G;
+    __shared__ double2 sV[WPB * GPW_][VM_ROW_G];
+    __shared__ double sA[WPB * GPW_][VM_ROW_G];
+    __shared__ double sP[WPB * GPW_][VM_ROW_G];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int gl = lane & (VM_G - 1), gi = lane / VM_G;
+    const int sl = w * GPW_ + gi;
+    const int c = (blockIdx.x * WPB + w) * GPW_ + gi;
+    bool live = c < a.Nc;
+    if (a.ctl && a.ctl->halt) live = false;  // uniform across the grid
+    int z = live ? a.cvn[c] : 0;
+    const bool ok = live && z >= 3 && z <= VM_ROW_G;
+    const int *row = a.cv + (size_t)(ok ? c : 0) * a.vmax;
+    double Lx = 1.0, Ly = 1.0;
+    double2 cp = make_double2(0.0, 0.0);
+    if (ok) {
+        const Inst &in = a.inst[a.cell_inst[c]];
+        Lx = in.Lx;
+        Ly = in.Ly;
+        cp = a.vpos[row[z - 2]];
+    }
+    int vid[VM_ROW_G / VM_G];
+#pragma unroll
+    for (int r = 0; r < VM_ROW_G / VM_G; ++r) {
+        int k = gl + VM_G * r;
+        vid[r] = -1;
+        if (ok && k < z) {
+            vid[r] = row[k];
+            sV[sl][k] = min_dist(a.vpos[vid[r]], cp, Lx, Ly);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < VM_ROW_G / VM_G; ++r) {
+        int k = gl + VM_G * r;
+        if (ok && k < z) {
+            double2 vc = sV[sl][k == 0 ? z - 1 : k - 1], vn = sV[sl][k];
+            sA[sl][k] = 0.5 * (vc.x + vn.x) * (vn.y - vc.y);
+            double dx = vc.x - vn.x, dy = vc.y - vn.y;
+            sP[sl][k] = sqrt(dx * dx + dy * dy);
+        }
+    }
+    __syncwarp();
+    double A = 0.0, P = 0.0;
+    if (ok && gl == 0) {
+        for (int n = 0; n < z; ++n) {
+            A += sA[sl][n];
+            P += sP[sl][n];
+        }
+        a.AP[c] = make_double2(A, P);
+    }
+    const int leader = lane & ~(VM_G - 1);
+    A = __shfl_sync(0xffffffffu, A, leader);
+    P = __shfl_sync(0xffffffffu, P, leader);
+    if (!scatter) return;  // uniform
+    double Adiff = 0.0, Pdiff = 0.0;
+    if (ok) {
+        Adiff = a.KA * (A - a.APpref[c].x);
+        Pdiff = a.KP * (P - a.APpref[c].y);
+    }
+#pragma unroll
+    for (int r = 0; r < VM_ROW_G / VM_G; ++r) {
+        int k = gl + VM_G * r;
+        if (ok && k < z) {
+            double2 vlast = sV[sl][k == 0 ? z - 1 : k - 1], vcur = sV[sl][k], vnext = sV[sl][k + 1 == z ? 0 : k + 1];
+            double dAx = 0.5 * (vlast.y - vnext.y), dAy = -0.5 * (vlast.x - vnext.x);
+            double lx = vlast.x - vcur.x, ly = vlast.y - vcur.y;
+            double ln = sqrt(lx * lx + ly * ly);
+            double nx = vcur.x - vnext.x, ny = vcur.y - vnext.y;
+            double nnm = sqrt(nx * nx + ny * ny);
+            double fx = 2.0 * (Adiff * dAx + Pdiff * (lx / ln - nx / nnm));
+            double fy = 2.0 * (Adiff * dAy + Pdiff * (ly / ln - ny / nnm));
+            atomicAdd(&a.F[vid[r]].x, fx);
+            atomicAdd(&a.F[vid[r]].y, fy);
+        }
+    }
+}
+
 // brownianParticleDynamics::integrateEquationsOfMotionCPU (src/updaters/brownianParticleDynamics.cpp:92-109)
 // + vertexModelBase::moveDegreesOfFreedom (src/models/vertexModelBase.cpp:11-47):
 // d = xi sqrt(2 dt T mu) + dt mu F, two normals per vertex (x then y)

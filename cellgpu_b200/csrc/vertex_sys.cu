@@ -30,6 +30,15 @@ static VertArgs vm_args(cg_system *s)
     return a;
 }
 
+// forces + geometry of every cell: 8 lanes per cell for rows up to 32 vertices, else a thread per cell
+static void launch_vm_forces(cg_system *s, const VertArgs &a)
+{
+    if (s->vmax <= VM_ROW_G)
+        k_vm_forces_groups<4><<<nblk(s->N, 4 * (32 / VM_G)), 128, 0, s->stream>>>(a, 1);
+    else
+        k_vm_forces<<<nblk(s->N, 128), 128, 0, s->stream>>>(a, 1);
+}
+
 static size_t vertex_bytes(long long Nc, int vmax, int n_inst)
 {
     long long Nv = 2 * Nc;
@@ -235,7 +244,7 @@ static int vm_compute_forces(cg_system *s)
     if (!s->topology_valid) return set_err(CG_ERR_STATE, "vertex topology not set");
     VertArgs a = vm_args(s);
     CG_CUDA(cudaMemsetAsync(s->F, 0, sizeof(double2) * s->Nv, s->stream));
-    k_vm_forces<<<nblk(s->N, 128), 128, 0, s->stream>>>(a, 1);
+    launch_vm_forces(s, a);
     s->kernels_enqueued += 1;
     CG_TRY(check_launch());
     return cg_synchronize(s);
@@ -273,7 +282,7 @@ static void vm_enqueue_step(cg_system *s, int kind, int t, double dt, double mu,
 {
     VertArgs a = vm_args(s);
     cudaMemsetAsync(s->F, 0, sizeof(double2) * s->Nv, s->stream);
-    k_vm_forces<<<nblk(s->N, 128), 128, 0, s->stream>>>(a, 1);
+    launch_vm_forces(s, a);
     if (kind == 0) {
         const double *nz = noise ? (per_step_noise ? noise + (size_t)t * 2 * s->Nv : noise) : nullptr;
         k_vm_brownian<<<nblk(s->Nv, 256), 256, 0, s->stream>>>(a, nz, dt, mu, T);
