@@ -631,6 +631,196 @@ CG_D bool t1_touch(int *h, int id, int &count)
     return false;
 }
 
+// ---- warp-cooperative sweep helpers: a cell row is held one entry per lane (lane k: entry k) ----
+constexpr unsigned T1_FULL = 0xffffffffu;
+
+// position of the single occurrence of target among the first n entries, or -1 when it does not
+// occur exactly once
+CG_D int wrow_find(int rk, int n, int target, int lane)
+{
+    unsigned m = __ballot_sync(T1_FULL, lane < n && rk == target);
+    return __popc(m) == 1 ? __ffs(m) - 1 : -1;
+}
+
+CG_D bool t1_touch_atomic(int *h, int id, int *count)
+{
+    unsigned sl = t1_hash_slot(id);
+    for (int p = 0; p < T1_HASH; ++p) {
+        int prev = atomicCAS(&h[sl], -1, id);
+        if (prev == -1) return atomicAdd(count, 1) + 1 < (3 * T1_HASH) / 4;
+        if (prev == id) return true;
+        sl = (sl + 1) & (T1_HASH - 1);
+    }
+    return false;
+}
+
+// t1_try for a whole warp (every lane calls it; the result, cs, vs and vertex2 are the same in every
+// lane). The four cell rows are loaded one entry per lane, found, cut and extended with ballots and
+// shuffles, and written back by the lanes. Returns 2, before writing anything, where rows are not
+// in the form that single-occurrence edits reproduce exactly (a target missing or repeated,
+// cells or vertices of the flip not distinct, rows shorter than 3); the caller then runs
+// t1_try_global in one lane. Needs vmax <= 32.
+CG_D int t1_try_warp(const VertArgs &a, const Inst &in, int key, int cs[4], int vs[4], int &vertex2, int lane)
+{
+    const int vertex1 = key / 3, vv = key % 3;
+    vertex2 = a.vn[3 * vertex1 + vv];
+    if (!(vertex1 < vertex2)) return 0;
+    double2 p1 = a.vpos[vertex1], p2 = a.vpos[vertex2];
+    int c3v1[3], c3v2[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        c3v1[f] = a.vcn[3 * vertex1 + f];
+        c3v2[f] = a.vcn[3 * vertex2 + f];
+    }
+    double2 e = min_dist(p1, p2, in.Lx, in.Ly);
+    if (!(__dsqrt_rn(__dadd_rn(__dmul_rn(e.x, e.x), __dmul_rn(e.y, e.y))) < a.t1)) return 0;
+    int c4 = cs[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        int t = c3v2[f];
+        if (t != c3v1[0] && t != c3v1[1] && t != c3v1[2]) c4 = t;
+    }
+    const int cid[4] = {c3v1[0], c3v1[1], c3v1[2], c4};
+    int nr[4];
+    int R0, R1, R2, R3;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) nr[q] = a.cvn[cid[q]];
+    R0 = lane < a.vmax ? a.cv[(size_t)cid[0] * a.vmax + lane] : 0;
+    R1 = lane < a.vmax ? a.cv[(size_t)cid[1] * a.vmax + lane] : 0;
+    R2 = lane < a.vmax ? a.cv[(size_t)cid[2] * a.vmax + lane] : 0;
+    R3 = lane < a.vmax ? a.cv[(size_t)cid[3] * a.vmax + lane] : 0;
+    auto getR = [&](int q) { return q == 0 ? R0 : q == 1 ? R1 : q == 2 ? R2 : R3; };
+    auto setR = [&](int q, int v) {
+        if (q == 0) R0 = v;
+        else if (q == 1) R1 = v;
+        else if (q == 2) R2 = v;
+        else R3 = v;
+    };
+    if (nr[0] < 3 || nr[1] < 3 || nr[2] < 3 || nr[3] < 3) return 2;
+    // vertex1's cells by the neighbours of vertex1 in their rows (t1_sets_d)
+    int i0 = -1, i1 = -1, i2 = -1, pos1[3], lq[3], nq[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        int rq = getR(q);
+        int p = wrow_find(rq, nr[q], vertex1, lane);
+        pos1[q] = p;
+        if (p < 0) return 2;
+        lq[q] = __shfl_sync(T1_FULL, rq, p == 0 ? nr[q] - 1 : p - 1);
+        nq[q] = __shfl_sync(T1_FULL, rq, p + 1 == nr[q] ? 0 : p + 1);
+        if (lq[q] == vertex2) i0 = q;
+        else if (nq[q] == vertex2) i2 = q;
+        else i1 = q;
+    }
+    if (i0 < 0 || i1 < 0 || i2 < 0 || c4 == cid[0] || c4 == cid[1] || c4 == cid[2] || cid[0] == cid[1] ||
+        cid[0] == cid[2] || cid[1] == cid[2])
+        return 2;
+    const int p3 = wrow_find(R3, nr[3], vertex2, lane);
+    if (p3 < 0) return 2;
+    cs[0] = cid[i0];
+    cs[1] = cid[i1];
+    cs[2] = cid[i2];
+    cs[3] = c4;
+    vs[0] = lq[i1];
+    vs[1] = nq[i1];
+    vs[3] = __shfl_sync(T1_FULL, R3, p3 == 0 ? nr[3] - 1 : p3 - 1);
+    vs[2] = __shfl_sync(T1_FULL, R3, p3 + 1 == nr[3] ? 0 : p3 + 1);
+    if (nr[i0] == 3 || nr[i2] == 3) return 0;
+    if (nr[i1] + 1 > a.vmax || nr[3] + 1 > a.vmax) return -1;
+    if (vs[1] == vs[2] || vs[1] == vertex1 || vs[1] == vertex2 || vs[2] == vertex1 || vs[2] == vertex2) return 2;
+    const int pa = wrow_find(getR(i0), nr[i0], vertex2, lane);  // vertex2 leaves cs[0]
+    if (pa < 0) return 2;
+    const int pb = pos1[i1], pc = pos1[i2];                      // after vertex1 in cs[1]; vertex1 leaves cs[2]
+    // ---- no return below this line: the flip is written
+    if (lane == 0) {
+        double2 mid = make_double2(__dadd_rn(p2.x, __dmul_rn(0.5, e.x)), __dadd_rn(p2.y, __dmul_rn(0.5, e.y)));
+        double2 n1 = make_double2(__dsub_rn(mid.x, e.y), __dadd_rn(mid.y, e.x));
+        double2 n2 = make_double2(__dadd_rn(mid.x, e.y), __dsub_rn(mid.y, e.x));
+        a.vpos[vertex1] = put_in_box(n1, in.Lx, in.Ly, in.iLx, in.iLy);
+        a.vpos[vertex2] = put_in_box(n2, in.Lx, in.Ly, in.iLx, in.iLy);
+    }
+    // rewiring (rows distinct): vcn of vertex1 / vertex2, vn of vertex1, vertex2, vs[1], vs[2]
+    if (lane < 3) {
+        int c = c3v1[lane];
+        a.vcn[3 * vertex1 + lane] = c == cs[2] ? cs[3] : c;
+    } else if (lane < 6) {
+        int c = c3v2[lane - 3];
+        a.vcn[3 * vertex2 + lane - 3] = c == cs[0] ? cs[1] : c;
+    }
+    if (lane < 12) {
+        const int t = lane / 3, f = lane % 3;
+        const int x = t == 0 ? vertex1 : t == 1 ? vertex2 : t == 2 ? vs[1] : vs[2];
+        int v = a.vn[3 * x + f];
+        if (t == 0 && v == vs[1]) v = vs[2];
+        else if (t == 1 && v == vs[2]) v = vs[1];
+        else if (t == 2 && v == vertex1) v = vertex2;
+        else if (t == 3 && v == vertex2) v = vertex1;
+        a.vn[3 * x + f] = v;
+    }
+    // rows: the four edits of the CPU sweep (row_remove / row_insert_after on single occurrences)
+    {
+        int r = getR(i0), up = __shfl_down_sync(T1_FULL, r, 1);
+        if (lane >= pa && lane < nr[i0] - 1) r = up;
+        setR(i0, r);
+        r = getR(i1);
+        int prev = __shfl_up_sync(T1_FULL, r, 1);
+        if (lane == pb + 1) r = vertex2;
+        else if (lane > pb + 1 && lane <= nr[i1]) r = prev;
+        setR(i1, r);
+        r = getR(i2);
+        up = __shfl_down_sync(T1_FULL, r, 1);
+        if (lane >= pc && lane < nr[i2] - 1) r = up;
+        setR(i2, r);
+        prev = __shfl_up_sync(T1_FULL, R3, 1);
+        if (lane == p3 + 1) R3 = vertex1;
+        else if (lane > p3 + 1 && lane <= nr[3]) R3 = prev;
+    }
+    nr[i0] -= 1;
+    nr[i1] += 1;
+    nr[i2] -= 1;
+    nr[3] += 1;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (lane < nr[q]) a.cv[(size_t)cid[q] * a.vmax + lane] = getR(q);
+        if (lane == 0) a.cvn[cid[q]] = nr[q];
+    }
+    __syncwarp();
+    return 1;
+}
+
+// t1_requeue for a whole warp: lanes 0-11 test one edge each, lane 0 queues the short ones
+CG_D void t1_requeue_warp(const VertArgs &a, const Inst &in, int key, int vertex2, const int vs[4], int *q, int head,
+                          int &n, int cap, bool &overflow, int lane)
+{
+    int k2 = -1;
+    if (lane < 12) {
+        const int t = lane / 3, s = lane % 3;
+        const int u = t == 0 ? key / 3 : t == 1 ? vertex2 : t == 2 ? vs[1] : vs[2];
+        const int w = a.vn[3 * u + s];
+        double2 pu = a.vpos[u], pw = a.vpos[w];
+        double2 e = u < w ? min_dist(pu, pw, in.Lx, in.Ly) : min_dist(pw, pu, in.Lx, in.Ly);
+        if (__dsqrt_rn(__dadd_rn(__dmul_rn(e.x, e.x), __dmul_rn(e.y, e.y))) < a.t1) {
+            if (u < w) {
+                k2 = 3 * u + s;
+            } else {
+                int sw = 0;
+                while (sw < 3 && a.vn[3 * w + sw] != u) ++sw;
+                if (sw < 3) k2 = 3 * w + sw;
+            }
+            if (k2 <= key) k2 = -1;
+        }
+    }
+    unsigned m = __ballot_sync(T1_FULL, k2 >= 0);
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        const int kk = __shfl_sync(T1_FULL, k2, src);
+        if (lane == 0) queue_push(q, head, n, cap, kk, overflow);
+    }
+    n = __shfl_sync(T1_FULL, n, 0);
+    overflow = __shfl_sync(T1_FULL, (int)overflow, 0) != 0;
+    __syncwarp();
+}
+
 // One block per instance. The candidates are sorted in parallel (bitonic, shared memory) and
 // evaluated in parallel on the state at the start of the sweep; then one thread replays the
 // sweep in ascending key order. A candidate rejected at the start stays rejected unless an
@@ -646,6 +836,7 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
     int *s_hash = s_v2 + T1_CAP;
     int *s_exq = s_hash + T1_HASH;
     unsigned char *s_dec = reinterpret_cast<unsigned char *>(s_exq + T1_EXQ);
+    __shared__ int s_tn;  // entries of the touched set
     const int inst = blockIdx.x;
     Ctl *ctl = a.ctl;
     if (ctl && ctl->halt) return;  // uniform
@@ -698,14 +889,17 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
             s_cs[i] = make_int4(cs[0], cs[1], cs[2], cs[3]);
             s_dec[i] = dec;
         }
+        if (threadIdx.x == 0) s_tn = 0;
         __syncthreads();
-        if (threadIdx.x == 0) {
-            // sweep: the sorted candidates merged with the keys queued by flips, kept in shared
-            // memory and moved to q[nc, 3 nv) if they outgrow it
+        if (threadIdx.x < 32) {
+            // sweep by warp 0, all lanes in step: the sorted candidates merged with the keys queued
+            // by flips, kept in shared memory and moved to q[nc, 3 nv) if they outgrow it
+            const int lane = threadIdx.x;
+            const bool warp_rows = a.vmax <= 32;
             int *ex = s_exq;
             int ecap = T1_EXQ;
             const int gcap = 3 * in.nv - nc;
-            int hm = 0, eh = 0, en = 0, touched_n = 0;
+            int hm = 0, eh = 0, en = 0;
             bool trust = true, overflow = false;
             while (hm < nc || eh < en) {
                 int key;
@@ -720,39 +914,57 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
                     pre = true;
                 }
                 if (pre && trust && s_dec[idx] == 0) {
-                    int4 c4 = s_cs[idx];
-                    bool stale = t1_touched(s_hash, 2 * (key / 3)) || t1_touched(s_hash, 2 * s_v2[idx]);
-                    if (!stale && c4.x >= 0)
-                        stale = t1_touched(s_hash, 2 * c4.x + 1) || t1_touched(s_hash, 2 * c4.y + 1) ||
-                                t1_touched(s_hash, 2 * c4.z + 1) || t1_touched(s_hash, 2 * c4.w + 1);
-                    if (!stale) continue;  // still rejected
+                    const int4 c4 = s_cs[idx];
+                    int id = -1;
+                    if (lane == 0) id = 2 * (key / 3);
+                    else if (lane == 1) id = 2 * s_v2[idx];
+                    else if (c4.x >= 0 && lane == 2) id = 2 * c4.x + 1;
+                    else if (c4.x >= 0 && lane == 3) id = 2 * c4.y + 1;
+                    else if (c4.x >= 0 && lane == 4) id = 2 * c4.z + 1;
+                    else if (c4.x >= 0 && lane == 5) id = 2 * c4.w + 1;
+                    if (!__any_sync(T1_FULL, id >= 0 && t1_touched(s_hash, id))) continue;  // still rejected
                 }
                 int cs[4] = {0, 0, 0, 0}, vs[4] = {0, 0, 0, 0}, vertex2 = 0;
-                int r = t1_try(a, in, key, cs, vs, vertex2);
+                int r = warp_rows ? t1_try_warp(a, in, key, cs, vs, vertex2, lane) : 2;
+                if (r == 2) {  // exact in-place edits by one lane
+                    int rr = 0;
+                    if (lane == 0) rr = t1_try_global(a, in, key, cs, vs, vertex2);
+                    r = __shfl_sync(T1_FULL, rr, 0);
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) {
+                        cs[t] = __shfl_sync(T1_FULL, cs[t], 0);
+                        vs[t] = __shfl_sync(T1_FULL, vs[t], 0);
+                    }
+                    vertex2 = __shfl_sync(T1_FULL, vertex2, 0);
+                    __syncwarp();
+                }
                 if (r < 0) {
                     status = CG_ERR_CAPACITY;
                     break;
                 }
                 if (r == 0) continue;
                 ++flips;
-                int ids[8] = {2 * (key / 3), 2 * vertex2, 2 * vs[1], 2 * vs[2],
-                              2 * cs[0] + 1, 2 * cs[1] + 1, 2 * cs[2] + 1, 2 * cs[3] + 1};
-                for (int t = 0; t < 8; ++t)
-                    if (!t1_touch(s_hash, ids[t], touched_n)) trust = false;
+                int tid = -1;
+                if (lane < 4) tid = 2 * (lane == 0 ? key / 3 : lane == 1 ? vertex2 : lane == 2 ? vs[1] : vs[2]);
+                else if (lane < 8) tid = 2 * cs[lane - 4] + 1;
+                bool ok = tid < 0 || t1_touch_atomic(s_hash, tid, &s_tn);
+                if (!__all_sync(T1_FULL, ok)) trust = false;
+                __syncwarp();
                 if (ex == s_exq && en + 12 > ecap) {  // room for one flip's keys, else move to global
                     int *g = q + nc;
-                    int m = en - eh;
+                    const int m = en - eh;
                     if (m + 12 > gcap) {
                         status = CG_ERR_CAPACITY;
                         break;
                     }
-                    for (int t = 0; t < m; ++t) g[t] = ex[eh + t];
+                    for (int t = lane; t < m; t += 32) g[t] = ex[eh + t];
+                    __syncwarp();
                     ex = g;
                     eh = 0;
                     en = m;
                     ecap = gcap;
                 }
-                t1_requeue(a, in, key, vertex2, vs, ex, eh, en, ecap, overflow);
+                t1_requeue_warp(a, in, key, vertex2, vs, ex, eh, en, ecap, overflow, lane);
                 if (overflow) {
                     status = CG_ERR_CAPACITY;
                     break;
