@@ -85,6 +85,8 @@ SIGNATURES = {
     "cg_precision": (_i, [_vp]),
     "cg_set_reference_positions": (_i, [_vp]),
     "cg_observables": (_i, [_vp, _d, _vp]),
+    "cg_spatial_sort": (_i, [_vp]),
+    "cg_get_tags": (_i, [_vp, _vp]),
     "cg_get_vertex_topology": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cg_set_vertex_topology": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cg_vertex_from_voronoi": (_i, [_vp, _vp]),

@@ -220,6 +220,11 @@ struct cg_system {
     int *vert_inst = nullptr, *vn = nullptr, *vcn = nullptr, *cvn = nullptr, *cv = nullptr;
     int *t1_cand = nullptr, *t1_count = nullptr;
     double t1 = 0.01;  // vertexModelBase default (src/models/vertexModelBase.cpp:59)
+    // spatial sorting (allocated on first use): keys, order / inverse, staging, CUB scratch, tags
+    unsigned long long *sort_key = nullptr;
+    int *sort_idx = nullptr, *tags = nullptr;
+    void *sort_tmp = nullptr, *sort_cub = nullptr;
+    size_t sort_tmp_bytes = 0;
     // observables (allocated on first use): reference positions, per-instance sums and means
     double2 *obs_ref = nullptr;
     double *obs_acc = nullptr, *obs_mean = nullptr;
@@ -1072,3 +1077,6 @@ extern "C" int cg_get_energies(cg_system *s, double *E)
 
 // observables
 #include "observables.cu"
+
+// spatial re-sorting
+#include "spatial_sort.cu"

@@ -61,6 +61,17 @@ class VoronoiBatch:
     def handle(self):
         return self._h
 
+    # -- spatial re-sorting
+    def spatial_sort(self):
+        """Reorder every instance's cells along a Hilbert curve (arrays and topology move with them)."""
+        check(self._lib.cg_spatial_sort(self._h))
+
+    def tags(self):
+        """For every current index, the index the cell had when the batch was created."""
+        out = np.zeros(self.Ntot, np.int32)
+        check(self._lib.cg_get_tags(self._h, ptr(out)))
+        return out
+
     # -- observables (per instance, on the device)
     OBS_FIELDS = ("mean_q", "var_q", "mean_A", "mean_P", "var_A", "var_P", "msd", "overlap")
 

@@ -267,6 +267,15 @@ int cg_precision(cg_system *sys);
 int cg_set_reference_positions(cg_system *sys);
 int cg_observables(cg_system *sys, double cutoff, double *out);
 
+/* Spatial re-sorting of a Voronoi batch (Simple2DCell::spatiallySortCells,
+ * src/models/Simple2DCell.cpp:438-477): the cells of every instance are reordered along a Hilbert
+ * curve over its box, so that neighbours sit near each other in memory. Every per-cell array and
+ * the neighbour rows move with their cells (rows keep their smallest-neighbour-first rotation);
+ * cells stay inside their instance's index range. cg_get_tags gives, for every current index, the
+ * index the cell had when the system was created (the reference's idxToTag). */
+int cg_spatial_sort(cg_system *sys);
+int cg_get_tags(cg_system *sys, int *idx_to_tag);
+
 /* counters: topology repairs, global retriangulations, T1 flips, fallbacks (per system) */
 int cg_counters(cg_system *sys, long long *out, int n);
 
