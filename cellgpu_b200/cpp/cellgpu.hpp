@@ -13,6 +13,7 @@
 //  * a failing call throws cellgpu::Error (the reference's HANDLE_ERROR throws std::exception).
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <memory>
 #include <random>
@@ -389,21 +390,31 @@ public:
         if (setcpu) throw Error(CG_ERR_ARG, "cellgpu_b200 runs on the GPU only");
     }
     void setReproducible(bool) {}
-    void setSortPeriod(int) {}
+    // re-sort the (Voronoi) configuration spatially every sp steps (src/Simulation.cpp:154-164)
+    void setSortPeriod(int sp) { sortPeriod = sp; }
     void setCurrentTime(Dscalar t) { Time = t; }
     void setCurrentTimestep(int t) { integerTimestep = t; }
     void performTimestep() { performTimesteps(1); }
     // n steps of every updater back to back on the device (one graph replay per updater chunk)
     void performTimesteps(int n)
     {
-        for (auto &u : updaters) u->Update(n);
-        integerTimestep += n;
-        Time += n * integrationTimestep;
+        while (n > 0) {
+            int chunk = n;
+            if (sortPeriod > 0) chunk = std::min(n, sortPeriod - integerTimestep % sortPeriod);
+            for (auto &u : updaters) u->Update(chunk);
+            integerTimestep += chunk;
+            Time += chunk * integrationTimestep;
+            n -= chunk;
+            if (sortPeriod > 0 && integerTimestep % sortPeriod == 0 && configuration &&
+                !configuration->isVertexModel())
+                check(cg_spatial_sort(configuration->handle()));
+        }
     }
 
     int integerTimestep = 0;
     Dscalar Time = 0.0;
     Dscalar integrationTimestep = 0.01;
+    int sortPeriod = -1;
 
 private:
     std::shared_ptr<Simple2DModel> configuration;

@@ -567,12 +567,26 @@ class Simulation:
         if self.configuration is not None:
             self.configuration.reproducible = bool(flag)
 
+    def setSortPeriod(self, sp):
+        """Spatially re-sort the (Voronoi) configuration every sp steps (src/Simulation.cpp:154-164);
+        sp <= 0 never sorts, as the reference's default."""
+        self.sortPeriod = int(sp)
+
     def performTimestep(self):
         self.performTimesteps(1)
 
     def performTimesteps(self, n):
-        """n steps of every updater back to back on the device."""
-        for u in self.updaters:
-            u.integrateEquationsOfMotion(n)
-        self.integerTimestep += n
-        self.Time += n * self.integrationTimestep
+        """n steps of every updater back to back on the device, with a spatial re-sort whenever
+        the step counter reaches a multiple of the sort period."""
+        sp = getattr(self, "sortPeriod", -1)
+        while n > 0:
+            chunk = n
+            if sp > 0:
+                chunk = min(n, sp - self.integerTimestep % sp)
+            for u in self.updaters:
+                u.integrateEquationsOfMotion(chunk)
+            self.integerTimestep += chunk
+            self.Time += chunk * self.integrationTimestep
+            n -= chunk
+            if sp > 0 and self.integerTimestep % sp == 0 and isinstance(self.configuration, VoronoiQuadraticEnergy):
+                self.configuration.batch.spatial_sort()
