@@ -254,6 +254,8 @@ def bench_batched(cg, torch, flush, steps=40, equil=150):
         b._lib.cg_set_stream(b.handle, st.cuda_stream)
         b.triangulate()
         b.spp_run(equil, dt=DT, mu=MU)
+        b.spatial_sort()
+        out[f"batched_{name}_autotune"] = b.autotune()
         s0 = C.c_int(0)
         b._lib.cg_poll(b.handle, C.byref(s0), None, 1)
         t = time_enqueued(torch, st, lambda: cg._lib.check(b._lib.cg_spp_enqueue(b.handle, 1, DT, MU)), steps, flush)

@@ -86,6 +86,7 @@ SIGNATURES = {
     "cg_set_reference_positions": (_i, [_vp]),
     "cg_observables": (_i, [_vp, _d, _vp]),
     "cg_spatial_sort": (_i, [_vp]),
+    "cg_autotune": (_i, [_vp, _vp, _vp]),
     "cg_get_tags": (_i, [_vp, _vp]),
     "cg_get_vertex_topology": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cg_set_vertex_topology": (_i, [_vp, _vp, _vp, _vp, _vp]),

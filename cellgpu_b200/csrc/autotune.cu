@@ -1,0 +1,92 @@
+// cellgpu_b200 -- launch-parameter autotuner. Included by system.cu.
+//
+// Times, on the system's current state, the runtime-selectable launch parameters and keeps the
+// fastest: the launch shape of the fused force pass (2 warps per block with at least 16 blocks per
+// SM, or 4 warps with at least 8) and the cell-list bin side of the global triangulation (0.8,
+// 1.0 or 1.25 mean cell spacings; the bin arrays allocated at creation hold all three). The local
+// repair's candidate capacities are compile-time shared-memory sizes and stay fixed. Cached step
+// graphs are dropped so the next run captures the chosen shape.
+
+static int grid_bins(cg_system *s, double target)
+{
+    int boff = 0;
+    std::vector<Inst> hi = s->h_inst;
+    for (auto &in : hi) {
+        in.nbx = std::max(1, (int)std::floor(in.Lx / target));
+        in.nby = std::max(1, (int)std::floor(in.Ly / target));
+        in.bsx = in.Lx / in.nbx;
+        in.bsy = in.Ly / in.nby;
+        in.bin_off = boff;
+        boff += in.nbx * in.nby;
+    }
+    if (boff > s->n_bins_cap) return set_err(CG_ERR_CAPACITY, "bin grid larger than allocated");
+    s->h_inst = hi;
+    s->n_bins = boff;
+    s->bin_target = target;
+    return upload_inst(s);
+}
+
+extern "C" int cg_autotune(cg_system *s, double *times_ms, int *choice)
+{
+    if (!s) return set_err(CG_ERR_ARG, "null system");
+    if (s->model != CG_MODEL_VORONOI) return CG_OK;  // the vertex-model kernels have one launch shape
+    if (!s->topology_valid) CG_TRY(triangulate_sys(s));
+    cudaEvent_t e0, e1;
+    CG_CUDA(cudaEventCreate(&e0));
+    CG_CUDA(cudaEventCreate(&e1));
+    VoroArgs a = sys_args(s);
+    const size_t fb = (s->precision == CG_FP64 ? sizeof(double2) : sizeof(float2)) * (size_t)s->N;
+    float best = 1e30f;
+    double t_force[2] = {0, 0}, t_bins[3] = {0, 0, 0};
+    for (int shape = 0; shape < 2; ++shape) {
+        for (int rep = 0; rep < 13; ++rep) {
+            if (rep == 3) cudaEventRecord(e0, s->stream);
+            cudaMemsetAsync(s->F, 0, fb, s->stream);
+            if (s->precision == CG_FP64) launch_groups<double, true, false>(a, s->N, s->stream, shape);
+            else launch_groups<float, true, false>(a, s->N, s->stream, shape);
+        }
+        cudaEventRecord(e1, s->stream);
+        CG_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        t_force[shape] = ms / 10.0;
+        if (ms < best) {
+            best = ms;
+            s->tune_force = shape;
+        }
+    }
+    const double targets[3] = {0.8, 1.0, 1.25};
+    int bbest = 0;
+    best = 1e30f;
+    for (int k = 0; k < 3; ++k) {
+        CG_TRY(grid_bins(s, targets[k]));
+        CG_TRY(triangulate_sys(s));  // warm-up
+        cudaEventRecord(e0, s->stream);
+        CG_TRY(triangulate_sys(s));
+        cudaEventRecord(e1, s->stream);
+        CG_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        t_bins[k] = ms;
+        if (ms < best) {
+            best = ms;
+            bbest = k;
+        }
+    }
+    CG_TRY(grid_bins(s, targets[bbest]));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CG_CUDA(cudaStreamSynchronize(s->stream));
+    for (auto &g : s->graphs) cudaGraphExecDestroy(g.exec);
+    s->graphs.clear();
+    if (times_ms) {
+        times_ms[0] = t_force[0];
+        times_ms[1] = t_force[1];
+        for (int k = 0; k < 3; ++k) times_ms[2 + k] = t_bins[k];
+    }
+    if (choice) {
+        choice[0] = s->tune_force;
+        choice[1] = bbest;
+    }
+    return CG_OK;
+}

@@ -45,11 +45,16 @@ extern "C" int cg_version(void) { return 100; }
 
 static inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
-// launch of the fused per-cell pass (groups of 8 lanes, CG_FORCE_WPB warps per block)
+// launch of the fused per-cell pass (groups of 8 lanes) in launch shape 0 or 1
 template <typename R, bool SCATTER, bool TEST>
-static inline void launch_groups(const VoroArgs &a, int N, cudaStream_t st)
+static inline void launch_groups(const VoroArgs &a, int N, cudaStream_t st, int shape = 0)
 {
-    k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB><<<nblk(N, CG_FORCE_WPB * GPW), CG_FORCE_WPB * 32, 0, st>>>(a);
+    if (shape == 1)
+        k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB_ALT, CG_FORCE_MINB_ALT>
+            <<<nblk(N, CG_FORCE_WPB_ALT * GPW), CG_FORCE_WPB_ALT * 32, 0, st>>>(a);
+    else
+        k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB, CG_FORCE_MINB>
+            <<<nblk(N, CG_FORCE_WPB * GPW), CG_FORCE_WPB * 32, 0, st>>>(a);
 }
 
 static Inst make_inst(double Lx, double Ly, int off, int n, int bin_off, double bin_target)
@@ -168,7 +173,7 @@ extern "C" int cg_spp_step(double *pos, double *theta, const double *F, const do
 struct cg_system {
     int model = CG_MODEL_VORONOI;
     int precision = CG_FP64;
-    int n_inst = 0, N = 0, K = 0, n_bins = 0;
+    int n_inst = 0, N = 0, K = 0, n_bins = 0, n_bins_cap = 0;
     std::vector<Inst> h_inst;
     std::vector<int> h_cell_inst;
     cudaStream_t stream = 0;
@@ -220,6 +225,9 @@ struct cg_system {
     int *vert_inst = nullptr, *vn = nullptr, *vcn = nullptr, *cvn = nullptr, *cv = nullptr;
     int *t1_cand = nullptr, *t1_count = nullptr;
     double t1 = 0.01;  // vertexModelBase default (src/models/vertexModelBase.cpp:59)
+    // autotuned launch choices: force-pass shape, cell-list bin side (in mean cell spacings)
+    int tune_force = 0;
+    double bin_target = 0.8;
     // spatial sorting (allocated on first use): keys, order / inverse, staging, CUB scratch, tags
     unsigned long long *sort_key = nullptr;
     int *sort_idx = nullptr, *tags = nullptr;
@@ -367,6 +375,7 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
     }
     s->N = off;
     s->n_bins = boff;
+    s->n_bins_cap = boff;
     int Nt = s->N;
     size_t r2 = precision == CG_FP64 ? sizeof(double2) : sizeof(float2);
     int st = sys_streams(s);
@@ -675,9 +684,9 @@ static void launch_force_test(cg_system *s, const VoroArgs &a, bool test)
     cudaMemsetAsync(s->F, 0, (s->precision == CG_FP64 ? sizeof(double2) : sizeof(float2)) * s->N,
                     s->stream);
     if (test)
-        launch_groups<R, true, true>(a, s->N, s->stream);
+        launch_groups<R, true, true>(a, s->N, s->stream, s->tune_force);
     else
-        launch_groups<R, true, false>(a, s->N, s->stream);
+        launch_groups<R, true, false>(a, s->N, s->stream, s->tune_force);
     s->kernels_enqueued += 1;
 }
 
@@ -761,7 +770,7 @@ static int enforce_t(cg_system *s)
 {
     VoroArgs a = sys_args(s);
     for (int attempt = 0; attempt < 3; ++attempt) {
-        launch_groups<R, false, true>(a, s->N, s->stream);
+        launch_groups<R, false, true>(a, s->N, s->stream, s->tune_force);
         launch_repair<R>(s, a, false);
         k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 0);
         CG_TRY(check_launch());
@@ -1080,3 +1089,6 @@ extern "C" int cg_get_energies(cg_system *s, double *E)
 
 // spatial re-sorting
 #include "spatial_sort.cu"
+
+// autotuner
+#include "autotune.cu"

@@ -478,8 +478,8 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<
     }
 }
 
-template <typename R, bool SCATTER, bool TEST, int WPB>
-__global__ void CG_FORCE_BOUNDS(WPB) k_voro_groups(VoroArgs a)
+template <typename R, bool SCATTER, bool TEST, int WPB, int MINB>
+__global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a)
 {
     __shared__ GrpTile<R> tile[WPB * GPW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;

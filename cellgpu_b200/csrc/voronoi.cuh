@@ -10,19 +10,17 @@ constexpr int R_MAX = 4;          // local repair rounds per step before escalat
 constexpr int CAND_LOCAL = 320;   // candidate slots per warp for the local (2-ring) star
 constexpr int CAND_GLOBAL = 384;  // candidate slots per warp for the cell-list star
 
-// launch shape of the fused per-cell pass: warps per block and (if > 0) the minimum resident blocks
-// per SM handed to __launch_bounds__; compile-time overridable for tuning sweeps
+// launch shapes of the fused per-cell pass (warps per block, minimum resident blocks per SM for
+// __launch_bounds__): shape 0 is the default, shape 1 the alternative the autotuner may pick;
+// both cap registers at 64 per thread
 #ifndef CG_FORCE_WPB
 #define CG_FORCE_WPB 2
 #endif
 #ifndef CG_FORCE_MINB
 #define CG_FORCE_MINB 16
 #endif
-#if CG_FORCE_MINB > 0
-#define CG_FORCE_BOUNDS(W) __launch_bounds__((W) * 32, CG_FORCE_MINB)
-#else
-#define CG_FORCE_BOUNDS(W) __launch_bounds__((W) * 32)
-#endif
+#define CG_FORCE_WPB_ALT 4
+#define CG_FORCE_MINB_ALT 8
 
 // device control block of one system
 struct Ctl {

@@ -61,6 +61,17 @@ class VoronoiBatch:
     def handle(self):
         return self._h
 
+    # -- autotuning of launch parameters
+    def autotune(self):
+        """Time the force pass's block shapes and the cell-list bin sides on the current state and
+        keep the fastest; returns the timings (ms) and the choices."""
+        t = np.zeros(5)
+        c = np.zeros(2, np.int32)
+        check(self._lib.cg_autotune(self._h, ptr(t), ptr(c)))
+        return {"force_pass_ms": t[:2].tolist(), "triangulation_ms": t[2:].tolist(),
+                "force_shape": ["2 warps/block", "4 warps/block"][int(c[0])],
+                "bin_side": [0.8, 1.0, 1.25][int(c[1])]}
+
     # -- spatial re-sorting
     def spatial_sort(self):
         """Reorder every instance's cells along a Hilbert curve (arrays and topology move with them)."""

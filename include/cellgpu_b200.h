@@ -276,6 +276,13 @@ int cg_observables(cg_system *sys, double cutoff, double *out);
 int cg_spatial_sort(cg_system *sys);
 int cg_get_tags(cg_system *sys, int *idx_to_tag);
 
+/* Autotuner (no counterpart in the reference): times the runtime-selectable launch parameters on
+ * the system's current state and keeps the fastest -- the fused force pass's block shape (0: 2 warps
+ * per block, 1: 4 warps) and the global triangulation's cell-list bin side (0: 0.8, 1: 1.0, 2: 1.25
+ * mean cell spacings). times_ms (5 values: force pass per shape, triangulation per bin side) and
+ * choice (2 values) may be NULL. Voronoi systems only (a no-op for the vertex model). */
+int cg_autotune(cg_system *sys, double *times_ms, int *choice);
+
 /* counters: topology repairs, global retriangulations, T1 flips, fallbacks (per system) */
 int cg_counters(cg_system *sys, long long *out, int n);
 
