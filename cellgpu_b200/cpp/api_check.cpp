@@ -83,7 +83,23 @@ int main(int argc, char **argv)
         fire2->minimize();
         double Vf = avm->computeEnergy();
 
-        printf("{\"voronoi\": {\"n\": %d, \"E0\": %.17g, ", nv, E0);
+        // line tension: alternating types, one gamma, then a symmetric 2 x 2 matrix
+        auto ten = std::make_shared<VoronoiQuadraticEnergyWithTension>(nv, 1.0, 3.8, true);
+        ten->setCellPositions(r2_points(nv, ten->L));
+        std::vector<int> types(nv);
+        for (int i = 0; i < nv; ++i) types[i] = i % 2;
+        ten->setCellType(types);
+        ten->setSurfaceTension(0.2);
+        ten->setUseSurfaceTension(true);
+        double T1 = ten->computeEnergy();
+        std::vector<Dscalar2> TF1 = ten->returnForces();
+        ten->setSurfaceTension(std::vector<Dscalar>{0.0, 0.35, 0.35, 0.0});
+        double T2 = ten->computeEnergy();
+
+        printf("{\"tension\": {\"E_simple\": %.17g, \"E_matrix\": %.17g, ", T1, T2);
+        print_head("F_simple", TF1, 4);
+        printf("}, ");
+        printf("\"voronoi\": {\"n\": %d, \"E0\": %.17g, ", nv, E0);
         print_head("F0", F0, 4);
         printf(", ");
         print_head("P_spp", P1, 4);

@@ -221,6 +221,55 @@ private:
 };
 using Voronoi2D = VoronoiQuadraticEnergy;
 
+// Voronoi model with line tension between cells of different types:
+// VoronoiQuadraticEnergyWithTension of inc/models/voronoiQuadraticEnergyWithTension.h:15-60
+class VoronoiQuadraticEnergyWithTension : public VoronoiQuadraticEnergy {
+public:
+    explicit VoronoiQuadraticEnergyWithTension(int n, bool reprod = false)
+        : VoronoiQuadraticEnergyWithTension(n, 1.0, 3.8, reprod) {}
+    VoronoiQuadraticEnergyWithTension(int n, Dscalar A0, Dscalar P0, bool reprod = false)
+        : VoronoiQuadraticEnergy(n, A0, P0, reprod)
+    {
+        setCellType(std::vector<int>(n, 0));
+    }
+    // Simple2DCell::setCellType
+    void setCellType(const std::vector<int> &types) { check(cg_set_cell_types(sys_, types.data())); }
+    void setUseSurfaceTension(bool use_tension)
+    {
+        Tension = use_tension;
+        apply();
+    }
+    void setSurfaceTension(Dscalar g)
+    {
+        gamma = g;
+        simpleTension = true;
+        apply();
+    }
+    // flattened ntypes x ntypes matrix, symmetric
+    void setSurfaceTension(const std::vector<Dscalar> &gammas)
+    {
+        int n = (int)std::lround(std::sqrt((double)gammas.size()));
+        if ((size_t)n * n != gammas.size()) throw Error(CG_ERR_ARG, "the tension matrix must be square");
+        tensionMatrix = gammas;
+        simpleTension = false;
+        apply();
+    }
+    Dscalar getSurfaceTension() const { return gamma; }
+
+private:
+    void apply()
+    {
+        if (!Tension) check(cg_set_tension(sys_, 0.0));
+        else if (simpleTension) check(cg_set_tension(sys_, gamma));
+        else
+            check(cg_set_tension_matrix(sys_, (int)std::lround(std::sqrt((double)tensionMatrix.size())),
+                                        tensionMatrix.data()));
+    }
+    Dscalar gamma = 0.0;
+    bool Tension = false, simpleTension = true;
+    std::vector<Dscalar> tensionMatrix;
+};
+
 // Vertex (AVM) model from the Delaunay dual of random cell positions:
 // VertexQuadraticEnergy(n, A0, P0, reprod, runSPVToInitialize) of inc/models/vertexQuadraticEnergy.h:20
 class VertexQuadraticEnergy : public Simple2DModel {

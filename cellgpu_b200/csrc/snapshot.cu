@@ -1,8 +1,9 @@
 // cellgpu_b200 -- snapshots of a system's state and exact resume. Included by system.cu.
 //
 // A snapshot is one self-describing host byte buffer: a header (model, precision, sizes, moduli,
-// T1 threshold, step counter), one record per instance (cells, box, noise key) and the per-cell
-// (and, for the vertex model, per-vertex) state with the topology. The device noise of a step is
+// T1 threshold, step counter, line tension), one record per instance (cells, box, noise key) and
+// the per-cell (and, for the vertex model, per-vertex) state with the topology, the cell types and
+// the tension matrix. The device noise of a step is
 // Philox keyed by the instance seed with the step and the local index as counters, so a system
 // restored from a snapshot draws the same noise as the original would have and continues the same
 // trajectory, up to the summation order of floating-point atomics. FIRE velocities and the
@@ -21,6 +22,8 @@ struct SnapHeader {
     int topology_valid, step;
     double KA, KP, t1;
     unsigned long long seed;
+    int has_types, tension_mode, ntypes, pad;  // line tension (Voronoi model)
+    double gamma;
 };
 
 struct SnapInst {
@@ -31,14 +34,17 @@ struct SnapInst {
 
 const char SNAP_MAGIC[8] = {'C', 'G', 'B', '2', 'S', 'N', 'P', '1'};
 
-// byte size of every array block, in the order they are stored
+// byte size of every array block, in the order they are stored (Voronoi: the cell types and the
+// tension matrix last, when present)
 void snap_layout(const SnapHeader &h, size_t sizes[9], int &count)
 {
     const size_t N = (size_t)h.N;
     if (h.model == CG_MODEL_VORONOI) {
         size_t s[] = {N * sizeof(double2), N * sizeof(double), N * sizeof(double2), N * sizeof(double2),
-                      N * sizeof(int), N * (size_t)h.K * sizeof(int)};
-        count = 6;
+                      N * sizeof(int), N * (size_t)h.K * sizeof(int),
+                      h.has_types ? N * sizeof(int) : 0,
+                      h.tension_mode == 2 ? (size_t)h.ntypes * h.ntypes * sizeof(double) : 0};
+        count = 8;
         for (int i = 0; i < count; ++i) sizes[i] = s[i];
     } else {
         const size_t Nv = (size_t)h.Nv;
@@ -64,7 +70,7 @@ SnapHeader snap_header(const cg_system *s)
     SnapHeader h;
     memset(&h, 0, sizeof(h));
     memcpy(h.magic, SNAP_MAGIC, 8);
-    h.version = 1;
+    h.version = 2;
     h.model = s->model;
     h.precision = s->precision;
     h.n_inst = s->n_inst;
@@ -77,6 +83,10 @@ SnapHeader snap_header(const cg_system *s)
     h.KP = s->KP;
     h.t1 = s->t1;
     h.seed = s->seed;
+    h.has_types = s->ctype ? 1 : 0;
+    h.tension_mode = s->tension_mode;
+    h.ntypes = s->tension_mode == 2 ? s->ntypes : 0;
+    h.gamma = s->gamma;
     return h;
 }
 
@@ -112,11 +122,11 @@ extern "C" int cg_snapshot(cg_system *s, void *buf, size_t bytes)
     size_t sizes[9];
     int count = 0;
     snap_layout(h, sizes, count);
-    const void *src_v[] = {s->pos, s->theta, s->motility, s->APpref, s->nn, s->nbr};
+    const void *src_v[] = {s->pos, s->theta, s->motility, s->APpref, s->nn, s->nbr, s->ctype, s->tmat};
     const void *src_m[] = {s->pos, s->theta, s->motility, s->APpref, s->vn, s->vcn, s->cvn, s->cv};
     const void *const *src = s->model == CG_MODEL_VORONOI ? src_v : src_m;
     for (int i = 0; i < count; ++i) {
-        CG_TRY(d2h(s, p, src[i], sizes[i]));
+        if (sizes[i]) CG_TRY(d2h(s, p, src[i], sizes[i]));
         p += sizes[i];
     }
     return CG_OK;
@@ -127,9 +137,10 @@ extern "C" int cg_restore(const void *buf, size_t bytes, cg_system **out)
     if (!buf || !out || bytes < sizeof(SnapHeader)) return set_err(CG_ERR_ARG, "bad args");
     SnapHeader h;
     memcpy(&h, buf, sizeof(h));
-    if (memcmp(h.magic, SNAP_MAGIC, 8) != 0 || h.version != 1) return set_err(CG_ERR_ARG, "not a cellgpu_b200 snapshot");
+    if (memcmp(h.magic, SNAP_MAGIC, 8) != 0 || h.version != 2) return set_err(CG_ERR_ARG, "not a cellgpu_b200 snapshot");
     if (h.n_inst <= 0 || h.N <= 0 || (h.model != CG_MODEL_VORONOI && h.model != CG_MODEL_VERTEX) ||
-        bytes < snap_total(h))
+        h.tension_mode < 0 || h.tension_mode > 2 || h.ntypes < 0 || (h.tension_mode == 2 && h.ntypes < 1) ||
+        (h.tension_mode && (h.model != CG_MODEL_VORONOI || !h.has_types)) || bytes < snap_total(h))
         return set_err(CG_ERR_ARG, "corrupt or truncated snapshot");
     const unsigned char *p = static_cast<const unsigned char *>(buf) + sizeof(h);
     std::vector<int> Ns(h.n_inst);
@@ -162,14 +173,19 @@ extern "C" int cg_restore(const void *buf, size_t bytes, cg_system **out)
         size_t sizes[9];
         int count = 0;
         snap_layout(h, sizes, count);
-        void *dst_v[] = {s->pos, s->theta, s->motility, s->APpref, s->nn, s->nbr};
+        if (h.has_types && (st = tension_alloc(s))) break;
+        if (h.tension_mode == 2 && (st = dalloc(s, &s->tmat, (size_t)h.ntypes * h.ntypes))) break;
+        void *dst_v[] = {s->pos, s->theta, s->motility, s->APpref, s->nn, s->nbr, s->ctype, s->tmat};
         void *dst_m[] = {s->pos, s->theta, s->motility, s->APpref, s->vn, s->vcn, s->cvn, s->cv};
         void **dst = h.model == CG_MODEL_VORONOI ? dst_v : dst_m;
         for (int i = 0; i < count && st == CG_OK; ++i) {
-            st = h2d(s, dst[i], p, sizes[i]);
+            if (sizes[i]) st = h2d(s, dst[i], p, sizes[i]);
             p += sizes[i];
         }
         if (st) break;
+        s->tension_mode = h.tension_mode;
+        s->ntypes = h.ntypes;
+        s->gamma = h.gamma;
         s->topology_valid = h.topology_valid != 0;
         Ctl c;
         if ((st = read_ctl(s, c))) break;

@@ -225,6 +225,11 @@ struct cg_system {
     int *vert_inst = nullptr, *vn = nullptr, *vcn = nullptr, *cvn = nullptr, *cv = nullptr;
     int *t1_cand = nullptr, *t1_count = nullptr;
     double t1 = 0.01;  // vertexModelBase default (src/models/vertexModelBase.cpp:59)
+    // line tension (off until set): per-cell types, mode, gamma or gamma matrix, per-cell term
+    int tension_mode = 0, ntypes = 0;
+    double gamma = 0.0;
+    int *ctype = nullptr;
+    double *tmat = nullptr, *TE = nullptr;
     // autotuned launch choices: force-pass shape, cell-list bin side (in mean cell spacings)
     int tune_force = 0;
     double bin_target = 0.8;
@@ -325,6 +330,12 @@ static VoroArgs sys_args(cg_system *s)
     a.cell_slot = s->cell_slot;
     a.bin_pos = s->bin_pos;
     a.n_bins = s->n_bins;
+    a.tension_mode = s->tension_mode;
+    a.ntypes = s->ntypes;
+    a.gamma = s->gamma;
+    a.ctype = s->ctype;
+    a.tmat = s->tmat;
+    a.TE = s->tension_mode ? s->TE : nullptr;
     return a;
 }
 
@@ -1080,6 +1091,9 @@ extern "C" int cg_get_energies(cg_system *s, double *E)
 
 // FIRE
 #include "fire_sys.cu"
+
+// line tension
+#include "tension.cu"
 
 // snapshots and exact resume
 #include "snapshot.cu"

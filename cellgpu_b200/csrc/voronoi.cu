@@ -336,6 +336,7 @@ struct GrpTile {
     double den[VG];
     typename Vec2<R>::T u[VG];
     typename Vec2<R>::T ca[VG];
+    double w[VG];  // line-tension weight of the edge h_k -> h_{k+1} (dual to neighbour k)
 };
 
 // Phases A-C of one group's cell (called by the whole warp; `ok` switches a group off): relative
@@ -407,6 +408,24 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
     A = group_sum<double>(Ap);
     P = group_sum<double>(Pp);
     if (TEST) fail = group_min(fail);
+    if (a.tension_mode) {  // uniform across the grid
+        // line tension: weight of every edge of the cell, and the cell's tension term sum w_k l_k
+        double Tp = 0.0;
+        const int tc = ok ? a.ctype[c] : 0;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            int k = gl + G * r;
+            if (ok && k < z) {
+                double w = tension_weight(a, tc, a.ctype[nbk[r]]);
+                T.w[k] = w;
+                double2 h0 = T.h[k], h1 = T.h[k + 1 == z ? 0 : k + 1];
+                double dx = h1.x - h0.x, dy = h1.y - h0.y;
+                Tp += w * sqrt(dx * dx + dy * dy);
+            }
+        }
+        Tp = group_sum<double>(Tp);
+        if (ok && gl == 0 && a.TE) a.TE[c] = Tp;
+    }
 }
 
 // Phases D-E (called by the whole warp): g_k = -dE_c/dh_k, the three Jacobian contractions of every
@@ -435,6 +454,13 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<
             R dPx = um.x - uk.x, dPy = um.y - uk.y;
             R gx = -R(2) * (Adiff * dAx + Pdiff * dPx);
             R gy = -R(2) * (Adiff * dAy + Pdiff * dPy);
+            if (a.tension_mode) {
+                // line tension of the cell's edges at h_k (VoronoiQuadraticEnergyWithTension:
+                // each cell's force terms count its unlike edges, src/models/voronoiQuadraticEnergyWithTension.cpp:351-361)
+                R wm = (R)T.w[km], wk = (R)T.w[k];
+                gx -= wm * um.x - wk * uk.x;
+                gy -= wm * um.y - wk * uk.y;
+            }
             // Jacobians of h_k (getdhdr, inc/utility/functions.h:234-287; always FP64: their entries
             // scale as 1/|ra x rb|^2). dh/dr_c = getdhdr(ra, rb) and dh/dr_a = getdhdr(-ra, rb-ra)
             // share the denominator 2 (ra x rb)^2 = 1 / (2 den^2).
@@ -1280,6 +1306,7 @@ __global__ void __launch_bounds__(256) k_energy(VoroArgs a, double *E)
         typename Vec2<R>::T ap = reinterpret_cast<typename Vec2<R>::T *>(a.AP)[c];
         double da = (double)ap.x - a.APpref[c].x, dp = (double)ap.y - a.APpref[c].y;
         e = a.KA * da * da + a.KP * dp * dp;
+        if (a.TE) e += 0.5 * a.TE[c];  // each unlike edge once, as computeEnergy counts it
         inst = a.cell_inst ? a.cell_inst[c] : 0;
     }
     // instances are contiguous: a block whose first and last cells share an instance reduces in

@@ -64,6 +64,19 @@ struct VoroArgs {
     int *bin_count, *bin_start, *bin_cells, *cell_bin, *cell_slot;
     double2 *bin_pos;
     int n_bins;
+    // line tension (tension_mode 0 off, 1 one gamma for unlike types, 2 gamma matrix)
+    int tension_mode, ntypes;
+    double gamma;
+    const int *ctype;
+    const double *tmat;  // ntypes x ntypes, row = the cell's own type
+    double *TE;          // per cell: sum over its unlike edges of gamma x length
 };
+
+// weight of the Voronoi edge between a cell of type ta and a neighbour of type tb
+CG_D double tension_weight(const VoroArgs &a, int ta, int tb)
+{
+    if (ta == tb) return 0.0;
+    return a.tension_mode == 1 ? a.gamma : a.tmat[ta * a.ntypes + tb];
+}
 
 }  // namespace cg

@@ -61,6 +61,21 @@ class VoronoiBatch:
     def handle(self):
         return self._h
 
+    # -- line tension (VoronoiQuadraticEnergyWithTension)
+    def set_cell_types(self, types):
+        t = np.ascontiguousarray(types, dtype=np.int32).reshape(self.Ntot)
+        check(self._lib.cg_set_cell_types(self._h, ptr(t)))
+
+    def set_tension(self, gamma):
+        """gamma per unit length on every edge between cells of different types (0: off)."""
+        check(self._lib.cg_set_tension(self._h, float(gamma)))
+
+    def set_tension_matrix(self, gamma):
+        """symmetric ntypes x ntypes matrix of edge tensions between types (empty: off)."""
+        g = np.ascontiguousarray(gamma, dtype=np.float64)
+        n = 0 if g.size == 0 else int(round(np.sqrt(g.size)))
+        check(self._lib.cg_set_tension_matrix(self._h, n, ptr(g.reshape(-1)) if n else None))
+
     # -- autotuning of launch parameters
     def autotune(self):
         """Time the force pass's block shapes and the cell-list bin sides on the current state and
@@ -395,6 +410,52 @@ class VoronoiQuadraticEnergy:
 
 
 Voronoi2D = VoronoiQuadraticEnergy
+
+
+class VoronoiQuadraticEnergyWithTension(VoronoiQuadraticEnergy):
+    """Voronoi model with line tension between cells of different types
+    (inc/models/voronoiQuadraticEnergyWithTension.h): one gamma for every unlike pair, or a
+    symmetric matrix of tensions between types (setSurfaceTension with a flattened list), applied
+    while setUseSurfaceTension(True)."""
+
+    def __init__(self, n, A0=1.0, P0=3.8, reprod=False, **kw):
+        super().__init__(n, A0, P0, reprod, **kw)
+        self.gamma = 0.0
+        self.Tension = False
+        self.simpleTension = True
+        self.tensionMatrix = None
+        self.batch.set_cell_types(np.zeros(self.Ncells, np.int32))
+
+    def _apply(self):
+        if not self.Tension:
+            self.batch.set_tension(0.0)
+        elif self.simpleTension:
+            self.batch.set_tension(self.gamma)
+        else:
+            self.batch.set_tension_matrix(self.tensionMatrix)
+        self.forcesUpToDate = False
+
+    def setCellType(self, types):
+        self.batch.set_cell_types(types)
+        self.forcesUpToDate = False
+
+    def setUseSurfaceTension(self, use_tension):
+        self.Tension = bool(use_tension)
+        self._apply()
+
+    def setSurfaceTension(self, g):
+        if np.ndim(g) == 0:
+            self.gamma, self.simpleTension = float(g), True
+        else:
+            flat = np.asarray(g, np.float64).reshape(-1)
+            n = int(round(np.sqrt(flat.size)))
+            if n * n != flat.size:
+                raise ValueError("the tension matrix must be square")
+            self.tensionMatrix, self.simpleTension = flat.reshape(n, n), False
+        self._apply()
+
+    def getSurfaceTension(self):
+        return self.gamma
 
 
 class selfPropelledParticleDynamics:

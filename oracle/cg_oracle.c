@@ -378,8 +378,80 @@ void cgo_voronoi_geometry(int N, const double *pos, const double *box, int K, co
  * cells sharing it, times dh/dr_i; the third Voronoi vertex (vother) is found through the
  * neighbour row of the base neighbour (lines 258-267). The 1e-18 norm clamp is THRESHOLD
  * (inc/std_include.h:16). Returns <0 on an inconsistent triangulation (the reference throws). */
+/* line tension between unlike cells: one gamma (ntypes == 0) or a row-major ntypes x ntypes matrix */
+typedef struct {
+    const int *ctype;
+    int ntypes;
+    double gamma;
+    const double *tmat;
+} tension_t;
+
+/* weight of the edge between a cell of type a and one of type b, as the reference reads it:
+ * gamma, or tensionMatrix[cellTypeIndexer(b, a)] = row a, column b
+ * (src/models/voronoiQuadraticEnergyWithTension.cpp:22-36, 612-620) */
+static double tension_w(const tension_t *t, int a, int b)
+{
+    if (!t || t->ctype[a] == t->ctype[b]) return 0.0;
+    return t->ntypes ? t->tmat[t->ctype[a] * t->ntypes + t->ctype[b]] : t->gamma;
+}
+
+static int voronoi_forces_impl(int N, const double *pos, const double *box, int K, const int *nn, const int *nbr,
+                               const double *AP, const double *APpref, double KA, double KP, const tension_t *ten,
+                               double *F);
+
 int cgo_voronoi_forces(int N, const double *pos, const double *box, int K, const int *nn, const int *nbr,
                        const double *AP, const double *APpref, double KA, double KP, double *F)
+{
+    return voronoi_forces_impl(N, pos, box, K, nn, nbr, AP, APpref, KA, KP, NULL, F);
+}
+
+/* VoronoiQuadraticEnergyWithTension::computeVoronoiSimpleTensionForceCPU and
+ * computeVoronoiTensionForceCPU (src/models/voronoiQuadraticEnergyWithTension.cpp:236-744): the
+ * force above plus, at each Voronoi vertex, the unit-vector derivatives of the unlike edges met
+ * there, each edge once from each of the two of the vertex's three cells that share it (the dT
+ * terms of lines 351-361, 413-422 and 443-452). ntypes == 0: one gamma for every unlike pair. */
+int cgo_voronoi_tension_forces(int N, const double *pos, const double *box, int K, const int *nn, const int *nbr,
+                               const double *AP, const double *APpref, double KA, double KP, const int *ctype,
+                               int ntypes, double gamma, const double *tmat, double *F)
+{
+    tension_t t = {ctype, ntypes, gamma, tmat};
+    return voronoi_forces_impl(N, pos, box, K, nn, nbr, AP, APpref, KA, KP, &t, F);
+}
+
+/* VoronoiQuadraticEnergyWithTension::computeEnergy (:101-159): the quadratic energy plus gamma l
+ * over every unlike Voronoi edge counted once (from its lower-indexed cell); the edge of
+ * neighbour n runs from Voronoi vertex n to vertex n+1. */
+double cgo_voronoi_tension_energy(int N, const double *pos, const double *box, int K, const int *nn,
+                                  const int *nbr, const double *AP, const double *APpref, double KA, double KP,
+                                  const int *ctype, int ntypes, double gamma, const double *tmat)
+{
+    tension_t t = {ctype, ntypes, gamma, tmat};
+    double E = cgo_voronoi_energy(N, AP, APpref, KA, KP);
+    double voro[2 * 64];
+    for (int i = 0; i < N; ++i) {
+        int z = nn[i];
+        const int *ns = nbr + i * K;
+        double rij[2], rik[2];
+        cgo_min_dist(box, pos + 2 * ns[z - 1], pos + 2 * i, rij);
+        for (int n = 0; n < z; ++n) {
+            cgo_min_dist(box, pos + 2 * ns[n], pos + 2 * i, rik);
+            circumcenter0(rij, rik, voro + 2 * n);
+            rij[0] = rik[0];
+            rij[1] = rik[1];
+        }
+        for (int n = 0; n < z; ++n) {
+            if (i >= ns[n] || ctype[i] == ctype[ns[n]]) continue;
+            const double *a = voro + 2 * n, *b = voro + 2 * ((n + 1) % z);
+            double dx = a[0] - b[0], dy = a[1] - b[1];
+            E += sqrt(dx * dx + dy * dy) * tension_w(&t, i, ns[n]);
+        }
+    }
+    return E;
+}
+
+static int voronoi_forces_impl(int N, const double *pos, const double *box, int K, const int *nn, const int *nbr,
+                               const double *AP, const double *APpref, double KA, double KP, const tension_t *ten,
+                               double *F)
 {
     const double thr = 1e-18;
     double voro[2 * 64];
@@ -442,6 +514,9 @@ int cgo_voronoi_forces(int N, const double *pos, const double *box, int K, const
             if (dnn < thr) dnn = thr;
             if (dln < thr) dln = thr;
             double dPi[2] = {dl[0] / dln - dn[0] / dnn, dl[1] / dln - dn[1] / dnn};
+            /* own unlike edges at vcur: (vcur, vnext) shared with base, (vlast, vcur) with other */
+            double wib = tension_w(ten, i, base), wio = tension_w(ten, i, other);
+            double dT[2] = {-wib * dn[0] / dnn + wio * dl[0] / dln, -wib * dn[1] / dnn + wio * dl[1] / dln};
 
             int z2 = nn[base];
             int dto = -1;
@@ -467,6 +542,10 @@ int cgo_voronoi_forces(int N, const double *pos, const double *box, int K, const
             if (dnn < thr) dnn = thr;
             if (dln < thr) dln = thr;
             double dPk[2] = {dl[0] / dln - dn[0] / dnn, dl[1] / dln - dn[1] / dnn};
+            /* base's unlike edges at vcur: (vcur, vnext) with i, (vcur, vother) with other */
+            double wbo = tension_w(ten, base, other);
+            dT[0] += wib * dl[0] / dln - wbo * dn[0] / dnn;
+            dT[1] += wib * dl[1] / dln - wbo * dn[1] / dnn;
 
             double dAj[2] = {0.5 * (vother[1] - vlast[1]), 0.5 * (vlast[0] - vother[0])};
             dl[0] = vother[0] - vcur[0]; dl[1] = vother[1] - vcur[1];
@@ -476,6 +555,9 @@ int cgo_voronoi_forces(int N, const double *pos, const double *box, int K, const
             if (dnn < thr) dnn = thr;
             if (dln < thr) dln = thr;
             double dPj[2] = {dl[0] / dln - dn[0] / dnn, dl[1] / dln - dn[1] / dnn};
+            /* other's unlike edges at vcur: (vlast, vcur) with i, (vother, vcur) with base */
+            dT[0] += -wio * dn[0] / dnn + wbo * dl[0] / dln;
+            dT[1] += -wio * dn[1] / dnn + wbo * dl[1] / dln;
 
             double ex = 2.0 * Adiff * dAi[0] + 2.0 * Pdiff * dPi[0];
             double ey = 2.0 * Adiff * dAi[1] + 2.0 * Pdiff * dPi[1];
@@ -483,6 +565,8 @@ int cgo_voronoi_forces(int N, const double *pos, const double *box, int K, const
             ey += 2.0 * Akd * dAk[1] + 2.0 * Pkd * dPk[1];
             ex += 2.0 * Ajd * dAj[0] + 2.0 * Pjd * dPj[0];
             ey += 2.0 * Ajd * dAj[1] + 2.0 * Pjd * dPj[1];
+            ex += dT[0];
+            ey += dT[1];
             /* v*M (inc/utility/Matrix.h:128-135) */
             const double *M = dh + 4 * n;
             fx += ex * M[0] + ey * M[2];

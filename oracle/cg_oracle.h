@@ -37,6 +37,12 @@ void cgo_voronoi_geometry(int N, const double *pos, const double *box, int K, co
 int cgo_voronoi_forces(int N, const double *pos, const double *box, int K, const int *nn, const int *nbr,
                        const double *AP, const double *APpref, double KA, double KP, double *F);
 double cgo_voronoi_energy(int N, const double *AP, const double *APpref, double KA, double KP);
+int cgo_voronoi_tension_forces(int N, const double *pos, const double *box, int K, const int *nn, const int *nbr,
+                               const double *AP, const double *APpref, double KA, double KP, const int *ctype,
+                               int ntypes, double gamma, const double *tmat, double *F);
+double cgo_voronoi_tension_energy(int N, const double *pos, const double *box, int K, const int *nn,
+                                  const int *nbr, const double *AP, const double *APpref, double KA, double KP,
+                                  const int *ctype, int ntypes, double gamma, const double *tmat);
 
 /* ---- self-propelled particle dynamics, CPU semantics (src/updaters/selfPropelledParticleDynamics.cpp:67-101) ---- */
 void cgo_spp_step(int N, double *pos, const double *box, const double *F, double *theta, const double *motility,

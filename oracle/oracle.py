@@ -68,6 +68,11 @@ def lib():
                                          C.c_double, _dp]
         L.cgo_voronoi_energy.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_double]
         L.cgo_voronoi_energy.restype = C.c_double
+        L.cgo_voronoi_tension_forces.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, _ip, _dp, _dp, C.c_double,
+                                                 C.c_double, _ip, C.c_int, C.c_double, C.c_void_p, _dp]
+        L.cgo_voronoi_tension_energy.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, _ip, _dp, _dp, C.c_double,
+                                                 C.c_double, _ip, C.c_int, C.c_double, C.c_void_p]
+        L.cgo_voronoi_tension_energy.restype = C.c_double
         L.cgo_spp_step.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double]
         L.cgo_voronoi_spp_run.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, _ip, _dp, _dp, _dp,
                                           C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp,
@@ -171,6 +176,43 @@ def voronoi_forces(pos, box, nn, nbr, AP, APpref, KA=1.0, KP=1.0):
 def voronoi_energy(AP, APpref, KA=1.0, KP=1.0):
     AP = _f64(AP)
     return lib().cgo_voronoi_energy(AP.shape[0], AP, _f64(APpref), KA, KP)
+
+
+def _tension_args(types, gamma, gammas):
+    types = np.ascontiguousarray(types, np.int32)
+    if gammas is None:
+        return types, 0, float(gamma), None, None
+    g = np.ascontiguousarray(gammas, np.float64)
+    return types, int(round(np.sqrt(g.size))), 0.0, g.ctypes.data_as(C.c_void_p), g
+
+
+def voronoi_tension_forces(pos, box, nn, nbr, AP, APpref, types, gamma=0.0, gammas=None, KA=1.0, KP=1.0):
+    """Forces with line tension between unlike cells: one gamma, or the ntypes x ntypes matrix
+    gammas (row = own type)."""
+    pos = _f64(pos)
+    nbr = np.ascontiguousarray(nbr, np.int32)
+    F = np.zeros((pos.shape[0], 2))
+    types, nt, g, tp, _keep = _tension_args(types, gamma, gammas)
+    st = lib().cgo_voronoi_tension_forces(pos.shape[0], pos, _box(box), nbr.shape[1],
+                                          np.ascontiguousarray(nn, np.int32), nbr, _f64(AP), _f64(APpref), KA,
+                                          KP, types, nt, g, tp, F)
+    if st:
+        raise RuntimeError("oracle: inconsistent triangulation")
+    return F
+
+
+def voronoi_tension_energy(pos, box, nn, nbr, AP, APpref, types, gamma=0.0, gammas=None, KA=1.0, KP=1.0):
+    pos = _f64(pos)
+    nbr = np.ascontiguousarray(nbr, np.int32)
+    types, nt, g, tp, _keep = _tension_args(types, gamma, gammas)
+    return lib().cgo_voronoi_tension_energy(pos.shape[0], pos, _box(box), nbr.shape[1],
+                                            np.ascontiguousarray(nn, np.int32), nbr, _f64(AP), _f64(APpref), KA,
+                                            KP, types, nt, g, tp)
+
+
+def spp_step(pos, box, F, theta, motility, noise, dt=0.01, mu=1.0):
+    """One self-propelled step in place (pos, theta) with the forces F and one normal per cell."""
+    lib().cgo_spp_step(pos.shape[0], pos, _box(box), _f64(F), theta, _f64(motility), _f64(noise), dt, mu)
 
 
 def voronoi_spp_run(pos, box, nn, nbr, theta, motility, APpref, noise, dt=0.01, mu=1.0, KA=1.0,

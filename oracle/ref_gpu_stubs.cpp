@@ -41,3 +41,5 @@ bool gpu_vm_test_edges_for_T1(double2*, int*, int*, int*, int*, int*, gpubox&, d
 bool gpu_zero_array(int*, int) { return cg_ref_gpu_stub("gpu_zero_array"); }
 bool gpu_zero_array(unsigned int*, int) { return cg_ref_gpu_stub("gpu_zero_array"); }
 bool gpu_zero_velocity(double2*, int) { return cg_ref_gpu_stub("gpu_zero_velocity"); }
+bool gpu_VoronoiTension_force_sets(double2*, double2*, double2*, int2*, int*, double2*, double4*, double2*, int2*, int*, double*, Index2D&, double, double, int, Index2D&, gpubox&) { return cg_ref_gpu_stub("gpu_VoronoiTension_force_sets"); }
+bool gpu_VoronoiSimpleTension_force_sets(double2*, double2*, double2*, int2*, int*, double2*, double4*, double2*, int2*, int*, double, double, double, int, Index2D&, gpubox&) { return cg_ref_gpu_stub("gpu_VoronoiSimpleTension_force_sets"); }

@@ -18,6 +18,7 @@
 #include "selfPropelledParticleDynamics.h"
 #include "vertexQuadraticEnergy.h"
 #include "voronoiQuadraticEnergy.h"
+#include "voronoiQuadraticEnergyWithTension.h"
 
 namespace {
 
@@ -26,6 +27,18 @@ class RefVoronoi : public VoronoiQuadraticEnergy {
   public:
     RefVoronoi(int n, Dscalar A0, Dscalar P0) : VoronoiQuadraticEnergy(n, A0, P0, true) {}
     int neigh_max() const { return neighMax; }
+    void retriangulate()
+    {
+        globalTriangulationCGAL();
+        resetLists();
+        allDelSets();
+    }
+};
+
+// the line-tension model, with the same retriangulation access
+class RefVoronoiTension : public VoronoiQuadraticEnergyWithTension {
+  public:
+    RefVoronoiTension(int n, Dscalar A0, Dscalar P0) : VoronoiQuadraticEnergyWithTension(n, A0, P0, true) {}
     void retriangulate()
     {
         globalTriangulationCGAL();
@@ -272,6 +285,33 @@ int ref_vertex_brownian_run(void *h, int steps, double dt, double T, double mu)
     }
     for (int t = 0; t < steps; ++t) s->sim->performTimestep();
     return 0;
+}
+
+// ---- Voronoi model with line tension: forces, A/P and energy of one state ---------------------
+// gammas == NULL: one tension gamma for every pair of unlike types (setSurfaceTension(g));
+// else an ntypes x ntypes matrix (setSurfaceTension(vector)). Returns computeEnergy().
+double ref_voronoi_tension_forces(int n, const double *pos, const int *types, const double *pref, double gamma,
+                                  int ntypes, const double *gammas, double *F, double *AP)
+{
+    RefVoronoiTension v(n, 1.0, 3.8);
+    v.setCPU(true);
+    std::vector<Dscalar2> p(n), ap(n);
+    for (int i = 0; i < n; ++i) {
+        p[i] = make_Dscalar2(pos[2 * i], pos[2 * i + 1]);
+        ap[i] = make_Dscalar2(pref[2 * i], pref[2 * i + 1]);
+    }
+    v.setCellPositions(p);
+    v.retriangulate();
+    std::vector<int> t(types, types + n);
+    v.setCellType(t);
+    v.setCellPreferences(ap);
+    if (gammas) v.setSurfaceTension(std::vector<Dscalar>(gammas, gammas + (size_t)ntypes * ntypes));
+    else v.setSurfaceTension(gamma);
+    v.setUseSurfaceTension(true);
+    v.computeForces();
+    to_host(v.returnForces(), reinterpret_cast<Dscalar2 *>(F), n);
+    to_host(v.returnAreaPeri(), reinterpret_cast<Dscalar2 *>(AP), n);
+    return v.computeEnergy();
 }
 
 }  // extern "C"

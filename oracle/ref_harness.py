@@ -47,8 +47,27 @@ def lib():
         L.ref_vertex_forces.restype = C.c_double
         L.ref_vertex_forces.argtypes = [C.c_void_p, _dp, _dp]
         L.ref_vertex_brownian_run.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.ref_voronoi_tension_forces.restype = C.c_double
+        L.ref_voronoi_tension_forces.argtypes = [C.c_int, _dp, _ip, _dp, C.c_double, C.c_int, C.c_void_p, _dp,
+                                                 _dp]
         _lib = L
     return _lib
+
+
+def voronoi_tension_forces(pos, types, pref, gamma=0.0, gammas=None):
+    """The reference's VoronoiQuadraticEnergyWithTension (CPU branch) on one state: forces, A/P and
+    computeEnergy(). gammas: an ntypes x ntypes matrix, else one gamma for unlike types."""
+    pos = np.ascontiguousarray(pos, np.float64)
+    n = len(pos)
+    F = np.zeros((n, 2))
+    AP = np.zeros((n, 2))
+    g = None if gammas is None else np.ascontiguousarray(gammas, np.float64)
+    nt = 0 if g is None else int(round(np.sqrt(g.size)))
+    with quiet():
+        E = lib().ref_voronoi_tension_forces(n, pos, np.ascontiguousarray(types, np.int32),
+                                             np.ascontiguousarray(pref, np.float64), float(gamma), nt,
+                                             None if g is None else g.ctypes.data_as(C.c_void_p), F, AP)
+    return F, AP, E
 
 
 class quiet:

@@ -92,6 +92,22 @@ def fire_case(N, seed, vertex=False):
                         pos1=pos1, nn1=nn1, nbr1=nbr1, F1=F1, AP1=AP1, E1=E1, cutoff=1e-10, max_iterations=3000)
 
 
+def tension_case(N, seed):
+    """VoronoiQuadraticEnergyWithTension: three cell types, one gamma for unlike types and a
+    symmetric tension matrix."""
+    L = float(np.sqrt(N))
+    rng = np.random.default_rng(seed)
+    pos = rng.random((N, 2)) * L
+    types = rng.integers(0, 3, N).astype(np.int32)
+    pref = np.stack([np.ones(N), rng.uniform(3.7, 3.9, N)], 1)
+    gammas = np.array([[0.0, 0.1, 0.3], [0.1, 0.0, 0.2], [0.3, 0.2, 0.0]])
+    Fs, APs, Es = R.voronoi_tension_forces(pos, types, pref, gamma=0.15)
+    Fm, APm, Em = R.voronoi_tension_forces(pos, types, pref, gammas=gammas)
+    np.savez_compressed(os.path.join(HERE, f"tension_N{N}_s{seed}.npz"), N=N, box=np.array([L, L]), pos=pos,
+                        types=types, pref=pref, gamma=0.15, gammas=gammas, F_simple=Fs, AP_simple=APs,
+                        E_simple=Es, F_matrix=Fm, AP_matrix=APm, E_matrix=Em)
+
+
 if __name__ == "__main__":
     if not R.available():
         raise SystemExit("oracle/_ref/libcgref.so missing: make -C oracle -f Makefile.ref")
@@ -100,4 +116,5 @@ if __name__ == "__main__":
     vertex_case(400, 15)
     fire_case(200, 3)
     fire_case(200, 4, vertex=True)
+    tension_case(400, 5)
     print("golden fixtures written to", HERE)

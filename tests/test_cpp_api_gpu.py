@@ -1,6 +1,6 @@
 """The C++ class API (cellgpu_b200/cpp/cellgpu.hpp: Simulation, VoronoiQuadraticEnergy,
-VertexQuadraticEnergy, selfPropelledParticleDynamics, brownianParticleDynamics,
-EnergyMinimizerFIRE) against the Python API on the same deterministic states.
+VoronoiQuadraticEnergyWithTension, VertexQuadraticEnergy, selfPropelledParticleDynamics,
+brownianParticleDynamics, EnergyMinimizerFIRE) against the Python API on the same deterministic states.
 
 Tolerances (written here): energies and forces of one state 1e-12 relative / absolute (same
 kernels); trajectories after 50 steps with device noise 1e-9 (floating-point atomics order);
@@ -59,6 +59,19 @@ def test_cpp_class_api_matches_python(cglib):
     b.fire_minimize(FireParams.defaults(force_cutoff=1e-10, max_iterations=10000))
     b.compute_forces()
     assert _rel(b.energies()[0], v["E_fire"]) < 1e-9
+
+    # VoronoiQuadraticEnergyWithTension through both APIs
+    from cellgpu_b200 import VoronoiQuadraticEnergyWithTension
+    t = VoronoiQuadraticEnergyWithTension(n, 1.0, 3.8, True)
+    t.setCellPositions(_r2(n, L))
+    t.setCellType(np.arange(n) % 2)
+    t.setSurfaceTension(0.2)
+    t.setUseSurfaceTension(True)
+    assert _rel(t.computeEnergy(), d["tension"]["E_simple"]) < 1e-12
+    assert np.abs(t.returnForces()[:4].ravel() - np.array(d["tension"]["F_simple"])).max() < 1e-12
+    t.setSurfaceTension([0.0, 0.35, 0.35, 0.0])
+    assert _rel(t.computeEnergy(), d["tension"]["E_matrix"]) < 1e-12
+    assert d["tension"]["E_matrix"] > d["tension"]["E_simple"] > v["E0"]
 
     nc = 240
     Lv = math.sqrt(nc)

@@ -92,6 +92,49 @@ def test_fire_vertex_golden(oracle):
     assert abs(oracle.voronoi_energy(AP, np.tile([1.0, 3.8], (Nc, 1))) - float(g["E1"])) < 1e-9
 
 
+@pytest.mark.parametrize("mode", ["simple", "matrix"])
+def test_tension_golden(oracle, mode):
+    """VoronoiQuadraticEnergyWithTension: forces and energy with one gamma for unlike types and
+    with a symmetric tension matrix."""
+    g = _load("tension_N*.npz")[0]
+    pos, box = g["pos"], tuple(g["box"])
+    nn, nbr = oracle.periodic_delaunay(pos, box, 16)
+    AP = oracle.voronoi_geometry(pos, box, nn, nbr)
+    kw = dict(gamma=float(g["gamma"])) if mode == "simple" else dict(gammas=g["gammas"])
+    F = oracle.voronoi_tension_forces(pos, box, nn, nbr, AP, g["pref"], g["types"], **kw)
+    E = oracle.voronoi_tension_energy(pos, box, nn, nbr, AP, g["pref"], g["types"], **kw)
+    assert np.abs(AP - g["AP_" + mode]).max() < 1e-12
+    assert force_error(F, g["F_" + mode]) < 1e-12
+    assert abs(E - float(g["E_" + mode])) < 1e-10 * abs(E)
+
+
+def test_tension_forces_are_a_gradient(oracle):
+    """The tension forces are minus the gradient of the quadratic energy plus every unlike edge's
+    gamma l counted from both of its cells (central differences, topology held fixed)."""
+    from helpers import monolayer
+    pos, box = monolayer(80, 11)
+    N = len(pos)
+    nn, nbr = oracle.periodic_delaunay(pos, box, 16)
+    rng = np.random.default_rng(3)
+    types = rng.integers(0, 2, N)
+    pref = np.tile([1.0, 3.8], (N, 1))
+
+    def energy(p):
+        AP = oracle.voronoi_geometry(p, box, nn, nbr)
+        quad = oracle.voronoi_energy(AP, pref)
+        return quad + 2.0 * (oracle.voronoi_tension_energy(p, box, nn, nbr, AP, pref, types, gamma=0.2) - quad)
+
+    AP = oracle.voronoi_geometry(pos, box, nn, nbr)
+    F = oracle.voronoi_tension_forces(pos, box, nn, nbr, AP, pref, types, gamma=0.2)
+    h = 1e-6
+    for c in rng.choice(N, 12, replace=False):
+        for d in range(2):
+            p1, p2 = pos.copy(), pos.copy()
+            p1[c, d] += h
+            p2[c, d] -= h
+            assert abs(-(energy(p1) - energy(p2)) / (2 * h) - F[c, d]) < 1e-6 * max(1.0, np.abs(F).max())
+
+
 @pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libcgref.so")),
                     reason="reference build not present")
 def test_live_reference_spp_matches_oracle(oracle):
