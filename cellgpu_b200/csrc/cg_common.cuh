@@ -242,6 +242,89 @@ CG_D int incircle0(double2 a, double2 b, double2 c)
 }
 
 // ------------------------------------------------------------------------------------------
+// The in-circle test of the triangulation, the same for every cell that asks it.
+//
+// Each cell evaluates predicates on positions relative to itself, formed by min_dist (one rounded
+// difference and one rounded wrap: each coordinate is off the exact periodic difference by at most
+// 1.5 u L, u = 2^-53, L = the larger box side). Exact arithmetic on those rounded inputs is exact
+// for that cell only: when four cells are cocircular to within that rounding (relaxed fluid states
+// drive Voronoi edges to zero length), two cells of the same quadrilateral can take opposite
+// decisions and the rows stop matching. So:
+//  * the floating-point filter decides only when its margin also covers the input rounding of this
+//    cell's frame and of the canonical frame below; then its sign is the sign of the exact periodic
+//    configuration, which every frame agrees on;
+//  * otherwise the four points are re-expressed relative to the one with the smallest global index,
+//    by min_dist from the absolute positions. Every cell computes the same doubles there, and the
+//    exact determinant of those doubles decides;
+//  * an exact zero (cocircular points) is resolved by simulation of simplicity (H. Edelsbrunner and
+//    E. P. Mucke, ACM Trans. Graph. 9, 1990): the lifted coordinate |p|^2 of the point with the
+//    smallest index is raised by an infinitesimal, so the sign is that of its cofactor, the
+//    orientation of the other three points. The triangulation is then the unique Delaunay
+//    triangulation of the perturbed set, whichever cell asks.
+// incircle_g(c; a, b, t) keeps the sign convention of incircle0 in c's frame: negative iff t lies
+// inside the circle through c, a and b (c, a, b counter-clockwise).
+// ------------------------------------------------------------------------------------------
+
+// sign of p x q + q x r + r x p (the orientation of p, q, r), exactly
+__device__ __noinline__ int orient3_exact(double2 p, double2 q, double2 r)
+{
+    double e1[4], e2[4], e3[4], s12[8], s[12], scr[12];
+    int n1 = exp_diff_prod(p.x, q.y, p.y, q.x, e1);
+    int n2 = exp_diff_prod(q.x, r.y, q.y, r.x, e2);
+    int n3 = exp_diff_prod(r.x, p.y, r.y, p.x, e3);
+    int n12 = exp_sum(n1, e1, n2, e2, s12, scr);
+    int ns = exp_sum(n12, s12, n3, e3, s, scr);
+    return exp_sign(ns, s);
+}
+
+// canonical-frame exact evaluation with the simulation-of-simplicity tie break
+__device__ __noinline__ int incircle_canonical(int ic, int ia, int ib, int it, const double2 *pos, double Lx,
+                                               double Ly)
+{
+    const int id[4] = {ic, ia, ib, it};
+    int j = 0;
+    for (int k = 1; k < 4; ++k)
+        if (id[k] < id[j]) j = k;
+    const double2 pm = pos[id[j]];
+    double2 q[3];
+    int n = 0;
+    for (int k = 0; k < 4; ++k)
+        if (k != j) q[n++] = min_dist(pos[id[k]], pm, Lx, Ly);
+    // D(c,a,b,t) as a 4x4 lifted determinant is alternating in its rows: moving the point of
+    // position j to the front takes j transpositions
+    const int par = (j & 1) ? -1 : 1;
+    int s = incircle0_exact(q[0].x, q[0].y, q[1].x, q[1].y, q[2].x, q[2].y);
+    if (s != 0) return par * s;
+    return -par * orient3_exact(q[0], q[1], q[2]);
+}
+
+// filter with the input-rounding margin: +-1, or 0 when the canonical evaluation must decide.
+// The derivative of D with respect to any coordinate is at most 4 M^3 (M = the largest |a|, |b|,
+// |t|; the canonical frame's coordinates are at most 2M): six coordinates, both frames, each input
+// off by at most 1.5 u L, doubled for safety -> 2 * (24 + 192) * 1.5 u L M^3 < 7.2e-14 L M^3, and
+// M^3 <= M^2 (1 + M^2) / 2 avoids a square root.
+// The arithmetic error of det is below 1e-14 times the sum of its terms' magnitudes, itself at
+// most 6 M^4 (|b.x t.y| + |b.y t.x| <= 2 M^2 and so on).
+CG_D int incircle_filter(double2 a, double2 b, double2 t, double Lmax)
+{
+    double aa = a.x * a.x + a.y * a.y, bb = b.x * b.x + b.y * b.y, tt = t.x * t.x + t.y * t.y;
+    double bxt = b.x * t.y - b.y * t.x, axt = a.x * t.y - a.y * t.x, axb = a.x * b.y - a.y * b.x;
+    double det = aa * bxt - bb * axt + tt * axb;
+    double m2 = fmax(aa, fmax(bb, tt));
+    double bound = m2 * (6.0e-14 * m2 + 3.6e-14 * Lmax * (1.0 + m2));
+    if (det > bound) return 1;
+    if (-det > bound) return -1;
+    return 0;
+}
+
+CG_D int incircle_g(double2 a, double2 b, double2 t, int ic, int ia, int ib, int it, const double2 *pos,
+                    double Lx, double Ly)
+{
+    int s = incircle_filter(a, b, t, fmax(Lx, Ly));
+    return s ? s : incircle_canonical(ic, ia, ib, it, pos, Lx, Ly);
+}
+
+// ------------------------------------------------------------------------------------------
 // Philox4x32-10 counter-based RNG (J. K. Salmon et al., "Parallel random numbers: as easy as
 // 1, 2, 3", SC'11), and normal deviates by the Box-Muller transform. Counter = (cell, step,
 // stream, 0), key = seed; a run can be resumed exactly from its step counter.

@@ -149,7 +149,7 @@ CG_D int cell_pass(const VoroArgs &a, int c, const int *row, int z, double2 pc, 
         double2 dC = min_dist(pos[nC], pc, Lx, Ly);
         if (TEST && !fail) {
             if (orient0(dB, dC) <= 0) fail = -(k + 1);
-            else if (c < nB && incircle0(dA, dB, dC) < 0) fail = k + 1;
+            else if (c < nB && incircle_g(dA, dB, dC, c, nA, nB, nC, pos, Lx, Ly) < 0) fail = k + 1;
         }
         double2 hnext = (kn == 0) ? hfirst : circum0<double>(dB, dC);
         Asum += fabs(0.5 * (hprev.x * hnext.y - hprev.y * hnext.x));
@@ -158,6 +158,7 @@ CG_D int cell_pass(const VoroArgs &a, int c, const int *row, int z, double2 pc, 
         hprev = hnext;
         dA = dB;
         dB = dC;
+        nA = nB;
         nB = nC;
     }
     A_out = (R)Asum;
@@ -360,6 +361,7 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
     // phase B: Voronoi vertices h_k = circumcentre(0, r_{k-1}, r_k) (inc/utility/functions.h:34-43);
     // exact local Delaunay test
     fail = 0x7fffffff;  // smallest failing slot (x2, +1 for orientation)
+    int undecided = 0;  // slots whose in-circle sign the filter left to the canonical evaluation
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
         int k = gl + G * r;
@@ -373,8 +375,22 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
             T.h[k] = make_double2(den * (an * rb.y - ra.y * bn), den * (ra.x * bn - an * rb.x));
             if (TEST) {
                 double2 rc = T.r[k + 1 == z ? 0 : k + 1];
-                if (orient0(rb, rc) <= 0) fail = min(fail, 2 * k + 1);
-                else if (c < nbk[r] && incircle0(ra, rb, rc) < 0) fail = min(fail, 2 * k);
+                if (orient0(rb, rc) <= 0) {
+                    fail = min(fail, 2 * k + 1);
+                } else if (c < nbk[r]) {
+                    int ic = incircle_filter(ra, rb, rc, fmax(Lx, Ly));
+                    if (ic < 0) fail = min(fail, 2 * k);
+                    if (ic == 0) undecided |= 1 << r;
+                }
+            }
+        }
+    }
+    if (TEST && __any_sync(0xffffffffu, undecided != 0)) {
+        for (int r = 0; r < 2; ++r) {
+            int k = gl + G * r;
+            if (undecided & (1 << r)) {
+                int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
+                if (incircle_canonical(c, row[km], nbk[r], row[kp], a.pos, Lx, Ly) < 0) fail = min(fail, 2 * k);
             }
         }
     }
@@ -622,11 +638,17 @@ __global__ void k_round_end(VoroArgs a, unsigned long long cond, int use_cond)
 // intervals reach below the smallest upper end. Writes global indices, CCW, rotated to start at the
 // smallest index. Returns z, -1 (not enclosed), -2 (capacity).
 // ------------------------------------------------------------------------------------------
-CG_D bool inner_than(double2 pa, double2 pc, int ic, double2 pb, int ib)
+struct StarFrame {
+    int self;            // global index of the cell at the origin
+    const double2 *pos;  // absolute positions, for the canonical-frame predicate
+    double Lx, Ly;
+};
+
+// is c's circle through (0,a,c) strictly inside b's circle (0,a,b)?  <=> c inside circle(0,a,b);
+// incircle_g never returns 0, so the order is strict
+CG_D bool inner_than(const StarFrame &f, double2 pa, int ia, double2 pc, int ic, double2 pb, int ib)
 {
-    // is c's circle through (0,a,c) strictly inside b's circle (0,a,b)?  <=> c inside circle(0,a,b)
-    int s = incircle0(pa, pb, pc);
-    return s < 0 || (s == 0 && ic < ib);
+    return incircle_g(pa, pb, pc, f.self, ia, ib, ic, f.pos, f.Lx, f.Ly) < 0;
 }
 
 // Position of the circle through 0, a and t in the pencil of circles through 0 and a: its centre is
@@ -636,17 +658,22 @@ CG_D bool inner_than(double2 pa, double2 pc, int ic, double2 pb, int ib)
 // u = 2^-53, the numerator's error is below 4u(|t.x dx| + |t.y dy|), the cross product's below
 // ED = 3u(|a.x t.y| + |a.y t.x|), and for den > ED the quotient's below
 // |num| ED / (den (den - ED)) + EN / (den - ED), plus u|s| for the division; the interval doubles
-// the total. Near-collinear t (den <= 2 ED) gets an unbounded interval.
-CG_D void pencil_key(double2 a, double2 t, double &lo, double &hi)
+// the total. The interval must also hold the key of every frame the exact comparison may use (see
+// incircle_g): inputs off by at most q = 4.5 u L per coordinate move num by at most
+// q (3|t|_1 + |a|_1) and den by at most q (|t|_1 + |a|_1), which is added the same way.
+// Near-collinear t (den <= 2 (ED + that)) gets an unbounded interval.
+CG_D void pencil_key(double2 a, double2 t, double Lmax, double &lo, double &hi)
 {
     const double u = 1.1102230246251565e-16;
+    const double q = 5.0 * u * Lmax;
     double dx = t.x - a.x, dy = t.y - a.y;
     double n1 = t.x * dx, n2 = t.y * dy;
     double num = n1 + n2;
-    double EN = 4.0 * u * (fabs(n1) + fabs(n2));
+    double ta = fabs(t.x) + fabs(t.y), aa = fabs(a.x) + fabs(a.y);
+    double EN = 4.0 * u * (fabs(n1) + fabs(n2)) + q * (3.0 * ta + aa);
     double d1 = a.x * t.y, d2 = a.y * t.x;
     double den = d1 - d2;
-    double ED = 3.0 * u * (fabs(d1) + fabs(d2));
+    double ED = 3.0 * u * (fabs(d1) + fabs(d2)) + q * (ta + aa);
     if (!(den > 2.0 * ED)) {
         lo = -HUGE_VAL;
         hi = HUGE_VAL;
@@ -660,8 +687,10 @@ CG_D void pencil_key(double2 a, double2 t, double &lo, double &hi)
     hi = s + err;
 }
 
-__device__ int warp_star(const double2 *rel, const int *gidx, int m, int K, int *out, int lane)
+__device__ int warp_star(const double2 *rel, const int *gidx, int m, int K, int *out, int lane,
+                         const StarFrame &f)
 {
+    const double Lmax = fmax(f.Lx, f.Ly);
     const unsigned full = 0xffffffffu;
     // nearest candidate
     double best = 1e300;
@@ -696,7 +725,7 @@ __device__ int warp_star(const double2 *rel, const int *gidx, int m, int K, int 
             double2 pt = rel[t];
             if (orient0(pa, pt) <= 0) continue;
             double lo, hi;
-            pencil_key(pa, pt, lo, hi);
+            pencil_key(pa, pt, Lmax, lo, hi);
             U = fmin(U, hi);
             any = true;
         }
@@ -709,16 +738,16 @@ __device__ int warp_star(const double2 *rel, const int *gidx, int m, int K, int 
             double2 pt = rel[t];
             if (orient0(pa, pt) <= 0) continue;
             double lo, hi;
-            pencil_key(pa, pt, lo, hi);
+            pencil_key(pa, pt, Lmax, lo, hi);
             if (!(lo <= U)) continue;
             ++cnt;
-            if (b < 0 || inner_than(pa, pt, gidx[t], rel[b], gidx[b])) b = t;
+            if (b < 0 || inner_than(f, pa, gidx[cur], pt, gidx[t], rel[b], gidx[b])) b = t;
         }
         unsigned has = __ballot_sync(full, cnt > 0);
         if (__reduce_add_sync(full, (unsigned)cnt) > 1u) {
             for (int off = 16; off > 0; off >>= 1) {
                 int ob = __shfl_xor_sync(full, b, off);
-                if (ob >= 0 && (b < 0 || inner_than(pa, rel[ob], gidx[ob], rel[b], gidx[b]))) b = ob;
+                if (ob >= 0 && (b < 0 || inner_than(f, pa, gidx[cur], rel[ob], gidx[ob], rel[b], gidx[b]))) b = ob;
             }
         } else {
             b = __shfl_sync(full, b, __ffs(has) - 1);
@@ -840,7 +869,8 @@ __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
         for (int t = lane; t < m; t += WARP)
             s_rel[w][t] = min_dist(a.pos[s_cand[w][t]], pc, in.Lx, in.Ly);
         __syncwarp();
-        int zs = warp_star(s_rel[w], s_cand[w], m, a.K, s_out[w], lane);
+        StarFrame fr = {c, a.pos, in.Lx, in.Ly};
+        int zs = warp_star(s_rel[w], s_cand[w], m, a.K, s_out[w], lane, fr);
         if (zs < 0) {
             if (lane == 0) {
                 atomicExch(&ctl->need_global, 1);
@@ -1051,7 +1081,9 @@ __global__ void __launch_bounds__(WPB * 32) k_check(VoroArgs a)
                 if (tested && z >= 3) {
                     int km = k == 0 ? z - 1 : k - 1;
                     double2 dA = sR[sl][km], dB = sR[sl][k], dC = sR[sl][kp];
-                    if (orient0(dB, dC) <= 0 || incircle0(dA, dB, dC) < 0) bad = true;
+                    if (orient0(dB, dC) <= 0 ||
+                        incircle_g(dA, dB, dC, c, row[km], u, v, a.pos, Lx, Ly) < 0)
+                        bad = true;
                 }
             }
             if (tested && k < zo) {
@@ -1165,7 +1197,8 @@ __global__ void __launch_bounds__(WPB * 32) k_star_global(VoroArgs a, int *statu
         m = warp_remove(s_idx[w], m, c, lane);
         for (int t = lane; t < m; t += WARP) s_rel[w][t] = min_dist(a.pos[s_idx[w][t]], pc, in.Lx, in.Ly);
         __syncwarp();
-        int z = warp_star(s_rel[w], s_idx[w], m, a.K, s_out[w], lane);
+        StarFrame fr = {c, a.pos, in.Lx, in.Ly};
+        int z = warp_star(s_rel[w], s_idx[w], m, a.K, s_out[w], lane, fr);
         bool ok = z > 0;
         double R = (double)min(wx, wy) * bs;
         if (ok) {
