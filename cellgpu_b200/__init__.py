@@ -7,6 +7,7 @@ from ._lib import (CG_ERR_ARG, CG_ERR_CAPACITY, CG_ERR_CUDA, CG_ERR_STATE, CG_ER
                    CG_ERR_TOPOLOGY, CG_FP64, CG_MIXED, CG_OK, CellGPUError, load)
 from ._lib import FireParams  # noqa: F401
 from .models import (EnergyMinimizerFIRE, Simulation, VertexBatch, VertexQuadraticEnergy,  # noqa: F401
+                     VertexQuadraticEnergyWithTension,
                      Voronoi2D, VoronoiBatch, VoronoiQuadraticEnergy, VoronoiQuadraticEnergyWithTension,
                      brownianParticleDynamics,
                      random_positions, restore, selfPropelledCellVertexDynamics,
@@ -14,7 +15,7 @@ from .models import (EnergyMinimizerFIRE, Simulation, VertexBatch, VertexQuadrat
 
 __all__ = [
     "CG_FP64", "CG_MIXED", "CellGPUError", "EnergyMinimizerFIRE", "FireParams", "load", "Simulation",
-    "VertexBatch", "VertexQuadraticEnergy", "Voronoi2D", "VoronoiBatch", "VoronoiQuadraticEnergy",
+    "VertexBatch", "VertexQuadraticEnergy", "VertexQuadraticEnergyWithTension", "Voronoi2D", "VoronoiBatch", "VoronoiQuadraticEnergy",
     "VoronoiQuadraticEnergyWithTension", "brownianParticleDynamics", "random_positions", "restore", "selfPropelledCellVertexDynamics",
     "selfPropelledParticleDynamics",
 ]

@@ -19,6 +19,7 @@
 #include <random>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "cellgpu_b200.h"
@@ -221,54 +222,6 @@ private:
 };
 using Voronoi2D = VoronoiQuadraticEnergy;
 
-// Voronoi model with line tension between cells of different types:
-// VoronoiQuadraticEnergyWithTension of inc/models/voronoiQuadraticEnergyWithTension.h:15-60
-class VoronoiQuadraticEnergyWithTension : public VoronoiQuadraticEnergy {
-public:
-    explicit VoronoiQuadraticEnergyWithTension(int n, bool reprod = false)
-        : VoronoiQuadraticEnergyWithTension(n, 1.0, 3.8, reprod) {}
-    VoronoiQuadraticEnergyWithTension(int n, Dscalar A0, Dscalar P0, bool reprod = false)
-        : VoronoiQuadraticEnergy(n, A0, P0, reprod)
-    {
-        setCellType(std::vector<int>(n, 0));
-    }
-    // Simple2DCell::setCellType
-    void setCellType(const std::vector<int> &types) { check(cg_set_cell_types(sys_, types.data())); }
-    void setUseSurfaceTension(bool use_tension)
-    {
-        Tension = use_tension;
-        apply();
-    }
-    void setSurfaceTension(Dscalar g)
-    {
-        gamma = g;
-        simpleTension = true;
-        apply();
-    }
-    // flattened ntypes x ntypes matrix, symmetric
-    void setSurfaceTension(const std::vector<Dscalar> &gammas)
-    {
-        int n = (int)std::lround(std::sqrt((double)gammas.size()));
-        if ((size_t)n * n != gammas.size()) throw Error(CG_ERR_ARG, "the tension matrix must be square");
-        tensionMatrix = gammas;
-        simpleTension = false;
-        apply();
-    }
-    Dscalar getSurfaceTension() const { return gamma; }
-
-private:
-    void apply()
-    {
-        if (!Tension) check(cg_set_tension(sys_, 0.0));
-        else if (simpleTension) check(cg_set_tension(sys_, gamma));
-        else
-            check(cg_set_tension_matrix(sys_, (int)std::lround(std::sqrt((double)tensionMatrix.size())),
-                                        tensionMatrix.data()));
-    }
-    Dscalar gamma = 0.0;
-    bool Tension = false, simpleTension = true;
-    std::vector<Dscalar> tensionMatrix;
-};
 
 // Vertex (AVM) model from the Delaunay dual of random cell positions:
 // VertexQuadraticEnergy(n, A0, P0, reprod, runSPVToInitialize) of inc/models/vertexQuadraticEnergy.h:20
@@ -306,6 +259,58 @@ public:
 private:
     unsigned long long seed_ = 0;
 };
+
+// Line tension between cells of different types: setCellType, setSurfaceTension (one gamma, or a
+// flattened symmetric ntypes x ntypes matrix) and setUseSurfaceTension of
+// VoronoiQuadraticEnergyWithTension (inc/models/voronoiQuadraticEnergyWithTension.h:15-60) and
+// VertexQuadraticEnergyWithTension (inc/models/vertexQuadraticEnergyWithTension.h). For the vertex
+// model computeEnergy includes the tension, which the reference leaves unimplemented.
+template <typename Model>
+class WithTension : public Model {
+public:
+    template <typename... Args>
+    explicit WithTension(Args &&...args) : Model(std::forward<Args>(args)...)
+    {
+        setCellType(std::vector<int>(this->Ncells, 0));
+    }
+    // Simple2DCell::setCellType
+    void setCellType(const std::vector<int> &types) { check(cg_set_cell_types(this->sys_, types.data())); }
+    void setUseSurfaceTension(bool use_tension)
+    {
+        Tension = use_tension;
+        apply();
+    }
+    void setSurfaceTension(Dscalar g)
+    {
+        gamma = g;
+        simpleTension = true;
+        apply();
+    }
+    void setSurfaceTension(const std::vector<Dscalar> &gammas)
+    {
+        int n = (int)std::lround(std::sqrt((double)gammas.size()));
+        if ((size_t)n * n != gammas.size()) throw Error(CG_ERR_ARG, "the tension matrix must be square");
+        tensionMatrix = gammas;
+        simpleTension = false;
+        apply();
+    }
+    Dscalar getSurfaceTension() const { return gamma; }
+
+private:
+    void apply()
+    {
+        if (!Tension) check(cg_set_tension(this->sys_, 0.0));
+        else if (simpleTension) check(cg_set_tension(this->sys_, gamma));
+        else
+            check(cg_set_tension_matrix(this->sys_, (int)std::lround(std::sqrt((double)tensionMatrix.size())),
+                                        tensionMatrix.data()));
+    }
+    Dscalar gamma = 0.0;
+    bool Tension = false, simpleTension = true;
+    std::vector<Dscalar> tensionMatrix;
+};
+using VoronoiQuadraticEnergyWithTension = WithTension<VoronoiQuadraticEnergy>;
+using VertexQuadraticEnergyWithTension = WithTension<VertexQuadraticEnergy>;
 
 // ---- updaters ------------------------------------------------------------------------------
 class updater {

@@ -34,9 +34,9 @@ struct SnapInst {
 
 const char SNAP_MAGIC[8] = {'C', 'G', 'B', '2', 'S', 'N', 'P', '1'};
 
-// byte size of every array block, in the order they are stored (Voronoi: the cell types and the
-// tension matrix last, when present)
-void snap_layout(const SnapHeader &h, size_t sizes[9], int &count)
+// byte size of every array block, in the order they are stored (the cell types and the tension
+// matrix last, when present)
+void snap_layout(const SnapHeader &h, size_t sizes[10], int &count)
 {
     const size_t N = (size_t)h.N;
     if (h.model == CG_MODEL_VORONOI) {
@@ -49,15 +49,17 @@ void snap_layout(const SnapHeader &h, size_t sizes[9], int &count)
     } else {
         const size_t Nv = (size_t)h.Nv;
         size_t s[] = {Nv * sizeof(double2), N * sizeof(double), N * sizeof(double2), N * sizeof(double2),
-                      3 * Nv * sizeof(int), 3 * Nv * sizeof(int), N * sizeof(int), N * (size_t)h.vmax * sizeof(int)};
-        count = 8;
+                      3 * Nv * sizeof(int), 3 * Nv * sizeof(int), N * sizeof(int), N * (size_t)h.vmax * sizeof(int),
+                      h.has_types ? N * sizeof(int) : 0,
+                      h.tension_mode == 2 ? (size_t)h.ntypes * h.ntypes * sizeof(double) : 0};
+        count = 10;
         for (int i = 0; i < count; ++i) sizes[i] = s[i];
     }
 }
 
 size_t snap_total(const SnapHeader &h)
 {
-    size_t sizes[9];
+    size_t sizes[10];
     int count = 0;
     snap_layout(h, sizes, count);
     size_t t = sizeof(SnapHeader) + (size_t)h.n_inst * sizeof(SnapInst);
@@ -119,11 +121,11 @@ extern "C" int cg_snapshot(cg_system *s, void *buf, size_t bytes)
         memcpy(p, &r, sizeof(r));
         p += sizeof(r);
     }
-    size_t sizes[9];
+    size_t sizes[10];
     int count = 0;
     snap_layout(h, sizes, count);
     const void *src_v[] = {s->pos, s->theta, s->motility, s->APpref, s->nn, s->nbr, s->ctype, s->tmat};
-    const void *src_m[] = {s->pos, s->theta, s->motility, s->APpref, s->vn, s->vcn, s->cvn, s->cv};
+    const void *src_m[] = {s->pos, s->theta, s->motility, s->APpref, s->vn, s->vcn, s->cvn, s->cv, s->ctype, s->tmat};
     const void *const *src = s->model == CG_MODEL_VORONOI ? src_v : src_m;
     for (int i = 0; i < count; ++i) {
         if (sizes[i]) CG_TRY(d2h(s, p, src[i], sizes[i]));
@@ -140,7 +142,7 @@ extern "C" int cg_restore(const void *buf, size_t bytes, cg_system **out)
     if (memcmp(h.magic, SNAP_MAGIC, 8) != 0 || h.version != 2) return set_err(CG_ERR_ARG, "not a cellgpu_b200 snapshot");
     if (h.n_inst <= 0 || h.N <= 0 || (h.model != CG_MODEL_VORONOI && h.model != CG_MODEL_VERTEX) ||
         h.tension_mode < 0 || h.tension_mode > 2 || h.ntypes < 0 || (h.tension_mode == 2 && h.ntypes < 1) ||
-        (h.tension_mode && (h.model != CG_MODEL_VORONOI || !h.has_types)) || bytes < snap_total(h))
+        (h.tension_mode && !h.has_types) || bytes < snap_total(h))
         return set_err(CG_ERR_ARG, "corrupt or truncated snapshot");
     const unsigned char *p = static_cast<const unsigned char *>(buf) + sizeof(h);
     std::vector<int> Ns(h.n_inst);
@@ -170,13 +172,13 @@ extern "C" int cg_restore(const void *buf, size_t bytes, cg_system **out)
         s->KA = h.KA;
         s->KP = h.KP;
         s->t1 = h.t1;
-        size_t sizes[9];
+        size_t sizes[10];
         int count = 0;
         snap_layout(h, sizes, count);
         if (h.has_types && (st = tension_alloc(s))) break;
         if (h.tension_mode == 2 && (st = dalloc(s, &s->tmat, (size_t)h.ntypes * h.ntypes))) break;
         void *dst_v[] = {s->pos, s->theta, s->motility, s->APpref, s->nn, s->nbr, s->ctype, s->tmat};
-        void *dst_m[] = {s->pos, s->theta, s->motility, s->APpref, s->vn, s->vcn, s->cvn, s->cv};
+        void *dst_m[] = {s->pos, s->theta, s->motility, s->APpref, s->vn, s->vcn, s->cvn, s->cv, s->ctype, s->tmat};
         void **dst = h.model == CG_MODEL_VORONOI ? dst_v : dst_m;
         for (int i = 0; i < count && st == CG_OK; ++i) {
             if (sizes[i]) st = h2d(s, dst[i], p, sizes[i]);

@@ -1,5 +1,7 @@
 // cellgpu_b200 -- line tension of the Voronoi model (VoronoiQuadraticEnergyWithTension,
-// src/models/voronoiQuadraticEnergyWithTension.cpp). Included by system.cu.
+// src/models/voronoiQuadraticEnergyWithTension.cpp) and of the vertex model
+// (VertexQuadraticEnergyWithTension, src/models/vertexQuadraticEnergyWithTension.cpp). Included by
+// system.cu.
 //
 // Cells carry an integer type (Simple2DCell::setCellType, src/models/Simple2DCell.cpp:219-230).
 // With tension on, every Voronoi edge between cells of different types carries gamma (one value,
@@ -9,6 +11,12 @@
 // gradient of sum_cells [KA (A-A0)^2 + KP (P-P0)^2 + sum over the cell's unlike edges of
 // gamma l] -- in the scatter form here each cell simply adds its unlike-edge term to its energy.
 // The energy, as the reference's computeEnergy (:101-159), counts each unlike edge once.
+//
+// Vertex model: each force set (vertex, cell) also carries -gamma times the unit vector from the
+// cell's next vertex to the vertex when the cell across that edge has another type, so every edge
+// contributes its gradient once to each of its two vertices: the forces are minus the gradient of
+// the quadratic energy plus gamma l over every unlike edge once, and that is the energy reported
+// (the reference leaves this model's computeEnergy unimplemented).
 
 static void drop_graphs(cg_system *s)
 {
@@ -28,7 +36,7 @@ static int tension_alloc(cg_system *s)
 
 extern "C" int cg_set_cell_types(cg_system *s, const int *types)
 {
-    if (!s || !types || s->model != CG_MODEL_VORONOI) return set_err(CG_ERR_ARG, "bad args");
+    if (!s || !types) return set_err(CG_ERR_ARG, "bad args");
     for (int i = 0; i < s->N; ++i)
         if (types[i] < 0) return set_err(CG_ERR_ARG, "cell types must be >= 0");
     if (s->tension_mode == 2)
@@ -40,7 +48,7 @@ extern "C" int cg_set_cell_types(cg_system *s, const int *types)
 
 extern "C" int cg_set_tension(cg_system *s, double gamma)
 {
-    if (!s || s->model != CG_MODEL_VORONOI || !(gamma == gamma)) return set_err(CG_ERR_ARG, "bad args");
+    if (!s || !(gamma == gamma)) return set_err(CG_ERR_ARG, "bad args");
     CG_TRY(tension_alloc(s));
     s->gamma = gamma;
     s->tension_mode = gamma != 0.0 ? 1 : 0;
@@ -50,7 +58,7 @@ extern "C" int cg_set_tension(cg_system *s, double gamma)
 
 extern "C" int cg_set_tension_matrix(cg_system *s, int ntypes, const double *gamma)
 {
-    if (!s || s->model != CG_MODEL_VORONOI || ntypes < 0 || (ntypes > 0 && !gamma))
+    if (!s || ntypes < 0 || (ntypes > 0 && !gamma))
         return set_err(CG_ERR_ARG, "bad args");
     // The reference weighs each edge by the matrix entry of one fixed ordering of its two cells'
     // types, and its computeEnergy by another; the two agree (and the forces are the gradient of

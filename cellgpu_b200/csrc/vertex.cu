@@ -25,7 +25,32 @@ struct VertArgs {
     int *cand;        // 3*Nv edge keys (3*v + slot), instance i at 3 * (its first vertex)
     int *cand_count;  // n_inst
     Ctl *ctl;
+    // line tension (VertexQuadraticEnergyWithTension): per-cell types, one gamma (mode 1) or a
+    // symmetric ntypes x ntypes matrix (mode 2); TE[c] = sum over the cell's unlike edges of gamma l
+    int tension_mode, ntypes;
+    double gamma;
+    const int *ctype;
+    const double *tmat;
+    double *TE;
 };
+
+// Tension of the edge from vertex v to the next vertex w of cell c's row: the cell across that edge
+// is the one of v's other two cells whose row holds w (the cellIdx2 search of
+// VertexQuadraticEnergyWithTension::computeVertexTensionForcesCPU,
+// src/models/vertexQuadraticEnergyWithTension.cpp:91-119); the weight is nonzero between types.
+CG_D double vm_edge_weight(const VertArgs &a, int c, int v, int w)
+{
+    int across = 0;
+    for (int f = 0; f < 3; ++f) {
+        int c2 = a.vcn[3 * v + f];
+        if (c2 == c) continue;
+        const int *r2 = a.cv + (size_t)c2 * a.vmax;
+        const int n2 = a.cvn[c2];
+        for (int n = 0; n < n2; ++n)
+            if (r2[n] == w) across = c2;
+    }
+    return tension_weight(a, a.ctype[c], a.ctype[across]);
+}
 
 // ------------------------------------------------------------------------------------------
 // geometry + forces. Per cell: the polygon relative to its vertex at slot z-2, signed shoelace
@@ -58,6 +83,7 @@ __global__ void k_vm_forces(VertArgs a, int scatter)
     double2 vlast = min_dist(a.vpos[row[z - 2]], cp, in.Lx, in.Ly);
     vcur = min_dist(a.vpos[row[z - 1]], cp, in.Lx, in.Ly);
     int vidx = row[z - 1];
+    double te = 0.0;
     for (int n = 0; n < z; ++n) {
         int nv = row[n];
         double2 vnext = min_dist(a.vpos[nv], cp, in.Lx, in.Ly);
@@ -68,12 +94,19 @@ __global__ void k_vm_forces(VertArgs a, int scatter)
         double nnm = sqrt(nx * nx + ny * ny);
         double fx = 2.0 * (Adiff * dAx + Pdiff * (lx / ln - nx / nnm));
         double fy = 2.0 * (Adiff * dAy + Pdiff * (ly / ln - ny / nnm));
+        if (a.tension_mode) {  // the edge to the next vertex (uniform across the grid)
+            double wt = vm_edge_weight(a, c, vidx, nv);
+            fx -= wt * nx / nnm;
+            fy -= wt * ny / nnm;
+            te += wt * nnm;
+        }
         atomicAdd(&a.F[vidx].x, fx);
         atomicAdd(&a.F[vidx].y, fy);
         vlast = vcur;
         vcur = vnext;
         vidx = nv;
     }
+    if (a.TE) a.TE[c] = te;
 }
 
 // The same pass with 8 lanes per cell (lane = vertex slot, rows up to VM_ROW_G vertices): the
@@ -141,7 +174,7 @@ __global__ void __launch_bounds__(WPB * 32) k_vm_forces_groups(VertArgs a, int s
     A = __shfl_sync(0xffffffffu, A, leader);
     P = __shfl_sync(0xffffffffu, P, leader);
     if (!scatter) return;  // uniform
-    double Adiff = 0.0, Pdiff = 0.0;
+    double Adiff = 0.0, Pdiff = 0.0, te = 0.0;
     if (ok) {
         Adiff = a.KA * (A - a.APpref[c].x);
         Pdiff = a.KP * (P - a.APpref[c].y);
@@ -158,9 +191,21 @@ __global__ void __launch_bounds__(WPB * 32) k_vm_forces_groups(VertArgs a, int s
             double nnm = sqrt(nx * nx + ny * ny);
             double fx = 2.0 * (Adiff * dAx + Pdiff * (lx / ln - nx / nnm));
             double fy = 2.0 * (Adiff * dAy + Pdiff * (ly / ln - ny / nnm));
+            if (a.tension_mode) {  // the edge to the next vertex (uniform across the grid)
+                double wt = vm_edge_weight(a, c, vid[r], row[k + 1 == z ? 0 : k + 1]);
+                fx -= wt * nx / nnm;
+                fy -= wt * ny / nnm;
+                te += wt * nnm;
+            }
             atomicAdd(&a.F[vid[r]].x, fx);
             atomicAdd(&a.F[vid[r]].y, fy);
         }
+    }
+    if (a.tension_mode) {
+        te += __shfl_xor_sync(0xffffffffu, te, 1);
+        te += __shfl_xor_sync(0xffffffffu, te, 2);
+        te += __shfl_xor_sync(0xffffffffu, te, 4);
+        if (ok && gl == 0 && a.TE) a.TE[c] = te;
     }
 }
 

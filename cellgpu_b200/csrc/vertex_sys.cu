@@ -27,6 +27,12 @@ static VertArgs vm_args(cg_system *s)
     a.cand = s->t1_cand;
     a.cand_count = s->t1_count;
     a.ctl = s->ctl;
+    a.tension_mode = s->tension_mode;
+    a.ntypes = s->ntypes;
+    a.gamma = s->gamma;
+    a.ctype = s->ctype;
+    a.tmat = s->tmat;
+    a.TE = s->tension_mode ? s->TE : nullptr;
     return a;
 }
 

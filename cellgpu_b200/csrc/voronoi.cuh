@@ -72,8 +72,10 @@ struct VoroArgs {
     double *TE;          // per cell: sum over its unlike edges of gamma x length
 };
 
-// weight of the Voronoi edge between a cell of type ta and a neighbour of type tb
-CG_D double tension_weight(const VoroArgs &a, int ta, int tb)
+// weight of the edge between a cell of type ta and a neighbour of type tb (Voronoi or vertex
+// model arguments: both carry tension_mode, gamma, ntypes and tmat)
+template <typename Args>
+CG_D double tension_weight(const Args &a, int ta, int tb)
 {
     if (ta == tb) return 0.0;
     return a.tension_mode == 1 ? a.gamma : a.tmat[ta * a.ntypes + tb];

@@ -412,14 +412,13 @@ class VoronoiQuadraticEnergy:
 Voronoi2D = VoronoiQuadraticEnergy
 
 
-class VoronoiQuadraticEnergyWithTension(VoronoiQuadraticEnergy):
-    """Voronoi model with line tension between cells of different types
-    (inc/models/voronoiQuadraticEnergyWithTension.h): one gamma for every unlike pair, or a
-    symmetric matrix of tensions between types (setSurfaceTension with a flattened list), applied
-    while setUseSurfaceTension(True)."""
+class _SurfaceTension:
+    """setCellType / setSurfaceTension / setUseSurfaceTension of the reference's
+    *QuadraticEnergyWithTension classes: one gamma for every unlike pair, or a symmetric matrix of
+    tensions between types (setSurfaceTension with a flattened list), applied while
+    setUseSurfaceTension(True)."""
 
-    def __init__(self, n, A0=1.0, P0=3.8, reprod=False, **kw):
-        super().__init__(n, A0, P0, reprod, **kw)
+    def _init_tension(self):
         self.gamma = 0.0
         self.Tension = False
         self.simpleTension = True
@@ -456,6 +455,15 @@ class VoronoiQuadraticEnergyWithTension(VoronoiQuadraticEnergy):
 
     def getSurfaceTension(self):
         return self.gamma
+
+
+class VoronoiQuadraticEnergyWithTension(_SurfaceTension, VoronoiQuadraticEnergy):
+    """Voronoi model with line tension between cells of different types
+    (inc/models/voronoiQuadraticEnergyWithTension.h)."""
+
+    def __init__(self, n, A0=1.0, P0=3.8, reprod=False, **kw):
+        VoronoiQuadraticEnergy.__init__(self, n, A0, P0, reprod, **kw)
+        self._init_tension()
 
 
 class selfPropelledParticleDynamics:
@@ -533,6 +541,16 @@ class VertexQuadraticEnergy:
 
     def enforceTopology(self):
         self.batch.enforce_topology()
+
+
+class VertexQuadraticEnergyWithTension(_SurfaceTension, VertexQuadraticEnergy):
+    """Vertex model with line tension on edges between cells of different types
+    (inc/models/vertexQuadraticEnergyWithTension.h). computeEnergy includes the tension (gamma l
+    over every unlike edge once), which the reference leaves unimplemented."""
+
+    def __init__(self, n, A0=1.0, P0=3.8, reprod=False, **kw):
+        VertexQuadraticEnergy.__init__(self, n, A0, P0, reprod, **kw)
+        self._init_tension()
 
 
 class brownianParticleDynamics:

@@ -276,14 +276,17 @@ int cg_observables(cg_system *sys, double cutoff, double *out);
 int cg_spatial_sort(cg_system *sys);
 int cg_get_tags(cg_system *sys, int *idx_to_tag);
 
-/* Line tension of the Voronoi model (VoronoiQuadraticEnergyWithTension,
- * src/models/voronoiQuadraticEnergyWithTension.cpp; Simple2DCell::setCellType): cells carry a
- * type (>= 0, all 0 by default); every Voronoi edge between cells of different types carries
- * gamma per unit length (cg_set_tension: setSurfaceTension(g); 0 switches tension off) or
- * gamma[type_self * ntypes + type_other] (cg_set_tension_matrix: setSurfaceTension(vector), a
- * symmetric ntypes x ntypes matrix; ntypes = 0 switches it off). Forces are the reference's
- * (each cell's terms count its unlike edges); cg_get_energies counts each unlike edge once, as the
- * reference's computeEnergy does. */
+/* Line tension (VoronoiQuadraticEnergyWithTension, src/models/voronoiQuadraticEnergyWithTension.cpp;
+ * VertexQuadraticEnergyWithTension, src/models/vertexQuadraticEnergyWithTension.cpp;
+ * Simple2DCell::setCellType): cells carry a type (>= 0, all 0 by default); every edge between
+ * cells of different types carries gamma per unit length (cg_set_tension: setSurfaceTension(g); 0
+ * switches tension off) or gamma[type_self * ntypes + type_other] (cg_set_tension_matrix:
+ * setSurfaceTension(vector), a symmetric ntypes x ntypes matrix, CG_ERR_ARG otherwise; ntypes = 0
+ * switches it off). Forces are the reference's: in the Voronoi model each cell's terms count its
+ * unlike edges, in the vertex model each force set adds the edge to its cell's next vertex.
+ * cg_get_energies counts each unlike edge once (the reference's Voronoi computeEnergy; the vertex
+ * model's is unimplemented there, and this is the energy its forces are the gradient of). Both
+ * models. */
 int cg_set_cell_types(cg_system *sys, const int *types);
 int cg_set_tension(cg_system *sys, double gamma);
 int cg_set_tension_matrix(cg_system *sys, int ntypes, const double *gamma);

@@ -764,9 +764,70 @@ static void force_set_vm(const double *vcur, const double *vlast, const double *
  * set of (vertex, cell) comes from the cell's (last, cur, next) vertices as stored by the geometry
  * pass at slot 3*v+f with vcn[3v+f] == cell (src/models/vertexModelBase.cpp:268-287); the force on a
  * vertex is the sum of its three sets in slot order. */
+/* the cell other than `cell` among vertex v's three cells whose row holds vertex w (the cellIdx2
+ * search of src/models/vertexQuadraticEnergyWithTension.cpp:108-119; the last match wins) */
+static int cell_across(int v, int w, int cell, const int *vcn, const int *cvn, const int *cv, int vmax)
+{
+    int out = 0;
+    for (int f = 0; f < 3; ++f) {
+        int c2 = vcn[3 * v + f];
+        if (c2 == cell) continue;
+        for (int n = 0; n < cvn[c2]; ++n)
+            if (cv[(size_t)c2 * vmax + n] == w) out = c2;
+    }
+    return out;
+}
+
+static void vertex_forces_impl(int Nc, int Nv, const double *vpos, const double *box, int vmax, const int *cvn,
+                               const int *cv, const int *vcn, const double *AP, const double *APpref, double KA,
+                               double KP, const tension_t *ten, double *F);
+
 void cgo_vertex_forces(int Nc, int Nv, const double *vpos, const double *box, int vmax, const int *cvn,
                        const int *cv, const int *vcn, const double *AP, const double *APpref, double KA,
                        double KP, double *F)
+{
+    vertex_forces_impl(Nc, Nv, vpos, box, vmax, cvn, cv, vcn, AP, APpref, KA, KP, NULL, F);
+}
+
+/* VertexQuadraticEnergyWithTension::computeVertexTensionForcesCPU
+ * (src/models/vertexQuadraticEnergyWithTension.cpp:65-151): each force set (vertex, cell) also gets
+ * -gamma (vcur - vnext) / |vcur - vnext| for the edge to the cell's next vertex when the cell across
+ * that edge has another type; gamma = the one value, or tensionMatrix[cellTypeIndexer(type of the
+ * set's cell, type across)] = row (type across), column (own type). No norm clamp. */
+void cgo_vertex_tension_forces(int Nc, int Nv, const double *vpos, const double *box, int vmax, const int *cvn,
+                               const int *cv, const int *vcn, const double *AP, const double *APpref, double KA,
+                               double KP, const int *ctype, int ntypes, double gamma, const double *tmat,
+                               double *F)
+{
+    tension_t t = {ctype, ntypes, gamma, tmat};
+    vertex_forces_impl(Nc, Nv, vpos, box, vmax, cvn, cv, vcn, AP, APpref, KA, KP, &t, F);
+}
+
+/* the quadratic energy plus gamma l over every edge between cells of different types, each edge
+ * once (the reference leaves VertexQuadraticEnergyWithTension::computeEnergy unimplemented; this is
+ * the energy whose gradient the forces above are) */
+double cgo_vertex_tension_energy(int Nc, const double *vpos, const double *box, int vmax, const int *cvn,
+                                 const int *cv, const int *vcn, const double *AP, const double *APpref, double KA,
+                                 double KP, const int *ctype, int ntypes, double gamma, const double *tmat)
+{
+    tension_t t = {ctype, ntypes, gamma, tmat};
+    double E = cgo_voronoi_energy(Nc, AP, APpref, KA, KP), ET = 0.0;
+    for (int i = 0; i < Nc; ++i) {
+        int z = cvn[i];
+        const int *row = cv + (size_t)i * vmax;
+        for (int n = 0; n < z; ++n) {
+            int v = row[n], w = row[(n + 1) % z];
+            double d[2];
+            cgo_min_dist(box, vpos + 2 * w, vpos + 2 * v, d);
+            ET += sqrt(d[0] * d[0] + d[1] * d[1]) * tension_w(&t, cell_across(v, w, i, vcn, cvn, cv, vmax), i);
+        }
+    }
+    return E + 0.5 * ET;
+}
+
+static void vertex_forces_impl(int Nc, int Nv, const double *vpos, const double *box, int vmax, const int *cvn,
+                               const int *cv, const int *vcn, const double *AP, const double *APpref, double KA,
+                               double KP, const tension_t *ten, double *F)
 {
     double *fs = (double *)calloc((size_t)6 * Nv, sizeof(double));
     for (int i = 0; i < Nc; ++i) {
@@ -785,6 +846,15 @@ void cgo_vertex_forces(int Nc, int Nv, const double *vpos, const double *box, in
             int nv = row[n];
             cgo_min_dist(box, vpos + 2 * nv, cp, vnext);
             if (fsidx >= 0) force_set_vm(vcur, vlast, vnext, Adiff, Pdiff, fs + 2 * (size_t)fsidx);
+            if (fsidx >= 0 && ten) {
+                double g = tension_w(ten, cell_across(vidx, nv, i, vcn, cvn, cv, vmax), i);
+                if (g != 0.0) {
+                    double dx = vcur[0] - vnext[0], dy = vcur[1] - vnext[1];
+                    double dn = sqrt(dx * dx + dy * dy);
+                    fs[2 * (size_t)fsidx] -= g * dx / dn;
+                    fs[2 * (size_t)fsidx + 1] -= g * dy / dn;
+                }
+            }
             vlast[0] = vcur[0]; vlast[1] = vcur[1];
             vcur[0] = vnext[0]; vcur[1] = vnext[1];
             vidx = nv;

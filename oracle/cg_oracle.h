@@ -72,6 +72,13 @@ void cgo_vertex_geometry(int Nc, const double *vpos, const double *box, int vmax
 void cgo_vertex_forces(int Nc, int Nv, const double *vpos, const double *box, int vmax, const int *cvn,
                        const int *cv, const int *vcn, const double *AP, const double *APpref, double KA,
                        double KP, double *F);
+void cgo_vertex_tension_forces(int Nc, int Nv, const double *vpos, const double *box, int vmax, const int *cvn,
+                               const int *cv, const int *vcn, const double *AP, const double *APpref, double KA,
+                               double KP, const int *ctype, int ntypes, double gamma, const double *tmat,
+                               double *F);
+double cgo_vertex_tension_energy(int Nc, const double *vpos, const double *box, int vmax, const int *cvn,
+                                 const int *cv, const int *vcn, const double *AP, const double *APpref, double KA,
+                                 double KP, const int *ctype, int ntypes, double gamma, const double *tmat);
 /* Sequential T1 sweep (src/models/vertexModelBase.cpp:507-787). Returns the number of flips performed,
  * writes each flip's (vertex1, vertex2) to events (capacity max_events pairs). Returns -2 if a cell
  * would exceed vmax vertices. */

@@ -83,6 +83,12 @@ def lib():
         L.cgo_vertex_geometry.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, _ip, _dp]
         L.cgo_vertex_forces.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip, _dp, _dp,
                                         C.c_double, C.c_double, _dp]
+        L.cgo_vertex_tension_forces.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip, _dp, _dp,
+                                                C.c_double, C.c_double, _ip, C.c_int, C.c_double, C.c_void_p,
+                                                _dp]
+        L.cgo_vertex_tension_energy.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip, _dp, _dp, C.c_double,
+                                                C.c_double, _ip, C.c_int, C.c_double, C.c_void_p]
+        L.cgo_vertex_tension_energy.restype = C.c_double
         L.cgo_vertex_t1.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_int, _ip, _ip, _ip, _ip,
                                     C.c_int, _ip]
         L.cgo_vertex_brownian_run.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _ip, _ip,
@@ -265,6 +271,28 @@ def vertex_forces(vpos, box, cvn, cv, vcn, AP, APpref, KA=1.0, KP=1.0):
                             np.ascontiguousarray(cvn, np.int32), cv, np.ascontiguousarray(vcn, np.int32),
                             _f64(AP), _f64(APpref), KA, KP, F)
     return F
+
+
+def vertex_tension_forces(vpos, box, cvn, cv, vcn, AP, APpref, types, gamma=0.0, gammas=None, KA=1.0, KP=1.0):
+    """Vertex forces with line tension on edges between cells of different types."""
+    vpos = _f64(vpos)
+    cv = np.ascontiguousarray(cv, np.int32)
+    F = np.zeros_like(vpos)
+    types, nt, g, tp, _keep = _tension_args(types, gamma, gammas)
+    lib().cgo_vertex_tension_forces(cv.shape[0], vpos.shape[0], vpos, _box(box), cv.shape[1],
+                                    np.ascontiguousarray(cvn, np.int32), cv, np.ascontiguousarray(vcn, np.int32),
+                                    _f64(AP), _f64(APpref), KA, KP, types, nt, g, tp, F)
+    return F
+
+
+def vertex_tension_energy(vpos, box, cvn, cv, vcn, AP, APpref, types, gamma=0.0, gammas=None, KA=1.0, KP=1.0):
+    vpos = _f64(vpos)
+    cv = np.ascontiguousarray(cv, np.int32)
+    types, nt, g, tp, _keep = _tension_args(types, gamma, gammas)
+    return lib().cgo_vertex_tension_energy(cv.shape[0], vpos, _box(box), cv.shape[1],
+                                           np.ascontiguousarray(cvn, np.int32), cv,
+                                           np.ascontiguousarray(vcn, np.int32), _f64(AP), _f64(APpref), KA, KP,
+                                           types, nt, g, tp)
 
 
 def vertex_t1(vpos, box, threshold, vn, vcn, cvn, cv, max_events=4096):

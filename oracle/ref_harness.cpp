@@ -19,6 +19,7 @@
 #include "vertexQuadraticEnergy.h"
 #include "voronoiQuadraticEnergy.h"
 #include "voronoiQuadraticEnergyWithTension.h"
+#include "vertexQuadraticEnergyWithTension.h"
 
 namespace {
 
@@ -48,9 +49,12 @@ class RefVoronoiTension : public VoronoiQuadraticEnergyWithTension {
 };
 
 // exposes the protected vertex-model arrays
-class RefVertex : public VertexQuadraticEnergy {
+// (the tension subclass computes the plain forces while its tension is off, so one class serves
+// both uses)
+class RefVertex : public VertexQuadraticEnergyWithTension {
   public:
-    RefVertex(int n, Dscalar A0, Dscalar P0) : VertexQuadraticEnergy(n, A0, P0, true, false) {}
+    RefVertex(int n, Dscalar A0, Dscalar P0) : VertexQuadraticEnergyWithTension(n, A0, P0, true, false) {}
+    void dirty() { forcesUpToDate = false; }
     int cells() const { return Ncells; }
     int vmax() const { return vertexMax; }
     GPUArray<int> &cell_vertices() { return cellVertices; }
@@ -263,7 +267,22 @@ double ref_vertex_forces(void *h, double *F, double *AP)
     s->vertex->computeForces();
     to_host(s->vertex->returnForces(), reinterpret_cast<Dscalar2 *>(F), nv);
     to_host(s->vertex->returnAreaPeri(), reinterpret_cast<Dscalar2 *>(AP), nc);
-    return s->vertex->computeEnergy();
+    // the quadratic part (VertexQuadraticEnergyWithTension::computeEnergy is not implemented)
+    return s->vertex->VertexQuadraticEnergy::computeEnergy();
+}
+
+// VertexQuadraticEnergyWithTension: cell types and one gamma (gammas == NULL) or an ntypes x ntypes
+// matrix, tension on (computeVertexTensionForcesCPU)
+void ref_vertex_set_tension(void *h, const int *types, double gamma, int ntypes, const double *gammas)
+{
+    RefSystem *s = reinterpret_cast<RefSystem *>(h);
+    int nc = s->vertex->cells();
+    std::vector<int> t(types, types + nc);
+    s->vertex->setCellType(t);
+    if (gammas) s->vertex->setSurfaceTension(std::vector<Dscalar>(gammas, gammas + (size_t)ntypes * ntypes));
+    else s->vertex->setSurfaceTension(gamma);
+    s->vertex->setUseSurfaceTension(true);
+    s->vertex->dirty();
 }
 
 // Brownian timesteps (CPU branch, reproducible noise: two deviates per vertex, x then y)

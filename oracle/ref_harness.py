@@ -47,6 +47,7 @@ def lib():
         L.ref_vertex_forces.restype = C.c_double
         L.ref_vertex_forces.argtypes = [C.c_void_p, _dp, _dp]
         L.ref_vertex_brownian_run.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.ref_vertex_set_tension.argtypes = [C.c_void_p, _ip, C.c_double, C.c_int, C.c_void_p]
         L.ref_voronoi_tension_forces.restype = C.c_double
         L.ref_voronoi_tension_forces.argtypes = [C.c_int, _dp, _ip, _dp, C.c_double, C.c_int, C.c_void_p, _dp,
                                                  _dp]
@@ -190,6 +191,13 @@ class RefVertex:
 
     def brownian_run(self, steps, dt=0.005, T=1e-3, mu=1.0):
         lib().ref_vertex_brownian_run(self.h, steps, dt, T, mu)
+
+    def set_tension(self, types, gamma=0.0, gammas=None):
+        """VertexQuadraticEnergyWithTension: cell types, one gamma or an ntypes x ntypes matrix."""
+        g = None if gammas is None else np.ascontiguousarray(gammas, np.float64)
+        nt = 0 if g is None else int(round(np.sqrt(g.size)))
+        lib().ref_vertex_set_tension(self.h, np.ascontiguousarray(types, np.int32), float(gamma), nt,
+                                     None if g is None else g.ctypes.data_as(C.c_void_p))
 
     def fire(self, dt=0.01, alpha_start=0.99, dt_max=0.1, dt_inc=1.05, dt_dec=0.95, alpha_dec=0.9, n_min=5,
              force_cutoff=1e-7, max_iterations=1000):

@@ -108,6 +108,30 @@ def tension_case(N, seed):
                         E_simple=Es, F_matrix=Fm, AP_matrix=APm, E_matrix=Em)
 
 
+def vertex_tension_case(Nc, seed):
+    """VertexQuadraticEnergyWithTension (CPU branch): three cell types, one gamma for unlike types
+    and a symmetric tension matrix, on the reference's reproducible Delaunay-dual state. E is the
+    quadratic part (the reference does not implement the tension energy)."""
+    with quiet():
+        rv = R.RefVertex(Nc)
+    cp, vp, vn, vcn, cvn, cv = rv.state()
+    rng = np.random.default_rng(seed)
+    types = rng.integers(0, 3, Nc).astype(np.int32)
+    pref = np.stack([np.ones(Nc), rng.uniform(3.7, 3.9, Nc)], 1)
+    gammas = np.array([[0.0, 0.1, 0.3], [0.1, 0.0, 0.2], [0.3, 0.2, 0.0]])
+    with quiet():
+        rv.set_preferences(pref)
+        rv.set_tension(types, gamma=0.15)
+        Fs, APs, Es = rv.forces()
+        rv.set_tension(types, gammas=gammas)
+        Fm, APm, Em = rv.forces()
+    L = float(np.sqrt(Nc))
+    np.savez_compressed(os.path.join(HERE, f"vertex_tension_Nc{Nc}_s{seed}.npz"), Nc=Nc, box=np.array([L, L]),
+                        vmax=rv.vmax, vpos=vp, vn=vn, vcn=vcn, cvn=cvn, cv=cv, types=types, pref=pref, gamma=0.15,
+                        gammas=gammas, F_simple=Fs, AP_simple=APs, E_simple=Es, F_matrix=Fm, AP_matrix=APm,
+                        E_matrix=Em)
+
+
 if __name__ == "__main__":
     if not R.available():
         raise SystemExit("oracle/_ref/libcgref.so missing: make -C oracle -f Makefile.ref")
@@ -117,4 +141,5 @@ if __name__ == "__main__":
     fire_case(200, 3)
     fire_case(200, 4, vertex=True)
     tension_case(400, 5)
+    vertex_tension_case(300, 7)
     print("golden fixtures written to", HERE)

@@ -135,6 +135,33 @@ def test_tension_forces_are_a_gradient(oracle):
             assert abs(-(energy(p1) - energy(p2)) / (2 * h) - F[c, d]) < 1e-6 * max(1.0, np.abs(F).max())
 
 
+@pytest.mark.parametrize("mode", ["simple", "matrix"])
+def test_vertex_tension_golden(oracle, mode):
+    """VertexQuadraticEnergyWithTension (CPU branch): forces with one gamma and with a symmetric
+    matrix on the reference's Delaunay-dual state; the tension energy (not implemented by the
+    reference) has these forces as its negative gradient."""
+    g = _load("vertex_tension_Nc*.npz")[0]
+    box = tuple(g["box"])
+    AP = oracle.vertex_geometry(g["vpos"], box, g["cvn"], g["cv"])
+    kw = dict(gamma=float(g["gamma"])) if mode == "simple" else dict(gammas=g["gammas"])
+    F = oracle.vertex_tension_forces(g["vpos"], box, g["cvn"], g["cv"], g["vcn"], AP, g["pref"], g["types"], **kw)
+    assert np.abs(AP - g["AP_" + mode]).max() < 1e-12
+    assert force_error(F, g["F_" + mode]) < 1e-12
+    assert abs(oracle.voronoi_energy(AP, g["pref"]) - float(g["E_" + mode])) < 1e-10
+
+    def energy(vp):
+        A = oracle.vertex_geometry(vp, box, g["cvn"], g["cv"])
+        return oracle.vertex_tension_energy(vp, box, g["cvn"], g["cv"], g["vcn"], A, g["pref"], g["types"], **kw)
+
+    h = 1e-6
+    for v in np.random.default_rng(2).choice(len(g["vpos"]), 12, replace=False):
+        for d in range(2):
+            p1, p2 = g["vpos"].copy(), g["vpos"].copy()
+            p1[v, d] += h
+            p2[v, d] -= h
+            assert abs(-(energy(p1) - energy(p2)) / (2 * h) - F[v, d]) < 1e-6 * max(1.0, np.abs(F).max())
+
+
 @pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libcgref.so")),
                     reason="reference build not present")
 def test_live_reference_spp_matches_oracle(oracle):

@@ -1,5 +1,6 @@
-"""GPU parity of the Voronoi model with line tension (VoronoiQuadraticEnergyWithTension) against
-the reference's outputs (tests/golden/tension_N*.npz) and the oracle, through the C ABI.
+"""GPU parity of line tension -- Voronoi model (VoronoiQuadraticEnergyWithTension) and vertex model
+(VertexQuadraticEnergyWithTension) -- against the reference's outputs (tests/golden/tension_N*.npz,
+tests/golden/vertex_tension_Nc*.npz) and the oracle, through the C ABI.
 
 Tolerances: FP64 forces force_error <= 1e-10, areas/perimeters relative 1e-12, energy relative
 1e-12 (summation order differs); mixed precision RMS force error <= 1e-6 of FP64.
@@ -173,3 +174,74 @@ def test_tension_survives_snapshot_and_sort(cglib):
     b.compute_forces()
     assert force_error(b.forces(), F0[tags]) < 1e-12
     assert abs(b.energies()[0] - E0) < 1e-12 * abs(E0)
+
+
+def _vertex_golden():
+    return dict(np.load(sorted(glob.glob(os.path.join(GOLD, "vertex_tension_Nc*.npz")))[0]))
+
+
+def _vertex_tension_batch(g, mode):
+    from cellgpu_b200 import VertexBatch
+    Nc = int(g["Nc"])
+    b = VertexBatch([Nc], [tuple(g["box"])], vmax=int(g["vmax"]))
+    b.set_vertex_topology(g["vn"], g["vcn"], g["cvn"], g["cv"])
+    b.set_positions(g["vpos"])
+    b.set_preferences(g["pref"])
+    b.set_cell_types(g["types"])
+    if mode == "simple":
+        b.set_tension(float(g["gamma"]))
+    else:
+        b.set_tension_matrix(g["gammas"])
+    return b
+
+
+@pytest.mark.parametrize("mode", ["simple", "matrix"])
+def test_vertex_tension_forces_match_reference(cglib, oracle, mode):
+    g = _vertex_golden()
+    b = _vertex_tension_batch(g, mode)
+    b.compute_forces()
+    np.testing.assert_allclose(b.area_perimeter(), g["AP_" + mode], rtol=1e-12, atol=1e-12)
+    assert force_error(b.forces(), g["F_" + mode]) < 1e-10
+    kw = dict(gamma=float(g["gamma"])) if mode == "simple" else dict(gammas=g["gammas"])
+    E = oracle.vertex_tension_energy(g["vpos"], tuple(g["box"]), g["cvn"], g["cv"], g["vcn"], g["AP_" + mode],
+                                     g["pref"], g["types"], **kw)
+    assert abs(b.energies()[0] - E) < 1e-12 * abs(E)
+    assert E > float(g["E_" + mode])  # the quadratic part plus a positive tension
+
+
+def test_vertex_tension_dynamics_and_resume(cglib, oracle, torch):
+    """Brownian steps with T1 transitions and tension: the forces of the state reached are the
+    oracle's on that state; a snapshot taken mid-run restores types and matrix and continues the
+    same trajectory."""
+    from cellgpu_b200 import restore
+    g = _vertex_golden()
+    b = _vertex_tension_batch(g, "matrix")
+    b.set_t1_threshold(0.04)
+    b.brownian_run(20, dt=0.005, mu=1.0, T=2e-3)
+    snap = b.snapshot()
+    b.brownian_run(20, dt=0.005, mu=1.0, T=2e-3)
+    r = restore(snap)
+    r.brownian_run(20, dt=0.005, mu=1.0, T=2e-3)
+    assert np.abs(r.positions() - b.positions()).max() < 1e-9
+    b.compute_forces()
+    vn, vcn, cvn, cv = b.vertex_topology()
+    vp = b.positions()
+    box = tuple(g["box"])
+    AP = oracle.vertex_geometry(vp, box, cvn, cv)
+    F = oracle.vertex_tension_forces(vp, box, cvn, cv, vcn, AP, g["pref"], g["types"], gammas=g["gammas"])
+    assert force_error(b.forces(), F) < 1e-10
+
+
+def test_vertex_tension_class_api(cglib):
+    """VertexQuadraticEnergyWithTension: tension raises the energy and leaves the net force zero."""
+    from cellgpu_b200 import VertexQuadraticEnergyWithTension
+    m = VertexQuadraticEnergyWithTension(200, 1.0, 3.8, True)
+    E0 = m.computeEnergy()
+    m.setCellType(np.arange(200) % 2)
+    m.setSurfaceTension(0.3)
+    m.setUseSurfaceTension(True)
+    E1 = m.computeEnergy()
+    assert E1 > E0
+    assert np.abs(m.returnForces().sum(axis=0)).max() < 1e-10
+    m.setUseSurfaceTension(False)
+    assert abs(m.computeEnergy() - E0) < 1e-12 * E0
