@@ -404,18 +404,26 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
         if (ok && k < z) {
             double2 h0 = T.h[k], h1 = T.h[k + 1 == z ? 0 : k + 1];
             double dx = h1.x - h0.x, dy = h1.y - h0.y;
-            double len = sqrt(dx * dx + dy * dy);
+            // one reciprocal square root gives the length and the unit vector; edges shorter than
+            // the 1e-18 THRESHOLD take the clamped reciprocal as the reference does
+            double l2 = dx * dx + dy * dy, len, il;
+            if (l2 > 1e-36) {
+                il = rsqrt(l2);
+                len = l2 * il;
+            } else {
+                len = sqrt(l2);
+                il = 1e18;
+            }
             Ap += fabs(0.5 * (h0.x * h1.y - h0.y * h1.x));
             Pp += len;
             if (SCATTER) {
                 V u;
                 if (sizeof(R) == sizeof(double)) {
-                    double il = 1.0 / (len < 1e-18 ? 1e-18 : len);
                     u = mk<R>((R)(dx * il), (R)(dy * il));
                 } else {
                     V rk = cvt<R>(T.r[k]);
-                    R il = R(1) / sqrt(rk.x * rk.x + rk.y * rk.y);
-                    u = mk<R>(-rk.y * il, rk.x * il);
+                    R ir = rsqrtf((float)(rk.x * rk.x + rk.y * rk.y));
+                    u = mk<R>(-rk.y * ir, rk.x * ir);
                 }
                 T.u[k] = u;
             }
