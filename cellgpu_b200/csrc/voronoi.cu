@@ -687,12 +687,26 @@ CG_D void pencil_key(double2 a, double2 t, double Lmax, double &lo, double &hi)
         hi = HUGE_VAL;
         return;
     }
-    double s = 0.5 * num / den;
-    double dm = den - ED;
-    double err = 0.5 * (fabs(num) * ED / (den * dm) + EN / dm) + 2.0 * u * fabs(s);
+    // one reciprocal: with dm = den - ED >= den / 2, the quotient's error
+    // 0.5 (|num| ED / (den dm) + EN / dm) is at most (|num| ED / den + EN) / den; forming s from the
+    // reciprocal rounds twice (3u|s| covers it and the bound's own rounding)
+    double id = 1.0 / den;
+    double s = 0.5 * num * id;
+    double err = (fabs(num) * ED * id + EN) * id + 3.0 * u * fabs(s);
     err *= 2.0;
     lo = s - err;
     hi = s + err;
+}
+
+// order-preserving map of a float onto an unsigned key (for the warp min reduction) and back
+CG_D unsigned float_order_key(float f)
+{
+    unsigned b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+CG_D float float_from_order_key(unsigned k)
+{
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
 }
 
 __device__ int warp_star(const double2 *rel, const int *gidx, int m, int K, int *out, int lane,
@@ -725,28 +739,43 @@ __device__ int warp_star(const double2 *rel, const int *gidx, int m, int K, int 
         if (lane == 0) out[z] = cur;
         ++z;
         double2 pa = rel[cur];
-        // pass 1: smallest upper end U of the key intervals of the counter-clockwise candidates
-        double U = HUGE_VAL;
+        // pass 1: key intervals of the counter-clockwise candidates (a lane keeps the lower ends of
+        // its first two) and their smallest upper end U over the warp, rounded up to a float so
+        // that one integer min reduction finds it (a U above the exact minimum only lets more
+        // candidates through to the exact comparison)
+        double klo0 = 0.0, klo1 = 0.0;
+        unsigned ccw = 0u;
+        unsigned ukey = 0xffffffffu;
         bool any = false;
-        for (int t = lane; t < m; t += WARP) {
+        for (int j = 0, t = lane; t < m; ++j, t += WARP) {
             if (t == cur) continue;
             double2 pt = rel[t];
             if (orient0(pa, pt) <= 0) continue;
             double lo, hi;
             pencil_key(pa, pt, Lmax, lo, hi);
-            U = fmin(U, hi);
+            if (j == 0) klo0 = lo;
+            else if (j == 1) klo1 = lo;
+            if (j < 2) ccw |= 1u << j;
+            ukey = min(ukey, float_order_key(__double2float_ru(hi)));
             any = true;
         }
         if (!__any_sync(full, any)) return -1;
-        for (int off = 16; off > 0; off >>= 1) U = fmin(U, __shfl_xor_sync(full, U, off));
+        ukey = __reduce_min_sync(full, ukey);
+        const double U = (double)float_from_order_key(ukey);
         // pass 2: only candidates with lo <= U can be the minimum; order them exactly
         int b = -1, cnt = 0;
-        for (int t = lane; t < m; t += WARP) {
+        for (int j = 0, t = lane; t < m; ++j, t += WARP) {
             if (t == cur) continue;
             double2 pt = rel[t];
-            if (orient0(pa, pt) <= 0) continue;
-            double lo, hi;
-            pencil_key(pa, pt, Lmax, lo, hi);
+            double lo;
+            if (j < 2) {
+                if (!(ccw & (1u << j))) continue;
+                lo = j == 0 ? klo0 : klo1;
+            } else {
+                if (orient0(pa, pt) <= 0) continue;
+                double hi;
+                pencil_key(pa, pt, Lmax, lo, hi);
+            }
             if (!(lo <= U)) continue;
             ++cnt;
             if (b < 0 || inner_than(f, pa, gidx[cur], pt, gidx[t], rel[b], gidx[b])) b = t;
