@@ -45,16 +45,30 @@ extern "C" int cg_version(void) { return 100; }
 
 static inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
+// cells per block of the fused pass: two resident waves of blocks over the N cells (148 SMs x
+// minb blocks each), in whole groups of cells. Against one group of cells per block this cut the
+// C2 force pass from 79.2 to 75.3 us (one wave: 75.6, four: 78.3) on the same B200.
+static inline int cells_per_block(int N, int wpb, int minb)
+{
+    const int grp = wpb * GPW;
+    const long long blocks = 148LL * minb * 2;
+    int cpb = (int)((N + blocks - 1) / blocks);
+    return std::max(grp, (cpb + grp - 1) / grp * grp);
+}
+
 // launch of the fused per-cell pass (groups of 8 lanes) in launch shape 0 or 1
 template <typename R, bool SCATTER, bool TEST>
 static inline void launch_groups(const VoroArgs &a, int N, cudaStream_t st, int shape = 0)
 {
-    if (shape == 1)
+    if (shape == 1) {
+        int cpb = cells_per_block(N, CG_FORCE_WPB_ALT, CG_FORCE_MINB_ALT);
         k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB_ALT, CG_FORCE_MINB_ALT>
-            <<<nblk(N, CG_FORCE_WPB_ALT * GPW), CG_FORCE_WPB_ALT * 32, 0, st>>>(a);
-    else
+            <<<nblk(N, cpb), CG_FORCE_WPB_ALT * 32, 0, st>>>(a, cpb);
+    } else {
+        int cpb = cells_per_block(N, CG_FORCE_WPB, CG_FORCE_MINB);
         k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB, CG_FORCE_MINB>
-            <<<nblk(N, CG_FORCE_WPB * GPW), CG_FORCE_WPB * 32, 0, st>>>(a);
+            <<<nblk(N, cpb), CG_FORCE_WPB * 32, 0, st>>>(a, cpb);
+    }
 }
 
 static Inst make_inst(double Lx, double Ly, int off, int n, int bin_off, double bin_target)

@@ -528,72 +528,78 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<
     }
 }
 
+// A block takes a contiguous run of cpb cells (a multiple of its WPB * GPW groups), so that in a
+// spatially sorted system the cells one SM works on are neighbours and their positions stay in L1.
 template <typename R, bool SCATTER, bool TEST, int WPB, int MINB>
-__global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a)
+__global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int cpb)
 {
     __shared__ GrpTile<R> tile[WPB * GPW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int gl = lane & (G - 1), gi = lane >> 3;
     const int sl = w * GPW + gi;
-    const int c = (blockIdx.x * WPB + w) * GPW + gi;
-    bool live = c < a.N;
-    if (a.ctl && a.ctl->halt) live = false;  // uniform across the grid
-    int z = 0;
-    double2 pc = make_double2(0, 0);
-    double Lx = 1, Ly = 1;
-    const int *row = nullptr;
-    if (live) {
-        const Inst &in = inst_of(a, c);
-        Lx = in.Lx;
-        Ly = in.Ly;
-        pc = a.pos[c];
-        z = a.nn[c];
-        row = a.nbr + (size_t)c * a.K;
-    }
-    const bool ok = live && z >= 3 && z <= VG;
-    int nbk[2];
-    double A, P;
-    int fail;
-    grp_geometry<R, SCATTER, TEST>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail);
-    if (ok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
-    // A cell whose own row fails the test holds its contributions back: the row is about to be
-    // replaced, and a stale row can contain a nearly collinear triangle whose Jacobians (1/cross^2)
-    // would swamp the forces. The repair commit adds the contributions of the new row.
-    bool hold = SCATTER && TEST && a.held && ok && fail != 0x7fffffff;
-    if (hold && gl == 0) a.held[c] = 1;
-    if (SCATTER) grp_scatter<R, 1>(a, c, z, ok && !hold, gl, tile[sl], nbk, A, P);
-    if (TEST && live && gl == 0 && (fail != 0x7fffffff || !ok)) {
-        if (!ok) {
-            if (a.ctl) {
-                atomicAdd(&a.ctl->n_flagged, 1);
-                claim_enqueue(a, c, a.ctl->epoch, 0);
-                if (z > VG) {
-                    atomicExch(&a.ctl->status, CG_ERR_CAPACITY);
-                    atomicExch(&a.ctl->halt, 1);
+    const int c_end = min(a.N, (blockIdx.x + 1) * cpb);
+    const bool halted = a.ctl && a.ctl->halt;  // uniform across the grid
+    for (int base = blockIdx.x * cpb + w * GPW; base < c_end; base += WPB * GPW) {  // warp-uniform
+        const int c = base + gi;
+        bool live = c < c_end && !halted;
+        int z = 0;
+        double2 pc = make_double2(0, 0);
+        double Lx = 1, Ly = 1;
+        const int *row = nullptr;
+        if (live) {
+            const Inst &in = inst_of(a, c);
+            Lx = in.Lx;
+            Ly = in.Ly;
+            pc = a.pos[c];
+            z = a.nn[c];
+            row = a.nbr + (size_t)c * a.K;
+        }
+        const bool ok = live && z >= 3 && z <= VG;
+        int nbk[2];
+        double A, P;
+        int fail;
+        grp_geometry<R, SCATTER, TEST>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail);
+        if (ok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
+        // A cell whose own row fails the test holds its contributions back: the row is about to be
+        // replaced, and a stale row can contain a nearly collinear triangle whose Jacobians (1/cross^2)
+        // would swamp the forces. The repair commit adds the contributions of the new row.
+        bool hold = SCATTER && TEST && a.held && ok && fail != 0x7fffffff;
+        if (hold && gl == 0) a.held[c] = 1;
+        if (SCATTER) grp_scatter<R, 1>(a, c, z, ok && !hold, gl, tile[sl], nbk, A, P);
+        if (TEST && live && gl == 0 && (fail != 0x7fffffff || !ok)) {
+            if (!ok) {
+                if (a.ctl) {
+                    atomicAdd(&a.ctl->n_flagged, 1);
+                    claim_enqueue(a, c, a.ctl->epoch, 0);
+                    if (z > VG) {
+                        atomicExch(&a.ctl->status, CG_ERR_CAPACITY);
+                        atomicExch(&a.ctl->halt, 1);
+                    }
+                } else if (a.mark) {
+                    a.mark[c] = 1;
+                    a.queue[0] = 1;
                 }
-            } else if (a.mark) {
-                a.mark[c] = 1;
-                a.queue[0] = 1;
-            }
-        } else {
-            int k = fail >> 1;
-            bool orient_fail = fail & 1;
-            int nk = row[k], nk1 = row[(k + 1) % z], nkm = row[(k + z - 1) % z];
-            if (a.ctl) {
-                int e = a.ctl->epoch;
-                atomicAdd(&a.ctl->n_flagged, 1);
-                claim_enqueue(a, c, e, 0);
-                claim_enqueue(a, nk, e, 0);
-                claim_enqueue(a, nk1, e, 0);
-                if (!orient_fail) claim_enqueue(a, nkm, e, 0);
-            } else if (a.mark) {
-                a.mark[c] = 1;
-                a.mark[nk] = 1;
-                a.mark[nk1] = 1;
-                if (!orient_fail) a.mark[nkm] = 1;
-                a.queue[0] = 1;
+            } else {
+                int k = fail >> 1;
+                bool orient_fail = fail & 1;
+                int nk = row[k], nk1 = row[(k + 1) % z], nkm = row[(k + z - 1) % z];
+                if (a.ctl) {
+                    int e = a.ctl->epoch;
+                    atomicAdd(&a.ctl->n_flagged, 1);
+                    claim_enqueue(a, c, e, 0);
+                    claim_enqueue(a, nk, e, 0);
+                    claim_enqueue(a, nk1, e, 0);
+                    if (!orient_fail) claim_enqueue(a, nkm, e, 0);
+                } else if (a.mark) {
+                    a.mark[c] = 1;
+                    a.mark[nk] = 1;
+                    a.mark[nk1] = 1;
+                    if (!orient_fail) a.mark[nkm] = 1;
+                    a.queue[0] = 1;
+                }
             }
         }
+        __syncwarp();
     }
 }
 
