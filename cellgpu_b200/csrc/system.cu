@@ -203,7 +203,7 @@ struct cg_system {
     void *AP = nullptr, *F = nullptr;
     int *nn = nullptr, *nbr = nullptr;
     int *mark = nullptr, *queue = nullptr, *stage_nn = nullptr, *stage_nbr = nullptr, *changed = nullptr;
-    int *held = nullptr;
+    int *held = nullptr, *undec = nullptr;
     Ctl *ctl = nullptr;
     int *bin_count = nullptr, *bin_start = nullptr, *bin_cells = nullptr, *cell_bin = nullptr,
         *cell_slot = nullptr;
@@ -336,6 +336,7 @@ static VoroArgs sys_args(cg_system *s)
     a.stage_nbr = s->stage_nbr;
     a.changed = s->changed;
     a.held = s->held;
+    a.undec = s->undec;
     a.ctl = s->ctl;
     a.bin_count = s->bin_count;
     a.bin_start = s->bin_start;
@@ -356,7 +357,7 @@ static VoroArgs sys_args(cg_system *s)
 static size_t voronoi_bytes(int N, int K, int n_bins, int n_inst, int precision)
 {
     size_t real2 = precision == CG_FP64 ? 16 : 8;
-    size_t per_cell = 4 /*cell_inst*/ + 4 /*held*/ + 16 * 3 /*pos, motility, APpref*/ + 8 /*theta*/ + 2 * real2 +
+    size_t per_cell = 4 /*cell_inst*/ + 4 /*held*/ + 4 /*undec*/ + 16 * 3 /*pos, motility, APpref*/ + 8 /*theta*/ + 2 * real2 +
                       4 + 4 * (size_t)K /*nn, nbr*/ + 4 /*mark*/ + 4 * (R_MAX + 1) /*queue*/ + 4 +
                       4 * (size_t)K /*stage*/ + 4 * R_MAX /*changed*/ + 4 * 3 + 16 /*cell list*/;
     return per_cell * (size_t)N + (size_t)n_bins * 8 + (size_t)n_inst * (sizeof(Inst) + 16) + 4096;
@@ -425,6 +426,7 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
         if ((st = dalloc(s, &s->stage_nbr, (size_t)Nt * K))) break;
         if ((st = dalloc(s, &s->changed, (size_t)Nt * R_MAX))) break;
         if ((st = dalloc(s, &s->held, Nt))) break;
+        if ((st = dalloc(s, &s->undec, Nt))) break;
         if ((st = dalloc(s, &s->ctl, 1))) break;
         if ((st = dalloc(s, &s->bin_count, s->n_bins + 1))) break;
         if ((st = dalloc(s, &s->bin_start, s->n_bins + 1))) break;
@@ -735,7 +737,7 @@ static void launch_round(cg_system *s, const VoroArgs &a, bool forces, cudaStrea
 template <typename R>
 static void launch_repair(cg_system *s, const VoroArgs &a, bool forces)
 {
-    k_repair_begin<<<1, 1, 0, s->stream>>>(a, 0ull, 0);
+    k_repair_begin<R><<<1, 256, 0, s->stream>>>(a, 0ull, 0, forces ? 1 : 0);
     for (int r = 0; r < R_MAX; ++r) launch_round<R>(s, a, forces, s->stream, 0ull, 0);
     s->kernels_enqueued += 1;
 }
@@ -873,7 +875,7 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
         CG_CUDA(cudaStreamBeginCaptureToGraph(s->stream, graph, deps.empty() ? nullptr : deps.data(), nullptr,
                                               deps.size(), mode));
         launch_force_test<R>(s, a, true);
-        k_repair_begin<<<1, 1, 0, s->stream>>>(a, (unsigned long long)h, 1);
+        k_repair_begin<R><<<1, 256, 0, s->stream>>>(a, (unsigned long long)h, 1, 1);
         s->kernels_enqueued += 1;
         st = capture_deps(s->stream);
         cudaGraph_t g2;
@@ -1059,6 +1061,7 @@ extern "C" int cg_launch_force_pass(cg_system *s, int with_test)
 {
     if (!s || s->model != CG_MODEL_VORONOI) return set_err(CG_ERR_ARG, "bad args");
     VoroArgs a = sys_args(s);
+    a.undec = nullptr;  // no repair follows: undecided slots count as failing edges
     if (s->precision == CG_FP64)
         launch_force_test<double>(s, a, with_test != 0);
     else

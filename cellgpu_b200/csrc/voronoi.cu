@@ -385,13 +385,16 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
             }
         }
     }
-    if (TEST && __any_sync(0xffffffffu, undecided != 0)) {
+    if (TEST && undecided) {
+        // rare: the canonical evaluation runs in k_repair_begin (keeping this kernel's registers for
+        // the common path); without a list, or when it is full, the edge counts as failing and the
+        // repair recomputes the stars with the canonical predicate
         for (int r = 0; r < 2; ++r) {
+            if (!(undecided & (1 << r))) continue;
             int k = gl + G * r;
-            if (undecided & (1 << r)) {
-                int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
-                if (incircle_canonical(c, row[km], nbk[r], row[kp], a.pos, Lx, Ly) < 0) fail = min(fail, 2 * k);
-            }
+            int idx = (a.undec && a.ctl) ? atomicAdd(&a.ctl->n_undec, 1) : a.N;
+            if (idx < a.N) a.undec[idx] = c * VG + k;
+            else fail = min(fail, 2 * k);
         }
     }
     __syncwarp();
@@ -609,12 +612,75 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int 
 // the next round. A round's kernels take their round index from the control block, so the rounds
 // can run inside a CUDA-graph WHILE node whose condition the device sets (cudaGraphSetConditional),
 // and an empty round costs nothing.
-__global__ void k_repair_begin(VoroArgs a, unsigned long long cond, int use_cond)
+// Start of the repair: first the slots the force pass's filter left undecided. Each is decided by
+// the canonical evaluation (incircle_canonical); a failing one is handled as the force pass handles
+// a failing edge: the cell's contributions, already scattered, are retracted and the cell is marked
+// held (once per cell), and the cell, the edge's other end and both apexes are queued. Then the
+// WHILE node is entered if queue 0 has cells.
+template <typename R>
+__global__ void __launch_bounds__(256) k_repair_begin(VoroArgs a, unsigned long long cond, int use_cond,
+                                                      int forces)
 {
+    constexpr int WPB = 8;
+    __shared__ GrpTile<R> tile[WPB * GPW];
     Ctl *ctl = a.ctl;
-    ctl->round = 0;
-    unsigned v = (!ctl->halt && ctl->q_count[0] > 0) ? 1u : 0u;
-    if (use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, v);
+    const int nu = min(ctl->n_undec, a.N);
+    if (!ctl->halt && nu > 0 && a.undec) {
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        const int gl = lane & (G - 1), gi = lane >> 3;
+        const int sl = w * GPW + gi;
+        const int e = ctl->epoch;
+        for (int base = w * GPW; base < nu; base += WPB * GPW) {  // warp-uniform
+            const int t = base + gi;
+            int c = 0, k = 0, z = 0;
+            const int *row = a.nbr;
+            double Lx = 1, Ly = 1;
+            double2 pc = make_double2(0, 0);
+            bool fails = false;
+            if (t < nu) {
+                const int en = a.undec[t];
+                c = en / VG;
+                k = en % VG;
+                z = a.nn[c];
+                row = a.nbr + (size_t)c * a.K;
+                const Inst &in = inst_of(a, c);
+                Lx = in.Lx;
+                Ly = in.Ly;
+                pc = a.pos[c];
+                if (gl == 0)
+                    fails = incircle_canonical(c, row[k == 0 ? z - 1 : k - 1], row[k], row[k + 1 == z ? 0 : k + 1],
+                                               a.pos, Lx, Ly) < 0;
+            }
+            fails = __shfl_sync(0xffffffffu, fails, lane & ~(G - 1));
+            // retract the contributions once per cell (unless the force pass already held them)
+            bool first = false;
+            if (fails && gl == 0) {
+                first = !forces || atomicExch(&a.held[c], 1) == 0;
+                atomicAdd(&ctl->n_flagged, 1);
+                claim_enqueue(a, c, e, 0);
+                claim_enqueue(a, row[k], e, 0);
+                claim_enqueue(a, row[k + 1 == z ? 0 : k + 1], e, 0);
+                claim_enqueue(a, row[k == 0 ? z - 1 : k - 1], e, 0);
+            }
+            first = __shfl_sync(0xffffffffu, first, lane & ~(G - 1));
+            if (forces) {
+                const bool ok = fails && first && z >= 3 && z <= VG;
+                int nbk[2];
+                double A, P;
+                int fl;
+                grp_geometry<R, true, false>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fl);
+                grp_scatter<R, -1>(a, c, z, ok, gl, tile[sl], nbk, A, P);
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ctl->n_undec = 0;
+        ctl->round = 0;
+        unsigned v = (!ctl->halt && ctl->q_count[0] > 0) ? 1u : 0u;
+        if (use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, v);
+    }
 }
 
 __global__ void k_round_end(VoroArgs a, unsigned long long cond, int use_cond)

@@ -29,6 +29,7 @@ struct Ctl {
     int need_global;         // a global retriangulation is required
     int status;              // CG_* code explaining halt
     int n_flagged;           // cells flagged by the test of this step
+    int n_undec;             // entries of VoroArgs::undec written by the test of this step
     int q_count[R_MAX + 1];  // per-round queue lengths
     int n_changed[R_MAX];    // per-round changed rows
     int step;                // completed integrator steps since creation
@@ -59,6 +60,7 @@ struct VoroArgs {
     int *stage_nbr; // N * K
     int *changed;   // R_MAX * N  (queue slots whose rows changed)
     int *held;      // N: 1 while a cell's contributions are held back (its own row failed the test)
+    int *undec;     // N: slots (c * 16 + k) whose in-circle sign the filter left undecided, or null
     Ctl *ctl;
     // cell list
     int *bin_count, *bin_start, *bin_cells, *cell_bin, *cell_slot;
