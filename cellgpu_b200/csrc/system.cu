@@ -618,8 +618,12 @@ extern "C" int cg_set_topology(cg_system *s, const int *nn, const int *nbr)
     if (!s || !nn || !nbr || s->model != CG_MODEL_VORONOI) return set_err(CG_ERR_ARG, "bad args");
     for (int i = 0; i < s->N; ++i)
         if (nn[i] < 3 || nn[i] > s->K) return set_err(CG_ERR_ARG, "row length out of range");
+    // rows on the device are padded with -1 past their length (the repair reads whole rows)
+    std::vector<int> rows(nbr, nbr + (size_t)s->N * s->K);
+    for (int i = 0; i < s->N; ++i)
+        for (int k = nn[i]; k < s->K; ++k) rows[(size_t)i * s->K + k] = -1;
     CG_TRY(h2d(s, s->nn, nn, sizeof(int) * s->N));
-    CG_TRY(h2d(s, s->nbr, nbr, sizeof(int) * (size_t)s->N * s->K));
+    CG_TRY(h2d(s, s->nbr, rows.data(), sizeof(int) * (size_t)s->N * s->K));
     s->topology_valid = true;
     return CG_OK;
 }

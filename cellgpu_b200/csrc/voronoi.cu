@@ -345,7 +345,8 @@ struct GrpTile {
 // test (TEST) and the edge unit vectors (SCATTER). nbk receives the neighbours of the lane's slots.
 template <typename R, bool SCATTER, bool TEST>
 CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok, double2 pc, double Lx,
-                       double Ly, int gl, GrpTile<R> &T, int (&nbk)[2], double &A, double &P, int &fail)
+                       double Ly, int gl, GrpTile<R> &T, int (&nbk)[2], double &A, double &P, int &fail,
+                       bool store_te = true)
 {
     using V = typename Vec2<R>::T;
 #pragma unroll
@@ -451,7 +452,7 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
             }
         }
         Tp = group_sum<double>(Tp);
-        if (ok && gl == 0 && a.TE) a.TE[c] = Tp;
+        if (ok && store_te && gl == 0 && a.TE) a.TE[c] = Tp;
     }
 }
 
@@ -459,7 +460,7 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
 // vertex, and the scatter of SIGN x (contribution) to the cell and its neighbours.
 template <typename R, int SIGN>
 CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<R> &T, const int (&nbk)[2],
-                      double A, double P)
+                      double A, double P, R sgn = R(SIGN))
 {
     using V = typename Vec2<R>::T;
     __syncwarp();
@@ -521,13 +522,11 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<
         int k = gl + G * r;
         if (ok && k < z) {
             V ca = T.ca[k + 1 == z ? 0 : k + 1];
-            if (SIGN > 0) atomic_add2<R>(a.F, nbk[r], cb[r].x + ca.x, cb[r].y + ca.y);
-            else atomic_add2<R>(a.F, nbk[r], -(cb[r].x + ca.x), -(cb[r].y + ca.y));
+            atomic_add2<R>(a.F, nbk[r], sgn * (cb[r].x + ca.x), sgn * (cb[r].y + ca.y));
         }
     }
     if (ok && gl == 0) {
-        if (SIGN > 0) atomic_add2<R>(a.F, c, sx, sy);
-        else atomic_add2<R>(a.F, c, -sx, -sy);
+        atomic_add2<R>(a.F, c, sgn * sx, sgn * sy);
     }
 }
 
@@ -956,18 +955,20 @@ __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
         // too (3-ring), for cells whose new star reaches further
         int lo = 0, hi = min(*vm, CAND_LOCAL);
         for (int ring = 0; ring < (round == 0 ? 1 : 2); ++ring) {
-            for (int base = lo; base < hi; base += WARP) {
-                int j = base + lane;
-                int x = j < hi ? s_cand[w][j] : -1;
-                int zx = x >= 0 ? a.nn[x] : 0;
-                int cnt = min(hi - base, WARP);
-                for (int p = 0; p < cnt; p += 2) {
-                    int src = p + (lane >> 4), e = lane & 15;
-                    int xs = __shfl_sync(full, x, src);
-                    int zs = __shfl_sync(full, zx, src);
-                    int v = (src < cnt && e < zs) ? a.nbr[(size_t)xs * a.K + e] : -1;
-                    if (v >= 0 && v != c && *vm < CAND_LOCAL) cand_insert(s_hash[w], s_cand[w], &s_m[w], v);
+            // rows are padded with -1 past their length, so whole rows are read without their
+            // lengths; a lane takes slot (lane & 15) of members lane >> 4, +2, +4, +6 of each group
+            // of 8 members, and the four loads are in flight together
+            for (int base = lo; base < hi; base += 8) {
+                const int e = lane & 15;
+                int v[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int j = base + (lane >> 4) + 2 * i;
+                    v[i] = (j < hi && e < a.K) ? a.nbr[(size_t)s_cand[w][j] * a.K + e] : -1;
                 }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (v[i] >= 0 && v[i] != c && *vm < CAND_LOCAL) cand_insert(s_hash[w], s_cand[w], &s_m[w], v[i]);
             }
             __syncwarp();
             lo = hi;
@@ -975,8 +976,13 @@ __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
         }
         int m = min(*vm, CAND_LOCAL);
         double2 pc = a.pos[c];
-        for (int t = lane; t < m; t += WARP)
-            s_rel[w][t] = min_dist(a.pos[s_cand[w][t]], pc, in.Lx, in.Ly);
+        for (int t = lane; t < m; t += 2 * WARP) {
+            const int t2 = t + WARP;
+            double2 p1 = a.pos[s_cand[w][t]];
+            double2 p2 = t2 < m ? a.pos[s_cand[w][t2]] : pc;
+            s_rel[w][t] = min_dist(p1, pc, in.Lx, in.Ly);
+            if (t2 < m) s_rel[w][t2] = min_dist(p2, pc, in.Lx, in.Ly);
+        }
         __syncwarp();
         StarFrame fr = {c, a.pos, in.Lx, in.Ly};
         int zs = warp_star(s_rel[w], s_cand[w], m, a.K, s_out[w], lane, fr);
@@ -994,10 +1000,11 @@ __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
     }
 }
 
-// Commit staged rows, one 8-lane group per queue slot (lane = Voronoi vertex, as in the force pass):
-// rows that changed retract their old contributions and add the new ones (forces stay consistent
-// with the topology), A/P are refreshed, and the old row is kept in the staging slot for the
-// consistency check. Unchanged rows whose force contributions the force pass held back add them now.
+// Commit staged rows, 16 lanes per queue slot: its first 8-lane group retracts the old row's
+// contributions while the second adds the new row's (same group code as the force pass), so the two
+// run side by side; A/P are refreshed from the new row, and the old row is kept in the staging slot
+// for the consistency check. Unchanged rows whose force contributions the force pass held back add
+// them now.
 template <typename R, bool FORCES, int WPB>
 __global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
 {
@@ -1008,12 +1015,15 @@ __global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
     if (round >= R_MAX) return;
     const int nq = ctl->q_count[round];
     const int *queue = a.queue + (size_t)round * a.N;
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int gl = lane & (G - 1), gi = lane >> 3;
     const int sl = w * GPW + gi;
-    const int step = gridDim.x * WPB * GPW;
-    for (int base = (blockIdx.x * WPB + w) * GPW; base < nq; base += step) {  // warp-uniform loop
-        const int q = base + gi;
+    const bool add = gi & 1;       // group 0 of a slot: old row (retract); group 1: new row (add)
+    const int hl = lane & 15;      // lane within the slot's 16 lanes = row slot it moves
+    const int step = gridDim.x * WPB * (GPW / 2);
+    for (int base = (blockIdx.x * WPB + w) * (GPW / 2); base < nq; base += step) {  // warp-uniform loop
+        const int q = base + (gi >> 1);
         const bool live = q < nq;
         int c = 0, zo = 0, zn = 0;
         if (live) {
@@ -1024,12 +1034,13 @@ __global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
         int *row = a.nbr + (size_t)c * a.K;
         int *srow = a.stage_nbr + (size_t)(live ? q : 0) * a.K;
         bool diff = live && zo != zn;
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            int k = gl + G * r;
-            if (live && !diff && k < zn && row[k] != srow[k]) diff = true;
-        }
-        diff = group_any(diff);
+        if (live && !diff && hl < zn && row[hl] != srow[hl]) diff = true;
+        int dv = diff ? 1 : 0;
+        dv |= __shfl_xor_sync(full, dv, 1);
+        dv |= __shfl_xor_sync(full, dv, 2);
+        dv |= __shfl_xor_sync(full, dv, 4);
+        dv |= __shfl_xor_sync(full, dv, 8);
+        diff = dv != 0;
         const bool was_held = live && a.held && a.held[c];
         double2 pc = make_double2(0, 0);
         double Lx = 1, Ly = 1;
@@ -1039,29 +1050,31 @@ __global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
             Ly = in.Ly;
             pc = a.pos[c];
         }
+        // retract (skipped if the force pass held the contributions back) / add and refresh A/P
+        const int *grow = add ? srow : row;
+        const int gz = add ? zn : zo;
+        const bool gok = add ? (live && (diff || (FORCES && was_held)) && zn >= 3 && zn <= VG)
+                             : (FORCES && live && diff && !was_held && zo >= 3 && zo <= VG);
         int nbk[2];
         double A, P;
         int fail;
-        if (FORCES) {
-            // retract the old row's contributions (skipped if the force pass held them back)
-            const bool ok1 = live && diff && !was_held && zo >= 3 && zo <= VG;
-            grp_geometry<R, true, false>(a, c, row, zo, ok1, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail);
-            grp_scatter<R, -1>(a, c, zo, ok1, gl, tile[sl], nbk, A, P);
+        grp_geometry<R, FORCES, false>(a, c, grow, gz, gok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail, add);
+        if (FORCES) grp_scatter<R, 1>(a, c, gz, gok, gl, tile[sl], nbk, A, P, add ? R(1) : R(-1));
+        if (add && gok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
+        __syncwarp();
+        // swap rows; lane hl moves slot hl (both rows read before either is written)
+        int nv = -1, ov = -1;
+        const bool mv = live && diff && hl < a.K;
+        if (mv) {
+            nv = hl < zn ? srow[hl] : -1;
+            ov = hl < zo ? row[hl] : -1;
         }
         __syncwarp();
-        // swap rows; each lane moves the slots it owns
-        if (live && diff) {
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                int k = gl + G * r;
-                if (k < a.K) {
-                    int t = (k < zn) ? srow[k] : -1;
-                    srow[k] = (k < zo) ? row[k] : -1;
-                    row[k] = t;
-                }
-            }
+        if (mv) {
+            row[hl] = nv;
+            srow[hl] = ov;
         }
-        if (live && gl == 0) {
+        if (live && hl == 0) {
             if (a.held) a.held[c] = 0;
             if (diff) {
                 a.stage_nn[q] = zo;
@@ -1069,13 +1082,6 @@ __global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
             } else {
                 a.stage_nn[q] = -1;  // unchanged: still checked against its partners
             }
-        }
-        // add the new row's contributions and refresh A/P
-        const bool ok2 = live && (diff || (FORCES && was_held)) && zn >= 3 && zn <= VG;
-        grp_geometry<R, FORCES, false>(a, c, row, zn, ok2, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail);
-        if (FORCES) grp_scatter<R, 1>(a, c, zn, ok2, gl, tile[sl], nbk, A, P);
-        if (ok2 && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
-        if (live && gl == 0) {
             int slot = atomicAdd(&ctl->n_changed[round], 1);
             a.changed[(size_t)round * a.N + slot] = q;
             if (diff) atomicAdd(&ctl->counters[2], 1ull);
@@ -1324,7 +1330,7 @@ __global__ void __launch_bounds__(WPB * 32) k_star_global(VoroArgs a, int *statu
             ok = __all_sync(0xffffffffu, good);
         }
         if (ok) {
-            if (lane < z) a.nbr[(size_t)c * a.K + lane] = s_out[w][lane];
+            if (lane < a.K) a.nbr[(size_t)c * a.K + lane] = lane < z ? s_out[w][lane] : -1;  // padded
             if (lane == 0) a.nn[c] = z;
             return;
         }
