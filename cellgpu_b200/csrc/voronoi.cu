@@ -931,7 +931,6 @@ __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
     __shared__ int s_out[WPB][KMAX];
     __shared__ int s_hash[WPB][CAND_HASH];
     __shared__ int s_m[WPB];
-    const unsigned full = 0xffffffffu;
     Ctl *ctl = a.ctl;
     if (ctl->halt) return;
     int round = ctl->round;
