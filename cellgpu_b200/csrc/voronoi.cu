@@ -584,7 +584,8 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int 
             } else {
                 int k = fail >> 1;
                 bool orient_fail = fail & 1;
-                int nk = row[k], nk1 = row[(k + 1) % z], nkm = row[(k + z - 1) % z];
+                const int *rw = a.nbr + (size_t)c * a.K;  // (re-derived: keeps the pointer out of the live set)
+                int nk = rw[k], nk1 = rw[k + 1 == z ? 0 : k + 1], nkm = rw[k == 0 ? z - 1 : k - 1];
                 if (a.ctl) {
                     int e = a.ctl->epoch;
                     atomicAdd(&a.ctl->n_flagged, 1);
