@@ -236,6 +236,8 @@ struct cg_system {
     // asynchronous host-buffer steps: copy stream, a second staging buffer, per-buffer events
     cudaStream_t copy_stream = nullptr;
     double *noise_buf2 = nullptr;
+    double *e2e_acc = nullptr;       // energy partial sums of k_energy_to_host (zero between calls)
+    unsigned *e2e_done = nullptr;    // its finished-block counter
     cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_consumed[2] = {nullptr, nullptr};
     int host_slot = 0;
     // vertex model (model == CG_MODEL_VERTEX): pos/F are per vertex, AP/APpref/theta/motility per cell
@@ -1040,6 +1042,26 @@ extern "C" int cg_spp_enqueue_host(cg_system *s, const double *host_noise, doubl
     CG_CUDA(cudaEventRecord(s->ev_consumed[slot], s->stream));
     if (host_energy) {
         VoroArgs a = sys_args(s);
+        // page-locked host memory (cudaHostAlloc / cudaHostRegister) is written by the kernel
+        // itself; other host memory takes the reduction and a device-to-host copy
+        cudaPointerAttributes pa;
+        if (cudaPointerGetAttributes(&pa, host_energy) != cudaSuccess) {
+            cudaGetLastError();  // not a CUDA pointer: clear the error, copy instead
+            pa.type = cudaMemoryTypeUnregistered;
+        }
+        if (pa.type == cudaMemoryTypeHost && pa.devicePointer) {
+            if (!s->e2e_acc) {
+                CG_TRY(dalloc(s, &s->e2e_acc, s->n_inst));  // zeroed
+                CG_TRY(dalloc(s, &s->e2e_done, 1));
+            }
+            double *dst = static_cast<double *>(pa.devicePointer);
+            if (s->precision == CG_FP64)
+                k_energy_to_host<double><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->e2e_acc, s->e2e_done, dst);
+            else
+                k_energy_to_host<float><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->e2e_acc, s->e2e_done, dst);
+            s->kernels_enqueued += 1;
+            return check_launch();
+        }
         CG_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * s->n_inst, s->stream));
         if (s->precision == CG_FP64)
             k_energy<double><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);

@@ -1475,4 +1475,54 @@ __global__ void __launch_bounds__(256) k_energy(VoroArgs a, double *E)
     }
 }
 
+// The same sums written straight into page-locked host memory (host_out: its device address):
+// block partials gather in acc (zero between calls); the last block to finish stores the totals
+// to the host buffer and clears acc and its counter for the next call. One kernel replaces a
+// memset, the reduction and a device-to-host copy, each a separate operation in the stream.
+template <typename R>
+__global__ void __launch_bounds__(256) k_energy_to_host(VoroArgs a, double *acc, unsigned *done, double *host_out)
+{
+    __shared__ double s_part[8];
+    __shared__ int s_last;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    int inst = 0;
+    if (c < a.N) {
+        typename Vec2<R>::T ap = reinterpret_cast<typename Vec2<R>::T *>(a.AP)[c];
+        double da = (double)ap.x - a.APpref[c].x, dp = (double)ap.y - a.APpref[c].y;
+        e = a.KA * da * da + a.KP * dp * dp;
+        if (a.TE) e += 0.5 * a.TE[c];
+        inst = a.cell_inst ? a.cell_inst[c] : 0;
+    }
+    const int c0 = blockIdx.x * blockDim.x, c1 = min(a.N, c0 + (int)blockDim.x) - 1;
+    const int i0 = a.cell_inst ? a.cell_inst[c0] : 0, i1 = a.cell_inst ? a.cell_inst[c1] : 0;
+    if (i0 == i1) {
+        for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
+        if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = e;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
+            atomicAdd(&acc[i0], t);
+        }
+    } else if (c < a.N) {
+        atomicAdd(&acc[inst], e);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        for (int i = threadIdx.x; i < a.n_inst; i += blockDim.x) {
+            unsigned long long v = atomicExch(reinterpret_cast<unsigned long long *>(&acc[i]), 0ull);
+            host_out[i] = __longlong_as_double((long long)v);
+        }
+        __threadfence_system();
+        if (threadIdx.x == 0) *done = 0u;
+    }
+}
+
 }  // namespace cg

@@ -203,7 +203,8 @@ int cg_spp_step_host(cg_system *sys, const double *host_noise, double dt, double
 /* The same step, asynchronous: host_noise (N normals; pinned memory, or the copy is staged by the
  * driver) is copied on the system's copy stream into one of two device buffers, so the copy for the
  * next step overlaps this one; the step waits for its copy; host_energy (may be NULL) receives the
- * per-instance energies. Nothing is synchronised: both host buffers must stay
+ * per-instance energies (page-locked host memory is written directly by the reduction kernel, other
+ * memory through a device-to-host copy). Nothing is synchronised: both host buffers must stay
  * untouched until the step has completed (cg_poll, cg_synchronize, or an event recorded on the
  * system stream). Energies are those of cg_spp_step_host. Halts behave as for cg_spp_enqueue. */
 int cg_spp_enqueue_host(cg_system *sys, const double *host_noise, double dt, double mu, double *host_energy);

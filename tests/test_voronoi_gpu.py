@@ -138,6 +138,36 @@ def _spp_setup(pos, box, seed, v0=0.05):
     return b, theta, mot, pref, rng
 
 
+def test_enqueue_host_energy_buffers(cglib, torch):
+    """Energies of the asynchronous host-buffer step, per instance of a batch: into page-locked host
+    memory (written by the reduction kernel itself) and into ordinary memory (copied), over
+    repeated calls (the kernel's accumulators return to zero); each equals cg_get_energies."""
+    from cellgpu_b200 import VoronoiBatch
+    (p1, b1), (p2, b2) = jittered_lattice(12, 14, 0.25, 31), jittered_lattice(10, 12, 0.25, 32)
+    Ns = [len(p1), len(p2)]
+    N = sum(Ns)
+    rng = np.random.default_rng(33)
+    b = VoronoiBatch(Ns, [b1, b2])
+    b.set_positions(np.concatenate([p1, p2]))
+    b.set_directors(rng.uniform(0, 2 * np.pi, N))
+    b.set_motility(np.tile([0.1, 1.0], (N, 1)))
+    b.set_preferences(np.column_stack([np.ones(N), np.linspace(3.7, 3.9, N)]))
+    b.triangulate()
+    lib = b._lib
+    noise = torch.from_numpy(rng.normal(size=(8, N))).pin_memory()
+    pinned = torch.zeros((4, 2), dtype=torch.float64).pin_memory()
+    plain = np.zeros((4, 2))
+    for i in range(4):
+        for buf, dst in ((pinned, C.c_void_p(pinned[i].data_ptr())), (plain, plain[i].ctypes.data_as(C.c_void_p))):
+            k = 2 * i + (buf is plain)
+            assert lib.cg_spp_enqueue_host(b.handle, C.c_void_p(noise[k].data_ptr()), 0.01, 1.0, dst) == 0
+            assert lib.cg_poll(b.handle, None, None, 1) == 0
+            got = np.asarray(buf[i])
+            E = b.energies()
+            np.testing.assert_allclose(got, E, rtol=1e-12)
+            assert np.all(got > 0)
+
+
 @pytest.mark.parametrize("N,steps,seed,v0,dt", [(300, 20, 10, 0.05, 0.01), (1500, 15, 11, 0.05, 0.01),
                                                (1152, 12, 12, 1.0, 0.05)])
 def test_spp_each_step_matches_oracle(cglib, oracle, torch, N, steps, seed, v0, dt):
