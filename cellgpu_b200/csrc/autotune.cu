@@ -77,7 +77,7 @@ extern "C" int cg_autotune(cg_system *s, double *times_ms, int *choice)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     CG_CUDA(cudaStreamSynchronize(s->stream));
-    for (auto &g : s->graphs) cudaGraphExecDestroy(g.exec);
+    for (auto &g : s->graphs) release_graph(g);
     s->graphs.clear();
     if (times_ms) {
         times_ms[0] = t_force[0];

@@ -222,13 +222,16 @@ struct cg_system {
     cudaStream_t own_stream = nullptr;
     cudaStream_t body_stream = nullptr;  // captures the bodies of conditional graph nodes
     struct GraphEntry {
-        int kind;  // 0 Voronoi SPP, 1 vertex Brownian, 2 vertex SPP, 3 FIRE iterations
+        int kind;  // 0 Voronoi SPP, 1 vertex Brownian, 2 vertex SPP, 3 FIRE iterations, 4 SPP + energy out
         int n;
         double dt, mu, T;
         const double *noise;
         cudaGraphExec_t exec;
         long long kernels;
         cg_fire_params fire;  // FIRE graphs: the parameters captured into the iteration kernels
+        // host-energy step graphs (kind 4): the graph kept for updating its energy kernel node
+        cudaGraph_t graph = nullptr;
+        cudaGraphNode_t energy_node = nullptr;
     };
     std::vector<GraphEntry> graphs;
     long long kernels_enqueued = 0;  // kernels of this library launched for this system
@@ -267,6 +270,12 @@ struct cg_system {
     int *fire_dofinst = nullptr;
 };
 
+static void release_graph(cg_system::GraphEntry &g)
+{
+    cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+}
+
 static int ndof(const cg_system *s) { return s->model == CG_MODEL_VERTEX ? s->Nv : s->N; }
 
 // Device memory of a system comes from the stream-ordered allocator on the system's stream, and
@@ -298,7 +307,7 @@ static int sys_streams(cg_system *s)
 static void sys_release(cg_system *s)
 {
     if (s->stream) cudaStreamSynchronize(s->stream);
-    for (auto &g : s->graphs) cudaGraphExecDestroy(g.exec);
+    for (auto &g : s->graphs) release_graph(g);
     s->graphs.clear();
     cudaStream_t fs = s->own_stream;
     for (void *p : s->allocs) {
@@ -845,9 +854,12 @@ static void enqueue_spp_steps(cg_system *s, int n, double dt, double mu, const d
 // repair rounds inside a WHILE conditional node (the device decides whether another round runs),
 // then integrate + move and the step epilogue. Kernels take queue lengths, epochs, rounds and the
 // step counter from the device control block, so one graph serves every call.
+// energy_node != null: the graph ends with k_energy_to_host writing to energy_dst, the graph
+// template is kept (*keep) and *energy_node is that kernel's node, for per-call destination updates
 template <typename R>
 static int build_graph(cg_system *s, int n, double dt, double mu, const double *noise, cudaGraphExec_t *exec,
-                       long long *static_kernels)
+                       long long *static_kernels, double *energy_dst = nullptr,
+                       cudaGraphNode_t *energy_node = nullptr, cudaGraph_t *keep = nullptr)
 {
     VoroArgs a = sys_args(s);
     cudaGraph_t graph;
@@ -875,6 +887,12 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
             k_spp<R><<<nblk((s->N + 1) / 2, SPP_BLOCK), SPP_BLOCK, 0, s->stream>>>(a, noise, dt, mu, 0u, 0);
             k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
             s->kernels_enqueued += 2;
+        }
+        if (energy_node) {
+            k_energy_to_host<R><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->e2e_acc, s->e2e_done, energy_dst);
+            s->kernels_enqueued += 1;
+            st = capture_deps(s->stream);
+            if (st == CG_OK) *energy_node = deps.empty() ? nullptr : deps[0];
         }
         cudaGraph_t g2;
         CG_CUDA(cudaStreamEndCapture(s->stream, &g2));
@@ -909,14 +927,23 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
         k_spp<R><<<nblk((s->N + 1) / 2, SPP_BLOCK), SPP_BLOCK, 0, s->stream>>>(a, nz, dt, mu, 0u, 0);
         k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
         s->kernels_enqueued += 2;
+        if (energy_node && t == n - 1) {
+            k_energy_to_host<R><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->e2e_acc, s->e2e_done, energy_dst);
+            s->kernels_enqueued += 1;
+        }
         st = capture_deps(s->stream);
+        if (st == CG_OK && energy_node && t == n - 1) *energy_node = deps.empty() ? nullptr : deps[0];
         CG_CUDA(cudaStreamEndCapture(s->stream, &g2));
     }
+    if (st == CG_OK && energy_node && !*energy_node) st = set_err(CG_ERR_CUDA, "energy node not captured");
     if (st == CG_OK) {
         cudaError_t e = cudaGraphInstantiate(exec, graph, 0);
         if (e != cudaSuccess) st = set_err(CG_ERR_CUDA, cudaGetErrorString(e));
     }
-    cudaGraphDestroy(graph);
+    if (st == CG_OK && keep)
+        *keep = graph;  // its nodes name the exec's nodes for later parameter updates
+    else
+        cudaGraphDestroy(graph);
     *static_kernels = s->kernels_enqueued - k0;
     s->kernels_enqueued = k0;
     return st;
@@ -1015,6 +1042,47 @@ extern "C" int cg_spp_step_host(cg_system *s, const double *host_noise, double d
     return CG_OK;
 }
 
+// one host-buffer step whose graph ends with the energy kernel writing to page-locked host memory;
+// the kernel node's destination is updated per call (cudaGraphExecKernelNodeSetParams), so the
+// step and its energy readout are one graph launch
+template <typename R>
+static int enqueue_energy_graph(cg_system *s, double dt, double mu, const double *noise, double *dst)
+{
+    if (!s->e2e_acc) {
+        CG_TRY(dalloc(s, &s->e2e_acc, s->n_inst));  // zeroed; the kernel leaves it zeroed
+        CG_TRY(dalloc(s, &s->e2e_done, 1));
+    }
+    for (auto &g : s->graphs)
+        if (g.kind == 4 && g.dt == dt && g.mu == mu && g.noise == noise) {
+            VoroArgs a = sys_args(s);
+            double *acc = s->e2e_acc, *d = dst;
+            unsigned *done = s->e2e_done;
+            void *args[] = {&a, &acc, &done, &d};
+            cudaKernelNodeParams kp;
+            memset(&kp, 0, sizeof(kp));
+            kp.func = (void *)k_energy_to_host<R>;
+            kp.gridDim = dim3(nblk(s->N, 256));
+            kp.blockDim = dim3(256);
+            kp.kernelParams = args;
+            CG_CUDA(cudaGraphExecKernelNodeSetParams(g.exec, g.energy_node, &kp));
+            CG_CUDA(cudaGraphLaunch(g.exec, s->stream));
+            s->kernels_enqueued += g.kernels;
+            return CG_OK;
+        }
+    cudaGraphExec_t exec;
+    cudaGraph_t keep = nullptr;
+    cudaGraphNode_t node = nullptr;
+    long long nk = 0;
+    CG_TRY(build_graph<R>(s, 1, dt, mu, noise, &exec, &nk, dst, &node, &keep));
+    cg_system::GraphEntry e{4, 1, dt, mu, 0.0, noise, exec, nk};
+    e.graph = keep;
+    e.energy_node = node;
+    s->graphs.push_back(e);
+    CG_CUDA(cudaGraphLaunch(exec, s->stream));
+    s->kernels_enqueued += nk;
+    return CG_OK;
+}
+
 extern "C" int cg_spp_enqueue_host(cg_system *s, const double *host_noise, double dt, double mu,
                                    double *host_energy)
 {
@@ -1028,6 +1096,17 @@ extern "C" int cg_spp_enqueue_host(cg_system *s, const double *host_noise, doubl
         }
         CG_TRY(dalloc(s, &s->noise_buf2, s->N));
     }
+    // page-locked host memory (cudaHostAlloc / cudaHostRegister) for the energies is written by
+    // the step graph's last kernel; other host memory takes a reduction and a device-to-host copy
+    double *edst = nullptr;
+    if (host_energy) {
+        cudaPointerAttributes pa;
+        if (cudaPointerGetAttributes(&pa, host_energy) != cudaSuccess) {
+            cudaGetLastError();  // not a CUDA pointer: clear the error, copy instead
+            pa.type = cudaMemoryTypeUnregistered;
+        }
+        if (pa.type == cudaMemoryTypeHost && pa.devicePointer) edst = static_cast<double *>(pa.devicePointer);
+    }
     int slot = s->host_slot;
     s->host_slot ^= 1;
     double *buf = slot ? s->noise_buf2 : s->noise_buf;
@@ -1036,32 +1115,17 @@ extern "C" int cg_spp_enqueue_host(cg_system *s, const double *host_noise, doubl
     CG_CUDA(cudaMemcpyAsync(buf, host_noise, sizeof(double) * s->N, cudaMemcpyHostToDevice, s->copy_stream));
     CG_CUDA(cudaEventRecord(s->ev_copied[slot], s->copy_stream));
     CG_CUDA(cudaStreamWaitEvent(s->stream, s->ev_copied[slot], 0));
-    int st = s->precision == CG_FP64 ? enqueue_graph<double>(s, 1, dt, mu, buf)
+    int st;
+    if (edst)
+        st = s->precision == CG_FP64 ? enqueue_energy_graph<double>(s, dt, mu, buf, edst)
+                                     : enqueue_energy_graph<float>(s, dt, mu, buf, edst);
+    else
+        st = s->precision == CG_FP64 ? enqueue_graph<double>(s, 1, dt, mu, buf)
                                      : enqueue_graph<float>(s, 1, dt, mu, buf);
     if (st) return st;
     CG_CUDA(cudaEventRecord(s->ev_consumed[slot], s->stream));
-    if (host_energy) {
+    if (host_energy && !edst) {
         VoroArgs a = sys_args(s);
-        // page-locked host memory (cudaHostAlloc / cudaHostRegister) is written by the kernel
-        // itself; other host memory takes the reduction and a device-to-host copy
-        cudaPointerAttributes pa;
-        if (cudaPointerGetAttributes(&pa, host_energy) != cudaSuccess) {
-            cudaGetLastError();  // not a CUDA pointer: clear the error, copy instead
-            pa.type = cudaMemoryTypeUnregistered;
-        }
-        if (pa.type == cudaMemoryTypeHost && pa.devicePointer) {
-            if (!s->e2e_acc) {
-                CG_TRY(dalloc(s, &s->e2e_acc, s->n_inst));  // zeroed
-                CG_TRY(dalloc(s, &s->e2e_done, 1));
-            }
-            double *dst = static_cast<double *>(pa.devicePointer);
-            if (s->precision == CG_FP64)
-                k_energy_to_host<double><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->e2e_acc, s->e2e_done, dst);
-            else
-                k_energy_to_host<float><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->e2e_acc, s->e2e_done, dst);
-            s->kernels_enqueued += 1;
-            return check_launch();
-        }
         CG_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * s->n_inst, s->stream));
         if (s->precision == CG_FP64)
             k_energy<double><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);

@@ -21,7 +21,7 @@
 static void drop_graphs(cg_system *s)
 {
     cudaStreamSynchronize(s->stream);
-    for (auto &g : s->graphs) cudaGraphExecDestroy(g.exec);  // graphs captured the old arguments
+    for (auto &g : s->graphs) release_graph(g);  // graphs captured the old arguments
     s->graphs.clear();
 }
 

@@ -145,7 +145,7 @@ extern "C" int cg_set_t1_threshold(cg_system *s, double threshold)
 {
     if (!s || s->model != CG_MODEL_VERTEX || !(threshold >= 0)) return set_err(CG_ERR_ARG, "bad args");
     s->t1 = threshold;
-    for (auto &g : s->graphs) cudaGraphExecDestroy(g.exec);  // graphs bake the threshold in
+    for (auto &g : s->graphs) release_graph(g);  // graphs bake the threshold in
     s->graphs.clear();
     return CG_OK;
 }
