@@ -60,19 +60,29 @@ static inline int cells_per_block(int N, int wpb, int minb)
     return std::max(grp, (cpb + grp - 1) / grp * grp);
 }
 
-// launch of the fused per-cell pass (groups of 8 lanes) in launch shape 0 or 1
-template <typename R, bool SCATTER, bool TEST>
-static inline void launch_groups(const VoroArgs &a, int N, cudaStream_t st, int shape = 0)
+// launch of the fused per-cell pass (groups of 8 lanes) in launch shape 0 or 1; rows of up to 16
+// slots take the fast form, wider rows (K = 32) the form with four slots per lane
+template <typename R, bool SCATTER, bool TEST, int NS>
+static inline void launch_groups_ns(const VoroArgs &a, int N, cudaStream_t st, int shape)
 {
     if (shape == 1) {
         int cpb = cells_per_block(N, CG_FORCE_WPB_ALT, CG_FORCE_MINB_ALT);
-        k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB_ALT, CG_FORCE_MINB_ALT>
+        k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB_ALT, CG_FORCE_MINB_ALT, NS>
             <<<nblk(N, cpb), CG_FORCE_WPB_ALT * 32, 0, st>>>(a, cpb);
     } else {
         int cpb = cells_per_block(N, CG_FORCE_WPB, CG_FORCE_MINB);
-        k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB, CG_FORCE_MINB>
+        k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB, CG_FORCE_MINB, NS>
             <<<nblk(N, cpb), CG_FORCE_WPB * 32, 0, st>>>(a, cpb);
     }
+}
+
+template <typename R, bool SCATTER, bool TEST>
+static inline void launch_groups(const VoroArgs &a, int N, cudaStream_t st, int shape = 0)
+{
+    if (a.K > VG)
+        launch_groups_ns<R, SCATTER, TEST, VG_MAX>(a, N, st, shape);
+    else
+        launch_groups_ns<R, SCATTER, TEST, VG>(a, N, st, shape);
 }
 
 static Inst make_inst(double Lx, double Ly, int off, int n, int bin_off, double bin_target)
@@ -393,7 +403,7 @@ extern "C" size_t cg_voronoi_footprint(int n_inst, const int *N, int K)
 extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, int K, int precision,
                                  cg_system **out)
 {
-    if (n_inst <= 0 || !N || !box || !out || K < 4 || K > VG ||
+    if (n_inst <= 0 || !N || !box || !out || K < 4 || K > VG_MAX || (K & 3) ||
         (precision != CG_FP64 && precision != CG_MIXED))
         return set_err(CG_ERR_ARG, "bad args");
     cg_system *s = new cg_system();
@@ -664,6 +674,8 @@ static int build_cell_list(cg_system *s)
     return check_launch();
 }
 
+static int grow_rows(cg_system *s);
+
 static int triangulate_sys(cg_system *s)
 {
     CG_TRY(build_cell_list(s));
@@ -675,6 +687,10 @@ static int triangulate_sys(cg_system *s)
     CG_TRY(check_launch());
     int st = 0;
     CG_TRY(d2h(s, &st, s->d_status, sizeof(int)));
+    if (st == CG_ERR_CAPACITY && s->K < VG_MAX) {  // a cell with more than K neighbours: widen, retry
+        CG_TRY(grow_rows(s));
+        return triangulate_sys(s);
+    }
     if (st) return set_err(st, st == CG_ERR_CAPACITY ? "neighbour capacity exceeded in triangulation"
                                                       : "global triangulation failed");
     k_validate<<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_status, s->d_zsum);
@@ -736,27 +752,46 @@ static void launch_force_test(cg_system *s, const VoroArgs &a, bool test)
     s->kernels_enqueued += 1;
 }
 
-template <typename R>
-static void launch_round(cg_system *s, const VoroArgs &a, bool forces, cudaStream_t st, unsigned long long cond,
-                         int use_cond)
+template <typename R, int NS>
+static void launch_round_ns(const VoroArgs &a, bool forces, cudaStream_t st, unsigned long long cond, int use_cond)
 {
     constexpr int WPB = 4;
     // commit / check: 8 queue slots per 64-thread block, so a short queue still spreads over the SMs
     constexpr int WPB_C = 2;
     k_star_local<WPB><<<148 * 4, WPB * 32, 0, st>>>(a);
     if (forces)
-        k_commit<R, true, WPB_C><<<148 * 8, WPB_C * 32, 0, st>>>(a);
+        k_commit<R, true, WPB_C, NS><<<148 * 8, WPB_C * 32, 0, st>>>(a);
     else
-        k_commit<R, false, WPB_C><<<148 * 8, WPB_C * 32, 0, st>>>(a);
-    k_check<WPB_C><<<148 * 8, WPB_C * 32, 0, st>>>(a);
+        k_commit<R, false, WPB_C, NS><<<148 * 8, WPB_C * 32, 0, st>>>(a);
+    k_check<WPB_C, NS><<<148 * 8, WPB_C * 32, 0, st>>>(a);
     k_round_end<<<1, 1, 0, st>>>(a, cond, use_cond);
+}
+
+template <typename R>
+static void launch_round(cg_system *s, const VoroArgs &a, bool forces, cudaStream_t st, unsigned long long cond,
+                         int use_cond)
+{
+    if (a.K > VG)
+        launch_round_ns<R, VG_MAX>(a, forces, st, cond, use_cond);
+    else
+        launch_round_ns<R, VG>(a, forces, st, cond, use_cond);
+}
+
+// start of the repair (undecided in-circle slots of the force pass, then the WHILE condition)
+template <typename R>
+static void launch_repair_begin(const VoroArgs &a, cudaStream_t st, unsigned long long cond, int use_cond, int forces)
+{
+    if (a.K > VG)
+        k_repair_begin<R, VG_MAX><<<1, 128, 0, st>>>(a, cond, use_cond, forces);
+    else
+        k_repair_begin<R, VG><<<1, 256, 0, st>>>(a, cond, use_cond, forces);
 }
 
 // repair rounds as plain launches (used outside graphs): every round is launched; empty rounds exit
 template <typename R>
 static void launch_repair(cg_system *s, const VoroArgs &a, bool forces)
 {
-    k_repair_begin<R><<<1, 256, 0, s->stream>>>(a, 0ull, 0, forces ? 1 : 0);
+    launch_repair_begin<R>(a, s->stream, 0ull, 0, forces ? 1 : 0);
     for (int r = 0; r < R_MAX; ++r) launch_round<R>(s, a, forces, s->stream, 0ull, 0);
     s->kernels_enqueued += 1;
 }
@@ -779,12 +814,44 @@ static int reset_ctl_after_halt(cg_system *s)
 }
 
 // handle a halted step: global retriangulation (or report the error)
+// Row capacity growth (the reference grows neighMax the same way, voronoiModelBase::
+// allDelSets / resetLists): rows go from K to 32 slots, copied and padded with -1; the staging rows
+// and the sort scratch are reallocated at the new width, and captured graphs (which hold the old
+// width and pointers) are dropped. The group kernels then run in their 32-slot form.
+__global__ void k_widen_rows(int N, int K, int K2, const int *src, int *dst)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    for (int k = 0; k < K2; ++k) dst[(size_t)c * K2 + k] = k < K ? src[(size_t)c * K + k] : -1;
+}
+
+static int grow_rows(cg_system *s)
+{
+    if (s->model != CG_MODEL_VORONOI || s->K >= VG_MAX)
+        return set_err(CG_ERR_CAPACITY, "neighbour capacity exceeded (more than 32 neighbours)");
+    const int K2 = VG_MAX;
+    CG_CUDA(cudaStreamSynchronize(s->stream));
+    for (auto &g : s->graphs) release_graph(g);
+    s->graphs.clear();
+    int *nbr2 = nullptr, *stage2 = nullptr;
+    CG_TRY(dalloc(s, &nbr2, (size_t)s->N * K2));
+    CG_TRY(dalloc(s, &stage2, (size_t)s->N * K2));
+    k_widen_rows<<<nblk(s->N, 256), 256, 0, s->stream>>>(s->N, s->K, K2, s->nbr, nbr2);
+    CG_TRY(check_launch());
+    s->nbr = nbr2;  // (the old blocks stay in the arena until the system is destroyed)
+    s->stage_nbr = stage2;
+    if (s->sort_tmp)
+        CG_TRY(dalloc(s, (char **)&s->sort_tmp, (size_t)s->N * std::max<size_t>(16, sizeof(int) * (size_t)(K2 + 1))));
+    s->K = K2;
+    return cg_synchronize(s);
+}
+
 static int recover(cg_system *s)
 {
     Ctl c;
     CG_TRY(read_ctl(s, c));
     if (!c.halt) return CG_OK;
-    if (c.status == CG_ERR_CAPACITY) return set_err(CG_ERR_CAPACITY, "neighbour capacity exceeded");
+    if (c.status == CG_ERR_CAPACITY) CG_TRY(grow_rows(s));
     CG_TRY(reset_ctl_after_halt(s));
     if (s->held) CG_CUDA(cudaMemsetAsync(s->held, 0, sizeof(int) * s->N, s->stream));
     return triangulate_sys(s);
@@ -903,7 +970,7 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
         CG_CUDA(cudaStreamBeginCaptureToGraph(s->stream, graph, deps.empty() ? nullptr : deps.data(), nullptr,
                                               deps.size(), mode));
         launch_force_test<R>(s, a, true);
-        k_repair_begin<R><<<1, 256, 0, s->stream>>>(a, (unsigned long long)h, 1, 1);
+        launch_repair_begin<R>(a, s->stream, (unsigned long long)h, 1, 1);
         s->kernels_enqueued += 1;
         st = capture_deps(s->stream);
         cudaGraph_t g2;

@@ -299,7 +299,8 @@ __global__ void __launch_bounds__(128) k_voro_cells(VoroArgs a)
 // ------------------------------------------------------------------------------------------
 constexpr int G = 8;
 constexpr int GPW = 32 / G;  // cells per warp
-constexpr int VG = 16;       // vertices per cell in the group kernel (K <= 16)
+constexpr int VG = 16;       // vertices per cell in the group kernels' fast form (K <= 16)
+constexpr int VG_MAX = 32;   // their wide form, for systems whose rows grew to K = 32
 
 template <typename R>
 CG_D R group_sum(R v)
@@ -330,27 +331,27 @@ CG_D bool group_any(bool v)
 // Shared-memory tile of one group's cell: relative neighbour positions r_k, Voronoi vertices h_k,
 // the reciprocal 1 / (2 r_{k-1} x r_k) (shared by h_k and its Jacobians), unit tangents of the
 // edges h_k -> h_{k+1}, and the dh_k/dr_{k-1} contraction consumed by the neighbouring lane.
-template <typename R>
+template <typename R, int NS = VG>
 struct GrpTile {
-    double2 r[VG];
-    double2 h[VG];
-    double den[VG];
-    typename Vec2<R>::T u[VG];
-    typename Vec2<R>::T ca[VG];
-    double w[VG];  // line-tension weight of the edge h_k -> h_{k+1} (dual to neighbour k)
+    double2 r[NS];
+    double2 h[NS];
+    double den[NS];
+    typename Vec2<R>::T u[NS];
+    typename Vec2<R>::T ca[NS];
+    double w[NS];  // line-tension weight of the edge h_k -> h_{k+1} (dual to neighbour k)
 };
 
 // Phases A-C of one group's cell (called by the whole warp; `ok` switches a group off): relative
 // neighbour positions (FP64, the exact Delaunay inputs), Voronoi vertices, A, P, the exact local
 // test (TEST) and the edge unit vectors (SCATTER). nbk receives the neighbours of the lane's slots.
-template <typename R, bool SCATTER, bool TEST>
+template <typename R, bool SCATTER, bool TEST, int NS = VG>
 CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok, double2 pc, double Lx,
-                       double Ly, int gl, GrpTile<R> &T, int (&nbk)[2], double &A, double &P, int &fail,
+                       double Ly, int gl, GrpTile<R, NS> &T, int (&nbk)[NS / G], double &A, double &P, int &fail,
                        bool store_te = true)
 {
     using V = typename Vec2<R>::T;
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
+    for (int r = 0; r < NS / G; ++r) {
         int k = gl + G * r;
         nbk[r] = -1;
         if (ok && k < z) {
@@ -364,7 +365,7 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
     fail = 0x7fffffff;  // smallest failing slot (x2, +1 for orientation)
     int undecided = 0;  // slots whose in-circle sign the filter left to the canonical evaluation
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
+    for (int r = 0; r < NS / G; ++r) {
         int k = gl + G * r;
         if (ok && k < z) {
             int km = k == 0 ? z - 1 : k - 1;
@@ -390,11 +391,11 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
         // rare: the canonical evaluation runs in k_repair_begin (keeping this kernel's registers for
         // the common path); without a list, or when it is full, the edge counts as failing and the
         // repair recomputes the stars with the canonical predicate
-        for (int r = 0; r < 2; ++r) {
+        for (int r = 0; r < NS / G; ++r) {
             if (!(undecided & (1 << r))) continue;
             int k = gl + G * r;
             int idx = (a.undec && a.ctl) ? atomicAdd(&a.ctl->n_undec, 1) : a.N;
-            if (idx < a.N) a.undec[idx] = c * VG + k;
+            if (idx < a.N) a.undec[idx] = c * NS + k;
             else fail = min(fail, 2 * k);
         }
     }
@@ -403,7 +404,7 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
     // are small differences), unit tangents
     double Ap = 0, Pp = 0;
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
+    for (int r = 0; r < NS / G; ++r) {
         int k = gl + G * r;
         if (ok && k < z) {
             double2 h0 = T.h[k], h1 = T.h[k + 1 == z ? 0 : k + 1];
@@ -441,7 +442,7 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
         double Tp = 0.0;
         const int tc = ok ? a.ctype[c] : 0;
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
+        for (int r = 0; r < NS / G; ++r) {
             int k = gl + G * r;
             if (ok && k < z) {
                 double w = tension_weight(a, tc, a.ctype[nbk[r]]);
@@ -458,8 +459,8 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
 
 // Phases D-E (called by the whole warp): g_k = -dE_c/dh_k, the three Jacobian contractions of every
 // vertex, and the scatter of SIGN x (contribution) to the cell and its neighbours.
-template <typename R, int SIGN>
-CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<R> &T, const int (&nbk)[2],
+template <typename R, int SIGN, int NS = VG>
+CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<R, NS> &T, const int (&nbk)[NS / G],
                       double A, double P, R sgn = R(SIGN))
 {
     using V = typename Vec2<R>::T;
@@ -470,9 +471,9 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<
         Pdiff = (R)(a.KP * (P - a.APpref[c].y));
     }
     R sx = 0, sy = 0;
-    V cb[2];
+    V cb[NS / G];
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
+    for (int r = 0; r < NS / G; ++r) {
         int k = gl + G * r;
         if (ok && k < z) {
             int km = k == 0 ? z - 1 : k - 1, kp = k + 1 == z ? 0 : k + 1;
@@ -518,7 +519,7 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<
     sy = group_sum<R>(sy);
     __syncwarp();
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
+    for (int r = 0; r < NS / G; ++r) {
         int k = gl + G * r;
         if (ok && k < z) {
             V ca = T.ca[k + 1 == z ? 0 : k + 1];
@@ -532,10 +533,10 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<
 
 // A block takes a contiguous run of cpb cells (a multiple of its WPB * GPW groups), so that in a
 // spatially sorted system the cells one SM works on are neighbours and their positions stay in L1.
-template <typename R, bool SCATTER, bool TEST, int WPB, int MINB>
+template <typename R, bool SCATTER, bool TEST, int WPB, int MINB, int NS = VG>
 __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int cpb)
 {
-    __shared__ GrpTile<R> tile[WPB * GPW];
+    __shared__ GrpTile<R, NS> tile[WPB * GPW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int gl = lane & (G - 1), gi = lane >> 3;
     const int sl = w * GPW + gi;
@@ -556,24 +557,24 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int 
             z = a.nn[c];
             row = a.nbr + (size_t)c * a.K;
         }
-        const bool ok = live && z >= 3 && z <= VG;
-        int nbk[2];
+        const bool ok = live && z >= 3 && z <= NS;
+        int nbk[NS / G];
         double A, P;
         int fail;
-        grp_geometry<R, SCATTER, TEST>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail);
+        grp_geometry<R, SCATTER, TEST, NS>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail);
         if (ok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
         // A cell whose own row fails the test holds its contributions back: the row is about to be
         // replaced, and a stale row can contain a nearly collinear triangle whose Jacobians (1/cross^2)
         // would swamp the forces. The repair commit adds the contributions of the new row.
         bool hold = SCATTER && TEST && a.held && ok && fail != 0x7fffffff;
         if (hold && gl == 0) a.held[c] = 1;
-        if (SCATTER) grp_scatter<R, 1>(a, c, z, ok && !hold, gl, tile[sl], nbk, A, P);
+        if (SCATTER) grp_scatter<R, 1, NS>(a, c, z, ok && !hold, gl, tile[sl], nbk, A, P);
         if (TEST && live && gl == 0 && (fail != 0x7fffffff || !ok)) {
             if (!ok) {
                 if (a.ctl) {
                     atomicAdd(&a.ctl->n_flagged, 1);
                     claim_enqueue(a, c, a.ctl->epoch, 0);
-                    if (z > VG) {
+                    if (z > NS) {
                         atomicExch(&a.ctl->status, CG_ERR_CAPACITY);
                         atomicExch(&a.ctl->halt, 1);
                     }
@@ -617,12 +618,12 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int 
 // a failing edge: the cell's contributions, already scattered, are retracted and the cell is marked
 // held (once per cell), and the cell, the edge's other end and both apexes are queued. Then the
 // WHILE node is entered if queue 0 has cells.
-template <typename R>
+template <typename R, int NS = VG>
 __global__ void __launch_bounds__(256) k_repair_begin(VoroArgs a, unsigned long long cond, int use_cond,
                                                       int forces)
 {
-    constexpr int WPB = 8;
-    __shared__ GrpTile<R> tile[WPB * GPW];
+    constexpr int WPB = NS == VG ? 8 : 4;  // launched with WPB warps (shared tiles stay under 48 KB)
+    __shared__ GrpTile<R, NS> tile[WPB * GPW];
     Ctl *ctl = a.ctl;
     const int nu = min(ctl->n_undec, a.N);
     if (!ctl->halt && nu > 0 && a.undec) {
@@ -639,8 +640,8 @@ __global__ void __launch_bounds__(256) k_repair_begin(VoroArgs a, unsigned long 
             bool fails = false;
             if (t < nu) {
                 const int en = a.undec[t];
-                c = en / VG;
-                k = en % VG;
+                c = en / NS;
+                k = en % NS;
                 z = a.nn[c];
                 row = a.nbr + (size_t)c * a.K;
                 const Inst &in = inst_of(a, c);
@@ -664,12 +665,12 @@ __global__ void __launch_bounds__(256) k_repair_begin(VoroArgs a, unsigned long 
             }
             first = __shfl_sync(0xffffffffu, first, lane & ~(G - 1));
             if (forces) {
-                const bool ok = fails && first && z >= 3 && z <= VG;
-                int nbk[2];
+                const bool ok = fails && first && z >= 3 && z <= NS;
+                int nbk[NS / G];
                 double A, P;
                 int fl;
-                grp_geometry<R, true, false>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fl);
-                grp_scatter<R, -1>(a, c, z, ok, gl, tile[sl], nbk, A, P);
+                grp_geometry<R, true, false, NS>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fl);
+                grp_scatter<R, -1, NS>(a, c, z, ok, gl, tile[sl], nbk, A, P);
             }
             __syncwarp();
         }
@@ -959,16 +960,18 @@ __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
             // lengths; a lane takes slot (lane & 15) of members lane >> 4, +2, +4, +6 of each group
             // of 8 members, and the four loads are in flight together
             for (int base = lo; base < hi; base += 8) {
-                const int e = lane & 15;
-                int v[4];
+                for (int eb = 0; eb < a.K; eb += 16) {  // rows wider than 16 (K = 32) in two halves
+                    const int e = eb + (lane & 15);
+                    int v[4];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int j = base + (lane >> 4) + 2 * i;
-                    v[i] = (j < hi && e < a.K) ? a.nbr[(size_t)s_cand[w][j] * a.K + e] : -1;
+                    for (int i = 0; i < 4; ++i) {
+                        const int j = base + (lane >> 4) + 2 * i;
+                        v[i] = (j < hi && e < a.K) ? a.nbr[(size_t)s_cand[w][j] * a.K + e] : -1;
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (v[i] >= 0 && v[i] != c && *vm < CAND_LOCAL) cand_insert(s_hash[w], s_cand[w], &s_m[w], v[i]);
                 }
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    if (v[i] >= 0 && v[i] != c && *vm < CAND_LOCAL) cand_insert(s_hash[w], s_cand[w], &s_m[w], v[i]);
             }
             __syncwarp();
             lo = hi;
@@ -1005,10 +1008,10 @@ __global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
 // run side by side; A/P are refreshed from the new row, and the old row is kept in the staging slot
 // for the consistency check. Unchanged rows whose force contributions the force pass held back add
 // them now.
-template <typename R, bool FORCES, int WPB>
+template <typename R, bool FORCES, int WPB, int NS = VG>
 __global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
 {
-    __shared__ GrpTile<R> tile[WPB * GPW];
+    __shared__ GrpTile<R, NS> tile[WPB * GPW];
     Ctl *ctl = a.ctl;
     if (ctl->halt) return;
     int round = ctl->round;
@@ -1020,7 +1023,7 @@ __global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
     const int gl = lane & (G - 1), gi = lane >> 3;
     const int sl = w * GPW + gi;
     const bool add = gi & 1;       // group 0 of a slot: old row (retract); group 1: new row (add)
-    const int hl = lane & 15;      // lane within the slot's 16 lanes = row slot it moves
+    const int hl = lane & 15;      // lane within the slot's 16 lanes: moves row slots hl, hl + 16
     const int step = gridDim.x * WPB * (GPW / 2);
     for (int base = (blockIdx.x * WPB + w) * (GPW / 2); base < nq; base += step) {  // warp-uniform loop
         const int q = base + (gi >> 1);
@@ -1034,7 +1037,9 @@ __global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
         int *row = a.nbr + (size_t)c * a.K;
         int *srow = a.stage_nbr + (size_t)(live ? q : 0) * a.K;
         bool diff = live && zo != zn;
-        if (live && !diff && hl < zn && row[hl] != srow[hl]) diff = true;
+#pragma unroll
+        for (int e = hl; e < NS; e += 16)
+            if (live && !diff && e < zn && row[e] != srow[e]) diff = true;
         int dv = diff ? 1 : 0;
         dv |= __shfl_xor_sync(full, dv, 1);
         dv |= __shfl_xor_sync(full, dv, 2);
@@ -1053,26 +1058,35 @@ __global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
         // retract (skipped if the force pass held the contributions back) / add and refresh A/P
         const int *grow = add ? srow : row;
         const int gz = add ? zn : zo;
-        const bool gok = add ? (live && (diff || (FORCES && was_held)) && zn >= 3 && zn <= VG)
-                             : (FORCES && live && diff && !was_held && zo >= 3 && zo <= VG);
-        int nbk[2];
+        const bool gok = add ? (live && (diff || (FORCES && was_held)) && zn >= 3 && zn <= NS)
+                             : (FORCES && live && diff && !was_held && zo >= 3 && zo <= NS);
+        int nbk[NS / G];
         double A, P;
         int fail;
-        grp_geometry<R, FORCES, false>(a, c, grow, gz, gok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail, add);
-        if (FORCES) grp_scatter<R, 1>(a, c, gz, gok, gl, tile[sl], nbk, A, P, add ? R(1) : R(-1));
+        grp_geometry<R, FORCES, false, NS>(a, c, grow, gz, gok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail, add);
+        if (FORCES) grp_scatter<R, 1, NS>(a, c, gz, gok, gl, tile[sl], nbk, A, P, add ? R(1) : R(-1));
         if (add && gok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
         __syncwarp();
-        // swap rows; lane hl moves slot hl (both rows read before either is written)
-        int nv = -1, ov = -1;
-        const bool mv = live && diff && hl < a.K;
-        if (mv) {
-            nv = hl < zn ? srow[hl] : -1;
-            ov = hl < zo ? row[hl] : -1;
+        // swap rows; lane hl moves slots hl and hl + 16 (both rows read before either is written)
+        int nv[NS / 16], ov[NS / 16];
+#pragma unroll
+        for (int t = 0; t < NS / 16; ++t) {
+            const int e = hl + 16 * t;
+            nv[t] = -1;
+            ov[t] = -1;
+            if (live && diff && e < a.K) {
+                nv[t] = e < zn ? srow[e] : -1;
+                ov[t] = e < zo ? row[e] : -1;
+            }
         }
         __syncwarp();
-        if (mv) {
-            row[hl] = nv;
-            srow[hl] = ov;
+#pragma unroll
+        for (int t = 0; t < NS / 16; ++t) {
+            const int e = hl + 16 * t;
+            if (live && diff && e < a.K) {
+                row[e] = nv[t];
+                srow[e] = ov[t];
+            }
         }
         if (live && hl == 0) {
             if (a.held) a.held[c] = 0;
@@ -1109,25 +1123,26 @@ CG_D bool row_has_pair(const int *row, int z, int u, int v)
 
 // does the row of cell x contain u immediately followed (cyclically) by v? Rows of 16-byte aligned
 // capacity (K % 4 == 0) are read with independent 16-byte loads, so a lookup costs one memory latency.
+template <int NS = VG>
 CG_D bool pair_in_row(const VoroArgs &a, int x, int u, int v)
 {
     const int *row = a.nbr + (size_t)x * a.K;
     if ((a.K & 3) != 0) return row_has_pair(row, a.nn[x], u, v);
     int z = a.nn[x];
-    int e[VG + 1];
+    int e[NS + 1];
     const int4 *r4 = reinterpret_cast<const int4 *>(row);
 #pragma unroll
-    for (int j = 0; j < VG / 4; ++j) {
+    for (int j = 0; j < NS / 4; ++j) {
         int4 t = (4 * j < a.K) ? r4[j] : make_int4(-1, -1, -1, -1);
         e[4 * j] = t.x;
         e[4 * j + 1] = t.y;
         e[4 * j + 2] = t.z;
         e[4 * j + 3] = t.w;
     }
-    e[VG] = -1;
+    e[NS] = -1;
     bool found = false;
 #pragma unroll
-    for (int k = 0; k < VG; ++k)
+    for (int k = 0; k < NS; ++k)
         if (k < z && e[k] == u) found = (k + 1 < z ? e[k + 1] : e[0]) == v;
     return found;
 }
@@ -1136,10 +1151,10 @@ CG_D bool pair_in_row(const VoroArgs &a, int x, int u, int v)
 // triangle (c,a,b) of the row must appear in the rows of a and b, every dropped triangle must be
 // gone from them, and a changed row must pass the exact local test. Offending cells are queued for
 // the next round.
-template <int WPB>
+template <int WPB, int NS = VG>
 __global__ void __launch_bounds__(WPB * 32) k_check(VoroArgs a)
 {
-    __shared__ double2 sR[WPB * GPW][VG];
+    __shared__ double2 sR[WPB * GPW][NS];
     Ctl *ctl = a.ctl;
     if (ctl->halt) return;
     int round = ctl->round;
@@ -1173,9 +1188,11 @@ __global__ void __launch_bounds__(WPB * 32) k_check(VoroArgs a)
             Ly = in.Ly;
             pc = a.pos[c];
         }
-        int nb[2] = {-1, -1};
+        int nb[NS / G];
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
+        for (int r = 0; r < NS / G; ++r) nb[r] = -1;
+#pragma unroll
+        for (int r = 0; r < NS / G; ++r) {
             int k = gl + G * r;
             if (live && k < z) {
                 nb[r] = row[k];
@@ -1185,12 +1202,12 @@ __global__ void __launch_bounds__(WPB * 32) k_check(VoroArgs a)
         __syncwarp();
         bool bad = tested && z < 3;
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
+        for (int r = 0; r < NS / G; ++r) {
             int k = gl + G * r;
             if (live && k < z) {
                 int kp = k + 1 == z ? 0 : k + 1;
                 int u = nb[r], v = row[kp];
-                bool in_u = pair_in_row(a, u, v, c), in_v = pair_in_row(a, v, c, u);
+                bool in_u = pair_in_row<NS>(a, u, v, c), in_v = pair_in_row<NS>(a, v, c, u);
                 if (!in_u) claim_enqueue(a, u, e, nq);
                 if (!in_v) claim_enqueue(a, v, e, nq);
                 if (tested && z >= 3) {
@@ -1203,8 +1220,8 @@ __global__ void __launch_bounds__(WPB * 32) k_check(VoroArgs a)
             }
             if (tested && k < zo) {
                 int u = orow[k], v = orow[k + 1 == zo ? 0 : k + 1];
-                if (!pair_in_row(a, c, u, v)) {  // dropped triangle
-                    bool in_u = pair_in_row(a, u, v, c), in_v = pair_in_row(a, v, c, u);
+                if (!pair_in_row<NS>(a, c, u, v)) {  // dropped triangle
+                    bool in_u = pair_in_row<NS>(a, u, v, c), in_v = pair_in_row<NS>(a, v, c, u);
                     if (in_u) claim_enqueue(a, u, e, nq);
                     if (in_v) claim_enqueue(a, v, e, nq);
                 }
@@ -1214,7 +1231,7 @@ __global__ void __launch_bounds__(WPB * 32) k_check(VoroArgs a)
         if (bad) {
             if (gl == 0) claim_enqueue(a, c, e, nq);
 #pragma unroll
-            for (int r = 0; r < 2; ++r)
+            for (int r = 0; r < NS / G; ++r)
                 if (nb[r] >= 0) claim_enqueue(a, nb[r], e, nq);
         }
         __syncwarp();

@@ -173,15 +173,23 @@ class VoronoiBatch:
         return out
 
     def topology(self):
+        """(nn, nbr): row lengths and rows of K entries. K is the system's current row capacity,
+        which grows from 16 to 32 when a cell gets more than 16 neighbours."""
+        self.K = int(self._lib.cg_neighbor_capacity(self._h))
         nn = np.zeros(self.Ntot, np.int32)
         nbr = np.zeros((self.Ntot, self.K), np.int32)
         check(self._lib.cg_get_topology(self._h, ptr(nn), ptr(nbr)))
         return nn, nbr
 
     def set_topology(self, nn, nbr):
+        self.K = int(self._lib.cg_neighbor_capacity(self._h))
         nn = np.ascontiguousarray(nn, np.int32)
-        nbr = np.ascontiguousarray(nbr, np.int32).reshape(self.Ntot, self.K)
-        check(self._lib.cg_set_topology(self._h, ptr(nn), ptr(nbr)))
+        nbr = np.asarray(nbr, np.int32).reshape(self.Ntot, -1)
+        if nbr.shape[1] > self.K:
+            raise ValueError(f"rows of {nbr.shape[1]} entries exceed the capacity {self.K}")
+        rows = np.full((self.Ntot, self.K), -1, np.int32)
+        rows[:, :nbr.shape[1]] = nbr
+        check(self._lib.cg_set_topology(self._h, ptr(nn), ptr(rows)))
 
     def energies(self):
         out = np.zeros(len(self.N))

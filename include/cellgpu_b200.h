@@ -121,7 +121,9 @@ int cg_voronoi_triangulate_noalloc(const double *pos, int N, double Lx, double L
 typedef struct cg_system cg_system;
 
 /* Create a batch of n_inst Voronoi monolayers with N[i] cells in boxes (box[2i], box[2i+1]).
- * K is the neighbour-row capacity, at most 16 (>= max coordination + 1; 16 is ample for random points).
+ * K is the neighbour-row capacity, a multiple of 4 up to 32; 16 covers nearly every cell of random
+ * points. A cell with more than K neighbours makes the system widen its rows to 32 (the reference
+ * grows neighMax the same way); cg_neighbor_capacity reports the current K.
  * precision: CG_FP64 or CG_MIXED. */
 int cg_voronoi_create(int n_inst, const int *N, const double *box, int K, int precision,
                       cg_system **out);
@@ -156,7 +158,7 @@ int cg_set_directors(cg_system *sys, const double *theta);
 int cg_get_directors(cg_system *sys, double *theta);
 int cg_get_forces(cg_system *sys, double *F);                 /* per dof */
 int cg_get_area_perimeter(cg_system *sys, double *AP);        /* per cell */
-int cg_get_topology(cg_system *sys, int *nn, int *nbr);       /* Voronoi rows (N x K) */
+int cg_get_topology(cg_system *sys, int *nn, int *nbr);       /* Voronoi rows (N x cg_neighbor_capacity) */
 int cg_set_topology(cg_system *sys, const int *nn, const int *nbr);
 /* vertex model wiring (vertexModelBase arrays, inc/models/Simple2DCell.h:160-290): vn[3*Nv] vertex
  * neighbours, vcn[3*Nv] cells of each vertex, cvn[Nc] vertices per cell, cv[Nc*vmax] cell vertices
