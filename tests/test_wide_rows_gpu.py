@@ -101,3 +101,28 @@ def test_wide_rows_agree_with_narrow(cglib, torch):
     assert np.abs(out[1][1] - out[0][1]).max() < 1e-9
     assert np.array_equal(out[1][2], out[0][2])
     assert out[0][3] > 0 and out[1][3] > 0  # the repair ran in both forms
+
+
+def test_rows_grow_during_steps(cglib, oracle):
+    """The rows overflow inside a step: the system starts from rows that fit 16 (the Delaunay rows
+    of the same cells with the ringed cell elsewhere), the step's repair or rebuild meets the
+    18-neighbour cell, the system widens to 32 and the run continues to a Delaunay state (the
+    strong forces on the ringed cell soon pull its coordination back down)."""
+    from cellgpu_b200 import VoronoiBatch
+    pos, box = _flower()
+    N = len(pos)
+    p1 = pos.copy()
+    p1[0] = [1.3, 1.7]
+    nn1, nbr1 = oracle.periodic_delaunay(p1, box, 16)
+    b = VoronoiBatch([N], [box])
+    b.set_positions(pos)
+    b.set_directors(np.zeros(N))
+    b.set_motility(np.tile([0.02, 1.0], (N, 1)))
+    b.set_preferences(np.tile([1.0, 3.8], (N, 1)))
+    b.set_topology(nn1, nbr1)
+    b.spp_run(3, dt=0.01)
+    assert b._lib.cg_neighbor_capacity(b.handle) == 32
+    b.enforce_topology()
+    nn, nbr = b.topology()
+    onn, onbr = oracle.periodic_delaunay(b.positions(), box, 32)
+    assert np.array_equal(_canon(nn, nbr), _canon(onn, onbr))
