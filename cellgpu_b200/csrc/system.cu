@@ -758,7 +758,7 @@ static void launch_round_ns(const VoroArgs &a, bool forces, cudaStream_t st, uns
     constexpr int WPB = 4;
     // commit / check: 8 queue slots per 64-thread block, so a short queue still spreads over the SMs
     constexpr int WPB_C = 2;
-    k_star_local<WPB><<<148 * 4, WPB * 32, 0, st>>>(a);
+    k_star_local<WPB><<<148 * STAR_MINB, WPB * 32, 0, st>>>(a);
     if (forces)
         k_commit<R, true, WPB_C, NS><<<148 * 8, WPB_C * 32, 0, st>>>(a);
     else

@@ -909,6 +909,7 @@ CG_D int warp_remove(int *cand, int m, int self, int lane)
 // two at a time (16 lanes each, rows hold at most 16 entries), and candidates are deduplicated in a
 // per-warp open-addressing table in shared memory, so collecting a ring costs a few parallel loads.
 constexpr int CAND_HASH = 512;  // > CAND_LOCAL + 32: the table never fills
+constexpr int STAR_MINB = 5;    // resident blocks of k_star_local per SM (its grid is one such wave)
 
 CG_D void cand_insert(int *table, int *list, int *count, int v)
 {
@@ -926,7 +927,7 @@ CG_D void cand_insert(int *table, int *list, int *count, int v)
 }
 
 template <int WPB>
-__global__ void __launch_bounds__(WPB * 32) k_star_local(VoroArgs a)
+__global__ void __launch_bounds__(WPB * 32, STAR_MINB) k_star_local(VoroArgs a)
 {
     __shared__ int s_cand[WPB][CAND_LOCAL];
     __shared__ double2 s_rel[WPB][CAND_LOCAL];
