@@ -246,6 +246,7 @@ struct cg_system {
     std::vector<GraphEntry> graphs;
     long long kernels_enqueued = 0;  // kernels of this library launched for this system
     double *noise_buf = nullptr;     // staging for host-supplied noise (one step)
+    double *draw_buf = nullptr;      // device normals of the step, drawn beside the repair rounds
     // asynchronous host-buffer steps: copy stream, a second staging buffer, per-buffer events
     cudaStream_t copy_stream = nullptr;
     double *noise_buf2 = nullptr;
@@ -384,7 +385,8 @@ static size_t voronoi_bytes(int N, int K, int n_bins, int n_inst, int precision)
     size_t real2 = precision == CG_FP64 ? 16 : 8;
     size_t per_cell = 4 /*cell_inst*/ + 4 /*held*/ + 4 /*undec*/ + 16 * 3 /*pos, motility, APpref*/ + 8 /*theta*/ + 2 * real2 +
                       4 + 4 * (size_t)K /*nn, nbr*/ + 4 /*mark*/ + 4 * (R_MAX + 1) /*queue*/ + 4 +
-                      4 * (size_t)K /*stage*/ + 4 * R_MAX /*changed*/ + 4 * 3 + 16 /*cell list*/;
+                      4 * (size_t)K /*stage*/ + 4 * R_MAX /*changed*/ + 4 * 3 + 16 /*cell list*/ +
+                      8 + 8 /*noise staging, device draw*/;
     return per_cell * (size_t)N + (size_t)n_bins * 8 + (size_t)n_inst * (sizeof(Inst) + 16) + 4096;
 }
 
@@ -463,6 +465,7 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
         if ((st = dalloc(s, &s->d_zsum, n_inst))) break;
         if ((st = dalloc(s, &s->d_energy, n_inst))) break;
         if ((st = dalloc(s, &s->noise_buf, Nt))) break;
+        if ((st = dalloc(s, &s->draw_buf, Nt))) break;
         size_t tmpb = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, tmpb, s->bin_count, s->bin_start, s->n_bins + 1);
         s->scan_tmp_bytes = tmpb;
@@ -983,14 +986,29 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
         cp.conditional.size = 1;
         cudaGraphNode_t cn;
         CG_CUDA(cudaGraphAddNode(&cn, graph, deps.data(), deps.size(), &cp));
+        // device noise: drawn by a kernel node beside the WHILE node, read by k_spp
+        cudaGraphNode_t dn = nullptr;
+        if (!noise) {
+            double *out = s->draw_buf;
+            void *args[] = {&a, &out};
+            cudaKernelNodeParams kp;
+            memset(&kp, 0, sizeof(kp));
+            kp.func = (void *)k_draw_noise;
+            kp.gridDim = dim3(nblk((s->N + 1) / 2, SPP_BLOCK));
+            kp.blockDim = dim3(SPP_BLOCK);
+            kp.kernelParams = args;
+            CG_CUDA(cudaGraphAddKernelNode(&dn, graph, deps.data(), deps.size(), &kp));
+            s->kernels_enqueued += 1;
+        }
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         CG_CUDA(cudaStreamBeginCaptureToGraph(s->body_stream, body, nullptr, nullptr, 0, mode));
         launch_round<R>(s, a, true, s->body_stream, (unsigned long long)h, 1);  // counted on the device
         cudaGraph_t gb;
         CG_CUDA(cudaStreamEndCapture(s->body_stream, &gb));
         deps.assign(1, cn);
+        if (dn) deps.push_back(dn);
         CG_CUDA(cudaStreamBeginCaptureToGraph(s->stream, graph, deps.data(), nullptr, deps.size(), mode));
-        const double *nz = noise;
+        const double *nz = noise ? noise : s->draw_buf;
         k_spp<R><<<nblk((s->N + 1) / 2, SPP_BLOCK), SPP_BLOCK, 0, s->stream>>>(a, nz, dt, mu, 0u, 0);
         k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
         s->kernels_enqueued += 2;

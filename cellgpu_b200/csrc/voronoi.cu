@@ -1425,6 +1425,39 @@ CG_D double2 cell_pair_noise(const VoroArgs &a, int c, uint32_t step, int &local
 // Two cells per thread: one Box-Muller pair serves both when they are consecutive cells of one
 // instance (the usual case) and the noise is generated on the device. step0 is the step counter
 // when there is no control block (raw caller).
+// the device normals of cells c0 and c0 + 1 at a step: one Box-Muller pair serves both when they
+// are consecutive cells of one instance with c0 at an even local index, else each takes its own
+CG_D double2 pair_draw(const VoroArgs &a, int c0, uint32_t step)
+{
+    const bool two = c0 + 1 < a.N;
+    int l0, l1;
+    double2 g0 = cell_pair_noise(a, c0, step, l0), xi;
+    xi.x = (l0 & 1) ? g0.y : g0.x;
+    xi.y = 0.0;
+    if (two) {
+        const Inst &i0 = inst_of(a, c0);
+        if (!(l0 & 1) && c0 + 1 < i0.off + i0.n) {
+            xi.y = g0.y;
+        } else {
+            double2 g1 = cell_pair_noise(a, c0 + 1, step, l1);
+            xi.y = (l1 & 1) ? g1.y : g1.x;
+        }
+    }
+    return xi;
+}
+
+// The same normals for every cell of the current step, into out[N]. The step graph runs this
+// beside the repair rounds (which leave most of the GPU idle), so k_spp reads them instead of
+// drawing them on the step's critical path; the values are the ones k_spp would draw.
+__global__ void k_draw_noise(VoroArgs a, double *out)
+{
+    const int c0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (c0 >= a.N) return;
+    const double2 xi = pair_draw(a, c0, (uint32_t)a.ctl->step);
+    out[c0] = xi.x;
+    if (c0 + 1 < a.N) out[c0 + 1] = xi.y;
+}
+
 template <typename R>
 __global__ void k_spp(VoroArgs a, const double *noise, double dt, double mu, uint32_t step0,
                       int zero_force)
@@ -1436,24 +1469,8 @@ __global__ void k_spp(VoroArgs a, const double *noise, double dt, double mu, uin
     if (c0 >= a.N) return;
     bool two = c0 + 1 < a.N;
     double2 xi;
-    if (noise) {
-        xi = make_double2(noise[c0], two ? noise[c0 + 1] : 0.0);
-    } else {
-        uint32_t step = ctl ? (uint32_t)ctl->step : step0;
-        int l0, l1;
-        double2 g0 = cell_pair_noise(a, c0, step, l0);
-        xi.x = (l0 & 1) ? g0.y : g0.x;
-        xi.y = 0.0;
-        if (two) {
-            const Inst &i0 = inst_of(a, c0);
-            if (!(l0 & 1) && c0 + 1 < i0.off + i0.n) {
-                xi.y = g0.y;
-            } else {
-                double2 g1 = cell_pair_noise(a, c0 + 1, step, l1);
-                xi.y = (l1 & 1) ? g1.y : g1.x;
-            }
-        }
-    }
+    if (noise) xi = make_double2(noise[c0], two ? noise[c0 + 1] : 0.0);
+    else xi = pair_draw(a, c0, ctl ? (uint32_t)ctl->step : step0);
     spp_cell<R>(a, c0, xi.x, dt, mu, zero_force);
     if (two) spp_cell<R>(a, c0 + 1, xi.y, dt, mu, zero_force);
 }
