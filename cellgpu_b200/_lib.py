@@ -64,6 +64,8 @@ SIGNATURES = {
     "cg_compute_forces": (_i, [_vp]),
     "cg_enforce_topology": (_i, [_vp]),
     "cg_set_seed": (_i, [_vp, _u64]),
+    "cg_set_deterministic": (_i, [_vp, _i]),
+    "cg_get_deterministic": (_i, [_vp]),
     "cg_set_instance_seeds": (_i, [_vp, _vp]),
     "cg_spp_run": (_i, [_vp, _i, _d, _d, _vp]),
     "cg_counters": (_i, [_vp, C.POINTER(C.c_longlong), _i]),

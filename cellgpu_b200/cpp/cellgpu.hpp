@@ -77,6 +77,8 @@ public:
 
     cg_system *handle() const { return sys_; }
     virtual bool isVertexModel() const = 0;
+    // order-independent (fixed-point) force sums: bit-identical forces and trajectories on reruns
+    void setDeterministic(bool on) { check(cg_set_deterministic(sys_, on ? 1 : 0)); }
     virtual int getNumberOfDegreesOfFreedom() { return cg_num_dofs(sys_); }
     int getNumberOfCells() const { return Ncells; }
 
@@ -425,7 +427,11 @@ private:
 // ---- Simulation (inc/Simulation.h:18-87; performTimestep, src/Simulation.cpp:141-166) -------
 class Simulation {
 public:
-    void setConfiguration(std::shared_ptr<Simple2DModel> config) { configuration = std::move(config); }
+    void setConfiguration(std::shared_ptr<Simple2DModel> config)
+    {
+        configuration = std::move(config);
+        if (configuration && reproducible) configuration->setDeterministic(true);
+    }
     void addUpdater(std::shared_ptr<updater> upd) { addUpdater(std::move(upd), configuration); }
     void addUpdater(std::shared_ptr<updater> upd, std::shared_ptr<Simple2DModel> config)
     {
@@ -443,7 +449,13 @@ public:
     {
         if (setcpu) throw Error(CG_ERR_ARG, "cellgpu_b200 runs on the GPU only");
     }
-    void setReproducible(bool) {}
+    // Reproducible runs (Simulation::setReproducible): besides fixed seeds, the configuration sums
+    // its forces in an order-independent way, so reruns give bit-identical trajectories.
+    void setReproducible(bool r)
+    {
+        reproducible = r;
+        if (configuration) configuration->setDeterministic(r);
+    }
     // re-sort the (Voronoi) configuration spatially every sp steps (src/Simulation.cpp:154-164)
     void setSortPeriod(int sp) { sortPeriod = sp; }
     void setCurrentTime(Dscalar t) { Time = t; }
@@ -473,6 +485,7 @@ public:
 private:
     std::shared_ptr<Simple2DModel> configuration;
     std::vector<std::shared_ptr<updater>> updaters;
+    bool reproducible = false;
 };
 
 using SimulationPtr = std::shared_ptr<Simulation>;

@@ -16,6 +16,8 @@ struct FireInst {
     int n_since, iterations, converged, ndof;
 };
 
+constexpr int FIRE_BLOCK = 256;  // threads (= dofs) per block of the per-dof FIRE kernels
+
 struct FireArgs {
     int ndof, n_inst;
     const Inst *inst;
@@ -23,6 +25,9 @@ struct FireArgs {
     double2 *pos, *vel;
     const double2 *F;
     FireInst *st;
+    // deterministic mode: (power, |F|^2, |v|^2) of every FIRE_BLOCK-dof block that lies inside one
+    // instance, summed per instance in a fixed order by k_fire_reduce; null: atomic sums
+    double *part;
     cg_fire_params prm;
     const Ctl *ctl;  // a halted step (pending global rebuild) freezes the iteration
 };
@@ -104,9 +109,15 @@ __global__ void __launch_bounds__(256) k_fire_vv2(FireArgs a)
                 tv += s_red[2][k];
                 tm = fmax(tm, s_red[3][k]);
             }
-            atomicAdd(&a.st[b0].power, tp);
-            atomicAdd(&a.st[b0].fnorm, tf);
-            atomicAdd(&a.st[b0].vnorm, tv);
+            if (a.part) {
+                a.part[3 * (size_t)blockIdx.x] = tp;
+                a.part[3 * (size_t)blockIdx.x + 1] = tf;
+                a.part[3 * (size_t)blockIdx.x + 2] = tv;
+            } else {
+                atomicAdd(&a.st[b0].power, tp);
+                atomicAdd(&a.st[b0].fnorm, tf);
+                atomicAdd(&a.st[b0].vnorm, tv);
+            }
             atomicMax(&a.st[b0].fmax_bits, (unsigned long long)__double_as_longlong(tm));
         }
         return;
@@ -122,16 +133,78 @@ __global__ void __launch_bounds__(256) k_fire_vv2(FireArgs a)
             fm = fmax(fm, __shfl_down_sync(full, fm, off));
         }
         if (lane == 0 && inst >= 0) {
-            atomicAdd(&a.st[inst].power, P);
-            atomicAdd(&a.st[inst].fnorm, ff);
-            atomicAdd(&a.st[inst].vnorm, vv);
+            if (!a.part) {  // (the deterministic mode sums these dofs in k_fire_reduce)
+                atomicAdd(&a.st[inst].power, P);
+                atomicAdd(&a.st[inst].fnorm, ff);
+                atomicAdd(&a.st[inst].vnorm, vv);
+            }
             atomicMax(&a.st[inst].fmax_bits, (unsigned long long)__double_as_longlong(fm));
         }
     } else if (inst >= 0) {
-        atomicAdd(&a.st[inst].power, P);
-        atomicAdd(&a.st[inst].fnorm, ff);
-        atomicAdd(&a.st[inst].vnorm, vv);
+        if (!a.part) {
+            atomicAdd(&a.st[inst].power, P);
+            atomicAdd(&a.st[inst].fnorm, ff);
+            atomicAdd(&a.st[inst].vnorm, vv);
+        }
         atomicMax(&a.st[inst].fmax_bits, (unsigned long long)__double_as_longlong(fm));
+    }
+}
+
+// Deterministic mode: the power and norm sums of every unconverged instance (one block per
+// instance), in an order fixed by the instance's dof range alone: the partial sums that k_fire_vv2
+// left for the instance's whole blocks, then its dofs in blocks shared with another instance (or in
+// the array's last, short block), recomputed from F and the half-kicked v. Each thread's share and
+// the tree that joins the shares are fixed, so the sums are bit-identical on every run.
+__global__ void __launch_bounds__(FIRE_BLOCK) k_fire_reduce(FireArgs a)
+{
+    __shared__ double s_red[3][FIRE_BLOCK / 32];
+    if (a.ctl && a.ctl->halt) return;  // uniform across the grid
+    FireInst &st = a.st[blockIdx.x];
+    if (st.converged) return;          // uniform across the block
+    const Inst &in = a.inst[blockIdx.x];
+    const int o = in.nv > 0 ? in.voff : in.off, n = in.nv > 0 ? in.nv : in.n;
+    const int bf = (o + FIRE_BLOCK - 1) / FIRE_BLOCK, bl = (o + n) / FIRE_BLOCK;  // whole blocks [bf, bl)
+    const int nb = max(bl - bf, 0);
+    const int lo_end = min(o + n, bf * FIRE_BLOCK), hi_start = max(lo_end, bl * FIRE_BLOCK);
+    const int nlo = lo_end - o, nhi = o + n - hi_start;
+    double P = 0, ff = 0, vv = 0;
+    for (int k = threadIdx.x; k < nb + nlo + nhi; k += blockDim.x) {
+        if (k < nb) {
+            const double *q = a.part + 3 * (size_t)(bf + k);
+            P += q[0];
+            ff += q[1];
+            vv += q[2];
+        } else {
+            const int i = k - nb < nlo ? o + (k - nb) : hi_start + (k - nb - nlo);
+            const double2 v = a.vel[i], f = a.F[i];
+            P += f.x * v.x + f.y * v.y;
+            ff += f.x * f.x + f.y * f.y;
+            vv += v.x * v.x + v.y * v.y;
+        }
+    }
+    const unsigned full = 0xffffffffu;
+    for (int off = 16; off > 0; off >>= 1) {
+        P += __shfl_down_sync(full, P, off);
+        ff += __shfl_down_sync(full, ff, off);
+        vv += __shfl_down_sync(full, vv, off);
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_red[0][w] = P;
+        s_red[1][w] = ff;
+        s_red[2][w] = vv;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tp = 0, tf = 0, tv = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            tp += s_red[0][k];
+            tf += s_red[1][k];
+            tv += s_red[2][k];
+        }
+        st.power = tp;
+        st.fnorm = tf;
+        st.vnorm = tv;
     }
 }
 

@@ -8,6 +8,7 @@ static int fire_alloc(cg_system *s)
     CG_TRY(dalloc(s, &fs, s->n_inst));
     s->fire_st = fs;
     CG_TRY(dalloc(s, &s->fire_dofinst, ndof(s)));
+    CG_TRY(dalloc(s, &s->fire_part, 3 * (size_t)nblk(ndof(s), FIRE_BLOCK)));
     if (s->model == CG_MODEL_VORONOI) {
         CG_CUDA(cudaMemcpyAsync(s->fire_dofinst, s->cell_inst, sizeof(int) * s->N, cudaMemcpyDeviceToDevice,
                                 s->stream));
@@ -30,6 +31,7 @@ static FireArgs fire_args(cg_system *s, const cg_fire_params &prm)
     a.vel = s->fire_vel;
     a.F = reinterpret_cast<const double2 *>(s->F);
     a.st = reinterpret_cast<FireInst *>(s->fire_st);
+    a.part = s->det ? s->fire_part : nullptr;
     a.prm = prm;
     a.ctl = s->ctl;
     return a;
@@ -42,10 +44,16 @@ static void fire_forces(cg_system *s, bool test_and_repair)
         VoroArgs a = sys_args(s);
         if (s->precision == CG_FP64) {
             launch_force_test<double>(s, a, test_and_repair);
-            if (test_and_repair) launch_repair<double>(s, a, true);
+            if (test_and_repair)
+                launch_repair<double>(s, a, true);
+            else
+                finish_forces<double>(s, a, s->stream);
         } else {
             launch_force_test<float>(s, a, test_and_repair);
-            if (test_and_repair) launch_repair<float>(s, a, true);
+            if (test_and_repair)
+                launch_repair<float>(s, a, true);
+            else
+                finish_forces<float>(s, a, s->stream);
         }
         if (test_and_repair) {
             k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 0);
@@ -54,8 +62,18 @@ static void fire_forces(cg_system *s, bool test_and_repair)
     } else {
         VertArgs a = vm_args(s);
         if (test_and_repair) vm_launch_t1(s, a);
-        cudaMemsetAsync(s->F, 0, sizeof(double2) * s->Nv, s->stream);
         launch_vm_forces(s, a);
+        s->kernels_enqueued += 1;
+    }
+}
+
+// second half-kick and the per-instance power / norm sums (in a fixed order in the deterministic mode)
+static void fire_vv2_reduce(cg_system *s, const FireArgs &f)
+{
+    k_fire_vv2<<<nblk(ndof(s), FIRE_BLOCK), FIRE_BLOCK, 0, s->stream>>>(f);
+    s->kernels_enqueued += 1;
+    if (f.part) {
+        k_fire_reduce<<<s->n_inst, FIRE_BLOCK, 0, s->stream>>>(f);
         s->kernels_enqueued += 1;
     }
 }
@@ -67,10 +85,10 @@ static void fire_enqueue_iteration(cg_system *s, const cg_fire_params &prm)
     int nd = ndof(s);
     k_fire_vv1<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
     fire_forces(s, true);
-    k_fire_vv2<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
+    fire_vv2_reduce(s, f);
     k_fire_mix<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
     k_fire_update<<<nblk(s->n_inst, 64), 64, 0, s->stream>>>(f, &s->ctl->counters[6]);
-    s->kernels_enqueued += 4;
+    s->kernels_enqueued += 3;
 }
 
 extern "C" int cg_fire_minimize(cg_system *s, const cg_fire_params *prm)
@@ -122,7 +140,7 @@ extern "C" int cg_fire_minimize(cg_system *s, const cg_fire_params *prm)
             CG_TRY(recover(s));
             fire_forces(s, false);
             int nd = ndof(s);
-            k_fire_vv2<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
+            fire_vv2_reduce(s, f);
             k_fire_mix<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
             k_fire_update<<<nblk(s->n_inst, 64), 64, 0, s->stream>>>(f, &s->ctl->counters[6]);
             CG_TRY(check_launch());

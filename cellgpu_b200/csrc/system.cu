@@ -247,6 +247,10 @@ struct cg_system {
     long long kernels_enqueued = 0;  // kernels of this library launched for this system
     double *noise_buf = nullptr;     // staging for host-supplied noise (one step)
     double *draw_buf = nullptr;      // device normals of the step, drawn beside the repair rounds
+    // deterministic force sums (cg_set_deterministic): fixed-point accumulator, 4 words per cell
+    int det = 0;
+    unsigned long long *Ffix = nullptr;
+    unsigned long long *Efix = nullptr;  // fixed-point energy sums, 2 words per instance
     // asynchronous host-buffer steps: copy stream, a second staging buffer, per-buffer events
     cudaStream_t copy_stream = nullptr;
     double *noise_buf2 = nullptr;
@@ -279,6 +283,7 @@ struct cg_system {
     double2 *fire_vel = nullptr;
     void *fire_st = nullptr;
     int *fire_dofinst = nullptr;
+    double *fire_part = nullptr;  // per-block partial sums of the deterministic FIRE reductions
 };
 
 static void release_graph(cg_system::GraphEntry &g)
@@ -354,6 +359,7 @@ static VoroArgs sys_args(cg_system *s)
     a.KP = s->KP;
     a.AP = s->AP;
     a.F = s->F;
+    a.Ffix = s->det ? s->Ffix : nullptr;
     a.nn = s->nn;
     a.nbr = s->nbr;
     a.mark = s->mark;
@@ -746,12 +752,24 @@ extern "C" int cg_voronoi_triangulate(const double *pos, int N, double Lx, doubl
 template <typename R>
 static void launch_force_test(cg_system *s, const VoroArgs &a, bool test)
 {
-    cudaMemsetAsync(s->F, 0, (s->precision == CG_FP64 ? sizeof(double2) : sizeof(float2)) * s->N,
-                    s->stream);
+    if (a.Ffix)
+        cudaMemsetAsync(a.Ffix, 0, 4 * sizeof(unsigned long long) * s->N, s->stream);
+    else
+        cudaMemsetAsync(s->F, 0, (s->precision == CG_FP64 ? sizeof(double2) : sizeof(float2)) * s->N,
+                        s->stream);
     if (test)
         launch_groups<R, true, true>(a, s->N, s->stream, s->tune_force);
     else
         launch_groups<R, true, false>(a, s->N, s->stream, s->tune_force);
+    s->kernels_enqueued += 1;
+}
+
+// deterministic mode: F from the fixed-point sums, once the force pass (and repair) is complete
+template <typename R>
+static void finish_forces(cg_system *s, const VoroArgs &a, cudaStream_t st)
+{
+    if (!a.Ffix) return;
+    k_fix_forces<R><<<nblk(s->N, 256), 256, 0, st>>>(a);
     s->kernels_enqueued += 1;
 }
 
@@ -797,6 +815,7 @@ static void launch_repair(cg_system *s, const VoroArgs &a, bool forces)
     launch_repair_begin<R>(a, s->stream, 0ull, 0, forces ? 1 : 0);
     for (int r = 0; r < R_MAX; ++r) launch_round<R>(s, a, forces, s->stream, 0ull, 0);
     s->kernels_enqueued += 1;
+    if (forces) finish_forces<R>(s, a, s->stream);
 }
 
 static int read_ctl(cg_system *s, Ctl &c) { return d2h(s, &c, s->ctl, sizeof(Ctl)); }
@@ -865,6 +884,7 @@ static int compute_forces_t(cg_system *s)
 {
     VoroArgs a = sys_args(s);
     launch_force_test<R>(s, a, false);
+    finish_forces<R>(s, a, s->stream);
     return check_launch();
 }
 
@@ -1009,6 +1029,7 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
         if (dn) deps.push_back(dn);
         CG_CUDA(cudaStreamBeginCaptureToGraph(s->stream, graph, deps.data(), nullptr, deps.size(), mode));
         const double *nz = noise ? noise : s->draw_buf;
+        finish_forces<R>(s, a, s->stream);
         k_spp<R><<<nblk((s->N + 1) / 2, SPP_BLOCK), SPP_BLOCK, 0, s->stream>>>(a, nz, dt, mu, 0u, 0);
         k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
         s->kernels_enqueued += 2;
@@ -1096,6 +1117,24 @@ extern "C" int cg_spp_enqueue(cg_system *s, int n_steps, double dt, double mu)
                                    : enqueue_graph<float>(s, n_steps, dt, mu, nullptr);
 }
 
+// per-instance energies into d_energy, enqueued (the deterministic mode sums in fixed point)
+static int enqueue_energies(cg_system *s)
+{
+    VoroArgs a = sys_args(s);  // N = cells: A/P and preferences are per cell in both models
+    unsigned long long *efix = a.Ffix ? s->Efix : nullptr;
+    if (!efix) CG_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * s->n_inst, s->stream));
+    if (s->precision == CG_FP64)
+        k_energy<double><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy, efix);
+    else
+        k_energy<float><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy, efix);
+    s->kernels_enqueued += 1;
+    if (efix) {
+        k_energy_from_fix<<<nblk(s->n_inst, 256), 256, 0, s->stream>>>(s->n_inst, efix, s->d_energy);
+        s->kernels_enqueued += 1;
+    }
+    return CG_OK;
+}
+
 // one step with host-supplied noise (copied in) and the per-instance energies copied out
 extern "C" int cg_spp_step_host(cg_system *s, const double *host_noise, double dt, double mu,
                                 double *host_energy)
@@ -1107,13 +1146,7 @@ extern "C" int cg_spp_step_host(cg_system *s, const double *host_noise, double d
     int st = s->precision == CG_FP64 ? enqueue_graph<double>(s, 1, dt, mu, s->noise_buf)
                                      : enqueue_graph<float>(s, 1, dt, mu, s->noise_buf);
     if (st) return st;
-    VoroArgs a = sys_args(s);
-    CG_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * s->n_inst, s->stream));
-    if (s->precision == CG_FP64)
-        k_energy<double><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
-    else
-        k_energy<float><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
-    s->kernels_enqueued += 1;
+    CG_TRY(enqueue_energies(s));
     if (host_energy)
         CG_CUDA(cudaMemcpyAsync(host_energy, s->d_energy, sizeof(double) * s->n_inst, cudaMemcpyDeviceToHost,
                                 s->stream));
@@ -1134,7 +1167,7 @@ template <typename R>
 static int enqueue_energy_graph(cg_system *s, double dt, double mu, const double *noise, double *dst)
 {
     if (!s->e2e_acc) {
-        CG_TRY(dalloc(s, &s->e2e_acc, s->n_inst));  // zeroed; the kernel leaves it zeroed
+        CG_TRY(dalloc(s, &s->e2e_acc, 2 * (size_t)s->n_inst));  // zeroed; the kernel leaves it zeroed
         CG_TRY(dalloc(s, &s->e2e_done, 1));
     }
     for (auto &g : s->graphs)
@@ -1210,13 +1243,7 @@ extern "C" int cg_spp_enqueue_host(cg_system *s, const double *host_noise, doubl
     if (st) return st;
     CG_CUDA(cudaEventRecord(s->ev_consumed[slot], s->stream));
     if (host_energy && !edst) {
-        VoroArgs a = sys_args(s);
-        CG_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * s->n_inst, s->stream));
-        if (s->precision == CG_FP64)
-            k_energy<double><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
-        else
-            k_energy<float><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
-        s->kernels_enqueued += 1;
+        CG_TRY(enqueue_energies(s));
         CG_CUDA(cudaMemcpyAsync(host_energy, s->d_energy, sizeof(double) * s->n_inst, cudaMemcpyDeviceToHost,
                                 s->stream));
     }
@@ -1241,10 +1268,13 @@ extern "C" int cg_launch_force_pass(cg_system *s, int with_test)
     if (!s || s->model != CG_MODEL_VORONOI) return set_err(CG_ERR_ARG, "bad args");
     VoroArgs a = sys_args(s);
     a.undec = nullptr;  // no repair follows: undecided slots count as failing edges
-    if (s->precision == CG_FP64)
+    if (s->precision == CG_FP64) {
         launch_force_test<double>(s, a, with_test != 0);
-    else
+        finish_forces<double>(s, a, s->stream);
+    } else {
         launch_force_test<float>(s, a, with_test != 0);
+        finish_forces<float>(s, a, s->stream);
+    }
     return check_launch();
 }
 
@@ -1269,15 +1299,35 @@ extern "C" int cg_spp_run(cg_system *s, int n_steps, double dt, double mu, const
 extern "C" int cg_get_energies(cg_system *s, double *E)
 {
     if (!s || !E) return set_err(CG_ERR_ARG, "bad args");
-    VoroArgs a = sys_args(s);  // N = cells: A/P and preferences are per cell in both models
-    CG_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * s->n_inst, s->stream));
-    if (s->precision == CG_FP64)
-        k_energy<double><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
-    else
-        k_energy<float><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->d_energy);
+    CG_TRY(enqueue_energies(s));
     CG_TRY(check_launch());
     return d2h(s, E, s->d_energy, sizeof(double) * s->n_inst);
 }
+
+// Deterministic force sums. Off: forces are summed with floating-point atomics, whose order (and
+// so the last bits of F, which a chaotic trajectory amplifies) varies from run to run. On: every
+// contribution is added to a per-cell (Voronoi) or per-vertex (vertex model) fixed-point
+// accumulator with integer atomics and F is converted from it once per force evaluation, so the
+// same inputs give bit-identical forces and trajectories on every run (the reference's kernels sum
+// each cell's force sets in a fixed order, src/models/voronoiQuadraticEnergy.cu:30-54). Costs
+// 32 bytes per cell (or vertex) and one conversion kernel per force evaluation.
+extern "C" int cg_set_deterministic(cg_system *s, int on)
+{
+    if (!s) return set_err(CG_ERR_ARG, "null system");
+    on = on ? 1 : 0;
+    if (on == s->det) return CG_OK;
+    if (on && !s->Ffix) {
+        CG_TRY(dalloc(s, &s->Ffix, 4 * (size_t)ndof(s)));
+        CG_TRY(dalloc(s, &s->Efix, 2 * (size_t)s->n_inst));
+    }
+    CG_CUDA(cudaStreamSynchronize(s->stream));
+    for (auto &g : s->graphs) release_graph(g);  // graphs captured the accumulation mode
+    s->graphs.clear();
+    s->det = on;
+    return CG_OK;
+}
+
+extern "C" int cg_get_deterministic(cg_system *s) { return s ? s->det : 0; }
 
 // allocation-free triangulation (file-scope device scratch)
 #include "noalloc.cu"

@@ -14,6 +14,7 @@ struct VertArgs {
     const int *cell_inst, *vert_inst;
     double2 *vpos;
     double2 *F;
+    unsigned long long *Ffix;  // null, or 4 words per vertex: fixed-point sums of F (fix_add1)
     double2 *AP;
     const double2 *APpref;
     double KA, KP;
@@ -59,6 +60,28 @@ CG_D double vm_edge_weight(const VertArgs &a, int c, int v, int w)
 // vnext, KA(A-A0), KP(P-P0)) (inc/utility/functions.h:330-354) -- added directly to the vertex's
 // force, which is the sum of its three sets (src/models/vertexQuadraticEnergy.cpp:100-112).
 // ------------------------------------------------------------------------------------------
+// add a force set to vertex v (the deterministic mode sums in fixed point, in any order exactly)
+CG_D void vm_add_force(double2 *F, unsigned long long *Ffix, int v, double fx, double fy)
+{
+    if (Ffix) {
+        fix_add1(Ffix + 4 * (size_t)v, fx);
+        fix_add1(Ffix + 4 * (size_t)v + 2, fy);
+    } else {
+        atomicAdd(&F[v].x, fx);
+        atomicAdd(&F[v].y, fy);
+    }
+}
+
+// deterministic mode: F of every vertex from its fixed-point sums
+__global__ void k_vm_fix_forces(VertArgs a)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= a.Nv) return;
+    const ulonglong2 *w = reinterpret_cast<const ulonglong2 *>(a.Ffix) + 2 * (size_t)v;
+    const ulonglong2 fx = w[0], fy = w[1];
+    a.F[v] = make_double2(fix_value(fx.x, fx.y), fix_value(fy.x, fy.y));
+}
+
 __global__ void k_vm_forces(VertArgs a, int scatter)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -100,8 +123,7 @@ __global__ void k_vm_forces(VertArgs a, int scatter)
             fy -= wt * ny / nnm;
             te += wt * nnm;
         }
-        atomicAdd(&a.F[vidx].x, fx);
-        atomicAdd(&a.F[vidx].y, fy);
+        vm_add_force(a.F, a.Ffix, vidx, fx, fy);
         vlast = vcur;
         vcur = vnext;
         vidx = nv;
@@ -197,8 +219,7 @@ __global__ void __launch_bounds__(WPB * 32) k_vm_forces_groups(VertArgs a, int s
                 fy -= wt * ny / nnm;
                 te += wt * nnm;
             }
-            atomicAdd(&a.F[vid[r]].x, fx);
-            atomicAdd(&a.F[vid[r]].y, fy);
+            vm_add_force(a.F, a.Ffix, vid[r], fx, fy);
         }
     }
     if (a.tension_mode) {

@@ -13,6 +13,7 @@ static VertArgs vm_args(cg_system *s)
     a.vert_inst = s->vert_inst;
     a.vpos = s->pos;
     a.F = reinterpret_cast<double2 *>(s->F);
+    a.Ffix = s->det ? s->Ffix : nullptr;
     a.AP = reinterpret_cast<double2 *>(s->AP);
     a.APpref = s->APpref;
     a.KA = s->KA;
@@ -36,13 +37,22 @@ static VertArgs vm_args(cg_system *s)
     return a;
 }
 
-// forces + geometry of every cell: 8 lanes per cell for rows up to 32 vertices, else a thread per cell
+// forces + geometry of every cell (F zeroed first): 8 lanes per cell for rows up to 32 vertices,
+// else a thread per cell; the deterministic mode then converts its fixed-point sums into F
 static void launch_vm_forces(cg_system *s, const VertArgs &a)
 {
+    if (a.Ffix)
+        cudaMemsetAsync(a.Ffix, 0, 4 * sizeof(unsigned long long) * s->Nv, s->stream);
+    else
+        cudaMemsetAsync(s->F, 0, sizeof(double2) * s->Nv, s->stream);
     if (s->vmax <= VM_ROW_G)
         k_vm_forces_groups<4><<<nblk(s->N, 4 * (32 / VM_G)), 128, 0, s->stream>>>(a, 1);
     else
         k_vm_forces<<<nblk(s->N, 128), 128, 0, s->stream>>>(a, 1);
+    if (a.Ffix) {
+        k_vm_fix_forces<<<nblk(s->Nv, 256), 256, 0, s->stream>>>(a);
+        s->kernels_enqueued += 1;
+    }
 }
 
 static size_t vertex_bytes(long long Nc, int vmax, int n_inst)
@@ -249,7 +259,6 @@ static int vm_compute_forces(cg_system *s)
 {
     if (!s->topology_valid) return set_err(CG_ERR_STATE, "vertex topology not set");
     VertArgs a = vm_args(s);
-    CG_CUDA(cudaMemsetAsync(s->F, 0, sizeof(double2) * s->Nv, s->stream));
     launch_vm_forces(s, a);
     s->kernels_enqueued += 1;
     CG_TRY(check_launch());
@@ -287,7 +296,6 @@ static void vm_enqueue_step(cg_system *s, int kind, int t, double dt, double mu,
                             bool per_step_noise)
 {
     VertArgs a = vm_args(s);
-    cudaMemsetAsync(s->F, 0, sizeof(double2) * s->Nv, s->stream);
     launch_vm_forces(s, a);
     if (kind == 0) {
         const double *nz = noise ? (per_step_noise ? noise + (size_t)t * 2 * s->Nv : noise) : nullptr;

@@ -94,6 +94,45 @@ CG_D void atomic_add2<float>(void *F, int i, float x, float y)
     atomicAdd(reinterpret_cast<float2 *>(F) + i, make_float2(x, y));
 }
 
+// Order-independent force sums (deterministic mode, VoroArgs::Ffix set). A contribution x is split
+// into hi = floor(x 2^20), a count of 2^-20, and lo = round((x 2^20 - hi) 2^44), a count of 2^-64;
+// both are added with 64-bit integer atomics. Integer addition commutes exactly, so a cell's sum
+// does not depend on the order in which its contributions arrive, and a retraction cancels its
+// addition exactly. Resolution 2^-65 per contribution; |x| < 2^42 (a larger or non-finite value
+// sets bit 62 of the lo word and the cell's force reads NaN).
+CG_D void fix_add1(unsigned long long *w, double x)
+{
+    if (!(fabs(x) < 0x1p42)) {
+        atomicOr(w + 1, 1ull << 62);
+        return;
+    }
+    const double t = x * 0x1p20;
+    const double h = floor(t);
+    const long long hi = (long long)h;
+    const long long lo = __double2ll_rn((t - h) * 0x1p44);
+    if (hi) atomicAdd(w, (unsigned long long)hi);
+    if (lo) atomicAdd(w + 1, (unsigned long long)lo);
+}
+
+CG_D double fix_value(unsigned long long hi, unsigned long long lo)
+{
+    if (lo >> 62) return __longlong_as_double(0x7ff8000000000000ll);
+    return ((double)(long long)hi + (double)lo * 0x1p-44) * 0x1p-20;
+}
+
+// add (x, y) to the force of cell i: F += (x, y), or to its fixed-point sums when Ffix is set
+template <typename R>
+CG_D void add_force(void *F, unsigned long long *Ffix, int i, R x, R y)
+{
+    if (Ffix) {
+        unsigned long long *w = Ffix + 4 * (size_t)i;
+        fix_add1(w, (double)x);
+        fix_add1(w + 2, (double)y);
+    } else {
+        atomic_add2<R>(F, i, x, y);
+    }
+}
+
 template <typename R>
 CG_D void store_ap(void *AP, int i, R A, R P)
 {
@@ -216,7 +255,7 @@ CG_D int cell_pass(const VoroArgs &a, int c, const int *row, int z, double2 pc, 
                 fax = cax;
                 fay = cay;
             } else {
-                atomic_add2<R>(a.F, row[k - 1], sign * (pendx + cax), sign * (pendy + cay));
+                add_force<R>(a.F, a.Ffix, row[k - 1], sign * (pendx + cax), sign * (pendy + cay));
             }
             pendx = cbx;
             pendy = cby;
@@ -232,8 +271,8 @@ CG_D int cell_pass(const VoroArgs &a, int c, const int *row, int z, double2 pc, 
                 hN = cvt<R>(circum0<double>(rB, rC));
             }
         }
-        atomic_add2<R>(a.F, row[z - 1], sign * (pendx + fax), sign * (pendy + fay));
-        atomic_add2<R>(a.F, c, sign * sx, sign * sy);
+        add_force<R>(a.F, a.Ffix, row[z - 1], sign * (pendx + fax), sign * (pendy + fay));
+        add_force<R>(a.F, a.Ffix, c, sign * sx, sign * sy);
     }
     return fail;
 }
@@ -523,11 +562,11 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<
         int k = gl + G * r;
         if (ok && k < z) {
             V ca = T.ca[k + 1 == z ? 0 : k + 1];
-            atomic_add2<R>(a.F, nbk[r], sgn * (cb[r].x + ca.x), sgn * (cb[r].y + ca.y));
+            add_force<R>(a.F, a.Ffix, nbk[r], sgn * (cb[r].x + ca.x), sgn * (cb[r].y + ca.y));
         }
     }
     if (ok && gl == 0) {
-        atomic_add2<R>(a.F, c, sgn * sx, sgn * sy);
+        add_force<R>(a.F, a.Ffix, c, sgn * sx, sgn * sy);
     }
 }
 
@@ -1446,6 +1485,18 @@ CG_D double2 pair_draw(const VoroArgs &a, int c0, uint32_t step)
     return xi;
 }
 
+// Deterministic mode: F of every cell from its fixed-point sums (after the step's force pass and
+// repair rounds, before anything reads F).
+template <typename R>
+__global__ void k_fix_forces(VoroArgs a)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.N) return;
+    const ulonglong2 *w = reinterpret_cast<const ulonglong2 *>(a.Ffix) + 2 * (size_t)i;
+    const ulonglong2 fx = w[0], fy = w[1];
+    reinterpret_cast<typename Vec2<R>::T *>(a.F)[i] = mk<R>((R)fix_value(fx.x, fx.y), (R)fix_value(fy.x, fy.y));
+}
+
 // The same normals for every cell of the current step, into out[N]. The step graph runs this
 // beside the repair rounds (which leave most of the GPU idle), so k_spp reads them instead of
 // drawing them on the step's critical path; the values are the ones k_spp would draw.
@@ -1478,8 +1529,10 @@ __global__ void k_spp(VoroArgs a, const double *noise, double dt, double mu, uin
 // ------------------------------------------------------------------------------------------
 // energies per instance (FP64 accumulation)
 // ------------------------------------------------------------------------------------------
+// Efix (deterministic mode): the sums go to 2 fixed-point words per instance (fix_add1), which
+// k_energy_from_fix converts into E
 template <typename R>
-__global__ void __launch_bounds__(256) k_energy(VoroArgs a, double *E)
+__global__ void __launch_bounds__(256) k_energy(VoroArgs a, double *E, unsigned long long *Efix)
 {
     __shared__ double s_part[8];
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1503,11 +1556,23 @@ __global__ void __launch_bounds__(256) k_energy(VoroArgs a, double *E)
         if (threadIdx.x == 0) {
             double t = 0.0;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
-            atomicAdd(&E[i0], t);
+            if (Efix) fix_add1(Efix + 2 * (size_t)i0, t);
+            else atomicAdd(&E[i0], t);
         }
     } else if (c < a.N) {
-        atomicAdd(&E[inst], e);
+        if (Efix) fix_add1(Efix + 2 * (size_t)inst, e);
+        else atomicAdd(&E[inst], e);
     }
+}
+
+// E[i] from the fixed-point sums of k_energy, which are left zeroed for the next call
+__global__ void k_energy_from_fix(int n, unsigned long long *Efix, double *E)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    E[i] = fix_value(Efix[2 * (size_t)i], Efix[2 * (size_t)i + 1]);
+    Efix[2 * (size_t)i] = 0ull;
+    Efix[2 * (size_t)i + 1] = 0ull;
 }
 
 // The same sums written straight into page-locked host memory (host_out: its device address):
@@ -1517,6 +1582,8 @@ __global__ void __launch_bounds__(256) k_energy(VoroArgs a, double *E)
 template <typename R>
 __global__ void __launch_bounds__(256) k_energy_to_host(VoroArgs a, double *acc, unsigned *done, double *host_out)
 {
+    // deterministic mode (a.Ffix set): acc holds 2 fixed-point words per instance (fix_add1)
+    unsigned long long *afix = a.Ffix ? reinterpret_cast<unsigned long long *>(acc) : nullptr;
     __shared__ double s_part[8];
     __shared__ int s_last;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1538,10 +1605,12 @@ __global__ void __launch_bounds__(256) k_energy_to_host(VoroArgs a, double *acc,
         if (threadIdx.x == 0) {
             double t = 0.0;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
-            atomicAdd(&acc[i0], t);
+            if (afix) fix_add1(afix + 2 * (size_t)i0, t);
+            else atomicAdd(&acc[i0], t);
         }
     } else if (c < a.N) {
-        atomicAdd(&acc[inst], e);
+        if (afix) fix_add1(afix + 2 * (size_t)inst, e);
+        else atomicAdd(&acc[inst], e);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1552,8 +1621,14 @@ __global__ void __launch_bounds__(256) k_energy_to_host(VoroArgs a, double *acc,
     if (s_last) {
         __threadfence();
         for (int i = threadIdx.x; i < a.n_inst; i += blockDim.x) {
-            unsigned long long v = atomicExch(reinterpret_cast<unsigned long long *>(&acc[i]), 0ull);
-            host_out[i] = __longlong_as_double((long long)v);
+            if (afix) {
+                const unsigned long long hi = atomicExch(afix + 2 * (size_t)i, 0ull);
+                const unsigned long long lo = atomicExch(afix + 2 * (size_t)i + 1, 0ull);
+                host_out[i] = fix_value(hi, lo);
+            } else {
+                unsigned long long v = atomicExch(reinterpret_cast<unsigned long long *>(&acc[i]), 0ull);
+                host_out[i] = __longlong_as_double((long long)v);
+            }
         }
         __threadfence_system();
         if (threadIdx.x == 0) *done = 0u;

@@ -154,6 +154,15 @@ class VoronoiBatch:
     def set_seed(self, seed):
         check(self._lib.cg_set_seed(self._h, int(seed) & (2**64 - 1)))
 
+    def set_deterministic(self, on=True):
+        """Order-independent (fixed-point) force sums: the same inputs then give bit-identical
+        forces and trajectories on every run (cg_set_deterministic)."""
+        check(self._lib.cg_set_deterministic(self._h, 1 if on else 0))
+
+    @property
+    def deterministic(self):
+        return bool(self._lib.cg_get_deterministic(self._h))
+
     def set_instance_seeds(self, seeds):
         """Philox key of each instance's device noise (its noise is then independent of where the
         instance sits in a batch)."""
@@ -662,8 +671,11 @@ class Simulation:
             raise NotImplementedError("cellgpu_b200 runs on the GPU only")
 
     def setReproducible(self, flag):
+        """Reproducible runs (Simulation::setReproducible): besides fixed seeds, the forces are
+        summed in an order-independent way, so reruns give bit-identical trajectories."""
         if self.configuration is not None:
             self.configuration.reproducible = bool(flag)
+            self.configuration.batch.set_deterministic(bool(flag))
 
     def setSortPeriod(self, sp):
         """Spatially re-sort the (Voronoi) configuration every sp steps (src/Simulation.cpp:154-164);

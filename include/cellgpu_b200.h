@@ -192,6 +192,17 @@ int cg_enforce_topology(cg_system *sys);  /* Voronoi: test+repair; vertex: T1 sw
  * cg_set_instance_seeds sets every seed_i explicitly (n_inst values). */
 int cg_set_seed(cg_system *sys, uint64_t seed);
 int cg_set_instance_seeds(cg_system *sys, const uint64_t *seeds);
+/* Deterministic force sums (the reference's kernels sum each cell's force sets in a fixed order,
+ * src/models/voronoiQuadraticEnergy.cu:30-54; Simulation::setReproducible maps here). Off (the
+ * default): floating-point atomics, whose order varies, so reruns agree only to rounding and a
+ * chaotic trajectory then drifts apart. On: forces are summed in 64-bit fixed point (2^-64
+ * resolution per contribution, |contribution| < 2^42, else the cell's force is NaN) with integer
+ * atomics, exact in any order, so the same inputs give bit-identical forces and trajectories.
+ * FIRE's per-instance power and norm sums are then taken in a fixed order (per-block partials
+ * joined by one block per instance) instead of with atomics. Allocates 32 bytes per cell (Voronoi)
+ * or vertex (vertex model) on first use; drops captured graphs. Both models. */
+int cg_set_deterministic(cg_system *sys, int on);
+int cg_get_deterministic(cg_system *sys);
 int cg_spp_run(cg_system *sys, int n_steps, double dt, double mu, const double *noise_dev);
 /* Enqueue n_steps RNG-driven SPP steps (one CUDA graph replay) with no host synchronisation.
  * A step that cannot finish on the device (a global rebuild is needed) sets a sticky halt flag and
