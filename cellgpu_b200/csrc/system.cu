@@ -61,17 +61,18 @@ static inline int cells_per_block(int N, int wpb, int minb)
 }
 
 // launch of the fused per-cell pass (groups of 8 lanes) in launch shape 0 or 1; rows of up to 16
-// slots take the fast form, wider rows (K = 32) the form with four slots per lane
-template <typename R, bool SCATTER, bool TEST, int NS>
+// slots take the fast form, wider rows (K = 32) the form with four slots per lane; with forces,
+// FIX = 1 is the form that sums them in fixed point (deterministic mode, VoroArgs::Ffix set)
+template <typename R, bool SCATTER, bool TEST, int NS, int FIX>
 static inline void launch_groups_ns(const VoroArgs &a, int N, cudaStream_t st, int shape)
 {
     if (shape == 1) {
         int cpb = cells_per_block(N, CG_FORCE_WPB_ALT, CG_FORCE_MINB_ALT);
-        k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB_ALT, CG_FORCE_MINB_ALT, NS>
+        k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB_ALT, CG_FORCE_MINB_ALT, NS, FIX>
             <<<nblk(N, cpb), CG_FORCE_WPB_ALT * 32, 0, st>>>(a, cpb);
     } else {
         int cpb = cells_per_block(N, CG_FORCE_WPB, CG_FORCE_MINB);
-        k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB, CG_FORCE_MINB, NS>
+        k_voro_groups<R, SCATTER, TEST, CG_FORCE_WPB, CG_FORCE_MINB, NS, FIX>
             <<<nblk(N, cpb), CG_FORCE_WPB * 32, 0, st>>>(a, cpb);
     }
 }
@@ -79,10 +80,19 @@ static inline void launch_groups_ns(const VoroArgs &a, int N, cudaStream_t st, i
 template <typename R, bool SCATTER, bool TEST>
 static inline void launch_groups(const VoroArgs &a, int N, cudaStream_t st, int shape = 0)
 {
+    if constexpr (SCATTER) {
+        if (a.Ffix) {
+            if (a.K > VG)
+                launch_groups_ns<R, SCATTER, TEST, VG_MAX, 1>(a, N, st, shape);
+            else
+                launch_groups_ns<R, SCATTER, TEST, VG, 1>(a, N, st, shape);
+            return;
+        }
+    }
     if (a.K > VG)
-        launch_groups_ns<R, SCATTER, TEST, VG_MAX>(a, N, st, shape);
+        launch_groups_ns<R, SCATTER, TEST, VG_MAX, 0>(a, N, st, shape);
     else
-        launch_groups_ns<R, SCATTER, TEST, VG>(a, N, st, shape);
+        launch_groups_ns<R, SCATTER, TEST, VG, 0>(a, N, st, shape);
 }
 
 static Inst make_inst(double Lx, double Ly, int off, int n, int bin_off, double bin_target)

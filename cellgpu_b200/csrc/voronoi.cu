@@ -120,11 +120,12 @@ CG_D double fix_value(unsigned long long hi, unsigned long long lo)
     return ((double)(long long)hi + (double)lo * 0x1p-44) * 0x1p-20;
 }
 
-// add (x, y) to the force of cell i: F += (x, y), or to its fixed-point sums when Ffix is set
-template <typename R>
+// add (x, y) to the force of cell i: F += (x, y), or to its fixed-point sums. FIX = -1 decides by
+// Ffix at run time; the force pass is compiled for one mode (FIX = 0 atomics, 1 fixed point).
+template <typename R, int FIX = -1>
 CG_D void add_force(void *F, unsigned long long *Ffix, int i, R x, R y)
 {
-    if (Ffix) {
+    if (FIX == 1 || (FIX == -1 && Ffix)) {
         unsigned long long *w = Ffix + 4 * (size_t)i;
         fix_add1(w, (double)x);
         fix_add1(w + 2, (double)y);
@@ -498,7 +499,7 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
 
 // Phases D-E (called by the whole warp): g_k = -dE_c/dh_k, the three Jacobian contractions of every
 // vertex, and the scatter of SIGN x (contribution) to the cell and its neighbours.
-template <typename R, int SIGN, int NS = VG>
+template <typename R, int SIGN, int NS = VG, int FIX = -1>
 CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<R, NS> &T, const int (&nbk)[NS / G],
                       double A, double P, R sgn = R(SIGN))
 {
@@ -562,17 +563,17 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<
         int k = gl + G * r;
         if (ok && k < z) {
             V ca = T.ca[k + 1 == z ? 0 : k + 1];
-            add_force<R>(a.F, a.Ffix, nbk[r], sgn * (cb[r].x + ca.x), sgn * (cb[r].y + ca.y));
+            add_force<R, FIX>(a.F, a.Ffix, nbk[r], sgn * (cb[r].x + ca.x), sgn * (cb[r].y + ca.y));
         }
     }
     if (ok && gl == 0) {
-        add_force<R>(a.F, a.Ffix, c, sgn * sx, sgn * sy);
+        add_force<R, FIX>(a.F, a.Ffix, c, sgn * sx, sgn * sy);
     }
 }
 
 // A block takes a contiguous run of cpb cells (a multiple of its WPB * GPW groups), so that in a
 // spatially sorted system the cells one SM works on are neighbours and their positions stay in L1.
-template <typename R, bool SCATTER, bool TEST, int WPB, int MINB, int NS = VG>
+template <typename R, bool SCATTER, bool TEST, int WPB, int MINB, int NS = VG, int FIX = 0>
 __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int cpb)
 {
     __shared__ GrpTile<R, NS> tile[WPB * GPW];
@@ -607,7 +608,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int 
         // would swamp the forces. The repair commit adds the contributions of the new row.
         bool hold = SCATTER && TEST && a.held && ok && fail != 0x7fffffff;
         if (hold && gl == 0) a.held[c] = 1;
-        if (SCATTER) grp_scatter<R, 1, NS>(a, c, z, ok && !hold, gl, tile[sl], nbk, A, P);
+        if (SCATTER) grp_scatter<R, 1, NS, FIX>(a, c, z, ok && !hold, gl, tile[sl], nbk, A, P);
         if (TEST && live && gl == 0 && (fail != 0x7fffffff || !ok)) {
             if (!ok) {
                 if (a.ctl) {
