@@ -256,3 +256,62 @@ def test_fire_vertex_reruns_bit_identical(cglib):
         b.close()
     for x, y in zip(*runs):
         assert np.array_equal(x, y)
+
+
+def _typed_batch(pos, box, mode, det, K=16):
+    from cellgpu_b200 import VoronoiBatch
+    N = len(pos)
+    rng = np.random.default_rng(51)
+    b = VoronoiBatch([N], [box], K=K)
+    b.set_positions(pos)
+    b.set_directors(rng.uniform(0, 2 * np.pi, N))
+    b.set_motility(np.tile([0.2, 1.0], (N, 1)))
+    b.set_preferences(np.tile([1.0, 3.8], (N, 1)))
+    b.set_seed(52)
+    if mode is not None:
+        b.set_cell_types(rng.integers(0, 3, N))
+        if mode == "simple":
+            b.set_tension(0.2)
+        else:
+            b.set_tension_matrix(np.array([[0.0, 0.1, 0.3], [0.1, 0.0, 0.2], [0.3, 0.2, 0.0]]))
+    b.set_deterministic(det)
+    b.triangulate()
+    return b
+
+
+@pytest.mark.parametrize("mode", ["simple", "matrix"])
+def test_tension_deterministic(cglib, mode):
+    """Line tension (one gamma, or a matrix over three types) with fixed-point sums: forces agree with
+    the atomic sums to rounding, and reruns are bit-identical."""
+    pos, box = monolayer(2000, 53)
+    a = _typed_batch(pos, box, mode, False)
+    a.compute_forces()
+    runs = []
+    for _ in range(2):
+        b = _typed_batch(pos, box, mode, True)
+        b.compute_forces()
+        assert force_error(b.forces(), a.forces()) < 1e-13
+        b.spp_run(100, dt=0.01)
+        runs.append((b.positions(), b.forces(), b.energies()))
+        b.close()
+    for x, y in zip(*runs):
+        assert np.array_equal(x, y)
+
+
+def test_wide_rows_deterministic(cglib):
+    """The 32-slot form of the force pass with fixed-point sums: it agrees with the 16-slot form, and
+    its reruns are bit-identical."""
+    pos, box = jittered_lattice(40, 46, 0.25, 41)
+    narrow = _typed_batch(pos, box, None, True, K=16)
+    narrow.compute_forces()
+    runs = []
+    for _ in range(2):
+        b = _typed_batch(pos, box, None, True, K=32)
+        b.compute_forces()
+        assert force_error(b.forces(), narrow.forces()) < 1e-13
+        b.spp_run(30, dt=0.02)
+        runs.append((b.positions(), b.forces(), b.counters()["rows_changed"]))
+        b.close()
+    for x, y in zip(*runs):
+        assert np.array_equal(x, y)
+    assert runs[0][2] > 0
