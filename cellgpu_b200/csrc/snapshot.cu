@@ -6,7 +6,9 @@
 // the tension matrix. The device noise of a step is
 // Philox keyed by the instance seed with the step and the local index as counters, so a system
 // restored from a snapshot draws the same noise as the original would have and continues the same
-// trajectory, up to the summation order of floating-point atomics. FIRE velocities and the
+// trajectory: bit for bit when the system sums in the deterministic mode (cg_set_deterministic,
+// which the snapshot records and the restore switches on), else up to the summation order of
+// floating-point atomics. FIRE velocities and the
 // derived quantities (forces, areas, perimeters) are not stored; they are recomputed.
 // The reference's state files (netCDF, src/databases/DatabaseNetCDFSPV.cpp:32-46,
 // DatabaseNetCDFAVM.cpp:33-52) hold positions and topology but no RNG state, so a run cannot be
@@ -22,7 +24,8 @@ struct SnapHeader {
     int topology_valid, step;
     double KA, KP, t1;
     unsigned long long seed;
-    int has_types, tension_mode, ntypes, pad;  // line tension (Voronoi model)
+    int has_types, tension_mode, ntypes;  // line tension
+    int flags;                            // bit 0: deterministic force sums (0 in older snapshots)
     double gamma;
 };
 
@@ -89,6 +92,7 @@ SnapHeader snap_header(const cg_system *s)
     h.tension_mode = s->tension_mode;
     h.ntypes = s->tension_mode == 2 ? s->ntypes : 0;
     h.gamma = s->gamma;
+    h.flags = s->det ? 1 : 0;
     return h;
 }
 
@@ -142,7 +146,7 @@ extern "C" int cg_restore(const void *buf, size_t bytes, cg_system **out)
     if (memcmp(h.magic, SNAP_MAGIC, 8) != 0 || h.version != 2) return set_err(CG_ERR_ARG, "not a cellgpu_b200 snapshot");
     if (h.n_inst <= 0 || h.N <= 0 || (h.model != CG_MODEL_VORONOI && h.model != CG_MODEL_VERTEX) ||
         h.tension_mode < 0 || h.tension_mode > 2 || h.ntypes < 0 || (h.tension_mode == 2 && h.ntypes < 1) ||
-        (h.tension_mode && !h.has_types) || bytes < snap_total(h))
+        (h.tension_mode && !h.has_types) || (h.flags & ~1) || bytes < snap_total(h))
         return set_err(CG_ERR_ARG, "corrupt or truncated snapshot");
     const unsigned char *p = static_cast<const unsigned char *>(buf) + sizeof(h);
     std::vector<int> Ns(h.n_inst);
@@ -189,6 +193,7 @@ extern "C" int cg_restore(const void *buf, size_t bytes, cg_system **out)
         s->ntypes = h.ntypes;
         s->gamma = h.gamma;
         s->topology_valid = h.topology_valid != 0;
+        if ((h.flags & 1) && (st = cg_set_deterministic(s, 1))) break;
         Ctl c;
         if ((st = read_ctl(s, c))) break;
         c.step = h.step;

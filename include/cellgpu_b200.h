@@ -259,7 +259,8 @@ int cg_fire_state(cg_system *sys, int *iterations, double *fmax_cpu, double *fno
  * positions, directors, motility, preferences, moduli, topology or vertex wiring, T1 threshold,
  * step counter) into a host buffer of cg_snapshot_size bytes; cg_restore builds a new system from
  * it. Device noise is keyed per instance and counted by step and local index, so the restored
- * system continues the original trajectory (up to the summation order of atomics). FIRE
+ * system continues the original trajectory: bit for bit in the deterministic mode (recorded in
+ * the snapshot and switched on by cg_restore), else up to the summation order of atomics. FIRE
  * velocities and derived quantities (forces, A/P) are not stored. */
 size_t cg_snapshot_size(cg_system *sys);
 int cg_snapshot(cg_system *sys, void *buf, size_t bytes);
