@@ -342,3 +342,44 @@ def test_resume_is_bit_exact(cglib):
     assert np.array_equal(r.directors(), b.directors())
     assert np.array_equal(r.forces(), b.forces())
     assert b.counters()["rows_changed"] > 0
+
+
+def test_batch_equals_singles_bit_for_bit(cglib):
+    """In the deterministic mode an instance's SPP trajectory does not depend on where it sits in a
+    batch, bit for bit: forces are sums of instance-local contributions in exact fixed point, the
+    topology is exact, and the device noise is keyed by the instance seed and local cell index.
+    (Energies agree to rounding: their per-block partial sums follow the batch's block boundaries.)"""
+    from cellgpu_b200 import VoronoiBatch
+    shapes = [(10, 12), (16, 16), (20, 22)]
+    lat = [jittered_lattice(nx, ny, 0.25, 40 + i) for i, (nx, ny) in enumerate(shapes)]
+    poss = [p for p, _ in lat]
+    boxes = [bx for _, bx in lat]
+    Ns = [len(p) for p in poss]
+    seeds = [11, 22, 33]
+    rng = np.random.default_rng(5)
+    ths = [rng.uniform(0, 2 * np.pi, n) for n in Ns]
+
+    def make(sel):
+        b = VoronoiBatch([Ns[i] for i in sel], [boxes[i] for i in sel])
+        b.set_positions(np.concatenate([poss[i] for i in sel]))
+        b.set_directors(np.concatenate([ths[i] for i in sel]))
+        b.set_motility(np.tile([0.3, 1.0], (sum(Ns[i] for i in sel), 1)))
+        b.set_instance_seeds([seeds[i] for i in sel])
+        b.set_deterministic(True)
+        b.triangulate()
+        b.spp_run(30, dt=0.02)
+        return b
+
+    order = [2, 0, 1]  # another placement of the same instances
+    b = make(order)
+    Pb, Fb, Eb = b.positions(), b.forces(), b.energies()
+    assert b.counters()["rows_changed"] > 0
+    off = 0
+    for j, i in enumerate(order):
+        s = make([i])
+        n = Ns[i]
+        assert np.array_equal(Pb[off:off + n], s.positions())
+        assert np.array_equal(Fb[off:off + n], s.forces())
+        # energies: per-block partial sums depend on where block boundaries fall in the batch
+        assert abs(Eb[j] - s.energies()[0]) <= 1e-13 * abs(Eb[j])
+        off += n
