@@ -12,7 +12,9 @@ batch completes.
 Every instance's result depends only on its own request: its initial state and its device noise
 are derived from the request's seed, the noise is keyed by the instance seed and the local cell
 index, and FIRE keeps per-instance state. So a request gives the same result alone and in a mix,
-up to the order of floating-point atomics.
+up to the order of floating-point atomics; with ``Server(deterministic=True)`` (fixed-point force
+sums) an SPP request's positions are the same bits in any mix, and reruns of a batch repeat
+exactly.
 
 The reference has no serving layer; this drives the same kernels as the class API
 (``VoronoiQuadraticEnergy``/``VertexQuadraticEnergy`` with ``selfPropelledParticleDynamics``,
@@ -88,9 +90,10 @@ def instance_seed(req):
     return int(np.random.default_rng([int(req.seed) & (2**63 - 1), 29]).integers(0, 2**63))
 
 
-def footprint(model, sizes, K=16, vmax=30):
+def footprint(model, sizes, K=16, vmax=30, deterministic=False):
     """Device bytes of a batch with these instance sizes, plus FIRE and staging buffers allocated
-    on first use (velocities, per-dof instance index)."""
+    on first use (velocities, per-dof instance index, and in the deterministic mode the fixed-point
+    accumulators)."""
     lib = load()
     arr = np.ascontiguousarray(sizes, dtype=np.int32)
     if model == "voronoi":
@@ -99,7 +102,8 @@ def footprint(model, sizes, K=16, vmax=30):
     else:
         base = lib.cg_vertex_footprint(len(arr), arr.ctypes.data, vmax)
         dofs = 2 * int(arr.sum())
-    return int(base + 24 * dofs + 8 * int(arr.sum()) + 256 * len(arr) + (1 << 16))
+    det = (32 * dofs + 16 * len(arr)) if deterministic else 0
+    return int(base + 24 * dofs + 8 * int(arr.sum()) + 256 * len(arr) + det + (1 << 16))
 
 
 def device_memory():
@@ -109,9 +113,10 @@ def device_memory():
     return f.value, t.value
 
 
-def run_batch(reqs):
+def run_batch(reqs, deterministic=False):
     """Run one batch of same-kind requests to completion on its own system (and stream); return
-    per-request (positions, energy, iterations, fmax)."""
+    per-request (positions, energy, iterations, fmax). deterministic: fixed-point force sums and
+    fixed-order FIRE reductions (cg_set_deterministic)."""
     model, task = reqs[0].model, reqs[0].task
     states = [initial_state(r) for r in reqs]
     Ns = [r.n for r in reqs]
@@ -124,6 +129,8 @@ def run_batch(reqs):
         b = VertexBatch(Ns, boxes)
         b.from_cells(pos)
     try:
+        if deterministic:
+            b.set_deterministic(True)
         b.set_preferences(np.concatenate([np.tile([1.0, r.p0], (r.n, 1)) for r in reqs]))
         b.set_instance_seeds([instance_seed(r) for r in reqs])
         if task == "spp":
@@ -157,13 +164,16 @@ class Server:
     """Continuous-batching request loop over ``lanes`` concurrent batches.
 
     memory_budget: bytes of device memory the resident batches may hold (default: 70 % of the
-    device's total memory). max_batch_cells / max_batch_requests bound one batch."""
+    device's total memory). max_batch_cells / max_batch_requests bound one batch. deterministic:
+    run every batch with order-independent sums (reproducible results)."""
 
-    def __init__(self, lanes=4, memory_budget=None, max_batch_cells=1 << 20, max_batch_requests=512):
+    def __init__(self, lanes=4, memory_budget=None, max_batch_cells=1 << 20, max_batch_requests=512,
+                 deterministic=False):
         if memory_budget is None:
             _, total = device_memory()
             memory_budget = int(0.7 * total)
         self.budget = int(memory_budget)
+        self.deterministic = bool(deterministic)
         self.max_cells = int(max_batch_cells)
         self.max_reqs = int(max_batch_requests)
         self.queue = collections.deque()
@@ -228,7 +238,7 @@ class Server:
                         continue
                     if picked and (cells + r.n > self.max_cells or len(picked) >= self.max_reqs):
                         break
-                    f = footprint(head.model, [x[0].n for x in picked] + [r.n])
+                    f = footprint(head.model, [x[0].n for x in picked] + [r.n], deterministic=self.deterministic)
                     if self.resident + f > self.budget:
                         break
                     picked.append(item)
@@ -259,7 +269,7 @@ class Server:
             reqs = [it[0] for it in items]
             t_start = time.perf_counter()
             try:
-                outs = run_batch(reqs)
+                outs = run_batch(reqs, self.deterministic)
                 err = None
             except Exception as e:  # the failure belongs to this batch's requests
                 outs, err = None, e

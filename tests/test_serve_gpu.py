@@ -85,3 +85,23 @@ def test_admission_by_footprint(cglib):
         fut = srv.submit(Request("voronoi", "spp", 500, seed=1, steps=5))
         with pytest.raises(MemoryError):
             fut.result()
+
+
+def test_deterministic_server_same_bits_alone_and_in_mix(cglib):
+    """Server(deterministic=True): an SPP request's positions are the same bits alone and in a
+    mixed batch, for both models (fixed-point force sums; noise keyed per instance)."""
+    from cellgpu_b200.serve import Server
+    reqs = [r for r in _requests() if r.task == "spp"]
+    alone = []
+    for r in reqs:
+        with Server(lanes=1, deterministic=True) as srv:
+            alone.append(srv.submit(copy.deepcopy(r)).result())
+    fill = [r for r in _fillers() if r.task == "spp"]
+    mix_in = fill[:2] + [copy.deepcopy(reqs[0])] + fill[2:4] + [copy.deepcopy(reqs[1])] + fill[4:]
+    where = [2, 5]
+    with Server(lanes=2, deterministic=True) as srv:
+        mix = [f.result() for f in srv.submit_many(mix_in)]
+    for a, k in zip(alone, where):
+        m = mix[k]
+        assert m.batch_requests > 1
+        assert np.array_equal(a.positions, m.positions)
