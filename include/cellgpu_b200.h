@@ -67,8 +67,9 @@ int cg_voronoi_geometry(const double *pos, const int *nn, const int *nbr, int K,
 /* Voronoi quadratic-energy forces, geometry included (one fused pass).
  * Replaces gpu_compute_voronoi_geometry + gpu_force_sets + gpu_sum_force_sets
  * (inc/models/voronoiQuadraticEnergy.cuh:20-54). F must be zeroed by the caller (forces are
- * accumulated); AP receives (A, P). APpref[c] = (A0, P0); KA, KP are the uniform moduli the reference
- * uses (inc/models/Simple2DCell.h:272-274). */
+ * accumulated with FP64 atomics, so the last bits of F can vary between calls; systems offer
+ * order-independent sums, cg_set_deterministic); AP receives (A, P). APpref[c] = (A0, P0); KA, KP
+ * are the uniform moduli the reference uses (inc/models/Simple2DCell.h:272-274). */
 int cg_voronoi_forces(const double *pos, const int *nn, const int *nbr, int K, int N, double Lx,
                       double Ly, const double *APpref, double KA, double KP, double *AP, double *F,
                       cudaStream_t stream);
