@@ -364,10 +364,11 @@ def replica_aggregate(total_s, done, n_cells, world, device):
     return (units / total_s if total_s > 0 else 0.0), total_s
 
 
-def workload_config(precision, world, sort=True):
+def workload_config(precision, world, sort=True, deterministic=False):
     return {"workload": "voronoi_spp_N262144_L512", "n_cells": N_CELLS, "box": BOX, "p0": P0, "v0": V0,
             "Dr": DR, "dt": DT, "precision": precision, "l2": "flushed (256 MB write) between timed steps",
             "spatial_sort": "Hilbert order once after equilibration" if sort else "none",
+            "force_sums": "fixed point (deterministic mode)" if deterministic else "floating-point atomics",
             "parallelism": f"replicas{world}"}
 
 
@@ -406,6 +407,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--deterministic", action="store_true",
+                    help="order-independent fixed-point force sums (cg_set_deterministic), the mode "
+                         "Simulation.setReproducible(true) selects")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-ensemble and vertex-model measurements")
@@ -474,6 +478,8 @@ def main():
     stream = torch.cuda.Stream()
     precision = cg.CG_FP64 if args.precision == "fp64" else cg.CG_MIXED
     b = make_system(cg, torch, stream, precision, seed=1 + rank)
+    if args.deterministic:
+        b.set_deterministic(True)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     # relax the random initial state (untimed): its first steps rearrange the tissue wholesale
     if args.equilibrate > 0:
@@ -558,7 +564,7 @@ def main():
         "warmup": max(3, args.warmup), "ms_per_step": 1e3 * total / max(done, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == cg.CG_FP64 else "f32+f64",
         "data": "synthetic",
-        "config": workload_config(args.precision, world, not args.no_sort),
+        "config": workload_config(args.precision, world, not args.no_sort, args.deterministic),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "kernel": "k_voro_groups (force+test)",
                      "kernel_ms": t_force * 1e3, "peak_kind": kind},

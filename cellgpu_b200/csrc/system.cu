@@ -260,7 +260,7 @@ struct cg_system {
     // deterministic force sums (cg_set_deterministic): fixed-point accumulator, 4 words per cell
     int det = 0;
     unsigned long long *Ffix = nullptr;
-    unsigned long long *Efix = nullptr;  // fixed-point energy sums, 2 words per instance
+    unsigned long long *Efix = nullptr;  // fixed-point energy sums, FIXW words per instance
     // asynchronous host-buffer steps: copy stream, a second staging buffer, per-buffer events
     cudaStream_t copy_stream = nullptr;
     double *noise_buf2 = nullptr;
@@ -763,7 +763,7 @@ template <typename R>
 static void launch_force_test(cg_system *s, const VoroArgs &a, bool test)
 {
     if (a.Ffix)
-        cudaMemsetAsync(a.Ffix, 0, 4 * sizeof(unsigned long long) * s->N, s->stream);
+        cudaMemsetAsync(a.Ffix, 0, 2 * FIXW * sizeof(unsigned long long) * s->N, s->stream);
     else
         cudaMemsetAsync(s->F, 0, (s->precision == CG_FP64 ? sizeof(double2) : sizeof(float2)) * s->N,
                         s->stream);
@@ -1177,7 +1177,7 @@ template <typename R>
 static int enqueue_energy_graph(cg_system *s, double dt, double mu, const double *noise, double *dst)
 {
     if (!s->e2e_acc) {
-        CG_TRY(dalloc(s, &s->e2e_acc, 2 * (size_t)s->n_inst));  // zeroed; the kernel leaves it zeroed
+        CG_TRY(dalloc(s, &s->e2e_acc, FIXW * (size_t)s->n_inst));  // zeroed; the kernel leaves it zeroed
         CG_TRY(dalloc(s, &s->e2e_done, 1));
     }
     for (auto &g : s->graphs)
@@ -1320,15 +1320,15 @@ extern "C" int cg_get_energies(cg_system *s, double *E)
 // accumulator with integer atomics and F is converted from it once per force evaluation, so the
 // same inputs give bit-identical forces and trajectories on every run (the reference's kernels sum
 // each cell's force sets in a fixed order, src/models/voronoiQuadraticEnergy.cu:30-54). Costs
-// 32 bytes per cell (or vertex) and one conversion kernel per force evaluation.
+// 48 bytes per cell (or vertex) and one conversion kernel per force evaluation.
 extern "C" int cg_set_deterministic(cg_system *s, int on)
 {
     if (!s) return set_err(CG_ERR_ARG, "null system");
     on = on ? 1 : 0;
     if (on == s->det) return CG_OK;
     if (on && !s->Ffix) {
-        CG_TRY(dalloc(s, &s->Ffix, 4 * (size_t)ndof(s)));
-        CG_TRY(dalloc(s, &s->Efix, 2 * (size_t)s->n_inst));
+        CG_TRY(dalloc(s, &s->Ffix, 2 * FIXW * (size_t)ndof(s)));
+        CG_TRY(dalloc(s, &s->Efix, FIXW * (size_t)s->n_inst));
     }
     CG_CUDA(cudaStreamSynchronize(s->stream));
     for (auto &g : s->graphs) release_graph(g);  // graphs captured the accumulation mode

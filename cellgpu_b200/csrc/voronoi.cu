@@ -94,17 +94,27 @@ CG_D void atomic_add2<float>(void *F, int i, float x, float y)
     atomicAdd(reinterpret_cast<float2 *>(F) + i, make_float2(x, y));
 }
 
-// Order-independent force sums (deterministic mode, VoroArgs::Ffix set). A contribution x is split
-// into hi = floor(x 2^20), a count of 2^-20, and lo = round((x 2^20 - hi) 2^44), a count of 2^-64;
-// both are added with 64-bit integer atomics. Integer addition commutes exactly, so a cell's sum
-// does not depend on the order in which its contributions arrive, and a retraction cancels its
-// addition exactly. Resolution 2^-65 per contribution; |x| < 2^42 (a larger or non-finite value
-// sets bit 62 of the lo word and the cell's force reads NaN).
+// Order-independent sums (deterministic mode, VoroArgs::Ffix set). A value x is kept in FIXW = 3
+// 64-bit integer words w[0..2] that hold x = w[0] 2^-20 + w[1] 2^-64 + w[2] 2^35 (w[0], w[2] signed,
+// w[1] non-negative): |x| >= 2^35 first moves its nearest multiple of 2^35 to w[2] (the
+// remainder, at most 2^34, is exact by Sterbenz's lemma), then hi = floor(x 2^20) goes to w[0] and
+// lo = round((x 2^20 - hi) 2^44) to w[1]. Each part is added with a 64-bit integer atomic. Integer
+// addition commutes exactly, so the sum does not depend on the order in which the parts arrive,
+// and a retraction cancels its addition exactly. Resolution 2^-65 per value; any finite |x| < 2^98
+// (the third word is touched only by |x| >= 2^35); a larger or non-finite x sets bit 62 of w[1]
+// and the sum reads NaN.
+constexpr int FIXW = 3;
+
 CG_D void fix_add1(unsigned long long *w, double x)
 {
-    if (!(fabs(x) < 0x1p42)) {
-        atomicOr(w + 1, 1ull << 62);
-        return;
+    if (!(fabs(x) < 0x1p35)) {
+        if (!(fabs(x) < 0x1p98)) {
+            atomicOr(w + 1, 1ull << 62);
+            return;
+        }
+        const double q = rint(x * 0x1p-35);
+        atomicAdd(w + 2, (unsigned long long)(long long)q);
+        x -= q * 0x1p35;
     }
     const double t = x * 0x1p20;
     const double h = floor(t);
@@ -114,10 +124,10 @@ CG_D void fix_add1(unsigned long long *w, double x)
     if (lo) atomicAdd(w + 1, (unsigned long long)lo);
 }
 
-CG_D double fix_value(unsigned long long hi, unsigned long long lo)
+CG_D double fix_value(unsigned long long hi, unsigned long long lo, unsigned long long top)
 {
     if (lo >> 62) return __longlong_as_double(0x7ff8000000000000ll);
-    return ((double)(long long)hi + (double)lo * 0x1p-44) * 0x1p-20;
+    return (double)(long long)top * 0x1p35 + ((double)(long long)hi + (double)lo * 0x1p-44) * 0x1p-20;
 }
 
 // add (x, y) to the force of cell i: F += (x, y), or to its fixed-point sums. FIX = -1 decides by
@@ -126,9 +136,9 @@ template <typename R, int FIX = -1>
 CG_D void add_force(void *F, unsigned long long *Ffix, int i, R x, R y)
 {
     if (FIX == 1 || (FIX == -1 && Ffix)) {
-        unsigned long long *w = Ffix + 4 * (size_t)i;
+        unsigned long long *w = Ffix + 2 * FIXW * (size_t)i;
         fix_add1(w, (double)x);
-        fix_add1(w + 2, (double)y);
+        fix_add1(w + FIXW, (double)y);
     } else {
         atomic_add2<R>(F, i, x, y);
     }
@@ -1493,9 +1503,10 @@ __global__ void k_fix_forces(VoroArgs a)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.N) return;
-    const ulonglong2 *w = reinterpret_cast<const ulonglong2 *>(a.Ffix) + 2 * (size_t)i;
-    const ulonglong2 fx = w[0], fy = w[1];
-    reinterpret_cast<typename Vec2<R>::T *>(a.F)[i] = mk<R>((R)fix_value(fx.x, fx.y), (R)fix_value(fy.x, fy.y));
+    const ulonglong2 *w = reinterpret_cast<const ulonglong2 *>(a.Ffix) + 3 * (size_t)i;  // 2 FIXW words
+    const ulonglong2 w0 = w[0], w1 = w[1], w2 = w[2];
+    reinterpret_cast<typename Vec2<R>::T *>(a.F)[i] =
+        mk<R>((R)fix_value(w0.x, w0.y, w1.x), (R)fix_value(w1.y, w2.x, w2.y));
 }
 
 // The same normals for every cell of the current step, into out[N]. The step graph runs this
@@ -1530,7 +1541,7 @@ __global__ void k_spp(VoroArgs a, const double *noise, double dt, double mu, uin
 // ------------------------------------------------------------------------------------------
 // energies per instance (FP64 accumulation)
 // ------------------------------------------------------------------------------------------
-// Efix (deterministic mode): the sums go to 2 fixed-point words per instance (fix_add1), which
+// Efix (deterministic mode): the sums go to FIXW fixed-point words per instance (fix_add1), which
 // k_energy_from_fix converts into E
 template <typename R>
 __global__ void __launch_bounds__(256) k_energy(VoroArgs a, double *E, unsigned long long *Efix)
@@ -1557,11 +1568,11 @@ __global__ void __launch_bounds__(256) k_energy(VoroArgs a, double *E, unsigned 
         if (threadIdx.x == 0) {
             double t = 0.0;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
-            if (Efix) fix_add1(Efix + 2 * (size_t)i0, t);
+            if (Efix) fix_add1(Efix + FIXW * (size_t)i0, t);
             else atomicAdd(&E[i0], t);
         }
     } else if (c < a.N) {
-        if (Efix) fix_add1(Efix + 2 * (size_t)inst, e);
+        if (Efix) fix_add1(Efix + FIXW * (size_t)inst, e);
         else atomicAdd(&E[inst], e);
     }
 }
@@ -1571,9 +1582,9 @@ __global__ void k_energy_from_fix(int n, unsigned long long *Efix, double *E)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    E[i] = fix_value(Efix[2 * (size_t)i], Efix[2 * (size_t)i + 1]);
-    Efix[2 * (size_t)i] = 0ull;
-    Efix[2 * (size_t)i + 1] = 0ull;
+    unsigned long long *w = Efix + FIXW * (size_t)i;
+    E[i] = fix_value(w[0], w[1], w[2]);
+    w[0] = w[1] = w[2] = 0ull;
 }
 
 // The same sums written straight into page-locked host memory (host_out: its device address):
@@ -1583,7 +1594,7 @@ __global__ void k_energy_from_fix(int n, unsigned long long *Efix, double *E)
 template <typename R>
 __global__ void __launch_bounds__(256) k_energy_to_host(VoroArgs a, double *acc, unsigned *done, double *host_out)
 {
-    // deterministic mode (a.Ffix set): acc holds 2 fixed-point words per instance (fix_add1)
+    // deterministic mode (a.Ffix set): acc holds FIXW fixed-point words per instance (fix_add1)
     unsigned long long *afix = a.Ffix ? reinterpret_cast<unsigned long long *>(acc) : nullptr;
     __shared__ double s_part[8];
     __shared__ int s_last;
@@ -1606,11 +1617,11 @@ __global__ void __launch_bounds__(256) k_energy_to_host(VoroArgs a, double *acc,
         if (threadIdx.x == 0) {
             double t = 0.0;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
-            if (afix) fix_add1(afix + 2 * (size_t)i0, t);
+            if (afix) fix_add1(afix + FIXW * (size_t)i0, t);
             else atomicAdd(&acc[i0], t);
         }
     } else if (c < a.N) {
-        if (afix) fix_add1(afix + 2 * (size_t)inst, e);
+        if (afix) fix_add1(afix + FIXW * (size_t)inst, e);
         else atomicAdd(&acc[inst], e);
     }
     __syncthreads();
@@ -1623,9 +1634,10 @@ __global__ void __launch_bounds__(256) k_energy_to_host(VoroArgs a, double *acc,
         __threadfence();
         for (int i = threadIdx.x; i < a.n_inst; i += blockDim.x) {
             if (afix) {
-                const unsigned long long hi = atomicExch(afix + 2 * (size_t)i, 0ull);
-                const unsigned long long lo = atomicExch(afix + 2 * (size_t)i + 1, 0ull);
-                host_out[i] = fix_value(hi, lo);
+                unsigned long long *w = afix + FIXW * (size_t)i;
+                const unsigned long long hi = atomicExch(w, 0ull), lo = atomicExch(w + 1, 0ull);
+                const unsigned long long top = atomicExch(w + 2, 0ull);
+                host_out[i] = fix_value(hi, lo, top);
             } else {
                 unsigned long long v = atomicExch(reinterpret_cast<unsigned long long *>(&acc[i]), 0ull);
                 host_out[i] = __longlong_as_double((long long)v);

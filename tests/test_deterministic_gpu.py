@@ -383,3 +383,21 @@ def test_batch_equals_singles_bit_for_bit(cglib):
         # energies: per-block partial sums depend on where block boundaries fall in the batch
         assert abs(Eb[j] - s.energies()[0]) <= 1e-13 * abs(Eb[j])
         off += n
+
+
+def test_random_start_large_contributions(cglib):
+    """From uniform random positions (the C2 start) near-degenerate triangles give force
+    contributions far above O(1); the deterministic mode sums them exactly (third word of the
+    fixed-point form) and the run stays finite, repeatable and equal in force to the atomic sums."""
+    pos, box = monolayer(65536, 61)
+    runs = []
+    for det in (True, True, False):
+        b = _spp_batch(pos, box, 62, det=det)
+        b.compute_forces()
+        F0 = b.forces()
+        b.spp_run(20, dt=0.01)
+        runs.append((F0, b.positions()))
+        b.close()
+    assert np.all(np.isfinite(runs[0][0])) and np.all(np.isfinite(runs[0][1]))
+    assert np.array_equal(runs[0][0], runs[1][0]) and np.array_equal(runs[0][1], runs[1][1])
+    assert force_error(runs[0][0], runs[2][0]) < 1e-12
