@@ -41,7 +41,7 @@ extern "C" int cg_autotune(cg_system *s, double *times_ms, int *choice)
     for (int shape = 0; shape < 2; ++shape) {
         for (int rep = 0; rep < 13; ++rep) {
             if (rep == 3) cudaEventRecord(e0, s->stream);
-            if (a.Ffix) cudaMemsetAsync(a.Ffix, 0, 2 * FIXW * sizeof(unsigned long long) * s->N, s->stream);
+            if (a.Ffix) cudaMemsetAsync(a.Ffix, 0, 2 * FIXF * sizeof(unsigned long long) * s->N, s->stream);
             else cudaMemsetAsync(s->F, 0, fb, s->stream);
             if (s->precision == CG_FP64) launch_groups<double, true, false>(a, s->N, s->stream, shape);
             else launch_groups<float, true, false>(a, s->N, s->stream, shape);

@@ -763,7 +763,7 @@ template <typename R>
 static void launch_force_test(cg_system *s, const VoroArgs &a, bool test)
 {
     if (a.Ffix)
-        cudaMemsetAsync(a.Ffix, 0, 2 * FIXW * sizeof(unsigned long long) * s->N, s->stream);
+        cudaMemsetAsync(a.Ffix, 0, 2 * FIXF * sizeof(unsigned long long) * s->N, s->stream);
     else
         cudaMemsetAsync(s->F, 0, (s->precision == CG_FP64 ? sizeof(double2) : sizeof(float2)) * s->N,
                         s->stream);
@@ -1320,14 +1320,14 @@ extern "C" int cg_get_energies(cg_system *s, double *E)
 // accumulator with integer atomics and F is converted from it once per force evaluation, so the
 // same inputs give bit-identical forces and trajectories on every run (the reference's kernels sum
 // each cell's force sets in a fixed order, src/models/voronoiQuadraticEnergy.cu:30-54). Costs
-// 48 bytes per cell (or vertex) and one conversion kernel per force evaluation.
+// 64 bytes per cell (or vertex) and one conversion kernel per force evaluation.
 extern "C" int cg_set_deterministic(cg_system *s, int on)
 {
     if (!s) return set_err(CG_ERR_ARG, "null system");
     on = on ? 1 : 0;
     if (on == s->det) return CG_OK;
     if (on && !s->Ffix) {
-        CG_TRY(dalloc(s, &s->Ffix, 2 * FIXW * (size_t)ndof(s)));
+        CG_TRY(dalloc(s, &s->Ffix, 2 * FIXF * (size_t)ndof(s)));
         CG_TRY(dalloc(s, &s->Efix, FIXW * (size_t)s->n_inst));
     }
     CG_CUDA(cudaStreamSynchronize(s->stream));

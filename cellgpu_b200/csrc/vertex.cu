@@ -14,7 +14,7 @@ struct VertArgs {
     const int *cell_inst, *vert_inst;
     double2 *vpos;
     double2 *F;
-    unsigned long long *Ffix;  // null, or 2 x 3 words per vertex: fixed-point sums of F (fix_add1)
+    unsigned long long *Ffix;  // null, or 2 x 4 words per vertex: fixed-point sums of F (fix_add_force)
     double2 *AP;
     const double2 *APpref;
     double KA, KP;
@@ -64,8 +64,8 @@ CG_D double vm_edge_weight(const VertArgs &a, int c, int v, int w)
 CG_D void vm_add_force(double2 *F, unsigned long long *Ffix, int v, double fx, double fy)
 {
     if (Ffix) {
-        fix_add1(Ffix + 2 * FIXW * (size_t)v, fx);
-        fix_add1(Ffix + 2 * FIXW * (size_t)v + FIXW, fy);
+        fix_add_force(Ffix + 2 * FIXF * (size_t)v, fx);
+        fix_add_force(Ffix + 2 * FIXF * (size_t)v + FIXF, fy);
     } else {
         atomicAdd(&F[v].x, fx);
         atomicAdd(&F[v].y, fy);
@@ -77,9 +77,9 @@ __global__ void k_vm_fix_forces(VertArgs a)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= a.Nv) return;
-    const ulonglong2 *w = reinterpret_cast<const ulonglong2 *>(a.Ffix) + 3 * (size_t)v;  // 2 FIXW words
-    const ulonglong2 w0 = w[0], w1 = w[1], w2 = w[2];
-    a.F[v] = make_double2(fix_value(w0.x, w0.y, w1.x), fix_value(w1.y, w2.x, w2.y));
+    const ulonglong2 *w = reinterpret_cast<const ulonglong2 *>(a.Ffix) + 4 * (size_t)v;  // 2 FIXF words
+    const ulonglong2 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
+    a.F[v] = make_double2(fix_force_value(w0, w1), fix_force_value(w2, w3));
 }
 
 __global__ void k_vm_forces(VertArgs a, int scatter)

@@ -42,7 +42,7 @@ static VertArgs vm_args(cg_system *s)
 static void launch_vm_forces(cg_system *s, const VertArgs &a)
 {
     if (a.Ffix)
-        cudaMemsetAsync(a.Ffix, 0, 2 * FIXW * sizeof(unsigned long long) * s->Nv, s->stream);
+        cudaMemsetAsync(a.Ffix, 0, 2 * FIXF * sizeof(unsigned long long) * s->Nv, s->stream);
     else
         cudaMemsetAsync(s->F, 0, sizeof(double2) * s->Nv, s->stream);
     if (s->vmax <= VM_ROW_G)

@@ -130,15 +130,36 @@ CG_D double fix_value(unsigned long long hi, unsigned long long lo, unsigned lon
     return (double)(long long)top * 0x1p35 + ((double)(long long)hi + (double)lo * 0x1p-44) * 0x1p-20;
 }
 
+// Force components take FIXF = 4 words: w[0] counts 2^-56 and takes every |x| < 2 in one atomic
+// (the common case; its resolution is FP64 rounding at 0.125), w[1..3] are the three-word form for
+// the rest. w[0] cannot overflow: the integer sum equals the sum over the contributions of the
+// cell's final rows (a retraction cancels its addition exactly), at most 33 terms below 2^57.
+constexpr int FIXF = 4;
+
+CG_D void fix_add_force(unsigned long long *w, double x)
+{
+    if (fabs(x) < 2.0) {
+        const long long f = __double2ll_rn(x * 0x1p56);
+        if (f) atomicAdd(w, (unsigned long long)f);
+        return;
+    }
+    fix_add1(w + 1, x);
+}
+
+CG_D double fix_force_value(ulonglong2 a, ulonglong2 b)  // (w[0], w[1]), (w[2], w[3])
+{
+    return (double)(long long)a.x * 0x1p-56 + fix_value(a.y, b.x, b.y);
+}
+
 // add (x, y) to the force of cell i: F += (x, y), or to its fixed-point sums. FIX = -1 decides by
 // Ffix at run time; the force pass is compiled for one mode (FIX = 0 atomics, 1 fixed point).
 template <typename R, int FIX = -1>
 CG_D void add_force(void *F, unsigned long long *Ffix, int i, R x, R y)
 {
     if (FIX == 1 || (FIX == -1 && Ffix)) {
-        unsigned long long *w = Ffix + 2 * FIXW * (size_t)i;
-        fix_add1(w, (double)x);
-        fix_add1(w + FIXW, (double)y);
+        unsigned long long *w = Ffix + 2 * FIXF * (size_t)i;
+        fix_add_force(w, (double)x);
+        fix_add_force(w + FIXF, (double)y);
     } else {
         atomic_add2<R>(F, i, x, y);
     }
@@ -1503,10 +1524,9 @@ __global__ void k_fix_forces(VoroArgs a)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.N) return;
-    const ulonglong2 *w = reinterpret_cast<const ulonglong2 *>(a.Ffix) + 3 * (size_t)i;  // 2 FIXW words
-    const ulonglong2 w0 = w[0], w1 = w[1], w2 = w[2];
-    reinterpret_cast<typename Vec2<R>::T *>(a.F)[i] =
-        mk<R>((R)fix_value(w0.x, w0.y, w1.x), (R)fix_value(w1.y, w2.x, w2.y));
+    const ulonglong2 *w = reinterpret_cast<const ulonglong2 *>(a.Ffix) + 4 * (size_t)i;  // 2 FIXF words
+    const ulonglong2 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
+    reinterpret_cast<typename Vec2<R>::T *>(a.F)[i] = mk<R>((R)fix_force_value(w0, w1), (R)fix_force_value(w2, w3));
 }
 
 // The same normals for every cell of the current step, into out[N]. The step graph runs this

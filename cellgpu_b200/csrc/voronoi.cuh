@@ -52,7 +52,7 @@ struct VoroArgs {
     double KA, KP;
     void *AP;       // double2 (FP64) or float2 (mixed)
     void *F;        // double2 (FP64) or float2 (mixed), accumulated with atomics
-    unsigned long long *Ffix;  // null, or 2 x 3 words per cell: fixed-point sums of F (order-independent)
+    unsigned long long *Ffix;  // null, or 2 x 4 words per cell: fixed-point sums of F (order-independent)
     int *nn, *nbr;
     // repair
     int *mark;

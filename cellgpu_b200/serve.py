@@ -102,7 +102,7 @@ def footprint(model, sizes, K=16, vmax=30, deterministic=False):
     else:
         base = lib.cg_vertex_footprint(len(arr), arr.ctypes.data, vmax)
         dofs = 2 * int(arr.sum())
-    det = (48 * dofs + 24 * len(arr)) if deterministic else 0
+    det = (64 * dofs + 24 * len(arr)) if deterministic else 0
     return int(base + 24 * dofs + 8 * int(arr.sum()) + 256 * len(arr) + det + (1 << 16))
 
 

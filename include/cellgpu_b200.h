@@ -196,12 +196,13 @@ int cg_set_instance_seeds(cg_system *sys, const uint64_t *seeds);
 /* Deterministic force sums (the reference's kernels sum each cell's force sets in a fixed order,
  * src/models/voronoiQuadraticEnergy.cu:30-54; Simulation::setReproducible maps here). Off (the
  * default): floating-point atomics, whose order varies, so reruns agree only to rounding and a
- * chaotic trajectory then drifts apart. On: forces are summed in fixed point, three 64-bit words
- * per component (2^-64 resolution per contribution, any finite |contribution| < 2^98, else the
- * cell's force is NaN), with integer atomics, exact in any order, so the same inputs give
- * bit-identical forces and trajectories.
+ * chaotic trajectory then drifts apart. On: forces are summed in fixed point with integer atomics,
+ * exact in any order, so the same inputs give bit-identical forces and trajectories. Four 64-bit
+ * words per component: contributions below 2 in magnitude go to one word of 2^-56 units, larger
+ * ones (any finite value below 2^98; beyond that the cell's force is NaN) to three words of 2^-64
+ * resolution.
  * FIRE's per-instance power and norm sums are then taken in a fixed order (per-block partials
- * joined by one block per instance) instead of with atomics. Allocates 48 bytes per cell (Voronoi)
+ * joined by one block per instance) instead of with atomics. Allocates 64 bytes per cell (Voronoi)
  * or vertex (vertex model) on first use; drops captured graphs. Both models. */
 int cg_set_deterministic(cg_system *sys, int on);
 int cg_get_deterministic(cg_system *sys);
