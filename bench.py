@@ -187,7 +187,7 @@ def e2e_steps(cg, torch, b, stream, steps):
 
 
 def bench_serving(n_requests, lanes=4, calib=16):
-    """C5: Poisson request stream through the continuous-batching server (cellgpu_b200.serve).
+    """Serving: Poisson request stream through the continuous-batching server (cellgpu_b200.serve).
     The arrival rate is 0.8x the service rate measured on a closed burst of `calib` requests from
     the same stream (the whole 10^4-request stream holds ~33 GB, far below 70 % of HBM, so the
     memory-filling rate of the workload spec cannot be reached; the rate saturates the GPU instead)."""
@@ -414,7 +414,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-ensemble and vertex-model measurements")
     ap.add_argument("--serve-requests", type=int, default=64,
-                    help="requests in the serving (C5) extra; 0 skips it")
+                    help="requests in the serving extra; 0 skips it")
     ap.add_argument("--serve-only", action="store_true",
                     help="run only the serving stream and print its JSON line")
     ap.add_argument("--case", default="c2", choices=["c2", "c3", "c4"],

@@ -45,13 +45,14 @@ extern "C" int cg_version(void) { return 100; }
 
 static inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
-// integrate + move: two cells per thread; 128-thread blocks spread a C2-sized pass over the 148
-// SMs in about seven blocks each (C2 step 118.7 -> 117.8 us against 256-thread blocks)
+// integrate + move: two cells per thread; 128-thread blocks spread a 262144-cell pass over the 148
+// SMs in about seven blocks each (its SPP step 118.7 -> 117.8 us against 256-thread blocks)
 constexpr int SPP_BLOCK = 128;
 
 // cells per block of the fused pass: two resident waves of blocks over the N cells (148 SMs x
 // minb blocks each), in whole groups of cells. Against one group of cells per block this cut the
-// C2 force pass from 79.2 to 75.3 us (one wave: 75.6, four: 78.3) on the same B200.
+// force pass of a 262144-cell monolayer from 79.2 to 75.3 us (one wave: 75.6, four: 78.3) on the
+// same B200.
 static inline int cells_per_block(int N, int wpb, int minb)
 {
     const int grp = wpb * GPW;

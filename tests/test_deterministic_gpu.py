@@ -386,7 +386,7 @@ def test_batch_equals_singles_bit_for_bit(cglib):
 
 
 def test_random_start_large_contributions(cglib):
-    """From uniform random positions (the C2 start) near-degenerate triangles give force
+    """From uniform random positions (how the bench's monolayer starts) near-degenerate triangles give force
     contributions far above O(1); the deterministic mode sums them exactly (third word of the
     fixed-point form) and the run stays finite, repeatable and equal in force to the atomic sums."""
     pos, box = monolayer(65536, 61)
