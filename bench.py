@@ -364,6 +364,27 @@ def replica_aggregate(total_s, done, n_cells, world, device):
     return (units / total_s if total_s > 0 else 0.0), total_s
 
 
+def bench_deterministic(cg, torch, stream, flush, precision, steps, equilibrate, sort):
+    """The same monolayer with order-independent fixed-point force sums (cg_set_deterministic, the
+    mode Simulation::setReproducible selects), prepared and timed as the main line: per-step device
+    time with the L2 flushed between steps."""
+    b = make_system(cg, torch, stream, precision, seed=1)
+    b.set_deterministic(True)
+    if equilibrate > 0:
+        b.spp_run(equilibrate, dt=DT, mu=MU)
+    if sort:
+        b.spatial_sort()
+    for _ in range(3):
+        cg._lib.check(b._lib.cg_spp_enqueue(b.handle, 1, DT, MU))
+    b._lib.cg_poll(b.handle, None, None, 1)
+    torch.cuda.synchronize()
+    total, done, _ = time_steps(cg, torch, b, stream, steps, flush)
+    b.close()
+    return {"value": N_CELLS * done / total if total > 0 else 0.0, "unit": "cell-steps/s",
+            "ms_per_step": 1e3 * total / max(done, 1), "steps": done,
+            "force_sums": "fixed point (deterministic mode)"}
+
+
 def workload_config(precision, world, sort=True, deterministic=False):
     return {"workload": "voronoi_spp_N262144_L512", "n_cells": N_CELLS, "box": BOX, "p0": P0, "v0": V0,
             "Dr": DR, "dt": DT, "precision": precision, "l2": "flushed (256 MB write) between timed steps",
@@ -530,6 +551,12 @@ def main():
     except Exception as e:
         mixed_err = {"error": str(e)}
     extras = {}
+    if not args.no_extras and world == 1 and not args.deterministic:
+        try:
+            extras["c2_deterministic"] = bench_deterministic(cg, torch, stream, flush, precision, args.steps,
+                                                             args.equilibrate, not args.no_sort)
+        except Exception as e:
+            extras["c2_deterministic"] = {"error": str(e)}
     if not args.no_extras and world == 1:
         try:
             extras["c4_ensemble"] = bench_batched(cg, torch, flush)
