@@ -337,3 +337,28 @@ def test_large_monolayer_invariants(cglib, N):
     AP = b.area_perimeter()
     assert abs(AP[:, 0].sum() - box[0] * box[1]) < 1e-6
     assert np.abs(F.sum(axis=0)).max() < 1e-8 * N
+
+
+@pytest.mark.parametrize("N", [262144])
+def test_large_monolayer_matches_oracle(cglib, oracle, N):
+    """The full-size monolayer (N = 262144, L = 512) against the oracle directly, after 20 SPP steps
+    from uniform positions (the repair's busiest regime): Delaunay rows bit-exact, A/P within
+    1e-12 relative and forces within the FP64 tolerance."""
+    pos, box = monolayer(N, 50)
+    b = _batch(pos, box)
+    pref = np.tile([1.0, 3.8], (N, 1))
+    b.set_preferences(pref)
+    b.triangulate()
+    b.spp_run(20, dt=0.01)
+    b.enforce_topology()
+    P = b.positions()
+    nn, nbr = b.topology()
+    onn, onbr = oracle.periodic_delaunay(P, box, 32)
+    m = int(max(nn.max(), onn.max()))
+    assert np.array_equal(nn, onn)
+    assert np.array_equal(canonical(nn, nbr)[:, :m], canonical(onn, onbr)[:, :m])
+    b.compute_forces()
+    AP = oracle.voronoi_geometry(P, box, onn, onbr)
+    F = oracle.voronoi_forces(P, box, onn, onbr, AP, pref)
+    np.testing.assert_allclose(b.area_perimeter(), AP, rtol=TOL_AP, atol=1e-12)
+    assert force_error(b.forces(), F) < TOL_F64
