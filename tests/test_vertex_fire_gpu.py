@@ -16,7 +16,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import canonical, force_error, jittered_lattice
+from helpers import canonical, force_error, jittered_lattice, monolayer
 
 pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -178,3 +178,36 @@ def test_fire_batch_instances_independent(cglib):
         s.fire_minimize(FireParams.defaults(force_cutoff=1e-10, max_iterations=4000))
         assert abs(s.energies()[0] - E[i]) < 1e-8 * max(1.0, E[i])
         off += n
+
+
+def test_vertex_full_size_matches_oracle(cglib, oracle, torch):
+    """The vertex workload at full size (16384 cells, L = 128, p0 ~ U[3.7, 3.9]) from the random
+    dual: the device dual equals the oracle's, and 5 Brownian steps with supplied noise (about 2300
+    T1 flips, most of them in these first steps) follow the oracle's sequential sweep: positions
+    within 1e-10, wiring and flip count exact."""
+    from cellgpu_b200 import VertexBatch
+    Nc = 16384
+    pos, box = monolayer(Nc, 70, L=128.0)
+    nn, nbr = oracle.periodic_delaunay(pos, box, 32)
+    vpos, vn, vcn, cvn, cv = oracle.vertex_from_delaunay(pos, box, nn, nbr, vmax=30)
+    b = VertexBatch([Nc], [box], vmax=30)
+    b.from_cells(pos)
+    assert np.abs(b.positions() - vpos).max() < 1e-12
+    gvn, gvcn, gcvn, gcv = b.vertex_topology()
+    assert np.array_equal(gvn, vn) and np.array_equal(gvcn, vcn) and np.array_equal(gcvn, cvn)
+    pref = np.column_stack([np.ones(Nc), np.random.default_rng(71).uniform(3.7, 3.9, Nc)])
+    b.set_preferences(pref)
+    b.set_t1_threshold(0.04)
+    steps = 5
+    noise = np.random.default_rng(72).normal(size=(steps, 2 * Nc, 2))
+    b.brownian_run(steps, dt=0.005, mu=1.0, T=1e-3,
+                   noise=torch.tensor(noise.reshape(steps, -1), device="cuda:0"))
+    F, AP, nt1 = oracle.vertex_brownian_run(vpos, box, vn, vcn, cvn, cv, pref, noise, dt=0.005, T=1e-3,
+                                           t1_threshold=0.04)
+    gvn, gvcn, gcvn, gcv = b.vertex_topology()
+    assert nt1 > 1000
+    assert b.counters()["t1_flips"] == nt1
+    assert np.abs(b.positions() - vpos).max() < 1e-10
+    assert np.array_equal(gvn, vn) and np.array_equal(gvcn, vcn) and np.array_equal(gcvn, cvn)
+    for c in range(Nc):
+        assert np.array_equal(gcv[c, :gcvn[c]], cv[c, :cvn[c]])
