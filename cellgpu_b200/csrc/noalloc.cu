@@ -1,21 +1,23 @@
 // cellgpu_b200 -- periodic Delaunay triangulation without any allocation.
 //
 // cg_voronoi_triangulate() builds a temporary system and therefore calls cudaMalloc/cudaFree. Some
-// callers cannot do that: code that enqueues work while another thread captures a CUDA graph in
-// global mode (allocation is an illegal call there), real-time loops where cudaFree's implicit
-// device synchronisation stalls every stream, and host applications that hand the library a fixed
-// device-memory budget up front (pre-partitioned memory, or another framework's caching allocator
-// that owns the heap). cg_voronoi_triangulate_noalloc() serves them: its scratch (the cell list,
-// the prefix-sum workspace and the status words) is one file-scope __device__ array of fixed size
-// that every GPU which loads this library reserves until the process exits.
+// callers cannot do that: host applications that hand the library a fixed device-memory budget up
+// front (pre-partitioned memory, or another framework's caching allocator that owns the heap),
+// loops where cudaFree's implicit device synchronisation stalls every stream, and threads that run
+// while another thread captures a CUDA graph in global mode (allocation is an illegal call for every
+// thread then). cg_voronoi_triangulate_noalloc() serves them: its scratch (the cell list, the
+// prefix-sum workspace and the status words) is one file-scope __device__ array of fixed size that
+// every GPU which loads this library reserves until the process exits.
 //
 // Limits: at most CG_NOALLOC_MAX_CELLS cells and CG_NOALLOC_MAX_BINS cell-list bins (bins are
 // about 0.8 x 0.8 in box units, so a box of area A uses about 1.56 A bins).
 //
 // Rules for callers:
+//  * The call is synchronous: it reads the status words back on `stream` and waits for them, so it
+//    cannot be captured into a graph. Beside another thread's global-mode capture, pass a
+//    cudaStreamNonBlocking stream (the legacy default stream synchronises with capturing streams).
 //  * The first call on a device resolves the array's device address with cudaGetSymbolAddress
-//    (with that device current) and sizes the scan workspace. Make that first call before any
-//    stream capture that includes this entry point.
+//    (with that device current) and sizes the scan workspace.
 //  * Every call uses the same array and leaves the previous call's contents in it; each call
 //    clears what has to start at zero. Calls that overlap on the GPU (two streams, two threads, or
 //    two devices' worth of work aimed at the same device) race on the array: serialise them.
@@ -46,19 +48,32 @@ constexpr int MAX_DEVICES = 64;
 static void *g_dev_addr[MAX_DEVICES];
 static std::mutex g_setup_mutex;
 
-// triangle-consistency and Euler count of one triangulation (status[0] != 0 on an inconsistency)
-__global__ void k_validate_one(cg::VoroArgs a, int *status, unsigned long long *zsum)
+// triangle-consistency and Euler count of one triangulation. status[0] is the star kernel's word:
+// when it reports a failure, rows may be missing or still hold the caller's old contents, so no row
+// is read. bad is set on an inconsistency. Every length and index is checked before it is used, so
+// rows that hold arbitrary values cannot send a read outside the caller's buffers.
+__global__ void k_validate_one(cg::VoroArgs a, const int *status, int *bad, unsigned long long *zsum)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.N) return;
+    if (c >= a.N || *status != 0) return;
     const int *row = a.nbr + (size_t)c * a.K;
     int z = a.nn[c];
+    if (z < 3 || z > a.K) {
+        atomicCAS(bad, 0, CG_ERR_TOPOLOGY);
+        return;
+    }
     atomicAdd(zsum, (unsigned long long)z);
     for (int k = 0; k < z; ++k) {
         int u = row[k], v = row[(k + 1) % z];
-        if (!cg::row_has_pair(a.nbr + (size_t)u * a.K, a.nn[u], v, c) ||
-            !cg::row_has_pair(a.nbr + (size_t)v * a.K, a.nn[v], c, u)) {
-            atomicCAS(status, 0, CG_ERR_TOPOLOGY);
+        bool ok = u >= 0 && u < a.N && v >= 0 && v < a.N;
+        if (ok) {
+            int zu = a.nn[u], zv = a.nn[v];
+            ok = zu >= 3 && zu <= a.K && zv >= 3 && zv <= a.K &&
+                 cg::row_has_pair(a.nbr + (size_t)u * a.K, zu, v, c) &&
+                 cg::row_has_pair(a.nbr + (size_t)v * a.K, zv, c, u);
+        }
+        if (!ok) {
+            atomicCAS(bad, 0, CG_ERR_TOPOLOGY);
             return;
         }
     }
@@ -131,7 +146,7 @@ extern "C" int cg_voronoi_triangulate_noalloc(const double *pos, int N, double L
     k_bin_scatter<<<nblk(N, 256), 256, 0, stream>>>(a);
     constexpr int WPB = 4;
     k_star_global<WPB><<<nblk(N, WPB), WPB * 32, 0, stream>>>(a, status);
-    k_validate_one<<<nblk(N, 256), 256, 0, stream>>>(a, status + 1, zsum);
+    k_validate_one<<<nblk(N, 256), 256, 0, stream>>>(a, status, status + 1, zsum);
     CG_TRY(check_launch());
     int h_status[2] = {0, 0};
     unsigned long long h_zsum = 0;

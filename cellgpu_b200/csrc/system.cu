@@ -749,6 +749,10 @@ extern "C" int cg_voronoi_triangulate(const double *pos, int N, double Lx, doubl
             break;
         }
         if ((st = triangulate_sys(s))) break;
+        if (s->K != K) {  // rows widened past the caller's capacity: the caller's buffers cannot hold them
+            st = set_err(CG_ERR_CAPACITY, "a cell has more neighbours than the row capacity K");
+            break;
+        }
         if (cudaMemcpyAsync(nn, s->nn, sizeof(int) * N, cudaMemcpyDeviceToDevice, stream) != cudaSuccess ||
             cudaMemcpyAsync(nbr, s->nbr, sizeof(int) * (size_t)N * K, cudaMemcpyDeviceToDevice, stream) !=
                 cudaSuccess)

@@ -95,22 +95,27 @@ int cg_spp_step(double *pos, double *theta, const double *F, const double *motil
 /* Periodic Delaunay triangulation of N points on the device (exact predicates), written as
  * counter-clockwise neighbour rows that start at the smallest neighbour index. Replaces the CPU/CGAL
  * voronoiModelBase::globalTriangulationCGAL (src/models/voronoiModelBase.cpp:281-351).
- * Allocates and frees its own scratch (cell list, candidate buffers). */
+ * Allocates and frees its own scratch (cell list, candidate buffers). The rows are the caller's, of
+ * capacity K: a cell with more than K neighbours returns CG_ERR_CAPACITY (retry with a larger K,
+ * as the reference grows neighMax). Synchronous: returns once the rows are written. */
 int cg_voronoi_triangulate(const double *pos, int N, double Lx, double Ly, int K, int *nn, int *nbr,
                            cudaStream_t stream);
 
 /* Allocation-free variant of cg_voronoi_triangulate. No counterpart in the reference: it exists
- * for callers that must not allocate device memory -- enqueueing while a CUDA graph is being
- * captured in global mode (cudaMalloc is illegal there), latency-critical loops where cudaFree's
- * implicit device synchronisation stalls other streams, and applications that give the library a
- * fixed device-memory budget (another allocator owns the heap). Its scratch is a file-scope
- * __device__ array of fixed size (about 2.9 MB) that each GPU loading this library keeps until
- * the process exits; inputs and outputs remain the caller's. Limits: N <= CG_NOALLOC_MAX_CELLS and
- * at most CG_NOALLOC_MAX_BINS cell-list bins (about 1.56 bins per unit of box area); larger inputs
- * get CG_ERR_CAPACITY. The first call on a device resolves the array's address with
- * cudaGetSymbolAddress and must come before any stream capture that includes this call. All calls
- * share the array (each clears what must start at zero): calls that overlap on the GPU race, so
- * serialise them. Calls no cudaMalloc, cudaFree or allocating library routine. */
+ * for callers that must not allocate device memory -- applications that give the library a fixed
+ * device-memory budget up front (another framework's caching allocator owns the heap), loops where
+ * cudaFree's implicit device synchronisation would stall every other stream, and host threads that
+ * run while another thread captures a CUDA graph in global mode (cudaMalloc is illegal for every
+ * thread then; call this on a cudaStreamNonBlocking stream, since the legacy default stream
+ * synchronises with the capturing stream). Its scratch is a file-scope __device__ array of fixed
+ * size (about 2.9 MB) that each GPU loading this library keeps until the process exits; inputs and
+ * outputs remain the caller's. Limits: N <= CG_NOALLOC_MAX_CELLS and at most CG_NOALLOC_MAX_BINS
+ * cell-list bins (about 1.56 bins per unit of box area); larger inputs get CG_ERR_CAPACITY, and so
+ * does a cell with more than K neighbours. The call is synchronous: it waits on `stream` for the
+ * status words, so it cannot itself be captured into a graph. Its first call on a device resolves
+ * the array's address with cudaGetSymbolAddress (with that device current). All calls share the
+ * array (each clears what must start at zero): calls that overlap on the GPU race, so serialise
+ * them. Calls no cudaMalloc, cudaFree or allocating library routine. */
 #define CG_NOALLOC_MAX_CELLS 65536
 #define CG_NOALLOC_MAX_BINS 131072
 int cg_voronoi_triangulate_noalloc(const double *pos, int N, double Lx, double Ly, int K, int *nn, int *nbr,

@@ -126,3 +126,23 @@ def test_rows_grow_during_steps(cglib, oracle):
     nn, nbr = b.topology()
     onn, onbr = oracle.periodic_delaunay(b.positions(), box, 32)
     assert np.array_equal(_canon(nn, nbr), _canon(onn, onbr))
+
+
+def test_raw_triangulation_reports_capacity_instead_of_widening(cglib, torch):
+    """cg_voronoi_triangulate writes into the caller's rows of capacity K. A cell with 18 Delaunay
+    neighbours and K = 16 must give CG_ERR_CAPACITY (the internal system may widen to 32, but the
+    caller's buffers cannot hold those rows), and K = 32 must succeed."""
+    pos, box = _flower()
+    N = len(pos)
+    dev = torch.device("cuda:0")
+    tpos = torch.tensor(pos, device=dev)
+    p = lambda t: C.c_void_p(t.data_ptr())
+    for K, want in ((16, -3), (32, 0)):
+        nn = torch.full((N,), -1, dtype=torch.int32, device=dev)
+        nbr = torch.full((N, K), -1, dtype=torch.int32, device=dev)
+        rc = cglib.cg_voronoi_triangulate(p(tpos), N, box[0], box[1], K, p(nn), p(nbr), None)
+        torch.cuda.synchronize()
+        assert rc == want, (K, rc, cglib.cg_last_error_string())
+        if rc == 0:
+            assert int(nn[0].item()) == 18
+            assert int(nn.sum().item()) == 6 * N
