@@ -113,32 +113,74 @@ def make_system(cg, torch, stream, precision, n_cells=N_CELLS, box=BOX, seed=1):
     return b
 
 
-def time_steps(cg, torch, b, stream, steps, flush):
-    """Per-step device time with an L2 flush between steps; returns (total_s, completed, kernels)."""
+def save_state(b, path):
+    """The prepared monolayer (positions, directors, Delaunay rows) as a compressed .npz."""
+    b.enforce_topology()
+    nn, nbr = b.topology()
+    np.savez_compressed(path, pos=b.positions(), theta=b.directors(), nn=nn, nbr=nbr)
+
+
+def load_state(cg, stream, precision, path):
+    """A system of the default workload's parameters in a state saved by save_state."""
+    d = np.load(path)
+    b = cg.VoronoiBatch([N_CELLS], [(BOX, BOX)], K=int(d["nbr"].shape[1]), precision=precision)
+    b.set_positions(d["pos"])
+    b.set_directors(d["theta"])
+    b.set_motility(np.tile([V0, DR], (N_CELLS, 1)))
+    b.set_preferences(np.tile([1.0, P0], (N_CELLS, 1)))
+    b.set_seed(1)
+    b._lib.cg_set_stream(b.handle, stream.cuda_stream)
+    b.set_topology(d["nn"], d["nbr"])
+    return b
+
+
+def time_steps(cg, torch, b, stream, steps, flush, max_attempts=8, dt=DT):
+    """Device time of `steps` completed steps with an L2 flush between steps. A step that halts (the
+    device repair could not finish it) is recovered by the host global rebuild (cg_poll), as the
+    reference falls back to globalTriangulationCGAL; the halted attempt's time and the recovery's
+    time (CUDA events around cg_poll: host round trips included) are both counted, and the halted
+    step is then run again. Returns (total_s, completed, kernels, record of halts/recovery)."""
     import ctypes as C
     lib = b._lib
-    for attempt in range(3):
+    total, done, kernels = 0.0, 0, 0
+    rec = {"attempts": 0, "halts": 0, "recovery_s": 0.0}
+    c0 = b.counters()
+    while done < steps and rec["attempts"] < max_attempts:
+        rec["attempts"] += 1
+        want = steps - done
         s0 = C.c_int(0)
-        lib.cg_poll(b.handle, C.byref(s0), None, 1)
+        lib.cg_poll(b.handle, C.byref(s0), None, 0)
         k0 = lib.cg_kernels_launched(b.handle)
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(steps)]
+              for _ in range(want)]
         with torch.cuda.stream(stream):
             torch.cuda._sleep(RUNAHEAD_CYCLES)  # let the host enqueue ahead of the device
-            for i in range(steps):
+            for i in range(want):
                 flush.zero_()
                 ev[i][0].record(stream)
-                cg._lib.check(lib.cg_spp_enqueue(b.handle, 1, DT, MU))
+                cg._lib.check(lib.cg_spp_enqueue(b.handle, 1, dt, MU))
                 ev[i][1].record(stream)
         stream.synchronize()
-        k1 = lib.cg_kernels_launched(b.handle)
+        kernels += lib.cg_kernels_launched(b.handle) - k0
         s1, h = C.c_int(0), C.c_int(0)
-        lib.cg_poll(b.handle, C.byref(s1), C.byref(h), 1)
-        done = s1.value - s0.value
-        total = sum(a.elapsed_time(e) for a, e in ev) / 1e3
-        if done == steps and not h.value:
-            return total, done, k1 - k0
-    return total, done, k1 - k0
+        lib.cg_poll(b.handle, C.byref(s1), C.byref(h), 0)
+        done += s1.value - s0.value
+        total += sum(a.elapsed_time(e) for a, e in ev) / 1e3
+        if h.value:
+            rec["halts"] += 1
+            r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            r0.record(stream)
+            cg._lib.check(lib.cg_poll(b.handle, None, None, 1))  # global rebuild
+            r1.record(stream)
+            r1.synchronize()
+            t = r0.elapsed_time(r1) / 1e3
+            rec["recovery_s"] += t
+            total += t
+    c1 = b.counters()
+    rec["global_rebuilds"] = int(c1.get("global_rebuilds", 0) - c0.get("global_rebuilds", 0))
+    rec["restarred_cells"] = int(c1.get("cells_restarred", 0) - c0.get("cells_restarred", 0))
+    rec["rows_changed"] = int(c1.get("rows_changed", 0) - c0.get("rows_changed", 0))
+    return total, done, kernels, rec
 
 
 def time_force_pass(cg, torch, b, stream, reps, flush):
@@ -237,13 +279,18 @@ def time_enqueued(torch, stream, fn, reps, flush=None):
     return sum(a.elapsed_time(e) for a, e in ev) / 1e3
 
 
-def bench_batched(cg, torch, flush, steps=40, equil=150):
-    """Batched ensemble (one system, one launch sequence per step for all instances) against the
-    plain path (one single-instance system per monolayer, steps enqueued instance by instance)."""
+def bench_batched(cg, torch, flush, steps=5000, equil=150, plain_steps=20, plain_sample=48):
+    """The batched-ensemble config: 512 monolayers run for `steps` steps in total. Batched arm: one
+    system for all instances, one launch sequence per step; the first `equil` steps from the
+    uniform random state are untimed (they rearrange the tissues wholesale), the remaining
+    steps - equil are timed with the L2 flushed between steps, halts and their recovery included
+    (time_steps). Plain arm: the single-instance drop-in, one system per monolayer, started from
+    the batched arm's equilibrated state; a sample of instances, one step of each per round, the L2
+    flushed between rounds as between the batched steps. FP64 and mixed precision."""
     import ctypes as C
     Ns, boxes, pos, theta, p0, v0 = c4_ensemble()
     total = int(Ns.sum())
-    out = {"n_instances": len(Ns), "cells": total}
+    out = {"n_instances": len(Ns), "cells": total, "steps_total": steps, "steps_untimed": equil}
     for name, prec in (("fp64", cg.CG_FP64), ("mixed", cg.CG_MIXED)):
         b = cg.VoronoiBatch(list(Ns), boxes, precision=prec)
         b.set_positions(np.concatenate(pos))
@@ -256,21 +303,18 @@ def bench_batched(cg, torch, flush, steps=40, equil=150):
         b.spp_run(equil, dt=DT, mu=MU)
         b.spatial_sort()
         out[f"batched_{name}_autotune"] = b.autotune()
-        s0 = C.c_int(0)
-        b._lib.cg_poll(b.handle, C.byref(s0), None, 1)
-        t = time_enqueued(torch, st, lambda: cg._lib.check(b._lib.cg_spp_enqueue(b.handle, 1, DT, MU)), steps, flush)
-        s1, h = C.c_int(0), C.c_int(0)
-        b._lib.cg_poll(b.handle, C.byref(s1), C.byref(h), 1)
-        done = s1.value - s0.value
+        t, done, _, rec = time_steps(cg, torch, b, st, steps - equil, flush)
         out[f"batched_{name}"] = total * done / t
         out[f"batched_{name}_ms_per_step"] = 1e3 * t / max(done, 1)
-        out[f"batched_{name}_counters"] = b.counters()
+        out[f"batched_{name}_timed_steps"] = done
+        out[f"batched_{name}_timed_window"] = rec
         if name == "fp64":
             keep_state = (b.positions(), b.directors())
         del b
-    # plain: the single-instance drop-in, one system per monolayer, sampled over a subset
+    # plain: the single-instance drop-in, one system per monolayer, sampled over a subset (the
+    # sort keeps every cell inside its instance's index range)
     rng = np.random.default_rng(11)
-    sample = rng.choice(len(Ns), 48, replace=False)
+    sample = rng.choice(len(Ns), plain_sample, replace=False)
     systems = []
     allpos, allth = keep_state
     offs = np.concatenate([[0], np.cumsum(Ns)])
@@ -285,18 +329,66 @@ def bench_batched(cg, torch, flush, steps=40, equil=150):
         s.triangulate()
         s.spp_run(5, dt=DT, mu=MU)
         systems.append(s)
-    plain_steps = 10
 
     def one_round():
         for s in systems:
             cg._lib.check(s._lib.cg_spp_enqueue(s.handle, 1, DT, MU))
 
-    t = time_enqueued(torch, st, one_round, plain_steps)
+    t = time_enqueued(torch, st, one_round, plain_steps, flush)
+    halted = 0
+    for s in systems:
+        h = C.c_int(0)
+        s._lib.cg_poll(s.handle, None, C.byref(h), 1)
+        halted += h.value
     cells = int(Ns[sample].sum())
     out["plain_fp64"] = cells * plain_steps / t
     out["plain_sample_instances"] = len(sample)
+    out["plain_steps"] = plain_steps
+    out["plain_halted_instances"] = halted
+    out["plain_l2"] = "flushed between rounds (one step of every sampled instance per round)"
     out["batched_over_plain_fp64"] = out["batched_fp64"] / out["plain_fp64"]
     out["batched_mixed_over_plain_fp64"] = out["batched_mixed"] / out["plain_fp64"]
+    return out
+
+
+def bench_c1(cg, torch, flush, steps=1000, cpu=True):
+    """The reference's own small case (plain FP64, single instance, the drop-in's latency case): N = 300
+    cells in a box of side sqrt(N) from seeded uniform positions, A0 = 1, p0 = 3.8, SPP v0 = 0.05,
+    Dr = 1, dt = 0.01, `steps` steps with a Delaunay test/repair every step. GPU: every step timed,
+    L2 flushed between steps, halts and recovery included; CPU: the reference's CPU path (local
+    test-and-repair and the default global retriangulation) on one core, same workload."""
+    n = 300
+    L = float(np.sqrt(n))
+    rng = np.random.default_rng(1)
+    b = cg.VoronoiBatch([n], [(L, L)], K=16)
+    b.set_positions(rng.random((n, 2)) * L)
+    b.set_directors(rng.uniform(0, 2 * np.pi, n))
+    b.set_motility(np.tile([0.05, 1.0], (n, 1)))
+    b.set_preferences(np.tile([1.0, 3.8], (n, 1)))
+    st = torch.cuda.Stream()
+    b._lib.cg_set_stream(b.handle, st.cuda_stream)
+    b.triangulate()
+    for _ in range(3):  # warm-up: graph capture
+        cg._lib.check(b._lib.cg_spp_enqueue(b.handle, 1, 0.01, MU))
+    b._lib.cg_poll(b.handle, None, None, 1)
+    t, done, _, rec = time_steps(cg, torch, b, st, steps, flush, dt=0.01)
+    out = {"workload": "voronoi_spp_N300 (box sqrt(300), v0 0.05, 1000 steps)", "cells": n, "steps": done,
+           "gpu_cell_steps_per_s": n * done / t, "gpu_ms_per_step": 1e3 * t / max(done, 1),
+           "timed_window": rec, "l2": "flushed between timed steps"}
+    b.close()
+    if cpu:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import ref_harness
+            if ref_harness.available():
+                loc = ref_harness.bench_c1(steps, local_repair=True)
+                glo = ref_harness.bench_c1(steps, local_repair=False)
+                out["cpu_reference_local"] = loc
+                out["cpu_reference_global"] = glo
+                best = max(loc["value"], glo["value"])
+                out["gpu_over_cpu_reference_best_mode"] = out["gpu_cell_steps_per_s"] / best
+        except Exception as e:
+            out["cpu_reference_error"] = str(e)
     return out
 
 
@@ -378,10 +470,10 @@ def bench_deterministic(cg, torch, stream, flush, precision, steps, equilibrate,
         cg._lib.check(b._lib.cg_spp_enqueue(b.handle, 1, DT, MU))
     b._lib.cg_poll(b.handle, None, None, 1)
     torch.cuda.synchronize()
-    total, done, _ = time_steps(cg, torch, b, stream, steps, flush)
+    total, done, _, rec = time_steps(cg, torch, b, stream, steps, flush)
     b.close()
     return {"value": N_CELLS * done / total if total > 0 else 0.0, "unit": "cell-steps/s",
-            "ms_per_step": 1e3 * total / max(done, 1), "steps": done,
+            "ms_per_step": 1e3 * total / max(done, 1), "steps": done, "timed_window": rec,
             "force_sums": "fixed point (deterministic mode)"}
 
 
@@ -410,14 +502,26 @@ def cpu_baseline_port(n_cells=N_CELLS, box=BOX, steps=3, seed=1):
             "sample": f"{steps} SPP steps of the N={n_cells} monolayer (full Delaunay rebuild per step)"}
 
 
-def cpu_reference(steps, all_cores=False):
+def cpu_reference(steps, all_cores=False, global_steps=0):
     """The reference's CPU path (oracle/_ref, its own sources) on a relaxed sample of the workload:
-    one instance on one core, or one instance per host core; the oracle port when _ref is absent."""
+    one instance on one core, or one instance per host core; the oracle port when _ref is absent.
+    On one core the record is the faster of the local test-and-repair mode and the default global
+    retriangulation mode (`global_steps` steps of it on the same state), with the other beside it."""
     ref = os.path.join(ROOT, "oracle", "_ref", "libcgref.so")
     if os.path.exists(ref):
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import ref_harness  # noqa
-        return ref_harness.bench_c2_all_cores(steps) if all_cores else ref_harness.bench_c2(steps)
+        if all_cores:
+            return ref_harness.bench_c2_all_cores(steps)
+        state = ref_harness.relaxed_c2_state(n_tile=N_CELLS // 16, reps=4, v0=V0, seed=1)
+        rec = ref_harness.bench_c2(steps, state=state)
+        if global_steps > 0:
+            glo = ref_harness.bench_c2(global_steps, state=state, local_repair=False)
+            rec["global_mode"] = {k: glo[k] for k in ("value", "unit", "sample")}
+            if glo["value"] > rec["value"]:  # report the faster mode as the baseline
+                glo["local_mode"] = {k: rec[k] for k in ("value", "unit", "sample")}
+                rec = glo
+        return rec
     return cpu_baseline_port(steps=steps)
 
 
@@ -446,6 +550,14 @@ def main():
                     help="time the equilibrated monolayer in its creation order (no spatial re-sort)")
     ap.add_argument("--equilibrate", type=int, default=300,
                     help="untimed SPP steps from the random initial state before warm-up")
+    ap.add_argument("--state-out", default=None,
+                    help="save the prepared (equilibrated, sorted) monolayer to this .npz")
+    ap.add_argument("--state-in", default=None,
+                    help="start from a monolayer saved by --state-out instead of preparing one "
+                         "(profiling runs: few launches before the measured ones)")
+    ap.add_argument("--force-pass-only", type=int, default=0,
+                    help="after preparing the state, launch the fused force pass this many times and "
+                         "exit (a profiler target)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -456,7 +568,7 @@ def main():
         if rank != 0:
             return
         t0 = time.perf_counter()
-        steps = max(1, min(args.steps, 3))
+        steps = max(1, min(args.steps, 20))
         base = cpu_reference(steps, all_cores=True)
         line = {"metric": METRIC, "value": base["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
                 "steps": steps, "warmup": 0, "ms_per_step": 1e3 * N_CELLS / base["value"],
@@ -498,17 +610,29 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     stream = torch.cuda.Stream()
     precision = cg.CG_FP64 if args.precision == "fp64" else cg.CG_MIXED
-    b = make_system(cg, torch, stream, precision, seed=1 + rank)
+    if args.state_in:
+        b = load_state(cg, stream, precision, args.state_in)
+    else:
+        b = make_system(cg, torch, stream, precision, seed=1 + rank)
     if args.deterministic:
         b.set_deterministic(True)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-    # relax the random initial state (untimed): its first steps rearrange the tissue wholesale
-    if args.equilibrate > 0:
-        b.spp_run(args.equilibrate, dt=DT, mu=MU)
-    # Hilbert-order the cells of the equilibrated monolayer once (untimed; the reference's
-    # spatial sorting, Simple2DCell::spatiallySortCells): neighbours sit close in memory
-    if not args.no_sort:
-        b.spatial_sort()
+    if not args.state_in:
+        # relax the random initial state (untimed): its first steps rearrange the tissue wholesale
+        if args.equilibrate > 0:
+            b.spp_run(args.equilibrate, dt=DT, mu=MU)
+        # Hilbert-order the cells of the equilibrated monolayer once (untimed; the reference's
+        # spatial sorting, Simple2DCell::spatiallySortCells): neighbours sit close in memory
+        if not args.no_sort:
+            b.spatial_sort()
+    if args.state_out and rank == 0:
+        save_state(b, args.state_out)
+    if args.force_pass_only > 0:
+        for _ in range(args.force_pass_only):
+            cg._lib.check(b._lib.cg_launch_force_pass(b.handle, 1))
+        torch.cuda.synchronize()
+        print(json.dumps({"force_pass_launches": args.force_pass_only, "n_cells": N_CELLS}))
+        return
     # warm-up (untimed; graph capture happens here)
     for _ in range(max(3, args.warmup)):
         cg._lib.check(b._lib.cg_spp_enqueue(b.handle, 1, DT, MU))
@@ -518,7 +642,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        total, done, kernels = time_steps(cg, torch, b, stream, args.steps, flush)
+        total, done, kernels, timed_window = time_steps(cg, torch, b, stream, args.steps, flush)
     torch.cuda.synchronize()
     value, total = replica_aggregate(total, done, N_CELLS, world, "cuda")
     # dominant kernel: fused geometry + force + exact test
@@ -559,6 +683,10 @@ def main():
             extras["c2_deterministic"] = {"error": str(e)}
     if not args.no_extras and world == 1:
         try:
+            extras["c1_plain"] = bench_c1(cg, torch, flush, cpu=not args.no_cpu_baseline)
+        except Exception as e:
+            extras["c1_plain"] = {"error": str(e)}
+        try:
             extras["c4_ensemble"] = bench_batched(cg, torch, flush)
         except Exception as e:
             extras["c4_ensemble"] = {"error": str(e)}
@@ -578,9 +706,11 @@ def main():
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         try:
-            cpu = cpu_reference(2)
+            cpu = cpu_reference(20, global_steps=3)
         except Exception as e:  # the baseline must not take the bench down
             cpu = {"error": str(e)}
+    c4 = extras.get("c4_ensemble", {})
+    ratios = {k: c4[k] for k in ("batched_over_plain_fp64", "batched_mixed_over_plain_fp64") if k in c4}
     prof = os.path.join(ROOT, "profiles", "force_pass_traffic.json")
     traffic = None
     if os.path.exists(prof):
@@ -599,6 +729,9 @@ def main():
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(kernels),
         "clocks": clk.summary(),
+        "batched_fp64_over_plain_fp64": ratios.get("batched_over_plain_fp64"),
+        "batched_mixed_over_plain_fp64": ratios.get("batched_mixed_over_plain_fp64"),
+        "timed_window": timed_window,
         "counters": counters,
         "equilibrate_steps": args.equilibrate,
         "mixed_force_error_vs_fp64": mixed_err,

@@ -225,30 +225,54 @@ def relaxed_c2_state(n_tile=16384, reps=4, relax_steps=120, v0=0.1, seed=1):
     return full, np.tile(th, reps * reps), Lt * reps
 
 
-def bench_c2(steps, n_cells=262144, box=512.0, v0=0.1, seed=1, barrier=None):
-    """The reference's CPU SPP path (local test-and-repair mode, as voronoi.cpp:106-107 switches to)
-    on the large monolayer in a relaxed state (relaxed_c2_state); returns the cpu_baseline record.
-    With a barrier (multi-process runs) every worker starts its timed steps together."""
+def bench_c2(steps, n_cells=262144, box=512.0, v0=0.1, seed=1, barrier=None, local_repair=True, state=None):
+    """The reference's CPU SPP path on the large monolayer in a relaxed state (relaxed_c2_state);
+    returns the cpu_baseline record. local_repair: the test-and-repair mode that voronoi.cpp:106-107
+    switches to (setCPU(false)); otherwise the reference's default CPU mode, a global
+    retriangulation every step (src/models/voronoiModelBase.cpp:556-564). With a barrier
+    (multi-process runs) every worker starts its timed steps together."""
     reps = 4
-    pos, th, L = relaxed_c2_state(n_tile=n_cells // (reps * reps), reps=reps, v0=v0, seed=seed)
+    if state is None:
+        state = relaxed_c2_state(n_tile=n_cells // (reps * reps), reps=reps, v0=v0, seed=seed)
+    pos, th, L = state
     assert abs(L - box) < 1e-9 and len(pos) == n_cells
     with quiet():
         r = RefVoronoi(n_cells)
         r.set_state(pos, th)
         r.set_motility(v0, 1.0)
-        r.spp_run(1, 0.01, True)  # first step builds the updater
+        r.spp_run(1, 0.01, local_repair)  # first step builds the updater
     if barrier is not None:
         barrier.wait()
     with quiet():
         t0 = time.perf_counter()
-        r.spp_run(steps, 0.01, True)
+        r.spp_run(steps, 0.01, local_repair)
         t1 = time.perf_counter()
     t = t1 - t0
+    mode = "local test-and-repair" if local_repair else "global retriangulation every step (default CPU mode)"
     return {"value": n_cells * steps / t, "unit": "cell-steps/s", "cores": 1, "kind": "reference",
-            "sample": f"{steps} SPP steps of the N={n_cells} monolayer, reference CPU path (local "
-                      f"test-and-repair), relaxed state (N/16 tile relaxed 120 steps by the reference, "
-                      f"tiled 4x4), 1 thread",
+            "sample": f"{steps} SPP steps of the N={n_cells} monolayer, reference CPU path ({mode}), "
+                      f"relaxed state (N/16 tile relaxed 120 steps by the reference, tiled 4x4), 1 thread",
+            "mode": "local" if local_repair else "global",
             "t0": t0, "t1": t1, "cell_steps": n_cells * steps}
+
+
+def bench_c1(steps=1000, n_cells=300, v0=0.05, seed=1, local_repair=True):
+    """The reference's own small case: N = 300 cells in a box of side sqrt(N) from seeded uniform
+    positions, A0 = 1, p0 = 3.8, SPP v0 = 0.05, Dr = 1, dt = 0.01, `steps` steps, reference CPU path,
+    one thread (local test-and-repair, or the default global retriangulation every step)."""
+    L = float(np.sqrt(n_cells))
+    rng = np.random.default_rng(seed)
+    with quiet():
+        r = RefVoronoi(n_cells)
+        r.set_state(rng.random((n_cells, 2)) * L, rng.uniform(0, 2 * np.pi, n_cells))
+        r.set_motility(v0, 1.0)
+        r.spp_run(1, 0.01, local_repair)
+        t0 = time.perf_counter()
+        r.spp_run(steps, 0.01, local_repair)
+        t1 = time.perf_counter()
+    return {"value": n_cells * steps / (t1 - t0), "unit": "cell-steps/s", "cores": 1, "kind": "reference",
+            "ms_per_step": 1e3 * (t1 - t0) / steps, "mode": "local" if local_repair else "global",
+            "sample": f"{steps} SPP steps of N={n_cells} (box sqrt(N), v0 {v0}), reference CPU path, 1 thread"}
 
 
 _BARRIER = None
