@@ -92,6 +92,8 @@ SIGNATURES = {
     "cg_set_cell_types": (_i, [_vp, _vp]),
     "cg_set_tension": (_i, [_vp, _d]),
     "cg_set_tension_matrix": (_i, [_vp, _i, _vp]),
+    "cg_set_exclusions": (_i, [_vp, _vp]),
+    "cg_get_external_forces": (_i, [_vp, _vp]),
     "cg_get_tags": (_i, [_vp, _vp]),
     "cg_get_vertex_topology": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cg_set_vertex_topology": (_i, [_vp, _vp, _vp, _vp, _vp]),

@@ -218,6 +218,15 @@ public:
         nbr.resize((size_t)Ncells * K);
         check(cg_get_topology(sys_, nn.data(), nbr.data()));
     }
+    // particle exclusions (voronoiModelBase::setExclusions, src/models/voronoiModelBase.cpp:85-104):
+    // excluded cells get v0 = Dr = 0 and, after every force evaluation, F = 0 with the computed
+    // force kept as the external force
+    void setExclusions(std::vector<int> &exes) { check(cg_set_exclusions(sys_, exes.data())); }
+    void getExternalForces(std::vector<Dscalar2> &out)
+    {
+        out.resize(Ncells);
+        check(cg_get_external_forces(sys_, reinterpret_cast<double *>(out.data())));
+    }
 
 private:
     unsigned long long seed_ = 0;

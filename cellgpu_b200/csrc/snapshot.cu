@@ -25,7 +25,8 @@ struct SnapHeader {
     double KA, KP, t1;
     unsigned long long seed;
     int has_types, tension_mode, ntypes;  // line tension
-    int flags;                            // bit 0: deterministic force sums (0 in older snapshots)
+    int flags;                            // bit 0: deterministic force sums (0 in older snapshots);
+                                          // bit 1: particle exclusions (a block of N flags, last)
     double gamma;
 };
 
@@ -46,8 +47,9 @@ void snap_layout(const SnapHeader &h, size_t sizes[10], int &count)
         size_t s[] = {N * sizeof(double2), N * sizeof(double), N * sizeof(double2), N * sizeof(double2),
                       N * sizeof(int), N * (size_t)h.K * sizeof(int),
                       h.has_types ? N * sizeof(int) : 0,
-                      h.tension_mode == 2 ? (size_t)h.ntypes * h.ntypes * sizeof(double) : 0};
-        count = 8;
+                      h.tension_mode == 2 ? (size_t)h.ntypes * h.ntypes * sizeof(double) : 0,
+                      (h.flags & 2) ? N * sizeof(int) : 0};
+        count = 9;
         for (int i = 0; i < count; ++i) sizes[i] = s[i];
     } else {
         const size_t Nv = (size_t)h.Nv;
@@ -92,7 +94,7 @@ SnapHeader snap_header(const cg_system *s)
     h.tension_mode = s->tension_mode;
     h.ntypes = s->tension_mode == 2 ? s->ntypes : 0;
     h.gamma = s->gamma;
-    h.flags = s->det ? 1 : 0;
+    h.flags = (s->det ? 1 : 0) | (s->n_excl > 0 ? 2 : 0);
     return h;
 }
 
@@ -128,7 +130,7 @@ extern "C" int cg_snapshot(cg_system *s, void *buf, size_t bytes)
     size_t sizes[10];
     int count = 0;
     snap_layout(h, sizes, count);
-    const void *src_v[] = {s->pos, s->theta, s->motility, s->APpref, s->nn, s->nbr, s->ctype, s->tmat};
+    const void *src_v[] = {s->pos, s->theta, s->motility, s->APpref, s->nn, s->nbr, s->ctype, s->tmat, s->excl};
     const void *src_m[] = {s->pos, s->theta, s->motility, s->APpref, s->vn, s->vcn, s->cvn, s->cv, s->ctype, s->tmat};
     const void *const *src = s->model == CG_MODEL_VORONOI ? src_v : src_m;
     for (int i = 0; i < count; ++i) {
@@ -146,7 +148,8 @@ extern "C" int cg_restore(const void *buf, size_t bytes, cg_system **out)
     if (memcmp(h.magic, SNAP_MAGIC, 8) != 0 || h.version != 2) return set_err(CG_ERR_ARG, "not a cellgpu_b200 snapshot");
     if (h.n_inst <= 0 || h.N <= 0 || (h.model != CG_MODEL_VORONOI && h.model != CG_MODEL_VERTEX) ||
         h.tension_mode < 0 || h.tension_mode > 2 || h.ntypes < 0 || (h.tension_mode == 2 && h.ntypes < 1) ||
-        (h.tension_mode && !h.has_types) || (h.flags & ~1) || bytes < snap_total(h))
+        (h.tension_mode && !h.has_types) || (h.flags & ~3) ||
+        ((h.flags & 2) && h.model != CG_MODEL_VORONOI) || bytes < snap_total(h))
         return set_err(CG_ERR_ARG, "corrupt or truncated snapshot");
     const unsigned char *p = static_cast<const unsigned char *>(buf) + sizeof(h);
     std::vector<int> Ns(h.n_inst);
@@ -181,7 +184,8 @@ extern "C" int cg_restore(const void *buf, size_t bytes, cg_system **out)
         snap_layout(h, sizes, count);
         if (h.has_types && (st = tension_alloc(s))) break;
         if (h.tension_mode == 2 && (st = dalloc(s, &s->tmat, (size_t)h.ntypes * h.ntypes))) break;
-        void *dst_v[] = {s->pos, s->theta, s->motility, s->APpref, s->nn, s->nbr, s->ctype, s->tmat};
+        if ((h.flags & 2) && ((st = dalloc(s, &s->excl, s->N)) || (st = dalloc(s, &s->ext_force, s->N)))) break;
+        void *dst_v[] = {s->pos, s->theta, s->motility, s->APpref, s->nn, s->nbr, s->ctype, s->tmat, s->excl};
         void *dst_m[] = {s->pos, s->theta, s->motility, s->APpref, s->vn, s->vcn, s->cvn, s->cv, s->ctype, s->tmat};
         void **dst = h.model == CG_MODEL_VORONOI ? dst_v : dst_m;
         for (int i = 0; i < count && st == CG_OK; ++i) {
@@ -189,6 +193,12 @@ extern "C" int cg_restore(const void *buf, size_t bytes, cg_system **out)
             p += sizes[i];
         }
         if (st) break;
+        if (h.flags & 2) {  // the exclusion flags are the last block
+            std::vector<int> fl(s->N);
+            memcpy(fl.data(), p - sizes[count - 1], sizeof(int) * (size_t)s->N);
+            s->n_excl = 0;
+            for (int f : fl) s->n_excl += f != 0;
+        }
         s->tension_mode = h.tension_mode;
         s->ntypes = h.ntypes;
         s->gamma = h.gamma;

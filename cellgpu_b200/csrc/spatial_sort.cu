@@ -153,6 +153,10 @@ extern "C" int cg_spatial_sort(cg_system *s)
     if (s->obs_ref) CG_TRY(sort_gather(s, s->obs_ref, sizeof(double2), order));
     if (s->ctype) CG_TRY(sort_gather(s, s->ctype, sizeof(int), order));
     if (s->TE) CG_TRY(sort_gather(s, s->TE, sizeof(double), order));
+    if (s->excl) {  // exclusions move with their cells (reIndexCellArray, voronoiModelBase.cpp:679)
+        CG_TRY(sort_gather(s, s->excl, sizeof(int), order));
+        CG_TRY(sort_gather(s, s->ext_force, sizeof(double2), order));
+    }
     // rows: old rows staged in sort_tmp (nn first, then nbr), new rows written in place
     int *nn_old = (int *)s->sort_tmp, *nbr_old = nn_old + N;
     CG_CUDA(cudaMemcpyAsync(nn_old, s->nn, sizeof(int) * N, cudaMemcpyDeviceToDevice, s->stream));

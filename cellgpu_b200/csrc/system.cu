@@ -227,7 +227,7 @@ struct cg_system {
     double *theta = nullptr;
     void *AP = nullptr, *F = nullptr;
     int *nn = nullptr, *nbr = nullptr;
-    int *mark = nullptr, *queue = nullptr, *stage_nn = nullptr, *stage_nbr = nullptr, *changed = nullptr;
+    int *mark = nullptr, *queue = nullptr, *stage_nn = nullptr, *stage_nbr = nullptr, *qslot = nullptr;
     int *held = nullptr, *undec = nullptr;
     Ctl *ctl = nullptr;
     int *bin_count = nullptr, *bin_start = nullptr, *bin_cells = nullptr, *cell_bin = nullptr,
@@ -290,6 +290,10 @@ struct cg_system {
     // observables (allocated on first use): reference positions, per-instance sums and means
     double2 *obs_ref = nullptr;
     double *obs_acc = nullptr, *obs_mean = nullptr;
+    // particle exclusions (off until set): per-cell flags, their count, external forces
+    int *excl = nullptr;
+    int n_excl = 0;
+    double2 *ext_force = nullptr;
     // FIRE (allocated on first use)
     double2 *fire_vel = nullptr;
     void *fire_st = nullptr;
@@ -377,7 +381,7 @@ static VoroArgs sys_args(cg_system *s)
     a.queue = s->queue;
     a.stage_nn = s->stage_nn;
     a.stage_nbr = s->stage_nbr;
-    a.changed = s->changed;
+    a.qslot = s->qslot;
     a.held = s->held;
     a.undec = s->undec;
     a.ctl = s->ctl;
@@ -402,7 +406,7 @@ static size_t voronoi_bytes(int N, int K, int n_bins, int n_inst, int precision)
     size_t real2 = precision == CG_FP64 ? 16 : 8;
     size_t per_cell = 4 /*cell_inst*/ + 4 /*held*/ + 4 /*undec*/ + 16 * 3 /*pos, motility, APpref*/ + 8 /*theta*/ + 2 * real2 +
                       4 + 4 * (size_t)K /*nn, nbr*/ + 4 /*mark*/ + 4 * (R_MAX + 1) /*queue*/ + 4 +
-                      4 * (size_t)K /*stage*/ + 4 * R_MAX /*changed*/ + 4 * 3 + 16 /*cell list*/ +
+                      4 * (size_t)K /*stage*/ + 4 * 2 /*qslot*/ + 4 * 3 + 16 /*cell list*/ +
                       8 + 8 /*noise staging, device draw*/;
     return per_cell * (size_t)N + (size_t)n_bins * 8 + (size_t)n_inst * (sizeof(Inst) + 16) + 4096;
 }
@@ -468,7 +472,7 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
         if ((st = dalloc(s, &s->queue, (size_t)Nt * (R_MAX + 1)))) break;
         if ((st = dalloc(s, &s->stage_nn, Nt))) break;
         if ((st = dalloc(s, &s->stage_nbr, (size_t)Nt * K))) break;
-        if ((st = dalloc(s, &s->changed, (size_t)Nt * R_MAX))) break;
+        if ((st = dalloc(s, &s->qslot, (size_t)Nt * 2))) break;
         if ((st = dalloc(s, &s->held, Nt))) break;
         if ((st = dalloc(s, &s->undec, Nt))) break;
         if ((st = dalloc(s, &s->ctl, 1))) break;
@@ -783,24 +787,27 @@ static void launch_force_test(cg_system *s, const VoroArgs &a, bool test)
 template <typename R>
 static void finish_forces(cg_system *s, const VoroArgs &a, cudaStream_t st)
 {
-    if (!a.Ffix) return;
-    k_fix_forces<R><<<nblk(s->N, 256), 256, 0, st>>>(a);
-    s->kernels_enqueued += 1;
+    if (a.Ffix) {
+        k_fix_forces<R><<<nblk(s->N, 256), 256, 0, st>>>(a);
+        s->kernels_enqueued += 1;
+    }
+    if (s->n_excl > 0) {  // excluded cells: F -> external force, F = 0
+        k_apply_exclusions<R><<<nblk(s->N, 256), 256, 0, st>>>(s->N, s->excl, a.F, s->ext_force);
+        s->kernels_enqueued += 1;
+    }
 }
 
 template <typename R, int NS>
 static void launch_round_ns(const VoroArgs &a, bool forces, cudaStream_t st, unsigned long long cond, int use_cond)
 {
     constexpr int WPB = 4;
-    // commit / check: 8 queue slots per 64-thread block, so a short queue still spreads over the SMs
+    // commit-and-check: 4 queue slots per 64-thread block, so a short queue still spreads over the SMs
     constexpr int WPB_C = 2;
     k_star_local<WPB><<<148 * STAR_MINB, WPB * 32, 0, st>>>(a);
     if (forces)
-        k_commit<R, true, WPB_C, NS><<<148 * 8, WPB_C * 32, 0, st>>>(a);
+        k_commit_check<R, true, WPB_C, NS><<<148 * 8, WPB_C * 32, 0, st>>>(a, cond, use_cond);
     else
-        k_commit<R, false, WPB_C, NS><<<148 * 8, WPB_C * 32, 0, st>>>(a);
-    k_check<WPB_C, NS><<<148 * 8, WPB_C * 32, 0, st>>>(a);
-    k_round_end<<<1, 1, 0, st>>>(a, cond, use_cond);
+        k_commit_check<R, false, WPB_C, NS><<<148 * 8, WPB_C * 32, 0, st>>>(a, cond, use_cond);
 }
 
 template <typename R>
@@ -845,7 +852,7 @@ static int reset_ctl_after_halt(cg_system *s)
     c.status = 0;
     c.n_flagged = 0;
     for (int r = 0; r <= R_MAX; ++r) c.q_count[r] = 0;
-    for (int r = 0; r < R_MAX; ++r) c.n_changed[r] = 0;
+    c.blocks_done = 0;
     c.epoch += R_MAX + 2;
     return h2d(s, s->ctl, &c, sizeof(Ctl));
 }
@@ -1293,14 +1300,14 @@ extern "C" int cg_launch_force_pass(cg_system *s, int with_test)
     return check_launch();
 }
 
-// kernels launched for this system: host-enqueued ones plus the 4 kernels of every repair round
+// kernels launched for this system: host-enqueued ones plus the 2 kernels of every repair round
 // executed inside graph WHILE nodes (counted on the device); synchronises the stream
 extern "C" long long cg_kernels_launched(cg_system *s)
 {
     if (!s) return 0;
     Ctl c;
     if (read_ctl(s, c) != CG_OK) return -1;
-    return s->kernels_enqueued + 4 * (long long)c.counters[7];
+    return s->kernels_enqueued + 2 * (long long)c.counters[7];
 }
 
 extern "C" int cg_spp_run(cg_system *s, int n_steps, double dt, double mu, const double *noise_dev)
@@ -1355,6 +1362,9 @@ extern "C" int cg_get_deterministic(cg_system *s) { return s ? s->det : 0; }
 
 // line tension
 #include "tension.cu"
+
+// particle exclusions
+#include "exclusions.cu"
 
 // snapshots and exact resume
 #include "snapshot.cu"

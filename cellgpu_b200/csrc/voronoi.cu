@@ -176,12 +176,15 @@ CG_D const Inst &inst_of(const VoroArgs &a, int c)
     return a.inst ? a.inst[a.cell_inst ? a.cell_inst[c] : 0] : a.inst0;
 }
 
-// claim cell x for epoch e (first claimer wins) and append it to queue q
+// claim cell x for epoch e (first claimer wins) and append it to queue q; its slot is recorded in
+// qslot[q & 1] (the round that reads it, q, and the round that writes the next claims, q + 1,
+// use different halves)
 CG_D void claim_enqueue(const VoroArgs &a, int x, int e, int q)
 {
     if (atomicMax(&a.mark[x], e) < e) {
         int slot = atomicAdd(&a.ctl->q_count[q], 1);
         a.queue[(size_t)q * a.N + slot] = x;
+        if (a.qslot) a.qslot[(size_t)(q & 1) * a.N + x] = slot;
     }
 }
 
@@ -755,23 +758,27 @@ __global__ void __launch_bounds__(256) k_repair_begin(VoroArgs a, unsigned long 
     }
 }
 
-__global__ void k_round_end(VoroArgs a, unsigned long long cond, int use_cond)
+// end of a repair round (one thread): count it, advance to the next round, and decide whether the
+// WHILE node runs another round; a queue that is still not empty after R_MAX rounds escalates to a
+// global rebuild
+CG_D void round_end(Ctl *ctl, unsigned long long cond, int use_cond)
 {
-    Ctl *ctl = a.ctl;
-    int r = ctl->round;
+    volatile Ctl *vc = ctl;
+    int r = vc->round;
     unsigned v = 0;
-    ctl->counters[7] += 1ull;  // executed round epilogues (4 kernels per round)
-    if (!ctl->halt) {
-        ctl->counters[1] += (unsigned long long)ctl->q_count[r];
-        if (ctl->q_count[r] > 0) ctl->counters[3] += 1ull;
+    ctl->counters[7] += 1ull;  // executed repair rounds (2 kernels each)
+    if (!vc->halt) {
+        const int qr = vc->q_count[r];
+        ctl->counters[1] += (unsigned long long)qr;
+        if (qr > 0) ctl->counters[3] += 1ull;
         int nxt = r + 1;
-        ctl->round = nxt;
-        if (ctl->q_count[nxt] > 0) {
+        vc->round = nxt;
+        if (nxt <= R_MAX && vc->q_count[nxt] > 0) {
             if (nxt >= R_MAX) {
                 // the local repair did not converge: escalate to a global rebuild
-                ctl->need_global = 1;
-                ctl->status = CG_ERR_TOPOLOGY;
-                ctl->halt = 1;
+                vc->need_global = 1;
+                vc->status = CG_ERR_TOPOLOGY;
+                vc->halt = 1;
             } else {
                 v = 1;
             }
@@ -1075,107 +1082,6 @@ __global__ void __launch_bounds__(WPB * 32, STAR_MINB) k_star_local(VoroArgs a)
     }
 }
 
-// Commit staged rows, 16 lanes per queue slot: its first 8-lane group retracts the old row's
-// contributions while the second adds the new row's (same group code as the force pass), so the two
-// run side by side; A/P are refreshed from the new row, and the old row is kept in the staging slot
-// for the consistency check. Unchanged rows whose force contributions the force pass held back add
-// them now.
-template <typename R, bool FORCES, int WPB, int NS = VG>
-__global__ void __launch_bounds__(WPB * 32) k_commit(VoroArgs a)
-{
-    __shared__ GrpTile<R, NS> tile[WPB * GPW];
-    Ctl *ctl = a.ctl;
-    if (ctl->halt) return;
-    int round = ctl->round;
-    if (round >= R_MAX) return;
-    const int nq = ctl->q_count[round];
-    const int *queue = a.queue + (size_t)round * a.N;
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int gl = lane & (G - 1), gi = lane >> 3;
-    const int sl = w * GPW + gi;
-    const bool add = gi & 1;       // group 0 of a slot: old row (retract); group 1: new row (add)
-    const int hl = lane & 15;      // lane within the slot's 16 lanes: moves row slots hl, hl + 16
-    const int step = gridDim.x * WPB * (GPW / 2);
-    for (int base = (blockIdx.x * WPB + w) * (GPW / 2); base < nq; base += step) {  // warp-uniform loop
-        const int q = base + (gi >> 1);
-        const bool live = q < nq;
-        int c = 0, zo = 0, zn = 0;
-        if (live) {
-            c = queue[q];
-            zo = a.nn[c];
-            zn = a.stage_nn[q];
-        }
-        int *row = a.nbr + (size_t)c * a.K;
-        int *srow = a.stage_nbr + (size_t)(live ? q : 0) * a.K;
-        bool diff = live && zo != zn;
-#pragma unroll
-        for (int e = hl; e < NS; e += 16)
-            if (live && !diff && e < zn && row[e] != srow[e]) diff = true;
-        int dv = diff ? 1 : 0;
-        dv |= __shfl_xor_sync(full, dv, 1);
-        dv |= __shfl_xor_sync(full, dv, 2);
-        dv |= __shfl_xor_sync(full, dv, 4);
-        dv |= __shfl_xor_sync(full, dv, 8);
-        diff = dv != 0;
-        const bool was_held = live && a.held && a.held[c];
-        double2 pc = make_double2(0, 0);
-        double Lx = 1, Ly = 1;
-        if (live) {
-            const Inst &in = inst_of(a, c);
-            Lx = in.Lx;
-            Ly = in.Ly;
-            pc = a.pos[c];
-        }
-        // retract (skipped if the force pass held the contributions back) / add and refresh A/P
-        const int *grow = add ? srow : row;
-        const int gz = add ? zn : zo;
-        const bool gok = add ? (live && (diff || (FORCES && was_held)) && zn >= 3 && zn <= NS)
-                             : (FORCES && live && diff && !was_held && zo >= 3 && zo <= NS);
-        int nbk[NS / G];
-        double A, P;
-        int fail;
-        grp_geometry<R, FORCES, false, NS>(a, c, grow, gz, gok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail, add);
-        if (FORCES) grp_scatter<R, 1, NS>(a, c, gz, gok, gl, tile[sl], nbk, A, P, add ? R(1) : R(-1));
-        if (add && gok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
-        __syncwarp();
-        // swap rows; lane hl moves slots hl and hl + 16 (both rows read before either is written)
-        int nv[NS / 16], ov[NS / 16];
-#pragma unroll
-        for (int t = 0; t < NS / 16; ++t) {
-            const int e = hl + 16 * t;
-            nv[t] = -1;
-            ov[t] = -1;
-            if (live && diff && e < a.K) {
-                nv[t] = e < zn ? srow[e] : -1;
-                ov[t] = e < zo ? row[e] : -1;
-            }
-        }
-        __syncwarp();
-#pragma unroll
-        for (int t = 0; t < NS / 16; ++t) {
-            const int e = hl + 16 * t;
-            if (live && diff && e < a.K) {
-                row[e] = nv[t];
-                srow[e] = ov[t];
-            }
-        }
-        if (live && hl == 0) {
-            if (a.held) a.held[c] = 0;
-            if (diff) {
-                a.stage_nn[q] = zo;
-                a.nn[c] = zn;
-            } else {
-                a.stage_nn[q] = -1;  // unchanged: still checked against its partners
-            }
-            int slot = atomicAdd(&ctl->n_changed[round], 1);
-            a.changed[(size_t)round * a.N + slot] = q;
-            if (diff) atomicAdd(&ctl->counters[2], 1ull);
-        }
-        __syncwarp();
-    }
-}
-
 CG_D int row_find(const int *row, int z, int v)
 {
     for (int k = 0; k < z; ++k)
@@ -1193,19 +1099,18 @@ CG_D bool row_has_pair(const int *row, int z, int u, int v)
     return row[t] == v;
 }
 
-// does the row of cell x contain u immediately followed (cyclically) by v? Rows of 16-byte aligned
-// capacity (K % 4 == 0) are read with independent 16-byte loads, so a lookup costs one memory latency.
+// does `row` (length z, capacity stride K) contain u immediately followed (cyclically) by v? Rows
+// of 16-byte aligned capacity (K % 4 == 0) are read with independent 16-byte loads, so a lookup
+// costs one memory latency.
 template <int NS = VG>
-CG_D bool pair_in_row(const VoroArgs &a, int x, int u, int v)
+CG_D bool pair_in(const int *row, int z, int K, int u, int v)
 {
-    const int *row = a.nbr + (size_t)x * a.K;
-    if ((a.K & 3) != 0) return row_has_pair(row, a.nn[x], u, v);
-    int z = a.nn[x];
+    if ((K & 3) != 0) return row_has_pair(row, z, u, v);
     int e[NS + 1];
     const int4 *r4 = reinterpret_cast<const int4 *>(row);
 #pragma unroll
     for (int j = 0; j < NS / 4; ++j) {
-        int4 t = (4 * j < a.K) ? r4[j] : make_int4(-1, -1, -1, -1);
+        int4 t = (4 * j < K) ? r4[j] : make_int4(-1, -1, -1, -1);
         e[4 * j] = t.x;
         e[4 * j + 1] = t.y;
         e[4 * j + 2] = t.z;
@@ -1219,95 +1124,196 @@ CG_D bool pair_in_row(const VoroArgs &a, int x, int u, int v)
     return found;
 }
 
-// Consistency of the processed rows of a round, one 8-lane group per row (lane = slot): every
-// triangle (c,a,b) of the row must appear in the rows of a and b, every dropped triangle must be
-// gone from them, and a changed row must pass the exact local test. Offending cells are queued for
-// the next round.
-template <int WPB, int NS = VG>
-__global__ void __launch_bounds__(WPB * 32) k_check(VoroArgs a)
+// The row cell x has at the end of the current round: its staged star when x is queued in this
+// round (queue slot from qslot, checked against the queue itself, so a stale entry from an earlier
+// round is never taken), else its current row, which no thread writes during the round.
+CG_D const int *future_row(const VoroArgs &a, int x, int round, int nq, const int *queue, int &z)
 {
-    __shared__ double2 sR[WPB * GPW][NS];
-    Ctl *ctl = a.ctl;
-    if (ctl->halt) return;
-    int round = ctl->round;
-    if (round >= R_MAX) return;
-    const int nch = ctl->n_changed[round];
-    const int e = ctl->epoch + round + 1;
-    const int nq = round + 1;
-    const int *queue = a.queue + (size_t)round * a.N;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int gl = lane & (G - 1), gi = lane >> 3;
-    const int sl = w * GPW + gi;
-    const int step = gridDim.x * WPB * GPW;
-    for (int base = (blockIdx.x * WPB + w) * GPW; base < nch; base += step) {  // warp-uniform loop
-        const int t = base + gi;
-        const bool live = t < nch;
-        int q = 0, c = 0, z = 0, zo = -1;
-        if (live) {
-            q = a.changed[(size_t)round * a.N + t];
-            c = queue[q];
-            z = a.nn[c];
-            zo = a.stage_nn[q];
-        }
-        const int *row = a.nbr + (size_t)c * a.K;
-        const int *orow = a.stage_nbr + (size_t)q * a.K;
-        const bool tested = live && zo >= 0;  // unchanged rows: nothing dropped, already tested
-        double2 pc = make_double2(0, 0);
-        double Lx = 1, Ly = 1;
-        if (tested) {
-            const Inst &in = inst_of(a, c);
-            Lx = in.Lx;
-            Ly = in.Ly;
-            pc = a.pos[c];
-        }
-        int nb[NS / G];
-#pragma unroll
-        for (int r = 0; r < NS / G; ++r) nb[r] = -1;
-#pragma unroll
-        for (int r = 0; r < NS / G; ++r) {
-            int k = gl + G * r;
-            if (live && k < z) {
-                nb[r] = row[k];
-                if (tested) sR[sl][k] = min_dist(a.pos[nb[r]], pc, Lx, Ly);
-            }
-        }
-        __syncwarp();
-        bool bad = tested && z < 3;
-#pragma unroll
-        for (int r = 0; r < NS / G; ++r) {
-            int k = gl + G * r;
-            if (live && k < z) {
-                int kp = k + 1 == z ? 0 : k + 1;
-                int u = nb[r], v = row[kp];
-                bool in_u = pair_in_row<NS>(a, u, v, c), in_v = pair_in_row<NS>(a, v, c, u);
-                if (!in_u) claim_enqueue(a, u, e, nq);
-                if (!in_v) claim_enqueue(a, v, e, nq);
-                if (tested && z >= 3) {
-                    int km = k == 0 ? z - 1 : k - 1;
-                    double2 dA = sR[sl][km], dB = sR[sl][k], dC = sR[sl][kp];
-                    if (orient0(dB, dC) <= 0 ||
-                        incircle_g(dA, dB, dC, c, row[km], u, v, a.pos, Lx, Ly) < 0)
-                        bad = true;
-                }
-            }
-            if (tested && k < zo) {
-                int u = orow[k], v = orow[k + 1 == zo ? 0 : k + 1];
-                if (!pair_in_row<NS>(a, c, u, v)) {  // dropped triangle
-                    bool in_u = pair_in_row<NS>(a, u, v, c), in_v = pair_in_row<NS>(a, v, c, u);
-                    if (in_u) claim_enqueue(a, u, e, nq);
-                    if (in_v) claim_enqueue(a, v, e, nq);
-                }
-            }
-        }
-        bad = group_any(bad);
-        if (bad) {
-            if (gl == 0) claim_enqueue(a, c, e, nq);
-#pragma unroll
-            for (int r = 0; r < NS / G; ++r)
-                if (nb[r] >= 0) claim_enqueue(a, nb[r], e, nq);
-        }
-        __syncwarp();
+    const int s = a.qslot[(size_t)(round & 1) * a.N + x];
+    if (s >= 0 && s < nq && queue[s] == x) {
+        z = a.stage_nn[s];
+        return a.stage_nbr + (size_t)s * a.K;
     }
+    z = a.nn[x];
+    return a.nbr + (size_t)x * a.K;
+}
+
+// Commit and check one repair round, 16 lanes per queue slot. Its first 8-lane group retracts the
+// old row's force contributions while the second adds the new (staged) row's, with the same group
+// code as the force pass; A/P are refreshed from the new row, which replaces the old one (padded
+// with -1). Unchanged rows whose contributions the force pass held back add them now. Then the
+// consistency check, against the rows every cell will have at the end of the round (future_row):
+// every triangle (c,u,v) of the new row must appear in the rows of u and v, every dropped triangle
+// must be gone from them, and a changed row must pass the exact local test (every edge). Offending
+// cells are claimed for the next round. The last block to finish ends the round (round_end).
+template <typename R, bool FORCES, int WPB, int NS = VG>
+__global__ void __launch_bounds__(WPB * 32) k_commit_check(VoroArgs a, unsigned long long cond, int use_cond)
+{
+    __shared__ GrpTile<R, NS> tile[WPB * GPW];
+    __shared__ int s_last;
+    Ctl *ctl = a.ctl;
+    const int round = ctl->round;
+    if (!ctl->halt && round < R_MAX) {
+        const int nq = ctl->q_count[round];
+        const int *queue = a.queue + (size_t)round * a.N;
+        const int e_next = ctl->epoch + round + 1;  // claim epoch of the next round
+        const unsigned full = 0xffffffffu;
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        const int gl = lane & (G - 1), gi = lane >> 3;
+        const int sl = w * GPW + gi;
+        const bool add = gi & 1;   // group 0 of a slot: old row (retract); group 1: new row (add)
+        const int hl = lane & 15;  // lane within the slot's 16 lanes
+        const int step = gridDim.x * WPB * (GPW / 2);
+        for (int base = (blockIdx.x * WPB + w) * (GPW / 2); base < nq; base += step) {  // warp-uniform
+            const int q = base + (gi >> 1);
+            const bool live = q < nq;
+            int c = 0, zo = 0, zn = 0;
+            if (live) {
+                c = queue[q];
+                zo = a.nn[c];
+                zn = a.stage_nn[q];
+            }
+            int *row = a.nbr + (size_t)c * a.K;
+            const int *srow = a.stage_nbr + (size_t)(live ? q : 0) * a.K;
+            bool diff = live && zo != zn;
+#pragma unroll
+            for (int e = hl; e < NS; e += 16)
+                if (live && !diff && e < zn && row[e] != srow[e]) diff = true;
+            int dv = diff ? 1 : 0;
+            dv |= __shfl_xor_sync(full, dv, 1);
+            dv |= __shfl_xor_sync(full, dv, 2);
+            dv |= __shfl_xor_sync(full, dv, 4);
+            dv |= __shfl_xor_sync(full, dv, 8);
+            diff = dv != 0;
+            const bool was_held = live && a.held && a.held[c];
+            double2 pc = make_double2(0, 0);
+            double Lx = 1, Ly = 1;
+            if (live) {
+                const Inst &in = inst_of(a, c);
+                Lx = in.Lx;
+                Ly = in.Ly;
+                pc = a.pos[c];
+            }
+            // this group's row (old or new) in registers: slot k = gl + G r and its successor
+            const int *grow = add ? srow : row;
+            const int gz = add ? zn : zo;
+            int ek[NS / G], ek1[NS / G];
+#pragma unroll
+            for (int r = 0; r < NS / G; ++r) {
+                const int k = gl + G * r;
+                ek[r] = -1;
+                ek1[r] = -1;
+                if (live && k < gz) {
+                    ek[r] = grow[k];
+                    ek1[r] = grow[k + 1 == gz ? 0 : k + 1];
+                }
+            }
+            // forces: retract the old row (unless the force pass held it back) / add the new one
+            const bool gok = add ? (live && (diff || (FORCES && was_held)) && zn >= 3 && zn <= NS)
+                                 : (FORCES && live && diff && !was_held && zo >= 3 && zo <= NS);
+            int nbk[NS / G];
+            double A, P;
+            int fail;
+            grp_geometry<R, FORCES, false, NS>(a, c, grow, gz, gok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail, add);
+            if (FORCES) grp_scatter<R, 1, NS>(a, c, gz, gok, gl, tile[sl], nbk, A, P, add ? R(1) : R(-1));
+            if (add && gok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
+            __syncwarp();
+            // the new row replaces the old one, padded with -1 (both were read above)
+            if (live && diff) {
+#pragma unroll
+                for (int t = 0; t < KMAX / 16; ++t) {
+                    const int e = hl + 16 * t;
+                    if (e < a.K) row[e] = e < zn ? srow[e] : -1;
+                }
+            }
+            if (live && hl == 0) {
+                if (a.held) a.held[c] = 0;
+                if (diff) {
+                    a.nn[c] = zn;
+                    atomicAdd(&ctl->counters[2], 1ull);
+                }
+            }
+            // consistency against the end-of-round rows
+            bool bad = false;
+            if (add) {
+                bad = live && diff && zn < 3;
+#pragma unroll
+                for (int r = 0; r < NS / G; ++r) {
+                    const int k = gl + G * r;
+                    if (live && k < zn) {
+                        const int u = ek[r], v = ek1[r];
+                        int zu, zv;
+                        const int *fu = future_row(a, u, round, nq, queue, zu);
+                        const int *fv = future_row(a, v, round, nq, queue, zv);
+                        if (!pair_in<NS>(fu, zu, a.K, v, c)) claim_enqueue(a, u, e_next, round + 1);
+                        if (!pair_in<NS>(fv, zv, a.K, c, u)) claim_enqueue(a, v, e_next, round + 1);
+                        if (diff && zn >= 3 && gok) {
+                            // exact local test of the new row (every edge): relative positions from
+                            // the group's tile (grp_geometry stored them)
+                            const int km = k == 0 ? zn - 1 : k - 1, kp = k + 1 == zn ? 0 : k + 1;
+                            const double2 dA = tile[sl].r[km], dB = tile[sl].r[k], dC = tile[sl].r[kp];
+                            const int um = srow[km];
+                            if (orient0(dB, dC) <= 0 || incircle_g(dA, dB, dC, c, um, u, v, a.pos, Lx, Ly) < 0)
+                                bad = true;
+                        }
+                    }
+                }
+            } else if (live && diff) {
+                // dropped triangles of the old row must be gone from the partners' rows
+#pragma unroll
+                for (int r = 0; r < NS / G; ++r) {
+                    const int k = gl + G * r;
+                    if (k < zo) {
+                        const int u = ek[r], v = ek1[r];
+                        if (!pair_in<NS>(srow, zn, a.K, u, v)) {
+                            int zu, zv;
+                            const int *fu = future_row(a, u, round, nq, queue, zu);
+                            const int *fv = future_row(a, v, round, nq, queue, zv);
+                            if (pair_in<NS>(fu, zu, a.K, v, c)) claim_enqueue(a, u, e_next, round + 1);
+                            if (pair_in<NS>(fv, zv, a.K, c, u)) claim_enqueue(a, v, e_next, round + 1);
+                        }
+                    }
+                }
+            }
+            bad = group_any(bad);
+            if (add && bad) {
+                if (gl == 0) claim_enqueue(a, c, e_next, round + 1);
+#pragma unroll
+                for (int r = 0; r < NS / G; ++r)
+                    if (ek[r] >= 0) claim_enqueue(a, ek[r], e_next, round + 1);
+            }
+            __syncwarp();
+        }
+    }
+    // the last block to finish ends the round (threadfence reduction: every block's claims are
+    // visible before its count is)
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&ctl->blocks_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        ctl->blocks_done = 0;
+        round_end(ctl, cond, use_cond);
+    }
+}
+
+// Particle exclusions (voronoiModelBase::setExclusions, src/models/voronoiModelBase.cpp:85-104, and
+// the summation with exclusions, src/models/voronoiQuadraticEnergy.cpp:368-377 /
+// gpu_sum_forces_with_exclusions_kernel, src/models/voronoiQuadraticEnergy.cu:59-93): once a force
+// evaluation is complete, an excluded cell's net force is kept as the external force -F and its
+// force is zeroed; other cells keep their external force at zero.
+template <typename R>
+__global__ void k_apply_exclusions(int N, const int *excl, void *F, double2 *ext)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N || !excl[c]) return;
+    typename Vec2<R>::T *f = reinterpret_cast<typename Vec2<R>::T *>(F) + c;
+    const typename Vec2<R>::T v = *f;
+    ext[c] = make_double2(-(double)v.x, -(double)v.y);
+    *f = mk<R>(R(0), R(0));
 }
 
 // end of a step: reset the per-step queue counters and advance the claim epoch
@@ -1318,7 +1324,6 @@ __global__ void k_step_done(Ctl *ctl, int advance_step)
     if (ctl->n_flagged) atomicAdd(&ctl->counters[0], (unsigned long long)ctl->n_flagged);
     ctl->n_flagged = 0;
     for (int r = 0; r <= R_MAX; ++r) ctl->q_count[r] = 0;
-    for (int r = 0; r < R_MAX; ++r) ctl->n_changed[r] = 0;
     ctl->round = 0;
     ctl->epoch += R_MAX + 2;
 }

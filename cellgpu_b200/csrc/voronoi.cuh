@@ -31,12 +31,12 @@ struct Ctl {
     int n_flagged;           // cells flagged by the test of this step
     int n_undec;             // entries of VoroArgs::undec written by the test of this step
     int q_count[R_MAX + 1];  // per-round queue lengths
-    int n_changed[R_MAX];    // per-round changed rows
     int step;                // completed integrator steps since creation
     int round;               // current local-repair round of this step
+    unsigned blocks_done;    // blocks of the current commit-and-check launch that have finished
     unsigned long long counters[8];  // 0 tests failed, 1 cells restarred, 2 rows changed, 3 rounds,
                                      // 4 global rebuilds, 5 T1 flips, 6 fire iterations,
-                                     // 7 executed repair-round epilogues
+                                     // 7 executed repair rounds (2 kernels each)
 };
 
 // everything a Voronoi kernel needs, passed by value
@@ -59,7 +59,7 @@ struct VoroArgs {
     int *queue;     // (R_MAX+1) * N
     int *stage_nn;  // N
     int *stage_nbr; // N * K
-    int *changed;   // R_MAX * N  (queue slots whose rows changed)
+    int *qslot;     // 2 * N: queue slot of each cell claimed for a round, by round parity
     int *held;      // N: 1 while a cell's contributions are held back (its own row failed the test)
     int *undec;     // N: slots (c * 16 + k) whose in-circle sign the filter left undecided, or null
     Ctl *ctl;

@@ -70,6 +70,23 @@ class VoronoiBatch:
         """gamma per unit length on every edge between cells of different types (0: off)."""
         check(self._lib.cg_set_tension(self._h, float(gamma)))
 
+    def set_exclusions(self, excluded):
+        """Particle exclusions (voronoiModelBase::setExclusions): cells with excluded[c] != 0 get
+        zero motility and, after every force evaluation, F = 0 with the computed force kept as the
+        external force -F. None clears the flags."""
+        if excluded is None:
+            check(self._lib.cg_set_exclusions(self._h, None))
+            return
+        e = np.ascontiguousarray(excluded, np.int32).reshape(-1)
+        if e.size != self.Ntot:
+            raise ValueError("one flag per cell")
+        check(self._lib.cg_set_exclusions(self._h, ptr(e)))
+
+    def external_forces(self):
+        out = np.zeros((self.Ntot, 2))
+        check(self._lib.cg_get_external_forces(self._h, ptr(out)))
+        return out
+
     def set_tension_matrix(self, gamma):
         """symmetric ntypes x ntypes matrix of edge tensions between types (empty: off)."""
         g = np.ascontiguousarray(gamma, dtype=np.float64)
@@ -424,6 +441,16 @@ class VoronoiQuadraticEnergy:
 
     def neighbors(self):
         return self.batch.topology()
+
+    def setExclusions(self, exes):
+        """voronoiModelBase::setExclusions (src/models/voronoiModelBase.cpp:85-104): cells with
+        exes[i] != 0 stop self-propelling (v0 = Dr = 0); their force is zeroed after every force
+        evaluation and kept as the external force (returnExternalForces)."""
+        self.batch.set_exclusions(exes)
+        self.forcesUpToDate = False
+
+    def returnExternalForces(self):
+        return self.batch.external_forces()
 
 
 Voronoi2D = VoronoiQuadraticEnergy

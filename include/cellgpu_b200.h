@@ -314,6 +314,18 @@ int cg_set_cell_types(cg_system *sys, const int *types);
 int cg_set_tension(cg_system *sys, double gamma);
 int cg_set_tension_matrix(cg_system *sys, int ntypes, const double *gamma);
 
+/* Particle exclusions (voronoiModelBase::setExclusions, src/models/voronoiModelBase.cpp:85-104, and
+ * the force summation with exclusions, gpu_sum_force_sets_with_exclusions,
+ * inc/models/voronoiQuadraticEnergy.cuh:41-54 / src/models/voronoiQuadraticEnergy.cpp:119-135,
+ * 368-377): cells with excluded[c] != 0 get zero motility (v0 = Dr = 0) now, and after every force
+ * evaluation their net force F is stored as the external force -F and F is set to 0, so they
+ * neither self-propel nor respond to forces. excluded = NULL clears every flag (motility is left as
+ * it is, as in the reference). The flags move with their cells under spatial sorting and are kept
+ * in snapshots. cg_get_external_forces copies the external forces, (x, y) per cell (0 for cells
+ * that are not excluded), to a host buffer of 2N doubles. Voronoi systems only. */
+int cg_set_exclusions(cg_system *sys, const int *excluded);
+int cg_get_external_forces(cg_system *sys, double *out);
+
 /* Autotuner (no counterpart in the reference): times the runtime-selectable launch parameters on
  * the system's current state and keeps the fastest -- the fused force pass's block shape (0: 2 warps
  * per block, 1: 4 warps) and the global triangulation's cell-list bin side (0: 0.8, 1: 1.0, 2: 1.25

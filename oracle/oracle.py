@@ -236,6 +236,34 @@ def voronoi_spp_run(pos, box, nn, nbr, theta, motility, APpref, noise, dt=0.01, 
     return F, AP
 
 
+def apply_exclusions(F, excluded):
+    """Particle exclusions after a force evaluation (src/models/voronoiQuadraticEnergy.cpp:368-377,
+    gpu_sum_forces_with_exclusions_kernel, src/models/voronoiQuadraticEnergy.cu:59-93): an excluded
+    cell's force becomes the external force -F and its force is zeroed. Returns (F, external)."""
+    ex = np.asarray(excluded) != 0
+    F = np.array(F, dtype=np.float64, copy=True)
+    ext = np.zeros_like(F)
+    ext[ex] = -F[ex]
+    F[ex] = 0.0
+    return F, ext
+
+
+def voronoi_spp_run_exclusions(pos, box, nn, nbr, theta, motility, APpref, noise, excluded, dt=0.01, mu=1.0,
+                               KA=1.0, KP=1.0):
+    """voronoi_spp_run with particle exclusions (motility must already hold v0 = Dr = 0 for the
+    excluded cells, as voronoiModelBase::setExclusions sets it, src/models/voronoiModelBase.cpp:85-104):
+    per step the geometry, the forces, the exclusions, one SPP step, and the Delaunay triangulation
+    of the new positions, in place. Returns (F, external, AP) of the last force evaluation."""
+    noise = _f64(noise).reshape(-1, pos.shape[0])
+    F = ext = AP = None
+    for t in range(noise.shape[0]):
+        AP = voronoi_geometry(pos, box, nn, nbr)
+        F, ext = apply_exclusions(voronoi_forces(pos, box, nn, nbr, AP, APpref, KA, KP), excluded)
+        spp_step(pos, box, F, theta, motility, noise[t], dt, mu)
+        nn[:], nbr[:] = periodic_delaunay(pos, box, nbr.shape[1])
+    return F, ext, AP
+
+
 def vertex_from_delaunay(pos, box, nn, nbr, vmax=30):
     pos = _f64(pos)
     N = pos.shape[0]

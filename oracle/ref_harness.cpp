@@ -15,6 +15,7 @@
 #include "EnergyMinimizerFIRE2D.h"
 #include "Simulation.h"
 #include "brownianParticleDynamics.h"
+#include "dynamicalFeatures.h"
 #include "selfPropelledParticleDynamics.h"
 #include "vertexQuadraticEnergy.h"
 #include "voronoiQuadraticEnergy.h"
@@ -139,6 +140,46 @@ double ref_voronoi_forces(void *h, double *F, double *AP)
     to_host(s->voro->returnForces(), reinterpret_cast<Dscalar2 *>(F), n);
     to_host(s->voro->returnAreaPeri(), reinterpret_cast<Dscalar2 *>(AP), n);
     return s->voro->computeEnergy();
+}
+
+// particle exclusions (voronoiModelBase::setExclusions) and the external forces the force
+// summation with exclusions stores for the excluded cells
+void ref_voronoi_set_exclusions(void *h, const int *exes)
+{
+    RefSystem *s = reinterpret_cast<RefSystem *>(h);
+    int n = s->voro->getNumberOfDegreesOfFreedom();
+    std::vector<int> e(exes, exes + n);
+    s->voro->setExclusions(e);
+}
+
+void ref_voronoi_external_forces(void *h, double *out)
+{
+    RefSystem *s = reinterpret_cast<RefSystem *>(h);
+    int n = s->voro->getNumberOfDegreesOfFreedom();
+    to_host(s->voro->external_forces, reinterpret_cast<Dscalar2 *>(out), n);
+}
+
+// the reference's observables on the current state: Simple2DCell::reportq, reportVarq and
+// reportVarAP (after a force evaluation, which refreshes the areas and perimeters), and
+// dynamicalFeatures::computeMSD / computeOverlapFunction of the current positions against `initial`
+void ref_voronoi_observables(void *h, const double *initial, double cutoff, double *out)
+{
+    RefSystem *s = reinterpret_cast<RefSystem *>(h);
+    int n = s->voro->getNumberOfDegreesOfFreedom();
+    s->voro->computeForces();
+    out[0] = s->voro->reportq();
+    out[1] = s->voro->reportVarq();
+    Dscalar2 v = s->voro->reportVarAP();
+    out[2] = v.x;
+    out[3] = v.y;
+    GPUArray<Dscalar2> init((unsigned int)n, false);
+    {
+        ArrayHandle<Dscalar2> hi(init, access_location::host, access_mode::overwrite);
+        for (int i = 0; i < n; ++i) hi.data[i] = make_Dscalar2(initial[2 * i], initial[2 * i + 1]);
+    }
+    dynamicalFeatures dyn(init, s->voro->Box);
+    out[4] = dyn.computeMSD(s->voro->cellPositions);
+    out[5] = dyn.computeOverlapFunction(s->voro->cellPositions, cutoff);
 }
 
 // state read-back: positions, directors, neighbour rows (K per row, -1 padded)

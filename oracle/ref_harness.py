@@ -34,6 +34,9 @@ def lib():
         L.ref_voronoi_forces.restype = C.c_double
         L.ref_voronoi_forces.argtypes = [C.c_void_p, _dp, _dp]
         L.ref_voronoi_get.argtypes = [C.c_void_p, _dp, C.c_void_p, C.c_int, _ip, _ip]
+        L.ref_voronoi_set_exclusions.argtypes = [C.c_void_p, _ip]
+        L.ref_voronoi_external_forces.argtypes = [C.c_void_p, _dp]
+        L.ref_voronoi_observables.argtypes = [C.c_void_p, _dp, C.c_double, _dp]
         L.ref_voronoi_spp_run.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
         L.ref_fire.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                C.c_double, C.c_int, C.c_double, C.c_int]
@@ -129,6 +132,21 @@ class RefVoronoi:
         AP = np.zeros((self.N, 2))
         E = lib().ref_voronoi_forces(self.h, F, AP)
         return F, AP, E
+
+    def set_exclusions(self, exes):
+        lib().ref_voronoi_set_exclusions(self.h, np.ascontiguousarray(exes, np.int32))
+
+    def external_forces(self):
+        out = np.zeros((self.N, 2))
+        lib().ref_voronoi_external_forces(self.h, out)
+        return out
+
+    def observables(self, initial, cutoff=0.5):
+        """reportq, reportVarq, reportVarAP (A, P) and dynamicalFeatures' MSD and overlap against
+        `initial`, on the current state."""
+        out = np.zeros(6)
+        lib().ref_voronoi_observables(self.h, np.ascontiguousarray(initial, np.float64), cutoff, out)
+        return dict(zip(("mean_q", "var_q", "var_A", "var_P", "msd", "overlap"), out))
 
     def state(self, K=16):
         pos = np.zeros((self.N, 2))

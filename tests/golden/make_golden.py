@@ -5,7 +5,7 @@ compiled in place from its sources by oracle/Makefile.ref (with the DelaunayCGAL
 oracle/shim) into oracle/_ref/libcgref.so. Run from the repository root, where the reference
 sources are available:
 
-    make -C oracle -f Makefile.ref && python tests/golden/make_golden.py
+    make -C oracle -f Makefile.ref && python tests/golden/make_golden.py [voronoi vertex fire tension exclusions observables]
 
 Each .npz holds the inputs and the reference's outputs of one case (small sizes, seeded).
 """
@@ -44,6 +44,53 @@ def voronoi_case(N, seed, steps, v0=0.05, dt=0.01):
     np.savez_compressed(os.path.join(HERE, f"voronoi_N{N}_s{seed}.npz"), N=N, box=np.array([L, L]), pos=pos,
                         theta=theta, v0=v0, Dr=1.0, dt=dt, steps=steps, noise=noise, F0=F0, AP0=AP0, E0=E0,
                         nn0=nn0, nbr0=nbr0, pos1=pos1, theta1=th1, nn1=nn1, nbr1=nbr1, F1=F1, AP1=AP1, E1=E1)
+
+
+def exclusions_case(N=400, seed=9, steps=5, v0=0.05, dt=0.01, every=7):
+    """Particle exclusions (voronoiModelBase::setExclusions): every `every`-th cell excluded; forces and
+    external forces on the initial state, then `steps` SPP steps (local repair) and the same again."""
+    L = float(np.sqrt(N))
+    rng = np.random.default_rng(seed)
+    pos = rng.random((N, 2)) * L
+    theta = rng.uniform(0, 2 * np.pi, N)
+    exes = (np.arange(N) % every == 3).astype(np.int32)
+    with quiet():
+        r = R.RefVoronoi(N)
+        r.set_state(pos, theta)
+        r.set_motility(v0, 1.0)
+        r.set_exclusions(exes)
+        F0, AP0, E0 = r.forces()
+        ext0 = r.external_forces()
+        r.spp_run(steps, dt, True)
+        pos1, th1, nn1, nbr1 = r.state()
+        F1, AP1, E1 = r.forces()
+        ext1 = r.external_forces()
+    noise = R.reproducible_normals(steps * N).reshape(steps, N)
+    np.savez_compressed(os.path.join(HERE, f"exclusions_N{N}_s{seed}.npz"), N=N, box=np.array([L, L]), pos=pos,
+                        theta=theta, v0=v0, Dr=1.0, dt=dt, steps=steps, noise=noise, exes=exes, F0=F0, ext0=ext0,
+                        AP0=AP0, E0=E0, pos1=pos1, theta1=th1, nn1=nn1, nbr1=nbr1, F1=F1, ext1=ext1)
+
+
+def observables_case(N=500, seed=11, steps=40, v0=0.3, dt=0.01):
+    """The reference's observables (Simple2DCell::reportq / reportVarq / reportVarAP and
+    dynamicalFeatures::computeMSD / computeOverlapFunction with cutoff 0.5) after `steps` SPP steps
+    from seeded uniform positions, with the positions before and after and the reference's A/P."""
+    L = float(np.sqrt(N))
+    rng = np.random.default_rng(seed)
+    pos = rng.random((N, 2)) * L
+    theta = rng.uniform(0, 2 * np.pi, N)
+    with quiet():
+        r = R.RefVoronoi(N)
+        r.set_state(pos, theta)
+        r.set_motility(v0, 1.0)
+        pos0, _, _, _ = r.state()
+        r.spp_run(steps, dt, True)
+        obs = r.observables(pos0, 0.5)
+        pos1, th1, nn1, nbr1 = r.state()
+        F1, AP1, E1 = r.forces()
+    np.savez_compressed(os.path.join(HERE, f"observables_N{N}_s{seed}.npz"), N=N, box=np.array([L, L]), pos0=pos0,
+                        pos1=pos1, nn1=nn1, nbr1=nbr1, AP1=AP1, cutoff=0.5,
+                        **{k: np.float64(v) for k, v in obs.items()})
 
 
 def vertex_case(Nc, steps, dt=0.005, T=1e-3, t1=0.04, seed=2):
@@ -135,11 +182,14 @@ def vertex_tension_case(Nc, seed):
 if __name__ == "__main__":
     if not R.available():
         raise SystemExit("oracle/_ref/libcgref.so missing: make -C oracle -f Makefile.ref")
-    voronoi_case(300, 1, 20)
-    voronoi_case(1000, 2, 10, v0=0.3)
-    vertex_case(400, 15)
-    fire_case(200, 3)
-    fire_case(200, 4, vertex=True)
-    tension_case(400, 5)
-    vertex_tension_case(300, 7)
+    cases = {
+        "voronoi": lambda: (voronoi_case(300, 1, 20), voronoi_case(1000, 2, 10, v0=0.3)),
+        "vertex": lambda: vertex_case(400, 15),
+        "fire": lambda: (fire_case(200, 3), fire_case(200, 4, vertex=True)),
+        "tension": lambda: (tension_case(400, 5), vertex_tension_case(300, 7)),
+        "exclusions": lambda: exclusions_case(),
+        "observables": lambda: observables_case(),
+    }
+    for name in sys.argv[1:] or list(cases):  # python make_golden.py [case ...]
+        cases[name]()
     print("golden fixtures written to", HERE)

@@ -186,3 +186,47 @@ def test_live_reference_spp_matches_oracle(oracle):
                            noise)
     assert np.abs(pos - p1).max() < 1e-11
     assert np.array_equal(canonical(nn, nbr), canonical(nn1, nbr1))
+
+
+def test_exclusions_golden(oracle):
+    """Particle exclusions (voronoiModelBase::setExclusions) against the reference's own outputs:
+    forces and external forces on the initial state, then SPP steps with the reference's deviates."""
+    g = _load("exclusions_N*.npz")[0]
+    N, box = int(g["N"]), tuple(g["box"])
+    ex = g["exes"]
+    pos = g["pos"].copy()
+    nn, nbr = oracle.periodic_delaunay(pos, box, 16)
+    pref = np.tile([1.0, 3.8], (N, 1))
+    AP = oracle.voronoi_geometry(pos, box, nn, nbr)
+    F, ext = oracle.apply_exclusions(oracle.voronoi_forces(pos, box, nn, nbr, AP, pref), ex)
+    assert np.all(F[ex != 0] == 0.0)
+    assert force_error(F, g["F0"]) < 1e-12
+    assert force_error(ext[ex != 0], g["ext0"][ex != 0]) < 1e-12 and np.all(g["ext0"][ex == 0] == 0.0)
+    theta = g["theta"].copy()
+    mot = np.tile([float(g["v0"]), float(g["Dr"])], (N, 1))
+    mot[ex != 0] = 0.0
+    F1, ext1, _ = oracle.voronoi_spp_run_exclusions(pos, box, nn, nbr, theta, mot, pref, g["noise"], ex,
+                                                    dt=float(g["dt"]))
+    assert np.abs(pos - g["pos1"]).max() < 1e-11
+    assert np.array_equal(canonical(nn, nbr), canonical(g["nn1"], g["nbr1"]))
+    AP = oracle.voronoi_geometry(pos, box, nn, nbr)
+    F, ext = oracle.apply_exclusions(oracle.voronoi_forces(pos, box, nn, nbr, AP, pref), ex)
+    assert force_error(F, g["F1"]) < 1e-10
+    assert force_error(ext[ex != 0], g["ext1"][ex != 0]) < 1e-10
+
+
+def test_observables_golden():
+    """The host formulas the observables tests use (mean and variance of q = P/sqrt(A), variances of
+    A and P, minimum-image MSD and overlap) reproduce the reference's own reportq / reportVarq /
+    reportVarAP and dynamicalFeatures outputs on the fixture."""
+    g = _load("observables_N*.npz")[0]
+    AP, box = g["AP1"], np.asarray(g["box"])
+    q = AP[:, 1] / np.sqrt(AP[:, 0])
+    d = g["pos1"] - g["pos0"]
+    d -= box * np.round(d / box)
+    r2 = np.sum(d * d, axis=1)
+    ref = {"mean_q": q.mean(), "var_q": np.mean((q - q.mean()) ** 2),
+           "var_A": np.mean((AP[:, 0] - AP[:, 0].mean()) ** 2), "var_P": np.mean((AP[:, 1] - AP[:, 1].mean()) ** 2),
+           "msd": r2.mean(), "overlap": np.mean(np.sqrt(r2) < float(g["cutoff"]))}
+    for k, v in ref.items():
+        assert abs(v - float(g[k])) <= 1e-12 * max(1.0, abs(v)), k

@@ -62,3 +62,31 @@ def test_vertex_observables(cglib):
     b.compute_forces()
     obs = b.observables(cutoff=0.02)
     _check(obs, 0, _host_obs(b.area_perimeter(), b.positions(), V0, box, 0.02))
+
+
+def _golden():
+    import glob
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    return dict(np.load(sorted(glob.glob(os.path.join(here, "observables_N*.npz")))[0]))
+
+
+def test_voronoi_observables_match_reference(cglib):
+    """Against the reference's own Simple2DCell::reportq / reportVarq / reportVarAP and
+    dynamicalFeatures::computeMSD / computeOverlapFunction (tests/golden/observables_N500_s11.npz):
+    the reference's state after 40 SPP steps, with its starting positions as the MSD reference.
+    Tolerance 1e-12 relative (summation order); overlap exact."""
+    from cellgpu_b200 import VoronoiBatch
+    g = _golden()
+    N, box = int(g["N"]), tuple(g["box"])
+    b = VoronoiBatch([N], [box])
+    b.set_positions(g["pos0"])
+    b.set_reference_positions()
+    b.set_positions(g["pos1"])
+    b.triangulate()
+    b.compute_forces()
+    obs = b.observables(cutoff=float(g["cutoff"]))
+    assert np.abs(b.area_perimeter() - g["AP1"]).max() < 1e-12
+    for k in ("mean_q", "var_q", "var_A", "var_P", "msd"):
+        assert abs(obs[k][0] - float(g[k])) <= 1e-12 * max(1.0, abs(float(g[k]))), k
+    assert obs["overlap"][0] == float(g["overlap"])

@@ -4,10 +4,12 @@ Tolerances (written here, used below):
   * topology (Delaunay neighbour rows, canonical rotation): bit-exact;
   * FP64 forces: force_error <= 1e-10 (max |dF| / max(|F|, RMS F); summation order differs);
   * FP64 areas/perimeters: relative 1e-12;
-  * mixed precision forces vs FP64 on a relaxed monolayer: RMS error <= 1e-6 and max <= 1e-5
-    (vertex geometry in FP64, energy derivatives and contractions in FP32; near force balance the
-    forces are differences of terms up to ~100x larger, so FP32 rounding of those terms bounds the
-    max error near 5e-6 -- measured and stated, not hidden).
+  * mixed precision forces vs FP64 on a relaxed monolayer: norm-wise max |dF| / max |F| <= 1e-6,
+    RMS error <= 1e-6 and per-cell max (the force_error normalisation) <= 1e-5. The per-cell
+    maximum does not reach 1e-6: near force balance a cell's force is the sum of ~18 terms about ten
+    times its size, and FP32 rounding of those terms alone leaves ~1e-6 to 5e-6 per cell
+    (tests/test_precision_study.py shows it on the oracle's own arithmetic). FP64 is the mode that
+    meets 1e-6 per cell; the mixed mode is measured and stated, not tuned to pass.
 """
 import ctypes as C
 
@@ -20,6 +22,7 @@ pytestmark = pytest.mark.gpu
 
 TOL_F64 = 1e-10
 TOL_AP = 1e-12
+TOL_MIXED_NORMWISE = 1e-6
 TOL_MIXED_RMS = 1e-6
 TOL_MIXED_MAX = 1e-5
 
@@ -277,7 +280,10 @@ def test_mixed_precision_force_error(cglib, oracle):
     err_relaxed = force_error(b32.forces(), F64)
     scale = np.sqrt(np.mean(np.sum(F64 ** 2, axis=1)))
     rms = np.sqrt(np.mean(np.sum((b32.forces() - F64) ** 2, axis=1))) / scale
-    print(f"mixed force error: random {err_random:.2e}, relaxed max {err_relaxed:.2e} rms {rms:.2e}")
+    normwise = np.linalg.norm(b32.forces() - F64, axis=1).max() / np.linalg.norm(F64, axis=1).max()
+    print(f"mixed force error: random {err_random:.2e}, relaxed max {err_relaxed:.2e} rms {rms:.2e} "
+          f"norm-wise {normwise:.2e}")
+    assert normwise < TOL_MIXED_NORMWISE
     assert rms < TOL_MIXED_RMS
     assert err_relaxed < TOL_MIXED_MAX
     assert err_random < TOL_MIXED_MAX
