@@ -361,6 +361,7 @@ static VoroArgs sys_args(cg_system *s)
 {
     VoroArgs a;
     memset(&a, 0, sizeof(a));
+    a.rows_padded = 1;  // every writer of system rows pads them with -1
     a.N = s->N;
     a.K = s->K;
     a.n_inst = s->n_inst;

@@ -418,10 +418,14 @@ struct GrpTile {
 // Phases A-C of one group's cell (called by the whole warp; `ok` switches a group off): relative
 // neighbour positions (FP64, the exact Delaunay inputs), Voronoi vertices, A, P, the exact local
 // test (TEST) and the edge unit vectors (SCATTER). nbk receives the neighbours of the lane's slots.
+// pre0: row[gl] when the caller has already loaded it (padded rows, loaded beside the row length so
+// that the neighbour gather waits for one load instead of two), else NO_PRE.
+constexpr int NO_PRE = -2;
+
 template <typename R, bool SCATTER, bool TEST, int NS = VG>
 CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok, double2 pc, double Lx,
                        double Ly, int gl, GrpTile<R, NS> &T, int (&nbk)[NS / G], double &A, double &P, int &fail,
-                       bool store_te = true)
+                       bool store_te = true, int pre0 = NO_PRE)
 {
     using V = typename Vec2<R>::T;
 #pragma unroll
@@ -429,7 +433,7 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
         int k = gl + G * r;
         nbk[r] = -1;
         if (ok && k < z) {
-            nbk[r] = row[k];
+            nbk[r] = (r == 0 && pre0 != NO_PRE) ? pre0 : row[k];
             T.r[k] = min_dist(a.pos[nbk[r]], pc, Lx, Ly);
         }
     }
@@ -535,14 +539,16 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
 // vertex, and the scatter of SIGN x (contribution) to the cell and its neighbours.
 template <typename R, int SIGN, int NS = VG, int FIX = -1>
 CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<R, NS> &T, const int (&nbk)[NS / G],
-                      double A, double P, R sgn = R(SIGN))
+                      double A, double P, R sgn = R(SIGN), bool have_pref = false,
+                      double2 pref = double2())
 {
     using V = typename Vec2<R>::T;
     __syncwarp();
     R Adiff = 0, Pdiff = 0;
     if (ok) {
-        Adiff = (R)(a.KA * (A - a.APpref[c].x));
-        Pdiff = (R)(a.KP * (P - a.APpref[c].y));
+        const double2 pp = have_pref ? pref : a.APpref[c];  // (A0, P0): the force pass loads it early
+        Adiff = (R)(a.KA * (A - pp.x));
+        Pdiff = (R)(a.KP * (P - pp.y));
     }
     R sx = 0, sy = 0;
     V cb[NS / G];
@@ -619,30 +625,34 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int 
     for (int base = blockIdx.x * cpb + w * GPW; base < c_end; base += WPB * GPW) {  // warp-uniform
         const int c = base + gi;
         bool live = c < c_end && !halted;
-        int z = 0;
-        double2 pc = make_double2(0, 0);
+        int z = 0, pre0 = NO_PRE;
+        double2 pc = make_double2(0, 0), pref = make_double2(0, 0);
         double Lx = 1, Ly = 1;
         const int *row = nullptr;
         if (live) {
+            // independent loads, issued together: position, row length, first row entry (rows of
+            // the system are padded, so it needs no length), preferences
+            row = a.nbr + (size_t)c * a.K;
+            pc = a.pos[c];
+            z = a.nn[c];
+            if (CG_FP_PRE_ROW && a.rows_padded && gl < a.K) pre0 = row[gl];
+            if (SCATTER && CG_FP_PRE_PREF) pref = a.APpref[c];
             const Inst &in = inst_of(a, c);
             Lx = in.Lx;
             Ly = in.Ly;
-            pc = a.pos[c];
-            z = a.nn[c];
-            row = a.nbr + (size_t)c * a.K;
         }
         const bool ok = live && z >= 3 && z <= NS;
         int nbk[NS / G];
         double A, P;
         int fail;
-        grp_geometry<R, SCATTER, TEST, NS>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail);
+        grp_geometry<R, SCATTER, TEST, NS>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail, true, pre0);
         if (ok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
         // A cell whose own row fails the test holds its contributions back: the row is about to be
         // replaced, and a stale row can contain a nearly collinear triangle whose Jacobians (1/cross^2)
         // would swamp the forces. The repair commit adds the contributions of the new row.
         bool hold = SCATTER && TEST && a.held && ok && fail != 0x7fffffff;
         if (hold && gl == 0) a.held[c] = 1;
-        if (SCATTER) grp_scatter<R, 1, NS, FIX>(a, c, z, ok && !hold, gl, tile[sl], nbk, A, P);
+        if (SCATTER) grp_scatter<R, 1, NS, FIX>(a, c, z, ok && !hold, gl, tile[sl], nbk, A, P, R(1), CG_FP_PRE_PREF != 0, pref);
         if (TEST && live && gl == 0 && (fail != 0x7fffffff || !ok)) {
             if (!ok) {
                 if (a.ctl) {

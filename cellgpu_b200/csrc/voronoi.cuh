@@ -21,6 +21,14 @@ constexpr int CAND_GLOBAL = 384;  // candidate slots per warp for the cell-list 
 #endif
 #define CG_FORCE_WPB_ALT 4
 #define CG_FORCE_MINB_ALT 8
+// the fused pass loads a cell's first row entry (CG_FP_PRE_ROW) and its preferences
+// (CG_FP_PRE_PREF) beside its position and row length, ahead of the geometry
+#ifndef CG_FP_PRE_ROW
+#define CG_FP_PRE_ROW 1
+#endif
+#ifndef CG_FP_PRE_PREF
+#define CG_FP_PRE_PREF 1
+#endif
 
 // device control block of one system
 struct Ctl {
@@ -54,6 +62,7 @@ struct VoroArgs {
     void *F;        // double2 (FP64) or float2 (mixed), accumulated with atomics
     unsigned long long *Ffix;  // null, or 2 x 4 words per cell: fixed-point sums of F (order-independent)
     int *nn, *nbr;
+    int rows_padded;  // rows hold -1 past their length (system rows): a row can be read before its length
     // repair
     int *mark;
     int *queue;     // (R_MAX+1) * N
