@@ -102,6 +102,10 @@ SIGNATURES = {
     "cg_vertex_spp_run": (_i, [_vp, _i, _d, _d, _vp]),
     "cg_set_t1_threshold": (_i, [_vp, _d]),
     "cg_fire_minimize": (_i, [_vp, _vp]),
+    "cg_fire_begin": (_i, [_vp, _vp]),
+    "cg_fire_advance": (_i, [_vp, _vp, _i, _vp]),
+    "cg_fire_begin_instances": (_i, [_vp, _vp, _i, _i]),
+    "cg_copy_instances": (_i, [_vp, _i, _vp, _i, _i]),
     "cg_fire_state": (_i, [_vp, _vp, _vp, _vp]),
 }
 

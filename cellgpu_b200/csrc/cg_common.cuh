@@ -26,6 +26,8 @@ struct Inst {
     double bsx, bsy;    // bin sides
     int voff, nv;       // vertex-model vertices (off/n are cells)
     unsigned long long seed;  // Philox key of the instance's device noise (counters are local indices)
+    unsigned step_off;  // added to the system's step counter in the noise counters: the instance's own
+                        // step count when it joined this system (0 for an instance created here)
 };
 
 // SplitMix64 finaliser (G. Steele, D. Lea, C. Flood, "Fast splittable pseudorandom number

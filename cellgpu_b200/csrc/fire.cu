@@ -259,11 +259,16 @@ __global__ void k_fire_update(FireArgs a, unsigned long long *iter_counter)
     st.fmax_bits = 0;
 }
 
-__global__ void k_fire_init(FireArgs a)
+// fresh FIRE state for the instances in [lo, hi) (all of them at the start of a minimisation; the
+// newly admitted ones when a serving batch is rebuilt around running instances)
+__global__ void k_fire_init(FireArgs a, int lo, int hi)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < a.ndof) a.vel[i] = make_double2(0.0, 0.0);
-    if (i < a.n_inst) {
+    if (i < a.ndof) {
+        const int d = a.dof_inst[i];
+        if (d >= lo && d < hi) a.vel[i] = make_double2(0.0, 0.0);
+    }
+    if (i >= lo && i < hi) {
         FireInst s;
         s.dt = a.prm.dt;
         s.alpha = a.prm.alpha_start;

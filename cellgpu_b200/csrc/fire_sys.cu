@@ -91,7 +91,9 @@ static void fire_enqueue_iteration(cg_system *s, const cg_fire_params &prm)
     s->kernels_enqueued += 3;
 }
 
-extern "C" int cg_fire_minimize(cg_system *s, const cg_fire_params *prm)
+// Start a minimisation: per-instance FIRE state reset (EnergyMinimizerFIRE's initial dt, alpha and
+// counters) and the forces of the current state (minimize's computeForces before the loop)
+extern "C" int cg_fire_begin(cg_system *s, const cg_fire_params *prm)
 {
     if (!s || !prm || prm->max_iterations < 0 || !(prm->dt > 0)) return set_err(CG_ERR_ARG, "bad args");
     if (!s->topology_valid) {
@@ -100,14 +102,49 @@ extern "C" int cg_fire_minimize(cg_system *s, const cg_fire_params *prm)
     }
     CG_TRY(fire_alloc(s));
     FireArgs f = fire_args(s, *prm);
-    k_fire_init<<<nblk(std::max(ndof(s), s->n_inst), 256), 256, 0, s->stream>>>(f);
+    k_fire_init<<<nblk(std::max(ndof(s), s->n_inst), 256), 256, 0, s->stream>>>(f, 0, s->n_inst);
     fire_forces(s, false);
-    CG_TRY(check_launch());
+    return check_launch();
+}
+
+// Fresh FIRE state for instances [first, first + count) only, the others keeping theirs, and the
+// forces of the current state: instances admitted into a batch whose other instances are already
+// minimising (serving). cg_fire_advance then continues all of them.
+extern "C" int cg_fire_begin_instances(cg_system *s, const cg_fire_params *prm, int first, int count)
+{
+    if (!s || !prm || prm->max_iterations < 0 || !(prm->dt > 0) || first < 0 || count < 0 ||
+        first + count > s->n_inst)
+        return set_err(CG_ERR_ARG, "bad args");
+    if (!s->topology_valid) {
+        if (s->model == CG_MODEL_VORONOI) CG_TRY(triangulate_sys(s));
+        else return set_err(CG_ERR_STATE, "vertex topology not set");
+    }
+    CG_TRY(fire_alloc(s));
+    FireArgs f = fire_args(s, *prm);
+    k_fire_init<<<nblk(std::max(ndof(s), s->n_inst), 256), 256, 0, s->stream>>>(f, first, first + count);
+    fire_forces(s, false);
+    return check_launch();
+}
+
+// Continue a minimisation started by cg_fire_begin for up to `iterations` more iterations of every
+// instance (in graphs of 16; instances that have converged or reached max_iterations stay frozen),
+// or until every instance has stopped. *n_stopped (may be NULL) receives the number of stopped
+// instances. Calls with the same parameters continue the same trajectory, so running a
+// minimisation in pieces gives the same result as one cg_fire_minimize call.
+extern "C" int cg_fire_advance(cg_system *s, const cg_fire_params *prm, int iterations, int *n_stopped)
+{
+    if (!s || !prm || iterations < 0) return set_err(CG_ERR_ARG, "bad args");
+    if (!s->fire_st) return set_err(CG_ERR_STATE, "cg_fire_begin first");
+    FireArgs f = fire_args(s, *prm);
     std::vector<FireInst> st(s->n_inst);
     const int chunk = 16;
-    int rounds = 0;
-    for (;;) {
-        // a graph of `chunk` iterations (direct launches of the same kernels if capture is refused)
+    int rounds = 0, stopped = 0;
+    for (int done = 0;; done += chunk) {
+        CG_TRY(d2h(s, st.data(), s->fire_st, sizeof(FireInst) * s->n_inst));
+        stopped = 0;
+        for (auto &x : st) stopped += x.converged ? 1 : 0;
+        if (stopped == s->n_inst || done >= iterations) break;
+        // a graph of `chunk` iterations
         cudaGraphExec_t exec = nullptr;
         long long nk = 0;
         for (auto &g : s->graphs)
@@ -134,10 +171,11 @@ extern "C" int cg_fire_minimize(cg_system *s, const cg_fire_params *prm)
         Ctl c;
         CG_TRY(read_ctl(s, c));
         if (c.halt) {
-            // a Voronoi step needed a global rebuild: rebuild, recompute forces and finish the
-            // halted iteration (its first half-kick and move already happened)
-            if (s->model != CG_MODEL_VORONOI) return vm_check_halt(s);
-            CG_TRY(recover(s));
+            // a Voronoi step needed a global rebuild, or a vertex T1 sweep wider rows: fix it,
+            // recompute forces and finish the halted iteration (its first half-kick and move
+            // already happened)
+            if (s->model == CG_MODEL_VORONOI) CG_TRY(recover(s));
+            else CG_TRY(vm_recover(s, nullptr));
             fire_forces(s, false);
             int nd = ndof(s);
             fire_vv2_reduce(s, f);
@@ -145,13 +183,16 @@ extern "C" int cg_fire_minimize(cg_system *s, const cg_fire_params *prm)
             k_fire_update<<<nblk(s->n_inst, 64), 64, 0, s->stream>>>(f, &s->ctl->counters[6]);
             CG_TRY(check_launch());
         }
-        CG_TRY(d2h(s, st.data(), s->fire_st, sizeof(FireInst) * s->n_inst));
-        bool all = true;
-        for (auto &x : st) all = all && x.converged;
-        if (all) break;
         if (++rounds > prm->max_iterations / chunk + 64) return set_err(CG_ERR_STATE, "FIRE did not stop");
     }
+    if (n_stopped) *n_stopped = stopped;
     return CG_OK;
+}
+
+extern "C" int cg_fire_minimize(cg_system *s, const cg_fire_params *prm)
+{
+    CG_TRY(cg_fire_begin(s, prm));
+    return cg_fire_advance(s, prm, prm->max_iterations + 16 * 64, nullptr);
 }
 
 extern "C" int cg_fire_state(cg_system *s, int *iterations, double *fmax_cpu, double *fnorm_gpu)

@@ -31,7 +31,8 @@ struct SnapHeader {
 };
 
 struct SnapInst {
-    int n, pad;
+    int n;
+    unsigned step_off;  // the instance's noise step offset (0 in older snapshots)
     double Lx, Ly;
     unsigned long long seed;
 };
@@ -124,6 +125,7 @@ extern "C" int cg_snapshot(cg_system *s, void *buf, size_t bytes)
         r.Lx = s->h_inst[i].Lx;
         r.Ly = s->h_inst[i].Ly;
         r.seed = s->h_inst[i].seed;
+        r.step_off = s->h_inst[i].step_off;
         memcpy(p, &r, sizeof(r));
         p += sizeof(r);
     }
@@ -155,6 +157,7 @@ extern "C" int cg_restore(const void *buf, size_t bytes, cg_system **out)
     std::vector<int> Ns(h.n_inst);
     std::vector<double> boxes(2 * (size_t)h.n_inst);
     std::vector<uint64_t> seeds(h.n_inst);
+    std::vector<unsigned> step_offs(h.n_inst);
     long long total = 0;
     for (int i = 0; i < h.n_inst; ++i) {
         SnapInst r;
@@ -164,6 +167,7 @@ extern "C" int cg_restore(const void *buf, size_t bytes, cg_system **out)
         boxes[2 * i] = r.Lx;
         boxes[2 * i + 1] = r.Ly;
         seeds[i] = r.seed;
+        step_offs[i] = r.step_off;
         total += r.n;
     }
     if (total != h.N) return set_err(CG_ERR_ARG, "corrupt snapshot (instance sizes)");
@@ -175,6 +179,7 @@ extern "C" int cg_restore(const void *buf, size_t bytes, cg_system **out)
     int st = CG_OK;
     do {
         s->seed = h.seed;
+        for (int i = 0; i < h.n_inst; ++i) s->h_inst[i].step_off = step_offs[i];
         if ((st = cg_set_instance_seeds(s, seeds.data()))) break;
         s->KA = h.KA;
         s->KP = h.KP;

@@ -272,7 +272,7 @@ struct cg_system {
     // vertex model (model == CG_MODEL_VERTEX): pos/F are per vertex, AP/APpref/theta/motility per cell
     int Nv = 0, vmax = 0;
     int *vert_inst = nullptr, *vn = nullptr, *vcn = nullptr, *cvn = nullptr, *cv = nullptr;
-    int *t1_cand = nullptr, *t1_count = nullptr;
+    int *t1_cand = nullptr, *t1_count = nullptr, *t1_resume = nullptr;
     double t1 = 0.01;  // vertexModelBase default (src/models/vertexModelBase.cpp:59)
     // line tension (off until set): per-cell types, mode, gamma or gamma matrix, per-cell term
     int tension_mode = 0, ntypes = 0;
@@ -1366,6 +1366,9 @@ extern "C" int cg_get_deterministic(cg_system *s) { return s ? s->det : 0; }
 
 // particle exclusions
 #include "exclusions.cu"
+
+// moving instances between systems (continuous batching)
+#include "batching.cu"
 
 // snapshots and exact resume
 #include "snapshot.cu"

@@ -25,6 +25,8 @@ struct VertArgs {
     double t1;
     int *cand;        // 3*Nv edge keys (3*v + slot), instance i at 3 * (its first vertex)
     int *cand_count;  // n_inst
+    int *t1_resume;   // 2 * n_inst: keys of an interrupted sweep kept at the start of the instance's
+                      // cand region, (sorted candidates, keys queued by flips); (0, 0) = none
     Ctl *ctl;
     // line tension (VertexQuadraticEnergyWithTension): per-cell types, one gamma (mode 1) or a
     // symmetric ntypes x ntypes matrix (mode 2); TE[c] = sum over the cell's unlike edges of gamma l
@@ -245,7 +247,7 @@ __global__ void k_vm_brownian(VertArgs a, const double *noise2, double dt, doubl
         r2 = noise2[2 * (size_t)v + 1];
     } else {
         // counter = the vertex's index within its instance, key = the instance's seed
-        double2 g = normal2(in.seed, (uint32_t)(v - in.voff), a.ctl ? (uint32_t)a.ctl->step : 0u, 1u);
+        double2 g = normal2(in.seed, (uint32_t)(v - in.voff), (a.ctl ? (uint32_t)a.ctl->step : 0u) + in.step_off, 1u);
         r1 = g.x;
         r2 = g.y;
     }
@@ -296,7 +298,7 @@ __global__ void k_vm_spp_directors(VertArgs a, const double *noise, double dt)
         xi = noise[c];
     } else {
         const Inst &in = a.inst[a.cell_inst[c]];
-        xi = normal2(in.seed, (uint32_t)(c - in.off), a.ctl ? (uint32_t)a.ctl->step : 0u, 2u).x;
+        xi = normal2(in.seed, (uint32_t)(c - in.off), (a.ctl ? (uint32_t)a.ctl->step : 0u) + in.step_off, 2u).x;
     }
     a.theta[c] = __dadd_rn(a.theta[c], __dmul_rn(xi, sqrt(__dmul_rn(__dmul_rn(2.0, dt), a.motility[c].y))));
 }
@@ -628,8 +630,12 @@ CG_D void t1_requeue(const VertArgs &a, const Inst &in, int key, int vertex2, co
 }
 
 // the whole sweep by one thread over the candidate keys q[0, nc) (sorted here); used when the
-// candidates do not fit the shared-memory path
-CG_D void t1_sweep_serial(const VertArgs &a, const Inst &in, int *q, int nc, int &flips, int &status)
+// candidates do not fit the shared-memory path, and to resume an interrupted sweep. A flip that
+// would overflow a cell row stops it before changing anything; the keys still to visit (that one
+// first) are then moved to q[0, m) and resume[0] = m, so the sweep can continue once the rows have
+// grown (the reference grows cellVertices at that point, src/models/vertexModelBase.cpp:474-500)
+CG_D void t1_sweep_serial(const VertArgs &a, const Inst &in, int *q, int nc, int &flips, int &status,
+                          int *resume)
 {
     const int cap = 3 * in.nv;
     for (int i = 1; i < nc; ++i) {
@@ -647,6 +653,12 @@ CG_D void t1_sweep_serial(const VertArgs &a, const Inst &in, int *q, int nc, int
         int cs[4] = {0, 0, 0, 0}, vs[4] = {0, 0, 0, 0}, vertex2 = 0;
         int r = t1_try(a, in, key, cs, vs, vertex2);
         if (r < 0) {
+            const int m = n - (head - 1);
+            for (int t = 0; t < m; ++t) q[t] = q[head - 1 + t];  // forward: never overtakes its source
+            if (resume) {
+                resume[0] = m;
+                resume[1] = 0;
+            }
             status = CG_ERR_CAPACITY;
             return;
         }
@@ -914,7 +926,8 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
     int *q = a.cand + 3 * (size_t)in.voff;
     int flips = 0, status = 0;
     if (nc > T1_CAP) {
-        if (threadIdx.x == 0) t1_sweep_serial(a, in, q, nc, flips, status);
+        if (threadIdx.x == 0)
+            t1_sweep_serial(a, in, q, nc, flips, status, a.t1_resume ? a.t1_resume + 2 * inst : nullptr);
     } else {
         int P = 1;
         while (P < nc) P <<= 1;
@@ -1005,6 +1018,18 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
                     __syncwarp();
                 }
                 if (r < 0) {
+                    // a cell row would overflow: keep the keys still to visit for a resumed sweep
+                    // once the rows have grown -- the sorted candidates from this one on (A), then
+                    // the keys queued by flips (B); B may sit in q above A, and the forward copy
+                    // never overtakes its source
+                    if (lane == 0 && a.t1_resume) {
+                        const bool from_ex = idx < 0;
+                        int na = 0, nb = 0;
+                        for (int t = from_ex ? hm : hm - 1; t < nc; ++t) q[na++] = s_key[t];
+                        for (int t = from_ex ? eh - 1 : eh; t < en; ++t) q[na + nb++] = ex[t];
+                        a.t1_resume[2 * inst] = na;
+                        a.t1_resume[2 * inst + 1] = nb;
+                    }
                     status = CG_ERR_CAPACITY;
                     break;
                 }
@@ -1043,6 +1068,45 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
         if (status && ctl) {
             atomicExch(&ctl->status, status);
             atomicExch(&ctl->halt, 1);
+        }
+    }
+}
+
+// Continue the sweeps that a row overflow interrupted, after the rows have grown: per instance with
+// keys kept (t1_resume), one thread merges the two sorted runs (A then B, in cand) into one sorted
+// list without repeats and runs the rest of the sweep on the current state, as the CPU sweep
+// continues after growing its rows. Launched with T1_SMEM bytes of dynamic shared memory.
+__global__ void k_vm_t1_resume(VertArgs a)
+{
+    extern __shared__ __align__(16) unsigned char t1_smem[];
+    int *buf = reinterpret_cast<int *>(t1_smem);  // T1_SMEM / 4 >= 2 T1_CAP ints
+    const int inst = blockIdx.x;
+    if (threadIdx.x != 0) return;
+    int *res = a.t1_resume + 2 * inst;
+    const int na = res[0], nb = res[1];
+    if (na + nb == 0) return;
+    const Inst &in = a.inst[inst];
+    int *q = a.cand + 3 * (size_t)in.voff;
+    int flips = 0, status = 0;
+    res[0] = res[1] = 0;
+    if (na + nb > 2 * T1_CAP) {
+        status = CG_ERR_CAPACITY;  // too many keys to merge here: the step fails as before
+    } else {
+        for (int t = 0; t < na + nb; ++t) buf[t] = q[t];
+        int i = 0, j = na, m = 0;
+        while (i < na || j < na + nb) {
+            int k;
+            if (j >= na + nb || (i < na && buf[i] <= buf[j])) k = buf[i++];
+            else k = buf[j++];
+            if (m == 0 || q[m - 1] != k) q[m++] = k;
+        }
+        t1_sweep_serial(a, in, q, m, flips, status, res);
+    }
+    if (a.ctl) {
+        atomicAdd(&a.ctl->counters[5], (unsigned long long)flips);
+        if (status) {
+            atomicExch(&a.ctl->status, status);
+            atomicExch(&a.ctl->halt, 1);
         }
     }
 }

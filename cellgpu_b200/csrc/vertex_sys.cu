@@ -27,6 +27,7 @@ static VertArgs vm_args(cg_system *s)
     a.t1 = s->t1;
     a.cand = s->t1_cand;
     a.cand_count = s->t1_count;
+    a.t1_resume = s->t1_resume;
     a.ctl = s->ctl;
     a.tension_mode = s->tension_mode;
     a.ntypes = s->ntypes;
@@ -101,6 +102,7 @@ extern "C" int cg_vertex_create(int n_inst, const int *Nc, const double *box, in
     s->Nv = 2 * off;
     // the T1 sweep stages up to T1_CAP candidates per instance in dynamic shared memory
     cudaFuncSetAttribute(k_vm_t1_replay, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T1_SMEM);
+    cudaFuncSetAttribute(k_vm_t1_resume, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T1_SMEM);
     int st = sys_streams(s);
     if (st != CG_OK) {
         sys_release(s);
@@ -122,6 +124,7 @@ extern "C" int cg_vertex_create(int n_inst, const int *Nc, const double *box, in
         if ((st = dalloc(s, &s->cv, (size_t)s->N * vmax))) break;
         if ((st = dalloc(s, &s->t1_cand, 3 * (size_t)s->Nv))) break;
         if ((st = dalloc(s, &s->t1_count, n_inst))) break;
+        if ((st = dalloc(s, &s->t1_resume, 2 * (size_t)n_inst))) break;
         if ((st = dalloc(s, &s->ctl, 1))) break;
         if ((st = dalloc(s, &s->d_energy, n_inst))) break;
         if ((st = dalloc(s, &s->noise_buf, 2 * (size_t)s->Nv))) break;
@@ -283,12 +286,56 @@ static int vm_check_halt(cg_system *s)
                                                  : "vertex model step failed");
 }
 
+// Cell rows grow from vmax to vmax2 entries (copied, padded with -1); captured graphs, which hold
+// the old rows and width, are dropped. The reference grows cellVertices the same way when a T1
+// transition needs it (vertexModelBase::growCellVerticesList, src/models/vertexModelBase.cpp:474-500).
+static int vm_grow_rows(cg_system *s, int vmax2)
+{
+    CG_CUDA(cudaStreamSynchronize(s->stream));
+    for (auto &g : s->graphs) release_graph(g);
+    s->graphs.clear();
+    int *cv2 = nullptr;
+    CG_TRY(dalloc(s, &cv2, (size_t)s->N * vmax2));
+    k_widen_rows<<<nblk(s->N, 256), 256, 0, s->stream>>>(s->N, s->vmax, vmax2, s->cv, cv2);
+    CG_TRY(check_launch());
+    s->cv = cv2;  // (the old block stays in the arena until the system is destroyed)
+    s->vmax = s->K = vmax2;
+    return cg_synchronize(s);
+}
+
+// After a halt: a T1 sweep that stopped because a flip would overflow a cell row kept the keys it
+// had still to visit; grow the rows and finish the sweep (repeatedly, if it stops again). Other
+// halts are errors. Returns CG_OK when the system runs on.
+static int vm_recover(cg_system *s, bool *recovered)
+{
+    if (recovered) *recovered = false;
+    for (int attempt = 0; attempt < 16; ++attempt) {
+        Ctl c;
+        CG_TRY(read_ctl(s, c));
+        if (!c.halt) return CG_OK;
+        std::vector<int> res(2 * (size_t)s->n_inst);
+        CG_TRY(d2h(s, res.data(), s->t1_resume, sizeof(int) * res.size()));
+        bool pending = false;
+        for (int v : res) pending = pending || v > 0;
+        if (c.status != CG_ERR_CAPACITY || !pending) return vm_check_halt(s);
+        CG_TRY(vm_grow_rows(s, s->vmax + 4));
+        c.halt = 0;
+        c.status = 0;
+        CG_TRY(h2d(s, s->ctl, &c, sizeof(Ctl)));
+        k_vm_t1_resume<<<s->n_inst, 32, T1_SMEM, s->stream>>>(vm_args(s));
+        s->kernels_enqueued += 1;
+        CG_TRY(check_launch());
+        if (recovered) *recovered = true;
+    }
+    return set_err(CG_ERR_CAPACITY, "vertex rows kept overflowing after growing");
+}
+
 static int vm_enforce(cg_system *s)
 {
     VertArgs a = vm_args(s);
     vm_launch_t1(s, a);
     CG_TRY(check_launch());
-    return vm_check_halt(s);
+    return vm_recover(s, nullptr);
 }
 
 // one integrator step of the vertex model: forces, integrate + move, T1 sweep
@@ -316,6 +363,9 @@ static int vm_run(cg_system *s, int kind, int n_steps, double dt, double mu, dou
 {
     if (!s->topology_valid) return set_err(CG_ERR_STATE, "vertex topology not set");
     const int chunk = 32;  // graphs of 32, 16, ..., 1 steps: any n_steps reuses at most six graphs
+    Ctl c0;
+    CG_TRY(read_ctl(s, c0));
+    int step_prev = c0.step;
     for (int done = 0; done < n_steps;) {
         int todo = chunk;
         while (todo > n_steps - done) todo >>= 1;
@@ -347,8 +397,20 @@ static int vm_run(cg_system *s, int kind, int n_steps, double dt, double mu, dou
             s->kernels_enqueued += nk;
         }
         CG_TRY(check_launch());
-        CG_TRY(vm_check_halt(s));
-        done += todo;
+        // a step whose T1 sweep stopped on a full cell row: grow the rows, finish its sweep and
+        // the step; the later steps of the chunk did nothing and run again (done counts completed
+        // steps only, so supplied noise stays aligned with the steps)
+        bool recovered = false;
+        CG_TRY(vm_recover(s, &recovered));
+        if (recovered) {
+            k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
+            s->kernels_enqueued += 1;
+            CG_TRY(check_launch());
+        }
+        Ctl c;
+        CG_TRY(read_ctl(s, c));
+        done += c.step - step_prev;
+        step_prev = c.step;
     }
     return CG_OK;
 }

@@ -1499,13 +1499,14 @@ CG_D void spp_cell(const VoroArgs &a, int c, double xi, double dt, double mu, in
 }
 
 // device noise of cell c: component (l & 1) of the Box-Muller pair with Philox counter
-// (l >> 1, step), key = the instance's seed, l = the cell's index within its instance -- so a cell's
-// noise does not depend on where its instance sits in a batch
+// (l >> 1, step + the instance's step offset), key = the instance's seed, l = the cell's index
+// within its instance -- so a cell's noise does not depend on where its instance sits in a batch,
+// nor on which system it has run in
 CG_D double2 cell_pair_noise(const VoroArgs &a, int c, uint32_t step, int &local)
 {
     const Inst &in = inst_of(a, c);
     local = c - in.off;
-    return normal2(in.seed, (uint32_t)(local >> 1), step, 0u);
+    return normal2(in.seed, (uint32_t)(local >> 1), step + in.step_off, 0u);
 }
 
 // Two cells per thread: one Box-Muller pair serves both when they are consecutive cells of one

@@ -254,6 +254,19 @@ class VoronoiBatch:
         p = params if params is not None else FireParams.defaults(**kw)
         check(self._lib.cg_fire_minimize(self._h, C.byref(p)))
 
+    def fire_begin(self, params=None, **kw):
+        """Start a FIRE minimisation that fire_advance continues in pieces."""
+        p = params if params is not None else FireParams.defaults(**kw)
+        check(self._lib.cg_fire_begin(self._h, C.byref(p)))
+        return p
+
+    def fire_advance(self, params, iterations):
+        """Up to `iterations` more FIRE iterations (fewer if every instance stops); returns the
+        number of stopped instances."""
+        n = C.c_int(0)
+        check(self._lib.cg_fire_advance(self._h, C.byref(params), int(iterations), C.byref(n)))
+        return n.value
+
     def fire_state(self):
         n = len(self.N)
         it = np.zeros(n, np.int32)
@@ -299,11 +312,16 @@ class VertexBatch(VoronoiBatch):
         check(self._lib.cg_get_forces(self._h, ptr(out)))
         return out
 
+    def row_capacity(self):
+        """Current cell-row width (vmax): it grows when a T1 transition needs longer rows."""
+        self.K = self.vmax = int(self._lib.cg_neighbor_capacity(self._h))
+        return self.vmax
+
     def vertex_topology(self):
         vn = np.zeros(3 * self.Nv, np.int32)
         vcn = np.zeros(3 * self.Nv, np.int32)
         cvn = np.zeros(self.Ntot, np.int32)
-        cv = np.zeros((self.Ntot, self.vmax), np.int32)
+        cv = np.zeros((self.Ntot, self.row_capacity()), np.int32)
         check(self._lib.cg_get_vertex_topology(self._h, ptr(vn), ptr(vcn), ptr(cvn), ptr(cv)))
         return vn, vcn, cvn, cv
 
@@ -311,7 +329,12 @@ class VertexBatch(VoronoiBatch):
         vn = np.ascontiguousarray(vn, np.int32)
         vcn = np.ascontiguousarray(vcn, np.int32)
         cvn = np.ascontiguousarray(cvn, np.int32)
-        cv = np.ascontiguousarray(cv, np.int32).reshape(self.Ntot, self.vmax)
+        cv = np.ascontiguousarray(cv, np.int32).reshape(self.Ntot, -1)
+        if cv.shape[1] != self.row_capacity():
+            w = np.full((self.Ntot, self.vmax), -1, np.int32)
+            k = min(self.vmax, cv.shape[1])
+            w[:, :k] = cv[:, :k]
+            cv = w
         check(self._lib.cg_set_vertex_topology(self._h, ptr(vn), ptr(vcn), ptr(cvn), ptr(cv)))
 
     def set_t1_threshold(self, t):

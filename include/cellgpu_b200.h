@@ -257,6 +257,29 @@ typedef struct {
     int n_min, max_iterations;
 } cg_fire_params;
 int cg_fire_minimize(cg_system *sys, const cg_fire_params *prm);
+/* The same minimisation in pieces (EnergyMinimizerFIRE::minimize split at its loop head): cg_fire_begin
+ * starts it (fresh per-instance state, forces of the current positions); cg_fire_advance runs up to
+ * `iterations` more iterations, or until every instance has stopped (converged or at max_iterations;
+ * *n_stopped receives their number, may be NULL). Stopped instances stay frozen, so a caller can
+ * read an instance's result as soon as it stops while the others continue; pieces with the same
+ * parameters give the same result as one cg_fire_minimize call. No counterpart in the reference
+ * (its minimize runs to the end in one call); the serving loop uses it to return results early. */
+int cg_fire_begin(cg_system *sys, const cg_fire_params *prm);
+int cg_fire_advance(cg_system *sys, const cg_fire_params *prm, int iterations, int *n_stopped);
+/* Fresh FIRE state for instances [first, first + count) only (the others keep theirs) and the forces
+ * of the current state: instances admitted into a serving batch beside instances that are already
+ * minimising. No counterpart in the reference. */
+int cg_fire_begin_instances(cg_system *sys, const cg_fire_params *prm, int first, int count);
+
+/* Continuous batching (no counterpart in the reference, which runs one monolayer per process): copy
+ * the whole state of instances [src_first, src_first + count) of src into instances
+ * [dst_first, dst_first + count) of dst -- positions, directors, preferences, motility, forces,
+ * areas and perimeters, topology (relabelled to dst's indices), FIRE velocities and per-instance
+ * FIRE state, cell types, exclusions, noise keys and step counts -- so they continue in dst exactly
+ * where they stopped in src (the noise of an instance is keyed by its own seed and step count, not by
+ * the system it runs in). Both systems must have the same model, precision, summation mode (and
+ * vmax), and the instances the same sizes and boxes. Synchronises src's and dst's streams. */
+int cg_copy_instances(cg_system *dst, int dst_first, cg_system *src, int src_first, int count);
 /* per instance: iterations, sqrt(max |F|^2) (CPU convention) and sqrt(mean |F|^2) (the reference's
  * GPU convention, src/updaters/EnergyMinimizerFIRE2D.cpp:184) of the last iteration */
 int cg_fire_state(cg_system *sys, int *iterations, double *fmax_cpu, double *fnorm_gpu);

@@ -211,3 +211,39 @@ def test_vertex_full_size_matches_oracle(cglib, oracle, torch):
     assert np.array_equal(gvn, vn) and np.array_equal(gvcn, vcn) and np.array_equal(gcvn, cvn)
     for c in range(Nc):
         assert np.array_equal(gcv[c, :gcvn[c]], cv[c, :cvn[c]])
+
+
+def test_t1_flip_into_a_full_row_grows_rows(cglib, oracle, torch):
+    """Cell rows created exactly as wide as the largest cell (vmax = 10): a T1 flip in the first
+    step's sweep adds an 11th vertex to such a cell. The sweep stops before that flip, the rows
+    grow and the sweep resumes where it stopped, as the reference grows vertexMax mid-sweep
+    (src/models/vertexModelBase.cpp:474-500,674-684). The hot Brownian run (about 300 flips) then
+    follows the oracle, whose rows are wide enough from the start: wiring exact, positions 1e-10."""
+    from cellgpu_b200 import VertexBatch
+    pos, box = monolayer(400, 43)
+    Nc = len(pos)
+    nn, nbr = oracle.periodic_delaunay(pos, box, 16)
+    vpos, vn, vcn, cvn, cv = oracle.vertex_from_delaunay(pos, box, nn, nbr, vmax=20)
+    vmax0 = int(cvn.max())
+    assert vmax0 == 10
+    b = VertexBatch([Nc], [box], vmax=vmax0)
+    b.from_cells(pos)
+    pref = np.tile([1.0, 3.85], (Nc, 1))
+    b.set_preferences(pref)
+    b.set_t1_threshold(0.08)
+    rng = np.random.default_rng(5)
+    steps = 40
+    noise = rng.normal(size=(steps, 2 * Nc, 2))
+    b.brownian_run(steps, dt=0.01, mu=1.0, T=0.02, noise=torch.tensor(noise.reshape(steps, -1), device="cuda:0"))
+    nt1 = 0
+    for t in range(steps):
+        _, _, k = oracle.vertex_brownian_run(vpos, box, vn, vcn, cvn, cv, pref, noise[t:t + 1], dt=0.01, T=0.02,
+                                            t1_threshold=0.08)
+        nt1 += k
+    assert b.row_capacity() > vmax0 and int(cvn.max()) > vmax0
+    gvn, gvcn, gcvn, gcv = b.vertex_topology()
+    assert np.array_equal(gvn, vn) and np.array_equal(gvcn, vcn) and np.array_equal(gcvn, cvn)
+    for c in range(Nc):
+        assert np.array_equal(gcv[c, :cvn[c]], cv[c, :cvn[c]])
+    assert np.abs(b.positions() - vpos).max() < 1e-10
+    assert b.counters()["t1_flips"] == nt1
