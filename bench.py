@@ -240,12 +240,11 @@ def bench_serving(n_requests, lanes=4, calib=16):
     res_c, span_c, _ = S.serve_poisson(burst, rate=0, lanes=lanes)
     rate = 0.8 * calib / span_c
     res, makespan, stats = S.serve_poisson(reqs, rate, lanes=lanes)
-    out = S.summarize(res, makespan)
-    fire = [r for q, r in zip(reqs, res) if q.task == "fire"]
+    out = S.summarize(res, makespan, reqs)
     out.update({"arrival_rate_per_s": rate, "lanes": lanes, "calibration_burst_s": span_c,
-                "fire_converged_fraction": float(np.mean([r.fmax <= 1e-10 for r in fire])) if fire else None,
-                "batches": stats["batches"], "peak_resident_bytes": stats["peak_resident_bytes"],
-                "budget_bytes": stats["budget_bytes"],
+                "batches": stats["batches"], "rebuilds": stats["rebuilds"],
+                "joined_running_batch": stats["joined_running_batch"],
+                "peak_resident_bytes": stats["peak_resident_bytes"], "budget_bytes": stats["budget_bytes"],
                 "workload": f"{n_requests} requests: 60% Voronoi / 40% vertex, N log-uniform [100, 65536], "
                             "p0 U[3.6,4.0], FIRE to 1e-10 (max 10^4 iterations) or 2000 SPP steps "
                             "(v0 0.05, dt 0.01), Poisson arrivals"})

@@ -1,20 +1,26 @@
 """Serving: continuous batching of FIRE minimisations and fixed-step dynamics runs.
 
 Requests (Voronoi or vertex model; SPP dynamics for a fixed number of steps, or FIRE to a force
-norm) arrive at any time. Each of ``lanes`` worker threads takes a batch when it is free: the
-oldest queued request fixes the batch's kind, and every queued request of the same kind joins it,
-within a cell budget and the device-memory budget (admission by the footprint the library reports
-for that batch shape). Batches run concurrently, each system on its own stream, with all state
-resident in HBM from the initial upload to the final read-back. Requests that arrive while
-batches run join the next batch that a free lane forms. Memory is returned to the budget when a
-batch completes.
+norm) arrive at any time. Each of ``lanes`` worker threads runs one batch at a time: a system
+holding many requests as instances, all state resident in HBM. A batch runs in chunks (SPP: a
+number of steps; FIRE: a number of iterations). At every chunk end:
+  * requests that have finished (SPP: their steps done; FIRE: converged or at the iteration cap)
+    leave the batch and their results are returned at once;
+  * queued requests of the batch's kind join it, as the device-memory budget allows (admission
+    by the footprint the library reports for the new batch shape);
+  * when requests joined, or finished ones hold half the batch's memory while others wait, the
+    batch is rebuilt as a new system: the running requests move into it with their whole state
+    (cg_copy_instances) and continue exactly where they stopped, the new ones start fresh
+    (cg_fire_begin_instances for FIRE), and the old system's memory returns to the budget.
+A free lane takes the oldest queued request's kind and every queued request of that kind. Batches
+run concurrently, each system on its own stream.
 
 Every instance's result depends only on its own request: its initial state and its device noise
-are derived from the request's seed, the noise is keyed by the instance seed and the local cell
-index, and FIRE keeps per-instance state. So a request gives the same result alone and in a mix,
-up to the order of floating-point atomics; with ``Server(deterministic=True)`` (fixed-point force
-sums) an SPP request's positions are the same bits in any mix, and reruns of a batch repeat
-exactly.
+are derived from the request's seed, the noise is keyed by the instance seed, its own step count
+and the local cell index, and FIRE keeps per-instance state that moves with the instance. So a
+request gives the same result alone and in a mix, whether it started a batch or joined one, up to
+the order of floating-point atomics; with ``Server(deterministic=True)`` (fixed-point force sums)
+an SPP request's positions are the same bits in any mix.
 
 The reference has no serving layer; this drives the same kernels as the class API
 (``VoronoiQuadraticEnergy``/``VertexQuadraticEnergy`` with ``selfPropelledParticleDynamics``,
@@ -69,8 +75,10 @@ class Result:
     t_submit: float
     t_start: float
     t_done: float
-    batch_requests: int
+    batch_requests: int        # requests in the batch during this request's last chunk
     batch_cells: int
+    joined: bool = False       # admitted into a batch that was already running
+    capped: bool = False       # FIRE: stopped at the iteration cap above the force threshold
 
     @property
     def latency(self):
@@ -113,51 +121,161 @@ def device_memory():
     return f.value, t.value
 
 
+SPP_CHUNK = 100     # SPP steps per chunk: requests join and leave a batch at chunk ends
+FIRE_CHUNK = 256    # FIRE iterations per chunk
+
+
+def spp_chunk(steps):
+    """The chunk length of an SPP batch: the largest divisor of the request's steps up to SPP_CHUNK
+    (every request of a batch has the same steps, so all finish at chunk ends)."""
+    for c in range(min(SPP_CHUNK, steps), 0, -1):
+        if steps % c == 0:
+            return c
+    return 1
+
+
+def fire_params(req):
+    return FireParams.defaults(force_cutoff=req.fire_tol, max_iterations=req.fire_max_iterations)
+
+
+@dataclasses.dataclass
+class _Slot:
+    req: Request
+    fut: Future
+    t_sub: float
+    t_start: float
+    done: int = 0          # SPP steps done
+    joined: bool = False
+    index: int = -1        # instance index in the batch's current system
+
+
+class RunningBatch:
+    """One serving batch: a system and its requests as instances (in slot order). build() makes a
+    new system from the slots still running (moved with their state) and new slots (fresh)."""
+
+    def __init__(self, model, task, deterministic=False):
+        self.model, self.task, self.det = model, task, bool(deterministic)
+        self.b = None
+        self.slots = []
+        self.prm = None
+
+    def build(self, fresh):
+        """Replace the system by one holding the running slots (state moved) followed by `fresh`."""
+        lib = load()
+        surv = list(self.slots)
+        order = surv + list(fresh)
+        init = [initial_state(sl.req) for sl in order]
+        Ns = [sl.req.n for sl in order]
+        boxes = [(L, L) for L, _, _ in init]
+        if self.model == "voronoi":
+            nb = VoronoiBatch(Ns, boxes)
+            pos = [p for _, p, _ in init]
+            if surv:  # the running slots' current positions (their rows then come with the copy)
+                P = self.b.positions()
+                off = self.b.offsets
+                for j, sl in enumerate(surv):
+                    pos[j] = P[off[sl.index]:off[sl.index + 1]]
+            nb.set_positions(np.concatenate(pos))
+        else:
+            # rows as wide as the running system's (they grow when a T1 transition needs it)
+            nb = VertexBatch(Ns, boxes, vmax=self.b.row_capacity() if surv else 30)
+            # the running slots' vertex state is overwritten by the copy below; their initial
+            # cells only give the new system its shape
+            nb.from_cells(np.concatenate([p for _, p, _ in init]))
+        try:
+            if self.det:
+                nb.set_deterministic(True)
+            nb.set_preferences(np.concatenate([np.tile([1.0, sl.req.p0], (sl.req.n, 1)) for sl in order]))
+            nb.set_instance_seeds([instance_seed(sl.req) for sl in order])
+            if self.task == "spp":
+                nb.set_directors(np.concatenate([t for _, _, t in init]))
+                nb.set_motility(np.concatenate([np.tile([sl.req.v0, 1.0], (sl.req.n, 1)) for sl in order]))
+            if self.model == "voronoi":
+                nb.triangulate()
+            for j, sl in enumerate(surv):
+                rc = lib.cg_copy_instances(nb.handle, j, self.b.handle, sl.index, 1)
+                if rc != 0:
+                    raise RuntimeError(f"cg_copy_instances failed: {lib.cg_last_error_string().decode()}")
+            if self.task == "fire":
+                self.prm = fire_params(order[0].req)
+                if surv:
+                    rc = lib.cg_fire_begin_instances(nb.handle, C.byref(self.prm), len(surv), len(fresh))
+                    if rc != 0:
+                        raise RuntimeError(lib.cg_last_error_string().decode())
+                else:
+                    nb.fire_begin(self.prm)
+        except Exception:
+            nb.close()
+            raise
+        if self.b is not None:
+            self.b.close()
+        self.b = nb
+        self.slots = order
+        for j, sl in enumerate(order):
+            sl.index = j
+
+    def run_chunk(self):
+        """One chunk; returns the mask of slots that have finished."""
+        if self.task == "spp":
+            n = spp_chunk(self.slots[0].req.steps)
+            self.b.spp_run(n, dt=self.slots[0].req.dt)
+            for sl in self.slots:
+                sl.done += n
+            return np.array([sl.done >= sl.req.steps for sl in self.slots])
+        self.b.fire_advance(self.prm, FIRE_CHUNK)
+        its, fmax, _ = self.b.fire_state()
+        self.its, self.fmax = its, fmax
+        return np.array([its[j] >= sl.req.fire_max_iterations or fmax[j] <= sl.req.fire_tol
+                         for j, sl in enumerate(self.slots)])
+
+    def results(self, mask, t_done):
+        """(slot, Result) of the slots in mask; they leave the batch."""
+        P = self.b.positions()
+        E = self.b.energies()
+        off = self.b.offsets if self.model == "voronoi" else 2 * self.b.offsets
+        cells = sum(sl.req.n for sl in self.slots)
+        out, keep = [], []
+        for j, sl in enumerate(self.slots):
+            if not mask[j]:
+                keep.append(sl)
+                continue
+            r = sl.req
+            if self.task == "spp":
+                its, fm, capped = r.steps, float("nan"), False
+            else:
+                its, fm = int(self.its[j]), float(self.fmax[j])
+                capped = fm > r.fire_tol
+            res = Result(r.rid, P[off[j]:off[j + 1]].copy(), float(E[j]), r.n * its, its, fm, sl.t_sub,
+                         sl.t_start, t_done, len(self.slots), cells, sl.joined, capped)
+            out.append((sl, res))
+        self.slots = keep
+        return out
+
+    def close(self):
+        if self.b is not None:
+            self.b.close()
+            self.b = None
+
+
 def run_batch(reqs, deterministic=False):
     """Run one batch of same-kind requests to completion on its own system (and stream); return
     per-request (positions, energy, iterations, fmax). deterministic: fixed-point force sums and
     fixed-order FIRE reductions (cg_set_deterministic)."""
-    model, task = reqs[0].model, reqs[0].task
-    states = [initial_state(r) for r in reqs]
-    Ns = [r.n for r in reqs]
-    boxes = [(L, L) for L, _, _ in states]
-    pos = np.concatenate([p for _, p, _ in states])
-    if model == "voronoi":
-        b = VoronoiBatch(Ns, boxes)
-        b.set_positions(pos)
-    else:
-        b = VertexBatch(Ns, boxes)
-        b.from_cells(pos)
+    rb = RunningBatch(reqs[0].model, reqs[0].task, deterministic)
+    now = time.perf_counter()
+    slots = [_Slot(r, None, now, now) for r in reqs]
+    rb.build(slots)
+    done = {}
     try:
-        if deterministic:
-            b.set_deterministic(True)
-        b.set_preferences(np.concatenate([np.tile([1.0, r.p0], (r.n, 1)) for r in reqs]))
-        b.set_instance_seeds([instance_seed(r) for r in reqs])
-        if task == "spp":
-            b.set_directors(np.concatenate([t for _, _, t in states]))
-            b.set_motility(np.concatenate([np.tile([r.v0, 1.0], (r.n, 1)) for r in reqs]))
-            if model == "voronoi":
-                b.triangulate()
-            b.spp_run(reqs[0].steps, dt=reqs[0].dt)
-            its = np.full(len(reqs), reqs[0].steps)
-            fmax = np.full(len(reqs), np.nan)
-        else:
-            if model == "voronoi":
-                b.triangulate()
-            b.fire_minimize(FireParams.defaults(force_cutoff=reqs[0].fire_tol,
-                                                max_iterations=reqs[0].fire_max_iterations))
-            its, fmax, _ = b.fire_state()  # fmax = sqrt(max |F|^2) per instance
-        P = b.positions()
-        E = b.energies()
+        while rb.slots:
+            m = rb.run_chunk()
+            if m.any():
+                for sl, res in rb.results(m, time.perf_counter()):
+                    done[id(sl)] = res
     finally:
-        b.close()
-    out = []
-    off = 0
-    for i, r in enumerate(reqs):
-        m = r.n if model == "voronoi" else 2 * r.n
-        out.append((P[off:off + m].copy(), float(E[i]), int(its[i]), float(fmax[i])))
-        off += m
-    return out
+        rb.close()
+    return [(done[id(sl)].positions, done[id(sl)].energy, done[id(sl)].iterations, done[id(sl)].fmax)
+            for sl in slots]
 
 
 class Server:
@@ -182,6 +300,8 @@ class Server:
         self.peak_resident = 0
         self.closing = False
         self.batches = 0
+        self.rebuilds = 0    # batches rebuilt around their running requests
+        self.joined = 0      # requests admitted into a running batch
         self._rid = 0
         self.threads = [threading.Thread(target=self._lane, daemon=True) for _ in range(int(lanes))]
         for t in self.threads:
@@ -230,20 +350,7 @@ class Server:
         while True:
             if self.queue:
                 head = self.queue[0][0]
-                key = head.key()
-                picked, cells, fp = [], 0, 0
-                for item in self.queue:
-                    r = item[0]
-                    if r.key() != key:
-                        continue
-                    if picked and (cells + r.n > self.max_cells or len(picked) >= self.max_reqs):
-                        break
-                    f = footprint(head.model, [x[0].n for x in picked] + [r.n], deterministic=self.deterministic)
-                    if self.resident + f > self.budget:
-                        break
-                    picked.append(item)
-                    cells += r.n
-                    fp = f
+                picked, fp = self._pick(head.key(), head.model, [])
                 if picked:
                     for item in picked:
                         self.queue.remove(item)
@@ -259,6 +366,26 @@ class Server:
                 return None
             self.cond.wait()
 
+    def _pick(self, key, model, running):
+        """Under the lock: queued requests of this key that fit beside the `running` sizes, while the
+        footprint of the resulting batch plus everything resident stays within the budget (a
+        rebuilt batch's old system stays resident until the rebuild is done)."""
+        picked, sizes = [], list(running)
+        fp = footprint(model, sizes, deterministic=self.deterministic) if sizes else 0
+        for item in self.queue:
+            r = item[0]
+            if r.key() != key:
+                continue
+            if sizes and (sum(sizes) + r.n > self.max_cells or len(sizes) >= self.max_reqs):
+                break
+            f = footprint(model, sizes + [r.n], deterministic=self.deterministic)
+            if self.resident + f > self.budget:
+                break
+            picked.append(item)
+            sizes.append(r.n)
+            fp = f
+        return picked, fp
+
     def _lane(self):
         while True:
             with self.cond:
@@ -266,26 +393,62 @@ class Server:
             if got is None:
                 return
             items, fp = got
-            reqs = [it[0] for it in items]
-            t_start = time.perf_counter()
+            key = items[0][0].key()
+            t0 = time.perf_counter()
+            rb = RunningBatch(items[0][0].model, items[0][0].task, self.deterministic)
+            fresh = [_Slot(r, fut, t_sub, t0) for r, fut, t_sub in items]
             try:
-                outs = run_batch(reqs, self.deterministic)
-                err = None
+                rb.build(fresh)
+                with self.cond:
+                    self.batches += 1
+                while rb.slots:
+                    mask = rb.run_chunk()
+                    freed = 0
+                    if mask.any():
+                        for sl, res in rb.results(mask, time.perf_counter()):
+                            sl.fut.set_result(res)
+                            freed += sl.req.n
+                    if not rb.slots:
+                        break
+                    # admission into the running batch: queued requests of its kind, and a rebuild
+                    # that returns the finished requests' memory while others wait
+                    with self.cond:
+                        running = [sl.req.n for sl in rb.slots]
+                        picked, fp_new = self._pick(key, rb.model, running)
+                        shrink = freed > 0 and bool(self.queue) and freed >= sum(running)
+                        rebuild = bool(picked) or shrink
+                        if rebuild:
+                            for item in picked:
+                                self.queue.remove(item)
+                            self.resident += fp_new  # held with the old system until the rebuild ends
+                            self.peak_resident = max(self.peak_resident, self.resident)
+                    if rebuild:
+                        now = time.perf_counter()
+                        joiners = [_Slot(r, fut, t_sub, now, joined=True) for r, fut, t_sub in picked]
+                        try:
+                            rb.build(joiners)
+                        except Exception as e:
+                            for sl in joiners:
+                                sl.fut.set_exception(e)
+                            raise
+                        finally:
+                            # the old system is gone (or, on failure, closed below): its memory
+                            # returns to the budget and the new footprint is what this lane holds
+                            with self.cond:
+                                self.resident -= fp
+                                self.rebuilds += 1
+                                self.joined += len(joiners)
+                                self.cond.notify_all()
+                            fp = fp_new
             except Exception as e:  # the failure belongs to this batch's requests
-                outs, err = None, e
-            t_done = time.perf_counter()
-            with self.cond:
-                self.resident -= fp
-                self.batches += 1
-                self.cond.notify_all()
-            cells = sum(r.n for r in reqs)
-            for k, (r, fut, t_sub) in enumerate(items):
-                if err is not None:
-                    fut.set_exception(err)
-                    continue
-                P, E, its, fmax = outs[k]
-                fut.set_result(Result(r.rid, P, E, r.n * its, its, fmax, t_sub, t_start, t_done,
-                                      len(reqs), cells))
+                for sl in rb.slots + fresh:
+                    if sl.fut is not None and not sl.fut.done():
+                        sl.fut.set_exception(e)
+            finally:
+                rb.close()
+                with self.cond:
+                    self.resident -= fp
+                    self.cond.notify_all()
 
 
 def request_stream(n_requests, seed=2026, n_min=100, n_max=65536, fire_fraction=0.5, vertex_fraction=0.4,
@@ -321,15 +484,34 @@ def serve_poisson(requests, rate, lanes=4, memory_budget=None):
                 time.sleep(d)
             futs.append(srv.submit(r))
         res = [f.result() for f in futs]
-        stats = {"batches": srv.batches, "peak_resident_bytes": srv.peak_resident, "budget_bytes": srv.budget}
+        stats = {"batches": srv.batches, "rebuilds": srv.rebuilds, "joined_running_batch": srv.joined,
+                 "peak_resident_bytes": srv.peak_resident, "budget_bytes": srv.budget}
     makespan = max(r.t_done for r in res) - t0
     return res, makespan, stats
 
 
-def summarize(results, makespan):
+def summarize(results, makespan, requests=None):
+    """Latency percentiles (all requests; and FIRE requests that reached their threshold apart from
+    those stopped at the iteration cap), aggregate cell-steps/s, batching statistics."""
     lat = np.array([r.latency for r in results])
     work = sum(r.work for r in results)
-    return {"requests": len(results), "p50_latency_s": float(np.percentile(lat, 50)),
-            "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean()),
-            "cell_steps_per_s": work / makespan, "makespan_s": makespan, "work_cell_steps": int(work),
-            "mean_batch_requests": float(np.mean([r.batch_requests for r in results]))}
+    out = {"requests": len(results), "p50_latency_s": float(np.percentile(lat, 50)),
+           "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean()),
+           "cell_steps_per_s": work / makespan, "makespan_s": makespan, "work_cell_steps": int(work),
+           "mean_batch_requests": float(np.mean([r.batch_requests for r in results])),
+           "joined_running_batch_fraction": float(np.mean([r.joined for r in results]))}
+    if requests is not None:
+        fire = [r for q, r in zip(requests, results) if q.task == "fire"]
+        spp = [r for q, r in zip(requests, results) if q.task == "spp"]
+        conv = [r for r in fire if not r.capped]
+        out["fire_requests"] = len(fire)
+        out["fire_capped_fraction"] = float(np.mean([r.capped for r in fire])) if fire else None
+        if conv:
+            lc = np.array([r.latency for r in conv])
+            out["fire_converged_p50_latency_s"] = float(np.percentile(lc, 50))
+            out["fire_converged_p99_latency_s"] = float(np.percentile(lc, 99))
+        if spp:
+            ls = np.array([r.latency for r in spp])
+            out["spp_p50_latency_s"] = float(np.percentile(ls, 50))
+            out["spp_p99_latency_s"] = float(np.percentile(ls, 99))
+    return out

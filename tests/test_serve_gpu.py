@@ -105,3 +105,83 @@ def test_deterministic_server_same_bits_alone_and_in_mix(cglib):
         m = mix[k]
         assert m.batch_requests > 1
         assert np.array_equal(a.positions, m.positions)
+
+
+def _join(reqs, deterministic):
+    """Run reqs[0] on a one-lane server and submit the others once its batch is running: they join
+    it at a chunk end (the batch is rebuilt around the running request)."""
+    import time
+
+    from cellgpu_b200.serve import Server
+    with Server(lanes=1, deterministic=deterministic) as srv:
+        first = srv.submit(copy.deepcopy(reqs[0]))
+        t0 = time.perf_counter()
+        while srv.batches == 0 and time.perf_counter() - t0 < 60:
+            time.sleep(0.001)
+        rest = [srv.submit(copy.deepcopy(r)) for r in reqs[1:]]
+        out = [first.result()] + [f.result() for f in rest]
+        joined = srv.joined
+    return out, joined
+
+
+@pytest.mark.parametrize("model", ["voronoi", "vertex"])
+def test_spp_request_joining_a_running_batch_same_bits(cglib, model):
+    """Deterministic mode: an SPP request admitted into a running batch, and the request whose state
+    moved into the rebuilt batch, both end with the positions they have alone, bit for bit."""
+    from cellgpu_b200.serve import Request, Server
+    reqs = [Request(model, "spp", 1200, p0=3.8, seed=21, steps=3000, v0=0.1),
+            Request(model, "spp", 500, p0=3.7, seed=22, steps=3000, v0=0.1)]
+    alone = []
+    for r in reqs:
+        with Server(lanes=1, deterministic=True) as srv:
+            alone.append(srv.submit(copy.deepcopy(r)).result())
+    mix, joined = _join(reqs, True)
+    assert joined >= 1 and mix[1].joined
+    for a, m in zip(alone, mix):
+        assert np.array_equal(a.positions, m.positions)
+        assert a.energy == m.energy
+
+
+def test_fire_request_joining_a_running_batch(cglib):
+    """FIRE requests admitted into a running minimisation batch reach the same minima as alone (the
+    running request's velocities and FIRE state move with it); the FIRE tolerances above."""
+    from cellgpu_b200.serve import Request, Server
+    reqs = [Request("voronoi", "fire", 900, p0=3.7, seed=31, fire_tol=1e-10, fire_max_iterations=20000),
+            Request("voronoi", "fire", 700, p0=3.7, seed=32, fire_tol=1e-10, fire_max_iterations=20000)]
+    alone = []
+    for r in reqs:
+        with Server(lanes=1) as srv:
+            alone.append(srv.submit(copy.deepcopy(r)).result())
+    mix, joined = _join(reqs, False)
+    assert joined >= 1 and mix[1].joined
+    for r, a, m in zip(reqs, alone, mix):
+        assert a.fmax <= r.fire_tol and m.fmax <= r.fire_tol
+        assert abs(a.energy - m.energy) <= 1e-9 * max(1.0, abs(a.energy))
+        assert _pdist(a.positions, m.positions, r.n) < 1e-6
+
+
+def test_fire_in_pieces_equals_one_call(cglib):
+    """cg_fire_begin + cg_fire_advance in pieces of 48 iterations give the same minimisation as one
+    cg_fire_minimize call (same iteration count, energies within 1e-12 relative)."""
+    from cellgpu_b200 import FireParams, VoronoiBatch
+    from helpers import monolayer
+    pos, box = monolayer(400, 71)
+    out = []
+    for pieces in (False, True):
+        b = VoronoiBatch([400], [box])
+        b.set_positions(pos)
+        b.set_preferences(np.tile([1.0, 3.7], (400, 1)))
+        b.set_deterministic(True)
+        b.triangulate()
+        prm = FireParams.defaults(force_cutoff=1e-10, max_iterations=4000)
+        if pieces:
+            b.fire_begin(prm)
+            while b.fire_advance(prm, 48) < 1:
+                pass
+        else:
+            b.fire_minimize(prm)
+        its, fmax, _ = b.fire_state()
+        out.append((int(its[0]), float(b.energies()[0]), b.positions()))
+    assert out[0][0] == out[1][0]
+    assert abs(out[0][1] - out[1][1]) <= 1e-12 * abs(out[0][1])
+    assert np.array_equal(out[0][2], out[1][2])
