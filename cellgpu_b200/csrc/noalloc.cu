@@ -104,8 +104,8 @@ static int setup(void **addr)
 
 }  // namespace cg_noalloc
 
-extern "C" int cg_voronoi_triangulate_noalloc(const double *pos, int N, double Lx, double Ly, int K, int *nn,
-                                              int *nbr, cudaStream_t stream)
+static int triangulate_noalloc(const double *pos, int N, double Lx, double Ly, int K, int *nn, int *nbr,
+                               cudaStream_t stream)
 {
     using namespace cg_noalloc;
     if (!pos || !nn || !nbr || N < 8 || K < 4 || K > KMAX || !(Lx > 0) || !(Ly > 0))
@@ -159,4 +159,18 @@ extern "C" int cg_voronoi_triangulate_noalloc(const double *pos, int N, double L
     if (h_zsum != 6ull * (unsigned long long)N)
         return set_err(CG_ERR_TOPOLOGY, "Euler check failed (sum of coordinations != 6N)");
     return CG_OK;
+}
+
+extern "C" int cg_voronoi_triangulate_noalloc(const double *pos, int N, double Lx, double Ly, int K, int *nn,
+                                              int *nbr, cudaStream_t stream)
+{
+    // This thread's calls (the status read-back waits on `stream`) would otherwise count as unsafe
+    // while another thread captures in global mode, and invalidate that capture; in thread-local
+    // mode other threads' captures are ignored. `stream` must then not be the legacy default stream,
+    // which synchronises with capturing streams. The caller's mode is restored on return.
+    cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+    CG_CUDA(cudaThreadExchangeStreamCaptureMode(&mode));
+    const int st = triangulate_noalloc(pos, N, Lx, Ly, K, nn, nbr, stream);
+    cudaThreadExchangeStreamCaptureMode(&mode);
+    return st;
 }
