@@ -929,14 +929,23 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
         if (threadIdx.x == 0)
             t1_sweep_serial(a, in, q, nc, flips, status, a.t1_resume ? a.t1_resume + 2 * inst : nullptr);
     } else {
+        // up to 32 candidates (the steady state): warp 0 alone sorts, evaluates and sweeps, with
+        // warp barriers instead of block barriers; the other warps leave now
+        const bool fast = nc <= 32;
+        if (fast && threadIdx.x >= 32) return;
+        const int nthr = fast ? 32 : blockDim.x;
+        auto bsync = [fast]() {
+            if (fast) __syncwarp();
+            else __syncthreads();  // uniform across the block
+        };
         int P = 1;
         while (P < nc) P <<= 1;
-        for (int i = threadIdx.x; i < P; i += blockDim.x) s_key[i] = i < nc ? q[i] : 0x7fffffff;
-        for (int i = threadIdx.x; i < T1_HASH; i += blockDim.x) s_hash[i] = -1;
-        __syncthreads();
+        for (int i = threadIdx.x; i < P; i += nthr) s_key[i] = i < nc ? q[i] : 0x7fffffff;
+        for (int i = threadIdx.x; i < T1_HASH; i += nthr) s_hash[i] = -1;
+        bsync();
         for (int k = 2; k <= P; k <<= 1) {
             for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                for (int i = threadIdx.x; i < P; i += nthr) {
                     int ixj = i ^ j;
                     if (ixj > i) {
                         int x = s_key[i], y = s_key[ixj];
@@ -947,11 +956,11 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
                         }
                     }
                 }
-                __syncthreads();
+                bsync();
             }
         }
         // start-of-sweep evaluation (read-only)
-        for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+        for (int i = threadIdx.x; i < nc; i += nthr) {
             int key = s_key[i];
             int v1 = key / 3;
             int v2 = a.vn[3 * v1 + key % 3];
@@ -969,7 +978,7 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
             s_dec[i] = dec;
         }
         if (threadIdx.x == 0) s_tn = 0;
-        __syncthreads();
+        bsync();
         if (threadIdx.x < 32) {
             // sweep by warp 0, all lanes in step: the sorted candidates merged with the keys queued
             // by flips, kept in shared memory and moved to q[nc, 3 nv) if they outgrow it
