@@ -8,8 +8,8 @@ number of steps; FIRE: a number of iterations). At every chunk end:
     leave the batch and their results are returned at once;
   * queued requests of the batch's kind join it, as the device-memory budget allows (admission
     by the footprint the library reports for the new batch shape);
-  * when requests joined, or finished ones hold half the batch's memory while others wait, the
-    batch is rebuilt as a new system: the running requests move into it with their whole state
+  * when requests joined, or finished ones hold half the batch, the batch is rebuilt as a new
+    system: the running requests move into it with their whole state
     (cg_copy_instances) and continue exactly where they stopped, the new ones start fresh
     (cg_fire_begin_instances for FIRE), and the old system's memory returns to the budget.
 A free lane takes the oldest queued request's kind and every queued request of that kind. Batches
@@ -225,20 +225,23 @@ class RunningBatch:
         self.b.fire_advance(self.prm, FIRE_CHUNK)
         its, fmax, _ = self.b.fire_state()
         self.its, self.fmax = its, fmax
-        return np.array([its[j] >= sl.req.fire_max_iterations or fmax[j] <= sl.req.fire_tol
-                         for j, sl in enumerate(self.slots)])
+        return np.array([its[sl.index] >= sl.req.fire_max_iterations or fmax[sl.index] <= sl.req.fire_tol
+                         for sl in self.slots])
 
     def results(self, mask, t_done):
-        """(slot, Result) of the slots in mask; they leave the batch."""
+        """(slot, Result) of the slots in mask (mask follows self.slots); they leave the batch. A slot's
+        instance in the system is sl.index: slots that left earlier stay in the system (frozen for
+        FIRE) until the next rebuild."""
         P = self.b.positions()
         E = self.b.energies()
         off = self.b.offsets if self.model == "voronoi" else 2 * self.b.offsets
         cells = sum(sl.req.n for sl in self.slots)
         out, keep = [], []
-        for j, sl in enumerate(self.slots):
-            if not mask[j]:
+        for m, sl in zip(mask, self.slots):
+            if not m:
                 keep.append(sl)
                 continue
+            j = sl.index
             r = sl.req
             if self.task == "spp":
                 its, fm, capped = r.steps, float("nan"), False
@@ -415,7 +418,10 @@ class Server:
                     with self.cond:
                         running = [sl.req.n for sl in rb.slots]
                         picked, fp_new = self._pick(key, rb.model, running)
-                        shrink = freed > 0 and bool(self.queue) and freed >= sum(running)
+                        # finished requests still in the system (stepped, or frozen FIRE instances
+                        # whose forces are still evaluated) once they hold half of it
+                        dead = rb.b.Ntot - sum(running)
+                        shrink = freed > 0 and dead >= sum(running)
                         rebuild = bool(picked) or shrink
                         if rebuild:
                             for item in picked:

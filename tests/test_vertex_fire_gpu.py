@@ -235,12 +235,14 @@ def test_t1_flip_into_a_full_row_grows_rows(cglib, oracle, torch):
     steps = 40
     noise = rng.normal(size=(steps, 2 * Nc, 2))
     b.brownian_run(steps, dt=0.01, mu=1.0, T=0.02, noise=torch.tensor(noise.reshape(steps, -1), device="cuda:0"))
-    nt1 = 0
+    nt1, widest = 0, 0
     for t in range(steps):
         _, _, k = oracle.vertex_brownian_run(vpos, box, vn, vcn, cvn, cv, pref, noise[t:t + 1], dt=0.01, T=0.02,
                                             t1_threshold=0.08)
         nt1 += k
-    assert b.row_capacity() > vmax0 and int(cvn.max()) > vmax0
+        widest = max(widest, int(cvn.max()))
+    assert widest > vmax0  # the oracle's run needs wider rows at some step
+    assert b.row_capacity() > vmax0
     gvn, gvcn, gcvn, gcv = b.vertex_topology()
     assert np.array_equal(gvn, vn) and np.array_equal(gvcn, vcn) and np.array_equal(gcvn, cvn)
     for c in range(Nc):
