@@ -473,7 +473,7 @@ CG_D void grp_geometry(const VoroArgs &a, int c, const int *row, int z, bool ok,
             if (!(undecided & (1 << r))) continue;
             int k = gl + G * r;
             int idx = (a.undec && a.ctl) ? atomicAdd(&a.ctl->n_undec, 1) : a.N;
-            if (idx < a.N) a.undec[idx] = c * NS + k;
+            if (idx < a.N) a.undec[idx] = c * KMAX + k;  // one encoding for every row width
             else fail = min(fail, 2 * k);
         }
     }
@@ -642,17 +642,30 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int 
             Ly = in.Ly;
         }
         const bool ok = live && z >= 3 && z <= NS;
-        int nbk[NS / G];
+        // Rows of at most G entries (nearly every cell of a tissue): when all four cells of the warp
+        // have them, the pass runs in its one-slot-per-lane form on the narrow tile (fewer live
+        // registers, no second-slot code)
+        const bool small = CG_FP_SMALL_PATH && NS > G && __all_sync(0xffffffffu, !live || z <= G);
+        GrpTile<R, G> &tile8 = *reinterpret_cast<GrpTile<R, G> *>(&tile[sl]);
+        int nbk[NS / G], nb8[1];
         double A, P;
         int fail;
-        grp_geometry<R, SCATTER, TEST, NS>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail, true, pre0);
+        if (small)
+            grp_geometry<R, SCATTER, TEST, G>(a, c, row, z, ok, pc, Lx, Ly, gl, tile8, nb8, A, P, fail, true, pre0);
+        else
+            grp_geometry<R, SCATTER, TEST, NS>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail, true, pre0);
         if (ok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
         // A cell whose own row fails the test holds its contributions back: the row is about to be
         // replaced, and a stale row can contain a nearly collinear triangle whose Jacobians (1/cross^2)
         // would swamp the forces. The repair commit adds the contributions of the new row.
         bool hold = SCATTER && TEST && a.held && ok && fail != 0x7fffffff;
         if (hold && gl == 0) a.held[c] = 1;
-        if (SCATTER) grp_scatter<R, 1, NS, FIX>(a, c, z, ok && !hold, gl, tile[sl], nbk, A, P, R(1), CG_FP_PRE_PREF != 0, pref);
+        if (SCATTER) {
+            if (small)
+                grp_scatter<R, 1, G, FIX>(a, c, z, ok && !hold, gl, tile8, nb8, A, P, R(1), CG_FP_PRE_PREF != 0, pref);
+            else
+                grp_scatter<R, 1, NS, FIX>(a, c, z, ok && !hold, gl, tile[sl], nbk, A, P, R(1), CG_FP_PRE_PREF != 0, pref);
+        }
         if (TEST && live && gl == 0 && (fail != 0x7fffffff || !ok)) {
             if (!ok) {
                 if (a.ctl) {
@@ -724,8 +737,8 @@ __global__ void __launch_bounds__(256) k_repair_begin(VoroArgs a, unsigned long 
             bool fails = false;
             if (t < nu) {
                 const int en = a.undec[t];
-                c = en / NS;
-                k = en % NS;
+                c = en / KMAX;
+                k = en % KMAX;
                 z = a.nn[c];
                 row = a.nbr + (size_t)c * a.K;
                 const Inst &in = inst_of(a, c);

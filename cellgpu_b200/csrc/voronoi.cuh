@@ -29,6 +29,10 @@ constexpr int CAND_GLOBAL = 384;  // candidate slots per warp for the cell-list 
 #ifndef CG_FP_PRE_PREF
 #define CG_FP_PRE_PREF 1
 #endif
+// rows of at most 8 entries in all four cells of a warp take the pass's one-slot-per-lane form
+#ifndef CG_FP_SMALL_PATH
+#define CG_FP_SMALL_PATH 0
+#endif
 
 // device control block of one system
 struct Ctl {
