@@ -159,9 +159,34 @@ def check(code):
 
 
 def ptr(a):
-    """Device or host pointer of a torch tensor / numpy array (None -> NULL)."""
+    """Device or host pointer of a torch tensor / numpy array (None -> NULL). The library reads
+    buffers in row-major order, so a strided view (a transpose, an index along the second axis)
+    is refused rather than read in the wrong order."""
     if a is None:
         return None
     if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor is not contiguous (row-major); pass .contiguous()")
         return C.c_void_p(a.data_ptr())
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array is not C-contiguous; pass np.ascontiguousarray(...)")
     return a.ctypes.data_as(C.c_void_p)
+
+
+def device_noise(noise, count):
+    """A caller's noise tensor as the library reads it: float64 on the GPU, at least `count` values,
+    row-major (a strided view is copied into order). Work queued on the caller's current stream,
+    such as the copy that filled the tensor, is finished first: the library reads it from its own
+    stream. None passes through (device noise)."""
+    if noise is None:
+        return None
+    import torch
+    if not isinstance(noise, torch.Tensor) or not noise.is_cuda:
+        raise ValueError("noise must be a CUDA tensor")
+    if noise.dtype != torch.float64:
+        raise ValueError("noise must be float64")
+    if noise.numel() < count:
+        raise ValueError(f"noise holds {noise.numel()} values, {count} needed")
+    noise = noise.contiguous()
+    torch.cuda.current_stream(noise.device).synchronize()
+    return noise

@@ -17,7 +17,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import CG_FP64, CG_MIXED, FireParams, check, load, ptr
+from ._lib import CG_FP64, CG_MIXED, FireParams, check, device_noise, load, ptr
 
 
 def _f64(a, shape):
@@ -240,7 +240,9 @@ class VoronoiBatch:
         check(self._lib.cg_enforce_topology(self._h))
 
     def spp_run(self, n_steps, dt=0.01, mu=1.0, noise=None):
-        """n_steps SPP steps; noise: optional device tensor (torch) of n_steps*N normals."""
+        """n_steps SPP steps; noise: optional device tensor (torch, float64) of n_steps*N normals,
+        step-major (row t holds step t's normals of every cell)."""
+        noise = device_noise(noise, int(n_steps) * self.Ntot)
         check(self._lib.cg_spp_run(self._h, int(n_steps), float(dt), float(mu), ptr(noise)))
 
     def synchronize(self):
@@ -341,10 +343,15 @@ class VertexBatch(VoronoiBatch):
         check(self._lib.cg_set_t1_threshold(self._h, float(t)))
 
     def brownian_run(self, n_steps, dt=0.005, mu=1.0, T=1e-3, noise=None):
-        """noise: optional device tensor with n_steps*2*Nv normals (x then y per vertex)."""
+        """noise: optional device tensor (torch, float64) with n_steps*2*Nv normals (x then y per
+        vertex), step-major."""
+        noise = device_noise(noise, int(n_steps) * 2 * self.Nv)
         check(self._lib.cg_brownian_run(self._h, int(n_steps), float(dt), float(mu), float(T), ptr(noise)))
 
     def spp_run(self, n_steps, dt=0.01, mu=1.0, noise=None):
+        """n_steps SPP steps of the cell-vertex model; noise: optional device tensor (torch,
+        float64) of n_steps*Nc director normals, step-major."""
+        noise = device_noise(noise, int(n_steps) * self.Ntot)
         check(self._lib.cg_vertex_spp_run(self._h, int(n_steps), float(dt), float(mu), ptr(noise)))
 
 

@@ -50,3 +50,27 @@ def test_restore_rejects_a_foreign_buffer():
     h = C.c_void_p()
     assert lib.cg_restore(junk, len(junk.raw), C.byref(h)) == CG_ERR_ARG
     assert b"snapshot" in lib.cg_last_error_string()
+
+
+def test_strided_buffers_are_refused():
+    """The library reads every buffer row-major: a strided numpy view or torch tensor (a transpose,
+    an index along the second axis) is refused instead of being read in the wrong order, and noise
+    tensors must be float64 CUDA tensors of the right size."""
+    import numpy as np
+    import pytest
+    import torch
+
+    from cellgpu_b200._lib import device_noise, ptr
+    a = np.zeros((6, 4))
+    assert ptr(a) is not None and ptr(None) is None
+    with pytest.raises(ValueError):
+        ptr(a[:, ::2])
+    with pytest.raises(ValueError):
+        ptr(a[:, [0, 2, 1]])  # numpy lays an index along axis 1 out column-major
+    t = torch.zeros(6, 4, dtype=torch.float64)
+    assert ptr(t) is not None
+    with pytest.raises(ValueError):
+        ptr(t.t())
+    assert device_noise(None, 10) is None
+    with pytest.raises(ValueError):
+        device_noise(t, 24)  # host tensor
