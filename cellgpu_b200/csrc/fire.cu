@@ -25,9 +25,13 @@ struct FireArgs {
     double2 *pos, *vel;
     const double2 *F;
     FireInst *st;
-    // deterministic mode: (power, |F|^2, |v|^2) of every FIRE_BLOCK-dof block that lies inside one
-    // instance, summed per instance in a fixed order by k_fire_reduce; null: atomic sums
+    // deterministic mode: the dofs of every instance in chunks of FIRE_BLOCK counted from the
+    // instance's first dof (chunk[j] = (instance, first dof); the chunks of instance i are
+    // [chunk_off[i], chunk_off[i+1])), and part[3 j ..] = (power, |F|^2, |v|^2) of chunk j, which
+    // k_fire_reduce sums per instance in a fixed order; null: atomic sums
     double *part;
+    const int2 *chunk;
+    const int *chunk_off;
     cg_fire_params prm;
     const Ctl *ctl;  // a halted step (pending global rebuild) freezes the iteration
 };
@@ -109,15 +113,9 @@ __global__ void __launch_bounds__(256) k_fire_vv2(FireArgs a)
                 tv += s_red[2][k];
                 tm = fmax(tm, s_red[3][k]);
             }
-            if (a.part) {
-                a.part[3 * (size_t)blockIdx.x] = tp;
-                a.part[3 * (size_t)blockIdx.x + 1] = tf;
-                a.part[3 * (size_t)blockIdx.x + 2] = tv;
-            } else {
-                atomicAdd(&a.st[b0].power, tp);
-                atomicAdd(&a.st[b0].fnorm, tf);
-                atomicAdd(&a.st[b0].vnorm, tv);
-            }
+            atomicAdd(&a.st[b0].power, tp);
+            atomicAdd(&a.st[b0].fnorm, tf);
+            atomicAdd(&a.st[b0].vnorm, tv);
             atomicMax(&a.st[b0].fmax_bits, (unsigned long long)__double_as_longlong(tm));
         }
         return;
@@ -133,54 +131,90 @@ __global__ void __launch_bounds__(256) k_fire_vv2(FireArgs a)
             fm = fmax(fm, __shfl_down_sync(full, fm, off));
         }
         if (lane == 0 && inst >= 0) {
-            if (!a.part) {  // (the deterministic mode sums these dofs in k_fire_reduce)
-                atomicAdd(&a.st[inst].power, P);
-                atomicAdd(&a.st[inst].fnorm, ff);
-                atomicAdd(&a.st[inst].vnorm, vv);
-            }
-            atomicMax(&a.st[inst].fmax_bits, (unsigned long long)__double_as_longlong(fm));
-        }
-    } else if (inst >= 0) {
-        if (!a.part) {
             atomicAdd(&a.st[inst].power, P);
             atomicAdd(&a.st[inst].fnorm, ff);
             atomicAdd(&a.st[inst].vnorm, vv);
+            atomicMax(&a.st[inst].fmax_bits, (unsigned long long)__double_as_longlong(fm));
         }
+    } else if (inst >= 0) {
+        atomicAdd(&a.st[inst].power, P);
+        atomicAdd(&a.st[inst].fnorm, ff);
+        atomicAdd(&a.st[inst].vnorm, vv);
         atomicMax(&a.st[inst].fmax_bits, (unsigned long long)__double_as_longlong(fm));
     }
 }
 
+// Deterministic mode, second half-kick: one block per chunk (FireArgs::chunk), so a block holds
+// the same dofs of its instance wherever the instance sits in the batch, and its partial sums
+// (a fixed shuffle tree, then the warps in order) depend on the instance alone. max |F|^2 is an
+// integer maximum of bit patterns, exact in any order.
+__global__ void __launch_bounds__(FIRE_BLOCK) k_fire_vv2_chunks(FireArgs a)
+{
+    __shared__ double s_red[3][FIRE_BLOCK / 32];
+    if (a.ctl && a.ctl->halt) return;  // uniform across the grid
+    const int2 ch = a.chunk[blockIdx.x];
+    const FireInst &st = a.st[ch.x];
+    if (st.converged) return;  // uniform across the block
+    const Inst &in = a.inst[ch.x];
+    const int end = in.nv > 0 ? in.voff + in.nv : in.off + in.n;
+    const int i = ch.y + threadIdx.x;
+    double P = 0, ff = 0, vv = 0, fm = 0;
+    if (i < end) {
+        const double dt = st.dt;
+        double2 v = a.vel[i], f = a.F[i];
+        v.x = __dadd_rn(v.x, __dmul_rn(__dmul_rn(0.5, dt), f.x));
+        v.y = __dadd_rn(v.y, __dmul_rn(__dmul_rn(0.5, dt), f.y));
+        a.vel[i] = v;
+        P = f.x * v.x + f.y * v.y;
+        ff = f.x * f.x + f.y * f.y;
+        vv = v.x * v.x + v.y * v.y;
+        fm = ff;
+    }
+    const unsigned full = 0xffffffffu;
+    for (int off = 16; off > 0; off >>= 1) {
+        P += __shfl_down_sync(full, P, off);
+        ff += __shfl_down_sync(full, ff, off);
+        vv += __shfl_down_sync(full, vv, off);
+        fm = fmax(fm, __shfl_down_sync(full, fm, off));
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_red[0][w] = P;
+        s_red[1][w] = ff;
+        s_red[2][w] = vv;
+        atomicMax(&a.st[ch.x].fmax_bits, (unsigned long long)__double_as_longlong(fm));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tp = 0, tf = 0, tv = 0;
+        for (int k = 0; k < FIRE_BLOCK / 32; ++k) {
+            tp += s_red[0][k];
+            tf += s_red[1][k];
+            tv += s_red[2][k];
+        }
+        a.part[3 * (size_t)blockIdx.x] = tp;
+        a.part[3 * (size_t)blockIdx.x + 1] = tf;
+        a.part[3 * (size_t)blockIdx.x + 2] = tv;
+    }
+}
+
 // Deterministic mode: the power and norm sums of every unconverged instance (one block per
-// instance), in an order fixed by the instance's dof range alone: the partial sums that k_fire_vv2
-// left for the instance's whole blocks, then its dofs in blocks shared with another instance (or in
-// the array's last, short block), recomputed from F and the half-kicked v. Each thread's share and
-// the tree that joins the shares are fixed, so the sums are bit-identical on every run.
+// instance) from its chunks' partial sums, thread t taking chunks t, t + FIRE_BLOCK, ... in order,
+// then the fixed tree. The order depends on the instance's dof count alone, so the sums are
+// bit-identical on every run and in every batch that holds the instance.
 __global__ void __launch_bounds__(FIRE_BLOCK) k_fire_reduce(FireArgs a)
 {
     __shared__ double s_red[3][FIRE_BLOCK / 32];
     if (a.ctl && a.ctl->halt) return;  // uniform across the grid
     FireInst &st = a.st[blockIdx.x];
     if (st.converged) return;          // uniform across the block
-    const Inst &in = a.inst[blockIdx.x];
-    const int o = in.nv > 0 ? in.voff : in.off, n = in.nv > 0 ? in.nv : in.n;
-    const int bf = (o + FIRE_BLOCK - 1) / FIRE_BLOCK, bl = (o + n) / FIRE_BLOCK;  // whole blocks [bf, bl)
-    const int nb = max(bl - bf, 0);
-    const int lo_end = min(o + n, bf * FIRE_BLOCK), hi_start = max(lo_end, bl * FIRE_BLOCK);
-    const int nlo = lo_end - o, nhi = o + n - hi_start;
+    const int j0 = a.chunk_off[blockIdx.x], j1 = a.chunk_off[blockIdx.x + 1];
     double P = 0, ff = 0, vv = 0;
-    for (int k = threadIdx.x; k < nb + nlo + nhi; k += blockDim.x) {
-        if (k < nb) {
-            const double *q = a.part + 3 * (size_t)(bf + k);
-            P += q[0];
-            ff += q[1];
-            vv += q[2];
-        } else {
-            const int i = k - nb < nlo ? o + (k - nb) : hi_start + (k - nb - nlo);
-            const double2 v = a.vel[i], f = a.F[i];
-            P += f.x * v.x + f.y * v.y;
-            ff += f.x * f.x + f.y * f.y;
-            vv += v.x * v.x + v.y * v.y;
-        }
+    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        const double *q = a.part + 3 * (size_t)j;
+        P += q[0];
+        ff += q[1];
+        vv += q[2];
     }
     const unsigned full = 0xffffffffu;
     for (int off = 16; off > 0; off >>= 1) {

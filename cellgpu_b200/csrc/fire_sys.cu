@@ -8,7 +8,26 @@ static int fire_alloc(cg_system *s)
     CG_TRY(dalloc(s, &fs, s->n_inst));
     s->fire_st = fs;
     CG_TRY(dalloc(s, &s->fire_dofinst, ndof(s)));
-    CG_TRY(dalloc(s, &s->fire_part, 3 * (size_t)nblk(ndof(s), FIRE_BLOCK)));
+    // chunks of FIRE_BLOCK dofs counted from each instance's first dof (deterministic reductions)
+    std::vector<int2> chunk;
+    std::vector<int> chunk_off(s->n_inst + 1, 0);
+    for (int i = 0; i < s->n_inst; ++i) {
+        const Inst &in = s->h_inst[i];
+        const int o = in.nv > 0 ? in.voff : in.off, n = in.nv > 0 ? in.nv : in.n;
+        chunk_off[i] = (int)chunk.size();
+        for (int d = 0; d < n; d += FIRE_BLOCK) chunk.push_back(make_int2(i, o + d));
+    }
+    chunk_off[s->n_inst] = (int)chunk.size();
+    s->fire_nchunk = (int)chunk.size();
+    CG_TRY(dalloc(s, &s->fire_part, 3 * (size_t)std::max(1, s->fire_nchunk)));
+    CG_TRY(dalloc(s, &s->fire_chunk, (size_t)std::max(1, s->fire_nchunk)));
+    CG_TRY(dalloc(s, &s->fire_chunk_off, (size_t)s->n_inst + 1));
+    if (s->fire_nchunk > 0)
+        CG_CUDA(cudaMemcpyAsync(s->fire_chunk, chunk.data(), sizeof(int2) * chunk.size(), cudaMemcpyHostToDevice,
+                                s->stream));
+    CG_CUDA(cudaMemcpyAsync(s->fire_chunk_off, chunk_off.data(), sizeof(int) * chunk_off.size(),
+                            cudaMemcpyHostToDevice, s->stream));
+    CG_CUDA(cudaStreamSynchronize(s->stream));  // the host vectors go out of scope
     if (s->model == CG_MODEL_VORONOI) {
         CG_CUDA(cudaMemcpyAsync(s->fire_dofinst, s->cell_inst, sizeof(int) * s->N, cudaMemcpyDeviceToDevice,
                                 s->stream));
@@ -32,6 +51,8 @@ static FireArgs fire_args(cg_system *s, const cg_fire_params &prm)
     a.F = reinterpret_cast<const double2 *>(s->F);
     a.st = reinterpret_cast<FireInst *>(s->fire_st);
     a.part = s->det ? s->fire_part : nullptr;
+    a.chunk = s->fire_chunk;
+    a.chunk_off = s->fire_chunk_off;
     a.prm = prm;
     a.ctl = s->ctl;
     return a;
@@ -67,13 +88,16 @@ static void fire_forces(cg_system *s, bool test_and_repair)
     }
 }
 
-// second half-kick and the per-instance power / norm sums (in a fixed order in the deterministic mode)
+// second half-kick and the per-instance power / norm sums (deterministic mode: in an order fixed
+// by each instance's dof count, so the same in any batch)
 static void fire_vv2_reduce(cg_system *s, const FireArgs &f)
 {
-    k_fire_vv2<<<nblk(ndof(s), FIRE_BLOCK), FIRE_BLOCK, 0, s->stream>>>(f);
-    s->kernels_enqueued += 1;
     if (f.part) {
+        if (s->fire_nchunk > 0) k_fire_vv2_chunks<<<s->fire_nchunk, FIRE_BLOCK, 0, s->stream>>>(f);
         k_fire_reduce<<<s->n_inst, FIRE_BLOCK, 0, s->stream>>>(f);
+        s->kernels_enqueued += 2;
+    } else {
+        k_fire_vv2<<<nblk(ndof(s), FIRE_BLOCK), FIRE_BLOCK, 0, s->stream>>>(f);
         s->kernels_enqueued += 1;
     }
 }

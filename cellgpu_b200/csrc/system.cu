@@ -298,7 +298,10 @@ struct cg_system {
     double2 *fire_vel = nullptr;
     void *fire_st = nullptr;
     int *fire_dofinst = nullptr;
-    double *fire_part = nullptr;  // per-block partial sums of the deterministic FIRE reductions
+    double *fire_part = nullptr;  // per-chunk partial sums of the deterministic FIRE reductions
+    int2 *fire_chunk = nullptr;   // (instance, first dof) of every chunk
+    int *fire_chunk_off = nullptr;
+    int fire_nchunk = 0;
 };
 
 static void release_graph(cg_system::GraphEntry &g)

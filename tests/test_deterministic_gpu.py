@@ -240,6 +240,36 @@ def test_fire_deterministic_reaches_same_minimum(cglib):
     assert np.all(np.abs(E_det - E_atomic) < 1e-8 * np.maximum(1.0, E_atomic))
 
 
+def test_fire_batch_equals_singles_bit_for_bit(cglib):
+    """In the deterministic mode a FIRE minimisation does not depend on where the instance sits in a
+    batch: the power and norm sums run over chunks counted from the instance's first dof, so an
+    instance gets the same iterations, positions and stopping point alone and at any offset."""
+    from cellgpu_b200 import FireParams, VoronoiBatch
+    Ns = [300, 1000, 257]
+    rng = np.random.default_rng(43)
+    poss = [rng.random((n, 2)) * np.sqrt(n) for n in Ns]
+
+    def run(sel):
+        b = VoronoiBatch([Ns[i] for i in sel], [(np.sqrt(Ns[i]), np.sqrt(Ns[i])) for i in sel])
+        b.set_positions(np.concatenate([poss[i] for i in sel]))
+        b.set_deterministic(True)
+        b.triangulate()
+        b.fire_minimize(FireParams.defaults(force_cutoff=1e-10, max_iterations=3000))
+        it, fmax, _ = b.fire_state()
+        out = b.positions(), it, fmax
+        b.close()
+        return out
+
+    order = [2, 0, 1]
+    P, it, fmax = run(order)
+    off = 0
+    for j, i in enumerate(order):
+        Ps, its, fms = run([i])
+        assert np.array_equal(P[off:off + Ns[i]], Ps)
+        assert it[j] == its[0] and fmax[j] == fms[0]
+        off += Ns[i]
+
+
 def test_fire_vertex_reruns_bit_identical(cglib):
     from cellgpu_b200 import FireParams, VertexBatch
     pos, box = jittered_lattice(16, 18, 0.3, 3)
