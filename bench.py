@@ -537,8 +537,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-ensemble and vertex-model measurements")
-    ap.add_argument("--serve-requests", type=int, default=64,
-                    help="requests in the serving extra; 0 skips it")
+    ap.add_argument("--serve-requests", type=int, default=2000,
+                    help="requests in the serving extra (about 2.5 minutes for 2000); 0 skips it")
     ap.add_argument("--serve-only", action="store_true",
                     help="run only the serving stream and print its JSON line")
     ap.add_argument("--case", default="c2", choices=["c2", "c3", "c4"],
