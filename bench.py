@@ -35,6 +35,7 @@ P0, V0, DR, DT, MU = 3.8, 0.1, 1.0, 0.01, 1.0
 # A0/P0 16; W A/P 16, F 16
 FORCE_PASS_BYTES = 92
 L2_FLUSH_BYTES = 256 << 20
+REPAIR_TUNE_STEPS = 5  # cg_autotune_repair runs 12 x this many real steps
 RUNAHEAD_CYCLES = 50_000_000  # ~25 ms device spin before a timed loop so no host gap is timed
 
 
@@ -299,9 +300,11 @@ def bench_batched(cg, torch, flush, steps=5000, equil=150, plain_steps=20, plain
         st = torch.cuda.Stream()
         b._lib.cg_set_stream(b.handle, st.cuda_stream)
         b.triangulate()
-        b.spp_run(equil, dt=DT, mu=MU)
+        b.spp_run(equil - 12 * REPAIR_TUNE_STEPS, dt=DT, mu=MU)
         b.spatial_sort()
         out[f"batched_{name}_autotune"] = b.autotune()
+        # the repair grids are timed on real steps: the last 12 x REPAIR_TUNE_STEPS untimed ones
+        out[f"batched_{name}_autotune_repair"] = b.autotune_repair(REPAIR_TUNE_STEPS, dt=DT, mu=MU)
         t, done, _, rec = time_steps(cg, torch, b, st, steps - equil, flush)
         out[f"batched_{name}"] = total * done / t
         out[f"batched_{name}_ms_per_step"] = 1e3 * t / max(done, 1)
@@ -535,6 +538,8 @@ def main():
                     help="order-independent fixed-point force sums (cg_set_deterministic), the mode "
                          "Simulation.setReproducible(true) selects")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-repair-tune", action="store_true",
+                    help="keep the default repair-round grids (no cg_autotune_repair before timing)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-ensemble and vertex-model measurements")
     ap.add_argument("--serve-requests", type=int, default=2000,
@@ -632,6 +637,8 @@ def main():
         torch.cuda.synchronize()
         print(json.dumps({"force_pass_launches": args.force_pass_only, "n_cells": N_CELLS}))
         return
+    # repair-round grids timed on real steps (untimed; 12 x REPAIR_TUNE_STEPS more relaxation steps)
+    repair_tune = None if args.no_repair_tune else b.autotune_repair(REPAIR_TUNE_STEPS, dt=DT, mu=MU)
     # warm-up (untimed; graph capture happens here)
     for _ in range(max(3, args.warmup)):
         cg._lib.check(b._lib.cg_spp_enqueue(b.handle, 1, DT, MU))
@@ -733,6 +740,7 @@ def main():
         "timed_window": timed_window,
         "counters": counters,
         "equilibrate_steps": args.equilibrate,
+        "repair_autotune": repair_tune,
         "mixed_force_error_vs_fp64": mixed_err,
         **extras,
         "cpu_baseline": cpu,

@@ -89,6 +89,7 @@ SIGNATURES = {
     "cg_observables": (_i, [_vp, _d, _vp]),
     "cg_spatial_sort": (_i, [_vp]),
     "cg_autotune": (_i, [_vp, _vp, _vp]),
+    "cg_autotune_repair": (_i, [_vp, _i, _d, _d, _vp, _vp]),
     "cg_set_cell_types": (_i, [_vp, _vp]),
     "cg_set_tension": (_i, [_vp, _d]),
     "cg_set_tension_matrix": (_i, [_vp, _i, _vp]),

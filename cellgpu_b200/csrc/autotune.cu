@@ -1,11 +1,14 @@
 // cellgpu_b200 -- launch-parameter autotuner. Included by system.cu.
 //
-// Times, on the system's current state, the runtime-selectable launch parameters and keeps the
-// fastest: the launch shape of the fused force pass (2 warps per block with at least 16 blocks per
-// SM, or 4 warps with at least 8) and the cell-list bin side of the global triangulation (0.8,
-// 1.0 or 1.25 mean cell spacings; the bin arrays allocated at creation hold all three). The local
-// repair's candidate capacities are compile-time shared-memory sizes and stay fixed. Cached step
-// graphs are dropped so the next run captures the chosen shape.
+// cg_autotune times, on the system's current state, the runtime-selectable launch parameters and
+// keeps the fastest: the launch shape of the fused force pass (2 warps per block with at least 16
+// blocks per SM, or 4 warps with at least 8) and the cell-list bin side of the global triangulation
+// (0.8, 1.0 or 1.25 mean cell spacings; the bin arrays allocated at creation hold all three).
+// cg_autotune_repair times the grids of the repair round's two launches on real SPP steps, which
+// are the only way to get a representative repair load. The repair queues hold every cell of the
+// system per round, so they cannot overflow and have no capacity to tune; the local star's
+// candidate capacity is a compile-time shared-memory size. Cached step graphs are dropped so the
+// next run captures the chosen shapes.
 
 static int grid_bins(cg_system *s, double target)
 {
@@ -90,6 +93,65 @@ extern "C" int cg_autotune(cg_system *s, double *times_ms, int *choice)
     if (choice) {
         choice[0] = s->tune_force;
         choice[1] = bbest;
+    }
+    return CG_OK;
+}
+
+// Repair-round grids: k_star_local with one wave of STAR_MINB or 2 blocks per SM, k_commit_check
+// with 4, 8 or 16 blocks per SM. Each pair runs `steps` SPP steps (device noise) twice and keeps
+// the faster window (a window with a halt pays for a global rebuild), timed with events around the
+// whole call. The system advances by 2 x 6 x steps steps.
+extern "C" int cg_autotune_repair(cg_system *s, int steps, double dt, double mu, double *times_ms, int *choice)
+{
+    if (!s || steps <= 0) return set_err(CG_ERR_ARG, "bad args");
+    if (s->model != CG_MODEL_VORONOI) return CG_OK;
+    if (!s->topology_valid) CG_TRY(triangulate_sys(s));
+    const int star[2] = {148 * STAR_MINB, 148 * 2};
+    const int commit[3] = {148 * 4, 148 * 8, 148 * 16};
+    cudaEvent_t e0, e1;
+    CG_CUDA(cudaEventCreate(&e0));
+    CG_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bs = 0, bc = 1;
+    for (int i = 0; i < 2; ++i) {
+        for (int j = 0; j < 3; ++j) {
+            s->tune_star_grid = star[i];
+            s->tune_commit_grid = commit[j];
+            for (auto &g : s->graphs) release_graph(g);
+            s->graphs.clear();
+            float t = 1e30f;
+            for (int rep = 0; rep < 2; ++rep) {
+                CG_CUDA(cudaEventRecord(e0, s->stream));
+                int st = s->precision == CG_FP64 ? spp_run_t<double>(s, steps, dt, mu, nullptr)
+                                                 : spp_run_t<float>(s, steps, dt, mu, nullptr);
+                if (st) {
+                    cudaEventDestroy(e0);
+                    cudaEventDestroy(e1);
+                    return st;
+                }
+                CG_CUDA(cudaEventRecord(e1, s->stream));
+                CG_CUDA(cudaEventSynchronize(e1));
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                t = std::min(t, ms / steps);
+            }
+            if (times_ms) times_ms[3 * i + j] = t;
+            if (t < best) {
+                best = t;
+                bs = i;
+                bc = j;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->tune_star_grid = star[bs];
+    s->tune_commit_grid = commit[bc];
+    for (auto &g : s->graphs) release_graph(g);
+    s->graphs.clear();
+    if (choice) {
+        choice[0] = s->tune_star_grid;
+        choice[1] = s->tune_commit_grid;
     }
     return CG_OK;
 }

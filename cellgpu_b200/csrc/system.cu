@@ -281,6 +281,7 @@ struct cg_system {
     double *tmat = nullptr, *TE = nullptr;
     // autotuned launch choices: force-pass shape, cell-list bin side (in mean cell spacings)
     int tune_force = 0;
+    int tune_star_grid = 0, tune_commit_grid = 0;  // repair-round grids (0: the defaults)
     double bin_target = 0.8;
     // spatial sorting (allocated on first use): keys, order / inverse, staging, CUB scratch, tags
     unsigned long long *sort_key = nullptr;
@@ -365,6 +366,8 @@ static VoroArgs sys_args(cg_system *s)
     VoroArgs a;
     memset(&a, 0, sizeof(a));
     a.rows_padded = 1;  // every writer of system rows pads them with -1
+    a.star_grid = s->tune_star_grid;
+    a.commit_grid = s->tune_commit_grid;
     a.N = s->N;
     a.K = s->K;
     a.n_inst = s->n_inst;
@@ -801,17 +804,23 @@ static void finish_forces(cg_system *s, const VoroArgs &a, cudaStream_t st)
     }
 }
 
+// default grids of the repair round: one wave of k_star_local (STAR_MINB resident blocks per SM),
+// 8 blocks of k_commit_check per SM; cg_autotune_repair can choose others
+constexpr int STAR_GRID = 148 * STAR_MINB;
+constexpr int COMMIT_GRID = 148 * 8;
+
 template <typename R, int NS>
 static void launch_round_ns(const VoroArgs &a, bool forces, cudaStream_t st, unsigned long long cond, int use_cond)
 {
     constexpr int WPB = 4;
     // commit-and-check: 4 queue slots per 64-thread block, so a short queue still spreads over the SMs
     constexpr int WPB_C = 2;
-    k_star_local<WPB><<<148 * STAR_MINB, WPB * 32, 0, st>>>(a);
+    const int gs = a.star_grid > 0 ? a.star_grid : STAR_GRID, gc = a.commit_grid > 0 ? a.commit_grid : COMMIT_GRID;
+    k_star_local<WPB><<<gs, WPB * 32, 0, st>>>(a);
     if (forces)
-        k_commit_check<R, true, WPB_C, NS><<<148 * 8, WPB_C * 32, 0, st>>>(a, cond, use_cond);
+        k_commit_check<R, true, WPB_C, NS><<<gc, WPB_C * 32, 0, st>>>(a, cond, use_cond);
     else
-        k_commit_check<R, false, WPB_C, NS><<<148 * 8, WPB_C * 32, 0, st>>>(a, cond, use_cond);
+        k_commit_check<R, false, WPB_C, NS><<<gc, WPB_C * 32, 0, st>>>(a, cond, use_cond);
 }
 
 template <typename R>

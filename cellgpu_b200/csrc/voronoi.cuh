@@ -67,6 +67,7 @@ struct VoroArgs {
     unsigned long long *Ffix;  // null, or 2 x 4 words per cell: fixed-point sums of F (order-independent)
     int *nn, *nbr;
     int rows_padded;  // rows hold -1 past their length (system rows): a row can be read before its length
+    int star_grid, commit_grid;  // blocks of the repair round's two launches (0: the defaults)
     // repair
     int *mark;
     int *queue;     // (R_MAX+1) * N

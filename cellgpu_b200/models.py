@@ -104,6 +104,15 @@ class VoronoiBatch:
                 "force_shape": ["2 warps/block", "4 warps/block"][int(c[0])],
                 "bin_side": [0.8, 1.0, 1.25][int(c[1])]}
 
+    def autotune_repair(self, steps=10, dt=0.01, mu=1.0):
+        """Time the repair round's launch grids on real SPP steps (device noise) and keep the
+        fastest. The system advances by 12 * steps steps. Returns ms per step for each (star grid,
+        commit grid) pair and the chosen grids."""
+        t = np.zeros(6)
+        c = np.zeros(2, np.int32)
+        check(self._lib.cg_autotune_repair(self._h, int(steps), float(dt), float(mu), ptr(t), ptr(c)))
+        return {"ms_per_step": t.tolist(), "star_grid": int(c[0]), "commit_grid": int(c[1])}
+
     # -- spatial re-sorting
     def spatial_sort(self):
         """Reorder every instance's cells along a Hilbert curve (arrays and topology move with them)."""

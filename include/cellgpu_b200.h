@@ -356,6 +356,15 @@ int cg_get_external_forces(cg_system *sys, double *out);
  * choice (2 values) may be NULL. Voronoi systems only (a no-op for the vertex model). */
 int cg_autotune(cg_system *sys, double *times_ms, int *choice);
 
+/* Repair-launch autotuner (no counterpart in the reference): times the grids of the local repair
+ * round's two launches (k_star_local: 148 x 5 or 148 x 2 blocks; k_commit_check: 148 x 4, 8 or 16)
+ * on real SPP steps with device noise, `steps` steps twice per pair, and keeps the fastest. The
+ * system ADVANCES by 12 x steps steps (run it in place of equilibration steps). The repair queues
+ * hold every cell per round and cannot overflow, so they have no capacity to tune. times_ms (6
+ * values, ms per step, star grid major) and choice (the two grids) may be NULL. Voronoi systems only
+ * (a no-op for the vertex model). */
+int cg_autotune_repair(cg_system *sys, int steps, double dt, double mu, double *times_ms, int *choice);
+
 /* counters: topology repairs, global retriangulations, T1 flips, fallbacks (per system) */
 int cg_counters(cg_system *sys, long long *out, int n);
 

@@ -3,7 +3,7 @@
 import numpy as np
 import pytest
 
-from helpers import canonical, force_error, monolayer
+from helpers import canonical, force_error, jittered_lattice, monolayer
 
 pytestmark = pytest.mark.gpu
 
@@ -30,3 +30,33 @@ def test_autotune_keeps_results(cglib):
     b.spp_run(30, dt=0.01)
     b.enforce_topology()
     assert np.isfinite(b.energies()).all()
+
+
+def test_autotune_repair_steps_are_real_steps(cglib):
+    """cg_autotune_repair runs 12 x steps real SPP steps while it times the repair grids: in the
+    deterministic mode the tuned system is bit-identical to one that ran as many steps with the
+    default grids, and stays so when both continue (the grids change no result)."""
+    from cellgpu_b200 import VoronoiBatch
+    pos, box = jittered_lattice(30, 34, 0.3, 73)
+    N = len(pos)
+
+    def make():
+        b = VoronoiBatch([N], [box])
+        b.set_positions(pos)
+        b.set_motility(np.tile([0.5, 1.0], (N, 1)))
+        b.set_instance_seeds([5])
+        b.set_deterministic(True)
+        b.triangulate()
+        return b
+
+    a, b = make(), make()
+    r = a.autotune_repair(steps=4, dt=0.02)
+    assert r["star_grid"] in (148 * 5, 148 * 2) and r["commit_grid"] in (148 * 4, 148 * 8, 148 * 16)
+    assert all(t > 0 for t in r["ms_per_step"])
+    b.spp_run(48, dt=0.02)
+    assert a.counters()["rows_changed"] > 0
+    assert np.array_equal(a.positions(), b.positions())
+    a.spp_run(20, dt=0.02)
+    b.spp_run(20, dt=0.02)
+    assert np.array_equal(a.positions(), b.positions())
+    assert np.array_equal(a.forces(), b.forces())
