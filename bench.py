@@ -538,6 +538,9 @@ def main():
                     help="order-independent fixed-point force sums (cg_set_deterministic), the mode "
                          "Simulation.setReproducible(true) selects")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-steps", type=int, default=0,
+                    help="run this many SPP steps through plain kernel launches (supplied noise, no "
+                         "graph) after preparing the state, then exit (profiling)")
     ap.add_argument("--no-repair-tune", action="store_true",
                     help="keep the default repair-round grids (no cg_autotune_repair before timing)")
     ap.add_argument("--no-extras", action="store_true",
@@ -636,6 +639,16 @@ def main():
             cg._lib.check(b._lib.cg_launch_force_pass(b.handle, 1))
         torch.cuda.synchronize()
         print(json.dumps({"force_pass_launches": args.force_pass_only, "n_cells": N_CELLS}))
+        return
+    if args.plain_steps > 0:
+        # profiling aid: SPP steps through plain kernel launches (supplied noise, no step graph, so
+        # every repair kernel can be profiled), then exit
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(7)
+        noise = torch.randn((args.plain_steps, N_CELLS), dtype=torch.float64, device="cuda", generator=gen)
+        b.spp_run(args.plain_steps, dt=DT, mu=MU, noise=noise)
+        torch.cuda.synchronize()
+        print(json.dumps({"plain_steps": args.plain_steps, "n_cells": N_CELLS}))
         return
     # repair-round grids timed on real steps (untimed; 12 x REPAIR_TUNE_STEPS more relaxation steps)
     repair_tune = None if args.no_repair_tune else b.autotune_repair(REPAIR_TUNE_STEPS, dt=DT, mu=MU)

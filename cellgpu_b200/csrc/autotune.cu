@@ -38,7 +38,7 @@ extern "C" int cg_autotune(cg_system *s, double *times_ms, int *choice)
     CG_CUDA(cudaEventCreate(&e0));
     CG_CUDA(cudaEventCreate(&e1));
     VoroArgs a = sys_args(s);
-    const size_t fb = (s->precision == CG_FP64 ? sizeof(double2) : sizeof(float2)) * (size_t)s->N;
+    const size_t fb = sizeof(double2) * (size_t)s->N;  // forces are FP64 in every precision
     float best = 1e30f;
     double t_force[2] = {0, 0}, t_bins[3] = {0, 0, 0};
     for (int shape = 0; shape < 2; ++shape) {

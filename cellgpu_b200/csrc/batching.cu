@@ -68,7 +68,7 @@ extern "C" int cg_copy_instances(cg_system *dst, int dst_first, cg_system *src, 
     CG_TRY(dd_copy(dst, (char *)dst->AP + r2 * cd0, (const char *)src->AP + r2 * cs0, r2 * nc));
     if (dst->model == CG_MODEL_VORONOI) {
         CG_TRY(dd_copy(dst, dst->pos + cd0, src->pos + cs0, nc));
-        CG_TRY(dd_copy(dst, (char *)dst->F + r2 * cd0, (const char *)src->F + r2 * cs0, r2 * nc));
+        CG_TRY(dd_copy(dst, (char *)dst->F + 16 * cd0, (const char *)src->F + 16 * cs0, 16 * nc));  // FP64
         CG_TRY(dd_copy(dst, dst->nn + cd0, src->nn + cs0, nc));
         k_copy_rows<<<nblk(nc, 256), 256, 0, dst->stream>>>(nc, src->K, dst->K, src->nbr + (size_t)cs0 * src->K,
                                                           dst->nbr + (size_t)cd0 * dst->K, dc);
@@ -88,7 +88,7 @@ extern "C" int cg_copy_instances(cg_system *dst, int dst_first, cg_system *src, 
     } else {
         const int vs0 = s0.voff, vd0 = d0.voff, dv = vd0 - vs0;
         CG_TRY(dd_copy(dst, dst->pos + vd0, src->pos + vs0, nv));
-        CG_TRY(dd_copy(dst, (char *)dst->F + r2 * vd0, (const char *)src->F + r2 * vs0, r2 * nv));
+        CG_TRY(dd_copy(dst, (char *)dst->F + 16 * vd0, (const char *)src->F + 16 * vs0, 16 * nv));
         k_copy_shift<<<nblk(3 * nv, 256), 256, 0, dst->stream>>>(3ll * nv, src->vn + 3 * (size_t)vs0,
                                                                   dst->vn + 3 * (size_t)vd0, dv);
         k_copy_shift<<<nblk(3 * nv, 256), 256, 0, dst->stream>>>(3ll * nv, src->vcn + 3 * (size_t)vs0,

@@ -3,7 +3,10 @@
 // conventions of velocityVerletCPU (:120-151) and fireStepCPU (:212-264): forceMax = max |F|^2,
 // dt clamped below by dt_min, the mix uses the forces just computed. Per-instance dt, alpha,
 // counters and the power / norm reductions live in device memory; an iteration is a handful of
-// kernels with no host round trip, and converged instances stop moving.
+// kernels with no host round trip, and converged instances stop moving. An iteration's kernels:
+// k_fire_mix_vv1 (the previous iteration's velocity mix, the first Verlet half, F zeroed), the
+// model's topology and force kernels, k_fire_vv2 (second half, sums, and in its last block the
+// per-instance update that decides the next mix).
 
 namespace cg {
 
@@ -13,6 +16,11 @@ struct FireInst {
     unsigned long long fmax_bits;  // max |F|^2 as the bit pattern of a non-negative double
     double fmax;                   // max |F|^2 of the last completed iteration
     double fnorm_last;             // sum |F|^2 of the last completed iteration
+    // the FIRE velocity mix that an iteration's update decided, applied by the next iteration's
+    // first kernel while mix_seq != mix_done: v <- 0 (mix_zero), else v <- (1 - mix_a) v +
+    // mix_a mix_s F (mix_a: alpha before the update, mix_s = sqrt(|v|^2 / |F|^2))
+    double mix_a, mix_s;
+    int mix_zero, mix_seq, mix_done;
     int n_since, iterations, converged, ndof;
 };
 
@@ -23,7 +31,7 @@ struct FireArgs {
     const Inst *inst;
     const int *dof_inst;
     double2 *pos, *vel;
-    const double2 *F;
+    double2 *F;
     FireInst *st;
     // deterministic mode: the dofs of every instance in chunks of FIRE_BLOCK counted from the
     // instance's first dof (chunk[j] = (instance, first dof); the chunks of instance i are
@@ -32,31 +40,89 @@ struct FireArgs {
     double *part;
     const int2 *chunk;
     const int *chunk_off;
+    unsigned *blocks_done;              // finished blocks of k_fire_vv2 (zero between launches)
+    unsigned long long *iter_counter;   // executed FIRE iterations (a device counter)
+    int zero_f;                         // k_fire_mix_vv1 zeroes F after reading it
     cg_fire_params prm;
     const Ctl *ctl;  // a halted step (pending global rebuild) freezes the iteration
 };
 
-// velocity Verlet, first half: d = dt v + dt^2/2 F ; v += dt/2 F ; move and wrap
-__global__ void k_fire_vv1(FireArgs a)
+// Start of an iteration: the velocity mix that the previous iteration's update decided (with that
+// iteration's forces, which F still holds), then the first velocity Verlet half: d = dt v +
+// dt^2/2 F ; v += dt/2 F ; move and wrap. With zero_f, F is then zeroed for the force kernels that
+// accumulate into it (every dof: the forces of stopped instances are recomputed too).
+__global__ void k_fire_mix_vv1(FireArgs a)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.ndof) return;
     if (a.ctl && a.ctl->halt) return;
     int inst = a.dof_inst[i];
     const FireInst &st = a.st[inst];
-    if (st.converged) return;
-    const Inst &in = a.inst[inst];
-    double dt = st.dt;
     double2 v = a.vel[i], f = a.F[i];
-    double dx = __dadd_rn(__dmul_rn(dt, v.x), __dmul_rn(__dmul_rn(__dmul_rn(0.5, dt), dt), f.x));
-    double dy = __dadd_rn(__dmul_rn(dt, v.y), __dmul_rn(__dmul_rn(__dmul_rn(0.5, dt), dt), f.y));
-    v.x = __dadd_rn(v.x, __dmul_rn(__dmul_rn(0.5, dt), f.x));
-    v.y = __dadd_rn(v.y, __dmul_rn(__dmul_rn(0.5, dt), f.y));
-    a.vel[i] = v;
-    double2 p = a.pos[i];
-    p.x = __dadd_rn(p.x, dx);
-    p.y = __dadd_rn(p.y, dy);
-    a.pos[i] = put_in_box(p, in.Lx, in.Ly, in.iLx, in.iLy);
+    bool store_v = false;
+    if (st.mix_seq != st.mix_done) {
+        if (st.mix_zero) {
+            v = make_double2(0.0, 0.0);
+        } else {
+            double scaling = st.mix_s;
+            double al = st.mix_a;
+            v.x = (1.0 - al) * v.x + al * scaling * f.x;
+            v.y = (1.0 - al) * v.y + al * scaling * f.y;
+        }
+        store_v = true;
+    }
+    if (!st.converged) {
+        const Inst &in = a.inst[inst];
+        double dt = st.dt;
+        double dx = __dadd_rn(__dmul_rn(dt, v.x), __dmul_rn(__dmul_rn(__dmul_rn(0.5, dt), dt), f.x));
+        double dy = __dadd_rn(__dmul_rn(dt, v.y), __dmul_rn(__dmul_rn(__dmul_rn(0.5, dt), dt), f.y));
+        v.x = __dadd_rn(v.x, __dmul_rn(__dmul_rn(0.5, dt), f.x));
+        v.y = __dadd_rn(v.y, __dmul_rn(__dmul_rn(0.5, dt), f.y));
+        store_v = true;
+        double2 p = a.pos[i];
+        p.x = __dadd_rn(p.x, dx);
+        p.y = __dadd_rn(p.y, dy);
+        a.pos[i] = put_in_box(p, in.Lx, in.Ly, in.iLx, in.iLy);
+    }
+    if (store_v) a.vel[i] = v;
+    if (a.zero_f) a.F[i] = make_double2(0.0, 0.0);
+}
+
+// End of an iteration for one instance whose sums are complete (fireStepCPU's decisions): the mix
+// for the next iteration's first kernel, with the alpha before this update; dt / alpha / N_since;
+// the iteration count and the convergence test of the loop head; the sums are cleared for the next
+// iteration. The mix that the previous update decided has been applied by now (mix_done).
+// Volatile: the last block of k_fire_vv2 reads sums that other blocks added.
+CG_D void fire_update(volatile FireInst &st, const cg_fire_params &p, unsigned long long *iter_counter)
+{
+    st.mix_done = st.mix_seq;
+    if (st.converged) return;
+    const double power = st.power, fnorm = st.fnorm, vnorm = st.vnorm;
+    st.mix_zero = !(power > 0) ? 1 : 0;
+    st.mix_s = fnorm > 0. ? sqrt(vnorm / fnorm) : 0.0;
+    st.mix_a = st.alpha;
+    st.mix_seq = st.mix_seq + 1;
+    st.iterations = st.iterations + 1;
+    atomicAdd(iter_counter, 1ull);
+    if (power > 0) {
+        if (st.n_since > p.n_min) {
+            st.dt = fmin(st.dt * p.dt_inc, p.dt_max);
+            st.alpha = st.alpha * p.alpha_dec;
+        }
+        st.n_since = st.n_since + 1;
+    } else {
+        double dt = st.dt * p.dt_dec;
+        st.dt = fmax(dt, p.dt_min);
+        st.alpha = p.alpha_start;
+    }
+    const double fmax = __longlong_as_double((long long)st.fmax_bits);
+    st.fmax = fmax;
+    st.fnorm_last = fnorm;
+    st.converged = !(st.iterations < p.max_iterations && sqrt(fmax) > p.force_cutoff) ? 1 : 0;
+    st.power = 0;
+    st.fnorm = 0;
+    st.vnorm = 0;
+    st.fmax_bits = 0;
 }
 
 // second half-kick with the new forces, then the FIRE reductions per instance. Degrees of freedom
@@ -118,12 +184,8 @@ __global__ void __launch_bounds__(256) k_fire_vv2(FireArgs a)
             atomicAdd(&a.st[b0].vnorm, tv);
             atomicMax(&a.st[b0].fmax_bits, (unsigned long long)__double_as_longlong(tm));
         }
-        return;
-    }
-    // warp-level segmented reduction (lanes of one instance are contiguous)
-    int first = __shfl_sync(full, inst, 0);
-    bool uniform = __all_sync(full, inst == first);
-    if (uniform) {
+    } else if (__all_sync(full, inst == __shfl_sync(full, inst, 0))) {
+        // warp-level segmented reduction (lanes of one instance are contiguous)
         for (int off = 16; off > 0; off >>= 1) {
             P += __shfl_down_sync(full, P, off);
             ff += __shfl_down_sync(full, ff, off);
@@ -142,6 +204,19 @@ __global__ void __launch_bounds__(256) k_fire_vv2(FireArgs a)
         atomicAdd(&a.st[inst].vnorm, vv);
         atomicMax(&a.st[inst].fmax_bits, (unsigned long long)__double_as_longlong(fm));
     }
+    // the last block to finish updates every instance (threadfence reduction: each block's sums
+    // are visible before its count is)
+    __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(a.blocks_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int k = threadIdx.x; k < a.n_inst; k += blockDim.x) fire_update(a.st[k], a.prm, a.iter_counter);
+    if (threadIdx.x == 0) *a.blocks_done = 0;
 }
 
 // Deterministic mode, second half-kick: one block per chunk (FireArgs::chunk), so a block holds
@@ -207,7 +282,10 @@ __global__ void __launch_bounds__(FIRE_BLOCK) k_fire_reduce(FireArgs a)
     __shared__ double s_red[3][FIRE_BLOCK / 32];
     if (a.ctl && a.ctl->halt) return;  // uniform across the grid
     FireInst &st = a.st[blockIdx.x];
-    if (st.converged) return;          // uniform across the block
+    if (st.converged) {  // uniform across the block
+        if (threadIdx.x == 0) fire_update(st, a.prm, a.iter_counter);  // (acknowledges the last mix)
+        return;
+    }
     const int j0 = a.chunk_off[blockIdx.x], j1 = a.chunk_off[blockIdx.x + 1];
     double P = 0, ff = 0, vv = 0;
     for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
@@ -239,62 +317,10 @@ __global__ void __launch_bounds__(FIRE_BLOCK) k_fire_reduce(FireArgs a)
         st.power = tp;
         st.fnorm = tf;
         st.vnorm = tv;
+        fire_update(st, a.prm, a.iter_counter);
     }
 }
 
-// FIRE mix v <- (1-alpha) v + alpha sqrt(|v|^2/|F|^2) F, or v <- 0 when the power is not positive
-__global__ void k_fire_mix(FireArgs a)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.ndof) return;
-    if (a.ctl && a.ctl->halt) return;
-    const FireInst &st = a.st[a.dof_inst[i]];
-    if (st.converged) return;
-    if (!(st.power > 0)) {
-        a.vel[i] = make_double2(0.0, 0.0);
-        return;
-    }
-    double scaling = st.fnorm > 0. ? sqrt(st.vnorm / st.fnorm) : 0.0;
-    double al = st.alpha;
-    double2 v = a.vel[i], f = a.F[i];
-    v.x = (1.0 - al) * v.x + al * scaling * f.x;
-    v.y = (1.0 - al) * v.y + al * scaling * f.y;
-    a.vel[i] = v;
-}
-
-// per instance: dt / alpha / N_since update, iteration count, convergence test of the loop head
-__global__ void k_fire_update(FireArgs a, unsigned long long *iter_counter)
-{
-    int inst = blockIdx.x * blockDim.x + threadIdx.x;
-    if (inst >= a.n_inst) return;
-    if (a.ctl && a.ctl->halt) return;
-    FireInst &st = a.st[inst];
-    if (st.converged) return;
-    st.iterations += 1;
-    atomicAdd(iter_counter, 1ull);
-    const cg_fire_params &p = a.prm;
-    if (st.power > 0) {
-        if (st.n_since > p.n_min) {
-            st.dt = fmin(st.dt * p.dt_inc, p.dt_max);
-            st.alpha = st.alpha * p.alpha_dec;
-        }
-        st.n_since += 1;
-    } else {
-        st.dt = st.dt * p.dt_dec;
-        st.dt = fmax(st.dt, p.dt_min);
-        st.alpha = p.alpha_start;
-    }
-    st.fmax = __longlong_as_double((long long)st.fmax_bits);
-    st.fnorm_last = st.fnorm;
-    st.converged = !(st.iterations < p.max_iterations && sqrt(st.fmax) > p.force_cutoff);
-    st.power = 0;
-    st.fnorm = 0;
-    st.vnorm = 0;
-    st.fmax_bits = 0;
-}
-
-// fresh FIRE state for the instances in [lo, hi) (all of them at the start of a minimisation; the
-// newly admitted ones when a serving batch is rebuilt around running instances)
 __global__ void k_fire_init(FireArgs a, int lo, int hi)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -310,6 +336,8 @@ __global__ void k_fire_init(FireArgs a, int lo, int hi)
         s.fmax_bits = 0;
         s.fmax = 110.0;  // minimize() starts the loop with forceMax = 110
         s.fnorm_last = 0;
+        s.mix_a = s.mix_s = 0;
+        s.mix_zero = s.mix_seq = s.mix_done = 0;
         s.n_since = 0;
         s.iterations = 0;
         s.converged = !(0 < a.prm.max_iterations && sqrt(110.0) > a.prm.force_cutoff);

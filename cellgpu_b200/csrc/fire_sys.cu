@@ -22,6 +22,7 @@ static int fire_alloc(cg_system *s)
     CG_TRY(dalloc(s, &s->fire_part, 3 * (size_t)std::max(1, s->fire_nchunk)));
     CG_TRY(dalloc(s, &s->fire_chunk, (size_t)std::max(1, s->fire_nchunk)));
     CG_TRY(dalloc(s, &s->fire_chunk_off, (size_t)s->n_inst + 1));
+    CG_TRY(dalloc(s, &s->fire_blocks_done, 1));
     if (s->fire_nchunk > 0)
         CG_CUDA(cudaMemcpyAsync(s->fire_chunk, chunk.data(), sizeof(int2) * chunk.size(), cudaMemcpyHostToDevice,
                                 s->stream));
@@ -48,34 +49,30 @@ static FireArgs fire_args(cg_system *s, const cg_fire_params &prm)
     a.dof_inst = s->fire_dofinst;
     a.pos = s->pos;
     a.vel = s->fire_vel;
-    a.F = reinterpret_cast<const double2 *>(s->F);
+    a.F = reinterpret_cast<double2 *>(s->F);
     a.st = reinterpret_cast<FireInst *>(s->fire_st);
     a.part = s->det ? s->fire_part : nullptr;
     a.chunk = s->fire_chunk;
     a.chunk_off = s->fire_chunk_off;
+    a.blocks_done = s->fire_blocks_done;
+    a.iter_counter = &s->ctl->counters[6];
+    a.zero_f = s->det ? 0 : 1;  // the deterministic mode sums into Ffix, which is cleared by memset
     a.prm = prm;
     a.ctl = s->ctl;
     return a;
 }
 
-// forces on the current topology (the loop head of minimize: computeForces before the loop)
-static void fire_forces(cg_system *s, bool test_and_repair)
+// forces on the current topology (the loop head of minimize: computeForces before the loop).
+// f_zeroed: F is already zero (k_fire_mix_vv1 cleared it), so its memset is left out.
+static void fire_forces(cg_system *s, bool test_and_repair, bool f_zeroed = false)
 {
     if (s->model == CG_MODEL_VORONOI) {
         VoroArgs a = sys_args(s);
-        if (s->precision == CG_FP64) {
-            launch_force_test<double>(s, a, test_and_repair);
-            if (test_and_repair)
-                launch_repair<double>(s, a, true);
-            else
-                finish_forces<double>(s, a, s->stream);
-        } else {
-            launch_force_test<float>(s, a, test_and_repair);
-            if (test_and_repair)
-                launch_repair<float>(s, a, true);
-            else
-                finish_forces<float>(s, a, s->stream);
-        }
+        launch_force_test<double>(s, a, test_and_repair, !f_zeroed);
+        if (test_and_repair)
+            launch_repair<double>(s, a, true);
+        else
+            finish_forces<double>(s, a, s->stream);
         if (test_and_repair) {
             k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 0);
             s->kernels_enqueued += 1;
@@ -83,7 +80,7 @@ static void fire_forces(cg_system *s, bool test_and_repair)
     } else {
         VertArgs a = vm_args(s);
         if (test_and_repair) vm_launch_t1(s, a);
-        launch_vm_forces(s, a);
+        launch_vm_forces(s, a, !f_zeroed);
         s->kernels_enqueued += 1;
     }
 }
@@ -102,17 +99,24 @@ static void fire_vv2_reduce(cg_system *s, const FireArgs &f)
     }
 }
 
-// one FIRE iteration: velocity Verlet (move, topology, forces), then the FIRE step
+// one FIRE iteration: the previous iteration's velocity mix and the first Verlet half (move),
+// topology and forces, then the second half with the sums and the per-instance update
 static void fire_enqueue_iteration(cg_system *s, const cg_fire_params &prm)
 {
     FireArgs f = fire_args(s, prm);
-    int nd = ndof(s);
-    k_fire_vv1<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
-    fire_forces(s, true);
+    k_fire_mix_vv1<<<nblk(ndof(s), 256), 256, 0, s->stream>>>(f);
+    s->kernels_enqueued += 1;
+    fire_forces(s, true, f.zero_f != 0);
     fire_vv2_reduce(s, f);
-    k_fire_mix<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
-    k_fire_update<<<nblk(s->n_inst, 64), 64, 0, s->stream>>>(f, &s->ctl->counters[6]);
-    s->kernels_enqueued += 3;
+}
+
+// FIRE reads and moves FP64 positions and forces: mixed-precision Voronoi systems (FP32 forces)
+// are refused
+static int fire_check(cg_system *s)
+{
+    if (s->model == CG_MODEL_VORONOI && s->precision != CG_FP64)
+        return set_err(CG_ERR_ARG, "FIRE needs an FP64 system");
+    return CG_OK;
 }
 
 // Start a minimisation: per-instance FIRE state reset (EnergyMinimizerFIRE's initial dt, alpha and
@@ -120,6 +124,7 @@ static void fire_enqueue_iteration(cg_system *s, const cg_fire_params &prm)
 extern "C" int cg_fire_begin(cg_system *s, const cg_fire_params *prm)
 {
     if (!s || !prm || prm->max_iterations < 0 || !(prm->dt > 0)) return set_err(CG_ERR_ARG, "bad args");
+    CG_TRY(fire_check(s));
     if (!s->topology_valid) {
         if (s->model == CG_MODEL_VORONOI) CG_TRY(triangulate_sys(s));
         else return set_err(CG_ERR_STATE, "vertex topology not set");
@@ -139,6 +144,7 @@ extern "C" int cg_fire_begin_instances(cg_system *s, const cg_fire_params *prm, 
     if (!s || !prm || prm->max_iterations < 0 || !(prm->dt > 0) || first < 0 || count < 0 ||
         first + count > s->n_inst)
         return set_err(CG_ERR_ARG, "bad args");
+    CG_TRY(fire_check(s));
     if (!s->topology_valid) {
         if (s->model == CG_MODEL_VORONOI) CG_TRY(triangulate_sys(s));
         else return set_err(CG_ERR_STATE, "vertex topology not set");
@@ -201,10 +207,7 @@ extern "C" int cg_fire_advance(cg_system *s, const cg_fire_params *prm, int iter
             if (s->model == CG_MODEL_VORONOI) CG_TRY(recover(s));
             else CG_TRY(vm_recover(s, nullptr));
             fire_forces(s, false);
-            int nd = ndof(s);
             fire_vv2_reduce(s, f);
-            k_fire_mix<<<nblk(nd, 256), 256, 0, s->stream>>>(f);
-            k_fire_update<<<nblk(s->n_inst, 64), 64, 0, s->stream>>>(f, &s->ctl->counters[6]);
             CG_TRY(check_launch());
         }
         if (++rounds > prm->max_iterations / chunk + 64) return set_err(CG_ERR_STATE, "FIRE did not stop");

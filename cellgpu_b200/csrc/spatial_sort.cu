@@ -148,7 +148,7 @@ extern "C" int cg_spatial_sort(cg_system *s)
     CG_TRY(sort_gather(s, s->motility, sizeof(double2), order));
     CG_TRY(sort_gather(s, s->APpref, sizeof(double2), order));
     CG_TRY(sort_gather(s, s->AP, r2, order));
-    CG_TRY(sort_gather(s, s->F, r2, order));
+    CG_TRY(sort_gather(s, s->F, sizeof(double2), order));  // forces are FP64 in every precision
     CG_TRY(sort_gather(s, s->tags, sizeof(int), order));
     if (s->obs_ref) CG_TRY(sort_gather(s, s->obs_ref, sizeof(double2), order));
     if (s->ctype) CG_TRY(sort_gather(s, s->ctype, sizeof(int), order));

@@ -303,6 +303,7 @@ struct cg_system {
     int2 *fire_chunk = nullptr;   // (instance, first dof) of every chunk
     int *fire_chunk_off = nullptr;
     int fire_nchunk = 0;
+    unsigned *fire_blocks_done = nullptr;  // k_fire_vv2's finished-block count
 };
 
 static void release_graph(cg_system::GraphEntry &g)
@@ -411,7 +412,7 @@ static VoroArgs sys_args(cg_system *s)
 static size_t voronoi_bytes(int N, int K, int n_bins, int n_inst, int precision)
 {
     size_t real2 = precision == CG_FP64 ? 16 : 8;
-    size_t per_cell = 4 /*cell_inst*/ + 4 /*held*/ + 4 /*undec*/ + 16 * 3 /*pos, motility, APpref*/ + 8 /*theta*/ + 2 * real2 +
+    size_t per_cell = 4 /*cell_inst*/ + 4 /*held*/ + 4 /*undec*/ + 16 * 3 /*pos, motility, APpref*/ + 8 /*theta*/ + real2 /*AP*/ + 16 /*F*/ +
                       4 + 4 * (size_t)K /*nn, nbr*/ + 4 /*mark*/ + 4 * (R_MAX + 1) /*queue*/ + 4 +
                       4 * (size_t)K /*stage*/ + 4 * 2 /*qslot*/ + 4 * 3 + 16 /*cell list*/ +
                       8 + 8 /*noise staging, device draw*/;
@@ -472,7 +473,7 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
         if ((st = dalloc(s, &s->APpref, Nt))) break;
         if ((st = dalloc(s, &s->theta, Nt))) break;
         if ((st = dalloc(s, (char **)&s->AP, r2 * Nt))) break;
-        if ((st = dalloc(s, (char **)&s->F, r2 * Nt))) break;
+        if ((st = dalloc(s, (char **)&s->F, sizeof(double2) * Nt))) break;  // FP64 in every precision
         if ((st = dalloc(s, &s->nn, Nt))) break;
         if ((st = dalloc(s, &s->nbr, (size_t)Nt * K))) break;
         if ((st = dalloc(s, &s->mark, Nt))) break;
@@ -656,7 +657,7 @@ static int get_real2(cg_system *s, const void *src, double *dst, int n)
 extern "C" int cg_get_forces(cg_system *s, double *F)
 {
     if (!s || !F) return set_err(CG_ERR_ARG, "bad args");
-    return get_real2(s, s->F, F, ndof(s));
+    return d2h(s, F, s->F, sizeof(double2) * ndof(s));  // forces are FP64 in every precision
 }
 extern "C" int cg_get_area_perimeter(cg_system *s, double *AP)
 {
@@ -776,13 +777,12 @@ extern "C" int cg_voronoi_triangulate(const double *pos, int N, double Lx, doubl
 
 // ---- one step of the Voronoi model ---------------------------------------------------------
 template <typename R>
-static void launch_force_test(cg_system *s, const VoroArgs &a, bool test)
+static void launch_force_test(cg_system *s, const VoroArgs &a, bool test, bool clear_f = true)
 {
     if (a.Ffix)
         cudaMemsetAsync(a.Ffix, 0, 2 * FIXF * sizeof(unsigned long long) * s->N, s->stream);
-    else
-        cudaMemsetAsync(s->F, 0, (s->precision == CG_FP64 ? sizeof(double2) : sizeof(float2)) * s->N,
-                        s->stream);
+    else if (clear_f)
+        cudaMemsetAsync(s->F, 0, sizeof(double2) * s->N, s->stream);
     if (test)
         launch_groups<R, true, true>(a, s->N, s->stream, s->tune_force);
     else

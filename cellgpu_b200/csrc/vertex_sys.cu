@@ -40,11 +40,12 @@ static VertArgs vm_args(cg_system *s)
 
 // forces + geometry of every cell (F zeroed first): 8 lanes per cell for rows up to 32 vertices,
 // else a thread per cell; the deterministic mode then converts its fixed-point sums into F
-static void launch_vm_forces(cg_system *s, const VertArgs &a)
+// clear_f = false: F is already zero (the caller's previous kernel cleared it)
+static void launch_vm_forces(cg_system *s, const VertArgs &a, bool clear_f = true)
 {
     if (a.Ffix)
         cudaMemsetAsync(a.Ffix, 0, 2 * FIXF * sizeof(unsigned long long) * s->Nv, s->stream);
-    else
+    else if (clear_f)
         cudaMemsetAsync(s->F, 0, sizeof(double2) * s->Nv, s->stream);
     if (s->vmax <= VM_ROW_G)
         k_vm_forces_groups<4><<<nblk(s->N, 4 * (32 / VM_G)), 128, 0, s->stream>>>(a, 1);

@@ -91,7 +91,11 @@ CG_D void atomic_add2<double>(void *F, int i, double x, double y)
 template <>
 CG_D void atomic_add2<float>(void *F, int i, float x, float y)
 {
-    atomicAdd(reinterpret_cast<float2 *>(F) + i, make_float2(x, y));
+    // forces are stored and summed in FP64 in every precision: the FP32 terms of the mixed mode
+    // are added without FP32 rounding of the sum
+    double *f = reinterpret_cast<double *>(F) + 2 * (size_t)i;
+    atomicAdd(f, (double)x);
+    atomicAdd(f + 1, (double)y);
 }
 
 // Order-independent sums (deterministic mode, VoroArgs::Ffix set). A value x is kept in FIXW = 3
@@ -1333,10 +1337,10 @@ __global__ void k_apply_exclusions(int N, const int *excl, void *F, double2 *ext
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= N || !excl[c]) return;
-    typename Vec2<R>::T *f = reinterpret_cast<typename Vec2<R>::T *>(F) + c;
-    const typename Vec2<R>::T v = *f;
-    ext[c] = make_double2(-(double)v.x, -(double)v.y);
-    *f = mk<R>(R(0), R(0));
+    double2 *f = reinterpret_cast<double2 *>(F) + c;
+    const double2 v = *f;
+    ext[c] = make_double2(-v.x, -v.y);
+    *f = make_double2(0.0, 0.0);
 }
 
 // end of a step: reset the per-step queue counters and advance the claim epoch
@@ -1492,8 +1496,8 @@ template <typename R>
 CG_D void spp_cell(const VoroArgs &a, int c, double xi, double dt, double mu, int zero_force)
 {
     const Inst &in = inst_of(a, c);
-    typename Vec2<R>::T f = reinterpret_cast<typename Vec2<R>::T *>(a.F)[c];
-    double fx = (double)f.x, fy = (double)f.y;
+    const double2 f = reinterpret_cast<const double2 *>(a.F)[c];  // FP64 in every precision
+    double fx = f.x, fy = f.y;
     double2 mot = a.motility[c];
     double th = a.theta[c];
     double s, co;
@@ -1508,7 +1512,7 @@ CG_D void spp_cell(const VoroArgs &a, int c, double xi, double dt, double mu, in
     p.x = __dadd_rn(p.x, dx);
     p.y = __dadd_rn(p.y, dy);
     a.pos[c] = put_in_box(p, in.Lx, in.Ly, in.iLx, in.iLy);
-    if (zero_force) reinterpret_cast<typename Vec2<R>::T *>(a.F)[c] = mk<R>(R(0), R(0));
+    if (zero_force) reinterpret_cast<double2 *>(a.F)[c] = make_double2(0.0, 0.0);
 }
 
 // device noise of cell c: component (l & 1) of the Box-Muller pair with Philox counter
@@ -1555,7 +1559,7 @@ __global__ void k_fix_forces(VoroArgs a)
     if (i >= a.N) return;
     const ulonglong2 *w = reinterpret_cast<const ulonglong2 *>(a.Ffix) + 4 * (size_t)i;  // 2 FIXF words
     const ulonglong2 w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
-    reinterpret_cast<typename Vec2<R>::T *>(a.F)[i] = mk<R>((R)fix_force_value(w0, w1), (R)fix_force_value(w2, w3));
+    reinterpret_cast<double2 *>(a.F)[i] = make_double2(fix_force_value(w0, w1), fix_force_value(w2, w3));
 }
 
 // The same normals for every cell of the current step, into out[N]. The step graph runs this

@@ -139,6 +139,18 @@ def test_fire_voronoi_golden(cglib):
     assert np.array_equal(canonical(nn, nbr), canonical(g["nn1"], g["nbr1"]))
 
 
+def test_fire_refuses_mixed_precision(cglib):
+    """FIRE moves FP64 positions with FP64 forces: a mixed-precision Voronoi system (FP32 forces)
+    is refused with an argument error instead of being read as FP64."""
+    from cellgpu_b200 import CG_MIXED, CellGPUError, FireParams, VoronoiBatch
+    pos, box = monolayer(300, 81)
+    b = VoronoiBatch([len(pos)], [box], precision=CG_MIXED)
+    b.set_positions(pos)
+    b.triangulate()
+    with pytest.raises(CellGPUError):
+        b.fire_minimize(FireParams.defaults(force_cutoff=1e-10, max_iterations=100))
+
+
 def test_fire_vertex_golden(cglib):
     from cellgpu_b200 import FireParams, VertexBatch
     g = _gold("fire_vertex_*.npz")
