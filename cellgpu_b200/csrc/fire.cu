@@ -92,37 +92,56 @@ __global__ void k_fire_mix_vv1(FireArgs a)
 // for the next iteration's first kernel, with the alpha before this update; dt / alpha / N_since;
 // the iteration count and the convergence test of the loop head; the sums are cleared for the next
 // iteration. The mix that the previous update decided has been applied by now (mix_done).
-// Volatile: the last block of k_fire_vv2 reads sums that other blocks added.
-CG_D void fire_update(volatile FireInst &st, const cg_fire_params &p, unsigned long long *iter_counter)
+// The state is read with L2 loads issued together (the last block of k_fire_vv2 reads sums that
+// other blocks added, which its L1 may hold stale), updated in registers and stored back.
+CG_D void fire_update(FireInst *sp, const cg_fire_params &p, unsigned long long *iter_counter)
 {
+    FireInst st;
+    st.dt = __ldcg(&sp->dt);
+    st.alpha = __ldcg(&sp->alpha);
+    st.power = __ldcg(&sp->power);
+    st.fnorm = __ldcg(&sp->fnorm);
+    st.vnorm = __ldcg(&sp->vnorm);
+    st.fmax_bits = __ldcg(&sp->fmax_bits);
+    st.fmax = __ldcg(&sp->fmax);
+    st.fnorm_last = __ldcg(&sp->fnorm_last);
+    st.mix_a = __ldcg(&sp->mix_a);
+    st.mix_s = __ldcg(&sp->mix_s);
+    st.mix_zero = __ldcg(&sp->mix_zero);
+    st.mix_seq = __ldcg(&sp->mix_seq);
+    st.mix_done = __ldcg(&sp->mix_done);
+    st.n_since = __ldcg(&sp->n_since);
+    st.iterations = __ldcg(&sp->iterations);
+    st.converged = __ldcg(&sp->converged);
+    st.ndof = __ldcg(&sp->ndof);
     st.mix_done = st.mix_seq;
-    if (st.converged) return;
-    const double power = st.power, fnorm = st.fnorm, vnorm = st.vnorm;
-    st.mix_zero = !(power > 0) ? 1 : 0;
-    st.mix_s = fnorm > 0. ? sqrt(vnorm / fnorm) : 0.0;
-    st.mix_a = st.alpha;
-    st.mix_seq = st.mix_seq + 1;
-    st.iterations = st.iterations + 1;
-    atomicAdd(iter_counter, 1ull);
-    if (power > 0) {
-        if (st.n_since > p.n_min) {
-            st.dt = fmin(st.dt * p.dt_inc, p.dt_max);
-            st.alpha = st.alpha * p.alpha_dec;
+    if (!st.converged) {
+        st.mix_zero = !(st.power > 0) ? 1 : 0;
+        st.mix_s = st.fnorm > 0. ? sqrt(st.vnorm / st.fnorm) : 0.0;
+        st.mix_a = st.alpha;
+        st.mix_seq += 1;
+        st.iterations += 1;
+        atomicAdd(iter_counter, 1ull);
+        if (st.power > 0) {
+            if (st.n_since > p.n_min) {
+                st.dt = fmin(st.dt * p.dt_inc, p.dt_max);
+                st.alpha = st.alpha * p.alpha_dec;
+            }
+            st.n_since += 1;
+        } else {
+            st.dt = st.dt * p.dt_dec;
+            st.dt = fmax(st.dt, p.dt_min);
+            st.alpha = p.alpha_start;
         }
-        st.n_since = st.n_since + 1;
-    } else {
-        double dt = st.dt * p.dt_dec;
-        st.dt = fmax(dt, p.dt_min);
-        st.alpha = p.alpha_start;
+        st.fmax = __longlong_as_double((long long)st.fmax_bits);
+        st.fnorm_last = st.fnorm;
+        st.converged = !(st.iterations < p.max_iterations && sqrt(st.fmax) > p.force_cutoff);
+        st.power = 0;
+        st.fnorm = 0;
+        st.vnorm = 0;
+        st.fmax_bits = 0;
     }
-    const double fmax = __longlong_as_double((long long)st.fmax_bits);
-    st.fmax = fmax;
-    st.fnorm_last = fnorm;
-    st.converged = !(st.iterations < p.max_iterations && sqrt(fmax) > p.force_cutoff) ? 1 : 0;
-    st.power = 0;
-    st.fnorm = 0;
-    st.vnorm = 0;
-    st.fmax_bits = 0;
+    *sp = st;
 }
 
 // second half-kick with the new forces, then the FIRE reductions per instance. Degrees of freedom
@@ -215,7 +234,7 @@ __global__ void __launch_bounds__(256) k_fire_vv2(FireArgs a)
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    for (int k = threadIdx.x; k < a.n_inst; k += blockDim.x) fire_update(a.st[k], a.prm, a.iter_counter);
+    for (int k = threadIdx.x; k < a.n_inst; k += blockDim.x) fire_update(a.st + k, a.prm, a.iter_counter);
     if (threadIdx.x == 0) *a.blocks_done = 0;
 }
 
@@ -283,7 +302,7 @@ __global__ void __launch_bounds__(FIRE_BLOCK) k_fire_reduce(FireArgs a)
     if (a.ctl && a.ctl->halt) return;  // uniform across the grid
     FireInst &st = a.st[blockIdx.x];
     if (st.converged) {  // uniform across the block
-        if (threadIdx.x == 0) fire_update(st, a.prm, a.iter_counter);  // (acknowledges the last mix)
+        if (threadIdx.x == 0) fire_update(&st, a.prm, a.iter_counter);  // (acknowledges the last mix)
         return;
     }
     const int j0 = a.chunk_off[blockIdx.x], j1 = a.chunk_off[blockIdx.x + 1];
@@ -317,7 +336,7 @@ __global__ void __launch_bounds__(FIRE_BLOCK) k_fire_reduce(FireArgs a)
         st.power = tp;
         st.fnorm = tf;
         st.vnorm = tv;
-        fire_update(st, a.prm, a.iter_counter);
+        fire_update(&st, a.prm, a.iter_counter);
     }
 }
 

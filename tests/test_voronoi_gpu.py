@@ -24,7 +24,7 @@ TOL_F64 = 1e-10
 TOL_AP = 1e-12
 TOL_MIXED_NORMWISE = 1e-6
 TOL_MIXED_RMS = 1e-6
-TOL_MIXED_MAX = 1e-5
+TOL_MIXED_MAX = 5e-6
 
 
 @pytest.fixture(scope="module")
