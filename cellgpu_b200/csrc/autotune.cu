@@ -1,8 +1,9 @@
 // cellgpu_b200 -- launch-parameter autotuner. Included by system.cu.
 //
 // cg_autotune times, on the system's current state, the runtime-selectable launch parameters and
-// keeps the fastest: the launch shape of the fused force pass (2 warps per block with at least 16
-// blocks per SM, or 4 warps with at least 8) and the cell-list bin side of the global triangulation
+// keeps the fastest: the launch shape of the fused force pass (8-lane groups with 2 warps per block
+// and at least 16 blocks per SM, or 4 warps with at least 8, or one thread per cell) and the
+// cell-list bin side of the global triangulation
 // (0.8, 1.0 or 1.25 mean cell spacings; the bin arrays allocated at creation hold all three).
 // cg_autotune_repair times the grids of the repair round's two launches on real SPP steps, which
 // are the only way to get a representative repair load. The repair queues hold every cell of the
@@ -40,8 +41,11 @@ extern "C" int cg_autotune(cg_system *s, double *times_ms, int *choice)
     VoroArgs a = sys_args(s);
     const size_t fb = sizeof(double2) * (size_t)s->N;  // forces are FP64 in every precision
     float best = 1e30f;
-    double t_force[2] = {0, 0}, t_bins[3] = {0, 0, 0};
-    for (int shape = 0; shape < 2; ++shape) {
+    double t_force[3] = {0, 0, 0}, t_bins[3] = {0, 0, 0};
+    // shape 2, the thread-per-cell form, only where it applies (FP64, atomic sums, no line
+    // tension, 16-slot rows)
+    const int n_shapes = (s->precision == CG_FP64 && thread_form_ok(a)) ? 3 : 2;
+    for (int shape = 0; shape < n_shapes; ++shape) {
         for (int rep = 0; rep < 13; ++rep) {
             if (rep == 3) cudaEventRecord(e0, s->stream);
             if (a.Ffix) cudaMemsetAsync(a.Ffix, 0, 2 * FIXF * sizeof(unsigned long long) * s->N, s->stream);
@@ -86,9 +90,8 @@ extern "C" int cg_autotune(cg_system *s, double *times_ms, int *choice)
     for (auto &g : s->graphs) release_graph(g);
     s->graphs.clear();
     if (times_ms) {
-        times_ms[0] = t_force[0];
-        times_ms[1] = t_force[1];
-        for (int k = 0; k < 3; ++k) times_ms[2 + k] = t_bins[k];
+        for (int k = 0; k < 3; ++k) times_ms[k] = t_force[k];
+        for (int k = 0; k < 3; ++k) times_ms[3 + k] = t_bins[k];
     }
     if (choice) {
         choice[0] = s->tune_force;

@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "voronoi.cu"
@@ -78,9 +79,29 @@ static inline void launch_groups_ns(const VoroArgs &a, int N, cudaStream_t st, i
     }
 }
 
+// the thread-per-cell form (launch shape 2): FP64 forces summed with atomics, no line tension,
+// 16-slot padded rows; other systems run shape 0
+#ifndef CG_THREAD_TPB
+#define CG_THREAD_TPB 128
+#endif
+#ifndef CG_THREAD_MINB
+#define CG_THREAD_MINB 5
+#endif
+static inline bool thread_form_ok(const VoroArgs &a)
+{
+    return !a.Ffix && a.tension_mode == 0 && a.K == VG && a.rows_padded;
+}
+
 template <typename R, bool SCATTER, bool TEST>
 static inline void launch_groups(const VoroArgs &a, int N, cudaStream_t st, int shape = 0)
 {
+    if constexpr (SCATTER && std::is_same<R, double>::value) {
+        if (shape == 2 && thread_form_ok(a)) {
+            k_voro_thread<TEST, CG_THREAD_TPB, CG_THREAD_MINB><<<nblk(N, CG_THREAD_TPB), CG_THREAD_TPB, 0, st>>>(a);
+            return;
+        }
+    }
+    if (shape == 2) shape = 0;
     if constexpr (SCATTER) {
         if (a.Ffix) {
             if (a.K > VG)
@@ -280,7 +301,7 @@ struct cg_system {
     int *ctype = nullptr;
     double *tmat = nullptr, *TE = nullptr;
     // autotuned launch choices: force-pass shape, cell-list bin side (in mean cell spacings)
-    int tune_force = 0;
+    int tune_force = 2;  // the thread-per-cell form where it applies (launch_groups), else shape 0
     int tune_star_grid = 0, tune_commit_grid = 0;  // repair-round grids (0: the defaults)
     double bin_target = 0.8;
     // spatial sorting (allocated on first use): keys, order / inverse, staging, CUB scratch, tags
@@ -440,6 +461,7 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
     cg_system *s = new cg_system();
     s->model = CG_MODEL_VORONOI;
     s->precision = precision;
+    if (const char *fs = getenv("CG_FORCE_SHAPE")) s->tune_force = atoi(fs);
     s->n_inst = n_inst;
     s->K = K;
     int off = 0, boff = 0;

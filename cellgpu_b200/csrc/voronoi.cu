@@ -183,13 +183,26 @@ CG_D const Inst &inst_of(const VoroArgs &a, int c)
 // claim cell x for epoch e (first claimer wins) and append it to queue q; its slot is recorded in
 // qslot[q & 1] (the round that reads it, q, and the round that writes the next claims, q + 1,
 // use different halves)
-CG_D void claim_enqueue(const VoroArgs &a, int x, int e, int q)
+CG_D void claim_enqueue(const VoroArgs &a, int x, int e, int q, int4 hint = make_int4(0, 0, 0, 0))
 {
     if (atomicMax(&a.mark[x], e) < e) {
         int slot = atomicAdd(&a.ctl->q_count[q], 1);
         a.queue[(size_t)q * a.N + slot] = x;
         if (a.qslot) a.qslot[(size_t)(q & 1) * a.N + x] = slot;
+        if (q == 0 && a.qhint) a.qhint[slot] = hint;
     }
+}
+
+// The claims of an in-circle failure of edge (c, n), whose apexes are m (before n in c's row) and p
+// (after it): the four cells, each with the edit of its row that flips the edge to (m, p) -- c and n
+// drop each other, p gains m between c and n, m gains p between n and c (the hints of the first
+// repair round's fast path, flip_edit)
+CG_D void claim_flip(const VoroArgs &a, int e, int c, int n, int m, int p)
+{
+    claim_enqueue(a, c, e, 0, make_int4(1, n, 0, 0));
+    claim_enqueue(a, n, e, 0, make_int4(1, c, 0, 0));
+    claim_enqueue(a, p, e, 0, make_int4(2, m, c, n));
+    claim_enqueue(a, m, e, 0, make_int4(2, p, n, c));
 }
 
 // ------------------------------------------------------------------------------------------
@@ -554,7 +567,10 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<
         Adiff = (R)(a.KA * (A - pp.x));
         Pdiff = (R)(a.KP * (P - pp.y));
     }
-    R sx = 0, sy = 0;
+    // the cell's own force and the pairs of contributions to each neighbour are summed in FP64 in
+    // both precisions (mixed mode: FP32 terms, no FP32 rounding of their sums)
+    using S = double;
+    S sx = 0, sy = 0;
     V cb[NS / G];
 #pragma unroll
     for (int r = 0; r < NS / G; ++r) {
@@ -593,26 +609,126 @@ CG_D void grp_scatter(const VoroArgs &a, int c, int z, bool ok, int gl, GrpTile<
             R a11 = (R)e11, a12 = (R)e12, a21 = (R)e21, a22 = (R)e22;
             R b11 = (R)(1.0 - d11 - e11), b12 = (R)(-d12 - e12), b21 = (R)(-d21 - e21),
               b22 = (R)(1.0 - d22 - e22);
-            sx += gx * c11 + gy * c21;
-            sy += gx * c12 + gy * c22;
+            if (sizeof(R) == sizeof(double)) {
+                sx += gx * c11 + gy * c21;
+                sy += gx * c12 + gy * c22;
+            } else {
+                sx += (S)(gx * c11) + (S)(gy * c21);
+                sy += (S)(gx * c12) + (S)(gy * c22);
+            }
             T.ca[k] = mk<R>(gx * a11 + gy * a21, gx * a12 + gy * a22);
             cb[r] = mk<R>(gx * b11 + gy * b21, gx * b12 + gy * b22);
         }
     }
-    sx = group_sum<R>(sx);
-    sy = group_sum<R>(sy);
+    sx = group_sum<S>(sx);
+    sy = group_sum<S>(sy);
     __syncwarp();
 #pragma unroll
     for (int r = 0; r < NS / G; ++r) {
         int k = gl + G * r;
         if (ok && k < z) {
             V ca = T.ca[k + 1 == z ? 0 : k + 1];
-            add_force<R, FIX>(a.F, a.Ffix, nbk[r], sgn * (cb[r].x + ca.x), sgn * (cb[r].y + ca.y));
+            if (sizeof(R) == sizeof(double))
+                add_force<R, FIX>(a.F, a.Ffix, nbk[r], sgn * (cb[r].x + ca.x), sgn * (cb[r].y + ca.y));
+            else
+                add_force<S, FIX>(a.F, a.Ffix, nbk[r], (S)sgn * ((S)cb[r].x + (S)ca.x),
+                                  (S)sgn * ((S)cb[r].y + (S)ca.y));
         }
     }
     if (ok && gl == 0) {
-        add_force<R, FIX>(a.F, a.Ffix, c, sgn * sx, sgn * sy);
+        add_force<S, FIX>(a.F, a.Ffix, c, (S)sgn * sx, (S)sgn * sy);
     }
+}
+
+// Cells whose row failed the exact test (fail: the smallest failing slot x 2, +1 for an
+// orientation failure), or whose row is unusable (!ok: fewer than 3 or more than NS entries), are
+// counted and queued for the repair with the cells of the failing edge (one thread per cell).
+CG_D void flag_cell(const VoroArgs &a, int c, int z, bool ok, int fail, int ns)
+{
+    if (!ok) {
+        if (a.ctl) {
+            atomicAdd(&a.ctl->n_flagged, 1);
+            claim_enqueue(a, c, a.ctl->epoch, 0);
+            if (z > ns) {
+                atomicExch(&a.ctl->status, CG_ERR_CAPACITY);
+                atomicExch(&a.ctl->halt, 1);
+            }
+        } else if (a.mark) {
+            a.mark[c] = 1;
+            a.queue[0] = 1;
+        }
+    } else {
+        int k = fail >> 1;
+        bool orient_fail = fail & 1;
+        const int *rw = a.nbr + (size_t)c * a.K;
+        int nk = rw[k], nk1 = rw[k + 1 == z ? 0 : k + 1], nkm = rw[k == 0 ? z - 1 : k - 1];
+        if (a.ctl) {
+            int e = a.ctl->epoch;
+            atomicAdd(&a.ctl->n_flagged, 1);
+            if (orient_fail) {
+                claim_enqueue(a, c, e, 0);
+                claim_enqueue(a, nk, e, 0);
+                claim_enqueue(a, nk1, e, 0);
+            } else {
+                claim_flip(a, e, c, nk, nkm, nk1);
+            }
+        } else if (a.mark) {
+            a.mark[c] = 1;
+            a.mark[nk] = 1;
+            a.mark[nk1] = 1;
+            if (!orient_fail) a.mark[nkm] = 1;
+            a.queue[0] = 1;
+        }
+    }
+}
+
+// One cell per 8-lane group of the fused pass (called by the whole warp; live switches a group off)
+template <typename R, bool SCATTER, bool TEST, int NS, int FIX>
+CG_D void grp_cell(const VoroArgs &a, int c, bool live, int gl, GrpTile<R, NS> &tl)
+{
+    int z = 0, pre0 = NO_PRE;
+    double2 pc = make_double2(0, 0), pref = make_double2(0, 0);
+    double Lx = 1, Ly = 1;
+    const int *row = nullptr;
+    if (live) {
+        // independent loads, issued together: position, row length, first row entry (rows of
+        // the system are padded, so it needs no length), preferences
+        row = a.nbr + (size_t)c * a.K;
+        pc = a.pos[c];
+        z = a.nn[c];
+        if (CG_FP_PRE_ROW && a.rows_padded && gl < a.K) pre0 = row[gl];
+        if (SCATTER && CG_FP_PRE_PREF) pref = a.APpref[c];
+        const Inst &in = inst_of(a, c);
+        Lx = in.Lx;
+        Ly = in.Ly;
+    }
+    const bool ok = live && z >= 3 && z <= NS;
+    // Rows of at most G entries (nearly every cell of a tissue): when all four cells of the warp
+    // have them, the pass runs in its one-slot-per-lane form on the narrow tile (fewer live
+    // registers, no second-slot code)
+    const bool small = CG_FP_SMALL_PATH && NS > G && __all_sync(0xffffffffu, !live || z <= G);
+    GrpTile<R, G> &tile8 = *reinterpret_cast<GrpTile<R, G> *>(&tl);
+    int nbk[NS / G], nb8[1];
+    double A, P;
+    int fail;
+    if (small)
+        grp_geometry<R, SCATTER, TEST, G>(a, c, row, z, ok, pc, Lx, Ly, gl, tile8, nb8, A, P, fail, true, pre0);
+    else
+        grp_geometry<R, SCATTER, TEST, NS>(a, c, row, z, ok, pc, Lx, Ly, gl, tl, nbk, A, P, fail, true, pre0);
+    if (ok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
+    // A cell whose own row fails the test holds its contributions back: the row is about to be
+    // replaced, and a stale row can contain a nearly collinear triangle whose Jacobians (1/cross^2)
+    // would swamp the forces. The repair commit adds the contributions of the new row.
+    bool hold = SCATTER && TEST && a.held && ok && fail != 0x7fffffff;
+    if (hold && gl == 0) a.held[c] = 1;
+    if (SCATTER) {
+        if (small)
+            grp_scatter<R, 1, G, FIX>(a, c, z, ok && !hold, gl, tile8, nb8, A, P, R(1), CG_FP_PRE_PREF != 0, pref);
+        else
+            grp_scatter<R, 1, NS, FIX>(a, c, z, ok && !hold, gl, tl, nbk, A, P, R(1), CG_FP_PRE_PREF != 0, pref);
+    }
+    if (TEST && live && gl == 0 && (fail != 0x7fffffff || !ok)) flag_cell(a, c, z, ok, fail, NS);
+    __syncwarp();
 }
 
 // A block takes a contiguous run of cpb cells (a multiple of its WPB * GPW groups), so that in a
@@ -628,83 +744,200 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int 
     const bool halted = a.ctl && a.ctl->halt;  // uniform across the grid
     for (int base = blockIdx.x * cpb + w * GPW; base < c_end; base += WPB * GPW) {  // warp-uniform
         const int c = base + gi;
-        bool live = c < c_end && !halted;
-        int z = 0, pre0 = NO_PRE;
-        double2 pc = make_double2(0, 0), pref = make_double2(0, 0);
-        double Lx = 1, Ly = 1;
-        const int *row = nullptr;
-        if (live) {
-            // independent loads, issued together: position, row length, first row entry (rows of
-            // the system are padded, so it needs no length), preferences
-            row = a.nbr + (size_t)c * a.K;
-            pc = a.pos[c];
-            z = a.nn[c];
-            if (CG_FP_PRE_ROW && a.rows_padded && gl < a.K) pre0 = row[gl];
-            if (SCATTER && CG_FP_PRE_PREF) pref = a.APpref[c];
-            const Inst &in = inst_of(a, c);
-            Lx = in.Lx;
-            Ly = in.Ly;
-        }
-        const bool ok = live && z >= 3 && z <= NS;
-        // Rows of at most G entries (nearly every cell of a tissue): when all four cells of the warp
-        // have them, the pass runs in its one-slot-per-lane form on the narrow tile (fewer live
-        // registers, no second-slot code)
-        const bool small = CG_FP_SMALL_PATH && NS > G && __all_sync(0xffffffffu, !live || z <= G);
-        GrpTile<R, G> &tile8 = *reinterpret_cast<GrpTile<R, G> *>(&tile[sl]);
-        int nbk[NS / G], nb8[1];
-        double A, P;
-        int fail;
-        if (small)
-            grp_geometry<R, SCATTER, TEST, G>(a, c, row, z, ok, pc, Lx, Ly, gl, tile8, nb8, A, P, fail, true, pre0);
-        else
-            grp_geometry<R, SCATTER, TEST, NS>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail, true, pre0);
-        if (ok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
-        // A cell whose own row fails the test holds its contributions back: the row is about to be
-        // replaced, and a stale row can contain a nearly collinear triangle whose Jacobians (1/cross^2)
-        // would swamp the forces. The repair commit adds the contributions of the new row.
-        bool hold = SCATTER && TEST && a.held && ok && fail != 0x7fffffff;
-        if (hold && gl == 0) a.held[c] = 1;
-        if (SCATTER) {
-            if (small)
-                grp_scatter<R, 1, G, FIX>(a, c, z, ok && !hold, gl, tile8, nb8, A, P, R(1), CG_FP_PRE_PREF != 0, pref);
-            else
-                grp_scatter<R, 1, NS, FIX>(a, c, z, ok && !hold, gl, tile[sl], nbk, A, P, R(1), CG_FP_PRE_PREF != 0, pref);
-        }
-        if (TEST && live && gl == 0 && (fail != 0x7fffffff || !ok)) {
-            if (!ok) {
-                if (a.ctl) {
-                    atomicAdd(&a.ctl->n_flagged, 1);
-                    claim_enqueue(a, c, a.ctl->epoch, 0);
-                    if (z > NS) {
-                        atomicExch(&a.ctl->status, CG_ERR_CAPACITY);
-                        atomicExch(&a.ctl->halt, 1);
-                    }
-                } else if (a.mark) {
-                    a.mark[c] = 1;
-                    a.queue[0] = 1;
-                }
-            } else {
-                int k = fail >> 1;
-                bool orient_fail = fail & 1;
-                const int *rw = a.nbr + (size_t)c * a.K;  // (re-derived: keeps the pointer out of the live set)
-                int nk = rw[k], nk1 = rw[k + 1 == z ? 0 : k + 1], nkm = rw[k == 0 ? z - 1 : k - 1];
-                if (a.ctl) {
-                    int e = a.ctl->epoch;
-                    atomicAdd(&a.ctl->n_flagged, 1);
-                    claim_enqueue(a, c, e, 0);
-                    claim_enqueue(a, nk, e, 0);
-                    claim_enqueue(a, nk1, e, 0);
-                    if (!orient_fail) claim_enqueue(a, nkm, e, 0);
-                } else if (a.mark) {
-                    a.mark[c] = 1;
-                    a.mark[nk] = 1;
-                    a.mark[nk1] = 1;
-                    if (!orient_fail) a.mark[nkm] = 1;
-                    a.queue[0] = 1;
+        grp_cell<R, SCATTER, TEST, NS, FIX>(a, c, c < c_end && !halted, gl, tile[sl]);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Thread-per-cell form of the fused pass (FP64, atomic force sums, no line tension, 16-slot padded
+// rows). One thread walks its cell's ring: the row's first eight entries come in two 16-byte loads,
+// the eight neighbour positions are gathered together into registers, and the vertices, the exact
+// test, A, P and the scatter run over the ring in registers, with no shared memory and no shuffles.
+// The group form spends most of its issue slots on exchanging ring neighbours between lanes
+// (shared-memory tiles, shuffles); here a cell's ring never leaves its thread. The vertex h_{k+1}
+// and the tangent u_k are formed again in the scatter pass (one reciprocal and one reciprocal square
+// root per vertex) instead of being held for all eight vertices. The formulas are the group form's.
+// Rows of 9-16 entries (about 1 % of the cells of a tissue) are run by the same warp afterwards, in
+// the group form (four cells at a time, 8 lanes each).
+// ------------------------------------------------------------------------------------------
+constexpr int TC_Z = 8;  // rows of at most this many entries run in the thread form
+
+template <typename T>
+CG_D T pick_z(const T (&v)[TC_Z], int i)  // v[i] for a run-time index i < TC_Z, by selects
+{
+    T x = v[0];
+#pragma unroll
+    for (int k = 1; k < TC_Z; ++k)
+        if (i == k) x = v[k];
+    return x;
+}
+
+// unit vector of the edge h0 -> h1 and its length (the group form's phase C)
+CG_D double2 edge_unit(double2 h0, double2 h1, double &len)
+{
+    const double dx = h1.x - h0.x, dy = h1.y - h0.y;
+    const double l2 = dx * dx + dy * dy;
+    double il;
+    if (l2 > 1e-36) {
+        il = rsqrt(l2);
+        len = l2 * il;
+    } else {
+        len = sqrt(l2);
+        il = 1e18;
+    }
+    return make_double2(dx * il, dy * il);
+}
+
+CG_D double2 vertex_h(double2 ra, double2 rb, double &den)
+{
+    const double an = ra.x * ra.x + ra.y * ra.y, bn = rb.x * rb.x + rb.y * rb.y;
+    den = 0.5 / (ra.x * rb.y - ra.y * rb.x);
+    return make_double2(den * (an * rb.y - ra.y * bn), den * (ra.x * bn - an * rb.x));
+}
+
+// Returns true when the row is 9-16 entries long (the caller runs it in the group form).
+template <bool TEST>
+CG_D bool thread_cell(const VoroArgs &a, int c)
+{
+    const int4 *r4 = reinterpret_cast<const int4 *>(a.nbr + (size_t)c * VG);
+    const int4 q0 = r4[0], q1 = r4[1];
+    const double2 pc = a.pos[c];
+    const int z = a.nn[c];
+    const double2 pref = a.APpref[c];
+    const Inst &in = inst_of(a, c);
+    const double Lx = in.Lx, Ly = in.Ly;
+    if (z > TC_Z && z <= VG) return true;
+    if (z < 3 || z > VG) {
+        if (TEST) flag_cell(a, c, z, false, 0, VG);
+        return false;
+    }
+    const int nb[TC_Z] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+    double2 r[TC_Z];
+#pragma unroll
+    for (int k = 0; k < TC_Z; ++k) {
+        r[k] = make_double2(0.0, 0.0);
+        if (k < z) r[k] = min_dist(a.pos[nb[k]], pc, Lx, Ly);
+    }
+    const double2 rl = pick_z(r, z - 1);
+    // vertices h_k = circumcentre(0, r_{k-1}, r_k), the exact local test, A and P
+    const double Lmax = fmax(Lx, Ly);
+    int fail = 0x7fffffff, undecided = 0;
+    double Asum = 0.0, Psum = 0.0, len;
+    double2 h0 = make_double2(0.0, 0.0), hprev = h0;
+#pragma unroll
+    for (int k = 0; k < TC_Z; ++k) {
+        if (k < z) {
+            const double2 ra = k == 0 ? rl : r[k == 0 ? 0 : k - 1], rb = r[k];
+            double2 rc = r[0];
+            if (k + 1 < TC_Z && k + 1 < z) rc = r[(k + 1) % TC_Z];
+            double den;
+            const double2 h = vertex_h(ra, rb, den);
+            if (TEST) {
+                if (orient0(rb, rc) <= 0) {
+                    fail = min(fail, 2 * k + 1);
+                } else if (c < nb[k]) {
+                    const int ic = incircle_filter(ra, rb, rc, Lmax);
+                    if (ic < 0) fail = min(fail, 2 * k);
+                    if (ic == 0) undecided |= 1 << k;
                 }
             }
+            if (k == 0) {
+                h0 = h;
+            } else {
+                edge_unit(hprev, h, len);
+                Asum += fabs(0.5 * (hprev.x * h.y - hprev.y * h.x));
+                Psum += len;
+            }
+            hprev = h;
         }
-        __syncwarp();
+    }
+    const double2 hlast = hprev;
+    const double2 ulast = edge_unit(hlast, h0, len);  // edge h_{z-1} -> h_0
+    Asum += fabs(0.5 * (hlast.x * h0.y - hlast.y * h0.x));
+    Psum += len;
+    if (TEST && undecided) {
+        // the canonical evaluation of these slots runs in the repair's first phase
+        for (int k = 0; k < TC_Z; ++k) {
+            if (!(undecided & (1 << k))) continue;
+            int idx = (a.undec && a.ctl) ? atomicAdd(&a.ctl->n_undec, 1) : a.N;
+            if (idx < a.N) a.undec[idx] = c * KMAX + k;
+            else fail = min(fail, 2 * k);
+        }
+    }
+    if (a.AP) store_ap<double>(a.AP, c, Asum, Psum);
+    const bool hold = TEST && a.held && fail != 0x7fffffff;
+    if (hold) a.held[c] = 1;
+    if (!hold) {
+        // g_k = -dE_c/dh_k and the three Jacobian contractions of every vertex, as in grp_scatter
+        const double Adiff = a.KA * (Asum - pref.x), Pdiff = a.KP * (Psum - pref.y);
+        double2 hm = hlast, hc = h0, um = ulast;
+        double dc;
+        vertex_h(rl, r[0], dc);
+        double sx = 0.0, sy = 0.0;
+        double2 ca0 = make_double2(0.0, 0.0), cbp = ca0;
+        int nprev = nb[0];
+#pragma unroll
+        for (int k = 0; k < TC_Z; ++k) {
+            if (k < z) {
+                double2 hn = h0;
+                double dn = 0.0;
+                if (k + 1 < TC_Z && k + 1 < z) hn = vertex_h(r[k], r[(k + 1) % TC_Z], dn);
+                const double2 uk = edge_unit(hc, hn, len);
+                const double dAx = 0.5 * (hn.y - hm.y), dAy = 0.5 * (hm.x - hn.x);
+                const double dPx = um.x - uk.x, dPy = um.y - uk.y;
+                const double gx = -2.0 * (Adiff * dAx + Pdiff * dPx);
+                const double gy = -2.0 * (Adiff * dAy + Pdiff * dPy);
+                const double2 ra = k == 0 ? rl : r[k == 0 ? 0 : k - 1], rb = r[k];
+                // the contractions of g with the three Jacobians of h = circumcentre(0, ra, rb) (getdhdr,
+                // inc/utility/functions.h:234-287), written through h itself: with den = 1 / (2 ra x rb),
+                // g.dh/dr_c = 2 den (g x (rb - ra)) h, g.dh/dr_a = -2 den (g x rb) (h - ra), and
+                // g.dh/dr_b = g - both (translation invariance); g x v = gx v.y - gy v.x
+                const double fc = 2.0 * dc * (gx * (rb.y - ra.y) - gy * (rb.x - ra.x));
+                const double fa = -2.0 * dc * (gx * rb.y - gy * rb.x);
+                const double scx = fc * hc.x, scy = fc * hc.y;
+                sx += scx;
+                sy += scy;
+                const double2 ca = make_double2(fa * (hc.x - ra.x), fa * (hc.y - ra.y));
+                const double2 cb = make_double2(gx - scx - ca.x, gy - scy - ca.y);
+                // the contribution to neighbour k-1 is cb_{k-1} + ca_k
+                if (k == 0) ca0 = ca;
+                else atomic_add2<double>(a.F, nprev, cbp.x + ca.x, cbp.y + ca.y);
+                cbp = cb;
+                nprev = nb[k];
+                hm = hc;
+                hc = hn;
+                um = uk;
+                dc = dn;
+            }
+        }
+        atomic_add2<double>(a.F, nprev, cbp.x + ca0.x, cbp.y + ca0.y);
+        atomic_add2<double>(a.F, c, sx, sy);
+    }
+    if (TEST && fail != 0x7fffffff) flag_cell(a, c, z, true, fail, VG);
+    return false;
+}
+
+template <bool TEST, int TPB, int MINB>
+__global__ void __launch_bounds__(TPB, MINB) k_voro_thread(VoroArgs a)
+{
+    __shared__ GrpTile<double, VG> dtile[TPB / WARP][GPW];  // each warp's group tiles for its longer rows
+    const int c = blockIdx.x * TPB + threadIdx.x;
+    const int lane = threadIdx.x & (WARP - 1), w = threadIdx.x / WARP;
+    const bool halted = a.ctl && a.ctl->halt;  // uniform across the grid
+    const bool defer = c < a.N && !halted && thread_cell<TEST>(a, c);
+    // the warp's rows of 9-16 entries, four at a time in its 8-lane groups
+    unsigned left = __ballot_sync(0xffffffffu, defer);
+    const int gl = lane & (G - 1), gi = lane >> 3;
+    while (left) {  // warp-uniform
+        int pick = -1;
+        unsigned m = left;
+        for (int i = 0; i <= gi && m; ++i) {
+            pick = __ffs(m) - 1;
+            m &= m - 1;
+            if (i < gi) pick = -1;
+        }
+        grp_cell<double, true, TEST, VG, 0>(a, pick >= 0 ? c - lane + pick : 0, pick >= 0, gl, dtile[w][gi]);
+        for (int i = 0; i < GPW && left; ++i) left &= left - 1;
     }
 }
 
@@ -719,6 +952,53 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int 
 // a failing edge: the cell's contributions, already scattered, are retracted and the cell is marked
 // held (once per cell), and the cell, the edge's other end and both apexes are queued. Then the
 // WHILE node is entered if queue 0 has cells.
+// Decide the undecided slots t = base + (lane >> 3) (one per 8-lane group; whole warp, the warp's
+// four group tiles in wt)
+template <typename R, int NS>
+CG_D void undec_groups(const VoroArgs &a, Ctl *ctl, int nu, int forces, int base, GrpTile<R, NS> *wt, int lane)
+{
+    const int gl = lane & (G - 1), gi = lane >> 3;
+    const int e = ctl->epoch;
+    const int t = base + gi;
+    int c = 0, k = 0, z = 0;
+    const int *row = a.nbr;
+    double Lx = 1, Ly = 1;
+    double2 pc = make_double2(0, 0);
+    bool fails = false;
+    if (t < nu) {
+        const int en = a.undec[t];
+        c = en / KMAX;
+        k = en % KMAX;
+        z = a.nn[c];
+        row = a.nbr + (size_t)c * a.K;
+        const Inst &in = inst_of(a, c);
+        Lx = in.Lx;
+        Ly = in.Ly;
+        pc = a.pos[c];
+        if (gl == 0)
+            fails = incircle_canonical(c, row[k == 0 ? z - 1 : k - 1], row[k], row[k + 1 == z ? 0 : k + 1],
+                                       a.pos, Lx, Ly) < 0;
+    }
+    fails = __shfl_sync(0xffffffffu, fails, lane & ~(G - 1));
+    // retract the contributions once per cell (unless the force pass already held them)
+    bool first = false;
+    if (fails && gl == 0) {
+        first = !forces || atomicExch(&a.held[c], 1) == 0;
+        atomicAdd(&ctl->n_flagged, 1);
+        claim_flip(a, e, c, row[k], row[k == 0 ? z - 1 : k - 1], row[k + 1 == z ? 0 : k + 1]);
+    }
+    first = __shfl_sync(0xffffffffu, first, lane & ~(G - 1));
+    if (forces) {
+        const bool ok = fails && first && z >= 3 && z <= NS;
+        int nbk[NS / G];
+        double A, P;
+        int fl;
+        grp_geometry<R, true, false, NS>(a, c, row, z, ok, pc, Lx, Ly, gl, wt[gi], nbk, A, P, fl);
+        grp_scatter<R, -1, NS>(a, c, z, ok, gl, wt[gi], nbk, A, P);
+    }
+    __syncwarp();
+}
+
 template <typename R, int NS = VG>
 __global__ void __launch_bounds__(256) k_repair_begin(VoroArgs a, unsigned long long cond, int use_cond,
                                                       int forces)
@@ -729,52 +1009,8 @@ __global__ void __launch_bounds__(256) k_repair_begin(VoroArgs a, unsigned long 
     const int nu = min(ctl->n_undec, a.N);
     if (!ctl->halt && nu > 0 && a.undec) {
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        const int gl = lane & (G - 1), gi = lane >> 3;
-        const int sl = w * GPW + gi;
-        const int e = ctl->epoch;
-        for (int base = w * GPW; base < nu; base += WPB * GPW) {  // warp-uniform
-            const int t = base + gi;
-            int c = 0, k = 0, z = 0;
-            const int *row = a.nbr;
-            double Lx = 1, Ly = 1;
-            double2 pc = make_double2(0, 0);
-            bool fails = false;
-            if (t < nu) {
-                const int en = a.undec[t];
-                c = en / KMAX;
-                k = en % KMAX;
-                z = a.nn[c];
-                row = a.nbr + (size_t)c * a.K;
-                const Inst &in = inst_of(a, c);
-                Lx = in.Lx;
-                Ly = in.Ly;
-                pc = a.pos[c];
-                if (gl == 0)
-                    fails = incircle_canonical(c, row[k == 0 ? z - 1 : k - 1], row[k], row[k + 1 == z ? 0 : k + 1],
-                                               a.pos, Lx, Ly) < 0;
-            }
-            fails = __shfl_sync(0xffffffffu, fails, lane & ~(G - 1));
-            // retract the contributions once per cell (unless the force pass already held them)
-            bool first = false;
-            if (fails && gl == 0) {
-                first = !forces || atomicExch(&a.held[c], 1) == 0;
-                atomicAdd(&ctl->n_flagged, 1);
-                claim_enqueue(a, c, e, 0);
-                claim_enqueue(a, row[k], e, 0);
-                claim_enqueue(a, row[k + 1 == z ? 0 : k + 1], e, 0);
-                claim_enqueue(a, row[k == 0 ? z - 1 : k - 1], e, 0);
-            }
-            first = __shfl_sync(0xffffffffu, first, lane & ~(G - 1));
-            if (forces) {
-                const bool ok = fails && first && z >= 3 && z <= NS;
-                int nbk[NS / G];
-                double A, P;
-                int fl;
-                grp_geometry<R, true, false, NS>(a, c, row, z, ok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fl);
-                grp_scatter<R, -1, NS>(a, c, z, ok, gl, tile[sl], nbk, A, P);
-            }
-            __syncwarp();
-        }
+        for (int base = w * GPW; base < nu; base += WPB * GPW)  // warp-uniform
+            undec_groups<R, NS>(a, ctl, nu, forces, base, tile + w * GPW, lane);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1031,14 +1267,136 @@ CG_D void cand_insert(int *table, int *list, int *count, int v)
     }
 }
 
+// per-warp shared memory of the local star: candidate positions relative to the cell, their
+// global indices, the deduplication table, the star and the candidate count
+struct StarSmem {
+    double2 rel[CAND_LOCAL];
+    int cand[CAND_LOCAL];
+    int hash[CAND_HASH];
+    int out[KMAX];
+    int m;
+};
+
+// First-round fast path: the row a single edge flip gives (whole warp). h is the hint the claim
+// left: {1, v, -, -} drops v; {2, v, a, b} inserts v between the consecutive entries a and b. The
+// row is rotated to start at its smallest entry and written to out. Returns the new length, or -1
+// when the row does not have the shape the edit expects (v missing or already there, a and b not
+// consecutive, fewer than 3 entries left, or no room), and the caller computes the star.
+// A flip is the whole repair when the failing edges of a step are apart; where they share cells, a
+// cell gets only the edit of the edge that claimed it first, and the round's check (partners'
+// rows, the exact test of every changed row) queues its cells for the next round, whose stars are
+// computed in full.
+CG_D int flip_edit(const int *row, int z, int K, int4 h, int *out, int lane)
+{
+    const unsigned full = 0xffffffffu;
+    const int v = lane < z ? row[lane] : -1;
+    const unsigned has = __ballot_sync(full, lane < z && v == h.y);
+    int nv, nz;
+    if (h.x == 1) {
+        if (__popc(has) != 1 || z - 1 < 3) return -1;
+        const int pos = __ffs(has) - 1;
+        nv = __shfl_sync(full, v, lane < pos ? lane : (lane + 1) & 31);
+        nz = z - 1;
+    } else {
+        const int nxt = __shfl_sync(full, v, lane + 1 >= z ? 0 : lane + 1);
+        const unsigned at = __ballot_sync(full, lane < z && v == h.z && nxt == h.w);
+        if (has != 0u || __popc(at) != 1 || z + 1 > K) return -1;
+        const int pos = __ffs(at) - 1;  // v goes after pos
+        nv = __shfl_sync(full, v, lane <= pos ? lane : lane - 1);
+        if (lane == pos + 1) nv = h.y;
+        nz = z + 1;
+    }
+    const int mn = __reduce_min_sync(full, lane < nz ? (unsigned)nv : 0xffffffffu);
+    const int r0 = __ffs(__ballot_sync(full, lane < nz && nv == mn)) - 1;
+    int src = lane + r0;
+    if (src >= nz) src -= nz;
+    const int rv = __shfl_sync(full, nv, src & 31);
+    if (lane < nz) out[lane] = rv;
+    __syncwarp();
+    return nz;
+}
+
+// exact star of the cell in queue slot q of `round` (whole warp); the result goes to the slot's
+// staging row, a failure halts the step
+CG_D void star_one(const VoroArgs &a, Ctl *ctl, int round, const int *queue, int q, StarSmem &S, int lane)
+{
+    volatile int *vm = &S.m;
+    int c = queue[q];
+    const Inst &in = inst_of(a, c);
+    int z = a.nn[c];
+    const int *row = a.nbr + (size_t)c * a.K;
+    if (round == 0 && a.qhint) {
+        const int4 h = a.qhint[q];
+        if (h.x != 0) {
+            const int nz = flip_edit(row, z, a.K, h, S.out, lane);
+            if (nz > 0) {
+                if (lane < nz) a.stage_nbr[(size_t)q * a.K + lane] = S.out[lane];
+                if (lane == 0) a.stage_nn[q] = nz;
+                __syncwarp();
+                return;
+            }
+        }
+    }
+    for (int i = lane; i < CAND_HASH; i += WARP) S.hash[i] = -1;
+    if (lane == 0) *vm = 0;
+    __syncwarp();
+    if (lane < z) cand_insert(S.hash, S.cand, &S.m, row[lane]);
+    __syncwarp();
+    // ring 1 expands the row's members; from round 1 on, ring 2 expands the new 2-ring members
+    // too (3-ring), for cells whose new star reaches further
+    int lo = 0, hi = min(*vm, CAND_LOCAL);
+    for (int ring = 0; ring < (round == 0 ? 1 : 2); ++ring) {
+        // rows are padded with -1 past their length, so whole rows are read without their
+        // lengths; a lane takes slot (lane & 15) of members lane >> 4, +2, +4, +6 of each group
+        // of 8 members, and the four loads are in flight together
+        for (int base = lo; base < hi; base += 8) {
+            for (int eb = 0; eb < a.K; eb += 16) {  // rows wider than 16 (K = 32) in two halves
+                const int e = eb + (lane & 15);
+                int v[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int j = base + (lane >> 4) + 2 * i;
+                    v[i] = (j < hi && e < a.K) ? a.nbr[(size_t)S.cand[j] * a.K + e] : -1;
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (v[i] >= 0 && v[i] != c && *vm < CAND_LOCAL) cand_insert(S.hash, S.cand, &S.m, v[i]);
+            }
+        }
+        __syncwarp();
+        lo = hi;
+        hi = min(*vm, CAND_LOCAL);
+    }
+    int m = min(*vm, CAND_LOCAL);
+    double2 pc = a.pos[c];
+    for (int t = lane; t < m; t += 2 * WARP) {
+        const int t2 = t + WARP;
+        double2 p1 = a.pos[S.cand[t]];
+        double2 p2 = t2 < m ? a.pos[S.cand[t2]] : pc;
+        S.rel[t] = min_dist(p1, pc, in.Lx, in.Ly);
+        if (t2 < m) S.rel[t2] = min_dist(p2, pc, in.Lx, in.Ly);
+    }
+    __syncwarp();
+    StarFrame fr = {c, a.pos, in.Lx, in.Ly};
+    int zs = warp_star(S.rel, S.cand, m, a.K, S.out, lane, fr);
+    if (zs < 0) {
+        if (lane == 0) {
+            atomicExch(&ctl->need_global, 1);
+            atomicExch(&ctl->status, zs == -2 ? CG_ERR_CAPACITY : CG_ERR_TOPOLOGY);
+            atomicExch(&ctl->halt, 1);
+        }
+        __syncwarp();
+        return;
+    }
+    if (lane < zs) a.stage_nbr[(size_t)q * a.K + lane] = S.out[lane];
+    if (lane == 0) a.stage_nn[q] = zs;
+    __syncwarp();
+}
+
 template <int WPB>
 __global__ void __launch_bounds__(WPB * 32, STAR_MINB) k_star_local(VoroArgs a)
 {
-    __shared__ int s_cand[WPB][CAND_LOCAL];
-    __shared__ double2 s_rel[WPB][CAND_LOCAL];
-    __shared__ int s_out[WPB][KMAX];
-    __shared__ int s_hash[WPB][CAND_HASH];
-    __shared__ int s_m[WPB];
+    __shared__ StarSmem s_star[WPB];
     Ctl *ctl = a.ctl;
     if (ctl->halt) return;
     int round = ctl->round;
@@ -1047,66 +1405,7 @@ __global__ void __launch_bounds__(WPB * 32, STAR_MINB) k_star_local(VoroArgs a)
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int gw = blockIdx.x * WPB + w, nw = gridDim.x * WPB;
     const int *queue = a.queue + (size_t)round * a.N;
-    volatile int *vm = &s_m[w];
-    for (int q = gw; q < nq; q += nw) {
-        int c = queue[q];
-        const Inst &in = inst_of(a, c);
-        int z = a.nn[c];
-        const int *row = a.nbr + (size_t)c * a.K;
-        for (int i = lane; i < CAND_HASH; i += WARP) s_hash[w][i] = -1;
-        if (lane == 0) *vm = 0;
-        __syncwarp();
-        if (lane < z) cand_insert(s_hash[w], s_cand[w], &s_m[w], row[lane]);
-        __syncwarp();
-        // ring 1 expands the row's members; from round 1 on, ring 2 expands the new 2-ring members
-        // too (3-ring), for cells whose new star reaches further
-        int lo = 0, hi = min(*vm, CAND_LOCAL);
-        for (int ring = 0; ring < (round == 0 ? 1 : 2); ++ring) {
-            // rows are padded with -1 past their length, so whole rows are read without their
-            // lengths; a lane takes slot (lane & 15) of members lane >> 4, +2, +4, +6 of each group
-            // of 8 members, and the four loads are in flight together
-            for (int base = lo; base < hi; base += 8) {
-                for (int eb = 0; eb < a.K; eb += 16) {  // rows wider than 16 (K = 32) in two halves
-                    const int e = eb + (lane & 15);
-                    int v[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        const int j = base + (lane >> 4) + 2 * i;
-                        v[i] = (j < hi && e < a.K) ? a.nbr[(size_t)s_cand[w][j] * a.K + e] : -1;
-                    }
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        if (v[i] >= 0 && v[i] != c && *vm < CAND_LOCAL) cand_insert(s_hash[w], s_cand[w], &s_m[w], v[i]);
-                }
-            }
-            __syncwarp();
-            lo = hi;
-            hi = min(*vm, CAND_LOCAL);
-        }
-        int m = min(*vm, CAND_LOCAL);
-        double2 pc = a.pos[c];
-        for (int t = lane; t < m; t += 2 * WARP) {
-            const int t2 = t + WARP;
-            double2 p1 = a.pos[s_cand[w][t]];
-            double2 p2 = t2 < m ? a.pos[s_cand[w][t2]] : pc;
-            s_rel[w][t] = min_dist(p1, pc, in.Lx, in.Ly);
-            if (t2 < m) s_rel[w][t2] = min_dist(p2, pc, in.Lx, in.Ly);
-        }
-        __syncwarp();
-        StarFrame fr = {c, a.pos, in.Lx, in.Ly};
-        int zs = warp_star(s_rel[w], s_cand[w], m, a.K, s_out[w], lane, fr);
-        if (zs < 0) {
-            if (lane == 0) {
-                atomicExch(&ctl->need_global, 1);
-                atomicExch(&ctl->status, zs == -2 ? CG_ERR_CAPACITY : CG_ERR_TOPOLOGY);
-                atomicExch(&ctl->halt, 1);
-            }
-            continue;
-        }
-        if (lane < zs) a.stage_nbr[(size_t)q * a.K + lane] = s_out[w][lane];
-        if (lane == 0) a.stage_nn[q] = zs;
-        __syncwarp();
-    }
+    for (int q = gw; q < nq; q += nw) star_one(a, ctl, round, queue, q, s_star[w], lane);
 }
 
 CG_D int row_find(const int *row, int z, int v)
@@ -1173,6 +1472,137 @@ CG_D const int *future_row(const VoroArgs &a, int x, int round, int nq, const in
 // every triangle (c,u,v) of the new row must appear in the rows of u and v, every dropped triangle
 // must be gone from them, and a changed row must pass the exact local test (every edge). Offending
 // cells are claimed for the next round. The last block to finish ends the round (round_end).
+// Commit and check queue slots base and base + 1 of `round` (whole warp: 16 lanes per slot, the
+// warp's four group tiles in wt)
+template <typename R, bool FORCES, int NS>
+CG_D void cc_pair(const VoroArgs &a, Ctl *ctl, int round, int nq, const int *queue, int e_next, int base,
+                  GrpTile<R, NS> *wt, int lane)
+{
+    const unsigned full = 0xffffffffu;
+    const int gl = lane & (G - 1), gi = lane >> 3;
+    GrpTile<R, NS> &tl = wt[gi];
+    const bool add = gi & 1;   // group 0 of a slot: old row (retract); group 1: new row (add)
+    const int hl = lane & 15;  // lane within the slot's 16 lanes
+    const int q = base + (gi >> 1);
+    const bool live = q < nq;
+    int c = 0, zo = 0, zn = 0;
+    if (live) {
+        c = queue[q];
+        zo = a.nn[c];
+        zn = a.stage_nn[q];
+    }
+    int *row = a.nbr + (size_t)c * a.K;
+    const int *srow = a.stage_nbr + (size_t)(live ? q : 0) * a.K;
+    bool diff = live && zo != zn;
+#pragma unroll
+    for (int e = hl; e < NS; e += 16)
+        if (live && !diff && e < zn && row[e] != srow[e]) diff = true;
+    int dv = diff ? 1 : 0;
+    dv |= __shfl_xor_sync(full, dv, 1);
+    dv |= __shfl_xor_sync(full, dv, 2);
+    dv |= __shfl_xor_sync(full, dv, 4);
+    dv |= __shfl_xor_sync(full, dv, 8);
+    diff = dv != 0;
+    const bool was_held = live && a.held && a.held[c];
+    double2 pc = make_double2(0, 0);
+    double Lx = 1, Ly = 1;
+    if (live) {
+        const Inst &in = inst_of(a, c);
+        Lx = in.Lx;
+        Ly = in.Ly;
+        pc = a.pos[c];
+    }
+    // this group's row (old or new) in registers: slot k = gl + G r and its successor
+    const int *grow = add ? srow : row;
+    const int gz = add ? zn : zo;
+    int ek[NS / G], ek1[NS / G];
+#pragma unroll
+    for (int r = 0; r < NS / G; ++r) {
+        const int k = gl + G * r;
+        ek[r] = -1;
+        ek1[r] = -1;
+        if (live && k < gz) {
+            ek[r] = grow[k];
+            ek1[r] = grow[k + 1 == gz ? 0 : k + 1];
+        }
+    }
+    // forces: retract the old row (unless the force pass held it back) / add the new one
+    const bool gok = add ? (live && (diff || (FORCES && was_held)) && zn >= 3 && zn <= NS)
+                         : (FORCES && live && diff && !was_held && zo >= 3 && zo <= NS);
+    int nbk[NS / G];
+    double A, P;
+    int fail;
+    grp_geometry<R, FORCES, false, NS>(a, c, grow, gz, gok, pc, Lx, Ly, gl, tl, nbk, A, P, fail, add);
+    if (FORCES) grp_scatter<R, 1, NS>(a, c, gz, gok, gl, tl, nbk, A, P, add ? R(1) : R(-1));
+    if (add && gok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
+    __syncwarp();
+    // the new row replaces the old one, padded with -1 (both were read above)
+    if (live && diff) {
+#pragma unroll
+        for (int t = 0; t < KMAX / 16; ++t) {
+            const int e = hl + 16 * t;
+            if (e < a.K) row[e] = e < zn ? srow[e] : -1;
+        }
+    }
+    if (live && hl == 0) {
+        if (a.held) a.held[c] = 0;
+        if (diff) {
+            a.nn[c] = zn;
+            atomicAdd(&ctl->counters[2], 1ull);
+        }
+    }
+    // consistency against the end-of-round rows
+    bool bad = false;
+    if (add) {
+        bad = live && diff && zn < 3;
+#pragma unroll
+        for (int r = 0; r < NS / G; ++r) {
+            const int k = gl + G * r;
+            if (live && k < zn) {
+                const int u = ek[r], v = ek1[r];
+                int zu, zv;
+                const int *fu = future_row(a, u, round, nq, queue, zu);
+                const int *fv = future_row(a, v, round, nq, queue, zv);
+                if (!pair_in<NS>(fu, zu, a.K, v, c)) claim_enqueue(a, u, e_next, round + 1);
+                if (!pair_in<NS>(fv, zv, a.K, c, u)) claim_enqueue(a, v, e_next, round + 1);
+                if (diff && zn >= 3 && gok) {
+                    // exact local test of the new row (every edge): relative positions from
+                    // the group's tile (grp_geometry stored them)
+                    const int km = k == 0 ? zn - 1 : k - 1, kp = k + 1 == zn ? 0 : k + 1;
+                    const double2 dA = tl.r[km], dB = tl.r[k], dC = tl.r[kp];
+                    const int um = srow[km];
+                    if (orient0(dB, dC) <= 0 || incircle_g(dA, dB, dC, c, um, u, v, a.pos, Lx, Ly) < 0)
+                        bad = true;
+                }
+            }
+        }
+    } else if (live && diff) {
+        // dropped triangles of the old row must be gone from the partners' rows
+#pragma unroll
+        for (int r = 0; r < NS / G; ++r) {
+            const int k = gl + G * r;
+            if (k < zo) {
+                const int u = ek[r], v = ek1[r];
+                if (!pair_in<NS>(srow, zn, a.K, u, v)) {
+                    int zu, zv;
+                    const int *fu = future_row(a, u, round, nq, queue, zu);
+                    const int *fv = future_row(a, v, round, nq, queue, zv);
+                    if (pair_in<NS>(fu, zu, a.K, v, c)) claim_enqueue(a, u, e_next, round + 1);
+                    if (pair_in<NS>(fv, zv, a.K, c, u)) claim_enqueue(a, v, e_next, round + 1);
+                }
+            }
+        }
+    }
+    bad = group_any(bad);
+    if (add && bad) {
+        if (gl == 0) claim_enqueue(a, c, e_next, round + 1);
+#pragma unroll
+        for (int r = 0; r < NS / G; ++r)
+            if (ek[r] >= 0) claim_enqueue(a, ek[r], e_next, round + 1);
+    }
+    __syncwarp();
+}
+
 template <typename R, bool FORCES, int WPB, int NS = VG>
 __global__ void __launch_bounds__(WPB * 32) k_commit_check(VoroArgs a, unsigned long long cond, int use_cond)
 {
@@ -1184,133 +1614,10 @@ __global__ void __launch_bounds__(WPB * 32) k_commit_check(VoroArgs a, unsigned 
         const int nq = ctl->q_count[round];
         const int *queue = a.queue + (size_t)round * a.N;
         const int e_next = ctl->epoch + round + 1;  // claim epoch of the next round
-        const unsigned full = 0xffffffffu;
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        const int gl = lane & (G - 1), gi = lane >> 3;
-        const int sl = w * GPW + gi;
-        const bool add = gi & 1;   // group 0 of a slot: old row (retract); group 1: new row (add)
-        const int hl = lane & 15;  // lane within the slot's 16 lanes
         const int step = gridDim.x * WPB * (GPW / 2);
-        for (int base = (blockIdx.x * WPB + w) * (GPW / 2); base < nq; base += step) {  // warp-uniform
-            const int q = base + (gi >> 1);
-            const bool live = q < nq;
-            int c = 0, zo = 0, zn = 0;
-            if (live) {
-                c = queue[q];
-                zo = a.nn[c];
-                zn = a.stage_nn[q];
-            }
-            int *row = a.nbr + (size_t)c * a.K;
-            const int *srow = a.stage_nbr + (size_t)(live ? q : 0) * a.K;
-            bool diff = live && zo != zn;
-#pragma unroll
-            for (int e = hl; e < NS; e += 16)
-                if (live && !diff && e < zn && row[e] != srow[e]) diff = true;
-            int dv = diff ? 1 : 0;
-            dv |= __shfl_xor_sync(full, dv, 1);
-            dv |= __shfl_xor_sync(full, dv, 2);
-            dv |= __shfl_xor_sync(full, dv, 4);
-            dv |= __shfl_xor_sync(full, dv, 8);
-            diff = dv != 0;
-            const bool was_held = live && a.held && a.held[c];
-            double2 pc = make_double2(0, 0);
-            double Lx = 1, Ly = 1;
-            if (live) {
-                const Inst &in = inst_of(a, c);
-                Lx = in.Lx;
-                Ly = in.Ly;
-                pc = a.pos[c];
-            }
-            // this group's row (old or new) in registers: slot k = gl + G r and its successor
-            const int *grow = add ? srow : row;
-            const int gz = add ? zn : zo;
-            int ek[NS / G], ek1[NS / G];
-#pragma unroll
-            for (int r = 0; r < NS / G; ++r) {
-                const int k = gl + G * r;
-                ek[r] = -1;
-                ek1[r] = -1;
-                if (live && k < gz) {
-                    ek[r] = grow[k];
-                    ek1[r] = grow[k + 1 == gz ? 0 : k + 1];
-                }
-            }
-            // forces: retract the old row (unless the force pass held it back) / add the new one
-            const bool gok = add ? (live && (diff || (FORCES && was_held)) && zn >= 3 && zn <= NS)
-                                 : (FORCES && live && diff && !was_held && zo >= 3 && zo <= NS);
-            int nbk[NS / G];
-            double A, P;
-            int fail;
-            grp_geometry<R, FORCES, false, NS>(a, c, grow, gz, gok, pc, Lx, Ly, gl, tile[sl], nbk, A, P, fail, add);
-            if (FORCES) grp_scatter<R, 1, NS>(a, c, gz, gok, gl, tile[sl], nbk, A, P, add ? R(1) : R(-1));
-            if (add && gok && gl == 0 && a.AP) store_ap<R>(a.AP, c, (R)A, (R)P);
-            __syncwarp();
-            // the new row replaces the old one, padded with -1 (both were read above)
-            if (live && diff) {
-#pragma unroll
-                for (int t = 0; t < KMAX / 16; ++t) {
-                    const int e = hl + 16 * t;
-                    if (e < a.K) row[e] = e < zn ? srow[e] : -1;
-                }
-            }
-            if (live && hl == 0) {
-                if (a.held) a.held[c] = 0;
-                if (diff) {
-                    a.nn[c] = zn;
-                    atomicAdd(&ctl->counters[2], 1ull);
-                }
-            }
-            // consistency against the end-of-round rows
-            bool bad = false;
-            if (add) {
-                bad = live && diff && zn < 3;
-#pragma unroll
-                for (int r = 0; r < NS / G; ++r) {
-                    const int k = gl + G * r;
-                    if (live && k < zn) {
-                        const int u = ek[r], v = ek1[r];
-                        int zu, zv;
-                        const int *fu = future_row(a, u, round, nq, queue, zu);
-                        const int *fv = future_row(a, v, round, nq, queue, zv);
-                        if (!pair_in<NS>(fu, zu, a.K, v, c)) claim_enqueue(a, u, e_next, round + 1);
-                        if (!pair_in<NS>(fv, zv, a.K, c, u)) claim_enqueue(a, v, e_next, round + 1);
-                        if (diff && zn >= 3 && gok) {
-                            // exact local test of the new row (every edge): relative positions from
-                            // the group's tile (grp_geometry stored them)
-                            const int km = k == 0 ? zn - 1 : k - 1, kp = k + 1 == zn ? 0 : k + 1;
-                            const double2 dA = tile[sl].r[km], dB = tile[sl].r[k], dC = tile[sl].r[kp];
-                            const int um = srow[km];
-                            if (orient0(dB, dC) <= 0 || incircle_g(dA, dB, dC, c, um, u, v, a.pos, Lx, Ly) < 0)
-                                bad = true;
-                        }
-                    }
-                }
-            } else if (live && diff) {
-                // dropped triangles of the old row must be gone from the partners' rows
-#pragma unroll
-                for (int r = 0; r < NS / G; ++r) {
-                    const int k = gl + G * r;
-                    if (k < zo) {
-                        const int u = ek[r], v = ek1[r];
-                        if (!pair_in<NS>(srow, zn, a.K, u, v)) {
-                            int zu, zv;
-                            const int *fu = future_row(a, u, round, nq, queue, zu);
-                            const int *fv = future_row(a, v, round, nq, queue, zv);
-                            if (pair_in<NS>(fu, zu, a.K, v, c)) claim_enqueue(a, u, e_next, round + 1);
-                            if (pair_in<NS>(fv, zv, a.K, c, u)) claim_enqueue(a, v, e_next, round + 1);
-                        }
-                    }
-                }
-            }
-            bad = group_any(bad);
-            if (add && bad) {
-                if (gl == 0) claim_enqueue(a, c, e_next, round + 1);
-#pragma unroll
-                for (int r = 0; r < NS / G; ++r)
-                    if (ek[r] >= 0) claim_enqueue(a, ek[r], e_next, round + 1);
-            }
-            __syncwarp();
-        }
+        for (int base = (blockIdx.x * WPB + w) * (GPW / 2); base < nq; base += step)  // warp-uniform
+            cc_pair<R, FORCES, NS>(a, ctl, round, nq, queue, e_next, base, tile + w * GPW, lane);
     }
     // the last block to finish ends the round (threadfence reduction: every block's claims are
     // visible before its count is)

@@ -97,11 +97,11 @@ class VoronoiBatch:
     def autotune(self):
         """Time the force pass's block shapes and the cell-list bin sides on the current state and
         keep the fastest; returns the timings (ms) and the choices."""
-        t = np.zeros(5)
+        t = np.zeros(6)
         c = np.zeros(2, np.int32)
         check(self._lib.cg_autotune(self._h, ptr(t), ptr(c)))
-        return {"force_pass_ms": t[:2].tolist(), "triangulation_ms": t[2:].tolist(),
-                "force_shape": ["2 warps/block", "4 warps/block"][int(c[0])],
+        return {"force_pass_ms": t[:3].tolist(), "triangulation_ms": t[3:].tolist(),
+                "force_shape": ["2 warps/block", "4 warps/block", "thread per cell"][int(c[0])],
                 "bin_side": [0.8, 1.0, 1.25][int(c[1])]}
 
     def autotune_repair(self, steps=10, dt=0.01, mu=1.0):

@@ -350,10 +350,13 @@ int cg_set_exclusions(cg_system *sys, const int *excluded);
 int cg_get_external_forces(cg_system *sys, double *out);
 
 /* Autotuner (no counterpart in the reference): times the runtime-selectable launch parameters on
- * the system's current state and keeps the fastest -- the fused force pass's block shape (0: 2 warps
- * per block, 1: 4 warps) and the global triangulation's cell-list bin side (0: 0.8, 1: 1.0, 2: 1.25
- * mean cell spacings). times_ms (5 values: force pass per shape, triangulation per bin side) and
- * choice (2 values) may be NULL. Voronoi systems only (a no-op for the vertex model). */
+ * the system's current state and keeps the fastest -- the fused force pass's launch shape (0: 8-lane
+ * groups, 2 warps per block; 1: groups, 4 warps per block; 2: one thread per cell, timed only where
+ * it applies: FP64 with atomic sums, no line tension, 16-slot rows) and the global triangulation's
+ * cell-list bin side (0: 0.8, 1: 1.0, 2: 1.25 mean cell spacings). A new system starts with shape 2
+ * where it applies, else shape 0. times_ms (6 values: force pass per shape, 0 for a shape not
+ * timed; triangulation per bin side) and choice (2 values) may be NULL. Voronoi systems only (a no-op
+ * for the vertex model). */
 int cg_autotune(cg_system *sys, double *times_ms, int *choice);
 
 /* Repair-launch autotuner (no counterpart in the reference): times the grids of the local repair

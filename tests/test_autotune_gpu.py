@@ -19,8 +19,9 @@ def test_autotune_keeps_results(cglib):
     F0 = b.forces()
     nn0, nbr0 = b.topology()
     r = b.autotune()
-    assert r["force_shape"] in ("2 warps/block", "4 warps/block") and r["bin_side"] in (0.8, 1.0, 1.25)
-    assert all(t > 0 for t in r["force_pass_ms"] + r["triangulation_ms"])
+    assert r["force_shape"] in ("2 warps/block", "4 warps/block", "thread per cell")
+    assert r["bin_side"] in (0.8, 1.0, 1.25)
+    assert all(t > 0 for t in r["force_pass_ms"] + r["triangulation_ms"])  # FP64: all three shapes
     b.triangulate()  # with the chosen bin side
     nn, nbr = b.topology()
     assert np.array_equal(canonical(nn, nbr), canonical(nn0, nbr0))
