@@ -730,11 +730,15 @@ def main():
             cpu = {"error": str(e)}
     c4 = extras.get("c4_ensemble", {})
     ratios = {k: c4[k] for k in ("batched_over_plain_fp64", "batched_mixed_over_plain_fp64") if k in c4}
+    # the force pass timed above: one thread per cell for FP64 with atomic sums, else 8-lane groups
+    thread_form = precision == cg.CG_FP64 and not args.deterministic
+    force_kernel = "k_voro_thread (force+test)" if thread_form else "k_voro_groups (force+test)"
     prof = os.path.join(ROOT, "profiles", "force_pass_traffic.json")
     traffic = None
     if os.path.exists(prof):
         with open(prof) as f:
-            traffic = json.load(f).get("traffic_bytes_per_launch")
+            tr = json.load(f)
+        traffic = tr.get("traffic_bytes_per_launch" if thread_form else "group_form_traffic_bytes_per_launch")
     line = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": done,
         "warmup": max(3, args.warmup), "ms_per_step": 1e3 * total / max(done, 1), "higher_is_better": True,
@@ -742,7 +746,7 @@ def main():
         "data": "synthetic",
         "config": workload_config(args.precision, world, not args.no_sort, args.deterministic),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": traffic, "kernel": "k_voro_groups (force+test)",
+                     "frac": achieved / hbm, "traffic": traffic, "kernel": force_kernel,
                      "kernel_ms": t_force * 1e3, "peak_kind": kind},
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},

@@ -249,6 +249,8 @@ struct cg_system {
     void *AP = nullptr, *F = nullptr;
     int *nn = nullptr, *nbr = nullptr;
     int *mark = nullptr, *queue = nullptr, *stage_nn = nullptr, *stage_nbr = nullptr, *qslot = nullptr;
+    int4 *qhint = nullptr;  // first-round row edits of edge flips, per queue slot
+    int *nclaim = nullptr;  // first-round claims per cell in the current step (zero between steps)
     int *held = nullptr, *undec = nullptr;
     Ctl *ctl = nullptr;
     int *bin_count = nullptr, *bin_start = nullptr, *bin_cells = nullptr, *cell_bin = nullptr,
@@ -411,6 +413,8 @@ static VoroArgs sys_args(cg_system *s)
     a.stage_nn = s->stage_nn;
     a.stage_nbr = s->stage_nbr;
     a.qslot = s->qslot;
+    a.qhint = s->qhint;
+    a.nclaim = s->nclaim;
     a.held = s->held;
     a.undec = s->undec;
     a.ctl = s->ctl;
@@ -435,7 +439,7 @@ static size_t voronoi_bytes(int N, int K, int n_bins, int n_inst, int precision)
     size_t real2 = precision == CG_FP64 ? 16 : 8;
     size_t per_cell = 4 /*cell_inst*/ + 4 /*held*/ + 4 /*undec*/ + 16 * 3 /*pos, motility, APpref*/ + 8 /*theta*/ + real2 /*AP*/ + 16 /*F*/ +
                       4 + 4 * (size_t)K /*nn, nbr*/ + 4 /*mark*/ + 4 * (R_MAX + 1) /*queue*/ + 4 +
-                      4 * (size_t)K /*stage*/ + 4 * 2 /*qslot*/ + 4 * 3 + 16 /*cell list*/ +
+                      4 * (size_t)K /*stage*/ + 4 * 2 /*qslot*/ + 16 /*qhint*/ + 4 /*nclaim*/ + 4 * 3 + 16 /*cell list*/ +
                       8 + 8 /*noise staging, device draw*/;
     return per_cell * (size_t)N + (size_t)n_bins * 8 + (size_t)n_inst * (sizeof(Inst) + 16) + 4096;
 }
@@ -503,6 +507,8 @@ extern "C" int cg_voronoi_create(int n_inst, const int *N, const double *box, in
         if ((st = dalloc(s, &s->stage_nn, Nt))) break;
         if ((st = dalloc(s, &s->stage_nbr, (size_t)Nt * K))) break;
         if ((st = dalloc(s, &s->qslot, (size_t)Nt * 2))) break;
+        if ((st = dalloc(s, &s->qhint, Nt))) break;
+        if ((st = dalloc(s, &s->nclaim, Nt))) break;
         if ((st = dalloc(s, &s->held, Nt))) break;
         if ((st = dalloc(s, &s->undec, Nt))) break;
         if ((st = dalloc(s, &s->ctl, 1))) break;
@@ -933,6 +939,7 @@ static int recover(cg_system *s)
     if (c.status == CG_ERR_CAPACITY) CG_TRY(grow_rows(s));
     CG_TRY(reset_ctl_after_halt(s));
     if (s->held) CG_CUDA(cudaMemsetAsync(s->held, 0, sizeof(int) * s->N, s->stream));
+    if (s->nclaim) CG_CUDA(cudaMemsetAsync(s->nclaim, 0, sizeof(int) * s->N, s->stream));
     return triangulate_sys(s);
 }
 

@@ -185,6 +185,7 @@ CG_D const Inst &inst_of(const VoroArgs &a, int c)
 // use different halves)
 CG_D void claim_enqueue(const VoroArgs &a, int x, int e, int q, int4 hint = make_int4(0, 0, 0, 0))
 {
+    if (q == 0 && a.nclaim) atomicAdd(&a.nclaim[x], 1);
     if (atomicMax(&a.mark[x], e) < e) {
         int slot = atomicAdd(&a.ctl->q_count[q], 1);
         a.queue[(size_t)q * a.N + slot] = x;
@@ -1282,10 +1283,11 @@ struct StarSmem {
 // row is rotated to start at its smallest entry and written to out. Returns the new length, or -1
 // when the row does not have the shape the edit expects (v missing or already there, a and b not
 // consecutive, fewer than 3 entries left, or no room), and the caller computes the star.
-// A flip is the whole repair when the failing edges of a step are apart; where they share cells, a
-// cell gets only the edit of the edge that claimed it first, and the round's check (partners'
-// rows, the exact test of every changed row) queues its cells for the next round, whose stars are
-// computed in full.
+// The edit is used only for a cell that exactly one claim of the step named (nclaim), so it does
+// not depend on the order of the claims; cells named by several failing edges get their stars. An
+// edited row that the round's check finds wanting (a partner's row disagrees, or an edge fails the
+// exact test: the cell had another failing edge, which only its first is reported for) queues the
+// cell itself for the next round, whose stars are computed in full.
 CG_D int flip_edit(const int *row, int z, int K, int4 h, int *out, int lane)
 {
     const unsigned full = 0xffffffffu;
@@ -1327,15 +1329,17 @@ CG_D void star_one(const VoroArgs &a, Ctl *ctl, int round, const int *queue, int
     const int *row = a.nbr + (size_t)c * a.K;
     if (round == 0 && a.qhint) {
         const int4 h = a.qhint[q];
-        if (h.x != 0) {
-            const int nz = flip_edit(row, z, a.K, h, S.out, lane);
-            if (nz > 0) {
-                if (lane < nz) a.stage_nbr[(size_t)q * a.K + lane] = S.out[lane];
-                if (lane == 0) a.stage_nn[q] = nz;
-                __syncwarp();
-                return;
-            }
+        const int claims = a.nclaim[c];
+        __syncwarp();
+        if (lane == 0) a.nclaim[c] = 0;  // every counted cell is in this queue: ready for the next step
+        const int nz = (h.x != 0 && claims == 1) ? flip_edit(row, z, a.K, h, S.out, lane) : -1;
+        if (nz > 0) {
+            if (lane < nz) a.stage_nbr[(size_t)q * a.K + lane] = S.out[lane];
+            if (lane == 0) a.stage_nn[q] = nz;
+            __syncwarp();
+            return;
         }
+        if (lane == 0 && h.x != 0) a.qhint[q].x = 0;  // the check then knows the row is a star
     }
     for (int i = lane; i < CAND_HASH; i += WARP) S.hash[i] = -1;
     if (lane == 0) *vm = 0;
@@ -1551,8 +1555,10 @@ CG_D void cc_pair(const VoroArgs &a, Ctl *ctl, int round, int nq, const int *que
             atomicAdd(&ctl->counters[2], 1ull);
         }
     }
-    // consistency against the end-of-round rows
-    bool bad = false;
+    // consistency against the end-of-round rows; a row from a first-round flip edit that a partner
+    // disagrees with is queued again itself (it may be the wrong one)
+    const bool edited = round == 0 && a.qhint && live && diff && a.qhint[q].x != 0;
+    bool bad = false, disagree = false;
     if (add) {
         bad = live && diff && zn < 3;
 #pragma unroll
@@ -1563,8 +1569,14 @@ CG_D void cc_pair(const VoroArgs &a, Ctl *ctl, int round, int nq, const int *que
                 int zu, zv;
                 const int *fu = future_row(a, u, round, nq, queue, zu);
                 const int *fv = future_row(a, v, round, nq, queue, zv);
-                if (!pair_in<NS>(fu, zu, a.K, v, c)) claim_enqueue(a, u, e_next, round + 1);
-                if (!pair_in<NS>(fv, zv, a.K, c, u)) claim_enqueue(a, v, e_next, round + 1);
+                if (!pair_in<NS>(fu, zu, a.K, v, c)) {
+                    claim_enqueue(a, u, e_next, round + 1);
+                    disagree = true;
+                }
+                if (!pair_in<NS>(fv, zv, a.K, c, u)) {
+                    claim_enqueue(a, v, e_next, round + 1);
+                    disagree = true;
+                }
                 if (diff && zn >= 3 && gok) {
                     // exact local test of the new row (every edge): relative positions from
                     // the group's tile (grp_geometry stored them)
@@ -1587,12 +1599,25 @@ CG_D void cc_pair(const VoroArgs &a, Ctl *ctl, int round, int nq, const int *que
                     int zu, zv;
                     const int *fu = future_row(a, u, round, nq, queue, zu);
                     const int *fv = future_row(a, v, round, nq, queue, zv);
-                    if (pair_in<NS>(fu, zu, a.K, v, c)) claim_enqueue(a, u, e_next, round + 1);
-                    if (pair_in<NS>(fv, zv, a.K, c, u)) claim_enqueue(a, v, e_next, round + 1);
+                    if (pair_in<NS>(fu, zu, a.K, v, c)) {
+                        claim_enqueue(a, u, e_next, round + 1);
+                        disagree = true;
+                    }
+                    if (pair_in<NS>(fv, zv, a.K, c, u)) {
+                        claim_enqueue(a, v, e_next, round + 1);
+                        disagree = true;
+                    }
                 }
             }
         }
     }
+    // both 8-lane groups of the slot (old row, new row) vote on the edited row
+    int dv2 = edited && disagree ? 1 : 0;
+    dv2 |= __shfl_xor_sync(0xffffffffu, dv2, 1);
+    dv2 |= __shfl_xor_sync(0xffffffffu, dv2, 2);
+    dv2 |= __shfl_xor_sync(0xffffffffu, dv2, 4);
+    dv2 |= __shfl_xor_sync(0xffffffffu, dv2, 8);
+    bad = bad || dv2 != 0;
     bad = group_any(bad);
     if (add && bad) {
         if (gl == 0) claim_enqueue(a, c, e_next, round + 1);

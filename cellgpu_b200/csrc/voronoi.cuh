@@ -75,6 +75,7 @@ struct VoroArgs {
     int *stage_nbr; // N * K
     int *qslot;     // 2 * N: queue slot of each cell claimed for a round, by round parity
     int4 *qhint;    // N: per slot of the first round's queue, the row edit of an edge flip, or 0
+    int *nclaim;    // N: claims naming each cell for the first round of the current step
     int *held;      // N: 1 while a cell's contributions are held back (its own row failed the test)
     int *undec;     // N: slots (c * 16 + k) whose in-circle sign the filter left undecided, or null
     Ctl *ctl;
