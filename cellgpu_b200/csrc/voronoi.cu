@@ -755,9 +755,10 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int 
 // the eight neighbour positions are gathered together into registers, and the vertices, the exact
 // test, A, P and the scatter run over the ring in registers, with no shared memory and no shuffles.
 // The group form spends most of its issue slots on exchanging ring neighbours between lanes
-// (shared-memory tiles, shuffles); here a cell's ring never leaves its thread. The vertex h_{k+1}
-// and the tangent u_k are formed again in the scatter pass (one reciprocal and one reciprocal square
-// root per vertex) instead of being held for all eight vertices. The formulas are the group form's.
+// (shared-memory tiles, shuffles); here a cell's ring never leaves its thread. The vertices and
+// their reciprocals go to a shared-memory column of the thread's own (no exchange, no barrier) for
+// the scatter pass, which forms the tangents u_k again (one reciprocal square root per vertex)
+// instead of holding them for all eight vertices.
 // Rows of 9-16 entries (about 1 % of the cells of a tissue) are run by the same warp afterwards, in
 // the group form (four cells at a time, 8 lanes each).
 // ------------------------------------------------------------------------------------------
@@ -796,9 +797,15 @@ CG_D double2 vertex_h(double2 ra, double2 rb, double &den)
     return make_double2(den * (an * rb.y - ra.y * bn), den * (ra.x * bn - an * rb.x));
 }
 
+// Per warp: the vertices h_k and reciprocals den_k of the lanes' cells ([slot][lane]: each lane
+// reads and writes its own column), formed once in the geometry pass and read back by the scatter.
+struct ThreadTile {
+    double hx[TC_Z][WARP], hy[TC_Z][WARP], den[TC_Z][WARP];
+};
+
 // Returns true when the row is 9-16 entries long (the caller runs it in the group form).
 template <bool TEST>
-CG_D bool thread_cell(const VoroArgs &a, int c)
+CG_D bool thread_cell(const VoroArgs &a, int c, ThreadTile &T, int lane)
 {
     const int4 *r4 = reinterpret_cast<const int4 *>(a.nbr + (size_t)c * VG);
     const int4 q0 = r4[0], q1 = r4[1];
@@ -833,6 +840,9 @@ CG_D bool thread_cell(const VoroArgs &a, int c)
             if (k + 1 < TC_Z && k + 1 < z) rc = r[(k + 1) % TC_Z];
             double den;
             const double2 h = vertex_h(ra, rb, den);
+            T.hx[k][lane] = h.x;
+            T.hy[k][lane] = h.y;
+            T.den[k][lane] = den;
             if (TEST) {
                 if (orient0(rb, rc) <= 0) {
                     fail = min(fail, 2 * k + 1);
@@ -872,8 +882,7 @@ CG_D bool thread_cell(const VoroArgs &a, int c)
         // g_k = -dE_c/dh_k and the three Jacobian contractions of every vertex, as in grp_scatter
         const double Adiff = a.KA * (Asum - pref.x), Pdiff = a.KP * (Psum - pref.y);
         double2 hm = hlast, hc = h0, um = ulast;
-        double dc;
-        vertex_h(rl, r[0], dc);
+        double dc = T.den[0][lane];
         double sx = 0.0, sy = 0.0;
         double2 ca0 = make_double2(0.0, 0.0), cbp = ca0;
         int nprev = nb[0];
@@ -882,7 +891,10 @@ CG_D bool thread_cell(const VoroArgs &a, int c)
             if (k < z) {
                 double2 hn = h0;
                 double dn = 0.0;
-                if (k + 1 < TC_Z && k + 1 < z) hn = vertex_h(r[k], r[(k + 1) % TC_Z], dn);
+                if (k + 1 < TC_Z && k + 1 < z) {
+                    hn = make_double2(T.hx[(k + 1) % TC_Z][lane], T.hy[(k + 1) % TC_Z][lane]);
+                    dn = T.den[(k + 1) % TC_Z][lane];
+                }
                 const double2 uk = edge_unit(hc, hn, len);
                 const double dAx = 0.5 * (hn.y - hm.y), dAy = 0.5 * (hm.x - hn.x);
                 const double dPx = um.x - uk.x, dPy = um.y - uk.y;
@@ -918,14 +930,20 @@ CG_D bool thread_cell(const VoroArgs &a, int c)
     return false;
 }
 
+union ThreadWarpSmem {
+    ThreadTile t;                 // the thread form's vertices
+    GrpTile<double, VG> g[GPW];   // then the group tiles of the warp's longer rows
+};
+
 template <bool TEST, int TPB, int MINB>
 __global__ void __launch_bounds__(TPB, MINB) k_voro_thread(VoroArgs a)
 {
-    __shared__ GrpTile<double, VG> dtile[TPB / WARP][GPW];  // each warp's group tiles for its longer rows
+    __shared__ ThreadWarpSmem wsm[TPB / WARP];
     const int c = blockIdx.x * TPB + threadIdx.x;
     const int lane = threadIdx.x & (WARP - 1), w = threadIdx.x / WARP;
     const bool halted = a.ctl && a.ctl->halt;  // uniform across the grid
-    const bool defer = c < a.N && !halted && thread_cell<TEST>(a, c);
+    const bool defer = c < a.N && !halted && thread_cell<TEST>(a, c, wsm[w].t, lane);
+    __syncwarp();  // the warp's vertex columns are free for its group tiles
     // the warp's rows of 9-16 entries, four at a time in its 8-lane groups
     unsigned left = __ballot_sync(0xffffffffu, defer);
     const int gl = lane & (G - 1), gi = lane >> 3;
@@ -937,7 +955,7 @@ __global__ void __launch_bounds__(TPB, MINB) k_voro_thread(VoroArgs a)
             m &= m - 1;
             if (i < gi) pick = -1;
         }
-        grp_cell<double, true, TEST, VG, 0>(a, pick >= 0 ? c - lane + pick : 0, pick >= 0, gl, dtile[w][gi]);
+        grp_cell<double, true, TEST, VG, 0>(a, pick >= 0 ? c - lane + pick : 0, pick >= 0, gl, wsm[w].g[gi]);
         for (int i = 0; i < GPW && left; ++i) left &= left - 1;
     }
 }
