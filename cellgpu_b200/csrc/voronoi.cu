@@ -752,27 +752,17 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int 
 // ------------------------------------------------------------------------------------------
 // Thread-per-cell form of the fused pass (FP64, atomic force sums, no line tension, 16-slot padded
 // rows). One thread walks its cell's ring: the row's first eight entries come in two 16-byte loads,
-// the eight neighbour positions are gathered together into registers, and the vertices, the exact
-// test, A, P and the scatter run over the ring in registers, with no shared memory and no shuffles.
+// the eight neighbour positions are gathered together, and the vertices, the exact test, A, P and
+// the scatter run over the ring in the thread, with no shuffles.
 // The group form spends most of its issue slots on exchanging ring neighbours between lanes
-// (shared-memory tiles, shuffles); here a cell's ring never leaves its thread. The vertices and
-// their reciprocals go to a shared-memory column of the thread's own (no exchange, no barrier) for
-// the scatter pass, which forms the tangents u_k again (one reciprocal square root per vertex)
-// instead of holding them for all eight vertices.
+// (shared-memory tiles, shuffles); here a cell's ring never leaves its thread. The relative
+// positions, vertices and reciprocals go to a shared-memory column of the thread's own (no
+// exchange, no barrier) for the scatter pass, which forms the tangents u_k again (one reciprocal
+// square root per vertex) instead of holding them for all eight vertices.
 // Rows of 9-16 entries (about 1 % of the cells of a tissue) are run by the same warp afterwards, in
 // the group form (four cells at a time, 8 lanes each).
 // ------------------------------------------------------------------------------------------
 constexpr int TC_Z = 8;  // rows of at most this many entries run in the thread form
-
-template <typename T>
-CG_D T pick_z(const T (&v)[TC_Z], int i)  // v[i] for a run-time index i < TC_Z, by selects
-{
-    T x = v[0];
-#pragma unroll
-    for (int k = 1; k < TC_Z; ++k)
-        if (i == k) x = v[k];
-    return x;
-}
 
 // unit vector of the edge h0 -> h1 and its length (the group form's phase C)
 CG_D double2 edge_unit(double2 h0, double2 h1, double &len)
@@ -797,10 +787,12 @@ CG_D double2 vertex_h(double2 ra, double2 rb, double &den)
     return make_double2(den * (an * rb.y - ra.y * bn), den * (ra.x * bn - an * rb.x));
 }
 
-// Per warp: the vertices h_k and reciprocals den_k of the lanes' cells ([slot][lane]: each lane
-// reads and writes its own column), formed once in the geometry pass and read back by the scatter.
+// Per warp: the relative neighbour positions r_k, vertices h_k and reciprocals den_k of the lanes'
+// cells ([slot][lane]: each lane reads and writes its own column, so no barrier), formed once in the
+// geometry pass and read back by the scatter. Holding them here rather than in registers keeps the
+// pass at 92 registers without spills (5 blocks of 4 warps per SM, as the 40 KB per block allows).
 struct ThreadTile {
-    double hx[TC_Z][WARP], hy[TC_Z][WARP], den[TC_Z][WARP];
+    double hx[TC_Z][WARP], hy[TC_Z][WARP], den[TC_Z][WARP], rx[TC_Z][WARP], ry[TC_Z][WARP];
 };
 
 // Returns true when the row is 9-16 entries long (the caller runs it in the group form).
@@ -820,13 +812,16 @@ CG_D bool thread_cell(const VoroArgs &a, int c, ThreadTile &T, int lane)
         return false;
     }
     const int nb[TC_Z] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-    double2 r[TC_Z];
 #pragma unroll
     for (int k = 0; k < TC_Z; ++k) {
-        r[k] = make_double2(0.0, 0.0);
-        if (k < z) r[k] = min_dist(a.pos[nb[k]], pc, Lx, Ly);
+        if (k < z) {
+            const double2 rk = min_dist(a.pos[nb[k]], pc, Lx, Ly);
+            T.rx[k][lane] = rk.x;
+            T.ry[k][lane] = rk.y;
+        }
     }
-    const double2 rl = pick_z(r, z - 1);
+    auto R = [&](int k) { return make_double2(T.rx[k][lane], T.ry[k][lane]); };
+    const double2 rl = R(z - 1);
     // vertices h_k = circumcentre(0, r_{k-1}, r_k), the exact local test, A and P
     const double Lmax = fmax(Lx, Ly);
     int fail = 0x7fffffff, undecided = 0;
@@ -835,9 +830,8 @@ CG_D bool thread_cell(const VoroArgs &a, int c, ThreadTile &T, int lane)
 #pragma unroll
     for (int k = 0; k < TC_Z; ++k) {
         if (k < z) {
-            const double2 ra = k == 0 ? rl : r[k == 0 ? 0 : k - 1], rb = r[k];
-            double2 rc = r[0];
-            if (k + 1 < TC_Z && k + 1 < z) rc = r[(k + 1) % TC_Z];
+            const double2 ra = k == 0 ? rl : R(k == 0 ? 0 : k - 1), rb = R(k);
+            const double2 rc = R(k + 1 < z ? k + 1 : 0);
             double den;
             const double2 h = vertex_h(ra, rb, den);
             T.hx[k][lane] = h.x;
@@ -900,7 +894,7 @@ CG_D bool thread_cell(const VoroArgs &a, int c, ThreadTile &T, int lane)
                 const double dPx = um.x - uk.x, dPy = um.y - uk.y;
                 const double gx = -2.0 * (Adiff * dAx + Pdiff * dPx);
                 const double gy = -2.0 * (Adiff * dAy + Pdiff * dPy);
-                const double2 ra = k == 0 ? rl : r[k == 0 ? 0 : k - 1], rb = r[k];
+                const double2 ra = k == 0 ? rl : R(k == 0 ? 0 : k - 1), rb = R(k);
                 // the contractions of g with the three Jacobians of h = circumcentre(0, ra, rb) (getdhdr,
                 // inc/utility/functions.h:234-287), written through h itself: with den = 1 / (2 ra x rb),
                 // g.dh/dr_c = 2 den (g x (rb - ra)) h, g.dh/dr_a = -2 den (g x rb) (h - ra), and
