@@ -382,6 +382,86 @@ CG_D void t1_sets_d(const VertArgs &a, int v1, int v2, int cs[4], int vs[4])
     vs[2] = nx;
 }
 
+// Start-of-sweep evaluation of the candidate edge `key` (read-only): vertex2, the cells of
+// t1_sets_d (cs; vs is not formed) and the decision (0: rejected, 1: evaluate at its turn). The data
+// are loaded in two batches instead of one dependent load per row entry: vn, the position and vcn of
+// vertex1; then vertex2's position and vcn with the sizes and first eight entries of vertex1's three
+// cell rows. The walk of find_in_cell_d then runs on registers in its own order (entry n-1 first,
+// then 0, 1, ...), so the result is the same; rows longer than eight entries or shorter than three
+// take the walk on global memory.
+constexpr int T1_ROW_FAST = 8;
+CG_D unsigned char t1_start_eval(const VertArgs &a, const Inst &in, int key, int &vertex2, int cs[4])
+{
+    const int v1 = key / 3;
+    const int v2 = a.vn[3 * v1 + key % 3];
+    vertex2 = v2;
+    const double2 p1 = a.vpos[v1];
+    int c3v1[3], c3v2[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) c3v1[f] = a.vcn[3 * v1 + f];
+    if (!(v1 < v2)) return 0;
+    const double2 p2 = a.vpos[v2];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) c3v2[f] = a.vcn[3 * v2 + f];
+    int n[3], r[3][T1_ROW_FAST];
+    const int lim = a.vmax < T1_ROW_FAST ? a.vmax : T1_ROW_FAST;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const int *row = a.cv + (size_t)c3v1[q] * a.vmax;
+        n[q] = a.cvn[c3v1[q]];
+#pragma unroll
+        for (int k = 0; k < T1_ROW_FAST; ++k) r[q][k] = k < lim ? row[k] : -1;
+    }
+    const double2 e = min_dist(p1, p2, in.Lx, in.Ly);
+    if (!(__dsqrt_rn(__dadd_rn(__dmul_rn(e.x, e.x), __dmul_rn(e.y, e.y))) < a.t1)) return 0;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        const int t = c3v2[f];
+        if (t != c3v1[0] && t != c3v1[1] && t != c3v1[2]) cs[3] = t;
+    }
+    int n0 = 0, n2 = 0;  // sizes of cs[0] and cs[2]
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const int c = c3v1[q], nq = n[q];
+        int l, cur, nx;
+        if (nq < 3 || nq > lim) {
+            find_in_cell_d(a.cv + (size_t)c * a.vmax, nq, v1, l, cur, nx);
+        } else {
+            l = r[q][0];
+            cur = r[q][0];
+#pragma unroll
+            for (int k = 1; k < T1_ROW_FAST; ++k) {
+                if (k == nq - 2) l = r[q][k];
+                if (k == nq - 1) cur = r[q][k];
+            }
+            nx = r[q][0];
+            bool done = false;
+#pragma unroll
+            for (int cn = 0; cn < T1_ROW_FAST; ++cn) {
+                if (!done && cn < nq) {
+                    nx = r[q][cn];
+                    if (cur == v1) {
+                        done = true;
+                    } else {
+                        l = cur;
+                        cur = nx;
+                    }
+                }
+            }
+        }
+        if (l == v2) {
+            cs[0] = c;
+            n0 = nq;
+        } else if (nx == v2) {
+            cs[2] = c;
+            n2 = nq;
+        } else {
+            cs[1] = c;
+        }
+    }
+    return (n0 == 3 || n2 == 3) ? 0 : 1;
+}
+
 CG_D void row_remove(int *row, int &n, int v)
 {
     int cidx = 0;
@@ -403,19 +483,61 @@ CG_D void row_insert_after(int *row, int &n, int v, int w)
     n += 1;
 }
 
-// insert key into the pending part q[head, n) of an ascending queue (no repeats)
-CG_D void queue_push(int *q, int head, int &n, int cap, int key, bool &overflow)
+// Keys queued by flips ahead of the sweep: a binary min-heap h[0, n), kept by one thread. A key may
+// be queued more than once; the sweep visits it once (it pops every copy together). Push and pop
+// cost O(log n), where inserting into a sorted run moved every pending key above the new one.
+CG_D void heap_push(int *h, int &n, int key)
 {
-    int k = n;
-    while (k > head && q[k - 1] > key) --k;
-    if (k > head && q[k - 1] == key) return;
-    if (n >= cap) {
-        overflow = true;
-        return;
+    int i = n++;
+    while (i > 0) {
+        const int p = (i - 1) >> 1;
+        const int hp = h[p];
+        if (hp <= key) break;
+        h[i] = hp;
+        i = p;
     }
-    for (int t = n; t > k; --t) q[t] = q[t - 1];
-    q[k] = key;
-    ++n;
+    h[i] = key;
+}
+
+CG_D int heap_pop(int *h, int &n)
+{
+    const int top = h[0];
+    const int last = h[--n];
+    int i = 0;
+    while (true) {
+        const int l = 2 * i + 1;
+        if (l >= n) break;
+        const int r = l + 1;
+        const int c = (r < n && h[r] < h[l]) ? r : l;
+        const int hc = h[c];
+        if (last <= hc) break;
+        h[i] = hc;
+        i = c;
+    }
+    if (n > 0) h[i] = last;
+    return top;
+}
+
+// the smallest key and all its copies
+CG_D int heap_pop_unique(int *h, int &n)
+{
+    const int k = heap_pop(h, n);
+    while (n > 0 && h[0] == k) heap_pop(h, n);
+    return k;
+}
+
+// the heap's keys in ascending order, in place
+CG_D void heap_sort_ascending(int *h, int n)
+{
+    for (int m = n; m > 1;) {
+        const int k = heap_pop(h, m);
+        h[m] = k;
+    }
+    for (int i = 0, j = n - 1; i < j; ++i, --j) {
+        const int t = h[i];
+        h[i] = h[j];
+        h[j] = t;
+    }
 }
 
 // One step of the sweep at edge key = 3*vertex1 + slot, on the current state (the body of the
@@ -593,8 +715,8 @@ CG_D int t1_try(const VertArgs &a, const Inst &in, int key, int cs[4], int vs[4]
 // Only edges shorter than the threshold are queued: a longer edge can become short only when one of
 // its ends moves, and the flip that moves it queues it again. The rows and positions are loaded
 // up front so the single sweeping thread waits for memory once, not once per edge.
-CG_D void t1_requeue(const VertArgs &a, const Inst &in, int key, int vertex2, const int vs[4], int *q,
-                     int head, int &n, int cap, bool &overflow)
+CG_D void t1_requeue(const VertArgs &a, const Inst &in, int key, int vertex2, const int vs[4], int *h, int &hn,
+                     int hcap, bool &overflow)
 {
     const int u4[4] = {key / 3, vertex2, vs[1], vs[2]};
     int w12[12];
@@ -624,16 +746,21 @@ CG_D void t1_requeue(const VertArgs &a, const Inst &in, int key, int vertex2, co
                 if (sw == 3) continue;
                 k2 = 3 * w + sw;
             }
-            if (k2 > key) queue_push(q, head, n, cap, k2, overflow);
+            if (k2 > key) {
+                if (hn >= hcap) overflow = true;
+                else heap_push(h, hn, k2);
+            }
         }
     }
 }
 
-// the whole sweep by one thread over the candidate keys q[0, nc) (sorted here); used when the
-// candidates do not fit the shared-memory path, and to resume an interrupted sweep. A flip that
-// would overflow a cell row stops it before changing anything; the keys still to visit (that one
-// first) are then moved to q[0, m) and resume[0] = m, so the sweep can continue once the rows have
-// grown (the reference grows cellVertices at that point, src/models/vertexModelBase.cpp:474-500)
+// the whole sweep by one thread over the candidate keys q[0, nc) (sorted here), the keys queued by
+// flips in a min-heap at q[nc, 3 nv); used when the candidates do not fit the shared-memory path,
+// and to resume an interrupted sweep. A flip that would overflow a cell row stops it before changing
+// anything; the keys still to visit are then left in q as two ascending runs, the candidates (A) and
+// the queued keys (B), with the interrupted key first in its run, and resume = {|A|, |B|}, so the
+// sweep can continue once the rows have grown (the reference grows cellVertices at that point,
+// src/models/vertexModelBase.cpp:474-500)
 CG_D void t1_sweep_serial(const VertArgs &a, const Inst &in, int *q, int nc, int &flips, int &status,
                           int *resume)
 {
@@ -646,25 +773,41 @@ CG_D void t1_sweep_serial(const VertArgs &a, const Inst &in, int *q, int nc, int
         }
         q[j + 1] = key;
     }
-    int head = 0, n = nc;
+    int *h = q + nc;
+    const int hcap = cap - nc;
+    int hm = 0, hn = 0;
     bool overflow = false;
-    while (head < n) {
-        int key = q[head++];
+    while (hm < nc || hn > 0) {
+        int key;
+        bool queued = false;
+        if (hn > 0 && (hm >= nc || h[0] <= q[hm])) {
+            key = heap_pop_unique(h, hn);
+            if (hm < nc && q[hm] == key) ++hm;  // also a candidate: visited once
+            queued = true;
+        } else {
+            key = q[hm++];
+        }
         int cs[4] = {0, 0, 0, 0}, vs[4] = {0, 0, 0, 0}, vertex2 = 0;
         int r = t1_try(a, in, key, cs, vs, vertex2);
         if (r < 0) {
-            const int m = n - (head - 1);
-            for (int t = 0; t < m; ++t) q[t] = q[head - 1 + t];  // forward: never overtakes its source
+            // forward copies never overtake their sources: A moves down from q[hm - 1, nc), and a key
+            // was queued only after a candidate was visited (hm >= 1), so B starts below q + nc
+            int na = 0, nb = 0;
+            if (!queued) q[na++] = key;
+            for (int t = hm; t < nc; ++t) q[na++] = q[t];
+            heap_sort_ascending(h, hn);
+            if (queued) q[na + nb++] = key;
+            for (int t = 0; t < hn; ++t) q[na + nb++] = h[t];
             if (resume) {
-                resume[0] = m;
-                resume[1] = 0;
+                resume[0] = na;
+                resume[1] = nb;
             }
             status = CG_ERR_CAPACITY;
             return;
         }
         if (r == 0) continue;
         ++flips;
-        t1_requeue(a, in, key, vertex2, vs, q, head, n, cap, overflow);
+        t1_requeue(a, in, key, vertex2, vs, h, hn, hcap, overflow);
         if (overflow) {
             status = CG_ERR_CAPACITY;
             return;
@@ -674,10 +817,12 @@ CG_D void t1_sweep_serial(const VertArgs &a, const Inst &in, int *q, int nc, int
 
 // Shared-memory sweep state (dynamic shared memory; T1_CAP candidates at most)
 constexpr int T1_CAP = 4096;
-constexpr int T1_HASH = 4096;  // touched vertices (2v) and cells (2c+1)
-constexpr int T1_EXQ = 2048;   // keys queued by flips, in shared memory until they outgrow it
+constexpr int T1_HASH = 4096;        // touched set as a hash: vertices and cells of larger instances
+constexpr int T1_BITS = 1 << 19;     // touched set as a bitmap: instances whose ids fit (64 KB)
+constexpr int T1_TOUCH_INTS = T1_BITS / 32 > T1_HASH ? T1_BITS / 32 : T1_HASH;
+constexpr int T1_EXQ = 2048;         // keys queued by flips, in shared memory until they outgrow it
 constexpr size_t T1_SMEM =
-    (size_t)T1_CAP * (sizeof(int4) + 2 * sizeof(int) + 1) + (size_t)(T1_HASH + T1_EXQ) * sizeof(int);
+    (size_t)T1_CAP * (sizeof(int4) + 2 * sizeof(int) + 1) + (size_t)(T1_TOUCH_INTS + T1_EXQ) * sizeof(int);
 
 CG_D unsigned t1_hash_slot(int id) { return ((unsigned)id * 2654435761u) >> 20; }  // 12 bits
 
@@ -688,22 +833,6 @@ CG_D bool t1_touched(const int *h, int id)
         int v = h[sl];
         if (v == id) return true;
         if (v < 0) return false;
-        sl = (sl + 1) & (T1_HASH - 1);
-    }
-    return false;
-}
-
-// returns false once the table is 3/4 full (the caller then stops trusting start-of-sweep results)
-CG_D bool t1_touch(int *h, int id, int &count)
-{
-    unsigned sl = t1_hash_slot(id);
-    for (int p = 0; p < T1_HASH; ++p) {
-        int v = h[sl];
-        if (v == id) return true;
-        if (v < 0) {
-            h[sl] = id;
-            return ++count < (3 * T1_HASH) / 4;
-        }
         sl = (sl + 1) & (T1_HASH - 1);
     }
     return false;
@@ -720,6 +849,7 @@ CG_D int wrow_find(int rk, int n, int target, int lane)
     return __popc(m) == 1 ? __ffs(m) - 1 : -1;
 }
 
+// returns false once the table is 3/4 full (the caller then stops trusting start-of-sweep results)
 CG_D bool t1_touch_atomic(int *h, int id, int *count)
 {
     unsigned sl = t1_hash_slot(id);
@@ -729,6 +859,49 @@ CG_D bool t1_touch_atomic(int *h, int id, int *count)
         if (prev == id) return true;
         sl = (sl + 1) & (T1_HASH - 1);
     }
+    return false;
+}
+
+// The sweep's touched set: the vertices (id 2 (v - voff)) and cells (id 2 (c - off) + 1) that its
+// flips have written. Where the instance's ids fit T1_BITS it is an exact bitmap, so the
+// start-of-sweep rejections stay usable for the whole sweep; otherwise the hash above. It is
+// cleared when the sweep's first flip is made (nothing is touched before).
+struct T1Touched {
+    int *h;
+    int *count;
+    bool bits;
+    int words;  // ints to clear
+    CG_D bool has(int id) const
+    {
+        if (bits) return ((reinterpret_cast<const unsigned *>(h)[id >> 5] >> (id & 31)) & 1u) != 0;
+        return t1_touched(h, id);
+    }
+    CG_D bool add(int id) const
+    {
+        if (bits) {
+            atomicOr(reinterpret_cast<unsigned *>(h) + (id >> 5), 1u << (id & 31));
+            return true;
+        }
+        return t1_touch_atomic(h, id, count);
+    }
+    CG_D void clear(int lane) const  // whole warp
+    {
+        const int fill = bits ? 0 : -1;
+        for (int i = lane; i < words; i += 32) h[i] = fill;
+        if (lane == 0) *count = 0;
+        __syncwarp();
+    }
+};
+
+// whether a flip of this sweep touched the data that candidate key's start-of-sweep evaluation read
+CG_D bool t1_cand_touched(const T1Touched &T, const Inst &in, int key, int v2, int4 c4)
+{
+    if (T.has(2 * (key / 3 - in.voff)) || T.has(2 * (v2 - in.voff))) return true;
+    if (c4.x < 0) return false;
+    const int c[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (c[k] >= 0 && T.has(2 * (c[k] - in.off) + 1)) return true;
     return false;
 }
 
@@ -866,7 +1039,7 @@ CG_D int t1_try_warp(const VertArgs &a, const Inst &in, int key, int cs[4], int 
 }
 
 // t1_requeue for a whole warp: lanes 0-11 test one edge each, lane 0 queues the short ones
-CG_D void t1_requeue_warp(const VertArgs &a, const Inst &in, int key, int vertex2, const int vs[4], int *q, int head,
+CG_D void t1_requeue_warp(const VertArgs &a, const Inst &in, int key, int vertex2, const int vs[4], int *q,
                           int &n, int cap, bool &overflow, int lane)
 {
     int k2 = -1;
@@ -892,7 +1065,10 @@ CG_D void t1_requeue_warp(const VertArgs &a, const Inst &in, int key, int vertex
         const int src = __ffs(m) - 1;
         m &= m - 1;
         const int kk = __shfl_sync(T1_FULL, k2, src);
-        if (lane == 0) queue_push(q, head, n, cap, kk, overflow);
+        if (lane == 0) {
+            if (n >= cap) overflow = true;
+            else heap_push(q, n, kk);
+        }
     }
     n = __shfl_sync(T1_FULL, n, 0);
     overflow = __shfl_sync(T1_FULL, (int)overflow, 0) != 0;
@@ -900,11 +1076,13 @@ CG_D void t1_requeue_warp(const VertArgs &a, const Inst &in, int key, int vertex
 }
 
 // One block per instance. The candidates are sorted in parallel (bitonic, shared memory) and
-// evaluated in parallel on the state at the start of the sweep; then one thread replays the
-// sweep in ascending key order. A candidate rejected at the start stays rejected unless an
-// earlier flip of this sweep touched one of its endpoints (positions, vn, vcn) or one of the four
-// cells around it (rows, sizes), which are exactly the data the test reads; such candidates, and
-// every candidate that was not rejected, are evaluated on the current state as the CPU sweep does.
+// evaluated in parallel on the state at the start of the sweep; then warp 0 replays the sweep in
+// ascending key order. A candidate rejected at the start stays rejected unless an earlier flip of
+// this sweep touched one of its endpoints (positions, vn, vcn) or one of the four cells around it
+// (rows, sizes), which are exactly the data the test reads; such candidates, and every candidate
+// that was not rejected, are evaluated on the current state as the CPU sweep does. Touched-ness
+// changes only at flips, so the warp decides the skips of 32 consecutive candidates at once, up to
+// the first one it must evaluate or the next key queued by a flip.
 __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
 {
     extern __shared__ __align__(16) unsigned char t1_smem[];
@@ -912,7 +1090,7 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
     int *s_key = reinterpret_cast<int *>(s_cs + T1_CAP);
     int *s_v2 = s_key + T1_CAP;
     int *s_hash = s_v2 + T1_CAP;
-    int *s_exq = s_hash + T1_HASH;
+    int *s_exq = s_hash + T1_TOUCH_INTS;
     unsigned char *s_dec = reinterpret_cast<unsigned char *>(s_exq + T1_EXQ);
     __shared__ int s_tn;  // entries of the touched set
     const int inst = blockIdx.x;
@@ -941,7 +1119,6 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
         int P = 1;
         while (P < nc) P <<= 1;
         for (int i = threadIdx.x; i < P; i += nthr) s_key[i] = i < nc ? q[i] : 0x7fffffff;
-        for (int i = threadIdx.x; i < T1_HASH; i += nthr) s_hash[i] = -1;
         bsync();
         for (int k = 2; k <= P; k <<= 1) {
             for (int j = k >> 1; j > 0; j >>= 1) {
@@ -961,56 +1138,61 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
         }
         // start-of-sweep evaluation (read-only)
         for (int i = threadIdx.x; i < nc; i += nthr) {
-            int key = s_key[i];
-            int v1 = key / 3;
-            int v2 = a.vn[3 * v1 + key % 3];
-            int cs[4] = {-1, -1, -1, -1}, vs[4];
-            unsigned char dec = 0;  // 0: rejected, 1: evaluate at its turn
-            if (v1 < v2) {
-                double2 e = min_dist(a.vpos[v1], a.vpos[v2], in.Lx, in.Ly);
-                if (__dsqrt_rn(__dadd_rn(__dmul_rn(e.x, e.x), __dmul_rn(e.y, e.y))) < a.t1) {
-                    t1_sets_d(a, v1, v2, cs, vs);
-                    dec = (a.cvn[cs[0]] == 3 || a.cvn[cs[2]] == 3) ? 0 : 1;
-                }
-            }
+            int v2, cs[4] = {-1, -1, -1, -1};
+            const unsigned char dec = t1_start_eval(a, in, s_key[i], v2, cs);
             s_v2[i] = v2;
             s_cs[i] = make_int4(cs[0], cs[1], cs[2], cs[3]);
             s_dec[i] = dec;
         }
-        if (threadIdx.x == 0) s_tn = 0;
         bsync();
         if (threadIdx.x < 32) {
             // sweep by warp 0, all lanes in step: the sorted candidates merged with the keys queued
-            // by flips, kept in shared memory and moved to q[nc, 3 nv) if they outgrow it
+            // by flips (a min-heap popped by lane 0), kept in shared memory and moved to q[nc, 3 nv)
+            // if they outgrow it
             const int lane = threadIdx.x;
             const bool warp_rows = a.vmax <= 32;
+            const int nbits = 2 * max(in.nv, in.n);
+            T1Touched T;
+            T.h = s_hash;
+            T.count = &s_tn;
+            T.bits = nbits <= T1_BITS;
+            T.words = T.bits ? (nbits + 31) / 32 : T1_HASH;
+            bool touched_any = false;  // no flip yet: nothing touched, the set not yet cleared
             int *ex = s_exq;
             int ecap = T1_EXQ;
             const int gcap = 3 * in.nv - nc;
-            int hm = 0, eh = 0, en = 0;
+            int hm = 0, en = 0;
             bool trust = true, overflow = false;
-            while (hm < nc || eh < en) {
+            while (hm < nc || en > 0) {
                 int key;
-                bool pre = false;
                 int idx = -1;
-                if (eh < en && (hm >= nc || ex[eh] <= s_key[hm])) {
-                    key = ex[eh++];
+                if (en > 0 && (hm >= nc || ex[0] <= s_key[hm])) {
+                    int k = 0;
+                    if (lane == 0) k = heap_pop_unique(ex, en);
+                    key = __shfl_sync(T1_FULL, k, 0);
+                    en = __shfl_sync(T1_FULL, en, 0);
+                    __syncwarp();
                     if (hm < nc && s_key[hm] == key) ++hm;  // queued again by a flip: evaluate once
                 } else {
+                    if (trust) {
+                        // skip the candidates rejected at the start and untouched since, up to the
+                        // next queued key
+                        const int bound = en > 0 ? ex[0] : 0x7fffffff;
+                        unsigned stop;
+                        while (true) {
+                            const int i = hm + lane;
+                            bool st = true;
+                            if (i < nc && s_key[i] < bound && s_dec[i] == 0)
+                                st = touched_any && t1_cand_touched(T, in, s_key[i], s_v2[i], s_cs[i]);
+                            stop = __ballot_sync(T1_FULL, st);
+                            if (stop) break;
+                            hm += 32;
+                        }
+                        hm += __ffs(stop) - 1;
+                        if (hm >= nc || (en > 0 && ex[0] <= s_key[hm])) continue;  // end of the list or a queued key
+                    }
                     idx = hm++;
                     key = s_key[idx];
-                    pre = true;
-                }
-                if (pre && trust && s_dec[idx] == 0) {
-                    const int4 c4 = s_cs[idx];
-                    int id = -1;
-                    if (lane == 0) id = 2 * (key / 3);
-                    else if (lane == 1) id = 2 * s_v2[idx];
-                    else if (c4.x >= 0 && lane == 2) id = 2 * c4.x + 1;
-                    else if (c4.x >= 0 && lane == 3) id = 2 * c4.y + 1;
-                    else if (c4.x >= 0 && lane == 4) id = 2 * c4.z + 1;
-                    else if (c4.x >= 0 && lane == 5) id = 2 * c4.w + 1;
-                    if (!__any_sync(T1_FULL, id >= 0 && t1_touched(s_hash, id))) continue;  // still rejected
                 }
                 int cs[4] = {0, 0, 0, 0}, vs[4] = {0, 0, 0, 0}, vertex2 = 0;
                 int r = warp_rows ? t1_try_warp(a, in, key, cs, vs, vertex2, lane) : 2;
@@ -1029,13 +1211,16 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
                 if (r < 0) {
                     // a cell row would overflow: keep the keys still to visit for a resumed sweep
                     // once the rows have grown -- the sorted candidates from this one on (A), then
-                    // the keys queued by flips (B); B may sit in q above A, and the forward copy
-                    // never overtakes its source
+                    // the keys queued by flips, sorted (B); a key was queued only after a candidate
+                    // was visited (hm >= 1), so B's forward copy from q[nc, ...) never overtakes
+                    // its source
                     if (lane == 0 && a.t1_resume) {
                         const bool from_ex = idx < 0;
                         int na = 0, nb = 0;
                         for (int t = from_ex ? hm : hm - 1; t < nc; ++t) q[na++] = s_key[t];
-                        for (int t = from_ex ? eh - 1 : eh; t < en; ++t) q[na + nb++] = ex[t];
+                        heap_sort_ascending(ex, en);
+                        if (from_ex) q[na + nb++] = key;
+                        for (int t = 0; t < en; ++t) q[na + nb++] = ex[t];
                         a.t1_resume[2 * inst] = na;
                         a.t1_resume[2 * inst + 1] = nb;
                     }
@@ -1044,27 +1229,28 @@ __global__ void __launch_bounds__(256) k_vm_t1_replay(VertArgs a)
                 }
                 if (r == 0) continue;
                 ++flips;
+                if (!touched_any) {
+                    T.clear(lane);
+                    touched_any = true;
+                }
                 int tid = -1;
-                if (lane < 4) tid = 2 * (lane == 0 ? key / 3 : lane == 1 ? vertex2 : lane == 2 ? vs[1] : vs[2]);
-                else if (lane < 8) tid = 2 * cs[lane - 4] + 1;
-                bool ok = tid < 0 || t1_touch_atomic(s_hash, tid, &s_tn);
+                if (lane < 4) tid = 2 * ((lane == 0 ? key / 3 : lane == 1 ? vertex2 : lane == 2 ? vs[1] : vs[2]) - in.voff);
+                else if (lane < 8) tid = 2 * (cs[lane - 4] - in.off) + 1;
+                bool ok = tid < 0 || T.add(tid);
                 if (!__all_sync(T1_FULL, ok)) trust = false;
                 __syncwarp();
                 if (ex == s_exq && en + 12 > ecap) {  // room for one flip's keys, else move to global
                     int *g = q + nc;
-                    const int m = en - eh;
-                    if (m + 12 > gcap) {
+                    if (en + 12 > gcap) {
                         status = CG_ERR_CAPACITY;
                         break;
                     }
-                    for (int t = lane; t < m; t += 32) g[t] = ex[eh + t];
+                    for (int t = lane; t < en; t += 32) g[t] = ex[t];  // a heap stays a heap
                     __syncwarp();
                     ex = g;
-                    eh = 0;
-                    en = m;
                     ecap = gcap;
                 }
-                t1_requeue_warp(a, in, key, vertex2, vs, ex, eh, en, ecap, overflow, lane);
+                t1_requeue_warp(a, in, key, vertex2, vs, ex, en, ecap, overflow, lane);
                 if (overflow) {
                     status = CG_ERR_CAPACITY;
                     break;
