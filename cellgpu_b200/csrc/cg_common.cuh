@@ -57,6 +57,25 @@ CG_HD double2 min_dist(double2 p1, double2 p2, double Lx, double Ly)
     return make_double2(x, y);
 }
 
+// min_dist with selects in place of the while loops, for warps whose lanes would take different
+// paths through them (the thread-per-cell force pass gathers eight neighbours per lane): after the
+// pre-reduction |x| <= 2 L, so each loop runs at most twice, and two conditional steps per loop give
+// the same sequence of additions, hence the same bits
+CG_D double wrap_sel(double x, double L, double h)
+{
+    if (!(fabs(x) <= 2.0 * L)) x -= L * rint(x / L);
+    x = x < -h ? x + L : x;
+    x = x < -h ? x + L : x;
+    x = x > h ? x - L : x;
+    x = x > h ? x - L : x;
+    return x;
+}
+
+CG_D double2 min_dist_sel(double2 p1, double2 p2, double Lx, double Ly)
+{
+    return make_double2(wrap_sel(p1.x - p2.x, Lx, Lx * 0.5), wrap_sel(p1.y - p2.y, Ly, Ly * 0.5));
+}
+
 // gpubox::putInBoxReal (inc/utility/gpubox.h:131-152): v = xi*p, wrap v into [0,1) by +-1.0,
 // p = L*v. Explicit round-to-nearest intrinsics keep the compiler from fusing anything.
 CG_D double2 put_in_box(double2 p, double Lx, double Ly, double iLx, double iLy)

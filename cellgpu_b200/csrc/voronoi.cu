@@ -764,19 +764,15 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_voro_groups(VoroArgs a, int 
 // ------------------------------------------------------------------------------------------
 constexpr int TC_Z = 8;  // rows of at most this many entries run in the thread form
 
-// unit vector of the edge h0 -> h1 and its length (the group form's phase C)
+// unit vector of the edge h0 -> h1 and its length, without a branch: the reciprocal square root
+// of max(l2, 1e-36), so an edge shorter than 1e-18 (a degenerate Voronoi edge) gets the
+// unit-vector scale 1e18 and a length of l2 * 1e18 (at most 1e-18)
 CG_D double2 edge_unit(double2 h0, double2 h1, double &len)
 {
     const double dx = h1.x - h0.x, dy = h1.y - h0.y;
     const double l2 = dx * dx + dy * dy;
-    double il;
-    if (l2 > 1e-36) {
-        il = rsqrt(l2);
-        len = l2 * il;
-    } else {
-        len = sqrt(l2);
-        il = 1e18;
-    }
+    const double il = rsqrt(fmax(l2, 1e-36));
+    len = l2 * il;
     return make_double2(dx * il, dy * il);
 }
 
@@ -815,7 +811,7 @@ CG_D bool thread_cell(const VoroArgs &a, int c, ThreadTile &T, int lane)
 #pragma unroll
     for (int k = 0; k < TC_Z; ++k) {
         if (k < z) {
-            const double2 rk = min_dist(a.pos[nb[k]], pc, Lx, Ly);
+            const double2 rk = min_dist_sel(a.pos[nb[k]], pc, Lx, Ly);
             T.rx[k][lane] = rk.x;
             T.ry[k][lane] = rk.y;
         }
