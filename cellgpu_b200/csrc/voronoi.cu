@@ -779,14 +779,16 @@ CG_D double2 edge_unit(double2 h0, double2 h1, double &len)
 CG_D double2 vertex_h(double2 ra, double2 rb, double &den)
 {
     const double an = ra.x * ra.x + ra.y * ra.y, bn = rb.x * rb.x + rb.y * rb.y;
-    den = 0.5 / (ra.x * rb.y - ra.y * rb.x);
+    // 0.5 / x as the correctly rounded reciprocal halved: the same double (halving is exact), with a
+    // shorter dependent chain than the division
+    den = 0.5 * __drcp_rn(ra.x * rb.y - ra.y * rb.x);
     return make_double2(den * (an * rb.y - ra.y * bn), den * (ra.x * bn - an * rb.x));
 }
 
 // Per warp: the relative neighbour positions r_k, vertices h_k and reciprocals den_k of the lanes'
 // cells ([slot][lane]: each lane reads and writes its own column, so no barrier), formed once in the
 // geometry pass and read back by the scatter. Holding them here rather than in registers keeps the
-// pass at 92 registers without spills (5 blocks of 4 warps per SM, as the 40 KB per block allows).
+// pass at 92 registers without spills (10 blocks of 2 warps per SM, as the 20 KB per block allows).
 struct ThreadTile {
     double hx[TC_Z][WARP], hy[TC_Z][WARP], den[TC_Z][WARP], rx[TC_Z][WARP], ry[TC_Z][WARP];
 };
