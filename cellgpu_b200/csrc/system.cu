@@ -1006,9 +1006,6 @@ static void enqueue_spp_steps(cg_system *s, int n, double dt, double mu, const d
     }
 }
 
-// grid of k_energy_to_host: runs of 256-cell chunks over at most two blocks per SM
-static int energy_grid(int N) { return std::min(nblk(N, 256), 2 * 148); }
-
 // Build a CUDA graph of n steps. Per step: zero F, fused force + exact test pass, then the local
 // repair rounds inside a WHILE conditional node (the device decides whether another round runs),
 // then integrate + move and the step epilogue. Kernels take queue lengths, epochs, rounds and the
@@ -1048,7 +1045,7 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
             s->kernels_enqueued += 2;
         }
         if (energy_node) {
-            k_energy_to_host<R><<<energy_grid(s->N), 256, 0, s->stream>>>(a, s->e2e_acc, s->e2e_done, energy_dst);
+            k_energy_to_host<R><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->e2e_acc, s->e2e_done, energy_dst);
             s->kernels_enqueued += 1;
             st = capture_deps(s->stream);
             if (st == CG_OK) *energy_node = deps.empty() ? nullptr : deps[0];
@@ -1103,7 +1100,7 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
         k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
         s->kernels_enqueued += 2;
         if (energy_node && t == n - 1) {
-            k_energy_to_host<R><<<energy_grid(s->N), 256, 0, s->stream>>>(a, s->e2e_acc, s->e2e_done, energy_dst);
+            k_energy_to_host<R><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->e2e_acc, s->e2e_done, energy_dst);
             s->kernels_enqueued += 1;
         }
         st = capture_deps(s->stream);
@@ -1248,7 +1245,7 @@ static int enqueue_energy_graph(cg_system *s, double dt, double mu, const double
             cudaKernelNodeParams kp;
             memset(&kp, 0, sizeof(kp));
             kp.func = (void *)k_energy_to_host<R>;
-            kp.gridDim = dim3(energy_grid(s->N));
+            kp.gridDim = dim3(nblk(s->N, 256));
             kp.blockDim = dim3(256);
             kp.kernelParams = args;
             CG_CUDA(cudaGraphExecKernelNodeSetParams(g.exec, g.energy_node, &kp));

@@ -1986,11 +1986,6 @@ __global__ void k_energy_from_fix(int n, unsigned long long *Efix, double *E)
 // block partials gather in acc (zero between calls); the last block to finish stores the totals
 // to the host buffer and clears acc and its counter for the next call. One kernel replaces a
 // memset, the reduction and a device-to-host copy, each a separate operation in the stream.
-// A block takes a contiguous run of 256-cell chunks (a grid of a few blocks per SM), and its thread
-// 0 adds the chunk sums of one instance in a register before one atomic per instance and block:
-// with a block per chunk, the blocks' atomics on one instance's sum and on the counter queued up
-// behind each other. The deterministic mode adds every chunk's sum in fixed point, the same values
-// that k_energy adds, so the two energies stay the same bits.
 template <typename R>
 __global__ void __launch_bounds__(256) k_energy_to_host(VoroArgs a, double *acc, unsigned *done, double *host_out)
 {
@@ -1998,49 +1993,32 @@ __global__ void __launch_bounds__(256) k_energy_to_host(VoroArgs a, double *acc,
     unsigned long long *afix = a.Ffix ? reinterpret_cast<unsigned long long *>(acc) : nullptr;
     __shared__ double s_part[8];
     __shared__ int s_last;
-    const int nch = (a.N + (int)blockDim.x - 1) / (int)blockDim.x;
-    const int per = (nch + (int)gridDim.x - 1) / (int)gridDim.x;
-    const int ch0 = blockIdx.x * per, ch1 = min(nch, ch0 + per);
-    double run = 0.0;  // thread 0: chunk sums of instance run_inst not yet added
-    int run_inst = -1;
-    for (int ch = ch0; ch < ch1; ++ch) {  // block-uniform
-        const int c = ch * blockDim.x + threadIdx.x;
-        double e = 0.0;
-        int inst = 0;
-        if (c < a.N) {
-            typename Vec2<R>::T ap = reinterpret_cast<typename Vec2<R>::T *>(a.AP)[c];
-            double da = (double)ap.x - a.APpref[c].x, dp = (double)ap.y - a.APpref[c].y;
-            e = a.KA * da * da + a.KP * dp * dp;
-            if (a.TE) e += 0.5 * a.TE[c];
-            inst = a.cell_inst ? a.cell_inst[c] : 0;
-        }
-        const int c0 = ch * blockDim.x, c1 = min(a.N, c0 + (int)blockDim.x) - 1;
-        const int i0 = a.cell_inst ? a.cell_inst[c0] : 0, i1 = a.cell_inst ? a.cell_inst[c1] : 0;
-        if (i0 == i1) {
-            for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
-            if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = e;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                double t = 0.0;
-                for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
-                if (afix) {
-                    fix_add1(afix + FIXW * (size_t)i0, t);
-                } else {
-                    if (i0 != run_inst) {
-                        if (run_inst >= 0) atomicAdd(&acc[run_inst], run);
-                        run = 0.0;
-                        run_inst = i0;
-                    }
-                    run += t;
-                }
-            }
-            __syncthreads();  // s_part is refilled by the next chunk
-        } else if (c < a.N) {
-            if (afix) fix_add1(afix + FIXW * (size_t)inst, e);
-            else atomicAdd(&acc[inst], e);
-        }
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    int inst = 0;
+    if (c < a.N) {
+        typename Vec2<R>::T ap = reinterpret_cast<typename Vec2<R>::T *>(a.AP)[c];
+        double da = (double)ap.x - a.APpref[c].x, dp = (double)ap.y - a.APpref[c].y;
+        e = a.KA * da * da + a.KP * dp * dp;
+        if (a.TE) e += 0.5 * a.TE[c];
+        inst = a.cell_inst ? a.cell_inst[c] : 0;
     }
-    if (threadIdx.x == 0 && run_inst >= 0) atomicAdd(&acc[run_inst], run);
+    const int c0 = blockIdx.x * blockDim.x, c1 = min(a.N, c0 + (int)blockDim.x) - 1;
+    const int i0 = a.cell_inst ? a.cell_inst[c0] : 0, i1 = a.cell_inst ? a.cell_inst[c1] : 0;
+    if (i0 == i1) {
+        for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
+        if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = e;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
+            if (afix) fix_add1(afix + FIXW * (size_t)i0, t);
+            else atomicAdd(&acc[i0], t);
+        }
+    } else if (c < a.N) {
+        if (afix) fix_add1(afix + FIXW * (size_t)inst, e);
+        else atomicAdd(&acc[inst], e);
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
