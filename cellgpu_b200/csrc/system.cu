@@ -1006,6 +1006,13 @@ static void enqueue_spp_steps(cg_system *s, int n, double dt, double mu, const d
     }
 }
 
+// whether a host-energy step graph reads the energy out in its integrator (k_spp_energy): with
+// floating-point force sums and outside the unrolled profiling form
+static bool energy_in_spp(const cg_system *s, bool unrolled)
+{
+    return !s->det && !unrolled;
+}
+
 // Build a CUDA graph of n steps. Per step: zero F, fused force + exact test pass, then the local
 // repair rounds inside a WHILE conditional node (the device decides whether another round runs),
 // then integrate + move and the step epilogue. Kernels take queue lengths, epochs, rounds and the
@@ -1096,15 +1103,26 @@ static int build_graph(cg_system *s, int n, double dt, double mu, const double *
         CG_CUDA(cudaStreamBeginCaptureToGraph(s->stream, graph, deps.data(), nullptr, deps.size(), mode));
         const double *nz = noise ? noise : s->draw_buf;
         finish_forces<R>(s, a, s->stream);
-        k_spp<R><<<nblk((s->N + 1) / 2, SPP_BLOCK), SPP_BLOCK, 0, s->stream>>>(a, nz, dt, mu, 0u, 0);
+        // the last step's energy readout: inside its integrator with floating-point sums, else a
+        // kernel after the step (fixed-point sums)
+        const bool fuse_e = energy_node && t == n - 1 && energy_in_spp(s, false);
+        if (fuse_e) {
+            k_spp_energy<R><<<nblk((s->N + 1) / 2, SPP_BLOCK), SPP_BLOCK, 0, s->stream>>>(
+                a, nz, dt, mu, s->e2e_acc, s->e2e_done, energy_dst);
+            st = capture_deps(s->stream);
+            if (st == CG_OK) *energy_node = deps.empty() ? nullptr : deps[0];
+        } else {
+            k_spp<R><<<nblk((s->N + 1) / 2, SPP_BLOCK), SPP_BLOCK, 0, s->stream>>>(a, nz, dt, mu, 0u, 0);
+        }
         k_step_done<<<1, 1, 0, s->stream>>>(s->ctl, 1);
         s->kernels_enqueued += 2;
-        if (energy_node && t == n - 1) {
+        if (energy_node && t == n - 1 && !fuse_e) {
             k_energy_to_host<R><<<nblk(s->N, 256), 256, 0, s->stream>>>(a, s->e2e_acc, s->e2e_done, energy_dst);
             s->kernels_enqueued += 1;
         }
-        st = capture_deps(s->stream);
-        if (st == CG_OK && energy_node && t == n - 1) *energy_node = deps.empty() ? nullptr : deps[0];
+        const int st2 = capture_deps(s->stream);
+        if (st == CG_OK) st = st2;
+        if (st == CG_OK && energy_node && t == n - 1 && !fuse_e) *energy_node = deps.empty() ? nullptr : deps[0];
         CG_CUDA(cudaStreamEndCapture(s->stream, &g2));
     }
     if (st == CG_OK && energy_node && !*energy_node) st = set_err(CG_ERR_CUDA, "energy node not captured");
@@ -1241,13 +1259,24 @@ static int enqueue_energy_graph(cg_system *s, double dt, double mu, const double
             VoroArgs a = sys_args(s);
             double *acc = s->e2e_acc, *d = dst;
             unsigned *done = s->e2e_done;
-            void *args[] = {&a, &acc, &done, &d};
+            const double *nz = noise ? noise : s->draw_buf;
+            double dtv = dt, muv = mu;
+            const char *unrolled = getenv("CG_GRAPH_UNROLLED");
             cudaKernelNodeParams kp;
             memset(&kp, 0, sizeof(kp));
-            kp.func = (void *)k_energy_to_host<R>;
-            kp.gridDim = dim3(nblk(s->N, 256));
-            kp.blockDim = dim3(256);
-            kp.kernelParams = args;
+            void *args_e[] = {&a, &acc, &done, &d};
+            void *args_s[] = {&a, &nz, &dtv, &muv, &acc, &done, &d};
+            if (energy_in_spp(s, unrolled && unrolled[0] == '1')) {
+                kp.func = (void *)k_spp_energy<R>;
+                kp.gridDim = dim3(nblk((s->N + 1) / 2, SPP_BLOCK));
+                kp.blockDim = dim3(SPP_BLOCK);
+                kp.kernelParams = args_s;
+            } else {
+                kp.func = (void *)k_energy_to_host<R>;
+                kp.gridDim = dim3(nblk(s->N, 256));
+                kp.blockDim = dim3(256);
+                kp.kernelParams = args_e;
+            }
             CG_CUDA(cudaGraphExecKernelNodeSetParams(g.exec, g.energy_node, &kp));
             CG_CUDA(cudaGraphLaunch(g.exec, s->stream));
             s->kernels_enqueued += g.kernels;

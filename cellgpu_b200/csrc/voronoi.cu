@@ -1982,6 +1982,18 @@ __global__ void k_energy_from_fix(int n, unsigned long long *Efix, double *E)
     w[0] = w[1] = w[2] = 0ull;
 }
 
+// the energy of cell c from its A/P and preferences (half its line-tension sum: each unlike edge
+// is counted by both of its cells)
+template <typename R>
+CG_D double cell_energy(const VoroArgs &a, int c)
+{
+    typename Vec2<R>::T ap = reinterpret_cast<typename Vec2<R>::T *>(a.AP)[c];
+    double da = (double)ap.x - a.APpref[c].x, dp = (double)ap.y - a.APpref[c].y;
+    double e = a.KA * da * da + a.KP * dp * dp;
+    if (a.TE) e += 0.5 * a.TE[c];
+    return e;
+}
+
 // The same sums written straight into page-locked host memory (host_out: its device address):
 // block partials gather in acc (zero between calls); the last block to finish stores the totals
 // to the host buffer and clears acc and its counter for the next call. One kernel replaces a
@@ -1997,10 +2009,7 @@ __global__ void __launch_bounds__(256) k_energy_to_host(VoroArgs a, double *acc,
     double e = 0.0;
     int inst = 0;
     if (c < a.N) {
-        typename Vec2<R>::T ap = reinterpret_cast<typename Vec2<R>::T *>(a.AP)[c];
-        double da = (double)ap.x - a.APpref[c].x, dp = (double)ap.y - a.APpref[c].y;
-        e = a.KA * da * da + a.KP * dp * dp;
-        if (a.TE) e += 0.5 * a.TE[c];
+        e = cell_energy<R>(a, c);
         inst = a.cell_inst ? a.cell_inst[c] : 0;
     }
     const int c0 = blockIdx.x * blockDim.x, c1 = min(a.N, c0 + (int)blockDim.x) - 1;
@@ -2037,6 +2046,71 @@ __global__ void __launch_bounds__(256) k_energy_to_host(VoroArgs a, double *acc,
                 unsigned long long v = atomicExch(reinterpret_cast<unsigned long long *>(&acc[i]), 0ull);
                 host_out[i] = __longlong_as_double((long long)v);
             }
+        }
+        __threadfence_system();
+        if (threadIdx.x == 0) *done = 0u;
+    }
+}
+
+// The step's integration with its energy readout (host-energy steps with floating-point force
+// sums): k_spp's two cells per thread, whose energies (of the configuration the forces were
+// computed on: A/P are not changed by the move) are summed per block of 256 cells and per instance
+// as k_energy_to_host sums them, the last block storing the totals to the host buffer. One kernel
+// instead of the integrator and a separate readout after the step's epilogue.
+template <typename R>
+__global__ void __launch_bounds__(128) k_spp_energy(VoroArgs a, const double *noise, double dt, double mu, double *acc,
+                                                    unsigned *done, double *host_out)
+{
+    __shared__ double s_part[4];
+    __shared__ int s_last;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    Ctl *ctl = a.ctl;
+    const int c0 = 2 * t;
+    const bool one = c0 < a.N, two = c0 + 1 < a.N;
+    double e0 = 0.0, e1 = 0.0;
+    int n0 = 0, n1 = 0;
+    if (one) {
+        e0 = cell_energy<R>(a, c0);
+        n0 = a.cell_inst ? a.cell_inst[c0] : 0;
+    }
+    if (two) {
+        e1 = cell_energy<R>(a, c0 + 1);
+        n1 = a.cell_inst ? a.cell_inst[c0 + 1] : 0;
+    }
+    if (one && !(ctl && ctl->halt)) {  // a halted step does not move (the host recovers it)
+        double2 xi;
+        if (noise) xi = make_double2(noise[c0], two ? noise[c0 + 1] : 0.0);
+        else xi = pair_draw(a, c0, ctl ? (uint32_t)ctl->step : 0u);
+        spp_cell<R>(a, c0, xi.x, dt, mu, 0);
+        if (two) spp_cell<R>(a, c0 + 1, xi.y, dt, mu, 0);
+    }
+    const int b0 = 2 * blockIdx.x * blockDim.x, b1 = min(a.N, b0 + 2 * (int)blockDim.x) - 1;
+    const int i0 = a.cell_inst ? a.cell_inst[b0] : 0, i1 = a.cell_inst ? a.cell_inst[b1] : 0;
+    if (i0 == i1) {
+        double e = e0 + e1;
+        for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
+        if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = e;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tsum = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tsum += s_part[w];
+            atomicAdd(&acc[i0], tsum);
+        }
+    } else {
+        if (one) atomicAdd(&acc[n0], e0);
+        if (two) atomicAdd(&acc[n1], e1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        for (int i = threadIdx.x; i < a.n_inst; i += blockDim.x) {
+            unsigned long long v = atomicExch(reinterpret_cast<unsigned long long *>(&acc[i]), 0ull);
+            host_out[i] = __longlong_as_double((long long)v);
         }
         __threadfence_system();
         if (threadIdx.x == 0) *done = 0u;
