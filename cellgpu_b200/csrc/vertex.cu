@@ -153,16 +153,34 @@ __global__ void __launch_bounds__(WPB * 32) k_vm_forces_groups(VertArgs a, int s
     const int c = (blockIdx.x * WPB + w) * GPW_ + gi;
     bool live = c < a.Nc;
     if (a.ctl && a.ctl->halt) live = false;  // uniform across the grid
+    // the row's entries (rows are allocated vmax wide), its length, the instance and the
+    // preferences are loaded together; then the vertex positions: two dependent loads before the
+    // arithmetic
+    const int *row = a.cv + (size_t)(live ? c : 0) * a.vmax;
     int z = live ? a.cvn[c] : 0;
+    int ent[VM_ROW_G / VM_G];
+#pragma unroll
+    for (int r = 0; r < VM_ROW_G / VM_G; ++r) {
+        const int k = gl + VM_G * r;
+        ent[r] = (live && k < a.vmax) ? row[k] : -1;
+    }
+    const double2 pref = live ? a.APpref[c] : make_double2(0.0, 0.0);
+    const int ci = live ? a.cell_inst[c] : 0;
     const bool ok = live && z >= 3 && z <= VM_ROW_G;
-    const int *row = a.cv + (size_t)(ok ? c : 0) * a.vmax;
+    // the reference vertex (slot z - 2) from the lane of the group that holds it
+    const int zz = ok ? z - 2 : 0;
+    int mine = ent[0];
+#pragma unroll
+    for (int r = 1; r < VM_ROW_G / VM_G; ++r)
+        if ((zz / VM_G) == r) mine = ent[r];
+    const int vref = __shfl_sync(0xffffffffu, mine, (lane & ~(VM_G - 1)) + (zz & (VM_G - 1)));
     double Lx = 1.0, Ly = 1.0;
     double2 cp = make_double2(0.0, 0.0);
     if (ok) {
-        const Inst &in = a.inst[a.cell_inst[c]];
+        const Inst &in = a.inst[ci];
         Lx = in.Lx;
         Ly = in.Ly;
-        cp = a.vpos[row[z - 2]];
+        cp = a.vpos[vref];
     }
     int vid[VM_ROW_G / VM_G];
 #pragma unroll
@@ -170,7 +188,7 @@ __global__ void __launch_bounds__(WPB * 32) k_vm_forces_groups(VertArgs a, int s
         int k = gl + VM_G * r;
         vid[r] = -1;
         if (ok && k < z) {
-            vid[r] = row[k];
+            vid[r] = ent[r];
             sV[sl][k] = min_dist(a.vpos[vid[r]], cp, Lx, Ly);
         }
     }
@@ -200,8 +218,8 @@ __global__ void __launch_bounds__(WPB * 32) k_vm_forces_groups(VertArgs a, int s
     if (!scatter) return;  // uniform
     double Adiff = 0.0, Pdiff = 0.0, te = 0.0;
     if (ok) {
-        Adiff = a.KA * (A - a.APpref[c].x);
-        Pdiff = a.KP * (P - a.APpref[c].y);
+        Adiff = a.KA * (A - pref.x);
+        Pdiff = a.KP * (P - pref.y);
     }
 #pragma unroll
     for (int r = 0; r < VM_ROW_G / VM_G; ++r) {
