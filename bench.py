@@ -353,6 +353,35 @@ def bench_batched(cg, torch, flush, steps=5000, equil=150, plain_steps=20, plain
     return out
 
 
+def profile_c4_steps(cg, torch, steps):
+    """A profiler target: the C4 ensemble prepared as bench_batched prepares it (150 steps from the
+    random state, spatial sort, autotune, repair autotune), 200 further steps, then `steps` steps
+    with supplied noise through plain launches, so that every kernel is a launch of its own, with
+    the CUDA profiler switched on for those steps only (ncu --profile-from-start off). Returns the
+    counters of those steps."""
+    Ns, boxes, pos, theta, p0, v0 = c4_ensemble()
+    b = cg.VoronoiBatch(list(Ns), boxes, precision=cg.CG_FP64)
+    b.set_positions(np.concatenate(pos))
+    b.set_directors(np.concatenate(theta))
+    b.set_motility(np.concatenate([np.tile([v, 1.0], (n, 1)) for n, v in zip(Ns, v0)]))
+    b.set_preferences(np.concatenate([np.tile([1.0, p], (n, 1)) for n, p in zip(Ns, p0)]))
+    b.triangulate()
+    b.spp_run(150, dt=DT, mu=MU)
+    b.spatial_sort()
+    b.autotune()
+    b.autotune_repair(REPAIR_TUNE_STEPS, dt=DT, mu=MU)
+    b.spp_run(200, dt=DT, mu=MU)
+    noise = torch.randn(steps, int(Ns.sum()), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    c0 = b.counters()
+    torch.cuda.profiler.start()
+    b.spp_run(steps, dt=DT, mu=MU, noise=noise)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    c1 = b.counters()
+    return {k: c1[k] - c0[k] for k in c1}
+
+
 def bench_c1(cg, torch, flush, steps=1000, cpu=True):
     """The reference's own small case (plain FP64, single instance, the drop-in's latency case): N = 300
     cells in a box of side sqrt(N) from seeded uniform positions, A0 = 1, p0 = 3.8, SPP v0 = 0.05,
@@ -553,6 +582,9 @@ def main():
                     help="c2: the headline line (default); c3 / c4: only the vertex-model or the "
                          "batched-ensemble measurement, printed as one JSON line")
     ap.add_argument("--c3-steps", type=int, default=10000, help="Brownian steps of the c3 case")
+    ap.add_argument("--c4-profile-steps", type=int, default=0,
+                    help="with --case c4: prepare the ensemble, run this many plain-launch steps with "
+                         "the CUDA profiler on, print their counters and exit (a profiler target)")
     ap.add_argument("--no-sort", action="store_true",
                     help="time the equilibrated monolayer in its creation order (no spatial re-sort)")
     ap.add_argument("--equilibrate", type=int, default=300,
@@ -602,6 +634,8 @@ def main():
             flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
             if args.case == "c3":
                 out = {"c3_vertex": bench_vertex(cg, torch, flush, steps=max(1001, args.c3_steps))}
+            elif args.c4_profile_steps > 0:
+                out = {"c4_profile_counters": profile_c4_steps(cg, torch, args.c4_profile_steps)}
             else:
                 out = {"c4_ensemble": bench_batched(cg, torch, flush)}
             print(json.dumps({"metric": METRIC, "impl": "ours", "n_gpus": 1, "case": args.case, **out}))
