@@ -578,9 +578,9 @@ def main():
                     help="requests in the serving extra (about 2.5 minutes for 2000); 0 skips it")
     ap.add_argument("--serve-only", action="store_true",
                     help="run only the serving stream and print its JSON line")
-    ap.add_argument("--case", default="c2", choices=["c2", "c3", "c4"],
-                    help="c2: the headline line (default); c3 / c4: only the vertex-model or the "
-                         "batched-ensemble measurement, printed as one JSON line")
+    ap.add_argument("--case", default="c2", choices=["c1", "c2", "c3", "c4"],
+                    help="c2: the headline line (default); c1 / c3 / c4: only the small plain case, the "
+                         "vertex-model or the batched-ensemble measurement, printed as one JSON line")
     ap.add_argument("--c3-steps", type=int, default=10000, help="Brownian steps of the c3 case")
     ap.add_argument("--c4-profile-steps", type=int, default=0,
                     help="with --case c4: prepare the ensemble, run this many plain-launch steps with "
@@ -632,7 +632,9 @@ def main():
     if args.case != "c2":
         if rank == 0:
             flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-            if args.case == "c3":
+            if args.case == "c1":
+                out = {"c1_plain": bench_c1(cg, torch, flush, cpu=not args.no_cpu_baseline)}
+            elif args.case == "c3":
                 out = {"c3_vertex": bench_vertex(cg, torch, flush, steps=max(1001, args.c3_steps))}
             elif args.c4_profile_steps > 0:
                 out = {"c4_profile_counters": profile_c4_steps(cg, torch, args.c4_profile_steps)}
