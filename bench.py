@@ -354,7 +354,7 @@ def bench_batched(cg, torch, flush, steps=5000, equil=150, plain_steps=20, plain
 
 
 def profile_c4_steps(cg, torch, steps):
-    """A profiler target: the C4 ensemble prepared as bench_batched prepares it (150 steps from the
+    """A profiler target: the 512-monolayer ensemble prepared as bench_batched prepares it (150 steps from the
     random state, spatial sort, autotune, repair autotune), 200 further steps, then `steps` steps
     with supplied noise through plain launches, so that every kernel is a launch of its own, with
     the CUDA profiler switched on for those steps only (ncu --profile-from-start off). Returns the

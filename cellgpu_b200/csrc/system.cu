@@ -82,7 +82,7 @@ static inline void launch_groups_ns(const VoroArgs &a, int N, cudaStream_t st, i
 // the thread-per-cell form (launch shape 2): FP64 forces summed with atomics, no line tension,
 // 16-slot padded rows; other systems run shape 0
 // (blocks of 2 warps: a block's registers and shared memory are freed when its slower warp ends,
-// which 4-warp blocks waited for longer; same occupancy, 48.1 against 48.5 us on C2)
+// which 4-warp blocks waited for longer; same occupancy, 48.1 against 48.5 us on a 262144-cell monolayer)
 #ifndef CG_THREAD_TPB
 #define CG_THREAD_TPB 64
 #endif
